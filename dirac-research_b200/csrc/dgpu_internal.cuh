@@ -1,0 +1,44 @@
+// Internal helpers shared by the CUDA translation units of libdiracgpu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "dirac_gpu.h"
+
+namespace dgpu {
+
+#define DGPU_CHECK_CUDA(expr)                                 \
+    do {                                                      \
+        cudaError_t _e = (expr);                              \
+        if (_e != cudaSuccess) {                              \
+            dgpu::set_last_cuda_error(_e, #expr, __FILE__, __LINE__); \
+            return DGPU_ERR_CUDA;                             \
+        }                                                     \
+    } while (0)
+
+// Every kernel launch of the library goes through this check, which also counts it
+// (dgpu_launch_count reports the running total).
+#define DGPU_CHECK_LAUNCH()                  \
+    do {                                     \
+        dgpu::count_launch();                \
+        DGPU_CHECK_CUDA(cudaGetLastError()); \
+    } while (0)
+
+void count_launch();
+
+void set_last_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Per-device scratch owned by the library: used when a caller passes scratch == NULL.
+// Grown with cudaMalloc on demand (synchronising the device first so that no kernel still
+// in flight uses the old buffer), kept until process exit.
+int library_scratch(size_t bytes, void** out);
+
+__host__ __device__ inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+}  // namespace dgpu

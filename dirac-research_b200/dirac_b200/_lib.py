@@ -1,0 +1,96 @@
+"""ctypes binding of libdiracgpu.so, the sm_100a C ABI declared in include/dirac_gpu.h.
+
+The library is built in place (``make -C dirac-research_b200``).  Importing this module
+fails loudly when it is missing: there is no CPU fallback for any entry point.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "libdiracgpu.so")
+
+DGPU_OK = 0
+ERRORS = {
+    -1: "DGPU_ERR_ARG",
+    -2: "DGPU_ERR_SIZE",
+    -3: "DGPU_ERR_CUDA",
+    -4: "DGPU_ERR_NOMEM",
+    -5: "DGPU_ERR_DEVICE",
+}
+
+
+class DgpuError(RuntimeError):
+    """A libdiracgpu entry point returned a negative status."""
+
+    def __init__(self, code, what=""):
+        self.code = code
+        name = ERRORS.get(code, str(code))
+        detail = ""
+        if code == -3 and _lib is not None:
+            detail = " (" + _lib.dgpu_last_error().decode(errors="replace") + ")"
+        super().__init__(f"{what}: {name}{detail}")
+
+
+_lib = None
+
+c_int = ctypes.c_int
+c_void_p = ctypes.c_void_p
+c_size_t = ctypes.c_size_t
+P_int = ctypes.POINTER(ctypes.c_int)
+P_void = ctypes.POINTER(ctypes.c_void_p)
+
+# name -> (restype, argtypes); mirrors include/dirac_gpu.h
+SIGNATURES = {
+    "dgpu_version": (ctypes.c_char_p, []),
+    "dgpu_device_check": (c_int, []),
+    "dgpu_last_error": (ctypes.c_char_p, []),
+    "dgpu_launch_count": (ctypes.c_ulonglong, []),
+    "dgpu_dwt_scratch_bytes": (c_size_t, [c_int, c_int, c_int]),
+    "dgpu_wavelet_transform": (
+        c_int,
+        [c_int, c_int, c_int, c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_int, c_int,
+         c_void_p, c_size_t, c_void_p],
+    ),
+    "dgpu_wavelet_transform_batch": (
+        c_int,
+        [c_int, c_int, P_int, P_int, P_void, P_int, P_int, P_int, P_void, P_int, P_int, P_int,
+         c_void_p, c_size_t, c_void_p],
+    ),
+    "dgpu_wavelet_transform_host": (
+        c_int,
+        [c_int, c_int, c_int, c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_int, c_int],
+    ),
+}
+
+
+def load(path=LIB_PATH):
+    """Load the library (once) and declare every entry point's signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"{path} is missing: build it with `make -C dirac-research_b200` "
+            "(the Dirac GPU path has no CPU fallback)"
+        )
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc, what):
+    if rc != DGPU_OK:
+        raise DgpuError(rc, what)
+    return rc
+
+
+def int_array(values):
+    return (ctypes.c_int * len(values))(*values)
+
+
+def ptr_array(values):
+    return (ctypes.c_void_p * len(values))(*values)

@@ -1,0 +1,102 @@
+/*
+ * dirac_gpu.h -- C ABI of the B200 (sm_100a) implementation of the Dirac research codec's
+ * data-parallel coding hot path.
+ *
+ * Every entry point takes plain pointers and sizes.  Unless the name ends in _host, array
+ * pointers are CUDA device pointers, `stream` is a cudaStream_t passed as void* (NULL =
+ * the legacy default stream) and the call is asynchronous on that stream.  Entry points
+ * return DGPU_OK (0) or a negative DGPU_ERR_* code; no C++ exception or CUDA error crosses
+ * this boundary (the reference turns its DiracException into return codes at its own C API
+ * the same way, libdirac_encoder/dirac_encoder.cpp:1074-1085).
+ *
+ * Sample conventions follow the reference: pictures are int16 (ValueType, 8-bit video is
+ * stored as u8 - 128, libdirac_common/pic_io.cpp:388-399) and wavelet coefficients are int32
+ * (CoeffType of the reference's plain-C build, libdirac_common/common.h:72-78).  Strides are
+ * in elements.
+ */
+#ifndef DIRAC_GPU_H
+#define DIRAC_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DGPU_OK 0
+#define DGPU_ERR_ARG (-1)     /* invalid argument (null pointer, bad enum, bad stride)   */
+#define DGPU_ERR_SIZE (-2)    /* size outside what the reference's algorithm defines     */
+#define DGPU_ERR_CUDA (-3)    /* a CUDA runtime call or kernel launch failed            */
+#define DGPU_ERR_NOMEM (-4)   /* device or host allocation failed / scratch too small    */
+#define DGPU_ERR_DEVICE (-5)  /* no usable sm_100 device                                 */
+
+/* Filters: numbering of the reference's WltFilter (libdirac_common/common_types.h:61-71).
+ * FIDELITY and any unknown value select DAUB9_7, as the reference's WaveletTransform
+ * constructor does (libdirac_common/wavelet_utils.cpp:406-435). */
+#define DGPU_DD9_7 0
+#define DGPU_LEGALL5_3 1
+#define DGPU_DD13_7 2
+#define DGPU_HAAR0 3
+#define DGPU_HAAR1 4
+#define DGPU_FIDELITY 5
+#define DGPU_DAUB9_7 6
+
+/* Direction: numbering of the reference's Direction (libdirac_common/common.h:93). */
+#define DGPU_FORWARD 0
+#define DGPU_BACKWARD 1
+
+/* Library version string; the compute capability (e.g. 100) of the current device, or
+ * DGPU_ERR_DEVICE when it is not an sm_100 part; text of the last CUDA failure. */
+const char* dgpu_version(void);
+int dgpu_device_check(void);
+const char* dgpu_last_error(void);
+
+/* Running total of kernel launches issued by this library in this process. */
+unsigned long long dgpu_launch_count(void);
+
+/* ---------------------------------------------------------------------------------------
+ * Wavelet transform
+ * Replaces WaveletTransform::Transform(Direction, PicArray&, CoeffArray&)
+ * (libdirac_common/wavelet_utils.h:700-718, wavelet_utils.cpp:440-485).
+ *
+ * pic: h x w int16 picture component.  coeff: ch x cw int32 array whose sides are the
+ * picture sides padded up to a multiple of 2^depth (Picture::InitWltData,
+ * libdirac_common/picture.cpp:201-219).  FORWARD replicates the last column/row into the
+ * padding and leaves coeff in the reference's Mallat layout (LL top-left, then HL, LH, HH
+ * per level).  BACKWARD reads coeff (left unchanged, unlike the reference's in-place
+ * synthesis, whose leftover contents no caller reads) and writes pic with the reference's
+ * truncating int32 -> int16 cast.  Every level side (cw >> (depth-1), ch >> (depth-1)) must
+ * be at least 6 for DD9_7/DD13_7, 4 for LEGALL5_3/DAUB9_7 and 2 for HAAR0/HAAR1.
+ *
+ * scratch: device memory of at least dgpu_dwt_scratch_bytes(cw, ch, depth) bytes holding the
+ * intermediate low-pass bands, or NULL to let the library use its own per-device buffer
+ * (grown with cudaMalloc on first use).
+ * ------------------------------------------------------------------------------------- */
+size_t dgpu_dwt_scratch_bytes(int cw, int ch, int depth);
+
+int dgpu_wavelet_transform(int direction, int filter, int depth,
+                           int16_t* pic, int w, int h, int pic_stride,
+                           int32_t* coeff, int cw, int ch, int coeff_stride,
+                           void* scratch, size_t scratch_bytes, void* stream);
+
+/* Several components / pictures in one launch per level: n transforms described by
+ * parallel arrays (each entry as in dgpu_wavelet_transform; all share `direction`).
+ * scratch must hold the sum of dgpu_dwt_scratch_bytes over the entries (each entry's share
+ * starting on a 256-byte boundary), or be NULL. */
+int dgpu_wavelet_transform_batch(int direction, int n, const int* filter, const int* depth,
+                                 int16_t* const* pic, const int* w, const int* h,
+                                 const int* pic_stride, int32_t* const* coeff, const int* cw,
+                                 const int* ch, const int* coeff_stride, void* scratch,
+                                 size_t scratch_bytes, void* stream);
+
+/* Host-buffer form of dgpu_wavelet_transform (the reference's calling convention: caller
+ * memory in host RAM).  Copies in, transforms, copies out, synchronises. */
+int dgpu_wavelet_transform_host(int direction, int filter, int depth,
+                                int16_t* pic, int w, int h, int pic_stride,
+                                int32_t* coeff, int cw, int ch, int coeff_stride);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DIRAC_GPU_H */

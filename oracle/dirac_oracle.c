@@ -1,0 +1,301 @@
+/*
+ * dirac_oracle.c -- TEST INFRASTRUCTURE ONLY (see dirac_oracle.h).
+ *
+ * Plain-C restatement of the Dirac hot path used as the parity checker for the CUDA
+ * kernels and as the timed CPU baseline.  Written from the reference's behaviour, not
+ * copied: the per-filter edge formulas of libdirac_common/wavelet_utils.cpp are expressed
+ * through a single rule (a neighbour index is clamped inside its own parity
+ * subsequence), which reproduces every explicit edge case of the reference for level
+ * sides >= orc_dwt_min_len(filter).
+ */
+#include "dirac_oracle.h"
+
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------------------------ */
+/* Wavelet transform                                                                     */
+/* ------------------------------------------------------------------------------------ */
+
+/* Kinds of lifting step (libdirac_common/wavelet_utils.h:490-616). */
+enum { LIFT_SHIFT2 = 0,  /* PredictStepShift/UpdateStepShift: (a+b+2^(s-1))>>s      */
+       LIFT_FOURTAP = 1, /* *StepFourTap<s,t1,t2>: (t1(a+b)+t2(c+d)+2^(s-1))>>s      */
+       LIFT_97 = 2,      /* *Step97<g>: (g*(a+b))>>12                                */
+       LIFT_HAAR = 3 };  /* Haar pair step (wavelet_utils.cpp:1342-1489)             */
+
+typedef struct {
+    int parity; /* 1: odd samples are updated from even ones; 0: the reverse */
+    int sign;   /* -1: "predict" (subtract), +1: "update" (add) */
+    int kind;
+    int shift, t1, t2, gain;
+} lift_step;
+
+typedef struct {
+    int nsteps;
+    int shift; /* ShiftRowLeft before analysis / ShiftRowRight after synthesis */
+    lift_step step[4];
+} filter_def;
+
+/* Analysis steps in order; synthesis runs them in reverse with the opposite sign.
+ * DD9_7   wavelet_utils.cpp:952-1042   LEGALL5_3 :805-877   DD13_7 :1136-1233
+ * HAAR0/1 :1342-1450                   DAUB9_7  :575-690 (also FIDELITY and unknown
+ * filters, which the WaveletTransform constructor maps to DAUB9_7, :406-435). */
+static filter_def get_filter(int filter) {
+    filter_def f;
+    memset(&f, 0, sizeof(f));
+    switch (filter) {
+    case ORC_DD9_7:
+        f.nsteps = 2; f.shift = 1;
+        f.step[0] = (lift_step){1, -1, LIFT_FOURTAP, 4, 9, -1, 0};
+        f.step[1] = (lift_step){0, +1, LIFT_SHIFT2, 2, 0, 0, 0};
+        break;
+    case ORC_LEGALL5_3:
+        f.nsteps = 2; f.shift = 1;
+        f.step[0] = (lift_step){1, -1, LIFT_SHIFT2, 1, 0, 0, 0};
+        f.step[1] = (lift_step){0, +1, LIFT_SHIFT2, 2, 0, 0, 0};
+        break;
+    case ORC_DD13_7:
+        f.nsteps = 2; f.shift = 1;
+        f.step[0] = (lift_step){1, -1, LIFT_FOURTAP, 4, 9, -1, 0};
+        f.step[1] = (lift_step){0, +1, LIFT_FOURTAP, 5, 9, -1, 0};
+        break;
+    case ORC_HAAR0:
+    case ORC_HAAR1:
+        f.nsteps = 2; f.shift = (filter == ORC_HAAR1) ? 1 : 0;
+        f.step[0] = (lift_step){1, -1, LIFT_HAAR, 0, 0, 0, 0};
+        f.step[1] = (lift_step){0, +1, LIFT_HAAR, 0, 0, 0, 0};
+        break;
+    default: /* DAUB9_7, FIDELITY, anything else */
+        f.nsteps = 4; f.shift = 1;
+        f.step[0] = (lift_step){1, -1, LIFT_97, 0, 0, 0, 6497};
+        f.step[1] = (lift_step){0, -1, LIFT_97, 0, 0, 0, 217};
+        f.step[2] = (lift_step){1, +1, LIFT_97, 0, 0, 0, 3616};
+        f.step[3] = (lift_step){0, +1, LIFT_97, 0, 0, 0, 1817};
+        break;
+    }
+    return f;
+}
+
+int orc_dwt_min_len(int filter) {
+    switch (filter) {
+    case ORC_DD9_7:
+    case ORC_DD13_7: return 6;
+    case ORC_HAAR0:
+    case ORC_HAAR1: return 2;
+    default: return 4;
+    }
+}
+
+static inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+/* One lifting step over a 1-D sequence x[0], x[s], ... x[(n-1)s] (n even).
+ * Target sample k = 2m+parity reads the other parity's subsequence q at
+ *   near: q[m-1+parity], q[m+parity]      far: q[m-2+parity], q[m+1+parity]
+ * with the subsequence index clamped to [0, n/2-1]. */
+static void lift_1d(int32_t* x, int n, int s, const lift_step* st, int sign) {
+    const int half = n >> 1;
+    const int other = 1 - st->parity;
+    for (int m = 0; m < half; ++m) {
+        const int p = st->parity;
+        const int ia = clampi(m - 1 + p, 0, half - 1);
+        const int ib = clampi(m + p, 0, half - 1);
+        const int a = x[(2 * ia + other) * s];
+        const int b = x[(2 * ib + other) * s];
+        int d;
+        switch (st->kind) {
+        case LIFT_SHIFT2:
+            d = (a + b + (1 << (st->shift - 1))) >> st->shift;
+            break;
+        case LIFT_FOURTAP: {
+            const int ic = clampi(m - 2 + p, 0, half - 1);
+            const int id = clampi(m + 1 + p, 0, half - 1);
+            const int c = x[(2 * ic + other) * s];
+            const int e = x[(2 * id + other) * s];
+            d = (st->t1 * (a + b) + st->t2 * (c + e) + (1 << (st->shift - 1))) >> st->shift;
+            break;
+        }
+        case LIFT_97:
+            d = (st->gain * (a + b)) >> 12;
+            break;
+        default: /* Haar: odd uses its left even partner, even uses its right odd partner */
+            d = p ? a : ((b + 1) >> 1);
+            break;
+        }
+        int32_t* t = &x[(2 * m + p) * s];
+        *t = (sign < 0) ? (*t - d) : (*t + d);
+    }
+}
+
+/* Mallat reorder of an xl x yl region (VHFilter::DeInterleave, wavelet_utils.cpp:540-573). */
+static void deinterleave(int32_t* c, int stride, int xl, int yl, int32_t* tmp) {
+    for (int j = 0; j < yl; ++j) memcpy(tmp + (size_t)j * xl, c + (size_t)j * stride, sizeof(int32_t) * xl);
+    const int xl2 = xl >> 1, yl2 = yl >> 1;
+    for (int j = 0; j < yl; ++j)
+        for (int i = 0; i < xl; ++i)
+            c[(size_t)((j & 1) * yl2 + (j >> 1)) * stride + (i & 1) * xl2 + (i >> 1)] = tmp[(size_t)j * xl + i];
+}
+
+/* VHFilter::Interleave, wavelet_utils.cpp:491-523. */
+static void interleave(int32_t* c, int stride, int xl, int yl, int32_t* tmp) {
+    for (int j = 0; j < yl; ++j) memcpy(tmp + (size_t)j * xl, c + (size_t)j * stride, sizeof(int32_t) * xl);
+    const int xl2 = xl >> 1, yl2 = yl >> 1;
+    for (int j = 0; j < yl; ++j)
+        for (int i = 0; i < xl; ++i)
+            c[(size_t)j * stride + i] = tmp[(size_t)((j & 1) * yl2 + (j >> 1)) * xl + (i & 1) * xl2 + (i >> 1)];
+}
+
+/* One analysis level on the top-left xl x yl region (VHFilter*::Split). */
+static void split_level(const filter_def* f, int32_t* c, int stride, int xl, int yl, int32_t* tmp) {
+    for (int j = 0; j < yl; ++j) {
+        int32_t* row = c + (size_t)j * stride;
+        if (f->shift)
+            for (int i = 0; i < xl; ++i) row[i] = (int32_t)((uint32_t)row[i] << f->shift);
+        for (int k = 0; k < f->nsteps; ++k) lift_1d(row, xl, 1, &f->step[k], f->step[k].sign);
+    }
+    for (int i = 0; i < xl; ++i)
+        for (int k = 0; k < f->nsteps; ++k) lift_1d(c + i, yl, stride, &f->step[k], f->step[k].sign);
+    deinterleave(c, stride, xl, yl, tmp);
+}
+
+/* One synthesis level (VHFilter*::Synth): vertical then horizontal, then ShiftRowRight. */
+static void synth_level(const filter_def* f, int32_t* c, int stride, int xl, int yl, int32_t* tmp) {
+    interleave(c, stride, xl, yl, tmp);
+    for (int i = 0; i < xl; ++i)
+        for (int k = f->nsteps - 1; k >= 0; --k) lift_1d(c + i, yl, stride, &f->step[k], -f->step[k].sign);
+    for (int j = 0; j < yl; ++j) {
+        int32_t* row = c + (size_t)j * stride;
+        for (int k = f->nsteps - 1; k >= 0; --k) lift_1d(row, xl, 1, &f->step[k], -f->step[k].sign);
+        if (f->shift) {
+            const int half = 1 << (f->shift - 1);
+            for (int i = 0; i < xl; ++i) row[i] = (row[i] + half) >> f->shift;
+        }
+    }
+}
+
+static int dwt_check(int filter, int depth, int cw, int ch) {
+    if (depth < 1 || depth > 8 || cw <= 0 || ch <= 0) return -1;
+    const int mul = 1 << depth;
+    if (cw % mul || ch % mul) return -2;
+    const int minlen = orc_dwt_min_len(filter);
+    if ((cw >> (depth - 1)) < minlen || (ch >> (depth - 1)) < minlen) return -3;
+    return 0;
+}
+
+/* WaveletTransform::Transform FORWARD (wavelet_utils.cpp:446-466). */
+int orc_dwt_forward(int filter, int depth, const int16_t* pic, int w, int h, int pic_stride,
+                    int32_t* coeff, int cw, int ch, int coeff_stride) {
+    int rc = dwt_check(filter, depth, cw, ch);
+    if (rc) return rc;
+    if (w <= 0 || h <= 0 || w > cw || h > ch) return -4;
+    /* pad-copy: the last column and row are replicated into the padding */
+    for (int j = 0; j < ch; ++j) {
+        const int16_t* src = pic + (size_t)(j < h ? j : h - 1) * pic_stride;
+        int32_t* dst = coeff + (size_t)j * coeff_stride;
+        for (int i = 0; i < cw; ++i) dst[i] = src[i < w ? i : w - 1];
+    }
+    const filter_def f = get_filter(filter);
+    int32_t* tmp = (int32_t*)malloc(sizeof(int32_t) * (size_t)cw * ch);
+    if (!tmp) return -5;
+    for (int l = 1, xl = cw, yl = ch; l <= depth; ++l, xl >>= 1, yl >>= 1)
+        split_level(&f, coeff, coeff_stride, xl, yl, tmp);
+    free(tmp);
+    return 0;
+}
+
+/* WaveletTransform::Transform BACKWARD (wavelet_utils.cpp:467-484). */
+int orc_dwt_backward(int filter, int depth, int32_t* coeff, int cw, int ch, int coeff_stride,
+                     int16_t* pic, int w, int h, int pic_stride) {
+    int rc = dwt_check(filter, depth, cw, ch);
+    if (rc) return rc;
+    if (w <= 0 || h <= 0 || w > cw || h > ch) return -4;
+    const filter_def f = get_filter(filter);
+    int32_t* tmp = (int32_t*)malloc(sizeof(int32_t) * (size_t)cw * ch);
+    if (!tmp) return -5;
+    for (int l = 1, xl = cw >> (depth - 1), yl = ch >> (depth - 1); l <= depth; ++l, xl <<= 1, yl <<= 1)
+        synth_level(&f, coeff, coeff_stride, xl, yl, tmp);
+    free(tmp);
+    for (int j = 0; j < h; ++j)
+        for (int i = 0; i < w; ++i) pic[(size_t)j * pic_stride + i] = (int16_t)coeff[(size_t)j * coeff_stride + i];
+    return 0;
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* Half-pel upconversion (UpConverter::DoUpConverter / RowLoop, upconvert.cpp:55-200)     */
+/* ------------------------------------------------------------------------------------ */
+
+static const int up_taps[4] = {21, -7, 3, -1};
+
+/* The reference accumulates in a ValueType (int16) `sum`, truncating after every add;
+   the casts below reproduce that. */
+int orc_upconvert(const int16_t* pic, int w, int h, int stride, int bit_depth, int16_t* up, int up_stride) {
+    if (w < 8 || h < 8 || bit_depth < 2 || bit_depth > 16) return -1;
+    const int lo = -(1 << (bit_depth - 1)), hi = (1 << (bit_depth - 1)) - 1;
+    /* vertical pass: even up-rows copy, odd up-rows interpolate between source rows y, y+1
+       (source row indices clamped to [0, h-1]); only even up-columns are written here */
+    for (int y = 0; y < h; ++y) {
+        int16_t* even_row = up + (size_t)(2 * y) * up_stride;
+        int16_t* odd_row = up + (size_t)(2 * y + 1) * up_stride;
+        for (int x = 0; x < w; ++x) {
+            even_row[2 * x] = pic[(size_t)y * stride + x];
+            int16_t sum = 16;
+            for (int t = 0; t < 4; ++t) {
+                const int ya = clampi(y - t, 0, h - 1), yb = clampi(y + 1 + t, 0, h - 1);
+                sum = (int16_t)(sum + (pic[(size_t)ya * stride + x] + pic[(size_t)yb * stride + x]) * up_taps[t]);
+            }
+            sum = (int16_t)(sum >> 5);
+            odd_row[2 * x] = (int16_t)clampi(sum, lo, hi);
+        }
+    }
+    /* horizontal pass on every up-row: odd columns from the even ones (even-column index
+       clamped to [0, w-1]) */
+    for (int r = 0; r < 2 * h; ++r) {
+        int16_t* row = up + (size_t)r * up_stride;
+        for (int x = 0; x < w; ++x) {
+            int16_t sum = 16;
+            for (int t = 0; t < 4; ++t) {
+                const int xa = clampi(x - t, 0, w - 1), xb = clampi(x + 1 + t, 0, w - 1);
+                sum = (int16_t)(sum + (row[2 * xa] + row[2 * xb]) * up_taps[t]);
+            }
+            sum = (int16_t)(sum >> 5);
+            row[2 * x + 1] = (int16_t)clampi(sum, lo, hi);
+        }
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* 2x decimation (DownConverter::DoDownConvert / RowLoop, downconvert.cpp:51-204,        */
+/* taps downconvert.h:82-89)                                                             */
+/* ------------------------------------------------------------------------------------ */
+
+static const int down_taps[6] = {86, 46, 4, -8, -4, 4};
+
+int orc_downconvert(const int16_t* pic, int w, int h, int stride, int16_t* out, int out_stride) {
+    const int ow = w / 2, oh = h / 2;
+    const int xlen = 2 * ow, ylen = 2 * oh; /* an odd last row/column is not used */
+    if (ow < 12 || oh < 12) return -1;
+    int16_t* rowbuf = (int16_t*)malloc(sizeof(int16_t) * (size_t)xlen);
+    if (!rowbuf) return -5;
+    for (int r = 0; r < oh; ++r) {
+        const int y = 2 * r;
+        for (int x = 0; x < xlen; ++x) {
+            int sum = 128;
+            for (int t = 0; t < 6; ++t) {
+                const int ya = clampi(y - t, 0, ylen - 1), yb = clampi(y + 1 + t, 0, ylen - 1);
+                sum += (pic[(size_t)ya * stride + x] + pic[(size_t)yb * stride + x]) * down_taps[t];
+            }
+            rowbuf[x] = (int16_t)(sum >> 8);
+        }
+        for (int c = 0; c < ow; ++c) {
+            const int x = 2 * c;
+            int sum = 128;
+            for (int t = 0; t < 6; ++t) {
+                const int xa = clampi(x - t, 0, xlen - 1), xb = clampi(x + 1 + t, 0, xlen - 1);
+                sum += (rowbuf[xa] + rowbuf[xb]) * down_taps[t];
+            }
+            out[(size_t)r * out_stride + c] = (int16_t)(sum >> 8);
+        }
+    }
+    free(rowbuf);
+    return 0;
+}

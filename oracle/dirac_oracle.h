@@ -1,0 +1,49 @@
+/*
+ * dirac_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C restatement of the Dirac research codec's data-parallel hot path, written
+ * for this project from the reference's behaviour (each function cites the reference
+ * file:line it restates).  It is the checker the tests compare the CUDA path against and
+ * the CPU baseline bench.py times; nothing in the product links or loads it.
+ *
+ * Conventions: pictures are int16 (the reference's ValueType), wavelet coefficients int32
+ * (CoeffType of the plain-C build), arrays dense row-major with an explicit stride in
+ * elements.  Functions return 0 on success and a negative value on invalid arguments.
+ */
+#ifndef DIRAC_ORACLE_H
+#define DIRAC_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Filter numbering follows the reference's WltFilter (libdirac_common/common_types.h:61-71). */
+enum { ORC_DD9_7 = 0, ORC_LEGALL5_3 = 1, ORC_DD13_7 = 2, ORC_HAAR0 = 3, ORC_HAAR1 = 4,
+       ORC_FIDELITY = 5, ORC_DAUB9_7 = 6 };
+
+/* Smallest level-region side a filter handles with its regular edge rule. */
+int orc_dwt_min_len(int filter);
+
+/* Forward transform: pad-copy pic (w x h) into coeff (cw x ch, multiples of 2^depth),
+ * then depth analysis levels in place (Mallat layout). */
+int orc_dwt_forward(int filter, int depth, const int16_t* pic, int w, int h, int pic_stride,
+                    int32_t* coeff, int cw, int ch, int coeff_stride);
+
+/* Inverse transform: depth synthesis levels in place on coeff, then truncating copy of the
+ * top-left w x h into pic. */
+int orc_dwt_backward(int filter, int depth, int32_t* coeff, int cw, int ch, int coeff_stride,
+                     int16_t* pic, int w, int h, int pic_stride);
+
+/* 2x half-pel upconversion, up is (2h) x (2w). */
+int orc_upconvert(const int16_t* pic, int w, int h, int stride, int bit_depth, int16_t* up,
+                  int up_stride);
+
+/* 2x decimation; out is (h/2) x (w/2). */
+int orc_downconvert(const int16_t* pic, int w, int h, int stride, int16_t* out, int out_stride);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
