@@ -1,0 +1,282 @@
+// Half-pel upconversion and 2x decimation (the motion-estimation pyramid) for sm_100a.
+//
+// Upconversion replaces UpConverter::DoUpConverter (libdirac_common/upconvert.cpp:55-200):
+// even output rows/columns copy the source, odd ones come from the 8-tap filter
+// (21, -7, 3, -1) with +16 >> 5, accumulated in an int16 as the reference does, then clipped
+// to the sample range; rows first, then columns.  Decimation replaces
+// DownConverter::DoDownConvert (libdirac_motionest/downconvert.cpp:51-204): a 12-tap
+// separable filter (86, 46, 4, -8, -4, 4) with +128 >> 8, vertical into an int16 row buffer,
+// then horizontal.  Both reference loops clamp source indices at the picture edges (their
+// three-loop edge handling is a clamp for the sizes they accept), which the kernels apply
+// per sample.
+//
+// Layout: one CTA per 64 x 16 tile of source samples.  The upconverter stages the source
+// tile plus a 4-sample halo in shared memory, computes the vertical half-pel rows there,
+// then writes each source sample's 2 x 2 output quad; every output row segment is a
+// contiguous 256-byte run.  The decimator stages its vertically filtered row buffer in
+// shared memory and writes one output sample per thread.
+
+#include "dgpu_internal.cuh"
+
+namespace dgpu {
+namespace {
+
+constexpr int UTX = 64, UTY = 16, UH = 4;  // upconvert tile and halo
+constexpr int UP_THREADS = 256;
+
+struct UpJob {
+    const int16_t* src;
+    int16_t* dst;
+    int w, h, src_stride, dst_stride;
+    int lo, hi;  // clip range
+    int tiles_x, tile_begin;
+};
+constexpr int MAX_UP_JOBS = 32;
+struct UpJobs {
+    int njobs;
+    UpJob job[MAX_UP_JOBS];
+};
+
+__device__ __forceinline__ int16_t up_tap_sum(int a0, int b0, int a1, int b1, int a2, int b2, int a3, int b3) {
+    // int16 accumulator, truncated after every addition (upconvert.cpp:90-96)
+    int16_t s = 16;
+    s = (int16_t)(s + (a0 + b0) * 21);
+    s = (int16_t)(s + (a1 + b1) * -7);
+    s = (int16_t)(s + (a2 + b2) * 3);
+    s = (int16_t)(s + (a3 + b3) * -1);
+    return (int16_t)(s >> 5);
+}
+
+__global__ void __launch_bounds__(UP_THREADS) upconvert_kernel(const __grid_constant__ UpJobs jobs) {
+    __shared__ int16_t src[UTY + 2 * UH][UTX + 2 * UH];  // source tile + halo (clamped)
+    __shared__ int16_t vh[UTY][UTX + 2 * UH];             // vertical half-pel rows
+
+    int j = 0;
+    while (j + 1 < jobs.njobs && jobs.job[j + 1].tile_begin <= (int)blockIdx.x) ++j;
+    const UpJob& jb = jobs.job[j];
+    const int t = blockIdx.x - jb.tile_begin;
+    const int ty = t / jb.tiles_x, tx = t - ty * jb.tiles_x;
+    const int x0 = tx * UTX, y0 = ty * UTY;
+
+    for (int idx = threadIdx.x; idx < (UTY + 2 * UH) * (UTX + 2 * UH); idx += UP_THREADS) {
+        const int r = idx / (UTX + 2 * UH), c = idx - r * (UTX + 2 * UH);
+        const int gy = clampi(y0 - UH + r, 0, jb.h - 1);
+        const int gx = clampi(x0 - UH + c, 0, jb.w - 1);
+        src[r][c] = jb.src[(size_t)gy * jb.src_stride + gx];
+    }
+    __syncthreads();
+    // vertical half-pel sample between source rows y and y+1, for every staged column
+    for (int idx = threadIdx.x; idx < UTY * (UTX + 2 * UH); idx += UP_THREADS) {
+        const int r = idx / (UTX + 2 * UH), c = idx - r * (UTX + 2 * UH);
+        const int gy = y0 + r;
+        // source rows gy - t and gy + 1 + t, clamped to the picture
+        int v[8];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            v[2 * k] = src[clampi(gy - k, 0, jb.h - 1) - (y0 - UH)][c];
+            v[2 * k + 1] = src[clampi(gy + 1 + k, 0, jb.h - 1) - (y0 - UH)][c];
+        }
+        const int16_t s = up_tap_sum(v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7]);
+        vh[r][c] = (int16_t)clampi(s, jb.lo, jb.hi);
+    }
+    __syncthreads();
+    // 2 x 2 output quads; a warp covers 32 consecutive source columns of one row
+    for (int idx = threadIdx.x; idx < UTY * UTX; idx += UP_THREADS) {
+        const int r = idx / UTX, c = idx - r * UTX;
+        const int gy = y0 + r, gx = x0 + c;
+        if (gy >= jb.h || gx >= jb.w) continue;
+        const int sc = c + UH;
+        int a[8], b[8];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int xl = clampi(gx - k, 0, jb.w - 1) - (x0 - UH);
+            const int xr = clampi(gx + 1 + k, 0, jb.w - 1) - (x0 - UH);
+            a[2 * k] = src[r + UH][xl];
+            a[2 * k + 1] = src[r + UH][xr];
+            b[2 * k] = vh[r][xl];
+            b[2 * k + 1] = vh[r][xr];
+        }
+        const int16_t e1 = (int16_t)clampi(up_tap_sum(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7]), jb.lo, jb.hi);
+        const int16_t o1 = (int16_t)clampi(up_tap_sum(b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7]), jb.lo, jb.hi);
+        const int16_t e0 = src[r + UH][sc];
+        const int16_t o0 = vh[r][sc];
+        int16_t* d0 = jb.dst + (size_t)(2 * gy) * jb.dst_stride + 2 * gx;
+        int16_t* d1 = d0 + jb.dst_stride;
+        // 4-byte aligned pair stores (dst_stride and the base are even-aligned)
+        *reinterpret_cast<short2*>(d0) = make_short2(e0, e1);
+        *reinterpret_cast<short2*>(d1) = make_short2(o0, o1);
+    }
+}
+
+// ---- decimation ---------------------------------------------------------------------------
+
+constexpr int DTX = 32, DTY = 8;  // output tile
+constexpr int DN_THREADS = 256;
+constexpr int DBUF_W = 2 * DTX + 12;
+
+struct DownJob {
+    const int16_t* src;
+    int16_t* dst;
+    int ow, oh, src_stride, dst_stride;  // output size; source region is 2*ow x 2*oh
+    int tiles_x, tile_begin;
+};
+constexpr int MAX_DOWN_JOBS = 32;
+struct DownJobs {
+    int njobs;
+    DownJob job[MAX_DOWN_JOBS];
+};
+
+__constant__ int c_down_taps[6] = {86, 46, 4, -8, -4, 4};
+
+__global__ void __launch_bounds__(DN_THREADS) downconvert_kernel(const __grid_constant__ DownJobs jobs) {
+    __shared__ int16_t rowbuf[DTY][DBUF_W];
+    int j = 0;
+    while (j + 1 < jobs.njobs && jobs.job[j + 1].tile_begin <= (int)blockIdx.x) ++j;
+    const DownJob& jb = jobs.job[j];
+    const int t = blockIdx.x - jb.tile_begin;
+    const int ty = t / jb.tiles_x, tx = t - ty * jb.tiles_x;
+    const int ox0 = tx * DTX, oy0 = ty * DTY;
+    const int xlen = 2 * jb.ow, ylen = 2 * jb.oh;
+    const int bx0 = 2 * ox0 - 5;  // source column of rowbuf[.][0]
+    for (int idx = threadIdx.x; idx < DTY * DBUF_W; idx += DN_THREADS) {
+        const int r = idx / DBUF_W, c = idx - r * DBUF_W;
+        const int oy = oy0 + r;
+        if (oy >= jb.oh) continue;
+        const int x = clampi(bx0 + c, 0, xlen - 1);
+        const int y = 2 * oy;
+        int sum = 128;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const int ya = clampi(y - k, 0, ylen - 1), yb = clampi(y + 1 + k, 0, ylen - 1);
+            sum += (jb.src[(size_t)ya * jb.src_stride + x] + jb.src[(size_t)yb * jb.src_stride + x]) * c_down_taps[k];
+        }
+        rowbuf[r][c] = (int16_t)(sum >> 8);
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < DTY * DTX; idx += DN_THREADS) {
+        const int r = idx / DTX, c = idx - r * DTX;
+        const int oy = oy0 + r, ox = ox0 + c;
+        if (oy >= jb.oh || ox >= jb.ow) continue;
+        const int x = 2 * ox;
+        int sum = 128;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const int xa = clampi(x - k, 0, xlen - 1) - bx0, xb = clampi(x + 1 + k, 0, xlen - 1) - bx0;
+            sum += (rowbuf[r][xa] + rowbuf[r][xb]) * c_down_taps[k];
+        }
+        jb.dst[(size_t)oy * jb.dst_stride + ox] = (int16_t)(sum >> 8);
+    }
+}
+
+// ---- clip ---------------------------------------------------------------------------------
+
+__global__ void clip_kernel(int16_t* p, int w, int h, int stride, int lo, int hi) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x < w && y < h) {
+        int16_t* q = p + (size_t)y * stride + x;
+        *q = (int16_t)clampi(*q, lo, hi);
+    }
+}
+
+}  // namespace
+
+int launch_upconvert(int n, const int16_t* const* src, const int* w, const int* h, const int* src_stride,
+                     const int* bit_depth, int16_t* const* dst, const int* dst_stride, cudaStream_t st) {
+    UpJobs jobs;
+    jobs.njobs = 0;
+    int tiles = 0;
+    for (int i = 0; i < n; ++i) {
+        if (!src[i] || !dst[i] || w[i] < 8 || h[i] < 8 || src_stride[i] < w[i] || dst_stride[i] < 2 * w[i] ||
+            (dst_stride[i] & 1) || (reinterpret_cast<uintptr_t>(dst[i]) & 3) || bit_depth[i] < 2 || bit_depth[i] > 15)
+            return DGPU_ERR_ARG;
+        UpJob& jb = jobs.job[jobs.njobs++];
+        jb.src = src[i];
+        jb.dst = dst[i];
+        jb.w = w[i];
+        jb.h = h[i];
+        jb.src_stride = src_stride[i];
+        jb.dst_stride = dst_stride[i];
+        jb.lo = -(1 << (bit_depth[i] - 1));
+        jb.hi = (1 << (bit_depth[i] - 1)) - 1;
+        jb.tiles_x = (w[i] + UTX - 1) / UTX;
+        jb.tile_begin = tiles;
+        tiles += jb.tiles_x * ((h[i] + UTY - 1) / UTY);
+        if (jobs.njobs == MAX_UP_JOBS || i == n - 1) {
+            upconvert_kernel<<<tiles, UP_THREADS, 0, st>>>(jobs);
+            DGPU_CHECK_LAUNCH();
+            jobs.njobs = 0;
+            tiles = 0;
+        }
+    }
+    return DGPU_OK;
+}
+
+int launch_downconvert(int n, const int16_t* const* src, const int* w, const int* h, const int* src_stride,
+                       int16_t* const* dst, const int* dst_stride, cudaStream_t st) {
+    DownJobs jobs;
+    jobs.njobs = 0;
+    int tiles = 0;
+    for (int i = 0; i < n; ++i) {
+        const int ow = w[i] / 2, oh = h[i] / 2;
+        if (!src[i] || !dst[i] || ow < 12 || oh < 12 || src_stride[i] < w[i] || dst_stride[i] < ow)
+            return DGPU_ERR_ARG;
+        DownJob& jb = jobs.job[jobs.njobs++];
+        jb.src = src[i];
+        jb.dst = dst[i];
+        jb.ow = ow;
+        jb.oh = oh;
+        jb.src_stride = src_stride[i];
+        jb.dst_stride = dst_stride[i];
+        jb.tiles_x = (ow + DTX - 1) / DTX;
+        jb.tile_begin = tiles;
+        tiles += jb.tiles_x * ((oh + DTY - 1) / DTY);
+        if (jobs.njobs == MAX_DOWN_JOBS || i == n - 1) {
+            downconvert_kernel<<<tiles, DN_THREADS, 0, st>>>(jobs);
+            DGPU_CHECK_LAUNCH();
+            jobs.njobs = 0;
+            tiles = 0;
+        }
+    }
+    return DGPU_OK;
+}
+
+int launch_clip(int16_t* p, int w, int h, int stride, int bit_depth, cudaStream_t st) {
+    if (!p || w <= 0 || h <= 0 || stride < w || bit_depth < 2 || bit_depth > 15) return DGPU_ERR_ARG;
+    dim3 grid((w + 255) / 256, h);
+    clip_kernel<<<grid, 256, 0, st>>>(p, w, h, stride, -(1 << (bit_depth - 1)), (1 << (bit_depth - 1)) - 1);
+    DGPU_CHECK_LAUNCH();
+    return DGPU_OK;
+}
+
+}  // namespace dgpu
+
+using namespace dgpu;
+
+extern "C" int dgpu_upconvert(const int16_t* pic, int w, int h, int stride, int bit_depth, int16_t* up,
+                              int up_stride, void* stream) {
+    return launch_upconvert(1, &pic, &w, &h, &stride, &bit_depth, &up, &up_stride, as_stream(stream));
+}
+
+extern "C" int dgpu_upconvert_batch(int n, const int16_t* const* pic, const int* w, const int* h,
+                                    const int* stride, const int* bit_depth, int16_t* const* up,
+                                    const int* up_stride, void* stream) {
+    if (n <= 0 || !pic || !w || !h || !stride || !bit_depth || !up || !up_stride) return DGPU_ERR_ARG;
+    return launch_upconvert(n, pic, w, h, stride, bit_depth, up, up_stride, as_stream(stream));
+}
+
+extern "C" int dgpu_downconvert(const int16_t* pic, int w, int h, int stride, int16_t* out, int out_stride,
+                                void* stream) {
+    return launch_downconvert(1, &pic, &w, &h, &stride, &out, &out_stride, as_stream(stream));
+}
+
+extern "C" int dgpu_downconvert_batch(int n, const int16_t* const* pic, const int* w, const int* h,
+                                      const int* stride, int16_t* const* out, const int* out_stride,
+                                      void* stream) {
+    if (n <= 0 || !pic || !w || !h || !stride || !out || !out_stride) return DGPU_ERR_ARG;
+    return launch_downconvert(n, pic, w, h, stride, out, out_stride, as_stream(stream));
+}
+
+extern "C" int dgpu_clip(int16_t* pic, int w, int h, int stride, int bit_depth, void* stream) {
+    return launch_clip(pic, w, h, stride, bit_depth, as_stream(stream));
+}

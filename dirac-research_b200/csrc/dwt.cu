@@ -124,7 +124,19 @@ __device__ __forceinline__ void lift_pass(int32_t* s, int len, int g0, int n, in
     }
 }
 
-// Per-filter analysis (Split) and synthesis (Synth) step sequences.
+// A lifting step as a type, so that step sequences can drive both the shared-memory and
+// the register code paths.
+template <int PAR_, int SIGN_, int KIND_, int SH__, int T1_, int T2_, int G_>
+struct Step {
+    static constexpr int PAR = PAR_, SIGN = SIGN_, KIND = KIND_, SHF = SH__, T1 = T1_, T2 = T2_, G = G_;
+};
+template <class S>
+using Inv = Step<S::PAR, -S::SIGN, S::KIND, S::SHF, S::T1, S::T2, S::G>;
+template <class... S>
+struct Steps {};
+
+// Per-filter analysis (Split) step sequences; synthesis (Synth) runs them in reverse with the
+// opposite sign.
 //   DD9_7     wavelet_utils.cpp:952-1133     LEGALL5_3 :805-949     DD13_7 :1136-1339
 //   HAAR0/1   :1342-1489                     DAUB9_7   :575-800 (also FIDELITY / unknown)
 template <int F>
@@ -133,61 +145,37 @@ struct Filter;
 template <>
 struct Filter<DGPU_DD9_7> {
     static constexpr int SHIFT = 1;
-    template <int AX>
-    __device__ static void analysis(int32_t* s, int len, int g0, int n, int l0, int l1) {
-        lift_pass<AX, 1, -1, K_FOURTAP, 4, 9, -1, 0>(s, len, g0, n, l0, l1); __syncthreads();
-        lift_pass<AX, 0, +1, K_SHIFT2, 2, 0, 0, 0>(s, len, g0, n, l0, l1); __syncthreads();
-    }
-    template <int AX>
-    __device__ static void synthesis(int32_t* s, int len, int g0, int n, int l0, int l1) {
-        lift_pass<AX, 0, -1, K_SHIFT2, 2, 0, 0, 0>(s, len, g0, n, l0, l1); __syncthreads();
-        lift_pass<AX, 1, +1, K_FOURTAP, 4, 9, -1, 0>(s, len, g0, n, l0, l1); __syncthreads();
-    }
+    using S1 = Step<1, -1, K_FOURTAP, 4, 9, -1, 0>;
+    using S2 = Step<0, +1, K_SHIFT2, 2, 0, 0, 0>;
+    using Analysis = Steps<S1, S2>;
+    using Synthesis = Steps<Inv<S2>, Inv<S1>>;
 };
 
 template <>
 struct Filter<DGPU_LEGALL5_3> {
     static constexpr int SHIFT = 1;
-    template <int AX>
-    __device__ static void analysis(int32_t* s, int len, int g0, int n, int l0, int l1) {
-        lift_pass<AX, 1, -1, K_SHIFT2, 1, 0, 0, 0>(s, len, g0, n, l0, l1); __syncthreads();
-        lift_pass<AX, 0, +1, K_SHIFT2, 2, 0, 0, 0>(s, len, g0, n, l0, l1); __syncthreads();
-    }
-    template <int AX>
-    __device__ static void synthesis(int32_t* s, int len, int g0, int n, int l0, int l1) {
-        lift_pass<AX, 0, -1, K_SHIFT2, 2, 0, 0, 0>(s, len, g0, n, l0, l1); __syncthreads();
-        lift_pass<AX, 1, +1, K_SHIFT2, 1, 0, 0, 0>(s, len, g0, n, l0, l1); __syncthreads();
-    }
+    using S1 = Step<1, -1, K_SHIFT2, 1, 0, 0, 0>;
+    using S2 = Step<0, +1, K_SHIFT2, 2, 0, 0, 0>;
+    using Analysis = Steps<S1, S2>;
+    using Synthesis = Steps<Inv<S2>, Inv<S1>>;
 };
 
 template <>
 struct Filter<DGPU_DD13_7> {
     static constexpr int SHIFT = 1;
-    template <int AX>
-    __device__ static void analysis(int32_t* s, int len, int g0, int n, int l0, int l1) {
-        lift_pass<AX, 1, -1, K_FOURTAP, 4, 9, -1, 0>(s, len, g0, n, l0, l1); __syncthreads();
-        lift_pass<AX, 0, +1, K_FOURTAP, 5, 9, -1, 0>(s, len, g0, n, l0, l1); __syncthreads();
-    }
-    template <int AX>
-    __device__ static void synthesis(int32_t* s, int len, int g0, int n, int l0, int l1) {
-        lift_pass<AX, 0, -1, K_FOURTAP, 5, 9, -1, 0>(s, len, g0, n, l0, l1); __syncthreads();
-        lift_pass<AX, 1, +1, K_FOURTAP, 4, 9, -1, 0>(s, len, g0, n, l0, l1); __syncthreads();
-    }
+    using S1 = Step<1, -1, K_FOURTAP, 4, 9, -1, 0>;
+    using S2 = Step<0, +1, K_FOURTAP, 5, 9, -1, 0>;
+    using Analysis = Steps<S1, S2>;
+    using Synthesis = Steps<Inv<S2>, Inv<S1>>;
 };
 
 template <int SHIFTBITS>
 struct HaarFilter {
     static constexpr int SHIFT = SHIFTBITS;
-    template <int AX>
-    __device__ static void analysis(int32_t* s, int len, int g0, int n, int l0, int l1) {
-        lift_pass<AX, 1, -1, K_HAAR, 0, 0, 0, 0>(s, len, g0, n, l0, l1); __syncthreads();
-        lift_pass<AX, 0, +1, K_HAAR, 0, 0, 0, 0>(s, len, g0, n, l0, l1); __syncthreads();
-    }
-    template <int AX>
-    __device__ static void synthesis(int32_t* s, int len, int g0, int n, int l0, int l1) {
-        lift_pass<AX, 0, -1, K_HAAR, 0, 0, 0, 0>(s, len, g0, n, l0, l1); __syncthreads();
-        lift_pass<AX, 1, +1, K_HAAR, 0, 0, 0, 0>(s, len, g0, n, l0, l1); __syncthreads();
-    }
+    using S1 = Step<1, -1, K_HAAR, 0, 0, 0, 0>;
+    using S2 = Step<0, +1, K_HAAR, 0, 0, 0, 0>;
+    using Analysis = Steps<S1, S2>;
+    using Synthesis = Steps<Inv<S2>, Inv<S1>>;
 };
 template <> struct Filter<DGPU_HAAR0> : HaarFilter<0> {};
 template <> struct Filter<DGPU_HAAR1> : HaarFilter<1> {};
@@ -195,21 +183,63 @@ template <> struct Filter<DGPU_HAAR1> : HaarFilter<1> {};
 template <>
 struct Filter<DGPU_DAUB9_7> {
     static constexpr int SHIFT = 1;
-    template <int AX>
-    __device__ static void analysis(int32_t* s, int len, int g0, int n, int l0, int l1) {
-        lift_pass<AX, 1, -1, K_97, 0, 0, 0, 6497>(s, len, g0, n, l0, l1); __syncthreads();
-        lift_pass<AX, 0, -1, K_97, 0, 0, 0, 217>(s, len, g0, n, l0, l1); __syncthreads();
-        lift_pass<AX, 1, +1, K_97, 0, 0, 0, 3616>(s, len, g0, n, l0, l1); __syncthreads();
-        lift_pass<AX, 0, +1, K_97, 0, 0, 0, 1817>(s, len, g0, n, l0, l1); __syncthreads();
-    }
-    template <int AX>
-    __device__ static void synthesis(int32_t* s, int len, int g0, int n, int l0, int l1) {
-        lift_pass<AX, 0, -1, K_97, 0, 0, 0, 1817>(s, len, g0, n, l0, l1); __syncthreads();
-        lift_pass<AX, 1, -1, K_97, 0, 0, 0, 3616>(s, len, g0, n, l0, l1); __syncthreads();
-        lift_pass<AX, 0, +1, K_97, 0, 0, 0, 217>(s, len, g0, n, l0, l1); __syncthreads();
-        lift_pass<AX, 1, +1, K_97, 0, 0, 0, 6497>(s, len, g0, n, l0, l1); __syncthreads();
-    }
+    using S1 = Step<1, -1, K_97, 0, 0, 0, 6497>;
+    using S2 = Step<0, -1, K_97, 0, 0, 0, 217>;
+    using S3 = Step<1, +1, K_97, 0, 0, 0, 3616>;
+    using S4 = Step<0, +1, K_97, 0, 0, 0, 1817>;
+    using Analysis = Steps<S1, S2, S3, S4>;
+    using Synthesis = Steps<Inv<S4>, Inv<S3>, Inv<S2>, Inv<S1>>;
 };
+
+// Shared-memory path: every step is one pass over the tile followed by a barrier.
+template <int AX, class... S>
+__device__ __forceinline__ void run_smem(Steps<S...>, int32_t* s, int len, int g0, int n, int l0, int l1) {
+    ((lift_pass<AX, S::PAR, S::SIGN, S::KIND, S::SHF, S::T1, S::T2, S::G>(s, len, g0, n, l0, l1),
+      __syncthreads()),
+     ...);
+}
+
+// Register path: a thread holds a segment of N consecutive samples of one line (SEG_HALO
+// halo samples on each side of its outputs).  All indices are compile-time.  A segment that
+// starts at the region's first sample (lo) or ends at its last (hi) holds SEG_HALO samples
+// outside the region; after loading and after every step they are overwritten with the
+// sample the reference's edge rule reads instead (the nearest in-region sample of the same
+// parity), which makes the in-region results identical to the clamped-index formulation.
+constexpr int SEG_HALO = 6;
+
+template <class S, int N>
+__device__ __forceinline__ void lift_regs(int (&v)[N]) {
+    constexpr int R = (S::KIND == K_FOURTAP) ? 3 : 1;
+#pragma unroll
+    for (int i = S::PAR; i < N; i += 2) {
+        if (i - R < 0 || i + R >= N) continue;
+        int d;
+        if constexpr (S::KIND == K_FOURTAP) {
+            d = lift_delta<S::PAR, S::KIND, S::SHF, S::T1, S::T2, S::G>(v[i - 1], v[i + 1], v[i - 3], v[i + 3]);
+        } else {
+            d = lift_delta<S::PAR, S::KIND, S::SHF, S::T1, S::T2, S::G>(v[i - 1], v[i + 1], 0, 0);
+        }
+        v[i] = (S::SIGN < 0) ? (v[i] - d) : (v[i] + d);
+    }
+}
+
+template <int N>
+__device__ __forceinline__ void repad(int (&v)[N], bool lo, bool hi) {
+    if (lo) {
+#pragma unroll
+        for (int i = 0; i < SEG_HALO; ++i) v[i] = v[SEG_HALO + (i & 1)];
+    }
+    if (hi) {
+#pragma unroll
+        for (int j = 0; j < SEG_HALO; ++j) v[N - SEG_HALO + j] = v[N - SEG_HALO - 2 + (j & 1)];
+    }
+}
+
+template <int N, class... S>
+__device__ __forceinline__ void run_regs(Steps<S...>, int (&v)[N], bool lo, bool hi) {
+    repad(v, lo, hi);
+    ((lift_regs<S>(v), repad(v, lo, hi)), ...);
+}
 
 __device__ __forceinline__ int find_job(const LevelJobs& jobs, int tile) {
     int j = 0;
@@ -240,8 +270,8 @@ __device__ void forward_tile(int32_t* s, const LevelJob& jb, int tx0, int ty0) {
     __syncthreads();
     // Horizontal lifting on every staged row (the vertical steps need the halo rows),
     // then vertical lifting on the tile's own columns.
-    Flt::template analysis<0>(s, SW, gx0, jb.xl, 0, SH);
-    Flt::template analysis<1>(s, SH, gy0, jb.yl, HALO, HALO + TX);
+    run_smem<0>(typename Flt::Analysis{}, s, SW, gx0, jb.xl, 0, SH);
+    run_smem<1>(typename Flt::Analysis{}, s, SH, gy0, jb.yl, HALO, HALO + TX);
     // Scatter into the Mallat quadrants (VHFilter::DeInterleave, wavelet_utils.cpp:540-573).
     const int xl2 = jb.xl >> 1, yl2 = jb.yl >> 1;
     for (int idx = threadIdx.x; idx < TY * (TX / 2); idx += NTHREADS) {
@@ -304,8 +334,8 @@ __device__ void inverse_tile(int32_t* s, const LevelJob& jb, int tx0, int ty0) {
     }
     __syncthreads();
     // Vertical synthesis on every staged column, then horizontal on the tile's own rows.
-    Flt::template synthesis<1>(s, SH, gy0, jb.yl, 0, SW);
-    Flt::template synthesis<0>(s, SW, gx0, jb.xl, HALO, HALO + TY);
+    run_smem<1>(typename Flt::Synthesis{}, s, SH, gy0, jb.yl, 0, SW);
+    run_smem<0>(typename Flt::Synthesis{}, s, SW, gx0, jb.xl, HALO, HALO + TY);
     // ShiftRowRight and store in natural order.
     for (int idx = threadIdx.x; idx < TY * TX; idx += NTHREADS) {
         const int r = idx / TX, c = idx - r * TX;
@@ -334,6 +364,187 @@ __global__ void __launch_bounds__(NTHREADS) dwt_inverse_level_kernel(const __gri
         case DGPU_HAAR0: inverse_tile<DGPU_HAAR0>(s, jb, tx0, ty0); break;
         case DGPU_HAAR1: inverse_tile<DGPU_HAAR1>(s, jb, tx0, ty0); break;
         default: inverse_tile<DGPU_DAUB9_7>(s, jb, tx0, ty0); break;
+    }
+}
+
+// ---- register-segment fast path (regions at least 64 x 64) ---------------------------
+//
+// A CTA owns a 64 x 64 tile (the last tile of a row / column is moved back to end exactly at
+// the region's edge, overlapping its neighbour, so every tile is full and every edge lies at
+// a fixed position inside a segment).  The tile plus an 8-sample halo is staged in shared
+// memory; each lifting direction is then run by threads that each hold a 44-sample segment
+// (32 outputs + 6-sample halo on each side) in registers.
+
+constexpr int FT = 64;                  // tile side
+constexpr int FH = 8;                   // staged halo
+constexpr int FS = FT + 2 * FH;         // staged side (80)
+constexpr int FP = FS + 1;              // pitch
+constexpr int SEG = 32;                 // outputs per segment
+constexpr int SEGN = SEG + 2 * SEG_HALO;  // registers per segment (44)
+constexpr int FAST_THREADS = 160;       // 80 lines x 2 segments
+
+template <int F>
+__device__ void forward_fast(int32_t* s, const LevelJob& jb, int x0, int y0) {
+    using Flt = Filter<F>;
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < FS * FS; idx += FAST_THREADS) {
+        const int r = idx / FS, c = idx - r * FS;
+        const int gy = y0 - FH + r, gx = x0 - FH + c;
+        if (gy < 0 || gy >= jb.yl || gx < 0 || gx >= jb.xl) continue;
+        int v;
+        if (jb.in16) {
+            v = jb.in16[(size_t)min(gy, jb.h - 1) * jb.in_stride + min(gx, jb.w - 1)];
+        } else {
+            v = jb.in32[(size_t)gy * jb.in_stride + gx];
+        }
+        s[r * FP + c] = (int32_t)((uint32_t)v << Flt::SHIFT);
+    }
+    __syncthreads();
+    // horizontal analysis on all 80 staged rows, two segments per row
+    {
+        const int seg = tid / FS, r = tid - seg * FS;
+        int v[SEGN];
+        const int32_t* src = s + r * FP + (FH - SEG_HALO) + SEG * seg;
+#pragma unroll
+        for (int i = 0; i < SEGN; ++i) v[i] = src[i];
+        run_regs(typename Flt::Analysis{}, v, x0 + SEG * seg == 0, x0 + SEG * seg + SEG == jb.xl);
+        __syncthreads();
+        int32_t* dst = s + r * FP + FH + SEG * seg;
+#pragma unroll
+        for (int k = 0; k < SEG; ++k) dst[k] = v[SEG_HALO + k];
+    }
+    __syncthreads();
+    // vertical analysis on the tile's 64 columns, two segments per column, stored straight
+    // into the Mallat quadrants
+    if (tid < 2 * FT) {
+        const int seg = tid / FT, c = tid - seg * FT;
+        int v[SEGN];
+        const int32_t* src = s + ((FH - SEG_HALO) + SEG * seg) * FP + FH + c;
+#pragma unroll
+        for (int i = 0; i < SEGN; ++i) v[i] = src[i * FP];
+        const int ys = y0 + SEG * seg;
+        run_regs(typename Flt::Analysis{}, v, ys == 0, ys + SEG == jb.yl);
+        const int gx = x0 + c;
+        const int xl2 = jb.xl >> 1, yl2 = jb.yl >> 1;
+        const int ox = gx >> 1;
+        const bool odd_x = gx & 1;
+        int32_t* even_row_dst = odd_x ? (jb.coeff + xl2 + ox) : (jb.ll + ox);
+        const int even_row_stride = odd_x ? jb.coeff_stride : jb.ll_stride;
+        int32_t* odd_row_dst = jb.coeff + (size_t)yl2 * jb.coeff_stride + (odd_x ? xl2 : 0) + ox;
+#pragma unroll
+        for (int k = 0; k < SEG; k += 2) {
+            const int oy = (ys + k) >> 1;
+            even_row_dst[(size_t)oy * even_row_stride] = v[SEG_HALO + k];
+            odd_row_dst[(size_t)oy * jb.coeff_stride] = v[SEG_HALO + k + 1];
+        }
+    }
+}
+
+template <int F>
+__device__ void inverse_fast(int32_t* s, const LevelJob& jb, int x0, int y0) {
+    using Flt = Filter<F>;
+    const int tid = threadIdx.x;
+    const int xl2 = jb.xl >> 1, yl2 = jb.yl >> 1;
+    for (int idx = tid; idx < FS * FS; idx += FAST_THREADS) {
+        const int r = idx / FS, c = idx - r * FS;
+        const int gy = y0 - FH + r, gx = x0 - FH + c;
+        if (gy < 0 || gy >= jb.yl || gx < 0 || gx >= jb.xl) continue;
+        const int qy = gy >> 1, qx = gx >> 1;
+        int32_t v;
+        if (((gx | gy) & 1) == 0) {
+            v = jb.ll[(size_t)qy * jb.ll_stride + qx];
+        } else {
+            v = jb.coeff[(size_t)((gy & 1) * yl2 + qy) * jb.coeff_stride + (gx & 1) * xl2 + qx];
+        }
+        s[r * FP + c] = v;
+    }
+    __syncthreads();
+    // vertical synthesis on all 80 staged columns
+    {
+        const int seg = tid / FS, c = tid - seg * FS;
+        int v[SEGN];
+        const int32_t* src = s + ((FH - SEG_HALO) + SEG * seg) * FP + c;
+#pragma unroll
+        for (int i = 0; i < SEGN; ++i) v[i] = src[i * FP];
+        const int ys = y0 + SEG * seg;
+        run_regs(typename Flt::Synthesis{}, v, ys == 0, ys + SEG == jb.yl);
+        __syncthreads();
+        int32_t* dst = s + (FH + SEG * seg) * FP + c;
+#pragma unroll
+        for (int k = 0; k < SEG; ++k) dst[k * FP] = v[SEG_HALO + k];
+    }
+    __syncthreads();
+    // horizontal synthesis and ShiftRowRight on the tile's 64 rows
+    {
+        int v[SEGN];
+        const bool active = tid < 2 * FT;
+        const int seg = tid / FT, r = FH + (tid - seg * FT);
+        if (active) {
+            const int32_t* src = s + r * FP + (FH - SEG_HALO) + SEG * seg;
+#pragma unroll
+            for (int i = 0; i < SEGN; ++i) v[i] = src[i];
+            const int xs = x0 + SEG * seg;
+            run_regs(typename Flt::Synthesis{}, v, xs == 0, xs + SEG == jb.xl);
+        }
+        __syncthreads();
+        if (active) {
+            int32_t* dst = s + r * FP + FH + SEG * seg;
+#pragma unroll
+            for (int k = 0; k < SEG; ++k) {
+                int32_t x = v[SEG_HALO + k];
+                if constexpr (Flt::SHIFT > 0) x = (x + (1 << (Flt::SHIFT - 1))) >> Flt::SHIFT;
+                dst[k] = x;
+            }
+        }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < FT * FT; idx += FAST_THREADS) {
+        const int r = idx / FT, c = idx - r * FT;
+        const int gy = y0 + r, gx = x0 + c;
+        const int32_t v = s[(FH + r) * FP + FH + c];
+        if (jb.out16) {
+            if (gy < jb.h && gx < jb.w) jb.out16[(size_t)gy * jb.out_stride + gx] = (int16_t)v;
+        } else {
+            jb.out32[(size_t)gy * jb.out_stride + gx] = v;
+        }
+    }
+}
+
+__device__ __forceinline__ void fast_tile_origin(const LevelJob& jb, int t, int& x0, int& y0) {
+    const int ty = t / jb.tiles_x, tx = t - ty * jb.tiles_x;
+    x0 = min(tx * FT, jb.xl - FT);
+    y0 = min(ty * FT, jb.yl - FT);
+}
+
+__global__ void __launch_bounds__(FAST_THREADS) dwt_forward_fast_kernel(const __grid_constant__ LevelJobs jobs) {
+    __shared__ int32_t s[FS * FP];
+    const int j = find_job(jobs, blockIdx.x);
+    const LevelJob& jb = jobs.job[j];
+    int x0, y0;
+    fast_tile_origin(jb, blockIdx.x - jb.tile_begin, x0, y0);
+    switch (jb.filter) {
+        case DGPU_DD9_7: forward_fast<DGPU_DD9_7>(s, jb, x0, y0); break;
+        case DGPU_LEGALL5_3: forward_fast<DGPU_LEGALL5_3>(s, jb, x0, y0); break;
+        case DGPU_DD13_7: forward_fast<DGPU_DD13_7>(s, jb, x0, y0); break;
+        case DGPU_HAAR0: forward_fast<DGPU_HAAR0>(s, jb, x0, y0); break;
+        case DGPU_HAAR1: forward_fast<DGPU_HAAR1>(s, jb, x0, y0); break;
+        default: forward_fast<DGPU_DAUB9_7>(s, jb, x0, y0); break;
+    }
+}
+
+__global__ void __launch_bounds__(FAST_THREADS) dwt_inverse_fast_kernel(const __grid_constant__ LevelJobs jobs) {
+    __shared__ int32_t s[FS * FP];
+    const int j = find_job(jobs, blockIdx.x);
+    const LevelJob& jb = jobs.job[j];
+    int x0, y0;
+    fast_tile_origin(jb, blockIdx.x - jb.tile_begin, x0, y0);
+    switch (jb.filter) {
+        case DGPU_DD9_7: inverse_fast<DGPU_DD9_7>(s, jb, x0, y0); break;
+        case DGPU_LEGALL5_3: inverse_fast<DGPU_LEGALL5_3>(s, jb, x0, y0); break;
+        case DGPU_DD13_7: inverse_fast<DGPU_DD13_7>(s, jb, x0, y0); break;
+        case DGPU_HAAR0: inverse_fast<DGPU_HAAR0>(s, jb, x0, y0); break;
+        case DGPU_HAAR1: inverse_fast<DGPU_HAAR1>(s, jb, x0, y0); break;
+        default: inverse_fast<DGPU_DAUB9_7>(s, jb, x0, y0); break;
     }
 }
 
@@ -387,29 +598,55 @@ int validate(const Entry& e) {
     return DGPU_OK;
 }
 
-int launch_jobs(bool forward, LevelJobs& jobs, int& total_tiles, cudaStream_t st) {
+// Jobs of one level go to the register fast path when their region is at least one full
+// tile in each direction, to the generic shared-memory path otherwise.
+struct LevelBatch {
+    LevelJobs fast, slow;
+    int fast_tiles = 0, slow_tiles = 0;
+    LevelBatch() { fast.njobs = slow.njobs = 0; }
+};
+
+int flush(bool forward, LevelBatch& b, bool fast_table, cudaStream_t st) {
+    LevelJobs& jobs = fast_table ? b.fast : b.slow;
+    int& tiles = fast_table ? b.fast_tiles : b.slow_tiles;
     if (jobs.njobs == 0) return DGPU_OK;
-    if (forward) {
-        dwt_forward_level_kernel<<<total_tiles, NTHREADS, 0, st>>>(jobs);
+    if (fast_table) {
+        if (forward) dwt_forward_fast_kernel<<<tiles, FAST_THREADS, 0, st>>>(jobs);
+        else dwt_inverse_fast_kernel<<<tiles, FAST_THREADS, 0, st>>>(jobs);
     } else {
-        dwt_inverse_level_kernel<<<total_tiles, NTHREADS, 0, st>>>(jobs);
+        if (forward) dwt_forward_level_kernel<<<tiles, NTHREADS, 0, st>>>(jobs);
+        else dwt_inverse_level_kernel<<<tiles, NTHREADS, 0, st>>>(jobs);
     }
     DGPU_CHECK_LAUNCH();
     jobs.njobs = 0;
-    total_tiles = 0;
+    tiles = 0;
     return DGPU_OK;
 }
 
-int add_job(bool forward, LevelJobs& jobs, int& total_tiles, const LevelJob& jb, cudaStream_t st) {
+int launch_jobs(bool forward, LevelBatch& b, cudaStream_t st) {
+    int rc = flush(forward, b, true, st);
+    if (rc) return rc;
+    return flush(forward, b, false, st);
+}
+
+// A side qualifies for the fast path when the tiles laid from 0 in steps of FT, with the last
+// one moved back to end at the edge, leave every non-edge segment's halo inside the region.
+bool fast_side(int n) { return n >= FT && (n % FT == 0 || n % FT >= SEG_HALO); }
+
+int add_job(bool forward, LevelBatch& b, const LevelJob& jb, cudaStream_t st) {
+    const bool fast = fast_side(jb.xl) && fast_side(jb.yl);
+    LevelJobs& jobs = fast ? b.fast : b.slow;
     if (jobs.njobs == MAXJ) {
-        int rc = launch_jobs(forward, jobs, total_tiles, st);
+        int rc = flush(forward, b, fast, st);
         if (rc) return rc;
     }
+    int& tiles = fast ? b.fast_tiles : b.slow_tiles;
     LevelJob j = jb;
-    j.tiles_x = (j.xl + TX - 1) / TX;
-    const int tiles_y = (j.yl + TY - 1) / TY;
-    j.tile_begin = total_tiles;
-    total_tiles += j.tiles_x * tiles_y;
+    const int tw = fast ? FT : TX, th = fast ? FT : TY;
+    j.tiles_x = (j.xl + tw - 1) / tw;
+    const int tiles_y = (j.yl + th - 1) / th;
+    j.tile_begin = tiles;
+    tiles += j.tiles_x * tiles_y;
     jobs.job[jobs.njobs++] = j;
     return DGPU_OK;
 }
@@ -417,9 +654,7 @@ int add_job(bool forward, LevelJobs& jobs, int& total_tiles, const LevelJob& jb,
 int run_entries(int direction, Entry* e, int n, cudaStream_t st) {
     int maxd = 0;
     for (int i = 0; i < n; ++i) maxd = e[i].depth > maxd ? e[i].depth : maxd;
-    LevelJobs jobs;
-    jobs.njobs = 0;
-    int total_tiles = 0;
+    LevelBatch batch;
     const bool fwd = direction == DGPU_FORWARD;
     if (fwd) {
         for (int l = 1; l <= maxd; ++l) {
@@ -448,10 +683,10 @@ int run_entries(int direction, Entry* e, int n, cudaStream_t st) {
                     jb.ll = (l & 1) ? E.scr.a : E.scr.b;
                     jb.ll_stride = jb.xl >> 1;
                 }
-                int rc = add_job(true, jobs, total_tiles, jb, st);
+                int rc = add_job(true, batch, jb, st);
                 if (rc) return rc;
             }
-            int rc = launch_jobs(true, jobs, total_tiles, st);
+            int rc = launch_jobs(true, batch, st);
             if (rc) return rc;
         }
     } else {
@@ -482,10 +717,10 @@ int run_entries(int direction, Entry* e, int n, cudaStream_t st) {
                     jb.out32 = (l & 1) ? E.scr.b : E.scr.a;
                     jb.out_stride = jb.xl;
                 }
-                int rc = add_job(false, jobs, total_tiles, jb, st);
+                int rc = add_job(false, batch, jb, st);
                 if (rc) return rc;
             }
-            int rc = launch_jobs(false, jobs, total_tiles, st);
+            int rc = launch_jobs(false, batch, st);
             if (rc) return rc;
         }
     }

@@ -60,7 +60,24 @@ SIGNATURES = {
         c_int,
         [c_int, c_int, c_int, c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_int, c_int],
     ),
+    "dgpu_upconvert": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p]),
+    "dgpu_upconvert_batch": (c_int, [c_int, P_void, P_int, P_int, P_int, P_int, P_void, P_int, c_void_p]),
+    "dgpu_downconvert": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_void_p]),
+    "dgpu_downconvert_batch": (c_int, [c_int, P_void, P_int, P_int, P_int, P_void, P_int, c_void_p]),
+    "dgpu_clip": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p]),
+    "dgpu_motion_compensate": (
+        c_int,
+        [c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+         P_void, P_int, P_void, P_void, c_int, c_int, c_void_p],
+    ),
 }
+
+
+class BlockParams(ctypes.Structure):
+    """dgpu_block_params: luma overlapped-block parameters and superblock counts."""
+
+    _fields_ = [(n, ctypes.c_int) for n in
+                ("precision", "xblen", "yblen", "xbsep", "ybsep", "xnum_sb", "ynum_sb")]
 
 
 def load(path=LIB_PATH):

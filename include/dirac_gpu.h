@@ -96,6 +96,71 @@ int dgpu_wavelet_transform_host(int direction, int filter, int depth,
                                 int16_t* pic, int w, int h, int pic_stride,
                                 int32_t* coeff, int cw, int ch, int coeff_stride);
 
+/* ---------------------------------------------------------------------------------------
+ * Half-pel upconversion
+ * Replaces UpConverter::DoUpConverter (libdirac_common/upconvert.cpp:55-200), as called by
+ * Picture::UpData (libdirac_common/picture.cpp:141-199) and EncPicture::UpOrigData
+ * (libdirac_encoder/enc_picture.cpp:131-159).  pic: h x w int16; up: (2h) x (2w) int16,
+ * up_stride even and up 4-byte aligned; samples clipped to [-2^(bit_depth-1),
+ * 2^(bit_depth-1)-1].  w, h >= 8 (the reference's edge loops overlap below that).
+ * ------------------------------------------------------------------------------------- */
+int dgpu_upconvert(const int16_t* pic, int w, int h, int stride, int bit_depth, int16_t* up,
+                   int up_stride, void* stream);
+int dgpu_upconvert_batch(int n, const int16_t* const* pic, const int* w, const int* h,
+                         const int* stride, const int* bit_depth, int16_t* const* up,
+                         const int* up_stride, void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * 2x decimation (one level of the motion-estimation pyramid)
+ * Replaces DownConverter::DoDownConvert (libdirac_motionest/downconvert.cpp:51-204) as
+ * PixelMatcher::MakePicHierarchy uses it (libdirac_motionest/pixel_match.cpp:158-182):
+ * out is (h/2) x (w/2); both output sides must be >= 12.
+ * ------------------------------------------------------------------------------------- */
+int dgpu_downconvert(const int16_t* pic, int w, int h, int stride, int16_t* out,
+                     int out_stride, void* stream);
+int dgpu_downconvert_batch(int n, const int16_t* const* pic, const int* w, const int* h,
+                           const int* stride, int16_t* const* out, const int* out_stride,
+                           void* stream);
+
+/* Picture::ClipComponent (libdirac_common/picture.cpp:221-283): clamp to the sample range. */
+int dgpu_clip(int16_t* pic, int w, int h, int stride, int bit_depth, void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Overlapped-block motion compensation
+ * Replaces MotionCompensator::CompensatePicture(const PicturePredParams&, AddOrSub,
+ * const MvData&, Picture*, Picture*[2]) (libdirac_common/mot_comp.h, mot_comp.cpp:63-1239).
+ *
+ * Block parameters are the luma level-2 OLBParams in the form
+ * PicturePredParams::SetBlockSizes keeps unchanged (lengths and separations multiples of 4,
+ * sep <= len <= 2 sep; libdirac_common/common.cpp:207-330); chroma parameters are derived
+ * from them by the chroma format as there.  Blocks = 4 x superblocks per direction.
+ * Block data (MvData, libdirac_common/motion.h:219-300), row-major over blocks:
+ *   mv1, mv2  int16 (x, y) per block, in units of the MV precision (mv2 may be NULL)
+ *   mode      uint8 per block: PredMode INTRA 0, REF1_ONLY 1, REF2_ONLY 2, REF1AND2 3
+ *   dc        int16 per block for Y, then U, then V (3 planes of blocks)
+ *   split     uint8 per superblock: 0 whole superblock, 1 four sub-superblocks, 2 blocks
+ * pic[3]: the picture's component planes, updated in place (add_or_sub 0 ADD, 1 SUBTRACT).
+ * ref1up/ref2up[3]: the references' upconverted planes ((2h_c) x (2w_c), dense), as
+ * produced by dgpu_upconvert; ref2up may be NULL for single-reference pictures.
+ * clip_*_depth > 0 clamps the ADD result to that bit depth (Picture::Clip fused);
+ * 0 leaves it unclipped.  Default (unit) reference weights only.
+ * ------------------------------------------------------------------------------------- */
+typedef struct {
+    int precision; /* MVPrecisionType: 0 pel, 1 half, 2 quarter, 3 eighth */
+    int xblen, yblen, xbsep, ybsep;
+    int xnum_sb, ynum_sb;
+} dgpu_block_params;
+
+#define DGPU_ADD 0
+#define DGPU_SUBTRACT 1
+
+int dgpu_motion_compensate(int add_or_sub, int cformat, int w, int h, const dgpu_block_params* bp,
+                           const int16_t* mv1, const int16_t* mv2, const uint8_t* mode,
+                           const int16_t* dc, const uint8_t* split, int16_t* const* pic,
+                           const int* pic_stride, const int16_t* const* ref1up,
+                           const int16_t* const* ref2up, int clip_luma_depth,
+                           int clip_chroma_depth, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -299,3 +299,152 @@ int orc_downconvert(const int16_t* pic, int w, int h, int stride, int16_t* out, 
     free(rowbuf);
     return 0;
 }
+
+/* ------------------------------------------------------------------------------------ */
+/* Overlapped-block motion compensation (MotionCompensator, mot_comp.cpp:63-1239)         */
+/* ------------------------------------------------------------------------------------ */
+/*
+ * The reference scatters each block's weighted prediction into a strip buffer in block
+ * raster order and flushes finished rows.  The restatement below gathers instead: every
+ * output sample sums the contributions of the (at most 2 x 2) prediction units that cover
+ * it, which is the same integer sum.  A unit is a block, a sub-superblock (2 blocks wide)
+ * or a whole superblock row segment (4 blocks wide), chosen by the superblock's split
+ * level (mot_comp.cpp:327-394); units are one block row high.  Weights are separable,
+ * V[y] * H[x], from the 1-D windows of MotionCompensator::CreateBlock (:735-804) with the
+ * edge variants of CalculateWeights (:710-724) chosen as at :353-383.
+ */
+
+/* One 1-D window (CreateBlock): length len, separation sep; flat_start pads the leading
+ * ramp to 8 (a block on the picture's left / top edge). */
+static void obmc_window(int len, int sep, int flat_start, int16_t* out) {
+    const int o = (len - sep) / 2;
+    if (o != 1) {
+        for (int x = 0; x < 2 * o; ++x) {
+            out[x] = (int16_t)(1 + (6 * x + o - 1) / (2 * o - 1));
+            out[x + sep] = (int16_t)(8 - out[x]);
+        }
+    } else {
+        out[0] = out[1 + sep] = 3;
+        out[1] = out[sep] = 5;
+    }
+    for (int x = 2 * o; x < sep; ++x) out[x] = 8;
+    if (flat_start)
+        for (int x = 0; x < 2 * o; ++x) out[x] = 8;
+}
+
+/* window value for edge class cls (0 leading edge, 1 interior, 2 trailing edge) */
+static int16_t obmc_weight(int len, int sep, int cls, int pos) {
+    int16_t buf[512];
+    if (cls == 2) {
+        obmc_window(len, sep, 1, buf);
+        return buf[len - 1 - pos];
+    }
+    obmc_window(len, sep, cls == 0, buf);
+    return buf[pos];
+}
+
+static inline int bchk(int v, int max) { return v < 0 ? 0 : (v >= max ? max - 1 : v); }
+
+/* BlockPixelPred for one sample (mot_comp.cpp:846-1239): the reference clamps upconverted
+ * coordinates with BChk(., 2*size - 1), i.e. to [0, 2*size - 2], whenever any sample of
+ * the block would leave that range, and the unclamped paths never leave it. */
+static int16_t pixel_pred(int prec, const int16_t* up, int cw, int ch, int px, int py, int mvx, int mvy) {
+    const int W2 = 2 * cw - 1, H2 = 2 * ch - 1, stride = 2 * cw;
+#define UP(yy, xx) ((int)up[(size_t)bchk((yy), H2) * stride + bchk((xx), W2)])
+    switch (prec) {
+    case 0:
+        return (int16_t)UP(2 * (py + mvy), 2 * (px + mvx));
+    case 1:
+        return (int16_t)UP(2 * py + mvy, 2 * px + mvx);
+    case 2: {
+        const int rx = mvx & 1, ry = mvy & 1;
+        const int bx = 2 * px + (mvx >> 1), by = 2 * py + (mvy >> 1);
+        return (int16_t)(((2 - rx) * (2 - ry) * UP(by, bx) + rx * (2 - ry) * UP(by, bx + 1) +
+                          (2 - rx) * ry * UP(by + 1, bx) + rx * ry * UP(by + 1, bx + 1) + 2) >> 2);
+    }
+    default: {
+        const int rx = mvx & 3, ry = mvy & 3;
+        const int bx = 2 * px + (mvx >> 2), by = 2 * py + (mvy >> 2);
+        return (int16_t)(((4 - rx) * (4 - ry) * UP(by, bx) + rx * (4 - ry) * UP(by, bx + 1) +
+                          (4 - rx) * ry * UP(by + 1, bx) + rx * ry * UP(by + 1, bx + 1) + 8) >> 4);
+    }
+    }
+#undef UP
+}
+
+int orc_motion_compensate(int add_or_sub, int cformat, int w, int h, const orc_block_params* bp,
+                          const int16_t* mv1, const int16_t* mv2, const uint8_t* mode,
+                          const int16_t* dc, const uint8_t* split, int16_t* const* pic,
+                          const int16_t* const* ref1up, const int16_t* const* ref2up) {
+    if (!bp || bp->xbsep <= 0 || bp->ybsep <= 0 || bp->xblen < bp->xbsep || bp->yblen < bp->ybsep ||
+        bp->xblen > 2 * bp->xbsep || bp->yblen > 2 * bp->ybsep || bp->xnum_sb <= 0 || bp->ynum_sb <= 0)
+        return -1;
+    const int xnb = 4 * bp->xnum_sb, ynb = 4 * bp->ynum_sb;
+    for (int c = 0; c < 3; ++c) {
+        const int xs = (c && cformat != ORC_444) ? 1 : 0;
+        const int ys = (c && cformat == ORC_420) ? 1 : 0;
+        const int cw = w >> xs, ch = h >> ys;
+        const int xblen = bp->xblen >> xs, xbsep = bp->xbsep >> xs;
+        const int yblen = bp->yblen >> ys, ybsep = bp->ybsep >> ys;
+        const int xoff = (xblen - xbsep) / 2, yoff = (yblen - ybsep) / 2;
+        int x_used = (cw + xbsep + (xblen - xbsep) / 2 - 1) / xbsep; /* NUM_USED_BLKS, :54 */
+        int y_used = (ch + ybsep + (yblen - ybsep) / 2 - 1) / ybsep;
+        if (x_used > xnb) x_used = xnb;
+        if (y_used > ynb) y_used = ynb;
+        int16_t* out = pic[c];
+        for (int py = 0; py < ch; ++py) {
+            for (int px = 0; px < cw; ++px) {
+                int acc = 0;
+                const int yb_hi = (py + yoff) / ybsep;
+                for (int yb = yb_hi - 1; yb <= yb_hi; ++yb) {
+                    if (yb < 0 || yb >= y_used) continue;
+                    const int pos_y = yb * ybsep - yoff;
+                    if (py < pos_y || py >= pos_y + yblen) continue;
+                    const int rcls = pos_y < 0 ? 0 : (yb + 1 < y_used ? 1 : 2);
+                    const int16_t V = obmc_weight(yblen, ybsep, rcls, py - pos_y);
+                    const int xb_hi = (px + xoff) / xbsep;
+                    int last_unit = -1;
+                    for (int xb = xb_hi - 1; xb <= xb_hi; ++xb) {
+                        if (xb < 0 || xb >= xnb) continue;
+                        if (px < xb * xbsep - xoff || px >= xb * xbsep - xoff + xblen) continue;
+                        const int sm = split[(size_t)(yb / 4) * bp->xnum_sb + xb / 4];
+                        const int nb = sm == 0 ? 4 : (sm == 1 ? 2 : 1);
+                        const int xs0 = xb - (xb % nb);
+                        if (xs0 == last_unit || xs0 >= x_used) continue;
+                        last_unit = xs0;
+                        const int pos_x = xs0 * xbsep - xoff;
+                        const int len = nb * xbsep + 2 * xoff;
+                        const int ccls = (pos_x >= 0 && xs0 + nb < x_used) ? 1 : (pos_x < 0 ? 0 : 2);
+                        const int16_t H = obmc_weight(len, nb * xbsep, ccls, px - pos_x);
+                        const int16_t wgt = (int16_t)(V * H);
+                        const size_t b = (size_t)yb * xnb + xs0;
+                        const int md = mode[b];
+                        int16_t pred;
+                        if (md == 0) {
+                            pred = dc[(size_t)c * xnb * ynb + b];
+                        } else {
+                            const int16_t* m1 = (md == 2) ? mv2 : mv1;
+                            const int16_t* u1 = (md == 2) ? ref2up[c] : ref1up[c];
+                            pred = pixel_pred(bp->precision, u1, cw, ch, px, py, m1[2 * b] >> xs, m1[2 * b + 1] >> ys);
+                            if (md == 3) {
+                                const int16_t p2 = pixel_pred(bp->precision, ref2up[c], cw, ch, px, py,
+                                                              mv2[2 * b] >> xs, mv2[2 * b + 1] >> ys);
+                                pred = (int16_t)((pred + p2 + 1) >> 1);
+                            }
+                        }
+                        acc = (int16_t)(acc + (int16_t)(pred * wgt));
+                    }
+                }
+                const int16_t v = (int16_t)(((int16_t)acc + 32) >> 6);
+                int16_t* o = &out[(size_t)py * cw + px];
+                *o = add_or_sub ? (int16_t)(*o - v) : (int16_t)(*o + v);
+            }
+        }
+    }
+    return 0;
+}
+
+void orc_clip(int16_t* pic, size_t n, int bit_depth) {
+    const int lo = -(1 << (bit_depth - 1)), hi = (1 << (bit_depth - 1)) - 1;
+    for (size_t i = 0; i < n; ++i) pic[i] = (int16_t)clampi(pic[i], lo, hi);
+}

@@ -13,6 +13,7 @@
 #ifndef DIRAC_ORACLE_H
 #define DIRAC_ORACLE_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -42,6 +43,31 @@ int orc_upconvert(const int16_t* pic, int w, int h, int stride, int bit_depth, i
 
 /* 2x decimation; out is (h/2) x (w/2). */
 int orc_downconvert(const int16_t* pic, int w, int h, int stride, int16_t* out, int out_stride);
+
+/* Overlapped-block parameters of a picture (luma, level 2 = single blocks), already in the
+ * form PicturePredParams::SetBlockSizes accepts unchanged (libdirac_common/common.cpp:207-330):
+ * lengths and separations multiples of 4, sep <= len <= 2 sep.  Blocks = 4 x superblocks. */
+typedef struct {
+    int precision; /* MVPrecisionType: 0 pel, 1 half, 2 quarter, 3 eighth */
+    int xblen, yblen, xbsep, ybsep;
+    int xnum_sb, ynum_sb;
+} orc_block_params;
+
+/* Chroma format numbering of the reference's ChromaFormat (format444 0, 422 1, 420 2). */
+enum { ORC_444 = 0, ORC_422 = 1, ORC_420 = 2 };
+
+/* Overlapped-block motion compensation of one picture (all three components):
+ * pic[c] (w_c x h_c, dense) -= / += the OBMC prediction built from the upconverted references
+ * ref1up[c] / ref2up[c] ((2 h_c) x (2 w_c)).  add_or_sub: 0 ADD, 1 SUBTRACT.  Block data:
+ * mv1/mv2 int16 (x,y) pairs per block, mode uint8 per block (0 INTRA, 1 REF1, 2 REF2,
+ * 3 REF1AND2), dc int16 [3][blocks], split uint8 per superblock.  No clipping. */
+int orc_motion_compensate(int add_or_sub, int cformat, int w, int h, const orc_block_params* bp,
+                          const int16_t* mv1, const int16_t* mv2, const uint8_t* mode,
+                          const int16_t* dc, const uint8_t* split, int16_t* const* pic,
+                          const int16_t* const* ref1up, const int16_t* const* ref2up);
+
+/* Picture::ClipComponent: clamp to [-2^(d-1), 2^(d-1)-1]. */
+void orc_clip(int16_t* pic, size_t n, int bit_depth);
 
 #ifdef __cplusplus
 }

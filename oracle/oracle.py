@@ -21,6 +21,31 @@ def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+class BlockParams(ctypes.Structure):
+    """orc_block_params / RefBlockDesc: precision, xblen, yblen, xbsep, ybsep, xnum_sb, ynum_sb."""
+
+    _fields_ = [(n, ctypes.c_int) for n in
+                ("precision", "xblen", "yblen", "xbsep", "ybsep", "xnum_sb", "ynum_sb")]
+
+
+def chroma_shift(cformat):
+    """(xshift, yshift) of the chroma planes for ChromaFormat 0 (444), 1 (422), 2 (420)."""
+    return {0: (0, 0), 1: (1, 0), 2: (1, 1)}[cformat]
+
+
+def _ptrs(arrs):
+    return (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+
+
+def _mc_args(mv1, mv2, mode, dc, split):
+    mv1 = np.ascontiguousarray(mv1, dtype=np.int16)
+    mv2 = np.ascontiguousarray(mv2 if mv2 is not None else mv1, dtype=np.int16)
+    mode = np.ascontiguousarray(mode, dtype=np.uint8)
+    dc = np.ascontiguousarray(dc, dtype=np.int16)
+    split = np.ascontiguousarray(split, dtype=np.uint8)
+    return mv1, mv2, mode, dc, split
+
+
 def padded(w, h, depth):
     mul = 1 << depth
     return (w + mul - 1) // mul * mul, (h + mul - 1) // mul * mul
@@ -31,6 +56,12 @@ class Oracle:
         if not os.path.exists(path):
             raise RuntimeError(f"{path} missing: run `make -C oracle oracle`")
         self.lib = ctypes.CDLL(path)
+
+    def clip(self, pic, bit_depth):
+        """Picture::ClipComponent, in place on a contiguous int16 array."""
+        assert pic.dtype == np.int16 and pic.flags["C_CONTIGUOUS"]
+        self.lib.orc_clip(_p(pic), ctypes.c_size_t(pic.size), ctypes.c_int(bit_depth))
+        return pic
 
     def dwt_min_len(self, filt):
         return self.lib.orc_dwt_min_len(filt)
@@ -71,6 +102,22 @@ class Oracle:
         rc = self.lib.orc_downconvert(_p(pic), w, h, w, _p(out), w // 2)
         if rc:
             raise ValueError(f"orc_downconvert rc={rc}")
+        return out
+
+
+    def motion_compensate(self, add_or_sub, cformat, pic, ref1, ref2, bp, mv1, mv2, mode, dc, split,
+                          luma_depth=8, chroma_depth=8):
+        """OBMC of a 3-component picture; refs are plain pictures (upconverted here)."""
+        out = [np.array(p, dtype=np.int16, copy=True, order="C") for p in pic]
+        r2 = ref2 if ref2 is not None else ref1
+        up1 = [self.upconvert(r, luma_depth if c == 0 else chroma_depth) for c, r in enumerate(ref1)]
+        up2 = [self.upconvert(r, luma_depth if c == 0 else chroma_depth) for c, r in enumerate(r2)]
+        mv1, mv2, mode, dc, split = _mc_args(mv1, mv2, mode, dc, split)
+        h, w = out[0].shape
+        rc = self.lib.orc_motion_compensate(add_or_sub, cformat, w, h, ctypes.byref(bp), _p(mv1), _p(mv2),
+                                            _p(mode), _p(dc), _p(split), _ptrs(out), _ptrs(up1), _ptrs(up2))
+        if rc:
+            raise ValueError(f"orc_motion_compensate rc={rc}")
         return out
 
 
@@ -118,4 +165,19 @@ class Reference:
         out = np.zeros((h // 2, w // 2), np.int16)
         if self.lib.ref_downconvert(_p(pic), w, h, _p(out)):
             raise ValueError("ref_downconvert failed")
+        return out
+
+    def motion_compensate(self, add_or_sub, cformat, pic, ref1, ref2, bp, mv1, mv2, mode, dc, split,
+                          luma_depth=8, chroma_depth=8):
+        out = [np.array(p, dtype=np.int16, copy=True, order="C") for p in pic]
+        nref = 2 if ref2 is not None else 1
+        r1 = [np.ascontiguousarray(r, dtype=np.int16) for r in ref1]
+        r2 = [np.ascontiguousarray(r, dtype=np.int16) for r in (ref2 if ref2 is not None else ref1)]
+        mv1, mv2, mode, dc, split = _mc_args(mv1, mv2, mode, dc, split)
+        h, w = out[0].shape
+        rc = self.lib.ref_motion_compensate(add_or_sub, cformat, w, h, luma_depth, chroma_depth,
+                                            ctypes.byref(bp), nref, _p(mv1), _p(mv2), _p(mode), _p(dc),
+                                            _p(split), _ptrs(out), _ptrs(r1), _ptrs(r2))
+        if rc:
+            raise ValueError("ref_motion_compensate failed")
         return out

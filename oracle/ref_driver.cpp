@@ -12,6 +12,9 @@
 #include <libdirac_common/wavelet_utils.h>
 #include <libdirac_common/upconvert.h>
 #include <libdirac_motionest/downconvert.h>
+#include <libdirac_common/picture.h>
+#include <libdirac_common/mot_comp.h>
+#include <libdirac_common/motion.h>
 
 using namespace dirac;
 
@@ -105,6 +108,81 @@ int ref_downconvert(const short* pic, int w, int h, short* out) {
         DownConverter dc;
         dc.DoDownConvert(p, o);
         read_pic(o, out);
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+// Block-motion description shared by the MC / ME stage drivers: per block (row-major over
+// ynb x xnb) int16 MV pairs (x, y) for reference 1 and 2, uint8 prediction mode
+// (PredMode: INTRA 0, REF1_ONLY 1, REF2_ONLY 2, REF1AND2 3), int16 DC per component, and a
+// uint8 superblock split level per superblock (ynsb x xnsb).
+struct RefBlockDesc {
+    int precision;          // MVPrecisionType: 0 pel, 1 half, 2 quarter, 3 eighth
+    int xblen, yblen, xbsep, ybsep;  // luma OLB parameters (level 2)
+    int xnum_sb, ynum_sb;   // blocks = 4 * superblocks in each direction
+};
+
+static void setup_ppp(PicturePredParams& ppp, const RefBlockDesc& d, ChromaFormat cf) {
+    ppp.SetMVPrecision((MVPrecisionType)d.precision);
+    ppp.SetBlockSizes(OLBParams(d.xblen, d.yblen, d.xbsep, d.ybsep), cf);
+    ppp.SetXNumSB(d.xnum_sb);
+    ppp.SetYNumSB(d.ynum_sb);
+    ppp.SetXNumBlocks(4 * d.xnum_sb);
+    ppp.SetYNumBlocks(4 * d.ynum_sb);
+}
+
+static void fill_mvdata(MvData& mv, const short* mv1, const short* mv2, const unsigned char* mode,
+                        const short* dc, const unsigned char* split, int nref) {
+    const int ynb = mv.Mode().LengthY(), xnb = mv.Mode().LengthX();
+    for (int j = 0; j < ynb; ++j)
+        for (int i = 0; i < xnb; ++i) {
+            const size_t b = (size_t)j * xnb + i;
+            mv.Vectors(1)[j][i] = MVector(mv1[2 * b], mv1[2 * b + 1]);
+            if (nref > 1) mv.Vectors(2)[j][i] = MVector(mv2[2 * b], mv2[2 * b + 1]);
+            mv.Mode()[j][i] = (PredMode)mode[b];
+            for (int c = 0; c < 3; ++c) mv.DC((CompSort)c)[j][i] = dc[(size_t)c * ynb * xnb + b];
+        }
+    for (int j = 0; j < mv.SBSplit().LengthY(); ++j)
+        for (int i = 0; i < mv.SBSplit().LengthX(); ++i)
+            mv.SBSplit()[j][i] = split[(size_t)j * mv.SBSplit().LengthX() + i];
+}
+
+// MotionCompensator::CompensatePicture (libdirac_common/mot_comp.cpp:63-192) on one picture:
+// pic[3] (in/out, component planes) gets the OBMC prediction from ref1[3]/ref2[3] (plain,
+// not upconverted: the reference upconverts them itself through Picture::UpData) added
+// (add_or_sub = 0) or subtracted (1).  cformat: ChromaFormat (0 444, 1 422, 2 420).
+int ref_motion_compensate(int add_or_sub, int cformat, int w, int h, int luma_depth, int chroma_depth,
+                          const RefBlockDesc* d, int nref, const short* mv1, const short* mv2,
+                          const unsigned char* mode, const short* dc, const unsigned char* split,
+                          short* const* pic, const short* const* ref1, const short* const* ref2) {
+    try {
+        const ChromaFormat cf = (ChromaFormat)cformat;
+        CodecParams cp(VIDEO_FORMAT_CIF, INTER_PICTURE, nref, true);
+        PicturePredParams& ppp = cp.GetPicPredParams();
+        setup_ppp(ppp, *d, cf);
+        MvData mv(ppp, 2);
+        fill_mvdata(mv, mv1, mv2, mode, dc, split, nref);
+
+        PictureParams pp(cf, w, h, luma_depth, chroma_depth);
+        pp.SetPicSort(PictureSort::InterRefPictureSort());
+        pp.SetPictureNum(1);
+        Picture r1(pp), r2(pp);
+        pp.SetPictureNum(5);
+        pp.Refs().push_back(1);
+        if (nref > 1) pp.Refs().push_back(2);
+        Picture cur(pp);
+        for (int c = 0; c < 3; ++c) {
+            fill_pic(cur.Data((CompSort)c), pic[c]);
+            fill_pic(r1.Data((CompSort)c), ref1[c]);
+            fill_pic(r2.Data((CompSort)c), nref > 1 ? ref2[c] : ref1[c]);
+        }
+        r1.GetPparams().SetPictureNum(1);
+        r2.GetPparams().SetPictureNum(2);
+        Picture* refs[2] = {&r1, &r2};
+        MotionCompensator::CompensatePicture(ppp, add_or_sub == 0 ? ADD : SUBTRACT, mv, &cur, refs);
+        for (int c = 0; c < 3; ++c) read_pic(cur.Data((CompSort)c), pic[c]);
         return 0;
     } catch (...) {
         return -1;

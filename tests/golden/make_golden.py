@@ -52,11 +52,55 @@ def conv_cases(ref):
     return out
 
 
+def mc_cases(ref):
+    """OBMC of small pictures: (w, h, cformat, precision, olb, nref) with random vectors,
+    modes, DC values and superblock splits, for ADD and SUBTRACT."""
+    from oracle import BlockParams, chroma_shift
+
+    rng = np.random.default_rng(42)
+    out = {}
+    cases = [(96, 64, 2, 2, (12, 12, 8, 8), 2), (100, 72, 1, 3, (16, 16, 12, 12), 2),
+             (64, 48, 0, 1, (8, 8, 8, 8), 1), (72, 56, 2, 0, (16, 12, 12, 8), 2)]
+    for k, (w, h, cf, prec, olb, nref) in enumerate(cases):
+        xbl, ybl, xbs, ybs = olb
+        xsb, ysb = (w + 4 * xbs - 1) // (4 * xbs), (h + 4 * ybs - 1) // (4 * ybs)
+        nb = (4 * ysb, 4 * xsb)
+        rr = 24 << prec
+        mv1 = rng.integers(-rr, rr, size=nb + (2,)).astype(np.int16)
+        mv2 = rng.integers(-rr, rr, size=nb + (2,)).astype(np.int16)
+        mode = rng.integers(0, 4 if nref == 2 else 2, size=nb).astype(np.uint8)
+        dc = rng.integers(-128, 128, size=(3,) + nb).astype(np.int16)
+        split = rng.integers(0, 3, size=(ysb, xsb)).astype(np.uint8)
+        xs, ys = chroma_shift(cf)
+
+        def mk():
+            return [rng.integers(-128, 128, size=(h, w)).astype(np.int16)] + \
+                   [rng.integers(-128, 128, size=(h >> ys, w >> xs)).astype(np.int16) for _ in range(2)]
+
+        pic, r1, r2 = mk(), mk(), mk()
+        bp = BlockParams(prec, xbl, ybl, xbs, ybs, xsb, ysb)
+        key = f"mc{k}"
+        out[key + "_meta"] = np.array([w, h, cf, prec, xbl, ybl, xbs, ybs, xsb, ysb, nref], np.int32)
+        for name, a in (("mv1", mv1), ("mv2", mv2), ("mode", mode), ("dc", dc), ("split", split)):
+            out[f"{key}_{name}"] = a
+        for c in range(3):
+            out[f"{key}_pic{c}"] = pic[c]
+            out[f"{key}_r1_{c}"] = r1[c]
+            out[f"{key}_r2_{c}"] = r2[c]
+        for aos in (0, 1):
+            res = ref.motion_compensate(aos, cf, pic, r1, r2 if nref == 2 else None, bp, mv1, mv2, mode, dc,
+                                        split)
+            for c in range(3):
+                out[f"{key}_out{aos}_{c}"] = res[c]
+    return out
+
+
 def main():
     ref = Reference()
     np.savez_compressed(os.path.join(HERE, "dwt.npz"), **dwt_cases(ref))
     np.savez_compressed(os.path.join(HERE, "convert.npz"), **conv_cases(ref))
-    print("wrote dwt.npz, convert.npz")
+    np.savez_compressed(os.path.join(HERE, "mc.npz"), **mc_cases(ref))
+    print("wrote dwt.npz, convert.npz, mc.npz")
 
 
 if __name__ == "__main__":

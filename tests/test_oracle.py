@@ -97,3 +97,56 @@ def test_convert_matches_live_reference(oracle):
         pic = rng.integers(-(1 << (bd - 1)), 1 << (bd - 1), size=(h, w)).astype(np.int16)
         np.testing.assert_array_equal(oracle.upconvert(pic, bd), ref.upconvert(pic, bd))
         np.testing.assert_array_equal(oracle.downconvert(pic), ref.downconvert(pic))
+
+
+def mc_case(g, k):
+    from oracle import BlockParams
+
+    w, h, cf, prec, xbl, ybl, xbs, ybs, xsb, ysb, nref = (int(v) for v in g[f"mc{k}_meta"])
+    bp = BlockParams(prec, xbl, ybl, xbs, ybs, xsb, ysb)
+    arrs = {n: g[f"mc{k}_{n}"] for n in ("mv1", "mv2", "mode", "dc", "split")}
+    pic = [g[f"mc{k}_pic{c}"] for c in range(3)]
+    r1 = [g[f"mc{k}_r1_{c}"] for c in range(3)]
+    r2 = [g[f"mc{k}_r2_{c}"] for c in range(3)] if nref == 2 else None
+    outs = {aos: [g[f"mc{k}_out{aos}_{c}"] for c in range(3)] for aos in (0, 1)}
+    return cf, bp, arrs, pic, r1, r2, outs
+
+
+def test_motion_compensation_golden(oracle, golden):
+    g = golden("mc.npz")
+    for k in range(4):
+        cf, bp, a, pic, r1, r2, outs = mc_case(g, k)
+        for aos in (0, 1):
+            res = oracle.motion_compensate(aos, cf, pic, r1, r2, bp, a["mv1"], a["mv2"], a["mode"], a["dc"],
+                                           a["split"])
+            for c in range(3):
+                np.testing.assert_array_equal(res[c], outs[aos][c], err_msg=f"case {k} aos {aos} comp {c}")
+
+
+@needs_ref
+def test_motion_compensation_matches_live_reference(oracle):
+    from oracle import BlockParams, chroma_shift
+
+    ref = Reference()
+    rng = np.random.default_rng(77)
+    for trial in range(12):
+        cf, prec = trial % 3, trial % 4
+        w, h = [(352, 288), (176, 144), (120, 72)][trial % 3]
+        xbl, ybl, xbs, ybs = [(12, 12, 8, 8), (16, 16, 12, 12), (24, 24, 16, 16), (8, 8, 8, 8)][trial % 4]
+        xsb, ysb = (w + 4 * xbs - 1) // (4 * xbs), (h + 4 * ybs - 1) // (4 * ybs)
+        bp = BlockParams(prec, xbl, ybl, xbs, ybs, xsb, ysb)
+        nb = (4 * ysb, 4 * xsb)
+        mv1 = rng.integers(-60 << prec, 60 << prec, size=nb + (2,)).astype(np.int16)
+        mv2 = rng.integers(-60 << prec, 60 << prec, size=nb + (2,)).astype(np.int16)
+        mode = rng.integers(0, 4, size=nb).astype(np.uint8)
+        dc = rng.integers(-128, 128, size=(3,) + nb).astype(np.int16)
+        split = rng.integers(0, 3, size=(ysb, xsb)).astype(np.uint8)
+        xs, ys = chroma_shift(cf)
+        mk = lambda: [rng.integers(-128, 128, size=(h, w)).astype(np.int16)] + [
+            rng.integers(-128, 128, size=(h >> ys, w >> xs)).astype(np.int16) for _ in range(2)]
+        pic, r1, r2 = mk(), mk(), mk()
+        for aos in (0, 1):
+            a = oracle.motion_compensate(aos, cf, pic, r1, r2, bp, mv1, mv2, mode, dc, split)
+            b = ref.motion_compensate(aos, cf, pic, r1, r2, bp, mv1, mv2, mode, dc, split)
+            for c in range(3):
+                np.testing.assert_array_equal(a[c], b[c])
