@@ -22,6 +22,7 @@
 // threads walking consecutive rows (horizontal lifting) or consecutive columns (vertical
 // lifting) hit distinct banks.
 
+#include <mutex>
 #include <new>
 
 #include "dgpu_internal.cuh"
@@ -814,4 +815,63 @@ extern "C" int dgpu_wavelet_transform_host(int direction, int filter, int depth,
     cudaFree(dpic);
     cudaFree(dcoeff);
     return rc;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free wavelet transform.
+//
+// Some callers cannot allocate device memory at the point where they transform: code running
+// under a device-memory budget that is already fully reserved, host threads that must not
+// synchronise the device (cudaMalloc / cudaFree may), or embedders whose allocator owns every
+// device byte.  dgpu_wavelet_transform_static serves them: the low-pass intermediates live in
+// the fixed array below, so the call needs neither a caller scratch buffer nor the library's
+// growable one.  The array costs DGPU_DWT_STATIC_SCRATCH_BYTES of memory on every GPU that
+// loads this library, for as long as the process lives.
+//
+// The array is shared by all calls on a device and keeps whatever the last call left in it.
+// Every level writes its low-pass band before the next level reads it, so nothing in it has
+// to start at zero.  Calls whose kernels overlap on the GPU (on different streams, or from
+// different host threads) race on the array and corrupt each other's results: serialise them.
+// ---------------------------------------------------------------------------------------------
+
+static __device__ __align__(256) unsigned char g_dwt_static_scratch[DGPU_DWT_STATIC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mu;
+void* g_static_scratch_addr[kStaticMaxDevices] = {};
+}  // namespace
+
+// Device address of g_dwt_static_scratch on the current device; looked up once per device
+// (the host-side name of a __device__ array is not a device address).
+static int static_scratch_address(void** out) {
+    int dev = 0;
+    DGPU_CHECK_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kStaticMaxDevices) return DGPU_ERR_DEVICE;
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (!g_static_scratch_addr[dev]) {
+        void* p = nullptr;
+        DGPU_CHECK_CUDA(cudaGetSymbolAddress(&p, g_dwt_static_scratch));
+        g_static_scratch_addr[dev] = p;
+    }
+    *out = g_static_scratch_addr[dev];
+    return DGPU_OK;
+}
+
+extern "C" int dgpu_wavelet_transform_static(int direction, int filter, int depth, int16_t* pic, int w, int h,
+                                             int pic_stride, int32_t* coeff, int cw, int ch, int coeff_stride,
+                                             void* stream) {
+    if (direction != DGPU_FORWARD && direction != DGPU_BACKWARD) return DGPU_ERR_ARG;
+    Entry e{filter, depth, pic, w, h, pic_stride, coeff, cw, ch, coeff_stride, {}};
+    int rc = validate(e);
+    if (rc) return rc;
+    const size_t need = entry_scratch_bytes(cw, ch);
+    if (need > DGPU_DWT_STATIC_SCRATCH_BYTES) return DGPU_ERR_SIZE;
+    void* base = nullptr;
+    rc = static_scratch_address(&base);
+    if (rc) return rc;
+    char* p = static_cast<char*>(base);
+    e.scr.a = reinterpret_cast<int32_t*>(p);
+    e.scr.b = reinterpret_cast<int32_t*>(p + align_up(scratch_a_elems(cw, ch) * 4, 256));
+    return run_entries(direction, &e, 1, as_stream(stream));
 }

@@ -56,6 +56,10 @@ SIGNATURES = {
         [c_int, c_int, P_int, P_int, P_void, P_int, P_int, P_int, P_void, P_int, P_int, P_int,
          c_void_p, c_size_t, c_void_p],
     ),
+    "dgpu_wavelet_transform_static": (
+        c_int,
+        [c_int, c_int, c_int, c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_int, c_int, c_void_p],
+    ),
     "dgpu_wavelet_transform_host": (
         c_int,
         [c_int, c_int, c_int, c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_int, c_int],

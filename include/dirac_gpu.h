@@ -96,6 +96,23 @@ int dgpu_wavelet_transform_host(int direction, int filter, int depth,
                                 int16_t* pic, int w, int h, int pic_stride,
                                 int32_t* coeff, int cw, int ch, int coeff_stride);
 
+/* Allocation-free form of dgpu_wavelet_transform, for callers that cannot allocate device
+ * memory when they transform (a fully reserved device-memory budget, threads that must not
+ * synchronise the device as cudaMalloc/cudaFree may, or an embedding allocator that owns
+ * all device memory).  It has no counterpart in the reference, which always transforms in
+ * host memory.  The low-pass intermediates live in one fixed device array of
+ * DGPU_DWT_STATIC_SCRATCH_BYTES per GPU, held from library load to process exit; it fits
+ * components with dgpu_dwt_scratch_bytes(cw, ch, depth) <= that size (any component up to
+ * 1920 x 1088, i.e. HD luma); larger ones return DGPU_ERR_SIZE.  The first call on a device
+ * looks the array's device address up (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  All calls on a device share the array: calls whose kernels overlap
+ * on the GPU race and must be serialised by the caller.  No allocation of any kind. */
+#define DGPU_DWT_STATIC_SCRATCH_BYTES (4u << 20)
+int dgpu_wavelet_transform_static(int direction, int filter, int depth,
+                                  int16_t* pic, int w, int h, int pic_stride,
+                                  int32_t* coeff, int cw, int ch, int coeff_stride,
+                                  void* stream);
+
 /* ---------------------------------------------------------------------------------------
  * Half-pel upconversion
  * Replaces UpConverter::DoUpConverter (libdirac_common/upconvert.cpp:55-200), as called by
