@@ -66,6 +66,21 @@ int orc_motion_compensate(int add_or_sub, int cformat, int w, int h, const orc_b
                           const int16_t* dc, const uint8_t* split, int16_t* const* pic,
                           const int16_t* const* ref1up, const int16_t* const* ref2up);
 
+/* Number of pyramid levels PixelMatcher uses for a w x h picture (pixel_match.cpp:94-95). */
+int orc_me_depth(int w, int h);
+
+/* Motion estimation of one picture against one (nref 1) or two references, as
+ * PictureCompressor::PixelME / SubPixelME / ModeDecisionME run it: stage 1 pel search over the
+ * pyramid, stage 2 lambda map + sub-pel refinement, stage 3 mode decision + DC.  Planes pic,
+ * ref1, ref2 are the three original components.  Outputs (blocks = 16 x superblocks):
+ * mv_out [nref][blocks][2] int16, cost_out [nref][blocks][3] = SAD, mvcost, total; after
+ * stage 3 mode_out [blocks], dc_out [3][blocks], split_out / sbcost_out [superblocks].
+ * MV precision must be half, quarter or eighth pel. */
+int orc_motion_estimate(int cformat, int w, int h, const orc_block_params* bp, int nref,
+                        const int16_t* const* pic, const int16_t* const* ref1, const int16_t* const* ref2,
+                        int luma_depth, float lambda, int stages, int16_t* mv_out, float* cost_out,
+                        uint8_t* mode_out, int16_t* dc_out, uint8_t* split_out, float* sbcost_out);
+
 /* Picture::ClipComponent: clamp to [-2^(d-1), 2^(d-1)-1]. */
 void orc_clip(int16_t* pic, size_t n, int bit_depth);
 

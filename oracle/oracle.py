@@ -121,6 +121,43 @@ class Oracle:
         return out
 
 
+    def motion_estimate(self, cformat, pic, ref1, ref2, bp, lambda_, stages=3, luma_depth=8):
+        return _me_call(self.lib.orc_motion_estimate, True, cformat, pic, ref1, ref2, bp, lambda_, stages,
+                        luma_depth)
+
+    def me_depth(self, w, h):
+        return self.lib.orc_me_depth(w, h)
+
+
+def _me_call(fn, is_oracle, cformat, pic, ref1, ref2, bp, lambda_, stages, luma_depth):
+    """Shared driver of orc_motion_estimate / ref_motion_estimate; returns a dict of arrays."""
+    nref = 2 if ref2 is not None else 1
+    pic = [np.ascontiguousarray(p, dtype=np.int16) for p in pic]
+    r1 = [np.ascontiguousarray(p, dtype=np.int16) for p in ref1]
+    r2 = [np.ascontiguousarray(p, dtype=np.int16) for p in (ref2 if ref2 is not None else ref1)]
+    h, w = pic[0].shape
+    nsb = bp.xnum_sb * bp.ynum_sb
+    nb = 16 * nsb
+    mv = np.zeros((nref, nb, 2), np.int16)
+    cost = np.zeros((nref, nb, 3), np.float32)
+    mode = np.zeros(nb, np.uint8)
+    dc = np.zeros((3, nb), np.int16)
+    split = np.zeros(nsb, np.uint8)
+    sbcost = np.zeros(nsb, np.float32)
+    if is_oracle:
+        rc = fn(cformat, w, h, ctypes.byref(bp), nref, _ptrs(pic), _ptrs(r1), _ptrs(r2), luma_depth,
+                ctypes.c_float(lambda_), stages, _p(mv), _p(cost), _p(mode), _p(dc), _p(split), _p(sbcost))
+    else:
+        rc = fn(cformat, w, h, luma_depth, luma_depth, ctypes.byref(bp), nref, _ptrs(pic), _ptrs(r1), _ptrs(r2),
+                ctypes.c_float(lambda_), stages, _p(mv), _p(cost), _p(mode), _p(dc), _p(split), _p(sbcost))
+    if rc:
+        raise ValueError(f"motion estimation failed rc={rc}")
+    ynb, xnb = 4 * bp.ynum_sb, 4 * bp.xnum_sb
+    return {"mv": mv.reshape(nref, ynb, xnb, 2), "cost": cost.reshape(nref, ynb, xnb, 3),
+            "mode": mode.reshape(ynb, xnb), "dc": dc.reshape(3, ynb, xnb),
+            "split": split.reshape(bp.ynum_sb, bp.xnum_sb), "sbcost": sbcost.reshape(bp.ynum_sb, bp.xnum_sb)}
+
+
 class Reference:
     """The reference codec itself (plain-C build), driven stage by stage."""
 
@@ -181,3 +218,7 @@ class Reference:
         if rc:
             raise ValueError("ref_motion_compensate failed")
         return out
+
+    def motion_estimate(self, cformat, pic, ref1, ref2, bp, lambda_, stages=3, luma_depth=8):
+        return _me_call(self.lib.ref_motion_estimate, False, cformat, pic, ref1, ref2, bp, lambda_, stages,
+                        luma_depth)

@@ -15,6 +15,11 @@
 #include <libdirac_common/picture.h>
 #include <libdirac_common/mot_comp.h>
 #include <libdirac_common/motion.h>
+#include <libdirac_encoder/enc_queue.h>
+#include <libdirac_encoder/enc_picture.h>
+#include <libdirac_motionest/pixel_match.h>
+#include <libdirac_motionest/me_subpel.h>
+#include <libdirac_motionest/me_mode_decn.h>
 
 using namespace dirac;
 
@@ -183,6 +188,94 @@ int ref_motion_compensate(int add_or_sub, int cformat, int w, int h, int luma_de
         Picture* refs[2] = {&r1, &r2};
         MotionCompensator::CompensatePicture(ppp, add_or_sub == 0 ? ADD : SUBTRACT, mv, &cur, refs);
         for (int c = 0; c < 3; ++c) read_pic(cur.Data((CompSort)c), pic[c]);
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+// Motion estimation of one picture against one or two references, run through the
+// reference's own classes as PictureCompressor::PixelME / SubPixelME / ModeDecisionME do
+// (libdirac_encoder/picture_compress.cpp:76-300): PixelMatcher::DoSearch (stage 1), then
+// MEData::SetLambdaMap(num_refs, lambda) and SubpelRefine::DoSubpel (stage 2), then
+// ModeDecider::DoModeDecn (stage 3).  Component planes pic/ref1/ref2[3] are the original
+// pictures (ME uses luma; mode decision's SetDC uses all three).  Outputs after the last
+// stage run: mv[ref][block] (x,y) int16, cost[ref][block] = (SAD, mvcost, total) float,
+// and after stage 3 mode, dc[3][block], split[sb], sbcost[sb].
+int ref_motion_estimate(int cformat, int w, int h, int luma_depth, int chroma_depth, const RefBlockDesc* d,
+                        int nref, const short* const* pic, const short* const* ref1, const short* const* ref2,
+                        float lambda, int stages, short* mv_out, float* cost_out, unsigned char* mode_out,
+                        short* dc_out, unsigned char* split_out, float* sbcost_out) {
+    try {
+        const ChromaFormat cf = (ChromaFormat)cformat;
+        EncoderParams ep(VIDEO_FORMAT_CIF, INTER_PICTURE, nref, true);
+        ep.SetFullSearch(false);
+        ep.SetCombinedME(false);
+        PicturePredParams& ppp = ep.GetPicPredParams();
+        setup_ppp(ppp, *d, cf);
+
+        EncQueue q;
+        PictureParams pp(cf, w, h, luma_depth, chroma_depth);
+        pp.SetPicSort(PictureSort::IntraRefPictureSort());
+        pp.SetPictureNum(0);
+        q.PushPicture(pp);
+        pp.SetPicSort(PictureSort::InterRefPictureSort());
+        pp.SetPictureNum(2);
+        q.PushPicture(pp);
+        pp.SetPictureNum(1);
+        pp.Refs().push_back(0);
+        if (nref > 1) pp.Refs().push_back(2);
+        q.PushPicture(pp);
+        const short* const* src[3] = {ref1, nref > 1 ? ref2 : ref1, pic};
+        const int pnum[3] = {0, 2, 1};
+        for (int k = 0; k < 3; ++k) {
+            EncPicture& ep_k = q.GetPicture(pnum[k]);
+            for (int c = 0; c < 3; ++c) fill_pic(ep_k.Data((CompSort)c), src[k][c]);
+            ep_k.SetOrigData();
+        }
+        EncPicture& cur = q.GetPicture(1);
+        cur.InitMEData(ppp, nref);
+        PixelMatcher pm(ep);
+        pm.DoSearch(q, 1);
+        MEData& me = cur.GetMEData();
+        if (stages >= 2) {
+            me.SetLambdaMap(nref, lambda);
+            if (d->precision != MV_PRECISION_PIXEL) {
+                SubpelRefine sr(ep);
+                sr.DoSubpel(q, 1);
+            }
+        }
+        if (stages >= 3) {
+            ModeDecider md(ep);
+            md.DoModeDecn(q, 1);
+        }
+        const int ynb = me.Mode().LengthY(), xnb = me.Mode().LengthX();
+        const size_t nb = (size_t)ynb * xnb;
+        for (int r = 1; r <= nref; ++r)
+            for (int j = 0; j < ynb; ++j)
+                for (int i = 0; i < xnb; ++i) {
+                    const size_t b = (size_t)j * xnb + i;
+                    const MVector& v = me.Vectors(r)[j][i];
+                    mv_out[((r - 1) * nb + b) * 2] = (short)v.x;
+                    mv_out[((r - 1) * nb + b) * 2 + 1] = (short)v.y;
+                    const MvCostData& cd = me.PredCosts(r)[j][i];
+                    cost_out[((r - 1) * nb + b) * 3] = cd.SAD;
+                    cost_out[((r - 1) * nb + b) * 3 + 1] = cd.mvcost;
+                    cost_out[((r - 1) * nb + b) * 3 + 2] = cd.total;
+                }
+        if (stages >= 3) {
+            for (int j = 0; j < ynb; ++j)
+                for (int i = 0; i < xnb; ++i) {
+                    const size_t b = (size_t)j * xnb + i;
+                    mode_out[b] = (unsigned char)me.Mode()[j][i];
+                    for (int c = 0; c < 3; ++c) dc_out[c * nb + b] = me.DC((CompSort)c)[j][i];
+                }
+            for (int j = 0; j < me.SBSplit().LengthY(); ++j)
+                for (int i = 0; i < me.SBSplit().LengthX(); ++i) {
+                    split_out[(size_t)j * me.SBSplit().LengthX() + i] = (unsigned char)me.SBSplit()[j][i];
+                    sbcost_out[(size_t)j * me.SBSplit().LengthX() + i] = me.SBCosts()[j][i];
+                }
+        }
         return 0;
     } catch (...) {
         return -1;

@@ -95,12 +95,42 @@ def mc_cases(ref):
     return out
 
 
+def me_cases(ref):
+    """Motion estimation (pel pyramid, sub-pel, mode decision) of small synthetic pictures."""
+    sys.path.insert(0, os.path.join(HERE, "..", "..", "dirac-research_b200"))
+    from dirac_b200 import synth
+    from oracle import BlockParams
+
+    out = {}
+    cases = [(176, 144, (12, 12, 8, 8), 2, 2, "420", 3), (160, 128, (16, 16, 12, 12), 3, 2, "422", 4),
+             (192, 144, (8, 8, 8, 8), 1, 1, "420", 5)]
+    for k, (w, h, olb, prec, nref, chroma, seed) in enumerate(cases):
+        seq = synth.make_sequence(w, h, 3, n_rects=6, vmax=6, seed=seed, chroma=chroma)
+        f = [[synth.to_signed(p) for p in fr] for fr in seq]
+        xbl, ybl, xbs, ybs = olb
+        bp = BlockParams(prec, xbl, ybl, xbs, ybs, (w + 4 * xbs - 1) // (4 * xbs), (h + 4 * ybs - 1) // (4 * ybs))
+        cf = {"444": 0, "422": 1, "420": 2}[chroma]
+        lam = 9.0 + k
+        res = ref.motion_estimate(cf, f[1], f[0], f[2] if nref == 2 else None, bp, lam, 3)
+        key = f"me{k}"
+        out[key + "_meta"] = np.array([w, h, cf, prec, xbl, ybl, xbs, ybs, bp.xnum_sb, bp.ynum_sb, nref], np.int32)
+        out[key + "_lambda"] = np.array([lam], np.float32)
+        for c in range(3):
+            out[f"{key}_pic{c}"] = f[1][c]
+            out[f"{key}_r1_{c}"] = f[0][c]
+            out[f"{key}_r2_{c}"] = f[2][c]
+        for name, a in res.items():
+            out[f"{key}_{name}"] = a
+    return out
+
+
 def main():
     ref = Reference()
     np.savez_compressed(os.path.join(HERE, "dwt.npz"), **dwt_cases(ref))
     np.savez_compressed(os.path.join(HERE, "convert.npz"), **conv_cases(ref))
     np.savez_compressed(os.path.join(HERE, "mc.npz"), **mc_cases(ref))
-    print("wrote dwt.npz, convert.npz, mc.npz")
+    np.savez_compressed(os.path.join(HERE, "me.npz"), **me_cases(ref))
+    print("wrote dwt.npz, convert.npz, mc.npz, me.npz")
 
 
 if __name__ == "__main__":

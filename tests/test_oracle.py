@@ -4,6 +4,8 @@ Golden fixtures in tests/golden were produced by running the reference's own C++
 (tests/golden/make_golden.py).  Where oracle/_ref is built, the oracle is additionally
 checked differentially against the live reference on fresh seeded inputs.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -150,3 +152,57 @@ def test_motion_compensation_matches_live_reference(oracle):
             b = ref.motion_compensate(aos, cf, pic, r1, r2, bp, mv1, mv2, mode, dc, split)
             for c in range(3):
                 np.testing.assert_array_equal(a[c], b[c])
+
+
+def me_case(g, k):
+    from oracle import BlockParams
+
+    w, h, cf, prec, xbl, ybl, xbs, ybs, xsb, ysb, nref = (int(v) for v in g[f"me{k}_meta"])
+    bp = BlockParams(prec, xbl, ybl, xbs, ybs, xsb, ysb)
+    pic = [g[f"me{k}_pic{c}"] for c in range(3)]
+    r1 = [g[f"me{k}_r1_{c}"] for c in range(3)]
+    r2 = [g[f"me{k}_r2_{c}"] for c in range(3)] if nref == 2 else None
+    want = {n: g[f"me{k}_{n}"] for n in ("mv", "cost", "mode", "dc", "split", "sbcost")}
+    return cf, bp, pic, r1, r2, float(g[f"me{k}_lambda"][0]), want
+
+
+def test_motion_estimation_golden(oracle, golden):
+    g = golden("me.npz")
+    for k in range(3):
+        cf, bp, pic, r1, r2, lam, want = me_case(g, k)
+        got = oracle.motion_estimate(cf, pic, r1, r2, bp, lam, 3)
+        for n, a in want.items():
+            np.testing.assert_array_equal(got[n], a, err_msg=f"case {k} {n}")
+
+
+def test_me_depth_formula(oracle):
+    # (int)min(log2(W/12), log2(H/12)) (libdirac_motionest/pixel_match.cpp:94-95)
+    assert oracle.me_depth(352, 288) == 4
+    assert oracle.me_depth(1920, 1080) == 6
+    assert oracle.me_depth(3840, 2160) == 7
+
+
+@needs_ref
+@pytest.mark.parametrize("case", range(6))
+def test_motion_estimation_matches_live_reference(oracle, case):
+    import sys
+
+    from oracle import BlockParams
+
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "dirac-research_b200"))
+    from dirac_b200 import synth
+
+    w, h, olb, prec, nref, chroma, vmax = [
+        (352, 288, (12, 12, 8, 8), 2, 2, "420", 8), (352, 288, (12, 12, 8, 8), 2, 1, "420", 8),
+        (720, 576, (12, 12, 8, 8), 3, 2, "422", 16), (480, 272, (16, 16, 12, 12), 1, 2, "444", 12),
+        (960, 540, (16, 16, 12, 12), 2, 2, "420", 24), (640, 360, (24, 24, 16, 16), 2, 2, "420", 24)][case]
+    seq = synth.make_sequence(w, h, 3, n_rects=12, vmax=vmax, seed=900 + case, chroma=chroma)
+    f = [[synth.to_signed(p) for p in fr] for fr in seq]
+    xbl, ybl, xbs, ybs = olb
+    bp = BlockParams(prec, xbl, ybl, xbs, ybs, (w + 4 * xbs - 1) // (4 * xbs), (h + 4 * ybs - 1) // (4 * ybs))
+    cf = {"444": 0, "422": 1, "420": 2}[chroma]
+    lam = float(2 * np.sqrt(4 * 10 ** ((12 - 7) / 2.5) / 16))
+    a = oracle.motion_estimate(cf, f[1], f[0], f[2] if nref == 2 else None, bp, lam, 3)
+    b = Reference().motion_estimate(cf, f[1], f[0], f[2] if nref == 2 else None, bp, lam, 3)
+    for n in a:
+        np.testing.assert_array_equal(a[n], b[n], err_msg=n)
