@@ -372,57 +372,75 @@ __global__ void __launch_bounds__(NTHREADS) dwt_inverse_level_kernel(const __gri
 //
 // A CTA owns a 64 x 64 tile (the last tile of a row / column is moved back to end exactly at
 // the region's edge, overlapping its neighbour, so every tile is full and every edge lies at
-// a fixed position inside a segment).  The tile plus an 8-sample halo is staged in shared
-// memory; each lifting direction is then run by threads that each hold a 44-sample segment
-// (32 outputs + 6-sample halo on each side) in registers.
+// a fixed position inside a segment).  Each lifting direction is run by threads that each hold
+// a 44-sample segment (32 outputs + a 6-sample halo on each side) of one line in registers.
+// The first direction's segments are loaded straight from global memory (16-byte vector loads
+// when the window is aligned and inside the picture, clamped scalar loads otherwise, so every
+// load of a thread is in flight at once); its 32 outputs go to shared memory, where the second
+// direction's segments are read from.  Forward: rows first, then columns stored straight into
+// the Mallat quadrants.  Inverse: columns first (gathered from the quadrants), then rows.
 
-constexpr int FT = 64;                  // tile side
-constexpr int FH = 8;                   // staged halo
-constexpr int FS = FT + 2 * FH;         // staged side (80)
-constexpr int FP = FS + 1;              // pitch
-constexpr int SEG = 32;                 // outputs per segment
+constexpr int FT = 64;                    // tile side
+constexpr int FH = 8;                     // halo lines above / left of the tile
+constexpr int SEG = 32;                   // outputs per segment
 constexpr int SEGN = SEG + 2 * SEG_HALO;  // registers per segment (44)
-constexpr int FAST_THREADS = 160;       // 80 lines x 2 segments
+constexpr int FLINES = FT + 2 * FH;       // lines the first direction covers (80)
+constexpr int FAST_THREADS = 2 * FLINES;  // 160: two segments per line
+constexpr int FWD_P = FT + 1;             // forward shared pitch: 80 rows x 64 columns
+constexpr int INV_P = FLINES + 1;         // inverse shared pitch: 64 rows x 80 columns
+
+// Load the 44-sample window [x - 6, x + 38) of one row into v (converted to int, << shift).
+// Columns are clamped to [0, xmax] and the row to [0, ymax]: in-region samples get the
+// reference's replicate padding, out-of-region ones get don't-care values that the edge
+// re-padding overwrites.
+template <class T, int SHIFT>
+__device__ __forceinline__ void load_row_window(int (&v)[SEGN], const T* base, int stride, int y, int ymax, int x,
+                                                int xmax) {
+    const T* row = base + (size_t)clampi(y, 0, ymax) * stride;
+    constexpr int PER16 = 16 / sizeof(T);  // elements per 16-byte vector
+    const int x8 = x - 8;                  // vector window [x - 8, x + 40)
+    const bool vec = x8 >= 0 && x + 40 <= xmax + 1 && ((reinterpret_cast<uintptr_t>(row + x8) & 15) == 0);
+    if (vec) {
+        T w[48];
+#pragma unroll
+        for (int k = 0; k < 48 / PER16; ++k)
+            *reinterpret_cast<int4*>(&w[k * PER16]) = *reinterpret_cast<const int4*>(row + x8 + k * PER16);
+#pragma unroll
+        for (int i = 0; i < SEGN; ++i) v[i] = (int)((uint32_t)(int)w[i + 2] << SHIFT);
+    } else {
+#pragma unroll
+        for (int i = 0; i < SEGN; ++i) v[i] = (int)((uint32_t)(int)row[clampi(x - SEG_HALO + i, 0, xmax)] << SHIFT);
+    }
+}
 
 template <int F>
 __device__ void forward_fast(int32_t* s, const LevelJob& jb, int x0, int y0) {
     using Flt = Filter<F>;
     const int tid = threadIdx.x;
-    for (int idx = tid; idx < FS * FS; idx += FAST_THREADS) {
-        const int r = idx / FS, c = idx - r * FS;
-        const int gy = y0 - FH + r, gx = x0 - FH + c;
-        if (gy < 0 || gy >= jb.yl || gx < 0 || gx >= jb.xl) continue;
-        int v;
-        if (jb.in16) {
-            v = jb.in16[(size_t)min(gy, jb.h - 1) * jb.in_stride + min(gx, jb.w - 1)];
-        } else {
-            v = jb.in32[(size_t)gy * jb.in_stride + gx];
-        }
-        s[r * FP + c] = (int32_t)((uint32_t)v << Flt::SHIFT);
-    }
-    __syncthreads();
-    // horizontal analysis on all 80 staged rows, two segments per row
+    // rows: 80 lines (the tile's 64 plus 8 above and below), two segments each
     {
-        const int seg = tid / FS, r = tid - seg * FS;
+        const int seg = tid / FLINES, r = tid - seg * FLINES;
+        const int xs = x0 + SEG * seg;
+        const int gy = y0 - FH + r;
         int v[SEGN];
-        const int32_t* src = s + r * FP + (FH - SEG_HALO) + SEG * seg;
-#pragma unroll
-        for (int i = 0; i < SEGN; ++i) v[i] = src[i];
-        run_regs(typename Flt::Analysis{}, v, x0 + SEG * seg == 0, x0 + SEG * seg + SEG == jb.xl);
-        __syncthreads();
-        int32_t* dst = s + r * FP + FH + SEG * seg;
+        if (jb.in16) {
+            load_row_window<int16_t, Flt::SHIFT>(v, jb.in16, jb.in_stride, gy, jb.h - 1, xs, jb.w - 1);
+        } else {
+            load_row_window<int32_t, Flt::SHIFT>(v, jb.in32, jb.in_stride, gy, jb.yl - 1, xs, jb.xl - 1);
+        }
+        run_regs(typename Flt::Analysis{}, v, xs == 0, xs + SEG == jb.xl);
+        int32_t* dst = s + r * FWD_P + SEG * seg;
 #pragma unroll
         for (int k = 0; k < SEG; ++k) dst[k] = v[SEG_HALO + k];
     }
     __syncthreads();
-    // vertical analysis on the tile's 64 columns, two segments per column, stored straight
-    // into the Mallat quadrants
+    // columns: the tile's 64, two segments each, stored straight into the Mallat quadrants
     if (tid < 2 * FT) {
         const int seg = tid / FT, c = tid - seg * FT;
         int v[SEGN];
-        const int32_t* src = s + ((FH - SEG_HALO) + SEG * seg) * FP + FH + c;
+        const int32_t* src = s + ((FH - SEG_HALO) + SEG * seg) * FWD_P + c;
 #pragma unroll
-        for (int i = 0; i < SEGN; ++i) v[i] = src[i * FP];
+        for (int i = 0; i < SEGN; ++i) v[i] = src[i * FWD_P];
         const int ys = y0 + SEG * seg;
         run_regs(typename Flt::Analysis{}, v, ys == 0, ys + SEG == jb.yl);
         const int gx = x0 + c;
@@ -446,67 +464,74 @@ __device__ void inverse_fast(int32_t* s, const LevelJob& jb, int x0, int y0) {
     using Flt = Filter<F>;
     const int tid = threadIdx.x;
     const int xl2 = jb.xl >> 1, yl2 = jb.yl >> 1;
-    for (int idx = tid; idx < FS * FS; idx += FAST_THREADS) {
-        const int r = idx / FS, c = idx - r * FS;
-        const int gy = y0 - FH + r, gx = x0 - FH + c;
-        if (gy < 0 || gy >= jb.yl || gx < 0 || gx >= jb.xl) continue;
-        const int qy = gy >> 1, qx = gx >> 1;
-        int32_t v;
-        if (((gx | gy) & 1) == 0) {
-            v = jb.ll[(size_t)qy * jb.ll_stride + qx];
-        } else {
-            v = jb.coeff[(size_t)((gy & 1) * yl2 + qy) * jb.coeff_stride + (gx & 1) * xl2 + qx];
-        }
-        s[r * FP + c] = v;
-    }
-    __syncthreads();
-    // vertical synthesis on all 80 staged columns
+    // columns: 80 lines (the tile's 64 plus 8 left and right), gathered from the quadrants
     {
-        const int seg = tid / FS, c = tid - seg * FS;
-        int v[SEGN];
-        const int32_t* src = s + ((FH - SEG_HALO) + SEG * seg) * FP + c;
-#pragma unroll
-        for (int i = 0; i < SEGN; ++i) v[i] = src[i * FP];
+        const int seg = tid / FLINES, c = tid - seg * FLINES;
+        const int gx = clampi(x0 - FH + c, 0, jb.xl - 1);
+        const int qx = gx >> 1;
+        // even rows come from LL (even column) or HL (odd column), odd rows from LH or HH
+        const int32_t* even_src = (gx & 1) ? (jb.coeff + xl2 + qx) : (jb.ll + qx);
+        const int even_stride = (gx & 1) ? jb.coeff_stride : jb.ll_stride;
+        const int32_t* odd_src = jb.coeff + (size_t)yl2 * jb.coeff_stride + (gx & 1) * xl2 + qx;
         const int ys = y0 + SEG * seg;
-        run_regs(typename Flt::Synthesis{}, v, ys == 0, ys + SEG == jb.yl);
-        __syncthreads();
-        int32_t* dst = s + (FH + SEG * seg) * FP + c;
-#pragma unroll
-        for (int k = 0; k < SEG; ++k) dst[k * FP] = v[SEG_HALO + k];
-    }
-    __syncthreads();
-    // horizontal synthesis and ShiftRowRight on the tile's 64 rows
-    {
         int v[SEGN];
-        const bool active = tid < 2 * FT;
-        const int seg = tid / FT, r = FH + (tid - seg * FT);
-        if (active) {
-            const int32_t* src = s + r * FP + (FH - SEG_HALO) + SEG * seg;
 #pragma unroll
-            for (int i = 0; i < SEGN; ++i) v[i] = src[i];
-            const int xs = x0 + SEG * seg;
-            run_regs(typename Flt::Synthesis{}, v, xs == 0, xs + SEG == jb.xl);
+        for (int i = 0; i < SEGN; ++i) {
+            const int gy = clampi(ys - SEG_HALO + i, 0, jb.yl - 1);
+            v[i] = (gy & 1) ? odd_src[(size_t)(gy >> 1) * jb.coeff_stride] : even_src[(size_t)(gy >> 1) * even_stride];
         }
-        __syncthreads();
-        if (active) {
-            int32_t* dst = s + r * FP + FH + SEG * seg;
+        run_regs(typename Flt::Synthesis{}, v, ys == 0, ys + SEG == jb.yl);
+        int32_t* dst = s + (SEG * seg) * INV_P + c;
 #pragma unroll
-            for (int k = 0; k < SEG; ++k) {
-                int32_t x = v[SEG_HALO + k];
-                if constexpr (Flt::SHIFT > 0) x = (x + (1 << (Flt::SHIFT - 1))) >> Flt::SHIFT;
-                dst[k] = x;
-            }
-        }
+        for (int k = 0; k < SEG; ++k) dst[k * INV_P] = v[SEG_HALO + k];
     }
     __syncthreads();
-    for (int idx = tid; idx < FT * FT; idx += FAST_THREADS) {
-        const int r = idx / FT, c = idx - r * FT;
-        const int gy = y0 + r, gx = x0 + c;
-        const int32_t v = s[(FH + r) * FP + FH + c];
+    // rows: the tile's 64, two segments each, then ShiftRowRight and the store
+    if (tid < 2 * FT) {
+        const int seg = tid / FT, r = tid - seg * FT;
+        int v[SEGN];
+        const int32_t* src = s + r * INV_P + (FH - SEG_HALO) + SEG * seg;
+#pragma unroll
+        for (int i = 0; i < SEGN; ++i) v[i] = src[i];
+        const int xs = x0 + SEG * seg;
+        run_regs(typename Flt::Synthesis{}, v, xs == 0, xs + SEG == jb.xl);
+        int o[SEG];
+#pragma unroll
+        for (int k = 0; k < SEG; ++k) {
+            int32_t x = v[SEG_HALO + k];
+            if constexpr (Flt::SHIFT > 0) x = (x + (1 << (Flt::SHIFT - 1))) >> Flt::SHIFT;
+            o[k] = x;
+        }
+        const int gy = y0 + r;
         if (jb.out16) {
-            if (gy < jb.h && gx < jb.w) jb.out16[(size_t)gy * jb.out_stride + gx] = (int16_t)v;
+            if (gy < jb.h) {
+                int16_t* row = jb.out16 + (size_t)gy * jb.out_stride + xs;
+                if (xs + SEG <= jb.w && (reinterpret_cast<uintptr_t>(row) & 15) == 0) {
+#pragma unroll
+                    for (int k = 0; k < SEG; k += 8) {
+                        int4 q;
+                        q.x = (int)(uint16_t)(int16_t)o[k] | ((int)(uint16_t)(int16_t)o[k + 1] << 16);
+                        q.y = (int)(uint16_t)(int16_t)o[k + 2] | ((int)(uint16_t)(int16_t)o[k + 3] << 16);
+                        q.z = (int)(uint16_t)(int16_t)o[k + 4] | ((int)(uint16_t)(int16_t)o[k + 5] << 16);
+                        q.w = (int)(uint16_t)(int16_t)o[k + 6] | ((int)(uint16_t)(int16_t)o[k + 7] << 16);
+                        *reinterpret_cast<int4*>(row + k) = q;
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < SEG; ++k)
+                        if (xs + k < jb.w) row[k] = (int16_t)o[k];
+                }
+            }
         } else {
-            jb.out32[(size_t)gy * jb.out_stride + gx] = v;
+            int32_t* row = jb.out32 + (size_t)gy * jb.out_stride + xs;
+            if ((reinterpret_cast<uintptr_t>(row) & 15) == 0) {
+#pragma unroll
+                for (int k = 0; k < SEG; k += 4)
+                    *reinterpret_cast<int4*>(row + k) = make_int4(o[k], o[k + 1], o[k + 2], o[k + 3]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < SEG; ++k) row[k] = o[k];
+            }
         }
     }
 }
@@ -518,7 +543,7 @@ __device__ __forceinline__ void fast_tile_origin(const LevelJob& jb, int t, int&
 }
 
 __global__ void __launch_bounds__(FAST_THREADS) dwt_forward_fast_kernel(const __grid_constant__ LevelJobs jobs) {
-    __shared__ int32_t s[FS * FP];
+    __shared__ int32_t s[FLINES * FWD_P];
     const int j = find_job(jobs, blockIdx.x);
     const LevelJob& jb = jobs.job[j];
     int x0, y0;
@@ -534,7 +559,7 @@ __global__ void __launch_bounds__(FAST_THREADS) dwt_forward_fast_kernel(const __
 }
 
 __global__ void __launch_bounds__(FAST_THREADS) dwt_inverse_fast_kernel(const __grid_constant__ LevelJobs jobs) {
-    __shared__ int32_t s[FS * FP];
+    __shared__ int32_t s[FT * INV_P];
     const int j = find_job(jobs, blockIdx.x);
     const LevelJob& jb = jobs.job[j];
     int x0, y0;
