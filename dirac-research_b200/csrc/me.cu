@@ -1,0 +1,1295 @@
+// Motion estimation for sm_100a: pel-accurate hierarchical block matching, sub-pel
+// refinement and superblock mode decision, bit-exact with the reference's decisions.
+//
+// Replaces PictureCompressor::PixelME / SubPixelME / ModeDecisionME and the classes they
+// drive (PixelMatcher, libdirac_motionest/pixel_match.cpp; MEData::SetLambdaMap,
+// libdirac_common/motion.cpp:128-333; SubpelRefine and BlockMatcher::RefineMatchSubp,
+// me_subpel.cpp, block_match.cpp:327-467; ModeDecider, me_mode_decn.cpp).
+//
+// Dependencies.  In every stage a block's predictor comes from neighbours decided before it
+// in raster order (left, top, top-right; plus top-left for sub-pel; the left, top-left and
+// top superblocks for mode decision), so each stage is a wavefront.  A wavefront stage is one
+// persistent launch: warps claim units in raster order from an atomic ticket, wait (bounded
+// spin) for the completion flags of the neighbours they read, and publish their own flag with
+// release semantics.  Raster-ordered tickets make this deadlock-free whatever the grid size:
+// the lowest unfinished ticket only waits on lower tickets, which are finished or running.
+// Work that does not depend on the raster order runs fully parallel first: for the pel search
+// these are the zero-centred and guide-centred candidate lists; only the predictor-centred
+// list is evaluated inside the wavefront.
+//
+// Exactness.  Candidates are evaluated in the reference's list order and the first strictly
+// smaller cost wins, as in the reference (a duplicate of an earlier candidate can never be
+// strictly smaller, so duplicates need no removal).  Sub-pel and superblock costs are float
+// sums the reference accumulates pixel by pixel in raster order from mvcost * lambda.  A float
+// sum of non-negative integers can only round when it crosses a power of two, so the warp
+// computes exact prefix sums with integer scans and applies one double -> float
+// round-to-nearest-even at each crossing (FloatSeq below), which reproduces the sequential
+// float result.  The library is compiled with --fmad=false: a*b+c is never fused.
+//
+// The lambda map's transition statistics are long double in the reference; that small step
+// (one value per block) runs on the host between the pel and the sub-pel stages.
+
+#include <cuda/atomic>
+
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "dgpu_internal.cuh"
+
+namespace dgpu {
+namespace {
+
+constexpr int WARPS_PER_CTA = 4;
+constexpr int ME_THREADS = 32 * WARPS_PER_CTA;
+constexpr long long SPIN_LIMIT = 1LL << 24;  // about 2 s of polling with __nanosleep(100)
+constexpr int MAX_ME_JOBS = 16;
+
+struct Olb {
+    int xblen, yblen, xbsep, ybsep, xoff, yoff;
+};
+
+inline Olb make_olb(int xblen, int yblen, int xbsep, int ybsep) {
+    return Olb{xblen, yblen, xbsep, ybsep, (xblen - xbsep) / 2, (yblen - ybsep) / 2};
+}
+
+struct Blim {
+    int xp, yp, xl, yl;
+};
+
+// BlockDiffParams::SetBlockLimits (me_utils.cpp:58-80); lengths may come out <= 0.
+__device__ __forceinline__ Blim block_limits(const Olb& o, int pw, int ph, int bx, int by) {
+    Blim b;
+    const int lx = bx * o.xbsep - o.xoff, ly = by * o.ybsep - o.yoff;
+    b.xp = lx > 0 ? lx : 0;
+    b.yp = ly > 0 ? ly : 0;
+    b.xl = o.xblen - b.xp + lx;
+    b.yl = o.yblen - b.yp + ly;
+    if (b.xp + b.xl - 1 > pw - 1) b.xl = pw - b.xp;
+    if (b.yp + b.yl - 1 > ph - 1) b.yl = ph - b.yp;
+    return b;
+}
+
+__device__ __forceinline__ int med3(int a, int b, int c) { return a + b + c - max(max(a, b), c) - min(min(a, b), c); }
+__device__ __forceinline__ short2 mv_median3(short2 a, short2 b, short2 c) {
+    return make_short2((short)med3(a.x, b.x, c.x), (short)med3(a.y, b.y, c.y));
+}
+__device__ __forceinline__ short2 mv_mean(short2 a, short2 b) {
+    return make_short2((short)((a.x + b.x + 1) >> 1), (short)((a.y + b.y + 1) >> 1));
+}
+__device__ __forceinline__ int norm1(int x, int y) { return abs(x) + abs(y); }
+// BlockMatcher::GetVarUp (block_match.cpp:213-220)
+__device__ __forceinline__ int getvarup(short2 pred, int mx, int my) {
+    return min(norm1(mx - pred.x, my - pred.y), norm1(mx, my));
+}
+
+// MvMedian of 0-4 vectors (motion.cpp:560-600)
+__device__ short2 mv_median_list(const short2* v, int n) {
+    if (n == 1) return v[0];
+    if (n == 2) return mv_mean(v[0], v[1]);
+    if (n == 3) return mv_median3(v[0], v[1], v[2]);
+    if (n == 4) {
+        int sx = 0, sy = 0, mxx = v[0].x, mnx = v[0].x, mxy = v[0].y, mny = v[0].y;
+        for (int i = 0; i < 4; ++i) {
+            sx += v[i].x;
+            sy += v[i].y;
+            mxx = max(mxx, (int)v[i].x);
+            mnx = min(mnx, (int)v[i].x);
+            mxy = max(mxy, (int)v[i].y);
+            mny = min(mny, (int)v[i].y);
+        }
+        return make_short2((short)((sx - (mxx + mnx) + 1) >> 1), (short)((sy - (mxy + mny) + 1) >> 1));
+    }
+    return make_short2(0, 0);
+}
+
+// The k-th candidate of AddNewVlist(centre, r, r) (block_match.cpp:89-126): the centre, then
+// (+i, 0), (-i, 0) for i = 1..r, then for j = 1..r and i = -r..r: (i, +j), (i, -j).
+__device__ __forceinline__ short2 cand_at(short2 c, int r, int k) {
+    if (k == 0) return c;
+    if (k <= 2 * r) {
+        const int i = (k + 1) >> 1;
+        return make_short2((short)(c.x + ((k & 1) ? i : -i)), c.y);
+    }
+    const int u = k - (2 * r + 1), per = 2 * (2 * r + 1);
+    const int j = u / per + 1, q = u - (j - 1) * per;
+    const int i = (q >> 1) - r;
+    return make_short2((short)(c.x + i), (short)(c.y + ((q & 1) ? -j : j)));
+}
+
+// ---- completion flags ---------------------------------------------------------------------
+
+__device__ __forceinline__ void publish(int* flag) {
+    cuda::atomic_ref<int, cuda::thread_scope_device> f(*flag);
+    f.store(1, cuda::memory_order_release);
+}
+
+// Every lane waits (acquire) until *flag is set; gives up after SPIN_LIMIT polls and records
+// the failure in *err (the host turns it into DGPU_ERR_CUDA).
+// Once any wait has timed out, every later wait returns at once, so a failed launch ends
+// within about one timeout.
+__device__ __forceinline__ void wait_flag(int* flag, int* err) {
+    cuda::atomic_ref<int, cuda::thread_scope_device> f(*flag);
+    cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
+    long long n = 0;
+    while (f.load(cuda::memory_order_acquire) == 0) {
+        if (++n > SPIN_LIMIT || ((n & 1023) == 0 && e.load(cuda::memory_order_relaxed) != 0)) {
+            atomicOr(err, 1);
+            return;
+        }
+        __nanosleep(100);
+    }
+}
+
+__device__ __forceinline__ int warp_ticket(int* counter) {
+    int t = 0;
+    if ((threadIdx.x & 31) == 0) t = atomicAdd(counter, 1);
+    return __shfl_sync(0xffffffffu, t, 0);
+}
+
+// ---- exact sequential float sums ------------------------------------------------------------
+
+// Running value of the reference's  sum = start; sum += (float)d  loop, for d >= 0 integers.
+struct FloatSeq {
+    double c;      // current float value of the sum (held exactly in a double)
+    double bound;  // smallest power of two above c: additions below it are exact
+};
+
+__device__ __forceinline__ double pow2_above(double c) {
+    if (c <= 0.0) return 16777216.0;  // integer partial sums from 0 are exact below 2^24
+    int e;
+    frexp(c, &e);  // c in [2^(e-1), 2^e)
+    return ldexp(1.0, e);
+}
+
+__device__ __forceinline__ FloatSeq float_seq_start(float start) {
+    FloatSeq f;
+    f.c = (double)start;
+    f.bound = pow2_above(f.c);
+    return f;
+}
+
+// Adds one term per lane (lane order = raster order; lanes without a term pass 0).
+__device__ __forceinline__ void float_seq_add(FloatSeq& f, int d) {
+    const int lane = threadIdx.x & 31;
+    const int total = __reduce_add_sync(0xffffffffu, d);
+    if (f.c + (double)total < f.bound) {  // no power of two crossed: every addition exact
+        f.c += (double)total;
+        return;
+    }
+    int pre = d;  // inclusive prefix over lanes
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, pre, o);
+        if (lane >= o) pre += v;
+    }
+    int base = 0;  // prefix already folded into f.c
+    for (;;) {
+        const double need = f.bound - f.c;
+        const unsigned m = __ballot_sync(0xffffffffu, (double)(pre - base) >= need);
+        if (m == 0) {
+            f.c += (double)(total - base);
+            return;
+        }
+        const int pk = __shfl_sync(0xffffffffu, pre, __ffs(m) - 1);
+        f.c = (double)__double2float_rn(f.c + (double)(pk - base));
+        f.bound = pow2_above(f.c);
+        base = pk;
+    }
+}
+
+// ---- block differences ----------------------------------------------------------------------
+
+// Integer SAD of one candidate against a same-size plane, coordinates clamped
+// (PelBlockDiff, me_utils.cpp:138-282).  Lanes own columns; warp-reduced.
+__device__ int pel_sad(const int16_t* pic, const int16_t* ref, int pw, int ph, const Blim& b, short2 mv) {
+    const int lane = threadIdx.x & 31;
+    int s = 0;
+    for (int c = lane; c < b.xl; c += 32) {
+        const int x = b.xp + c;
+        const int rx = clampi(x + mv.x, 0, pw - 1);
+        for (int j = 0; j < b.yl; ++j) {
+            const int y = b.yp + j;
+            const int ry = clampi(y + mv.y, 0, ph - 1);
+            s += abs((int)(int16_t)(pic[(size_t)y * pw + x] - ref[(size_t)ry * pw + rx]));
+        }
+    }
+    return __reduce_add_sync(0xffffffffu, s);
+}
+
+// Prediction sample from an upconverted reference (uw x uh) at precision p (1 half,
+// 2 quarter, 3 eighth), coordinates clamped to the array (me_utils.cpp:410-1170).
+__device__ __forceinline__ int up_at(const int16_t* up, int uw, int uh, int yy, int xx) {
+    return up[(size_t)clampi(yy, 0, uh - 1) * uw + clampi(xx, 0, uw - 1)];
+}
+__device__ __forceinline__ int up_pred(const int16_t* up, int uw, int uh, int p, int x, int y, int mx, int my) {
+    if (p == 1) return up_at(up, uw, uh, 2 * y + my, 2 * x + mx);
+    if (p == 2) {
+        const int rx = mx & 1, ry = my & 1;
+        const int bx = 2 * x + (mx >> 1), by = 2 * y + (my >> 1);
+        return ((2 - rx) * (2 - ry) * up_at(up, uw, uh, by, bx) + rx * (2 - ry) * up_at(up, uw, uh, by, bx + 1) +
+                (2 - rx) * ry * up_at(up, uw, uh, by + 1, bx) + rx * ry * up_at(up, uw, uh, by + 1, bx + 1) + 2) >> 2;
+    }
+    const int rx = mx & 3, ry = my & 3;
+    const int bx = 2 * x + (mx >> 2), by = 2 * y + (my >> 2);
+    return ((4 - rx) * (4 - ry) * up_at(up, uw, uh, by, bx) + rx * (4 - ry) * up_at(up, uw, uh, by, bx + 1) +
+            (4 - rx) * ry * up_at(up, uw, uh, by + 1, bx) + rx * ry * up_at(up, uw, uh, by + 1, bx + 1) + 8) >> 4;
+}
+
+// Float sum, in raster order from start, of |pred - pic| over a block: the cost loop of
+// BlockDiff{Half,Quarter,Eighth}Pel::Diff.  Returns the reference's float result.
+__device__ float subpel_cost(const int16_t* pic, int pw, const int16_t* up, int uw, int uh, int p, const Blim& b,
+                             int mx, int my, float start) {
+    const int lane = threadIdx.x & 31;
+    FloatSeq f = float_seq_start(start);
+    for (int j = 0; j < b.yl; ++j) {
+        const int y = b.yp + j;
+        for (int c0 = 0; c0 < b.xl; c0 += 32) {
+            int d = 0;
+            if (c0 + lane < b.xl) {
+                const int x = b.xp + c0 + lane;
+                d = abs(up_pred(up, uw, uh, p, x, y, mx, my) - pic[(size_t)y * pw + x]);
+            }
+            float_seq_add(f, d);
+        }
+    }
+    return (float)f.c;
+}
+
+// BiBlock*Pel::Diff (me_utils.cpp:1172-1785): |((2 pic - p1) - p2) >> 1| with int16
+// intermediates, summed in float from 0 (exact: integer sums below 2^24).  The eighth-pel
+// version walks the second reference from the first one's integer start position when the
+// second one needs bounds checking (me_utils.cpp:1764-1768); reproduced here.
+__device__ float bi_cost(const int16_t* pic, int pw, const int16_t* up1, const int16_t* up2, int uw, int uh, int p,
+                         const Blim& b, short2 mv1, short2 mv2) {
+    if (b.xl <= 0 || b.yl <= 0) return 0.0f;
+    int m2x = mv2.x, m2y = mv2.y;
+    if (p == 3) {
+        const int sx = (b.xp << 1) + (mv2.x >> 2), sy = (b.yp << 1) + (mv2.y >> 2);
+        if (sx < 0 || sx + (b.xl << 1) >= uw || sy < 0 || sy + (b.yl << 1) >= uh) {
+            m2x = ((mv1.x >> 2) << 2) | (mv2.x & 3);
+            m2y = ((mv1.y >> 2) << 2) | (mv2.y & 3);
+        }
+    }
+    const int lane = threadIdx.x & 31;
+    int s = 0;
+    for (int c = lane; c < b.xl; c += 32) {
+        const int x = b.xp + c;
+        for (int j = 0; j < b.yl; ++j) {
+            const int y = b.yp + j;
+            const int16_t dd = (int16_t)((pic[(size_t)y * pw + x] << 1) - up_pred(up1, uw, uh, p, x, y, mv1.x, mv1.y));
+            const int16_t t = (int16_t)((dd - up_pred(up2, uw, uh, p, x, y, m2x, m2y)) >> 1);
+            s += abs((int)t);
+        }
+    }
+    return (float)__reduce_add_sync(0xffffffffu, s);
+}
+
+// IntraBlockDiff::CalcDC and ::Diff (me_utils.cpp:284-408): truncating mean, SAD against it.
+__device__ int block_dc(const int16_t* pic, int pw, const Blim& b) {
+    if (b.xl <= 0 || b.yl <= 0) return 0;
+    const int lane = threadIdx.x & 31;
+    int s = 0;
+    for (int c = lane; c < b.xl; c += 32)
+        for (int j = 0; j < b.yl; ++j) s += pic[(size_t)(b.yp + j) * pw + b.xp + c];
+    s = __reduce_add_sync(0xffffffffu, s);
+    return (int)(int16_t)(s / (b.xl * b.yl));
+}
+
+__device__ float intra_cost(const int16_t* pic, int pw, const Blim& b, int16_t& dc) {
+    if (b.xl <= 0 || b.yl <= 0) {
+        dc = 0;
+        return 0.0f;
+    }
+    dc = (int16_t)block_dc(pic, pw, b);
+    const int lane = threadIdx.x & 31;
+    int s = 0;
+    for (int c = lane; c < b.xl; c += 32)
+        for (int j = 0; j < b.yl; ++j) s += abs(pic[(size_t)(b.yp + j) * pw + b.xp + c] - dc);
+    return (float)__reduce_add_sync(0xffffffffu, s);
+}
+
+// ============================================================================================
+// Pel search (pixel_match.cpp)
+// ============================================================================================
+
+struct PelJob {
+    const int16_t* pic;     // this level's picture plane (dense, pw x ph)
+    const int16_t* ref;     // this level's reference plane
+    int pw, ph;
+    int xnb, ynb;           // block grid of this level
+    short2* mv;             // vectors of this level (output)
+    float* cost;            // (SAD, mvcost, total) per block (output)
+    const short2* guide;    // vectors of the coarser level, or null at the coarsest
+    int gxnb, gynb;
+    int radius;             // min(level + 1, 5)
+    int* best_sad;          // zero + guide lists: best SAD (INT_MAX if the block is empty)
+    short2* best_mv;
+    int* flags;             // completion flags of the wavefront
+    int first;              // first global unit index of this job
+};
+
+struct PelLaunch {
+    int njobs, total;
+    Olb o;
+    int* ticket;
+    int* err;
+    PelJob job[MAX_ME_JOBS];
+};
+
+__device__ __forceinline__ int find_pel_job(const PelLaunch& L, int u) {
+    int j = 0;
+    while (j + 1 < L.njobs && L.job[j + 1].first <= u) ++j;
+    return j;
+}
+
+// Parallel phase: the zero-centred and the guide-centred lists of every block.
+__global__ void __launch_bounds__(ME_THREADS) pel_lists_kernel(const __grid_constant__ PelLaunch L) {
+    const int u = blockIdx.x * WARPS_PER_CTA + (threadIdx.x >> 5);
+    if (u >= L.total) return;
+    const PelJob& J = L.job[find_pel_job(L, u)];
+    const int b = u - J.first;
+    const int by = b / J.xnb, bx = b - by * J.xnb;
+    const Blim bl = block_limits(L.o, J.pw, J.ph, bx, by);
+    int best = INT_MAX;
+    short2 bmv = make_short2(0, 0);
+    if (bl.xl > 0 && bl.yl > 0) {
+        const int n = (2 * J.radius + 1) * (2 * J.radius + 1);
+        for (int k = 0; k < n; ++k) {
+            const short2 c = cand_at(make_short2(0, 0), J.radius, k);
+            const int s = pel_sad(J.pic, J.ref, J.pw, J.ph, bl, c);
+            if (s < best) {
+                best = s;
+                bmv = c;
+            }
+        }
+        if (J.guide) {
+            const int gx = clampi(bx >> 1, 0, J.gxnb - 1), gy = clampi(by >> 1, 0, J.gynb - 1);
+            const short2 g = J.guide[(size_t)gy * J.gxnb + gx];
+            const short2 g2 = make_short2((short)(g.x * 2), (short)(g.y * 2));
+            for (int k = 0; k < n; ++k) {
+                const short2 c = cand_at(g2, J.radius, k);
+                const int s = pel_sad(J.pic, J.ref, J.pw, J.ph, bl, c);
+                if (s < best) {
+                    best = s;
+                    bmv = c;
+                }
+            }
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        J.best_sad[b] = best;
+        J.best_mv[b] = bmv;
+    }
+}
+
+// Wavefront phase: raster predictor, predictor-centred list, final vectors and costs
+// (PixelMatcher::MatchPic / DoBlock, BlockMatcher::FindBestMatchPel).
+__global__ void __launch_bounds__(ME_THREADS) pel_wavefront_kernel(const __grid_constant__ PelLaunch L) {
+    for (;;) {
+        const int u = warp_ticket(L.ticket);
+        if (u >= L.total) return;
+        const PelJob& J = L.job[find_pel_job(L, u)];
+        const int b = u - J.first;
+        const int by = b / J.xnb, bx = b - by * J.xnb;
+        const int W = J.xnb;
+        if (bx > 0) wait_flag(&J.flags[b - 1], L.err);
+        if (by > 0) {
+            wait_flag(&J.flags[b - W], L.err);
+            if (bx < W - 1) wait_flag(&J.flags[b - W + 1], L.err);
+        }
+        const short2* mv = J.mv;
+        short2 pred = make_short2(0, 0);
+        if (by == 0) {
+            if (bx > 0) pred = __ldcg(&mv[b - 1]);
+        } else if (bx == 0) {
+            pred = __ldcg(&mv[b - W]);
+        } else if (bx < W - 1) {
+            pred = mv_median3(__ldcg(&mv[b - 1]), __ldcg(&mv[b - W]), __ldcg(&mv[b - W + 1]));
+        } else {
+            pred = mv_mean(__ldcg(&mv[b - W]), __ldcg(&mv[b - 1]));
+        }
+        const Blim bl = block_limits(L.o, J.pw, J.ph, bx, by);
+        int best = J.best_sad[b];
+        short2 bmv = J.best_mv[b];
+        float sad;
+        if (bl.xl > 0 && bl.yl > 0) {
+            const int n = (2 * J.radius + 1) * (2 * J.radius + 1);
+            for (int k = 0; k < n; ++k) {
+                const short2 c = cand_at(pred, J.radius, k);
+                const int s = pel_sad(J.pic, J.ref, J.pw, J.ph, bl, c);
+                if (s < best) {
+                    best = s;
+                    bmv = c;
+                }
+            }
+            sad = (float)best;
+        } else {
+            bmv = make_short2(0, 0);
+            sad = 10000000.0f;
+        }
+        if ((threadIdx.x & 31) == 0) {
+            const float mvcost = (float)norm1(bmv.x - pred.x, bmv.y - pred.y);
+            J.mv[b] = bmv;
+            J.cost[3 * b] = sad;
+            J.cost[3 * b + 1] = mvcost;
+            J.cost[3 * b + 2] = sad + 0.0f * mvcost;
+            publish(&J.flags[b]);
+        }
+        __syncwarp();
+    }
+}
+
+// ============================================================================================
+// Sub-pel refinement (me_subpel.cpp:65-176, block_match.cpp:327-467)
+// ============================================================================================
+
+struct SubJob {
+    const int16_t* pic;  // luma, pw x ph
+    const int16_t* up;   // upconverted original reference, 2pw x 2ph
+    int pw, ph, xnb, ynb;
+    short2* mv;          // in: pel vectors; out: sub-pel vectors
+    float* cost;         // (SAD, mvcost, total) per block, in and out
+    const float* lambda; // lambda map
+    int* flags;
+    int first;
+};
+
+struct SubLaunch {
+    int njobs, total, prec;
+    Olb o;
+    int* ticket;
+    int* err;
+    SubJob job[MAX_ME_JOBS];
+};
+
+__device__ __forceinline__ int find_sub_job(const SubLaunch& L, int u) {
+    int j = 0;
+    while (j + 1 < L.njobs && L.job[j + 1].first <= u) ++j;
+    return j;
+}
+
+struct Cost3 {
+    float SAD, mvcost, total;
+};
+
+// One candidate of a BlockDiff*Pel::Diff(..., mvcost, lambda, best_costs, best_mv) call.
+__device__ __forceinline__ void try_cand(const SubJob& J, int p, const Blim& bl, short2 c, float mvcost,
+                                         float lambda, Cost3& best, short2& best_mv) {
+    if (bl.xl <= 0 || bl.yl <= 0) return;
+    const float start = mvcost * lambda;
+    const float sum = subpel_cost(J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, p, bl, c.x, c.y, start);
+    if (sum < best.total) {
+        best_mv = c;
+        best.total = sum;
+        best.mvcost = mvcost;
+        best.SAD = sum - start;
+    }
+}
+
+__global__ void __launch_bounds__(ME_THREADS) subpel_wavefront_kernel(const __grid_constant__ SubLaunch L) {
+    const int prec = L.prec;
+    for (;;) {
+        const int u = warp_ticket(L.ticket);
+        if (u >= L.total) return;
+        const SubJob& J = L.job[find_sub_job(L, u)];
+        const int b = u - J.first;
+        const int by = b / J.xnb, bx = b - by * J.xnb;
+        const int W = J.xnb, H = J.ynb;
+        // neighbours in SubpelRefine::m_nshift order: left, top-left, top, top-right
+        const int nsx[4] = {-1, -1, 0, 1}, nsy[4] = {0, -1, -1, -1};
+        short2 nbr[4];
+        int n = 0;
+        const bool all = bx > 0 && by > 0 && bx < W - 1;
+        for (int i = 0; i < 4; ++i) {
+            const int x = bx + nsx[i], y = by + nsy[i];
+            if (all || (x >= 0 && y >= 0 && x < W && y < H)) {
+                wait_flag(&J.flags[y * W + x], L.err);
+                nbr[n++] = __ldcg(&J.mv[y * W + x]);
+            }
+        }
+        const short2 pred = mv_median_list(nbr, n);
+        const float lambda = J.lambda[b];
+        const Blim bl = block_limits(L.o, J.pw, J.ph, bx, by);
+        short2 mv = J.mv[b];
+        Cost3 cost{J.cost[3 * b], 0.0f, 0.0f};
+        cost.mvcost = (float)getvarup(pred, mv.x << prec, mv.y << prec);
+        cost.total = cost.SAD + lambda * cost.mvcost;
+        const float area2 = (float)(2 * bl.xl * bl.yl);
+        short2 out_mv;
+        Cost3 out_cost;
+        if (cost.SAD < area2) {
+            out_mv = make_short2((short)(mv.x << prec), (short)(mv.y << prec));
+            out_cost = cost;
+        } else {
+            Cost3 pc{0.0f, 0.0f, 0.0f};
+            pc.SAD = (bl.xl > 0 && bl.yl > 0)
+                         ? subpel_cost(J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, prec, bl, pred.x, pred.y, 0.0f)
+                         : 0.0f;
+            pc.total = pc.SAD;
+            if (pc.SAD < area2) {
+                out_mv = pred;
+                out_cost = pc;
+            } else {
+                Cost3 best = cost;
+                short2 bmv = mv;
+                bool bailed = false;
+                for (int i = 1; i <= prec; ++i) {
+                    bmv = make_short2((short)(bmv.x << 1), (short)(bmv.y << 1));
+                    short2 tb = bmv;
+                    const int sh = prec - i;
+                    const short2 c4[4] = {make_short2(bmv.x - 1, bmv.y), make_short2(bmv.x + 1, bmv.y),
+                                          make_short2(bmv.x, bmv.y - 1), make_short2(bmv.x, bmv.y + 1)};
+                    for (int q = 0; q < 4; ++q)
+                        try_cand(J, i, bl, c4[q], (float)getvarup(pred, c4[q].x << sh, c4[q].y << sh), lambda, best,
+                                 tb);
+                    if (tb.x != bmv.x) {
+                        const short2 nb = tb;
+                        const short2 c2[2] = {make_short2(nb.x, nb.y - 1), make_short2(nb.x, nb.y + 1)};
+                        for (int q = 0; q < 2; ++q)
+                            try_cand(J, i, bl, c2[q], (float)getvarup(pred, c2[q].x << sh, c2[q].y << sh), lambda,
+                                     best, tb);
+                    } else if (tb.y != bmv.y) {
+                        const short2 nb = tb;
+                        const short2 c2[2] = {make_short2(nb.x - 1, nb.y), make_short2(nb.x + 1, nb.y)};
+                        for (int q = 0; q < 2; ++q)
+                            try_cand(J, i, bl, c2[q], (float)getvarup(pred, c2[q].x << sh, c2[q].y << sh), lambda,
+                                     best, tb);
+                    }
+                    bmv = tb;
+                    if ((double)best.total > 1.1 * (double)pc.total) {
+                        bailed = true;
+                        break;
+                    }
+                }
+                if (bailed) {
+                    out_mv = pred;
+                    out_cost = pc;
+                } else {
+                    out_mv = bmv;
+                    out_cost = best;
+                }
+            }
+        }
+        if ((threadIdx.x & 31) == 0) {
+            J.mv[b] = out_mv;
+            J.cost[3 * b] = out_cost.SAD;
+            J.cost[3 * b + 1] = out_cost.mvcost;
+            J.cost[3 * b + 2] = out_cost.total;
+            publish(&J.flags[b]);
+        }
+        __syncwarp();
+    }
+}
+
+// ============================================================================================
+// Mode decision (me_mode_decn.cpp:66-537)
+// ============================================================================================
+
+// Data of one level (0 superblocks, 1 sub-superblocks, 2 blocks).
+struct LevelData {
+    int xnb, ynb;
+    short2* mv[2];
+    float* cost[2];     // (SAD, mvcost, total)
+    uint8_t* mode;
+    int16_t* dcy;       // DC of Y (level 2: the picture's DC(Y_COMP) array)
+    const float* lambda;
+};
+
+struct ModeJob {
+    const int16_t* pic;  // luma pw x ph
+    const int16_t* up[2];
+    int pw, ph;
+    LevelData lev[3];
+    float* sbcost;
+    uint8_t* split;
+    int xnsb, ynsb;
+    int* flags;          // per superblock
+    int first;
+};
+
+struct ModeLaunch {
+    int njobs, total, nref, prec;
+    Olb lb[3];
+    float level_factor[3];
+    int* ticket;
+    int* err;
+    ModeJob job[4];
+};
+
+__device__ __forceinline__ int find_mode_job(const ModeLaunch& L, int u) {
+    int j = 0;
+    while (j + 1 < L.njobs && L.job[j + 1].first <= u) ++j;
+    return j;
+}
+
+// ModeDecider::DoME: the unit's four guide vectors as candidates (BlockMatcher::FindBestMatchSubp).
+__device__ void do_me(const ModeLaunch& L, const ModeJob& J, int x, int y, int level) {
+    const LevelData& me = J.lev[level];
+    const LevelData& guide = J.lev[level + 1];
+    const LevelData& blk = J.lev[2];
+    const int gx = x << 1, gy = y << 1;
+    const int xb = x << (2 - level), yb = y << (2 - level);
+    const size_t k = (size_t)y * me.xnb + x;
+    const float lambda = me.lambda[k];
+    const Blim bl = block_limits(L.lb[level], J.pw, J.ph, x, y);
+    for (int r = 0; r < L.nref; ++r) {
+        short2 c[4];
+        int nc = 0;
+        for (int j = 0; j < 2; ++j)
+            for (int i = 0; i < 2; ++i) {
+                const short2 v = __ldcg(&guide.mv[r][(size_t)(gy + j) * guide.xnb + gx + i]);
+                bool dup = false;
+                for (int q = 0; q < nc; ++q) dup |= (c[q].x == v.x && c[q].y == v.y);
+                if (!dup) c[nc++] = v;
+            }
+        const short2* bv = blk.mv[r];
+        const int W = blk.xnb;
+        short2 pred = make_short2(0, 0);
+        if (xb > 0 && yb > 0)
+            pred = mv_median3(__ldcg(&bv[(size_t)yb * W + xb - 1]), __ldcg(&bv[(size_t)(yb - 1) * W + xb - 1]),
+                              __ldcg(&bv[(size_t)(yb - 1) * W + xb]));
+        else if (xb == 0 && yb > 0)
+            pred = mv_mean(__ldcg(&bv[(size_t)(yb - 1) * W + xb]), __ldcg(&bv[(size_t)(yb - 1) * W + xb + 1]));
+        else if (xb > 0 && yb == 0)
+            pred = mv_mean(__ldcg(&bv[(size_t)yb * W + xb - 1]), __ldcg(&bv[(size_t)(yb + 1) * W + xb - 1]));
+        Cost3 best{me.cost[r][3 * k], me.cost[r][3 * k + 1], 100000000.0f};
+        short2 bmv = me.mv[r][k];
+        for (int q = 0; q < nc; ++q) {
+            if (bl.xl <= 0 || bl.yl <= 0) break;
+            const float mvcost = (float)getvarup(pred, c[q].x, c[q].y);
+            const float start = mvcost * lambda;
+            const float sum = subpel_cost(J.pic, J.pw, J.up[r], 2 * J.pw, 2 * J.ph, L.prec, bl, c[q].x, c[q].y, start);
+            if (sum < best.total) {
+                bmv = c[q];
+                best.total = sum;
+                best.mvcost = mvcost;
+                best.SAD = sum - start;
+            }
+        }
+        if ((threadIdx.x & 31) == 0) {
+            me.mv[r][k] = bmv;
+            me.cost[r][3 * k] = best.SAD;
+            me.cost[r][3 * k + 1] = best.mvcost;
+            me.cost[r][3 * k + 2] = best.total;
+        }
+        __syncwarp();
+    }
+}
+
+// ModeDecider::DoUnitDecn: best of REF1 / REF2 / bi-prediction / intra for one unit.
+__device__ float do_unit_decn(const ModeLaunch& L, const ModeJob& J, int x, int y, int level) {
+    const LevelData& me = J.lev[level];
+    const size_t k = (size_t)y * me.xnb + x;
+    const float lambda = me.lambda[k];
+    const float mode_cost = 0.0f;
+    const float f = L.level_factor[level];
+    const Blim bl = block_limits(L.lb[level], J.pw, J.ph, x, y);
+    int mode = 1;
+    const float t1 = __ldcg(&me.cost[0][3 * k + 2]) * f;
+    float min_cost = t1 + mode_cost;
+    float best_sad = __ldcg(&me.cost[0][3 * k]);
+    float t2 = 0.0f;
+    if (L.nref > 1) {
+        t2 = __ldcg(&me.cost[1][3 * k + 2]) * f;
+        float unit = t2 + mode_cost;
+        if (unit < min_cost) {
+            mode = 2;
+            min_cost = unit;
+            best_sad = __ldcg(&me.cost[1][3 * k]);
+        }
+        const float bmvcost = __ldcg(&me.cost[0][3 * k + 1]) + __ldcg(&me.cost[1][3 * k + 1]);
+        const float bsad = bi_cost(J.pic, J.pw, J.up[0], J.up[1], 2 * J.pw, 2 * J.ph, L.prec, bl,
+                                   __ldcg(&me.mv[0][k]), __ldcg(&me.mv[1][k]));
+        float btotal = bsad + lambda * bmvcost;
+        btotal *= f;
+        unit = btotal + mode_cost;
+        if (unit < min_cost) {
+            mode = 3;
+            min_cost = unit;
+            best_sad = bsad;
+        }
+    }
+    int16_t dc = 0;
+    bool set_dc = false;
+    if (level == 2 && (double)best_sad > 4.0 * L.lb[level].xblen * L.lb[level].yblen) {
+        float ic = intra_cost(J.pic, J.pw, bl, dc);
+        set_dc = true;
+        ic *= f;
+        const float unit = ic + mode_cost;
+        if (unit < min_cost && (double)ic < 0.85 * (double)best_sad) {
+            mode = 0;
+            min_cost = unit;
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        me.cost[0][3 * k + 2] = t1;
+        if (L.nref > 1) me.cost[1][3 * k + 2] = t2;
+        me.mode[k] = (uint8_t)mode;
+        if (set_dc) me.dcy[k] = dc;
+    }
+    __syncwarp();
+    return min_cost;
+}
+
+// ModeDecider::DoLevelDecn for superblock (xsb, ysb) at one level.
+__device__ void do_level_decn(const ModeLaunch& L, const ModeJob& J, int xsb, int ysb, int level) {
+    const int xs = xsb << level, ys = ysb << level;
+    const int n = 1 << level;
+    const size_t sb = (size_t)ysb * J.xnsb + xsb;
+    float sb_cost = 0.0f;
+    for (int j = ys; j < ys + n; ++j)
+        for (int i = xs; i < xs + n; ++i) {
+            if (level < 2) do_me(L, J, i, j, level);
+            sb_cost += do_unit_decn(L, J, i, j, level);
+        }
+    if (level == 2) {
+        if ((threadIdx.x & 31) == 0) {
+            J.split[sb] = 2;
+            J.sbcost[sb] = sb_cost;
+        }
+        __syncwarp();
+        return;
+    }
+    const float cur = __ldcg(&J.sbcost[sb]);
+    if (sb_cost <= cur) {
+        const LevelData& lv = J.lev[level];
+        const LevelData& bl = J.lev[2];
+        const int span = 1 << (2 - level);
+        const int lane = threadIdx.x & 31;
+        // propagate the units' decisions to their blocks (16 blocks per superblock); lane 0
+        // does every write of a superblock so that its release publishes them all
+        for (int t = 0; t < 16 && lane == 0; ++t) {
+            const int v = (ysb << 2) + (t >> 2), u = (xsb << 2) + (t & 3);
+            const int j = v / span, i = u / span;
+            const size_t src = (size_t)j * lv.xnb + i, dst = (size_t)v * bl.xnb + u;
+            bl.mode[dst] = __ldcg(&lv.mode[src]);
+            bl.dcy[dst] = __ldcg(&lv.dcy[src]);
+            bl.mv[0][dst] = __ldcg(&lv.mv[0][src]);
+            if (L.nref > 1) bl.mv[1][dst] = __ldcg(&lv.mv[1][src]);
+        }
+        if (lane == 0) {
+            J.sbcost[sb] = sb_cost;
+            J.split[sb] = (uint8_t)level;
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(ME_THREADS) mode_wavefront_kernel(const __grid_constant__ ModeLaunch L) {
+    for (;;) {
+        const int u = warp_ticket(L.ticket);
+        if (u >= L.total) return;
+        const ModeJob& J = L.job[find_mode_job(L, u)];
+        const int s = u - J.first;
+        const int ysb = s / J.xnsb, xsb = s - ysb * J.xnsb;
+        if (xsb > 0) wait_flag(&J.flags[s - 1], L.err);
+        if (ysb > 0) {
+            wait_flag(&J.flags[s - J.xnsb], L.err);
+            if (xsb > 0) wait_flag(&J.flags[s - J.xnsb - 1], L.err);
+        }
+        do_level_decn(L, J, xsb, ysb, 2);
+        const float old = __ldcg(&J.sbcost[(size_t)ysb * J.xnsb + xsb]);
+        do_level_decn(L, J, xsb, ysb, 1);
+        if (__ldcg(&J.sbcost[(size_t)ysb * J.xnsb + xsb]) <= old) do_level_decn(L, J, xsb, ysb, 0);
+        if ((threadIdx.x & 31) == 0) publish(&J.flags[s]);
+        __syncwarp();
+    }
+}
+
+// ============================================================================================
+// DC values (ModeDecider::SetDC, me_mode_decn.cpp:540-573)
+// ============================================================================================
+
+struct DcJob {
+    const int16_t* pic;
+    int pw, ph;
+    Olb o;
+    int16_t* tmp;   // block DCs
+    int16_t* dc;    // output plane (last row left as it is)
+    int xnb, ynb;
+    int first;
+};
+
+struct DcLaunch {
+    int njobs, total;
+    DcJob job[MAX_ME_JOBS];
+};
+
+__global__ void __launch_bounds__(ME_THREADS) block_dc_kernel(const __grid_constant__ DcLaunch L) {
+    const int u = blockIdx.x * WARPS_PER_CTA + (threadIdx.x >> 5);
+    if (u >= L.total) return;
+    int j = 0;
+    while (j + 1 < L.njobs && L.job[j + 1].first <= u) ++j;
+    const DcJob& J = L.job[j];
+    const int b = u - J.first;
+    const int by = b / J.xnb, bx = b - by * J.xnb;
+    const int dc = block_dc(J.pic, J.pw, block_limits(J.o, J.pw, J.ph, bx, by));
+    if ((threadIdx.x & 31) == 0) J.tmp[b] = (int16_t)dc;
+}
+
+__global__ void smooth_dc_kernel(const __grid_constant__ DcLaunch L) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= L.total) return;
+    int j = 0;
+    while (j + 1 < L.njobs && L.job[j + 1].first <= u) ++j;
+    const DcJob& J = L.job[j];
+    const int b = u - J.first;
+    const int y = b / J.xnb, x = b - y * J.xnb;
+    const int W = J.xnb;
+    if (y == J.ynb - 1) return;
+    const int16_t* t = J.tmp;
+    int16_t v;
+    if (y == 0 || x == 0 || x == W - 1) {
+        v = t[b];
+    } else {
+        v = (int16_t)((t[b - W - 1] + 3 * t[b - W] + t[b - W + 1] + 3 * t[b - 1] + 3 * t[b + 1] + t[b + W - 1] +
+                       3 * t[b + W] + t[b + W + 1] + 8) >> 4);
+    }
+    J.dc[b] = v;
+}
+
+}  // namespace
+
+// ============================================================================================
+// Host side
+// ============================================================================================
+
+namespace {
+
+// FindTransitions (motion.cpp:201-333) for one reference: the vector-variation map (the SAD
+// map computed first is overwritten in the reference and has no effect), widened to whole
+// superblocks.  long double as in the reference.
+void find_transitions(const short2* mv, int W, int H, std::vector<uint8_t>& trans) {
+    std::vector<double> val((size_t)W * H, 0.0);
+    long double total = 0.0;
+    for (int j = 1; j < H - 1; ++j)
+        for (int i = 1; i < W - 1; ++i) {
+            double v = 0.0;
+            const short2 c = mv[(size_t)j * W + i];
+            for (int q = -1; q <= 1; ++q)
+                for (int p = -1; p <= 1; ++p) {
+                    const short2 o = mv[(size_t)(j + q) * W + i + p];
+                    const double d = (double)(std::abs(o.x - c.x) + std::abs(o.y - c.y));
+                    if (d > v) v = d;
+                }
+            val[(size_t)j * W + i] = v;
+            total += v;
+        }
+    const long double mean = total / (long double)(W * H);
+    long double sd = 0.0;
+    for (int j = 1; j < H - 1; ++j)
+        for (int i = 1; i < W - 1; ++i) {
+            double diff = (double)(val[(size_t)j * W + i] - mean);
+            diff *= diff;
+            sd += diff;
+        }
+    sd /= (long double)(W * H);
+    sd = std::sqrt(sd);
+    const double threshold = (double)(mean + 3 * sd);
+    trans.assign((size_t)W * H, 0);
+    for (size_t k = 0; k < (size_t)W * H; ++k) trans[k] = val[k] >= threshold;
+    for (int j = 0; j < H / 4; ++j)
+        for (int i = 0; i < W / 4; ++i) {
+            uint8_t any = 0;
+            for (int q = 4 * j; q < 4 * (j + 1); ++q)
+                for (int p = 4 * i; p < 4 * (i + 1); ++p) any |= trans[(size_t)q * W + p];
+            for (int q = 4 * j; q < 4 * (j + 1); ++q)
+                for (int p = 4 * i; p < 4 * (i + 1); ++p) trans[(size_t)q * W + p] = any;
+        }
+}
+
+// MEData::SetLambdaMap(num_refs, lambda) (motion.cpp:128-171).
+void lambda_map(const short2* mv1, const short2* mv2, int nref, int W, int H, float lambda, float* out) {
+    std::vector<uint8_t> t1, t2;
+    find_transitions(mv1, W, H, t1);
+    if (nref > 1) find_transitions(mv2, W, H, t2);
+    for (int j = 0; j < H; ++j)
+        for (int i = 0; i < W; ++i) {
+            const size_t k = (size_t)j * W + i;
+            float l;
+            if (nref == 1) {
+                l = t1[k] ? 0.0f : lambda;
+            } else if (t1[k] && t2[k]) {
+                l = 0.0f;
+            } else if (t1[k] || t2[k]) {
+                l = (float)(lambda / 4.0);
+            } else {
+                l = lambda;
+            }
+            if (i < 4 || j < 4) l = (float)(l / 5.0);
+            out[k] = l;
+        }
+}
+
+// MEData::SetLambdaMap(level, block map, wt) (motion.cpp:173-196).
+void level_lambda_map(const float* blk, int W, int level, int lw, int lh, float wt, float* out) {
+    const int f = 1 << (2 - level);
+    for (int j = 0; j < lh; ++j)
+        for (int i = 0; i < lw; ++i) {
+            float l = blk[(size_t)(f * j) * W + f * i];
+            for (int q = f * j; q < f * (j + 1); ++q)
+                for (int p = f * i; p < f * (i + 1); ++p) l = std::max(blk[(size_t)q * W + p], l);
+            out[(size_t)j * lw + i] = l * wt;
+        }
+}
+
+// A bump allocator over the caller's (or the library's) workspace.
+struct Arena {
+    char* base;
+    size_t used, cap;
+    template <class T>
+    T* take(size_t n) {
+        used = align_up(used, 256);
+        T* p = reinterpret_cast<T*>(base ? base + used : nullptr);
+        used += n * sizeof(T);
+        return p;
+    }
+};
+
+struct MeGeometry {
+    int w, h, depth, nref, cformat;
+    Olb lb[3];
+    int xnb[13], ynb[13], pw[13], ph[13];
+    int xnsb, ynsb;
+};
+
+int me_depth(int w, int h) {
+    return (int)std::min(std::log((double)w / 12.0) / std::log(2.0), std::log((double)h / 12.0) / std::log(2.0));
+}
+
+int me_geometry(int cformat, int w, int h, const dgpu_block_params* bp, int nref, MeGeometry& g) {
+    if (!bp || nref < 1 || nref > 2 || bp->precision < 1 || bp->precision > 3) return DGPU_ERR_ARG;
+    if (bp->xbsep <= 0 || bp->ybsep <= 0 || bp->xblen < bp->xbsep || bp->yblen < bp->ybsep ||
+        bp->xblen > 2 * bp->xbsep || bp->yblen > 2 * bp->ybsep || bp->xnum_sb <= 0 || bp->ynum_sb <= 0)
+        return DGPU_ERR_SIZE;
+    g.w = w;
+    g.h = h;
+    g.nref = nref;
+    g.cformat = cformat;
+    g.lb[2] = make_olb(bp->xblen, bp->yblen, bp->xbsep, bp->ybsep);
+    g.lb[1] = make_olb(g.lb[2].xblen + g.lb[2].xbsep, g.lb[2].yblen + g.lb[2].xbsep, 2 * g.lb[2].xbsep,
+                       2 * g.lb[2].ybsep);
+    g.lb[0] = make_olb(g.lb[1].xblen + g.lb[1].xbsep, g.lb[1].yblen + g.lb[1].xbsep, 2 * g.lb[1].xbsep,
+                       2 * g.lb[1].ybsep);
+    g.depth = me_depth(w, h);
+    if (g.depth < 1 || g.depth > 12) return DGPU_ERR_SIZE;
+    g.xnsb = bp->xnum_sb;
+    g.ynsb = bp->ynum_sb;
+    g.xnb[0] = 4 * bp->xnum_sb;
+    g.ynb[0] = 4 * bp->ynum_sb;
+    g.pw[0] = w;
+    g.ph[0] = h;
+    for (int l = 1; l <= g.depth; ++l) {
+        g.pw[l] = w / (1 << l);
+        g.ph[l] = h / (1 << l);
+        if (g.pw[l] / 2 < 12 && l < g.depth) return DGPU_ERR_SIZE;
+        g.xnb[l] = (g.xnb[l - 1] >> 1) + (g.pw[l] % g.lb[2].xbsep != 0);
+        g.ynb[l] = (g.ynb[l - 1] >> 1) + (g.ph[l] % g.lb[2].ybsep != 0);
+        // the reference reads outside its vector array when a level has a single column
+        if (g.xnb[l] < 2) return DGPU_ERR_SIZE;
+    }
+    return DGPU_OK;
+}
+
+struct MeBuffers {
+    int16_t* down[3][13];          // pyramid planes of pic, ref1, ref2 (level >= 1)
+    short2* mv[13][2];             // level >= 1 vectors
+    float* cost[13][2];
+    int* best_sad[13][2];
+    short2* best_mv[13][2];
+    int* flags;                    // one flag per unit, reused by every wavefront
+    int* ctl;                      // [0] ticket, [1] error
+    int16_t* up[2];                // upconverted original references
+    float* lambda[3];              // level maps 0, 1, 2
+    short2* lmv[2][2];             // levels 0 and 1: vectors per ref
+    float* lcost[2][2];
+    uint8_t* lmode[2];
+    int16_t* ldcy[2];
+    int16_t* dctmp;
+};
+
+size_t layout(const MeGeometry& g, MeBuffers& B, Arena& a) {
+    for (int s = 0; s < 3; ++s)
+        for (int l = 1; l <= g.depth; ++l) B.down[s][l] = a.take<int16_t>((size_t)g.pw[l] * g.ph[l]);
+    for (int l = 0; l <= g.depth; ++l)
+        for (int r = 0; r < 2; ++r) {
+            const size_t n = (size_t)g.xnb[l] * g.ynb[l];
+            B.mv[l][r] = l ? a.take<short2>(n) : nullptr;
+            B.cost[l][r] = l ? a.take<float>(3 * n) : nullptr;
+            B.best_sad[l][r] = a.take<int>(n);
+            B.best_mv[l][r] = a.take<short2>(n);
+        }
+    size_t maxunits = 0;
+    for (int l = 0; l <= g.depth; ++l) maxunits = std::max(maxunits, (size_t)g.xnb[l] * g.ynb[l]);
+    B.flags = a.take<int>(2 * maxunits);
+    B.ctl = a.take<int>(64);
+    for (int r = 0; r < 2; ++r) B.up[r] = a.take<int16_t>(4 * (size_t)g.w * g.h);
+    const size_t nb = (size_t)g.xnb[0] * g.ynb[0];
+    B.lambda[2] = a.take<float>(nb);
+    B.lambda[1] = a.take<float>(nb / 4);
+    B.lambda[0] = a.take<float>(nb / 16);
+    for (int lv = 0; lv < 2; ++lv) {
+        const size_t n = lv ? nb / 4 : nb / 16;
+        for (int r = 0; r < 2; ++r) {
+            B.lmv[lv][r] = a.take<short2>(n);
+            B.lcost[lv][r] = a.take<float>(3 * n);
+        }
+        B.lmode[lv] = a.take<uint8_t>(n);
+        B.ldcy[lv] = a.take<int16_t>(n);
+    }
+    B.dctmp = a.take<int16_t>(3 * nb);
+    return a.used;
+}
+
+int launch_pel(PelLaunch& L, int* ctl, cudaStream_t st) {
+    if (L.njobs == 0) return DGPU_OK;
+    L.ticket = ctl;
+    L.err = ctl + 1;
+    DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
+    pel_lists_kernel<<<(L.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, 0, st>>>(L);
+    DGPU_CHECK_LAUNCH();
+    const int grid = std::min((L.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, 148 * 8);
+    pel_wavefront_kernel<<<grid, ME_THREADS, 0, st>>>(L);
+    DGPU_CHECK_LAUNCH();
+    return DGPU_OK;
+}
+
+}  // namespace
+}  // namespace dgpu
+
+using namespace dgpu;
+
+extern "C" int dgpu_me_depth(int w, int h) { return me_depth(w, h); }
+
+extern "C" size_t dgpu_me_workspace_bytes(int cformat, int w, int h, const dgpu_block_params* bp, int nref) {
+    MeGeometry g;
+    if (me_geometry(cformat, w, h, bp, nref, g) != DGPU_OK) return 0;
+    MeBuffers B;
+    Arena a{nullptr, 0, 0};
+    return layout(g, B, a) + 256;
+}
+
+extern "C" int dgpu_motion_estimate(int cformat, int w, int h, const dgpu_block_params* bp, int nref,
+                                    const int16_t* const* pic, const int16_t* const* ref1,
+                                    const int16_t* const* ref2, int luma_depth, float lambda, int stages,
+                                    int16_t* mv_out, float* cost_out, uint8_t* mode_out, int16_t* dc_out,
+                                    uint8_t* split_out, float* sbcost_out, void* workspace, size_t ws_bytes,
+                                    void* stream) {
+    if (!pic || !ref1 || !pic[0] || !ref1[0] || !mv_out || !cost_out) return DGPU_ERR_ARG;
+    if (nref == 2 && (!ref2 || !ref2[0])) return DGPU_ERR_ARG;
+    if (stages >= 3 && (!mode_out || !dc_out || !split_out || !sbcost_out || !pic[1] || !pic[2]))
+        return DGPU_ERR_ARG;
+    if (cformat < 0 || cformat > 2 || luma_depth < 2 || luma_depth > 15) return DGPU_ERR_ARG;
+    MeGeometry g;
+    int rc = me_geometry(cformat, w, h, bp, nref, g);
+    if (rc) return rc;
+    if (g.lb[0].xblen > 32 * 8 || g.lb[2].xblen > 64) return DGPU_ERR_SIZE;
+    cudaStream_t st = as_stream(stream);
+    const size_t need = dgpu_me_workspace_bytes(cformat, w, h, bp, nref);
+    if (!workspace) {
+        rc = library_scratch(need, &workspace);
+        if (rc) return rc;
+    } else if (ws_bytes < need) {
+        return DGPU_ERR_NOMEM;
+    }
+    MeBuffers B;
+    Arena a{static_cast<char*>(workspace), 0, need};
+    layout(g, B, a);
+    DGPU_CHECK_CUDA(cudaMemsetAsync(B.ctl, 0, 2 * sizeof(int), st));
+    const int16_t* src0[3] = {pic[0], ref1[0], nref > 1 ? ref2[0] : ref1[0]};
+    const size_t nb = (size_t)g.xnb[0] * g.ynb[0];
+    short2* mv0[2] = {reinterpret_cast<short2*>(mv_out), reinterpret_cast<short2*>(mv_out) + nb};
+    float* cost0[2] = {cost_out, cost_out + 3 * nb};
+
+    // ---- pyramids (PixelMatcher::MakePicHierarchy) ----
+    for (int l = 1; l <= g.depth; ++l) {
+        const int16_t* in[3];
+        int16_t* out[3];
+        int iw[3], ih[3], is[3], os[3];
+        const int ns = nref > 1 ? 3 : 2;
+        for (int s = 0; s < ns; ++s) {
+            in[s] = l == 1 ? src0[s] : B.down[s][l - 1];
+            out[s] = B.down[s][l];
+            iw[s] = g.pw[l - 1];
+            ih[s] = g.ph[l - 1];
+            is[s] = g.pw[l - 1];
+            os[s] = g.pw[l];
+        }
+        rc = dgpu_downconvert_batch(ns, in, iw, ih, is, out, os, stream);
+        if (rc) return rc;
+    }
+    // ---- pel search, coarsest level first (PixelMatcher::DoSearch) ----
+    for (int l = g.depth; l >= 0; --l) {
+        PelLaunch L{};
+        L.o = g.lb[2];
+        int total = 0;
+        for (int r = 0; r < nref; ++r) {
+            PelJob& J = L.job[L.njobs++];
+            J.pic = l ? B.down[0][l] : src0[0];
+            J.ref = l ? B.down[1 + r][l] : src0[1 + r];
+            J.pw = g.pw[l];
+            J.ph = g.ph[l];
+            J.xnb = g.xnb[l];
+            J.ynb = g.ynb[l];
+            J.mv = l ? B.mv[l][r] : mv0[r];
+            J.cost = l ? B.cost[l][r] : cost0[r];
+            J.guide = l < g.depth ? B.mv[l + 1][r] : nullptr;
+            J.gxnb = l < g.depth ? g.xnb[l + 1] : 0;
+            J.gynb = l < g.depth ? g.ynb[l + 1] : 0;
+            J.radius = std::min(l + 1, 5);
+            J.best_sad = B.best_sad[l][r];
+            J.best_mv = B.best_mv[l][r];
+            J.flags = B.flags + (size_t)r * g.xnb[l] * g.ynb[l];
+            J.first = total;
+            total += J.xnb * J.ynb;
+        }
+        L.total = total;
+        DGPU_CHECK_CUDA(cudaMemsetAsync(B.flags, 0, sizeof(int) * total, st));
+        rc = launch_pel(L, B.ctl, st);
+        if (rc) return rc;
+    }
+    int err_host = 0;
+    if (stages >= 2) {
+        // ---- lambda map on the host (long double statistics, as the reference) ----
+        std::vector<short2> hmv(nref * nb);
+        std::vector<float> hl(nb);
+        DGPU_CHECK_CUDA(cudaMemcpyAsync(hmv.data(), mv_out, sizeof(short2) * nref * nb, cudaMemcpyDeviceToHost, st));
+        DGPU_CHECK_CUDA(cudaMemcpyAsync(&err_host, B.ctl + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
+        if (err_host) return DGPU_ERR_CUDA;
+        lambda_map(hmv.data(), hmv.data() + nb, nref, g.xnb[0], g.ynb[0], lambda, hl.data());
+        DGPU_CHECK_CUDA(cudaMemcpyAsync(B.lambda[2], hl.data(), sizeof(float) * nb, cudaMemcpyHostToDevice, st));
+        // ---- upconverted original references (EncPicture::UpOrigData) ----
+        for (int r = 0; r < nref; ++r) {
+            rc = dgpu_upconvert(src0[1 + r], w, h, w, luma_depth, B.up[r], 2 * w, stream);
+            if (rc) return rc;
+        }
+        // ---- sub-pel refinement ----
+        SubLaunch S{};
+        S.o = g.lb[2];
+        S.prec = bp->precision;
+        int total = 0;
+        for (int r = 0; r < nref; ++r) {
+            SubJob& J = S.job[S.njobs++];
+            J.pic = src0[0];
+            J.up = B.up[r];
+            J.pw = w;
+            J.ph = h;
+            J.xnb = g.xnb[0];
+            J.ynb = g.ynb[0];
+            J.mv = mv0[r];
+            J.cost = cost0[r];
+            J.lambda = B.lambda[2];
+            J.flags = B.flags + (size_t)r * nb;
+            J.first = total;
+            total += (int)nb;
+        }
+        S.total = total;
+        S.ticket = B.ctl;
+        S.err = B.ctl + 1;
+        DGPU_CHECK_CUDA(cudaMemsetAsync(B.flags, 0, sizeof(int) * total, st));
+        DGPU_CHECK_CUDA(cudaMemsetAsync(B.ctl, 0, sizeof(int), st));
+        const int grid = std::min((total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, 148 * 8);
+        subpel_wavefront_kernel<<<grid, ME_THREADS, 0, st>>>(S);
+        DGPU_CHECK_LAUNCH();
+        if (stages >= 3) {
+            // ---- lambda maps of the superblock and sub-superblock levels ----
+            const float f0 = (float)(16 * g.lb[2].xblen * g.lb[2].yblen) / (float)(g.lb[0].xblen * g.lb[0].yblen);
+            const float f1 = (float)(4 * g.lb[2].xblen * g.lb[2].yblen) / (float)(g.lb[1].xblen * g.lb[1].yblen);
+            std::vector<float> l0(nb / 16), l1(nb / 4);
+            level_lambda_map(hl.data(), g.xnb[0], 0, g.xnb[0] / 4, g.ynb[0] / 4, (float)(1.0 / f0), l0.data());
+            level_lambda_map(hl.data(), g.xnb[0], 1, g.xnb[0] / 2, g.ynb[0] / 2, (float)(1.0 / f1), l1.data());
+            DGPU_CHECK_CUDA(cudaMemcpyAsync(B.lambda[0], l0.data(), sizeof(float) * l0.size(), cudaMemcpyHostToDevice, st));
+            DGPU_CHECK_CUDA(cudaMemcpyAsync(B.lambda[1], l1.data(), sizeof(float) * l1.size(), cudaMemcpyHostToDevice, st));
+            // fresh level data (a new MEData in the reference): zero vectors, costs, DCs
+            for (int lv = 0; lv < 2; ++lv) {
+                const size_t n = lv ? nb / 4 : nb / 16;
+                for (int r = 0; r < 2; ++r) {
+                    DGPU_CHECK_CUDA(cudaMemsetAsync(B.lmv[lv][r], 0, sizeof(short2) * n, st));
+                    DGPU_CHECK_CUDA(cudaMemsetAsync(B.lcost[lv][r], 0, sizeof(float) * 3 * n, st));
+                }
+                DGPU_CHECK_CUDA(cudaMemsetAsync(B.ldcy[lv], 0, sizeof(int16_t) * n, st));
+                DGPU_CHECK_CUDA(cudaMemsetAsync(B.lmode[lv], 0, n, st));
+            }
+            // the picture's DC arrays start at zero (a fresh MvData)
+            DGPU_CHECK_CUDA(cudaMemsetAsync(dc_out, 0, sizeof(int16_t) * 3 * nb, st));
+            ModeLaunch M{};
+            M.nref = nref;
+            M.prec = bp->precision;
+            for (int i = 0; i < 3; ++i) M.lb[i] = g.lb[i];
+            M.level_factor[0] = f0;
+            M.level_factor[1] = f1;
+            M.level_factor[2] = 1.0f;
+            ModeJob& J = M.job[M.njobs++];
+            J.pic = src0[0];
+            J.up[0] = B.up[0];
+            J.up[1] = nref > 1 ? B.up[1] : B.up[0];
+            J.pw = w;
+            J.ph = h;
+            for (int lv = 0; lv < 3; ++lv) {
+                LevelData& D = J.lev[lv];
+                D.xnb = g.xnb[0] >> (2 - lv);
+                D.ynb = g.ynb[0] >> (2 - lv);
+                D.lambda = B.lambda[lv];
+                if (lv == 2) {
+                    D.mv[0] = mv0[0];
+                    D.mv[1] = nref > 1 ? mv0[1] : mv0[0];
+                    D.cost[0] = cost0[0];
+                    D.cost[1] = nref > 1 ? cost0[1] : cost0[0];
+                    D.mode = mode_out;
+                    D.dcy = dc_out;
+                } else {
+                    D.mv[0] = B.lmv[lv][0];
+                    D.mv[1] = B.lmv[lv][1];
+                    D.cost[0] = B.lcost[lv][0];
+                    D.cost[1] = B.lcost[lv][1];
+                    D.mode = B.lmode[lv];
+                    D.dcy = B.ldcy[lv];
+                }
+            }
+            J.sbcost = sbcost_out;
+            J.split = split_out;
+            J.xnsb = g.xnsb;
+            J.ynsb = g.ynsb;
+            J.flags = B.flags;
+            J.first = 0;
+            M.total = g.xnsb * g.ynsb;
+            M.ticket = B.ctl;
+            M.err = B.ctl + 1;
+            DGPU_CHECK_CUDA(cudaMemsetAsync(B.flags, 0, sizeof(int) * M.total, st));
+            DGPU_CHECK_CUDA(cudaMemsetAsync(B.ctl, 0, sizeof(int), st));
+            const int mgrid = std::min((M.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, 148 * 8);
+            mode_wavefront_kernel<<<mgrid, ME_THREADS, 0, st>>>(M);
+            DGPU_CHECK_LAUNCH();
+            // ---- DC values of all three components ----
+            DcLaunch D{};
+            int dtotal = 0;
+            for (int c = 0; c < 3; ++c) {
+                const int xs = (c && cformat != 0) ? 1 : 0, ys = (c && cformat == 2) ? 1 : 0;
+                DcJob& Jd = D.job[D.njobs++];
+                Jd.pic = pic[c];
+                Jd.pw = w >> xs;
+                Jd.ph = h >> ys;
+                Jd.o = make_olb(g.lb[2].xblen >> xs, g.lb[2].yblen >> ys, g.lb[2].xbsep >> xs, g.lb[2].ybsep >> ys);
+                Jd.tmp = B.dctmp + (size_t)c * nb;
+                Jd.dc = dc_out + (size_t)c * nb;
+                Jd.xnb = g.xnb[0];
+                Jd.ynb = g.ynb[0];
+                Jd.first = dtotal;
+                dtotal += (int)nb;
+            }
+            D.total = dtotal;
+            block_dc_kernel<<<(dtotal + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, 0, st>>>(D);
+            DGPU_CHECK_LAUNCH();
+            smooth_dc_kernel<<<(dtotal + 255) / 256, 256, 0, st>>>(D);
+            DGPU_CHECK_LAUNCH();
+        }
+    }
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(&err_host, B.ctl + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
+    if (err_host) return DGPU_ERR_CUDA;
+    return DGPU_OK;
+}

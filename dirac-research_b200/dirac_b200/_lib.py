@@ -74,6 +74,13 @@ SIGNATURES = {
         [c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
          P_void, P_int, P_void, P_void, c_int, c_int, c_void_p],
     ),
+    "dgpu_me_depth": (c_int, [c_int, c_int]),
+    "dgpu_me_workspace_bytes": (c_size_t, [c_int, c_int, c_int, c_void_p, c_int]),
+    "dgpu_motion_estimate": (
+        c_int,
+        [c_int, c_int, c_int, c_void_p, c_int, P_void, P_void, P_void, c_int, ctypes.c_float, c_int,
+         c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p],
+    ),
 }
 
 

@@ -103,3 +103,46 @@ class MotionCompensator:
             _lib.ptr_array([u.data_ptr() for u in ref1up]), _lib.ptr_array([u.data_ptr() for u in ups2]),
             clip_depths[0], clip_depths[1], _sp(stream))
         _lib.check(rc, "dgpu_motion_compensate")
+
+
+class MotionEstimator:
+    """Mirror of PictureCompressor::PixelME / SubPixelME / ModeDecisionME for one picture.
+
+    Estimate(pic, ref1, ref2=None, lambda_=..., stages=3) takes the original component planes
+    as int16 CUDA tensors and returns a dict of CUDA tensors: mv (nref, ynb, xnb, 2) int16,
+    cost (nref, ynb, xnb, 3) float32 (SAD, mvcost, total), and after stage 3 mode (ynb, xnb)
+    uint8, dc (3, ynb, xnb) int16, split / sbcost (ynsb, xnsb)."""
+
+    def __init__(self, bp, cformat=FORMAT420, luma_depth=8):
+        self.lib = _lib.load()
+        self.bp = bp
+        self.cformat = cformat
+        self.luma_depth = luma_depth
+
+    def Estimate(self, pic, ref1, ref2=None, lambda_=10.0, stages=3, stream=None):
+        for t in list(pic) + list(ref1) + (list(ref2) if ref2 is not None else []):
+            _i16(t, "plane")
+            if not t.is_contiguous():
+                raise ValueError("motion estimation planes must be dense")
+        nref = 2 if ref2 is not None else 1
+        h, w = pic[0].shape
+        bp = self.bp
+        ynb, xnb = 4 * bp.ynum_sb, 4 * bp.xnum_sb
+        dev = pic[0].device
+        out = {
+            "mv": torch.zeros((nref, ynb, xnb, 2), dtype=torch.int16, device=dev),
+            "cost": torch.zeros((nref, ynb, xnb, 3), dtype=torch.float32, device=dev),
+            "mode": torch.zeros((ynb, xnb), dtype=torch.uint8, device=dev),
+            "dc": torch.zeros((3, ynb, xnb), dtype=torch.int16, device=dev),
+            "split": torch.zeros((bp.ynum_sb, bp.xnum_sb), dtype=torch.uint8, device=dev),
+            "sbcost": torch.zeros((bp.ynum_sb, bp.xnum_sb), dtype=torch.float32, device=dev),
+        }
+        r2 = ref2 if ref2 is not None else ref1
+        rc = self.lib.dgpu_motion_estimate(
+            self.cformat, w, h, ctypes.byref(bp), nref, _lib.ptr_array([p.data_ptr() for p in pic]),
+            _lib.ptr_array([p.data_ptr() for p in ref1]), _lib.ptr_array([p.data_ptr() for p in r2]),
+            self.luma_depth, ctypes.c_float(lambda_), stages, out["mv"].data_ptr(), out["cost"].data_ptr(),
+            out["mode"].data_ptr(), out["dc"].data_ptr(), out["split"].data_ptr(), out["sbcost"].data_ptr(),
+            None, 0, _sp(stream))
+        _lib.check(rc, "dgpu_motion_estimate")
+        return out

@@ -178,6 +178,36 @@ int dgpu_motion_compensate(int add_or_sub, int cformat, int w, int h, const dgpu
                            const int16_t* const* ref2up, int clip_luma_depth,
                            int clip_chroma_depth, void* stream);
 
+/* ---------------------------------------------------------------------------------------
+ * Motion estimation of one picture
+ * Replaces PictureCompressor::PixelME / SubPixelME / ModeDecisionME
+ * (libdirac_encoder/picture_compress.cpp:76-300) and the classes they drive: PixelMatcher
+ * (libdirac_motionest/pixel_match.cpp:59-380), MEData::SetLambdaMap
+ * (libdirac_common/motion.cpp:128-196), SubpelRefine (me_subpel.cpp:65-176) and ModeDecider
+ * (me_mode_decn.cpp:66-573).
+ *
+ * pic, ref1, ref2: the original (not reconstructed) component planes, dense (stride = width),
+ * device memory; only luma is searched, all three feed the DC values.  nref 1 or 2.  stages:
+ * 1 pel search over the pyramid, 2 adds the lambda map (lambda: the picture's ME lambda,
+ * e.g. EncoderParams::L1MELambda) and sub-pel refinement, 3 adds mode decision and DC values.
+ * MV precision (bp->precision) must be 1 (half), 2 (quarter) or 3 (eighth).
+ * Outputs, device memory, blocks = 16 x superblocks, row-major:
+ *   mv_out    int16 [nref][blocks][2]           cost_out  float [nref][blocks][3] (SAD, mvcost, total)
+ *   mode_out  uint8 [blocks]    dc_out int16 [3][blocks]    split_out uint8 / sbcost_out float [superblocks]
+ * The call synchronises the stream once (between stages 1 and 2, where the host computes the
+ * lambda map's statistics as the reference does in long double) and at its end.
+ * workspace: at least dgpu_me_workspace_bytes(...) bytes of device memory, or NULL for the
+ * library's own buffer.  A wait that times out inside a kernel returns DGPU_ERR_CUDA.
+ * ------------------------------------------------------------------------------------- */
+int dgpu_me_depth(int w, int h);
+size_t dgpu_me_workspace_bytes(int cformat, int w, int h, const dgpu_block_params* bp, int nref);
+int dgpu_motion_estimate(int cformat, int w, int h, const dgpu_block_params* bp, int nref,
+                         const int16_t* const* pic, const int16_t* const* ref1,
+                         const int16_t* const* ref2, int luma_depth, float lambda, int stages,
+                         int16_t* mv_out, float* cost_out, uint8_t* mode_out, int16_t* dc_out,
+                         uint8_t* split_out, float* sbcost_out, void* workspace, size_t ws_bytes,
+                         void* stream);
+
 #ifdef __cplusplus
 }
 #endif

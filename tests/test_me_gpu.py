@@ -1,0 +1,94 @@
+"""GPU parity of motion estimation (pel pyramid search, lambda map + sub-pel refinement, mode
+decision + DC) against the oracle, stage by stage, and against the reference's golden
+fixtures.  Vectors, modes, splits and DCs are integers; costs are the reference's float
+values: all compared bit-exactly."""
+import numpy as np
+import pytest
+import torch
+
+from test_oracle import me_case
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def synth_frames(w, h, chroma, seed, vmax=8, nr=8):
+    from dirac_b200 import synth
+
+    seq = synth.make_sequence(w, h, 3, n_rects=nr, vmax=vmax, seed=seed, chroma=chroma)
+    return [[synth.to_signed(p) for p in fr] for fr in seq]
+
+
+def run_gpu(gpu, cf, bp, pic, r1, r2, lam, stages):
+    from oracle import BlockParams
+
+    bpg = gpu.BlockParams(*(getattr(bp, f) for f, _ in BlockParams._fields_))
+    me = gpu.MotionEstimator(bpg, cf)
+    out = me.Estimate([dev(p) for p in pic], [dev(p) for p in r1], [dev(p) for p in r2] if r2 is not None else None,
+                      lam, stages)
+    return {k: v.cpu().numpy() for k, v in out.items()}
+
+
+KEYS = {1: ("mv", "cost"), 2: ("mv", "cost"), 3: ("mv", "cost", "mode", "dc", "split", "sbcost")}
+
+
+def compare(got, want, stages, msg):
+    for k in KEYS[stages]:
+        a, b = got[k], want[k]
+        if k in ("mv", "cost"):
+            a, b = a[: b.shape[0]], b
+        if not np.array_equal(a, b):
+            bad = np.argwhere(a != b)
+            raise AssertionError(f"{msg}: {k} differs at {len(bad)} places, first {bad[:3].tolist()}: "
+                                 f"gpu {a[tuple(bad[0])]} oracle {b[tuple(bad[0])]}")
+
+
+def test_me_golden(gpu, golden):
+    g = golden("me.npz")
+    for k in range(3):
+        cf, bp, pic, r1, r2, lam, want = me_case(g, k)
+        got = run_gpu(gpu, cf, bp, pic, r1, r2, lam, 3)
+        compare(got, want, 3, f"golden case {k}")
+
+
+CASES = [
+    # w, h, olb, prec, nref, chroma, vmax, nrects
+    (352, 288, (12, 12, 8, 8), 2, 2, "420", 8, 8),
+    (352, 288, (12, 12, 8, 8), 2, 1, "420", 8, 8),
+    (720, 576, (12, 12, 8, 8), 3, 2, "422", 16, 16),
+    (480, 272, (16, 16, 12, 12), 1, 2, "444", 12, 12),
+    (1920, 1080, (16, 16, 12, 12), 2, 2, "420", 24, 24),
+]
+
+
+@pytest.mark.parametrize("stages", [1, 2, 3])
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_me_vs_oracle(gpu, oracle, case, stages):
+    from oracle import BlockParams
+
+    w, h, olb, prec, nref, chroma, vmax, nr = CASES[case]
+    f = synth_frames(w, h, chroma, seed=4000 + case, vmax=vmax, nr=nr)
+    xbl, ybl, xbs, ybs = olb
+    bp = BlockParams(prec, xbl, ybl, xbs, ybs, (w + 4 * xbs - 1) // (4 * xbs), (h + 4 * ybs - 1) // (4 * ybs))
+    cf = {"444": 0, "422": 1, "420": 2}[chroma]
+    lam = 10.0
+    r2 = f[2] if nref == 2 else None
+    want = oracle.motion_estimate(cf, f[1], f[0], r2, bp, lam, stages)
+    got = run_gpu(gpu, cf, bp, f[1], f[0], r2, lam, stages)
+    compare(got, want, stages, f"case {case} stages {stages}")
+
+
+def test_me_nondyadic_lambda(gpu, oracle):
+    """A lambda with a long mantissa makes the float cost sums round: the GPU must still
+    reproduce the reference's sequential float accumulation."""
+    from oracle import BlockParams
+
+    f = synth_frames(352, 288, "420", seed=77, vmax=10, nr=10)
+    bp = BlockParams(2, 12, 12, 8, 8, 11, 9)
+    lam = float(np.float32(2 * np.sqrt(4 * 10 ** ((12 - 5.5) / 2.5) / 16)))
+    want = oracle.motion_estimate(2, f[1], f[0], f[2], bp, lam, 3)
+    got = run_gpu(gpu, 2, bp, f[1], f[0], f[2], lam, 3)
+    compare(got, want, 3, "non-dyadic lambda")
