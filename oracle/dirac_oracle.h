@@ -81,6 +81,22 @@ int orc_motion_estimate(int cformat, int w, int h, const orc_block_params* bp, i
                         int luma_depth, float lambda, int stages, int16_t* mv_out, float* cost_out,
                         uint8_t* mode_out, int16_t* dc_out, uint8_t* split_out, float* sbcost_out);
 
+/* QuantiserLists (common.cpp:931-981): quantisation factor x4 and reconstruction offsets x4. */
+int orc_qf4(int q);
+int orc_intra_offset4(int q);
+int orc_inter_offset4(int q);
+/* Subband b (1-based, SubbandList order: per level HH, LH, HL; DC last) of a cw x ch array. */
+void orc_band_rect(int depth, int cw, int ch, int b, int* xp, int* yp, int* xl, int* yl);
+
+/* Residue coding of one transformed component: quantiser choice per band (band weights,
+ * entropy factors and the code-block grid per band are inputs), then quantisation with
+ * in-place reconstruction of c (cw x ch, dense).  Outputs per band: quantiser, skip flag,
+ * estimated bits; per code block (bands concatenated, raster) the skip flag; optionally the
+ * signed quantised indices qout (cw x ch; the intra DC band holds its prediction residues). */
+int orc_code_residue(int intra, int depth, int32_t* c, int cw, int ch, float lambda, const float* band_wt,
+                     const float* band_ecf, const int* band_ncb, int* band_qidx, int* band_skip, int* band_bits,
+                     uint8_t* cb_skip, int32_t* qout);
+
 /* Picture::ClipComponent: clamp to [-2^(d-1), 2^(d-1)-1]. */
 void orc_clip(int16_t* pic, size_t n, int bit_depth);
 

@@ -128,6 +128,25 @@ class Oracle:
     def me_depth(self, w, h):
         return self.lib.orc_me_depth(w, h)
 
+    def code_residue(self, intra, depth, coeff, lambda_, band_wt, band_ecf, band_ncb):
+        """Quantiser choice + quantisation; returns (recon, qidx, skip, bits, cb_skip, qindices)."""
+        c = np.array(coeff, dtype=np.int32, copy=True, order="C")
+        ch, cw = c.shape
+        nb = 3 * depth + 1
+        wt = np.ascontiguousarray(band_wt, dtype=np.float32)
+        ecf = np.ascontiguousarray(band_ecf, dtype=np.float32)
+        ncb = np.ascontiguousarray(band_ncb, dtype=np.int32)
+        q = np.zeros(nb, np.int32)
+        sk = np.zeros(nb, np.int32)
+        bits = np.zeros(nb, np.int32)
+        cbs = np.zeros(int(np.sum(ncb[0::2] * ncb[1::2])), np.uint8)
+        qo = np.zeros_like(c)
+        rc = self.lib.orc_code_residue(intra, depth, _p(c), cw, ch, ctypes.c_float(lambda_), _p(wt), _p(ecf), _p(ncb),
+                                       _p(q), _p(sk), _p(bits), _p(cbs), _p(qo))
+        if rc:
+            raise ValueError(f"orc_code_residue rc={rc}")
+        return c, q, sk, bits, cbs, qo
+
 
 def _me_call(fn, is_oracle, cformat, pic, ref1, ref2, bp, lambda_, stages, luma_depth):
     """Shared driver of orc_motion_estimate / ref_motion_estimate; returns a dict of arrays."""
@@ -222,3 +241,25 @@ class Reference:
     def motion_estimate(self, cformat, pic, ref1, ref2, bp, lambda_, stages=3, luma_depth=8):
         return _me_call(self.lib.ref_motion_estimate, False, cformat, pic, ref1, ref2, bp, lambda_, stages,
                         luma_depth)
+
+    def code_residue(self, cformat, w, h, comp, intra, filt, depth, coeff, lambda_, cpd_scale=1.0):
+        """The reference's residue coding of one component; returns a dict with the
+        reconstruction and the per-band / per-code-block choices and their inputs."""
+        c = np.array(coeff, dtype=np.int32, copy=True, order="C")
+        ch, cw = c.shape
+        nb = 3 * depth + 1
+        q = np.zeros(nb, np.int32)
+        sk = np.zeros(nb, np.int32)
+        wt = np.zeros(nb, np.float64)
+        ecf = np.zeros(nb, np.float32)
+        bits = np.zeros(nb, np.int32)
+        ncb = np.zeros(2 * nb, np.int32)
+        cbs = np.zeros(1 << 20, np.uint8)
+        rc = self.lib.ref_code_residue(cformat, w, h, comp, intra, filt, depth, _p(c), cw, ch, ctypes.c_float(lambda_),
+                                       ctypes.c_float(cpd_scale), _p(q), _p(sk), _p(wt), _p(ecf), _p(bits), _p(ncb),
+                                       _p(cbs))
+        if rc:
+            raise ValueError("ref_code_residue failed")
+        ncbt = int(np.sum(ncb[0::2] * ncb[1::2]))
+        return {"recon": c, "qidx": q, "skip": sk, "wt": wt, "ecf": ecf, "bits": bits, "ncb": ncb,
+                "cb_skip": cbs[:ncbt].copy()}

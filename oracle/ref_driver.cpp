@@ -20,6 +20,9 @@
 #include <libdirac_motionest/pixel_match.h>
 #include <libdirac_motionest/me_subpel.h>
 #include <libdirac_motionest/me_mode_decn.h>
+#include <libdirac_encoder/quant_chooser.h>
+#include <libdirac_encoder/comp_compress.h>
+#include <libdirac_byteio/component_byteio.h>
 
 using namespace dirac;
 
@@ -276,6 +279,105 @@ int ref_motion_estimate(int cformat, int w, int h, int luma_depth, int chroma_de
                     sbcost_out[(size_t)j * me.SBSplit().LengthX() + i] = me.SBCosts()[j][i];
                 }
         }
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+// Residue coding of one transformed component, as PictureCompressor::CodeResidue runs it
+// (libdirac_encoder/picture_compress.cpp:391-461): band weights (CoeffArray::SetBandWeights),
+// code blocks (SetupCodeBlocks :582-601), quantiser choice per band from DC to HF
+// (SelectQuantisers / SelectMultiQuants :603-677, with the intra DC band's AddSubAverage
+// :679-709 restated here because those PictureCompressor members are private), then
+// CompCompressor::Compress, which quantises and reconstructs every coefficient in place.
+// coeff (ch x cw) is read and overwritten with the reconstruction.  Per band (band-list
+// order, 1-based band b at index b-1): quantiser index, skip flag, weight, entropy factor,
+// estimated bits, code-block grid (x, y) and the code blocks' skip flags (concatenated).
+int ref_code_residue(int cformat, int w, int h, int comp, int intra, int filter, int depth, int* coeff, int cw,
+                     int ch, float lambda, float cpd_scale, int* band_qidx, int* band_skip, double* band_wt,
+                     float* band_ecf, int* band_bits, int* band_ncb, unsigned char* cb_skip) {
+    try {
+        const ChromaFormat cf = (ChromaFormat)cformat;
+        const PictureType pt = intra ? INTRA_PICTURE : INTER_PICTURE;
+        EncoderParams ep(VIDEO_FORMAT_CUSTOM, pt, 2, true);
+        ep.SetXl(w);
+        ep.SetYl(h);
+        ep.SetTransformDepth(depth);
+        ep.SetTransformFilter((WltFilter)filter);
+        ep.SetUsualCodeBlocks(pt);
+        EntropyCorrector* ec = new EntropyCorrector(depth);
+        ep.SetEntropyFactors(ec);
+        PictureParams pp(cf, w, h, 8, 8);
+        pp.SetPicSort(intra ? PictureSort::IntraRefPictureSort() : PictureSort::InterRefPictureSort());
+        if (!intra) pp.Refs().push_back(0);
+        CoeffArray c(ch, cw, (CompSort)comp);
+        fill_arr(c, coeff);
+        SubbandList& bands = c.BandList();
+        bands.Init(depth, cw, ch);
+        c.SetBandWeights(ep, pp, (CompSort)comp, cpd_scale);
+        for (int b = 1; b <= bands.Length(); ++b) {
+            int xr = 1, yr = 1;
+            if (ep.SpatialPartition()) {
+                const int level = depth - (b - 1) / 3;
+                const CodeBlocks& cb = ep.GetCodeBlocks(level);
+                xr = cb.HorizontalCodeBlocks();
+                yr = cb.VerticalCodeBlocks();
+            }
+            bands(b).SetNumBlocks(yr, xr);
+        }
+        OneDArray<unsigned int> est_bits(Range(1, 3 * depth + 1));
+        for (int b = bands.Length(); b >= 1; --b) {
+            Subband& node = bands(b);
+            node.SetUsingMultiQuants(ep.GetCodeBlockMode() == QUANT_MULTIPLE &&
+                                     (node.GetCodeBlocks().LengthX() > 1 || node.GetCodeBlocks().LengthY() > 1));
+        }
+        for (int b = bands.Length(); b >= 1; --b) {
+            Subband& node = bands(b);
+            QuantChooser qc(c, lambda);
+            const bool dc_intra = (b == bands.Length()) && intra;
+            if (dc_intra) {  // AddSubAverage(SUBTRACT): raster DPCM of the DC band
+                ValueType last = 0;
+                for (int j = 0; j < node.Yl(); ++j)
+                    for (int i = 0; i < node.Xl(); ++i) {
+                        const ValueType keep = c[j][i];
+                        c[j][i] -= last;
+                        last = keep;
+                    }
+            }
+            const float ecf = ep.EntropyFactors().Factor(b, pp, (CompSort)comp);
+            qc.SetEntropyCorrection(ecf);
+            const int bits = qc.GetBestQuant(node);
+            if (dc_intra) {  // AddSubAverage(ADD)
+                ValueType last = 0;
+                for (int j = 0; j < node.Yl(); ++j)
+                    for (int i = 0; i < node.Xl(); ++i) {
+                        c[j][i] += last;
+                        last = c[j][i];
+                    }
+            }
+            node.SetSkip(bits == 0);
+            est_bits[b] = bits;
+            band_ecf[b - 1] = ecf;
+            band_bits[b - 1] = bits;
+        }
+        size_t k = 0;
+        for (int b = 1; b <= bands.Length(); ++b) {
+            const Subband& node = bands(b);
+            band_qidx[b - 1] = node.QuantIndex();
+            band_skip[b - 1] = node.Skipped() ? 1 : 0;
+            band_wt[b - 1] = node.Wt();
+            const TwoDArray<CodeBlock>& cbs = node.GetCodeBlocks();
+            band_ncb[2 * (b - 1)] = cbs.LengthX();
+            band_ncb[2 * (b - 1) + 1] = cbs.LengthY();
+            for (int j = 0; j < cbs.LengthY(); ++j)
+                for (int i = 0; i < cbs.LengthX(); ++i) cb_skip[k++] = cbs[j][i].Skipped() ? 1 : 0;
+        }
+        CompCompressor cc(ep, pp);
+        ComponentByteIO* out = cc.Compress(c, bands, (CompSort)comp, est_bits);
+        delete out;
+        read_arr(c, coeff);
+        delete ec;
         return 0;
     } catch (...) {
         return -1;
