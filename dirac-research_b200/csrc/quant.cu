@@ -1,0 +1,751 @@
+// Quantiser selection statistics and quantisation with reconstruction, for sm_100a.
+//
+// Replaces the data-parallel part of PictureCompressor::SelectQuantisers / QuantChooser
+// (libdirac_encoder/picture_compress.cpp:603-709, quant_chooser.cpp:62-362) and the
+// quantise-and-reconstruct arithmetic of the band coders (GenericBandCodec::CodeVal /
+// CodeCoeffBlock / ClearBlock, band_codec_template.h:53-174, 470-557; IntraDCBandCodec,
+// band_codec.cpp:81-96; CompCompressor::Compress, comp_compress.cpp:64-156).
+//
+// Flow for a batch of components:
+//   1. (intra) the DC band's raster DPCM against the previous int16 value
+//      (AddSubAverage) into a work copy; band and code-block absolute maxima.
+//   2. statistics per band, per candidate quantiser q and per sampling pattern (every 2nd
+//      column and row for the integral and half-step passes, every 2nd row for the
+//      quarter-step pass): count0 = sum of quantised magnitudes, positive / negative counts
+//      and the 4th-power error sum, the last as an exact 128-bit integer.  A sum that the
+//      reference's sequential double accumulation could round (a term of 9741 or more, or a
+//      total of 2^53 or more) is flagged.
+//   3. host: the reference's three-pass Lagrangian search in double precision with the host
+//      libm (exactly the reference's arithmetic); flagged sums are recomputed first by a
+//      sequential double kernel in the reference's order.
+//   4. quantise and reconstruct in place; the intra DC band (prediction from reconstructed
+//      neighbours) as an anti-diagonal wavefront in one CTA.
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "dgpu_internal.cuh"
+
+namespace dgpu {
+namespace {
+
+constexpr int QMAX = 101;          // candidate quantisers per band with statistics (covers |c| < 2^24)
+constexpr int MAX_BANDS = 3 * 8 + 1;
+constexpr uint64_t EXACT_TERM = 9741;  // pow4 of smaller values is exact in double
+constexpr int STAT_THREADS = 256;
+
+// QuantiserLists (libdirac_common/common.cpp:931-981)
+__host__ __device__ inline int qf4(int q) {
+    if (q == 0) return 4;
+    if (q == 1) return 5;
+    const unsigned long long base = 1ull << (q / 4);
+    unsigned long long f;
+    switch (q % 4) {
+        case 0: f = 4 * base; break;
+        case 1: f = (503829 * base + 52958) / 105917; break;
+        case 2: f = (665857 * base + 58854) / 117708; break;
+        default: f = (440253 * base + 32722) / 65444; break;
+    }
+    return (int)f;
+}
+__host__ __device__ inline int intra_off4(int q) { return q == 0 ? 1 : (q == 1 ? 2 : (qf4(q) + 1) >> 1); }
+__host__ __device__ inline int inter_off4(int q) { return q == 0 ? 1 : (q == 1 ? 2 : (3 * qf4(q) + 4) >> 3); }
+
+// SubbandList::Init (wavelet_utils.cpp:144-190): band b (1-based) of a cw x ch array.
+__host__ __device__ inline void band_rect(int depth, int cw, int ch, int b, int& xp, int& yp, int& xl, int& yl) {
+    if (b == 3 * depth + 1) {
+        xp = 0;
+        yp = 0;
+        xl = cw >> depth;
+        yl = ch >> depth;
+        return;
+    }
+    const int level = (b - 1) / 3 + 1, kind = (b - 1) % 3;
+    xl = cw >> level;
+    yl = ch >> level;
+    xp = (kind == 0 || kind == 2) ? xl : 0;
+    yp = (kind == 0 || kind == 1) ? yl : 0;
+}
+
+struct Stat {  // statistics of one (band, pattern, q), device accumulators
+    unsigned long long count0;
+    unsigned long long posneg;   // positive count (low 32 bits) + negative count (high 32)
+    unsigned long long err_lo, err_hi;
+    unsigned int inexact;
+    unsigned int pad;
+};
+
+struct Comp {
+    const int32_t* coeff;     // transformed component (dense, cw x ch)
+    int32_t* dcwork;          // intra: the DC band after DPCM (xl x yl of the DC band)
+    int cw, ch, depth, intra;
+    int nbands;
+    int band_first;           // index of band 1 in the global band tables
+};
+
+struct BandTask {  // one band: where its data lives and where its statistics go
+    const int32_t* data;      // top-left of the band in its array
+    int stride, xl, yl;
+    int comp;
+    int band;                 // global band index
+    int cb_first, xn, yn;     // code blocks of the band
+};
+
+constexpr int MAX_COMPS = 48;
+constexpr int MAX_TASKS = MAX_COMPS * MAX_BANDS;
+
+struct BandTable {
+    int ntasks;
+    BandTask task[MAX_TASKS];
+};
+
+// ---- 1. DC DPCM and maxima ----------------------------------------------------------------
+
+__global__ void dc_dpcm_kernel(const int32_t* c, int stride, int xl, int yl, int32_t* out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= xl * yl) return;
+    const int j = k / xl, i = k - j * xl;
+    const int prev = k == 0 ? 0 : (int)(int16_t)c[(size_t)((k - 1) / xl) * stride + (k - 1) % xl];
+    out[k] = c[(size_t)j * stride + i] - prev;
+}
+
+// Per band: max |c|.  Per code block: max |c| (for QuantChooser::SetSkip).  Lanes of a warp
+// that fall in the same code block combine their maxima before one atomic.
+__global__ void band_max_kernel(const BandTask* tasks, int* band_max, int* cb_max) {
+    const BandTask T = tasks[blockIdx.y];
+    const int n = T.xl * T.yl;
+    const int stride = gridDim.x * blockDim.x;
+    int m = 0;
+    for (int k0 = blockIdx.x * blockDim.x; k0 < n; k0 += stride) {
+        const int k = k0 + threadIdx.x;
+        int a = 0, cb = -1;
+        if (k < n) {
+            const int j = k / T.xl, i = k - j * T.xl;
+            a = abs(T.data[(size_t)j * T.stride + i]);
+            int cx = (int)(((long long)i * T.xn) / T.xl);
+            while (cx + 1 < T.xn && ((cx + 1) * T.xl) / T.xn <= i) ++cx;
+            while (cx > 0 && (cx * T.xl) / T.xn > i) --cx;
+            int cy = (int)(((long long)j * T.yn) / T.yl);
+            while (cy + 1 < T.yn && ((cy + 1) * T.yl) / T.yn <= j) ++cy;
+            while (cy > 0 && (cy * T.yl) / T.yn > j) --cy;
+            cb = T.cb_first + cy * T.xn + cx;
+        }
+        m = max(m, a);
+        const unsigned grp = __match_any_sync(0xffffffffu, cb);
+        const int gm = __reduce_max_sync(grp, (unsigned)a);
+        if (cb >= 0 && gm > 0 && (threadIdx.x & 31) == __ffs(grp) - 1) atomicMax(&cb_max[cb], gm);
+    }
+    m = __reduce_max_sync(0xffffffffu, (unsigned)m);
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(&band_max[T.band], m);
+}
+
+// ---- 2. statistics ------------------------------------------------------------------------
+
+// Number of quantisers whose statistics a band needs: 4 * (bit length of max) + 5 covers
+// the reference's 4 * floor(log2 max) + 5 whatever its libm rounding.
+__device__ __forceinline__ int stat_range(int maxv) {
+    if (maxv < 1) return 0;
+    const int bitlen = 32 - __clz(maxv);
+    return min(4 * bitlen + 5, QMAX);
+}
+
+// grid: x = chunks of the band's sampled coefficients, y = task, z = pattern (0: 2x2, 1: 1x2).
+__global__ void __launch_bounds__(STAT_THREADS) stats_kernel(const BandTask* tasks, const int* band_max,
+                                                             Stat* stats) {
+    const BandTask T = tasks[blockIdx.y];
+    const int pattern = blockIdx.z;
+    const int xr = pattern ? 1 : 2;
+    const int nq = stat_range(band_max[T.band]);
+    const int sx = (T.xl + xr - 1) / xr, sy = (T.yl + 1) / 2;
+    const int nsamp = sx * sy;
+    const int per_cta = STAT_THREADS * 8;
+    const int base = blockIdx.x * per_cta;
+    if (base >= nsamp || nq == 0) return;
+    __shared__ unsigned long long s_c0[QMAX], s_pn[QMAX], s_lo[QMAX], s_hi[QMAX];
+    __shared__ unsigned int s_inx[QMAX];
+    for (int q = threadIdx.x; q < QMAX; q += STAT_THREADS) {
+        s_c0[q] = s_pn[q] = s_lo[q] = s_hi[q] = 0;
+        s_inx[q] = 0;
+    }
+    __syncthreads();
+    int a[8];
+    bool neg[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const int k = base + t * STAT_THREADS + threadIdx.x;
+        a[t] = -1;
+        neg[t] = false;
+        if (k < nsamp) {
+            const int sj = k / sx, si = k - sj * sx;
+            const int v = T.data[(size_t)(2 * sj) * T.stride + xr * si];
+            a[t] = abs(v);
+            neg[t] = v <= 0;
+        }
+    }
+    const int lane = threadIdx.x & 31;
+    for (int q = (pattern ? 0 : 0); q < nq; q += (pattern ? 1 : 2)) {
+        const unsigned qf = (unsigned)qf4(q);
+        const int off = inter_off4(q);
+        unsigned long long c0 = 0, lo = 0, hi = 0;
+        unsigned int pos = 0, ng = 0, inx = 0;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            if (a[t] < 0) continue;
+            const unsigned qv = ((unsigned)a[t] << 2) / qf;
+            unsigned long long e;
+            if (qv == 0) {
+                e = (unsigned long long)a[t];
+            } else {
+                c0 += qv;
+                const int r = (int)((qv * qf + off + 2) >> 2);
+                e = (unsigned long long)llabs((long long)a[t] - r);
+                if (neg[t]) ++ng; else ++pos;
+            }
+            if (e >= EXACT_TERM) {
+                inx = 1;
+            } else {
+                const unsigned long long p = e * e * e * e;
+                lo += p;
+                if (lo < p) ++hi;
+            }
+        }
+        // warp reduction (128-bit sum with carries)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long olo = __shfl_down_sync(0xffffffffu, lo, o);
+            const unsigned long long ohi = __shfl_down_sync(0xffffffffu, hi, o);
+            const unsigned long long nlo = lo + olo;
+            hi += ohi + (nlo < lo ? 1 : 0);
+            lo = nlo;
+            c0 += __shfl_down_sync(0xffffffffu, c0, o);
+        }
+        pos = __reduce_add_sync(0xffffffffu, pos);
+        ng = __reduce_add_sync(0xffffffffu, ng);
+        inx = __reduce_or_sync(0xffffffffu, inx);
+        if (lane == 0) {
+            atomicAdd(&s_c0[q], c0);
+            atomicAdd(&s_pn[q], (unsigned long long)pos | ((unsigned long long)ng << 32));
+            const unsigned long long old = atomicAdd(&s_lo[q], lo);
+            atomicAdd(&s_hi[q], hi + (old + lo < old ? 1 : 0));
+            if (inx) atomicOr(&s_inx[q], 1u);
+        }
+    }
+    __syncthreads();
+    Stat* S = stats + ((size_t)T.band * 2 + pattern) * QMAX;
+    for (int q = threadIdx.x; q < nq; q += STAT_THREADS) {
+        if (s_c0[q] == 0 && s_pn[q] == 0 && s_lo[q] == 0 && s_hi[q] == 0 && s_inx[q] == 0) continue;
+        atomicAdd(&S[q].count0, s_c0[q]);
+        atomicAdd(&S[q].posneg, s_pn[q]);
+        const unsigned long long old = atomicAdd(&S[q].err_lo, s_lo[q]);
+        atomicAdd(&S[q].err_hi, s_hi[q] + (old + s_lo[q] < old ? 1 : 0));
+        if (s_inx[q]) atomicOr(&S[q].inexact, 1u);
+    }
+}
+
+// Fallback: the reference's sequential double accumulation of pow4(error) for one
+// (band, pattern, q) per thread, in its raster order (quant_chooser.cpp:149-264).
+struct SeqCase {
+    int task, pattern, q;
+};
+
+__global__ void seq_error_kernel(const BandTask* tasks, const SeqCase* cases, int ncases, double* out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ncases) return;
+    const SeqCase C = cases[k];
+    const BandTask T = tasks[C.task];
+    const int xr = C.pattern ? 1 : 2;
+    const int qf = qf4(C.q), off = inter_off4(C.q);
+    double s = 0.0;
+    for (int j = 0; j < T.yl; j += 2)
+        for (int i = 0; i < T.xl; i += xr) {
+            const int a = abs(T.data[(size_t)j * T.stride + i]);
+            const int qv = (a << 2) / qf;
+            double e;
+            if (!qv) {
+                e = (double)a;
+            } else {
+                e = (double)(a - ((qv * qf + off + 2) >> 2));
+            }
+            s = __dadd_rn(s, __dmul_rn(__dmul_rn(__dmul_rn(e, e), e), e));
+        }
+    out[k] = s;
+}
+
+// ---- 4. quantise and reconstruct ------------------------------------------------------------
+
+struct QBand {
+    int32_t* data;      // band top-left in the coefficient array (reconstructed in place)
+    int32_t* qout;      // band top-left in the index array, or null
+    int stride;
+    int xl, yl, xn, yn;
+    int qf, off, skip;
+    const uint8_t* cb_skip;  // code blocks of this band
+    int first;          // first thread-chunk index
+};
+
+constexpr int MAX_QBANDS = 48;
+struct QLaunch {
+    int n;
+    QBand band[MAX_QBANDS];
+};
+
+__device__ __forceinline__ int cb_index(int pos, int len, int n) {
+    int c = (int)(((long long)pos * n) / len);
+    while (c + 1 < n && ((c + 1) * len) / n <= pos) ++c;
+    while (c > 0 && (c * len) / n > pos) --c;
+    return c;
+}
+
+__global__ void quantise_kernel(const __grid_constant__ QLaunch L) {
+    int b = 0;
+    while (b + 1 < L.n && L.band[b + 1].first <= (int)blockIdx.x) ++b;
+    const QBand& B = L.band[b];
+    const int k = (blockIdx.x - B.first) * blockDim.x + threadIdx.x;
+    if (k >= B.xl * B.yl) return;
+    const int j = k / B.xl, i = k - j * B.xl;
+    int32_t* v = B.data + (size_t)j * B.stride + i;
+    int r = 0, qi = 0;
+    if (!B.skip && !B.cb_skip[cb_index(j, B.yl, B.yn) * B.xn + cb_index(i, B.xl, B.xn)]) {
+        const int val = *v;
+        const unsigned qv = ((unsigned)abs(val) << 2) / (unsigned)B.qf;
+        if (qv) {
+            r = (int)((qv * (unsigned)B.qf + B.off + 2) >> 2);
+            if (val <= 0) r = -r;
+        }
+        qi = val < 0 ? -(int)qv : (int)qv;
+    }
+    *v = r;
+    if (B.qout) B.qout[(size_t)j * B.stride + i] = qi;
+}
+
+// Intra DC band: prediction from reconstructed left / top-left / top neighbours
+// (GetPrediction, band_codec_template.h:531-557), one anti-diagonal per step.
+__global__ void dc_intra_kernel(int32_t* c, int32_t* qout, int stride, int xl, int yl, int xn, int yn, int qf,
+                                int off, const uint8_t* cb_skip) {
+    for (int t = 0; t < xl + yl - 1; ++t) {
+        for (int x = threadIdx.x; x < xl; x += blockDim.x) {
+            const int y = t - x;
+            if (y < 0 || y >= yl) continue;
+            int pred;
+            if (y != 0) {
+                if (x != 0) {
+                    const int sum = c[(size_t)y * stride + x - 1] + c[(size_t)(y - 1) * stride + x - 1] +
+                                    c[(size_t)(y - 1) * stride + x] + 3 / 2;
+                    pred = sum < 0 ? (sum - 2) / 3 : sum / 3;
+                } else {
+                    pred = c[(size_t)(y - 1) * stride];
+                }
+            } else {
+                pred = x != 0 ? c[x - 1] : 0;
+            }
+            pred = (int16_t)pred;
+            int32_t* v = c + (size_t)y * stride + x;
+            const bool skip = cb_skip[cb_index(y, yl, yn) * xn + cb_index(x, xl, xn)];
+            if (skip) {
+                *v = pred;
+                if (qout) qout[(size_t)y * stride + x] = 0;
+            } else {
+                const int val = (int16_t)(*v - pred);
+                const unsigned qv = ((unsigned)abs(val) << 2) / (unsigned)qf;
+                int r = 0;
+                if (qv) {
+                    r = (int)((qv * (unsigned)qf + off + 2) >> 2);
+                    if (val <= 0) r = -r;
+                }
+                if (qout) qout[(size_t)y * stride + x] = val < 0 ? -(int)qv : (int)qv;
+                *v = r + pred;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---- host: the reference's Lagrangian choice (quant_chooser.cpp:62-147, 266-318) -------------
+
+struct HostStat {
+    double error;
+    int count0, pos, neg;
+};
+
+struct CostD {
+    double Error, ENTROPY, TOTAL;
+};
+
+CostD lagrangian(const HostStat& s, int count1, float wt, float lambda, float ecf) {
+    CostD c;
+    c.Error = s.error / double(count1);
+    c.Error = std::sqrt(c.Error) / (wt * wt);
+    double p0 = double(s.count0) / double(s.count0 + count1);
+    double p1 = 1.0 - p0;
+    if (p0 != 0.0 && p1 != 0.0)
+        c.ENTROPY = -(p0 * std::log(p0) + p1 * std::log(p1)) / std::log(2.0);
+    else
+        c.ENTROPY = 0.0;
+    c.ENTROPY *= double(s.count0 + count1);
+    c.ENTROPY /= double(count1);
+    double se;
+    if (s.pos + s.neg != 0) {
+        p0 = double(s.neg) / double(s.pos + s.neg);
+        p1 = 1.0 - p0;
+        if (p0 != 0.0 && p1 != 0.0)
+            se = -((p0 * std::log(p0) + p1 * std::log(p1)) / std::log(2.0));
+        else
+            se = 0.0;
+    } else {
+        se = 0.0;
+    }
+    se *= double(s.neg + s.pos);
+    se /= double(count1);
+    c.ENTROPY += se;
+    c.ENTROPY *= ecf;
+    c.TOTAL = c.Error + lambda * c.ENTROPY;
+    return c;
+}
+
+}  // namespace
+}  // namespace dgpu
+
+using namespace dgpu;
+
+extern "C" int dgpu_quant_factor4(int q) { return (q < 0 || q > 119) ? DGPU_ERR_ARG : qf4(q); }
+
+extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth, int32_t* const* coeff,
+                                       const int* cw, const int* ch, const float* lambda, const float* band_wt,
+                                       const float* band_ecf, const int* band_ncb, int* band_qidx, int* band_skip,
+                                       int* band_bits, uint8_t* cb_skip, int32_t* const* qout, void* workspace,
+                                       size_t ws_bytes, void* stream) {
+    if (n <= 0 || n > MAX_COMPS || !intra || !depth || !coeff || !cw || !ch || !lambda || !band_wt || !band_ecf ||
+        !band_ncb || !band_qidx || !band_skip || !band_bits || !cb_skip)
+        return DGPU_ERR_ARG;
+    cudaStream_t st = as_stream(stream);
+    // ---- geometry and task tables ----
+    std::vector<Comp> comps(n);
+    std::vector<BandTask> tasks;
+    int nb_total = 0, ncb_total = 0;
+    std::vector<int> band_cb_first;
+    size_t dcwork_elems = 0;
+    for (int c = 0; c < n; ++c) {
+        const int d = depth[c];
+        if (!coeff[c] || d < 1 || d > 8 || cw[c] <= 0 || ch[c] <= 0 || cw[c] % (1 << d) || ch[c] % (1 << d))
+            return DGPU_ERR_ARG;
+        comps[c] = Comp{coeff[c], nullptr, cw[c], ch[c], d, intra[c] ? 1 : 0, 3 * d + 1, nb_total};
+        for (int b = 1; b <= 3 * d + 1; ++b) {
+            const int xn = band_ncb[2 * (nb_total + b - 1)], yn = band_ncb[2 * (nb_total + b - 1) + 1];
+            if (xn <= 0 || yn <= 0) return DGPU_ERR_ARG;
+            band_cb_first.push_back(ncb_total);
+            ncb_total += xn * yn;
+        }
+        if (intra[c]) dcwork_elems += (size_t)(cw[c] >> d) * (ch[c] >> d);
+        nb_total += 3 * d + 1;
+    }
+    if (nb_total > MAX_TASKS) return DGPU_ERR_ARG;
+    // ---- workspace ----
+    const size_t need = align_up(sizeof(BandTask) * nb_total, 256) + align_up(sizeof(int) * nb_total, 256) +
+                        align_up(sizeof(int) * ncb_total, 256) + align_up(sizeof(Stat) * nb_total * 2 * QMAX, 256) +
+                        align_up(sizeof(int32_t) * dcwork_elems, 256) + align_up(ncb_total, 256) +
+                        align_up((sizeof(SeqCase) + sizeof(double)) * nb_total * 2 * QMAX, 256) + 256;
+    if (!workspace) {
+        int rc = library_scratch(need, &workspace);
+        if (rc) return rc;
+    } else if (ws_bytes < need) {
+        return DGPU_ERR_NOMEM;
+    }
+    char* p = static_cast<char*>(workspace);
+    auto take = [&](size_t bytes) {
+        char* q = p;
+        p += align_up(bytes, 256);
+        return q;
+    };
+    BandTask* d_tasks = reinterpret_cast<BandTask*>(take(sizeof(BandTask) * nb_total));
+    int* d_band_max = reinterpret_cast<int*>(take(sizeof(int) * nb_total));
+    int* d_cb_max = reinterpret_cast<int*>(take(sizeof(int) * ncb_total));
+    Stat* d_stats = reinterpret_cast<Stat*>(take(sizeof(Stat) * nb_total * 2 * QMAX));
+    int32_t* d_dcwork = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * dcwork_elems));
+    uint8_t* d_cbskip = reinterpret_cast<uint8_t*>(take(ncb_total));
+    SeqCase* d_cases = reinterpret_cast<SeqCase*>(take(sizeof(SeqCase) * nb_total * 2 * QMAX));
+    double* d_seq = reinterpret_cast<double*>(take(sizeof(double) * nb_total * 2 * QMAX));
+
+    size_t dcoff = 0;
+    for (int c = 0; c < n; ++c) {
+        Comp& C = comps[c];
+        if (C.intra) {
+            C.dcwork = d_dcwork + dcoff;
+            dcoff += (size_t)(C.cw >> C.depth) * (C.ch >> C.depth);
+        }
+        for (int b = 1; b <= C.nbands; ++b) {
+            int xp, yp, xl, yl;
+            band_rect(C.depth, C.cw, C.ch, b, xp, yp, xl, yl);
+            BandTask T;
+            const bool dcw = C.intra && b == C.nbands;
+            T.data = dcw ? C.dcwork : C.coeff + (size_t)yp * C.cw + xp;
+            T.stride = dcw ? xl : C.cw;
+            T.xl = xl;
+            T.yl = yl;
+            T.comp = c;
+            T.band = C.band_first + b - 1;
+            T.cb_first = band_cb_first[T.band];
+            T.xn = band_ncb[2 * T.band];
+            T.yn = band_ncb[2 * T.band + 1];
+            tasks.push_back(T);
+        }
+    }
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(d_tasks, tasks.data(), sizeof(BandTask) * nb_total, cudaMemcpyHostToDevice, st));
+    DGPU_CHECK_CUDA(cudaMemsetAsync(d_band_max, 0, sizeof(int) * nb_total, st));
+    DGPU_CHECK_CUDA(cudaMemsetAsync(d_cb_max, 0, sizeof(int) * ncb_total, st));
+    DGPU_CHECK_CUDA(cudaMemsetAsync(d_stats, 0, sizeof(Stat) * nb_total * 2 * QMAX, st));
+    // ---- 1. DC DPCM (intra) and maxima ----
+    for (int c = 0; c < n; ++c) {
+        const Comp& C = comps[c];
+        if (!C.intra) continue;
+        const int xl = C.cw >> C.depth, yl = C.ch >> C.depth;
+        dc_dpcm_kernel<<<(xl * yl + 255) / 256, 256, 0, st>>>(C.coeff, C.cw, xl, yl, C.dcwork);
+        DGPU_CHECK_LAUNCH();
+    }
+    {
+        dim3 grid(64, nb_total);
+        band_max_kernel<<<grid, 256, 0, st>>>(d_tasks, d_band_max, d_cb_max);
+        DGPU_CHECK_LAUNCH();
+    }
+    // ---- 2. statistics ----
+    {
+        int maxs = 0;
+        for (const BandTask& T : tasks) maxs = std::max(maxs, T.xl * ((T.yl + 1) / 2));
+        dim3 grid((maxs + STAT_THREADS * 8 - 1) / (STAT_THREADS * 8), nb_total, 2);
+        stats_kernel<<<grid, STAT_THREADS, 0, st>>>(d_tasks, d_band_max, d_stats);
+        DGPU_CHECK_LAUNCH();
+    }
+    std::vector<Stat> hs((size_t)nb_total * 2 * QMAX);
+    std::vector<int> hmax(nb_total), hcb(ncb_total);
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(hs.data(), d_stats, sizeof(Stat) * hs.size(), cudaMemcpyDeviceToHost, st));
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(hmax.data(), d_band_max, sizeof(int) * nb_total, cudaMemcpyDeviceToHost, st));
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(hcb.data(), d_cb_max, sizeof(int) * ncb_total, cudaMemcpyDeviceToHost, st));
+    DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
+    // ---- 3a. sums the exact path could not represent: sequential double kernel ----
+    std::vector<SeqCase> cases;
+    std::vector<int> case_of((size_t)nb_total * 2 * QMAX, -1);
+    for (int t = 0; t < nb_total; ++t)
+        for (int pat = 0; pat < 2; ++pat)
+            for (int q = 0; q < QMAX; ++q) {
+                const Stat& S = hs[((size_t)t * 2 + pat) * QMAX + q];
+                if (S.inexact || S.err_hi != 0 || S.err_lo >= (1ull << 53)) {
+                    case_of[((size_t)t * 2 + pat) * QMAX + q] = (int)cases.size();
+                    cases.push_back(SeqCase{t, pat, q});
+                }
+            }
+    std::vector<double> seq(cases.size());
+    if (!cases.empty()) {
+        DGPU_CHECK_CUDA(cudaMemcpyAsync(d_cases, cases.data(), sizeof(SeqCase) * cases.size(), cudaMemcpyHostToDevice, st));
+        seq_error_kernel<<<((int)cases.size() + 127) / 128, 128, 0, st>>>(d_tasks, d_cases, (int)cases.size(), d_seq);
+        DGPU_CHECK_LAUNCH();
+        DGPU_CHECK_CUDA(cudaMemcpyAsync(seq.data(), d_seq, sizeof(double) * cases.size(), cudaMemcpyDeviceToHost, st));
+        DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
+    }
+    auto host_stat = [&](int t, int pat, int q) {
+        const size_t k = ((size_t)t * 2 + pat) * QMAX + q;
+        const Stat& S = hs[k];
+        HostStat h;
+        h.count0 = (int)(uint32_t)S.count0;
+        h.pos = (int)(uint32_t)(S.posneg & 0xffffffffu);
+        h.neg = (int)(uint32_t)(S.posneg >> 32);
+        h.error = case_of[k] >= 0 ? seq[case_of[k]] : (double)S.err_lo;
+        return h;
+    };
+    // ---- 3b. the reference's three-pass Lagrangian choice per band ----
+    std::vector<uint8_t> hskip(ncb_total, 0);
+    for (int t = 0; t < nb_total; ++t) {
+        const BandTask& T = tasks[t];
+        const int maxv = hmax[t];
+        int q = 0, bits = 0;
+        if (maxv >= 1) {
+            const int max_bit = int(std::floor(std::log(float(maxv)) / std::log(2.0)));
+            const int nq = 4 * max_bit + 5;
+            if (nq > QMAX) return DGPU_ERR_SIZE;
+            std::vector<CostD> cost(nq);
+            int lo = 0, hi = nq - 1, step = 4, pat = 0, xr = 2, mn = 0;
+            for (int pass = 0; pass < 3; ++pass) {
+                if (pass == 1) {
+                    lo = std::max(mn - 2, 0);
+                    hi = std::min(mn + 2, nq - 1);
+                    step = 2;
+                } else if (pass == 2) {
+                    lo = std::max(mn - 1, 0);
+                    hi = std::min(mn + 1, nq - 1);
+                    step = 1;
+                    pat = 1;
+                    xr = 1;
+                }
+                const int count1 = (T.xl / xr) * (T.yl / 2);
+                for (int qq = lo; qq <= hi; qq += step)
+                    cost[qq] = lagrangian(host_stat(t, pat, qq), count1, band_wt[t], lambda[T.comp], band_ecf[t]);
+                mn = lo;
+                for (int qq = lo + step; qq <= hi; qq += step)
+                    if (cost[qq].TOTAL < cost[mn].TOTAL) mn = qq;
+            }
+            const double bit_sum = cost[mn].ENTROPY * T.xl * T.yl;
+            bits = int(bit_sum);
+            q = mn;
+            const int thr = qf4(q);
+            for (int k = 0; k < T.xn * T.yn; ++k) hskip[T.cb_first + k] = (hcb[T.cb_first + k] << 2) < thr;
+        }
+        band_qidx[t] = q;
+        band_bits[t] = bits;
+        band_skip[t] = bits == 0;
+    }
+    std::memcpy(cb_skip, hskip.data(), ncb_total);
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(d_cbskip, hskip.data(), ncb_total, cudaMemcpyHostToDevice, st));
+    // ---- 4. quantise and reconstruct, DC bands first ----
+    for (int c = 0; c < n; ++c) {
+        const Comp& C = comps[c];
+        const int t = C.band_first + C.nbands - 1;
+        if (!C.intra || band_skip[t]) continue;
+        const int xl = C.cw >> C.depth, yl = C.ch >> C.depth;
+        const int q = band_qidx[t];
+        const int threads = std::min(1024, ((xl + 31) / 32) * 32);
+        dc_intra_kernel<<<1, threads, 0, st>>>(const_cast<int32_t*>(C.coeff), qout ? qout[c] : nullptr, C.cw, xl, yl, tasks[t].xn,
+                                               tasks[t].yn, qf4(q), intra_off4(q), d_cbskip + tasks[t].cb_first);
+        DGPU_CHECK_LAUNCH();
+    }
+    QLaunch L{};
+    int chunks = 0;
+    auto flush = [&]() -> int {
+        if (L.n == 0) return DGPU_OK;
+        quantise_kernel<<<chunks, 256, 0, st>>>(L);
+        DGPU_CHECK_LAUNCH();
+        L.n = 0;
+        chunks = 0;
+        return DGPU_OK;
+    };
+    for (int t = 0; t < nb_total; ++t) {
+        const BandTask& T = tasks[t];
+        const Comp& C = comps[T.comp];
+        if (C.intra && t == C.band_first + C.nbands - 1 && !band_skip[t]) continue;  // done above
+        int xp, yp, xl, yl;
+        band_rect(C.depth, C.cw, C.ch, t - C.band_first + 1, xp, yp, xl, yl);
+        if (L.n == MAX_QBANDS) {
+            int rc = flush();
+            if (rc) return rc;
+        }
+        QBand& B = L.band[L.n++];
+        B.data = const_cast<int32_t*>(C.coeff) + (size_t)yp * C.cw + xp;
+        B.qout = qout && qout[T.comp] ? qout[T.comp] + (size_t)yp * C.cw + xp : nullptr;
+        B.stride = C.cw;
+        B.xl = xl;
+        B.yl = yl;
+        B.xn = T.xn;
+        B.yn = T.yn;
+        B.qf = qf4(band_qidx[t]);
+        B.off = C.intra ? intra_off4(band_qidx[t]) : inter_off4(band_qidx[t]);
+        B.skip = band_skip[t];
+        B.cb_skip = d_cbskip + T.cb_first;
+        B.first = chunks;
+        chunks += (xl * yl + 255) / 256;
+    }
+    return flush();
+}
+
+// CoeffArray::SetBandWeights (libdirac_common/wavelet_utils.cpp:192-382) with
+// PerceptualWeight (:384-395): perceptual weights of the 3*depth+1 bands of one component,
+// then the compensation for the unscaled lifting filters.  Host-only helper (no GPU use);
+// types and operation order follow the reference (float frequencies, double weights).
+extern "C" int dgpu_band_weights(int filter, int depth, int cw, int ch, int comp, int cformat, float cpd,
+                                 float cpd_scale, int field_coding, double* out) {
+    if (!out || depth < 1 || depth > 8 || cw <= 0 || ch <= 0) return DGPU_ERR_ARG;
+    const int nb = 3 * depth + 1;
+    // Subband::SetWt takes a float (wavelet_utils.cpp:112): every stored weight is rounded
+    auto set_wt = [](double w) -> double { return (double)(float)w; };
+    const float c = cpd * cpd_scale;
+    float chroma_xfac = 1.0f, chroma_yfac = 1.0f;
+    if (comp != 0) {
+        if (cformat == 1) {
+            chroma_xfac = 2.0f;
+            chroma_yfac = 1.0f;
+        } else if (cformat == 2) {
+            chroma_xfac = 2.0f;
+            chroma_yfac = 2.0f;
+        }
+    }
+    int xp, yp, xl, yl;
+    band_rect(depth, cw, ch, 1, xp, yp, xl, yl);
+    const int xlen = 2 * xl, ylen = 2 * yl;
+    auto scale_of = [&](int b) { return b == nb ? (1 << depth) : (1 << ((b - 1) / 3 + 1)); };
+    if (c != 0.0f) {
+        for (int b = 1; b <= nb; ++b) {
+            band_rect(depth, cw, ch, b, xp, yp, xl, yl);
+            float xfreq = c * (float(xp) + (float(xl) / 2.0)) / float(xlen);
+            float yfreq = c * (float(yp) + (float(yl) / 2.0)) / float(ylen);
+            if (field_coding) yfreq /= 2.0;
+            const float xf = xfreq / chroma_xfac, yf = yfreq / chroma_yfac;
+            double freq_sqd(xf * xf + yf * yf);
+            if (comp != 0) freq_sqd *= 1.2;
+            const float w = 0.255 * std::pow(1.0 + 0.2561 * freq_sqd, 0.75);
+            out[b - 1] = set_wt(w);
+        }
+        float min_weight = out[nb - 1];
+        for (int b = 1; b <= nb - 1; ++b) min_weight = ((min_weight > out[b - 1]) ? out[b - 1] : min_weight);
+        out[nb - 1] = set_wt(min_weight);
+        double overall = 0.0;
+        for (int b = 1; b <= nb; ++b) {
+            const double frac = 1.0 / ((double)scale_of(b) * scale_of(b));
+            overall += frac / (out[b - 1] * out[b - 1]);
+        }
+        overall = std::sqrt(overall);
+        for (int b = nb; b > 0; --b) out[b - 1] = set_wt(out[b - 1] * overall);
+    } else {
+        for (int b = 1; b <= nb; ++b) out[b - 1] = set_wt(1.0);
+    }
+    double lfac, hfac;
+    int filt_shift;
+    switch (filter) {
+        case DGPU_DD9_7: lfac = 1.218660804; hfac = 0.780720058; filt_shift = 1; break;
+        case DGPU_LEGALL5_3: lfac = 1.179535649; hfac = 0.81649658; filt_shift = 1; break;
+        case DGPU_DD13_7: lfac = 1.235705971; hfac = 0.780719354; filt_shift = 1; break;
+        case DGPU_HAAR0: lfac = 1.414213562; hfac = 0.707106781; filt_shift = 0; break;
+        case DGPU_HAAR1: lfac = 1.414213562; hfac = 0.707106781; filt_shift = 1; break;
+        case DGPU_DAUB9_7: lfac = 1.149604398; hfac = 0.869864452; filt_shift = 1; break;
+        default: lfac = 1.0; hfac = 1.0; filt_shift = 0; break;
+    }
+    double cf = (1 << (depth * filt_shift)) / std::pow(lfac, 2 * depth);
+    out[nb - 1] = set_wt(out[nb - 1] * cf);
+    for (int level = 1; level <= depth; ++level) {
+        const int shift = (depth - level + 1) * filt_shift;
+        for (int orient = 3; orient >= 1; --orient) {
+            const int idx = 3 * (depth - level) + orient;
+            cf = 1.0 / std::pow(lfac, 2 * (depth - level));
+            band_rect(depth, cw, ch, idx, xp, yp, xl, yl);
+            if (xp != 0 && yp != 0)
+                cf /= (hfac * hfac);
+            else
+                cf /= (lfac * hfac);
+            cf *= double(1 << shift);
+            out[idx - 1] = set_wt(out[idx - 1] * cf);
+        }
+    }
+    return DGPU_OK;
+}
+
+// EncoderParams::SetUsualCodeBlocks (common.cpp:488-510) as PictureCompressor::SetupCodeBlocks
+// applies it (picture_compress.cpp:582-601): code blocks (x, y) per band from the luma size.
+extern "C" int dgpu_code_blocks(int depth, int luma_w, int luma_h, int spatial_partition, int* ncb) {
+    if (!ncb || depth < 1 || depth > 8) return DGPU_ERR_ARG;
+    const int nb = 3 * depth + 1;
+    const int xl_pad = (luma_w + (1 << depth) - 1) & ~((1 << depth) - 1);
+    const int yl_pad = (luma_h + (1 << depth) - 1) & ~((1 << depth) - 1);
+    for (int b = 1; b <= nb; ++b) {
+        int xr = 1, yr = 1;
+        if (spatial_partition) {
+            const int level = depth - (b - 1) / 3;
+            if (level == 0) {
+                xr = std::max(1, (xl_pad >> depth) / 4);
+                yr = std::max(1, (yl_pad >> depth) / 4);
+            } else {
+                const int i = depth - level + 1;
+                xr = std::max(1, (xl_pad >> i) / 12);
+                yr = std::max(1, (yl_pad >> i) / 12);
+            }
+        }
+        ncb[2 * (b - 1)] = xr;
+        ncb[2 * (b - 1) + 1] = yr;
+    }
+    return DGPU_OK;
+}

@@ -124,13 +124,42 @@ def me_cases(ref):
     return out
 
 
+def quant_cases(ref):
+    """Residue coding (quantiser choice, quantisation, reconstruction) of transformed
+    synthetic components, intra and inter, run by the reference's own classes."""
+    sys.path.insert(0, os.path.join(HERE, "..", "..", "dirac-research_b200"))
+    from dirac_b200 import synth
+    from oracle import Oracle
+
+    orc = Oracle()
+    out = {}
+    cases = [(176, 144, 4, 6, 1, 0, 7), (176, 144, 4, 0, 0, 1, 7), (128, 96, 3, 1, 1, 2, 5),
+             (160, 128, 4, 2, 0, 0, 9)]
+    for k, (w, h, depth, filt, intra, comp, qf) in enumerate(cases):
+        seq = synth.make_sequence(w, h, 2, n_rects=6, vmax=6, seed=70 + k)
+        f = [synth.to_signed(p) for p in seq[0]]
+        g = [synth.to_signed(p) for p in seq[1]]
+        pic = f[comp] if intra else np.clip(f[comp].astype(np.int32) - g[comp], -128, 127).astype(np.int16)
+        coeff = orc.dwt_forward(filt, depth, pic)
+        lam = 10 ** ((12 - qf) / 2.5) / 16 * (1 if intra else 4)
+        r = ref.code_residue(2, w, h, comp, intra, filt, depth, coeff, lam)
+        key = f"q{k}"
+        out[key + "_meta"] = np.array([w, h, depth, filt, intra, comp], np.int32)
+        out[key + "_lambda"] = np.array([lam], np.float32)
+        out[key + "_coeff"] = coeff
+        for name, a in r.items():
+            out[f"{key}_{name}"] = a
+    return out
+
+
 def main():
     ref = Reference()
     np.savez_compressed(os.path.join(HERE, "dwt.npz"), **dwt_cases(ref))
     np.savez_compressed(os.path.join(HERE, "convert.npz"), **conv_cases(ref))
     np.savez_compressed(os.path.join(HERE, "mc.npz"), **mc_cases(ref))
     np.savez_compressed(os.path.join(HERE, "me.npz"), **me_cases(ref))
-    print("wrote dwt.npz, convert.npz, mc.npz, me.npz")
+    np.savez_compressed(os.path.join(HERE, "quant.npz"), **quant_cases(ref))
+    print("wrote dwt.npz, convert.npz, mc.npz, me.npz, quant.npz")
 
 
 if __name__ == "__main__":

@@ -206,3 +206,79 @@ def test_motion_estimation_matches_live_reference(oracle, case):
     b = Reference().motion_estimate(cf, f[1], f[0], f[2] if nref == 2 else None, bp, lam, 3)
     for n in a:
         np.testing.assert_array_equal(a[n], b[n], err_msg=n)
+
+
+def quant_case(g, k):
+    w, h, depth, filt, intra, comp = (int(v) for v in g[f"q{k}_meta"])
+    names = ("recon", "qidx", "skip", "wt", "ecf", "bits", "ncb", "cb_skip")
+    return (w, h, depth, filt, intra, comp, float(g[f"q{k}_lambda"][0]), g[f"q{k}_coeff"],
+            {n: g[f"q{k}_{n}"] for n in names})
+
+
+def test_code_residue_golden(oracle, golden):
+    g = golden("quant.npz")
+    for k in range(4):
+        w, h, depth, filt, intra, comp, lam, coeff, want = quant_case(g, k)
+        recon, q, sk, bits, cbs, _ = oracle.code_residue(intra, depth, coeff, lam, want["wt"].astype(np.float32),
+                                                         want["ecf"], want["ncb"])
+        np.testing.assert_array_equal(recon, want["recon"], err_msg=f"case {k}")
+        np.testing.assert_array_equal(sk, want["skip"])
+        np.testing.assert_array_equal(q[sk == 0], want["qidx"][sk == 0])
+        np.testing.assert_array_equal(bits, want["bits"])
+        np.testing.assert_array_equal(cbs, want["cb_skip"])
+
+
+def test_quantiser_factor_table(oracle):
+    from dirac_b200 import _lib
+
+    lib = _lib.load()
+    # QuantiserLists: qf4[0]=4, qf4[1]=5, then 4 * 2^(q/4) with fixed rational steps
+    assert [lib.dgpu_quant_factor4(q) for q in range(8)] == [4, 5, 6, 7, 8, 10, 11, 13]
+    assert lib.dgpu_quant_factor4(40) == 4096
+    assert [lib.dgpu_quant_factor4(q) for q in range(120)] == [oracle.lib.orc_qf4(q) for q in range(120)]
+
+
+def test_band_weights_and_code_blocks_match_reference_fixtures(golden):
+    """Host helpers dgpu_band_weights / dgpu_code_blocks reproduce the reference's
+    SetBandWeights and code-block grid (the fixtures hold the reference's values; CPD 20, the
+    default video format's)."""
+    from dirac_b200 import quant
+
+    g = golden("quant.npz")
+    for k in range(4):
+        w, h, depth, filt, intra, comp, lam, coeff, want = quant_case(g, k)
+        ch, cw = coeff.shape
+        wt = quant.band_weights(filt, depth, cw, ch, comp, 2, 20.0, 1.0)
+        np.testing.assert_array_equal(wt, want["wt"], err_msg=f"case {k}")
+        np.testing.assert_array_equal(quant.code_blocks(depth, w, h), want["ncb"])
+
+
+@needs_ref
+@pytest.mark.parametrize("case", range(6))
+def test_code_residue_matches_live_reference(oracle, case):
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "dirac-research_b200"))
+    from dirac_b200 import quant, synth
+
+    w, h, depth, filt, intra, comp, qf, cf = [(352, 288, 4, 6, 1, 0, 7, 2), (352, 288, 4, 0, 0, 1, 7, 2),
+                                              (720, 576, 5, 2, 1, 0, 5, 1), (720, 576, 4, 1, 0, 2, 9, 2),
+                                              (1920, 1080, 4, 6, 1, 0, 7, 2), (1280, 720, 3, 3, 0, 0, 6, 2)][case]
+    seq = synth.make_sequence(w, h, 2, n_rects=12, vmax=12, seed=300 + case,
+                              chroma={2: "420", 1: "422", 0: "444"}[cf])
+    f = [synth.to_signed(p) for p in seq[0]]
+    g = [synth.to_signed(p) for p in seq[1]]
+    pic = f[comp] if intra else np.clip(f[comp].astype(np.int32) - g[comp], -128, 127).astype(np.int16)
+    coeff = oracle.dwt_forward(filt, depth, pic)
+    lam = 10 ** ((12 - qf) / 2.5) / 16 * (1 if intra else 4)
+    r = Reference().code_residue(cf, w, h, comp, intra, filt, depth, coeff, lam)
+    ch, cw = coeff.shape
+    np.testing.assert_array_equal(quant.band_weights(filt, depth, cw, ch, comp, cf, 20.0, 1.0), r["wt"])
+    np.testing.assert_array_equal(quant.code_blocks(depth, w, h), r["ncb"])
+    recon, q, sk, bits, cbs, _ = oracle.code_residue(intra, depth, coeff, lam, r["wt"].astype(np.float32), r["ecf"],
+                                                     r["ncb"])
+    np.testing.assert_array_equal(recon, r["recon"])
+    np.testing.assert_array_equal(sk, r["skip"])
+    np.testing.assert_array_equal(q[sk == 0], r["qidx"][sk == 0])
+    np.testing.assert_array_equal(bits, r["bits"])
+    np.testing.assert_array_equal(cbs, r["cb_skip"])
