@@ -994,66 +994,393 @@ int me_geometry(int cformat, int w, int h, const dgpu_block_params* bp, int nref
     return DGPU_OK;
 }
 
-struct MeBuffers {
-    int16_t* down[3][13];          // pyramid planes of pic, ref1, ref2 (level >= 1)
-    short2* mv[13][2];             // level >= 1 vectors
+// Device buffers of one batch: per picture (pyramid planes, upconverted luma) and per
+// task (the per-level search state, flags, lambda maps, mode-decision levels).
+struct PicBufs {
+    int16_t* down[13];   // pyramid levels >= 1 of the picture's luma
+    int16_t* up;         // upconverted luma (used when the picture is a reference)
+};
+
+struct TaskBufs {
+    short2* mv[13][2];   // level >= 1 vectors
     float* cost[13][2];
     int* best_sad[13][2];
     short2* best_mv[13][2];
-    int* flags;                    // one flag per unit, reused by every wavefront
-    int* ctl;                      // [0] ticket, [1] error
-    int16_t* up[2];                // upconverted original references
-    float* lambda[3];              // level maps 0, 1, 2
-    short2* lmv[2][2];             // levels 0 and 1: vectors per ref
+    int* flags;          // 2 * max units of any level
+    float* lambda[3];    // level maps 0, 1, 2
+    short2* lmv[2][2];   // mode-decision levels 0 and 1
     float* lcost[2][2];
     uint8_t* lmode[2];
     int16_t* ldcy[2];
-    int16_t* dctmp;
+    int16_t* dctmp;      // block DCs of the three components
 };
 
-size_t layout(const MeGeometry& g, MeBuffers& B, Arena& a) {
-    for (int s = 0; s < 3; ++s)
-        for (int l = 1; l <= g.depth; ++l) B.down[s][l] = a.take<int16_t>((size_t)g.pw[l] * g.ph[l]);
-    for (int l = 0; l <= g.depth; ++l)
-        for (int r = 0; r < 2; ++r) {
-            const size_t n = (size_t)g.xnb[l] * g.ynb[l];
-            B.mv[l][r] = l ? a.take<short2>(n) : nullptr;
-            B.cost[l][r] = l ? a.take<float>(3 * n) : nullptr;
-            B.best_sad[l][r] = a.take<int>(n);
-            B.best_mv[l][r] = a.take<short2>(n);
-        }
-    size_t maxunits = 0;
-    for (int l = 0; l <= g.depth; ++l) maxunits = std::max(maxunits, (size_t)g.xnb[l] * g.ynb[l]);
-    B.flags = a.take<int>(2 * maxunits);
-    B.ctl = a.take<int>(64);
-    for (int r = 0; r < 2; ++r) B.up[r] = a.take<int16_t>(4 * (size_t)g.w * g.h);
-    const size_t nb = (size_t)g.xnb[0] * g.ynb[0];
-    B.lambda[2] = a.take<float>(nb);
-    B.lambda[1] = a.take<float>(nb / 4);
-    B.lambda[0] = a.take<float>(nb / 16);
-    for (int lv = 0; lv < 2; ++lv) {
-        const size_t n = lv ? nb / 4 : nb / 16;
-        for (int r = 0; r < 2; ++r) {
-            B.lmv[lv][r] = a.take<short2>(n);
-            B.lcost[lv][r] = a.take<float>(3 * n);
-        }
-        B.lmode[lv] = a.take<uint8_t>(n);
-        B.ldcy[lv] = a.take<int16_t>(n);
-    }
-    B.dctmp = a.take<int16_t>(3 * nb);
+size_t pic_layout(const MeGeometry& g, PicBufs& P, Arena& a, bool need_up) {
+    for (int l = 1; l <= g.depth; ++l) P.down[l] = a.take<int16_t>((size_t)g.pw[l] * g.ph[l]);
+    P.up = need_up ? a.take<int16_t>(4 * (size_t)g.w * g.h) : nullptr;
     return a.used;
 }
 
-int launch_pel(PelLaunch& L, int* ctl, cudaStream_t st) {
+size_t task_layout(const MeGeometry& g, TaskBufs& T, Arena& a) {
+    for (int l = 0; l <= g.depth; ++l)
+        for (int r = 0; r < 2; ++r) {
+            const size_t n = (size_t)g.xnb[l] * g.ynb[l];
+            T.mv[l][r] = l ? a.take<short2>(n) : nullptr;
+            T.cost[l][r] = l ? a.take<float>(3 * n) : nullptr;
+            T.best_sad[l][r] = a.take<int>(n);
+            T.best_mv[l][r] = a.take<short2>(n);
+        }
+    size_t maxunits = 0;
+    for (int l = 0; l <= g.depth; ++l) maxunits = std::max(maxunits, (size_t)g.xnb[l] * g.ynb[l]);
+    T.flags = a.take<int>(2 * maxunits);
+    const size_t nb = (size_t)g.xnb[0] * g.ynb[0];
+    T.lambda[2] = a.take<float>(nb);
+    T.lambda[1] = a.take<float>(nb / 4);
+    T.lambda[0] = a.take<float>(nb / 16);
+    for (int lv = 0; lv < 2; ++lv) {
+        const size_t n = lv ? nb / 4 : nb / 16;
+        for (int r = 0; r < 2; ++r) {
+            T.lmv[lv][r] = a.take<short2>(n);
+            T.lcost[lv][r] = a.take<float>(3 * n);
+        }
+        T.lmode[lv] = a.take<uint8_t>(n);
+        T.ldcy[lv] = a.take<int16_t>(n);
+    }
+    T.dctmp = a.take<int16_t>(3 * nb);
+    return a.used;
+}
+
+constexpr int MAX_MODE_JOBS = 4;
+
+template <class Launch, class Kernel>
+int launch_wavefront(Launch& L, Kernel kernel, int* ctl, cudaStream_t st) {
     if (L.njobs == 0) return DGPU_OK;
     L.ticket = ctl;
     L.err = ctl + 1;
     DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
-    pel_lists_kernel<<<(L.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, 0, st>>>(L);
-    DGPU_CHECK_LAUNCH();
     const int grid = std::min((L.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, 148 * 8);
-    pel_wavefront_kernel<<<grid, ME_THREADS, 0, st>>>(L);
+    kernel<<<grid, ME_THREADS, 0, st>>>(L);
     DGPU_CHECK_LAUNCH();
+    return DGPU_OK;
+}
+
+struct BatchArgs {
+    int cformat, w, h, luma_depth, stages, prec;
+    int npics, ntasks;
+    const int16_t* const* pics;  // npics * 3 planes
+    const int* task_pic;
+    const int* task_ref[2];      // second may hold -1 entries
+    const float* task_lambda;
+    int16_t* const* mv_out;
+    float* const* cost_out;
+    uint8_t* const* mode_out;
+    int16_t* const* dc_out;
+    uint8_t* const* split_out;
+    float* const* sbcost_out;
+};
+
+size_t batch_bytes(const MeGeometry& g, const BatchArgs& A, std::vector<PicBufs>* P, std::vector<TaskBufs>* T,
+                   char* base, int** ctl) {
+    Arena a{base, 0, 0};
+    std::vector<char> is_ref(A.npics, 0);
+    for (int t = 0; t < A.ntasks; ++t)
+        for (int r = 0; r < 2; ++r)
+            if (A.task_ref[r][t] >= 0) is_ref[A.task_ref[r][t]] = 1;
+    PicBufs pb;
+    for (int p = 0; p < A.npics; ++p) {
+        pic_layout(g, pb, a, is_ref[p] && A.stages >= 2);
+        if (P) P->push_back(pb);
+    }
+    TaskBufs tb;
+    for (int t = 0; t < A.ntasks; ++t) {
+        task_layout(g, tb, a);
+        if (T) T->push_back(tb);
+    }
+    int* c = a.take<int>(64);
+    if (ctl) *ctl = c;
+    return a.used + 256;
+}
+
+int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStream_t st) {
+    std::vector<PicBufs> P;
+    std::vector<TaskBufs> T;
+    int* ctl = nullptr;
+    batch_bytes(g, A, &P, &T, static_cast<char*>(workspace), &ctl);
+    DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, 2 * sizeof(int), st));
+    const size_t nb = (size_t)g.xnb[0] * g.ynb[0];
+    auto luma = [&](int p) { return A.pics[3 * p]; };
+    auto nref_of = [&](int t) { return A.task_ref[1][t] >= 0 ? 2 : 1; };
+    auto ref_of = [&](int t, int r) { return r == 1 && A.task_ref[1][t] >= 0 ? A.task_ref[1][t] : A.task_ref[0][t]; };
+    auto mv0 = [&](int t, int r) { return reinterpret_cast<short2*>(A.mv_out[t]) + (size_t)r * nb; };
+    auto cost0 = [&](int t, int r) { return A.cost_out[t] + (size_t)r * 3 * nb; };
+    std::vector<char> used(A.npics, 0);
+    for (int t = 0; t < A.ntasks; ++t) {
+        used[A.task_pic[t]] = 1;
+        for (int r = 0; r < nref_of(t); ++r) used[ref_of(t, r)] = 1;
+    }
+    // ---- pyramids of every picture involved (PixelMatcher::MakePicHierarchy) ----
+    for (int l = 1; l <= g.depth; ++l) {
+        std::vector<const int16_t*> in;
+        std::vector<int16_t*> out;
+        for (int p = 0; p < A.npics; ++p) {
+            if (!used[p]) continue;
+            in.push_back(l == 1 ? luma(p) : P[p].down[l - 1]);
+            out.push_back(P[p].down[l]);
+        }
+        for (size_t i = 0; i < in.size(); i += 32) {
+            const int k = (int)std::min<size_t>(32, in.size() - i);
+            std::vector<int> iw(k, g.pw[l - 1]), ih(k, g.ph[l - 1]), os(k, g.pw[l]);
+            const int rc = dgpu_downconvert_batch(k, in.data() + i, iw.data(), ih.data(), iw.data(), out.data() + i,
+                                                  os.data(), st);
+            if (rc) return rc;
+        }
+    }
+    // ---- pel search, coarsest level first ----
+    for (int l = g.depth; l >= 0; --l) {
+        PelLaunch L{};
+        L.o = g.lb[2];
+        int total = 0;
+        auto flush = [&]() -> int {
+            if (L.njobs == 0) return DGPU_OK;
+            L.total = total;
+            L.ticket = ctl;
+            L.err = ctl + 1;
+            // the candidate-list phase covers every unit: one warp per unit
+            pel_lists_kernel<<<(total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, 0, st>>>(L);
+            DGPU_CHECK_LAUNCH();
+            const int rc = launch_wavefront(L, pel_wavefront_kernel, ctl, st);
+            L.njobs = 0;
+            total = 0;
+            return rc;
+        };
+        for (int t = 0; t < A.ntasks; ++t)
+            for (int r = 0; r < nref_of(t); ++r) {
+                if (L.njobs == MAX_ME_JOBS) {
+                    const int rc = flush();
+                    if (rc) return rc;
+                }
+                PelJob& J = L.job[L.njobs++];
+                const int pp = A.task_pic[t], rp = ref_of(t, r);
+                J.pic = l ? P[pp].down[l] : luma(pp);
+                J.ref = l ? P[rp].down[l] : luma(rp);
+                J.pw = g.pw[l];
+                J.ph = g.ph[l];
+                J.xnb = g.xnb[l];
+                J.ynb = g.ynb[l];
+                J.mv = l ? T[t].mv[l][r] : mv0(t, r);
+                J.cost = l ? T[t].cost[l][r] : cost0(t, r);
+                J.guide = l < g.depth ? T[t].mv[l + 1][r] : nullptr;
+                J.gxnb = l < g.depth ? g.xnb[l + 1] : 0;
+                J.gynb = l < g.depth ? g.ynb[l + 1] : 0;
+                J.radius = std::min(l + 1, 5);
+                J.best_sad = T[t].best_sad[l][r];
+                J.best_mv = T[t].best_mv[l][r];
+                J.flags = T[t].flags + (size_t)r * g.xnb[l] * g.ynb[l];
+                J.first = total;
+                total += J.xnb * J.ynb;
+                DGPU_CHECK_CUDA(cudaMemsetAsync(J.flags, 0, sizeof(int) * J.xnb * J.ynb, st));
+            }
+        const int rc = flush();
+        if (rc) return rc;
+    }
+    int err_host = 0;
+    if (A.stages >= 2) {
+        // ---- lambda maps on the host (long double statistics, as the reference) ----
+        std::vector<std::vector<short2>> hmv(A.ntasks, std::vector<short2>(2 * nb));
+        std::vector<std::vector<float>> hl(A.ntasks, std::vector<float>(nb));
+        for (int t = 0; t < A.ntasks; ++t)
+            DGPU_CHECK_CUDA(cudaMemcpyAsync(hmv[t].data(), A.mv_out[t], sizeof(short2) * nref_of(t) * nb,
+                                            cudaMemcpyDeviceToHost, st));
+        DGPU_CHECK_CUDA(cudaMemcpyAsync(&err_host, ctl + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
+        if (err_host) return DGPU_ERR_CUDA;
+        for (int t = 0; t < A.ntasks; ++t) {
+            lambda_map(hmv[t].data(), hmv[t].data() + nb, nref_of(t), g.xnb[0], g.ynb[0], A.task_lambda[t],
+                       hl[t].data());
+            DGPU_CHECK_CUDA(cudaMemcpyAsync(T[t].lambda[2], hl[t].data(), sizeof(float) * nb, cudaMemcpyHostToDevice, st));
+        }
+        // ---- upconverted original references (EncPicture::UpOrigData) ----
+        {
+            std::vector<const int16_t*> in;
+            std::vector<int16_t*> out;
+            for (int p = 0; p < A.npics; ++p)
+                if (P[p].up) {
+                    in.push_back(luma(p));
+                    out.push_back(P[p].up);
+                }
+            for (size_t i = 0; i < in.size(); i += 32) {
+                const int k = (int)std::min<size_t>(32, in.size() - i);
+                std::vector<int> iw(k, g.w), ih(k, g.h), bd(k, A.luma_depth), us(k, 2 * g.w);
+                const int rc = dgpu_upconvert_batch(k, in.data() + i, iw.data(), ih.data(), iw.data(), bd.data(),
+                                                    out.data() + i, us.data(), st);
+                if (rc) return rc;
+            }
+        }
+        // ---- sub-pel refinement ----
+        {
+            SubLaunch S{};
+            S.o = g.lb[2];
+            S.prec = A.prec;
+            int total = 0;
+            for (int t = 0; t < A.ntasks; ++t)
+                for (int r = 0; r < nref_of(t); ++r) {
+                    if (S.njobs == MAX_ME_JOBS) {
+                        S.total = total;
+                        const int rc = launch_wavefront(S, subpel_wavefront_kernel, ctl, st);
+                        if (rc) return rc;
+                        S.njobs = 0;
+                        total = 0;
+                    }
+                    SubJob& J = S.job[S.njobs++];
+                    J.pic = luma(A.task_pic[t]);
+                    J.up = P[ref_of(t, r)].up;
+                    J.pw = g.w;
+                    J.ph = g.h;
+                    J.xnb = g.xnb[0];
+                    J.ynb = g.ynb[0];
+                    J.mv = mv0(t, r);
+                    J.cost = cost0(t, r);
+                    J.lambda = T[t].lambda[2];
+                    J.flags = T[t].flags + (size_t)r * nb;
+                    J.first = total;
+                    total += (int)nb;
+                    DGPU_CHECK_CUDA(cudaMemsetAsync(J.flags, 0, sizeof(int) * nb, st));
+                }
+            S.total = total;
+            const int rc = launch_wavefront(S, subpel_wavefront_kernel, ctl, st);
+            if (rc) return rc;
+        }
+        if (A.stages >= 3) {
+            const float f0 = (float)(16 * g.lb[2].xblen * g.lb[2].yblen) / (float)(g.lb[0].xblen * g.lb[0].yblen);
+            const float f1 = (float)(4 * g.lb[2].xblen * g.lb[2].yblen) / (float)(g.lb[1].xblen * g.lb[1].yblen);
+            std::vector<std::vector<float>> l0(A.ntasks), l1(A.ntasks);
+            for (int t = 0; t < A.ntasks; ++t) {
+                l0[t].resize(nb / 16);
+                l1[t].resize(nb / 4);
+                level_lambda_map(hl[t].data(), g.xnb[0], 0, g.xnb[0] / 4, g.ynb[0] / 4, (float)(1.0 / f0), l0[t].data());
+                level_lambda_map(hl[t].data(), g.xnb[0], 1, g.xnb[0] / 2, g.ynb[0] / 2, (float)(1.0 / f1), l1[t].data());
+                DGPU_CHECK_CUDA(cudaMemcpyAsync(T[t].lambda[0], l0[t].data(), sizeof(float) * l0[t].size(),
+                                                cudaMemcpyHostToDevice, st));
+                DGPU_CHECK_CUDA(cudaMemcpyAsync(T[t].lambda[1], l1[t].data(), sizeof(float) * l1[t].size(),
+                                                cudaMemcpyHostToDevice, st));
+                // fresh level data (a new MEData in the reference) and zero DC arrays (a fresh MvData)
+                for (int lv = 0; lv < 2; ++lv) {
+                    const size_t n = lv ? nb / 4 : nb / 16;
+                    for (int r = 0; r < 2; ++r) {
+                        DGPU_CHECK_CUDA(cudaMemsetAsync(T[t].lmv[lv][r], 0, sizeof(short2) * n, st));
+                        DGPU_CHECK_CUDA(cudaMemsetAsync(T[t].lcost[lv][r], 0, sizeof(float) * 3 * n, st));
+                    }
+                    DGPU_CHECK_CUDA(cudaMemsetAsync(T[t].ldcy[lv], 0, sizeof(int16_t) * n, st));
+                    DGPU_CHECK_CUDA(cudaMemsetAsync(T[t].lmode[lv], 0, n, st));
+                }
+                DGPU_CHECK_CUDA(cudaMemsetAsync(A.dc_out[t], 0, sizeof(int16_t) * 3 * nb, st));
+            }
+            ModeLaunch M{};
+            M.prec = A.prec;
+            for (int i = 0; i < 3; ++i) M.lb[i] = g.lb[i];
+            M.level_factor[0] = f0;
+            M.level_factor[1] = f1;
+            M.level_factor[2] = 1.0f;
+            int total = 0;
+            // one launch per reference count: the kernel takes nref per launch
+            for (int want_nref = 1; want_nref <= 2; ++want_nref) {
+                M.nref = want_nref;
+                for (int t = 0; t < A.ntasks; ++t) {
+                    if (nref_of(t) != want_nref) continue;
+                    if (M.njobs == MAX_MODE_JOBS) {
+                        M.total = total;
+                        const int rc = launch_wavefront(M, mode_wavefront_kernel, ctl, st);
+                        if (rc) return rc;
+                        M.njobs = 0;
+                        total = 0;
+                    }
+                    ModeJob& J = M.job[M.njobs++];
+                    J.pic = luma(A.task_pic[t]);
+                    J.up[0] = P[ref_of(t, 0)].up;
+                    J.up[1] = P[ref_of(t, 1)].up;
+                    J.pw = g.w;
+                    J.ph = g.h;
+                    for (int lv = 0; lv < 3; ++lv) {
+                        LevelData& D = J.lev[lv];
+                        D.xnb = g.xnb[0] >> (2 - lv);
+                        D.ynb = g.ynb[0] >> (2 - lv);
+                        D.lambda = T[t].lambda[lv];
+                        if (lv == 2) {
+                            D.mv[0] = mv0(t, 0);
+                            D.mv[1] = want_nref > 1 ? mv0(t, 1) : mv0(t, 0);
+                            D.cost[0] = cost0(t, 0);
+                            D.cost[1] = want_nref > 1 ? cost0(t, 1) : cost0(t, 0);
+                            D.mode = A.mode_out[t];
+                            D.dcy = A.dc_out[t];
+                        } else {
+                            D.mv[0] = T[t].lmv[lv][0];
+                            D.mv[1] = T[t].lmv[lv][1];
+                            D.cost[0] = T[t].lcost[lv][0];
+                            D.cost[1] = T[t].lcost[lv][1];
+                            D.mode = T[t].lmode[lv];
+                            D.dcy = T[t].ldcy[lv];
+                        }
+                    }
+                    J.sbcost = A.sbcost_out[t];
+                    J.split = A.split_out[t];
+                    J.xnsb = g.xnsb;
+                    J.ynsb = g.ynsb;
+                    J.flags = T[t].flags;
+                    J.first = total;
+                    total += g.xnsb * g.ynsb;
+                    DGPU_CHECK_CUDA(cudaMemsetAsync(J.flags, 0, sizeof(int) * g.xnsb * g.ynsb, st));
+                }
+                M.total = total;
+                const int rc = launch_wavefront(M, mode_wavefront_kernel, ctl, st);
+                if (rc) return rc;
+                M.njobs = 0;
+                total = 0;
+            }
+            // ---- DC values of all three components ----
+            DcLaunch D{};
+            int dtotal = 0;
+            auto dflush = [&]() -> int {
+                if (D.njobs == 0) return DGPU_OK;
+                D.total = dtotal;
+                block_dc_kernel<<<(dtotal + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, 0, st>>>(D);
+                DGPU_CHECK_LAUNCH();
+                smooth_dc_kernel<<<(dtotal + 255) / 256, 256, 0, st>>>(D);
+                DGPU_CHECK_LAUNCH();
+                D.njobs = 0;
+                dtotal = 0;
+                return DGPU_OK;
+            };
+            for (int t = 0; t < A.ntasks; ++t)
+                for (int c = 0; c < 3; ++c) {
+                    if (D.njobs == MAX_ME_JOBS) {
+                        const int rc = dflush();
+                        if (rc) return rc;
+                    }
+                    const int xs = (c && A.cformat != 0) ? 1 : 0, ys = (c && A.cformat == 2) ? 1 : 0;
+                    DcJob& Jd = D.job[D.njobs++];
+                    Jd.pic = A.pics[3 * A.task_pic[t] + c];
+                    Jd.pw = g.w >> xs;
+                    Jd.ph = g.h >> ys;
+                    Jd.o = make_olb(g.lb[2].xblen >> xs, g.lb[2].yblen >> ys, g.lb[2].xbsep >> xs, g.lb[2].ybsep >> ys);
+                    Jd.tmp = T[t].dctmp + (size_t)c * nb;
+                    Jd.dc = A.dc_out[t] + (size_t)c * nb;
+                    Jd.xnb = g.xnb[0];
+                    Jd.ynb = g.ynb[0];
+                    Jd.first = dtotal;
+                    dtotal += (int)nb;
+                }
+            const int rc = dflush();
+            if (rc) return rc;
+        }
+    }
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(&err_host, ctl + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
+    return err_host ? DGPU_ERR_CUDA : DGPU_OK;
+}
+
+int check_args(int cformat, int luma_depth, const MeGeometry& g) {
+    if (cformat < 0 || cformat > 2 || luma_depth < 2 || luma_depth > 15) return DGPU_ERR_ARG;
+    if (g.lb[2].xblen > 64) return DGPU_ERR_SIZE;
     return DGPU_OK;
 }
 
@@ -1064,12 +1391,86 @@ using namespace dgpu;
 
 extern "C" int dgpu_me_depth(int w, int h) { return me_depth(w, h); }
 
-extern "C" size_t dgpu_me_workspace_bytes(int cformat, int w, int h, const dgpu_block_params* bp, int nref) {
+extern "C" size_t dgpu_me_batch_workspace_bytes(int cformat, int w, int h, const dgpu_block_params* bp, int npics,
+                                                int ntasks, const int* task_ref2, int stages) {
     MeGeometry g;
-    if (me_geometry(cformat, w, h, bp, nref, g) != DGPU_OK) return 0;
-    MeBuffers B;
-    Arena a{nullptr, 0, 0};
-    return layout(g, B, a) + 256;
+    if (me_geometry(cformat, w, h, bp, 2, g) != DGPU_OK || npics <= 0 || ntasks <= 0) return 0;
+    std::vector<int> zeros(ntasks, 0);
+    BatchArgs A{};
+    A.npics = npics;
+    A.ntasks = ntasks;
+    A.stages = stages;
+    A.task_ref[0] = zeros.data();
+    A.task_ref[1] = task_ref2 ? task_ref2 : zeros.data();
+    // every picture may be a reference: size for the worst case
+    std::vector<int> all(npics);
+    for (int p = 0; p < npics; ++p) all[p] = p;
+    BatchArgs B = A;
+    std::vector<int> r0(std::max(npics, ntasks), 0);
+    for (int t = 0; t < std::max(npics, ntasks); ++t) r0[t] = t % npics;
+    B.ntasks = std::max(npics, ntasks);
+    B.task_ref[0] = r0.data();
+    std::vector<int> none(B.ntasks, -1);
+    B.task_ref[1] = none.data();
+    return batch_bytes(g, B, nullptr, nullptr, nullptr, nullptr);
+}
+
+extern "C" size_t dgpu_me_workspace_bytes(int cformat, int w, int h, const dgpu_block_params* bp, int nref) {
+    return dgpu_me_batch_workspace_bytes(cformat, w, h, bp, 3, 1, nullptr, 3);
+}
+
+extern "C" int dgpu_motion_estimate_batch(int cformat, int w, int h, const dgpu_block_params* bp, int luma_depth,
+                                          int npics, const int16_t* const* pics, int ntasks, const int* task_pic,
+                                          const int* task_ref1, const int* task_ref2, const float* task_lambda,
+                                          int stages, int16_t* const* mv_out, float* const* cost_out,
+                                          uint8_t* const* mode_out, int16_t* const* dc_out, uint8_t* const* split_out,
+                                          float* const* sbcost_out, void* workspace, size_t ws_bytes, void* stream) {
+    if (npics <= 0 || ntasks <= 0 || !pics || !task_pic || !task_ref1 || !task_ref2 || !task_lambda || !mv_out ||
+        !cost_out)
+        return DGPU_ERR_ARG;
+    if (stages >= 3 && (!mode_out || !dc_out || !split_out || !sbcost_out)) return DGPU_ERR_ARG;
+    MeGeometry g;
+    int rc = me_geometry(cformat, w, h, bp, 2, g);
+    if (rc) return rc;
+    rc = check_args(cformat, luma_depth, g);
+    if (rc) return rc;
+    for (int p = 0; p < npics; ++p)
+        for (int c = 0; c < (stages >= 3 ? 3 : 1); ++c)
+            if (!pics[3 * p + c]) return DGPU_ERR_ARG;
+    for (int t = 0; t < ntasks; ++t) {
+        if (task_pic[t] < 0 || task_pic[t] >= npics || task_ref1[t] < 0 || task_ref1[t] >= npics ||
+            task_ref2[t] >= npics || !mv_out[t] || !cost_out[t])
+            return DGPU_ERR_ARG;
+        if (stages >= 3 && (!mode_out[t] || !dc_out[t] || !split_out[t] || !sbcost_out[t])) return DGPU_ERR_ARG;
+    }
+    BatchArgs A{};
+    A.cformat = cformat;
+    A.w = w;
+    A.h = h;
+    A.luma_depth = luma_depth;
+    A.stages = stages;
+    A.prec = bp->precision;
+    A.npics = npics;
+    A.ntasks = ntasks;
+    A.pics = pics;
+    A.task_pic = task_pic;
+    A.task_ref[0] = task_ref1;
+    A.task_ref[1] = task_ref2;
+    A.task_lambda = task_lambda;
+    A.mv_out = mv_out;
+    A.cost_out = cost_out;
+    A.mode_out = mode_out;
+    A.dc_out = dc_out;
+    A.split_out = split_out;
+    A.sbcost_out = sbcost_out;
+    const size_t need = batch_bytes(g, A, nullptr, nullptr, nullptr, nullptr);
+    if (!workspace) {
+        rc = library_scratch(need, &workspace);
+        if (rc) return rc;
+    } else if (ws_bytes < need) {
+        return DGPU_ERR_NOMEM;
+    }
+    return run_batch(g, A, workspace, as_stream(stream));
 }
 
 extern "C" int dgpu_motion_estimate(int cformat, int w, int h, const dgpu_block_params* bp, int nref,
@@ -1078,218 +1479,12 @@ extern "C" int dgpu_motion_estimate(int cformat, int w, int h, const dgpu_block_
                                     int16_t* mv_out, float* cost_out, uint8_t* mode_out, int16_t* dc_out,
                                     uint8_t* split_out, float* sbcost_out, void* workspace, size_t ws_bytes,
                                     void* stream) {
-    if (!pic || !ref1 || !pic[0] || !ref1[0] || !mv_out || !cost_out) return DGPU_ERR_ARG;
-    if (nref == 2 && (!ref2 || !ref2[0])) return DGPU_ERR_ARG;
-    if (stages >= 3 && (!mode_out || !dc_out || !split_out || !sbcost_out || !pic[1] || !pic[2]))
-        return DGPU_ERR_ARG;
-    if (cformat < 0 || cformat > 2 || luma_depth < 2 || luma_depth > 15) return DGPU_ERR_ARG;
-    MeGeometry g;
-    int rc = me_geometry(cformat, w, h, bp, nref, g);
-    if (rc) return rc;
-    if (g.lb[0].xblen > 32 * 8 || g.lb[2].xblen > 64) return DGPU_ERR_SIZE;
-    cudaStream_t st = as_stream(stream);
-    const size_t need = dgpu_me_workspace_bytes(cformat, w, h, bp, nref);
-    if (!workspace) {
-        rc = library_scratch(need, &workspace);
-        if (rc) return rc;
-    } else if (ws_bytes < need) {
-        return DGPU_ERR_NOMEM;
-    }
-    MeBuffers B;
-    Arena a{static_cast<char*>(workspace), 0, need};
-    layout(g, B, a);
-    DGPU_CHECK_CUDA(cudaMemsetAsync(B.ctl, 0, 2 * sizeof(int), st));
-    const int16_t* src0[3] = {pic[0], ref1[0], nref > 1 ? ref2[0] : ref1[0]};
-    const size_t nb = (size_t)g.xnb[0] * g.ynb[0];
-    short2* mv0[2] = {reinterpret_cast<short2*>(mv_out), reinterpret_cast<short2*>(mv_out) + nb};
-    float* cost0[2] = {cost_out, cost_out + 3 * nb};
-
-    // ---- pyramids (PixelMatcher::MakePicHierarchy) ----
-    for (int l = 1; l <= g.depth; ++l) {
-        const int16_t* in[3];
-        int16_t* out[3];
-        int iw[3], ih[3], is[3], os[3];
-        const int ns = nref > 1 ? 3 : 2;
-        for (int s = 0; s < ns; ++s) {
-            in[s] = l == 1 ? src0[s] : B.down[s][l - 1];
-            out[s] = B.down[s][l];
-            iw[s] = g.pw[l - 1];
-            ih[s] = g.ph[l - 1];
-            is[s] = g.pw[l - 1];
-            os[s] = g.pw[l];
-        }
-        rc = dgpu_downconvert_batch(ns, in, iw, ih, is, out, os, stream);
-        if (rc) return rc;
-    }
-    // ---- pel search, coarsest level first (PixelMatcher::DoSearch) ----
-    for (int l = g.depth; l >= 0; --l) {
-        PelLaunch L{};
-        L.o = g.lb[2];
-        int total = 0;
-        for (int r = 0; r < nref; ++r) {
-            PelJob& J = L.job[L.njobs++];
-            J.pic = l ? B.down[0][l] : src0[0];
-            J.ref = l ? B.down[1 + r][l] : src0[1 + r];
-            J.pw = g.pw[l];
-            J.ph = g.ph[l];
-            J.xnb = g.xnb[l];
-            J.ynb = g.ynb[l];
-            J.mv = l ? B.mv[l][r] : mv0[r];
-            J.cost = l ? B.cost[l][r] : cost0[r];
-            J.guide = l < g.depth ? B.mv[l + 1][r] : nullptr;
-            J.gxnb = l < g.depth ? g.xnb[l + 1] : 0;
-            J.gynb = l < g.depth ? g.ynb[l + 1] : 0;
-            J.radius = std::min(l + 1, 5);
-            J.best_sad = B.best_sad[l][r];
-            J.best_mv = B.best_mv[l][r];
-            J.flags = B.flags + (size_t)r * g.xnb[l] * g.ynb[l];
-            J.first = total;
-            total += J.xnb * J.ynb;
-        }
-        L.total = total;
-        DGPU_CHECK_CUDA(cudaMemsetAsync(B.flags, 0, sizeof(int) * total, st));
-        rc = launch_pel(L, B.ctl, st);
-        if (rc) return rc;
-    }
-    int err_host = 0;
-    if (stages >= 2) {
-        // ---- lambda map on the host (long double statistics, as the reference) ----
-        std::vector<short2> hmv(nref * nb);
-        std::vector<float> hl(nb);
-        DGPU_CHECK_CUDA(cudaMemcpyAsync(hmv.data(), mv_out, sizeof(short2) * nref * nb, cudaMemcpyDeviceToHost, st));
-        DGPU_CHECK_CUDA(cudaMemcpyAsync(&err_host, B.ctl + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-        DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
-        if (err_host) return DGPU_ERR_CUDA;
-        lambda_map(hmv.data(), hmv.data() + nb, nref, g.xnb[0], g.ynb[0], lambda, hl.data());
-        DGPU_CHECK_CUDA(cudaMemcpyAsync(B.lambda[2], hl.data(), sizeof(float) * nb, cudaMemcpyHostToDevice, st));
-        // ---- upconverted original references (EncPicture::UpOrigData) ----
-        for (int r = 0; r < nref; ++r) {
-            rc = dgpu_upconvert(src0[1 + r], w, h, w, luma_depth, B.up[r], 2 * w, stream);
-            if (rc) return rc;
-        }
-        // ---- sub-pel refinement ----
-        SubLaunch S{};
-        S.o = g.lb[2];
-        S.prec = bp->precision;
-        int total = 0;
-        for (int r = 0; r < nref; ++r) {
-            SubJob& J = S.job[S.njobs++];
-            J.pic = src0[0];
-            J.up = B.up[r];
-            J.pw = w;
-            J.ph = h;
-            J.xnb = g.xnb[0];
-            J.ynb = g.ynb[0];
-            J.mv = mv0[r];
-            J.cost = cost0[r];
-            J.lambda = B.lambda[2];
-            J.flags = B.flags + (size_t)r * nb;
-            J.first = total;
-            total += (int)nb;
-        }
-        S.total = total;
-        S.ticket = B.ctl;
-        S.err = B.ctl + 1;
-        DGPU_CHECK_CUDA(cudaMemsetAsync(B.flags, 0, sizeof(int) * total, st));
-        DGPU_CHECK_CUDA(cudaMemsetAsync(B.ctl, 0, sizeof(int), st));
-        const int grid = std::min((total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, 148 * 8);
-        subpel_wavefront_kernel<<<grid, ME_THREADS, 0, st>>>(S);
-        DGPU_CHECK_LAUNCH();
-        if (stages >= 3) {
-            // ---- lambda maps of the superblock and sub-superblock levels ----
-            const float f0 = (float)(16 * g.lb[2].xblen * g.lb[2].yblen) / (float)(g.lb[0].xblen * g.lb[0].yblen);
-            const float f1 = (float)(4 * g.lb[2].xblen * g.lb[2].yblen) / (float)(g.lb[1].xblen * g.lb[1].yblen);
-            std::vector<float> l0(nb / 16), l1(nb / 4);
-            level_lambda_map(hl.data(), g.xnb[0], 0, g.xnb[0] / 4, g.ynb[0] / 4, (float)(1.0 / f0), l0.data());
-            level_lambda_map(hl.data(), g.xnb[0], 1, g.xnb[0] / 2, g.ynb[0] / 2, (float)(1.0 / f1), l1.data());
-            DGPU_CHECK_CUDA(cudaMemcpyAsync(B.lambda[0], l0.data(), sizeof(float) * l0.size(), cudaMemcpyHostToDevice, st));
-            DGPU_CHECK_CUDA(cudaMemcpyAsync(B.lambda[1], l1.data(), sizeof(float) * l1.size(), cudaMemcpyHostToDevice, st));
-            // fresh level data (a new MEData in the reference): zero vectors, costs, DCs
-            for (int lv = 0; lv < 2; ++lv) {
-                const size_t n = lv ? nb / 4 : nb / 16;
-                for (int r = 0; r < 2; ++r) {
-                    DGPU_CHECK_CUDA(cudaMemsetAsync(B.lmv[lv][r], 0, sizeof(short2) * n, st));
-                    DGPU_CHECK_CUDA(cudaMemsetAsync(B.lcost[lv][r], 0, sizeof(float) * 3 * n, st));
-                }
-                DGPU_CHECK_CUDA(cudaMemsetAsync(B.ldcy[lv], 0, sizeof(int16_t) * n, st));
-                DGPU_CHECK_CUDA(cudaMemsetAsync(B.lmode[lv], 0, n, st));
-            }
-            // the picture's DC arrays start at zero (a fresh MvData)
-            DGPU_CHECK_CUDA(cudaMemsetAsync(dc_out, 0, sizeof(int16_t) * 3 * nb, st));
-            ModeLaunch M{};
-            M.nref = nref;
-            M.prec = bp->precision;
-            for (int i = 0; i < 3; ++i) M.lb[i] = g.lb[i];
-            M.level_factor[0] = f0;
-            M.level_factor[1] = f1;
-            M.level_factor[2] = 1.0f;
-            ModeJob& J = M.job[M.njobs++];
-            J.pic = src0[0];
-            J.up[0] = B.up[0];
-            J.up[1] = nref > 1 ? B.up[1] : B.up[0];
-            J.pw = w;
-            J.ph = h;
-            for (int lv = 0; lv < 3; ++lv) {
-                LevelData& D = J.lev[lv];
-                D.xnb = g.xnb[0] >> (2 - lv);
-                D.ynb = g.ynb[0] >> (2 - lv);
-                D.lambda = B.lambda[lv];
-                if (lv == 2) {
-                    D.mv[0] = mv0[0];
-                    D.mv[1] = nref > 1 ? mv0[1] : mv0[0];
-                    D.cost[0] = cost0[0];
-                    D.cost[1] = nref > 1 ? cost0[1] : cost0[0];
-                    D.mode = mode_out;
-                    D.dcy = dc_out;
-                } else {
-                    D.mv[0] = B.lmv[lv][0];
-                    D.mv[1] = B.lmv[lv][1];
-                    D.cost[0] = B.lcost[lv][0];
-                    D.cost[1] = B.lcost[lv][1];
-                    D.mode = B.lmode[lv];
-                    D.dcy = B.ldcy[lv];
-                }
-            }
-            J.sbcost = sbcost_out;
-            J.split = split_out;
-            J.xnsb = g.xnsb;
-            J.ynsb = g.ynsb;
-            J.flags = B.flags;
-            J.first = 0;
-            M.total = g.xnsb * g.ynsb;
-            M.ticket = B.ctl;
-            M.err = B.ctl + 1;
-            DGPU_CHECK_CUDA(cudaMemsetAsync(B.flags, 0, sizeof(int) * M.total, st));
-            DGPU_CHECK_CUDA(cudaMemsetAsync(B.ctl, 0, sizeof(int), st));
-            const int mgrid = std::min((M.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, 148 * 8);
-            mode_wavefront_kernel<<<mgrid, ME_THREADS, 0, st>>>(M);
-            DGPU_CHECK_LAUNCH();
-            // ---- DC values of all three components ----
-            DcLaunch D{};
-            int dtotal = 0;
-            for (int c = 0; c < 3; ++c) {
-                const int xs = (c && cformat != 0) ? 1 : 0, ys = (c && cformat == 2) ? 1 : 0;
-                DcJob& Jd = D.job[D.njobs++];
-                Jd.pic = pic[c];
-                Jd.pw = w >> xs;
-                Jd.ph = h >> ys;
-                Jd.o = make_olb(g.lb[2].xblen >> xs, g.lb[2].yblen >> ys, g.lb[2].xbsep >> xs, g.lb[2].ybsep >> ys);
-                Jd.tmp = B.dctmp + (size_t)c * nb;
-                Jd.dc = dc_out + (size_t)c * nb;
-                Jd.xnb = g.xnb[0];
-                Jd.ynb = g.ynb[0];
-                Jd.first = dtotal;
-                dtotal += (int)nb;
-            }
-            D.total = dtotal;
-            block_dc_kernel<<<(dtotal + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, 0, st>>>(D);
-            DGPU_CHECK_LAUNCH();
-            smooth_dc_kernel<<<(dtotal + 255) / 256, 256, 0, st>>>(D);
-            DGPU_CHECK_LAUNCH();
-        }
-    }
-    DGPU_CHECK_CUDA(cudaMemcpyAsync(&err_host, B.ctl + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-    DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
-    if (err_host) return DGPU_ERR_CUDA;
-    return DGPU_OK;
+    if (!pic || !ref1 || (nref == 2 && !ref2) || nref < 1 || nref > 2) return DGPU_ERR_ARG;
+    const int16_t* pics[9] = {pic[0], pic[1], pic[2], ref1[0], ref1[1], ref1[2],
+                              nref == 2 ? ref2[0] : nullptr, nref == 2 ? ref2[1] : nullptr,
+                              nref == 2 ? ref2[2] : nullptr};
+    const int task_pic = 0, task_ref1 = 1, task_ref2 = nref == 2 ? 2 : -1;
+    return dgpu_motion_estimate_batch(cformat, w, h, bp, luma_depth, nref == 2 ? 3 : 2, pics, 1, &task_pic,
+                                      &task_ref1, &task_ref2, &lambda, stages, &mv_out, &cost_out, &mode_out, &dc_out,
+                                      &split_out, &sbcost_out, workspace, ws_bytes, stream);
 }

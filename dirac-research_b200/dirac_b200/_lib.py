@@ -76,10 +76,25 @@ SIGNATURES = {
     ),
     "dgpu_me_depth": (c_int, [c_int, c_int]),
     "dgpu_me_workspace_bytes": (c_size_t, [c_int, c_int, c_int, c_void_p, c_int]),
+    "dgpu_me_batch_workspace_bytes": (c_size_t, [c_int, c_int, c_int, c_void_p, c_int, c_int, P_int, c_int]),
+    "dgpu_motion_estimate_batch": (
+        c_int,
+        [c_int, c_int, c_int, c_void_p, c_int, c_int, P_void, c_int, P_int, P_int, P_int, c_void_p, c_int,
+         P_void, P_void, P_void, P_void, P_void, P_void, c_void_p, c_size_t, c_void_p],
+    ),
     "dgpu_motion_estimate": (
         c_int,
         [c_int, c_int, c_int, c_void_p, c_int, P_void, P_void, P_void, c_int, ctypes.c_float, c_int,
          c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p],
+    ),
+    "dgpu_quant_factor4": (c_int, [c_int]),
+    "dgpu_band_weights": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, ctypes.c_float, ctypes.c_float, c_int,
+                                  c_void_p]),
+    "dgpu_code_blocks": (c_int, [c_int, c_int, c_int, c_int, c_void_p]),
+    "dgpu_code_residue_batch": (
+        c_int,
+        [c_int, P_int, P_int, P_void, P_int, P_int, c_void_p, c_void_p, c_void_p, P_int, P_int, P_int, P_int,
+         c_void_p, P_void, c_void_p, c_size_t, c_void_p],
     ),
 }
 

@@ -146,3 +146,42 @@ class MotionEstimator:
             None, 0, _sp(stream))
         _lib.check(rc, "dgpu_motion_estimate")
         return out
+
+    def EstimateBatch(self, pics, tasks, stages=3, stream=None, outs=None):
+        """Batched motion estimation.  pics: list of 3-plane pictures (dense int16 CUDA
+        tensors); tasks: list of (pic index, ref1 index, ref2 index or -1, lambda).  Returns
+        (or fills, when outs is given) one output dict per task, as Estimate does."""
+        bp = self.bp
+        h, w = pics[0][0].shape
+        ynb, xnb = 4 * bp.ynum_sb, 4 * bp.xnum_sb
+        dev = pics[0][0].device
+        if outs is None:
+            outs = [self.new_outputs(dev) for _ in tasks]
+        planes = [p for pic in pics for p in pic]
+        for t in planes:
+            _i16(t, "plane")
+        n = len(tasks)
+        rc = self.lib.dgpu_motion_estimate_batch(
+            self.cformat, w, h, ctypes.byref(bp), self.luma_depth, len(pics),
+            _lib.ptr_array([p.data_ptr() for p in planes]), n,
+            _lib.int_array([t[0] for t in tasks]), _lib.int_array([t[1] for t in tasks]),
+            _lib.int_array([t[2] for t in tasks]),
+            (ctypes.c_float * n)(*[t[3] for t in tasks]), stages,
+            _lib.ptr_array([o["mv"].data_ptr() for o in outs]), _lib.ptr_array([o["cost"].data_ptr() for o in outs]),
+            _lib.ptr_array([o["mode"].data_ptr() for o in outs]), _lib.ptr_array([o["dc"].data_ptr() for o in outs]),
+            _lib.ptr_array([o["split"].data_ptr() for o in outs]),
+            _lib.ptr_array([o["sbcost"].data_ptr() for o in outs]), None, 0, _sp(stream))
+        _lib.check(rc, "dgpu_motion_estimate_batch")
+        return outs
+
+    def new_outputs(self, dev):
+        bp = self.bp
+        ynb, xnb = 4 * bp.ynum_sb, 4 * bp.xnum_sb
+        return {
+            "mv": torch.zeros((2, ynb, xnb, 2), dtype=torch.int16, device=dev),
+            "cost": torch.zeros((2, ynb, xnb, 3), dtype=torch.float32, device=dev),
+            "mode": torch.zeros((ynb, xnb), dtype=torch.uint8, device=dev),
+            "dc": torch.zeros((3, ynb, xnb), dtype=torch.int16, device=dev),
+            "split": torch.zeros((bp.ynum_sb, bp.xnum_sb), dtype=torch.uint8, device=dev),
+            "sbcost": torch.zeros((bp.ynum_sb, bp.xnum_sb), dtype=torch.float32, device=dev),
+        }

@@ -201,12 +201,64 @@ int dgpu_motion_compensate(int add_or_sub, int cformat, int w, int h, const dgpu
  * ------------------------------------------------------------------------------------- */
 int dgpu_me_depth(int w, int h);
 size_t dgpu_me_workspace_bytes(int cformat, int w, int h, const dgpu_block_params* bp, int nref);
+
+/* Batched form: ntasks pictures estimated in the same launches (a GOP's pictures, all the
+ * same size, format and block parameters).  pics holds npics pictures' three planes
+ * (pics[3*p + c]); task t estimates picture task_pic[t] against task_ref1[t] and, when
+ * task_ref2[t] >= 0, task_ref2[t], with lambda task_lambda[t].  Each picture's pyramid and
+ * (for references) upconverted luma are computed once for all tasks.  Outputs per task as in
+ * dgpu_motion_estimate (arrays of per-task device pointers).  One synchronisation for all
+ * lambda maps, one at the end. */
+size_t dgpu_me_batch_workspace_bytes(int cformat, int w, int h, const dgpu_block_params* bp, int npics,
+                                     int ntasks, const int* task_ref2, int stages);
+int dgpu_motion_estimate_batch(int cformat, int w, int h, const dgpu_block_params* bp, int luma_depth,
+                               int npics, const int16_t* const* pics, int ntasks, const int* task_pic,
+                               const int* task_ref1, const int* task_ref2, const float* task_lambda,
+                               int stages, int16_t* const* mv_out, float* const* cost_out,
+                               uint8_t* const* mode_out, int16_t* const* dc_out, uint8_t* const* split_out,
+                               float* const* sbcost_out, void* workspace, size_t ws_bytes, void* stream);
 int dgpu_motion_estimate(int cformat, int w, int h, const dgpu_block_params* bp, int nref,
                          const int16_t* const* pic, const int16_t* const* ref1,
                          const int16_t* const* ref2, int luma_depth, float lambda, int stages,
                          int16_t* mv_out, float* cost_out, uint8_t* mode_out, int16_t* dc_out,
                          uint8_t* split_out, float* sbcost_out, void* workspace, size_t ws_bytes,
                          void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Quantiser selection and quantisation of transformed components
+ * Replaces PictureCompressor::SelectQuantisers / SelectMultiQuants with QuantChooser
+ * (libdirac_encoder/picture_compress.cpp:603-709, quant_chooser.cpp:62-362) and the
+ * quantise-and-reconstruct arithmetic of CompCompressor::Compress and the band coders
+ * (comp_compress.cpp:64-156, band_codec_template.h:53-174, 470-557, band_codec.cpp:81-96).
+ *
+ * n components per call (up to 48).  coeff[c]: device, dense cw[c] x ch[c] int32 in the
+ * Mallat layout (the forward transform's output); reconstructed in place.  Per component:
+ * intra flag, transform depth, lambda (the component's quantiser lambda,
+ * PictureCompressor::GetCompLambda).  Per band, for all components concatenated in band-list
+ * order (band b of component c at index sum of earlier components' 3*depth+1, plus b-1):
+ * band_wt (CoeffArray::SetBandWeights, as float), band_ecf (EntropyCorrector::Factor) and
+ * band_ncb (code blocks x, y: EncoderParams::SetUsualCodeBlocks / SetupCodeBlocks) are host
+ * inputs; band_qidx, band_skip, band_bits (estimated bits) are host outputs, and cb_skip
+ * (host, all code blocks concatenated in raster order) receives the code-block skip flags.
+ * qout[c] (device, optional, same layout as coeff) receives the signed quantised indices (the
+ * intra DC band holds its prediction residues' indices).  The call synchronises the stream:
+ * the Lagrangian choice runs on the host in double precision like the reference's.
+ * ------------------------------------------------------------------------------------- */
+int dgpu_quant_factor4(int q);
+
+/* Host-only helpers (no GPU use) for the inputs above: CoeffArray::SetBandWeights
+ * (libdirac_common/wavelet_utils.cpp:192-395; cpd = EncoderParams::CPD(), cpd_scale as
+ * PictureCompressor::CodeResidue computes it) and the code-block grid of
+ * EncoderParams::SetUsualCodeBlocks (common.cpp:488-510; luma size, as the reference uses it
+ * for every component). */
+int dgpu_band_weights(int filter, int depth, int cw, int ch, int comp, int cformat, float cpd,
+                      float cpd_scale, int field_coding, double* out);
+int dgpu_code_blocks(int depth, int luma_w, int luma_h, int spatial_partition, int* ncb);
+int dgpu_code_residue_batch(int n, const int* intra, const int* depth, int32_t* const* coeff,
+                            const int* cw, const int* ch, const float* lambda, const float* band_wt,
+                            const float* band_ecf, const int* band_ncb, int* band_qidx, int* band_skip,
+                            int* band_bits, uint8_t* cb_skip, int32_t* const* qout, void* workspace,
+                            size_t ws_bytes, void* stream);
 
 #ifdef __cplusplus
 }

@@ -92,3 +92,26 @@ def test_me_nondyadic_lambda(gpu, oracle):
     want = oracle.motion_estimate(2, f[1], f[0], f[2], bp, lam, 3)
     got = run_gpu(gpu, 2, bp, f[1], f[0], f[2], lam, 3)
     compare(got, want, 3, "non-dyadic lambda")
+
+
+def test_me_batch_matches_oracle_per_task(gpu, oracle):
+    """A GOP-like batch: I B B P B B P with the reference's L1-separation-3 references,
+    all estimated in shared launches; every task must equal its single-picture oracle run."""
+    from oracle import BlockParams
+
+    w, h = 352, 288
+    from dirac_b200 import synth
+
+    seq = synth.make_sequence(w, h, 7, n_rects=10, vmax=10, seed=808)
+    f = [[synth.to_signed(p) for p in fr] for fr in seq]
+    bp = BlockParams(2, 12, 12, 8, 8, 11, 9)
+    bpg = gpu.BlockParams(2, 12, 12, 8, 8, 11, 9)
+    # display order; references as SequenceCompressor sets them for L1_sep = 3
+    tasks = [(3, 0, -1, 10.0), (1, 0, 3, 10.0), (2, 1, 3, 10.0), (6, 3, 0, 10.0), (4, 3, 6, 10.0),
+             (5, 4, 6, 10.0)]
+    me = gpu.MotionEstimator(bpg, 2)
+    outs = me.EstimateBatch([[dev(p) for p in fr] for fr in f], tasks, 3)
+    for (p, r1, r2, lam), o in zip(tasks, outs):
+        want = oracle.motion_estimate(2, f[p], f[r1], f[r2] if r2 >= 0 else None, bp, lam, 3)
+        got = {k: v.cpu().numpy() for k, v in o.items()}
+        compare(got, want, 3, f"task pic {p}")
