@@ -410,6 +410,32 @@ using namespace dgpu;
 
 extern "C" int dgpu_quant_factor4(int q) { return (q < 0 || q > 119) ? DGPU_ERR_ARG : qf4(q); }
 
+// Device workspace of one dgpu_code_residue_batch call: task table, band and code-block
+// maxima, statistics, intra DC prediction residues, code-block skip flags and the
+// sequential-sum fallback cases.
+static size_t residue_ws_need(int nb_total, int ncb_total, size_t dcwork_elems) {
+    return align_up(sizeof(BandTask) * nb_total, 256) + align_up(sizeof(int) * nb_total, 256) +
+           align_up(sizeof(int) * ncb_total, 256) + align_up(sizeof(Stat) * nb_total * 2 * QMAX, 256) +
+           align_up(sizeof(int32_t) * dcwork_elems, 256) + align_up(ncb_total, 256) +
+           align_up((sizeof(SeqCase) + sizeof(double)) * nb_total * 2 * QMAX, 256) + 256;
+}
+
+extern "C" size_t dgpu_code_residue_workspace_bytes(int n, const int* intra, const int* depth, const int* cw,
+                                                     const int* ch, const int* band_ncb) {
+    if (n <= 0 || n > MAX_COMPS || !intra || !depth || !cw || !ch || !band_ncb) return 0;
+    int nb_total = 0, ncb_total = 0;
+    size_t dcwork_elems = 0;
+    for (int c = 0; c < n; ++c) {
+        const int d = depth[c];
+        if (d < 1 || d > 8) return 0;
+        for (int b = 0; b < 3 * d + 1; ++b)
+            ncb_total += band_ncb[2 * (nb_total + b)] * band_ncb[2 * (nb_total + b) + 1];
+        if (intra[c]) dcwork_elems += (size_t)(cw[c] >> d) * (ch[c] >> d);
+        nb_total += 3 * d + 1;
+    }
+    return residue_ws_need(nb_total, ncb_total, dcwork_elems);
+}
+
 extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth, int32_t* const* coeff,
                                        const int* cw, const int* ch, const float* lambda, const float* band_wt,
                                        const float* band_ecf, const int* band_ncb, int* band_qidx, int* band_skip,
@@ -441,10 +467,7 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     }
     if (nb_total > MAX_TASKS) return DGPU_ERR_ARG;
     // ---- workspace ----
-    const size_t need = align_up(sizeof(BandTask) * nb_total, 256) + align_up(sizeof(int) * nb_total, 256) +
-                        align_up(sizeof(int) * ncb_total, 256) + align_up(sizeof(Stat) * nb_total * 2 * QMAX, 256) +
-                        align_up(sizeof(int32_t) * dcwork_elems, 256) + align_up(ncb_total, 256) +
-                        align_up((sizeof(SeqCase) + sizeof(double)) * nb_total * 2 * QMAX, 256) + 256;
+    const size_t need = residue_ws_need(nb_total, ncb_total, dcwork_elems);
     if (!workspace) {
         int rc = library_scratch(need, &workspace);
         if (rc) return rc;

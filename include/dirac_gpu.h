@@ -254,6 +254,10 @@ int dgpu_quant_factor4(int q);
 int dgpu_band_weights(int filter, int depth, int cw, int ch, int comp, int cformat, float cpd,
                       float cpd_scale, int field_coding, double* out);
 int dgpu_code_blocks(int depth, int luma_w, int luma_h, int spatial_partition, int* ncb);
+/* Device workspace bytes one dgpu_code_residue_batch call with these components needs
+ * (0 on invalid arguments). */
+size_t dgpu_code_residue_workspace_bytes(int n, const int* intra, const int* depth, const int* cw,
+                                         const int* ch, const int* band_ncb);
 int dgpu_code_residue_batch(int n, const int* intra, const int* depth, int32_t* const* coeff,
                             const int* cw, const int* ch, const float* lambda, const float* band_wt,
                             const float* band_ecf, const int* band_ncb, int* band_qidx, int* band_skip,

@@ -263,3 +263,41 @@ class Reference:
         ncbt = int(np.sum(ncb[0::2] * ncb[1::2]))
         return {"recon": c, "qidx": q, "skip": sk, "wt": wt, "ecf": ecf, "bits": bits, "ncb": ncb,
                 "cb_skip": cbs[:ncbt].copy()}
+
+
+class RefEncParams(ctypes.Structure):
+    """Mirror of RefEncParams in oracle/ref_encoder.cpp."""
+
+    _fields_ = [("video_format", ctypes.c_int), ("cformat", ctypes.c_int), ("width", ctypes.c_int),
+                ("height", ctypes.c_int), ("qf", ctypes.c_float), ("l1_sep", ctypes.c_int),
+                ("num_l1", ctypes.c_int), ("cpd", ctypes.c_float), ("xblen", ctypes.c_int),
+                ("yblen", ctypes.c_int), ("xbsep", ctypes.c_int), ("ybsep", ctypes.c_int),
+                ("mv_precision", ctypes.c_int), ("intra_filter", ctypes.c_int), ("inter_filter", ctypes.c_int),
+                ("wlt_depth", ctypes.c_int)]
+
+
+def reference_encode(cfg, frames, freeze=True, path=REF_SO):
+    """Encode 8-bit frames [(Y, U, V) uint8 planes] with the reference encoder's public API.
+    cfg: dict with the RefEncParams fields.  Returns (recon frames as (Y, U, V) uint8 planes
+    by picture number, per-picture intra flags, total bitstream bytes)."""
+    lib = Reference(path).lib
+    p = RefEncParams(**cfg)
+    n = len(frames)
+    flat = np.concatenate([np.concatenate([np.ascontiguousarray(c, np.uint8).ravel() for c in f]) for f in frames])
+    recon = np.zeros_like(flat)
+    ptype = np.zeros(n, np.int32)
+    nbytes = ctypes.c_longlong(0)
+    rc = lib.ref_encode_sequence(ctypes.byref(p), n, _p(flat), int(freeze), _p(recon), _p(ptype), ctypes.byref(nbytes))
+    if rc:
+        raise ValueError("ref_encode_sequence failed")
+    shapes = [c.shape for c in frames[0]]
+    fsize = sum(int(np.prod(s)) for s in shapes)
+    out = []
+    for i in range(n):
+        fr, o = [], i * fsize
+        for s in shapes:
+            k = int(np.prod(s))
+            fr.append(recon[o:o + k].reshape(s))
+            o += k
+        out.append(tuple(fr))
+    return out, ptype, nbytes.value

@@ -152,6 +152,51 @@ def quant_cases(ref):
     return out
 
 
+ENCODE_CASES = [
+    # (name, w, h, frames, seed A, seed B, switch frame or None, n_rects, vmax, qf, num_l1,
+    #  intra filter, inter filter, depth, xblen, yblen, xbsep, ybsep, precision)
+    ("cif", 352, 288, 16, 1, None, None, 8, 8, 7.0, 19, 1, 0, 4, 12, 12, 8, 8, 2),
+    ("reconfig", 176, 144, 14, 11, 12, 3, 4, 4, 7.0, 19, 1, 0, 3, 12, 12, 8, 8, 2),
+    ("cut_b", 176, 144, 14, 11, 12, 5, 4, 4, 7.0, 19, 1, 0, 3, 12, 12, 8, 8, 2),
+    ("cut_p", 176, 144, 14, 11, 12, 7, 4, 4, 7.0, 19, 1, 0, 3, 12, 12, 8, 8, 2),
+    ("gop", 176, 144, 13, 21, None, None, 6, 6, 5.0, 2, 6, 2, 4, 16, 16, 12, 12, 3),
+]
+
+
+def encode_inputs(case):
+    """8-bit frames of one ENCODE_CASES entry and its RefEncParams fields."""
+    sys.path.insert(0, os.path.join(HERE, "..", "..", "dirac-research_b200"))
+    from dirac_b200 import synth
+
+    (name, w, h, n, sa, sb, sw, nr, vm, qf, nl1, fi, fr, depth, xbl, ybl, xbs, ybs, prec) = case
+    seq = synth.make_sequence(w, h, n, n_rects=nr, vmax=vm, seed=sa)
+    if sb is not None:
+        seq = seq[:sw] + synth.make_sequence(w, h, n, n_rects=nr, vmax=vm, seed=sb)[sw:]
+    cfg = dict(video_format=0, cformat=2, width=w, height=h, qf=qf, l1_sep=3, num_l1=nl1, cpd=20.0, xblen=xbl,
+               yblen=ybl, xbsep=xbs, ybsep=ybs, mv_precision=prec, intra_filter=fi, inter_filter=fr, wlt_depth=depth)
+    return seq, cfg
+
+
+def encode_cases():
+    """The reference encoder run through its public API (initial entropy-correction factors
+    kept, as a coding loop without the arithmetic coder does): CRC-32 of every locally
+    decoded plane and the picture types, for sequences that exercise the plain GOP, the
+    switch to P-only sub-groups and cut detection."""
+    import zlib
+
+    from oracle import reference_encode
+
+    out = {}
+    for case in ENCODE_CASES:
+        seq, cfg = encode_inputs(case)
+        rec, ptype, nbytes = reference_encode(cfg, seq, freeze=True)
+        name = case[0]
+        out[name + "_crc"] = np.array([[zlib.crc32(np.ascontiguousarray(p).tobytes()) for p in f] for f in rec],
+                                      np.uint32)
+        out[name + "_ptype"] = ptype
+    return out
+
+
 def main():
     ref = Reference()
     np.savez_compressed(os.path.join(HERE, "dwt.npz"), **dwt_cases(ref))
@@ -159,7 +204,8 @@ def main():
     np.savez_compressed(os.path.join(HERE, "mc.npz"), **mc_cases(ref))
     np.savez_compressed(os.path.join(HERE, "me.npz"), **me_cases(ref))
     np.savez_compressed(os.path.join(HERE, "quant.npz"), **quant_cases(ref))
-    print("wrote dwt.npz, convert.npz, mc.npz, me.npz, quant.npz")
+    np.savez_compressed(os.path.join(HERE, "encode.npz"), **encode_cases())
+    print("wrote dwt.npz, convert.npz, mc.npz, me.npz, quant.npz, encode.npz")
 
 
 if __name__ == "__main__":
