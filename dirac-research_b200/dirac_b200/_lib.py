@@ -91,6 +91,7 @@ SIGNATURES = {
     "dgpu_band_weights": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, ctypes.c_float, ctypes.c_float, c_int,
                                   c_void_p]),
     "dgpu_code_blocks": (c_int, [c_int, c_int, c_int, c_int, c_void_p]),
+    "dgpu_code_residue_workspace_bytes": (c_size_t, [c_int, P_int, P_int, P_int, P_int, P_int]),
     "dgpu_code_residue_batch": (
         c_int,
         [c_int, P_int, P_int, P_void, P_int, P_int, c_void_p, c_void_p, c_void_p, P_int, P_int, P_int, P_int,
