@@ -1,0 +1,840 @@
+// Sequence encoder: the reference's frame-coding loop over the library's kernels, with all
+// picture data resident on the device.
+//
+// Host side: the GOP state machine of FrameSequenceCompressor / SequenceCompressor
+// (libdirac_encoder/seq_compress.cpp:151-192 CanEncode, 194-499 CompressNextPicture,
+// 563-632 SetPicTypeAndRefs, 664-686 CodedToDisplay), the lambdas of
+// EncoderParams::CalcLambdas (libdirac_common/common.cpp:451-476) and
+// PictureCompressor::GetCompLambda (libdirac_encoder/picture_compress.cpp:532-580), the
+// perceptual-weight scale and intra-block ratio of PictureCompressor::CodeResidue /
+// IntraModeAnalyse (picture_compress.cpp:300-320, 418-428).
+//
+// Device side, per picture: motion estimation (batched over every picture whose references
+// are known, ahead of coding order: estimation reads only original pictures), motion
+// compensation (SUBTRACT) against the upconverted reconstructed references, the forward
+// transform of the three components in one batch, quantiser choice and quantisation, the
+// inverse transform, motion compensation (ADD) with the clip fused, and the upconversion of
+// reference pictures when a later picture first needs them (Picture::UpData,
+// libdirac_common/picture.cpp:141-199).
+//
+// Device memory: one arena per encoder, cut into max_pictures picture slots (original,
+// working / reconstructed planes, coefficients, quantised indices, upconverted planes, motion
+// data) plus the workspaces of motion estimation, transform and quantisation, all sized at
+// creation.  A 1080p 4:2:0 slot is about 64 MB.
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <new>
+#include <vector>
+
+#include "dgpu_internal.cuh"
+
+namespace dgpu {
+namespace {
+
+constexpr int kIntraMode = 0;  // PredMode INTRA (libdirac_common/common.h:84)
+constexpr int kMaxCountTasks = 64;
+
+struct Lambdas {
+    float i, l1, l2, me;
+};
+
+// EncoderParams::CalcLambdas: float members, std::sqrt of a float member.
+Lambdas calc_lambdas(float qf) {
+    Lambdas L;
+    L.i = (float)(std::pow(10.0, (12.0 - (double)qf) / 2.5) / 16.0);
+    L.l1 = (float)((double)L.i * 4.0);
+    L.l2 = (float)((double)L.i * 32.0);
+    L.me = (float)((double)std::sqrt(L.l1) * 2.0);
+    return L;
+}
+
+// ---------------------------------------------------------------------------------------
+// small kernels: input conversion, output conversion, intra-block counts
+// ---------------------------------------------------------------------------------------
+struct Planes3 {
+    const void* src[3];
+    int16_t* orig[3];
+    int16_t* data[3];
+    int n[3];
+};
+
+// Unsigned input samples to codec samples (value - 2^(depth-1)), as StreamFrameInput reads
+// them (libdirac_common/pic_io.cpp:388-399), written to the original and working planes.
+template <typename T>
+__global__ void load_kernel(const __grid_constant__ Planes3 P, int off_luma, int off_chroma) {
+    const int c = blockIdx.y;
+    const T* __restrict__ src = static_cast<const T*>(P.src[c]);
+    const int off = c == 0 ? off_luma : off_chroma;
+    const int n = P.n[c];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int16_t v = (int16_t)((int)src[i] - off);
+        P.orig[c][i] = v;
+        P.data[c][i] = v;
+    }
+}
+
+template <typename T>
+__global__ void output_kernel(const int16_t* __restrict__ rec, int n, int off, T* __restrict__ dst) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        dst[i] = (T)((int)rec[i] + off);
+}
+
+struct CountArgs {
+    const uint8_t* mode[kMaxCountTasks];
+    int n;
+};
+
+// Number of INTRA blocks per task (PictureCompressor::IntraModeAnalyse's count).
+__global__ void count_intra_kernel(const __grid_constant__ CountArgs A, int* __restrict__ counts) {
+    const uint8_t* __restrict__ m = A.mode[blockIdx.x];
+    int c = 0;
+    for (int i = threadIdx.x; i < A.n; i += blockDim.x) c += m[i] == kIntraMode;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    __shared__ int part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += part[k];
+        counts[blockIdx.x] = t;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// host structures
+// ---------------------------------------------------------------------------------------
+struct Slot {
+    int16_t* orig[3];
+    int16_t* data[3];
+    int32_t* coeff[3];
+    int32_t* qout[3];
+    int16_t* up[3];
+    int16_t* mv;
+    float* cost;
+    uint8_t* mode;
+    int16_t* dc;
+    uint8_t* split;
+    float* sbcost;
+    int pnum = -1;  // -1: free
+};
+
+struct Pic {
+    int pnum = -1;
+    int slot = -1;
+    bool typed = false, intra = true, is_ref = true, coded = false, cut = false;
+    std::vector<int> refs;
+    bool me_valid = false;
+    std::vector<int> me_refs;
+    double ratio = 0.0;
+    bool up_valid = false;
+    dgpu_picture_info info{};
+    std::vector<int> bands;        // [3][nb][3]
+    std::vector<uint8_t> cb_skip;  // [3][ncb]
+
+    bool is_b() const {
+        return refs.size() == 2 && ((refs[0] < pnum && refs[1] > pnum) || (refs[0] > pnum && refs[1] < pnum));
+    }
+};
+
+struct Encoder {
+    dgpu_encoder_params P{};
+    cudaStream_t st = nullptr;
+    Lambdas L{};
+    int xs = 0, ys = 0;          // chroma shifts
+    int w[3]{}, h[3]{};          // component sizes
+    int pw[3]{}, ph[3]{};        // padded (transform) sizes
+    dgpu_block_params bp{};
+    int nblocks = 0, nsb = 0, nb = 0;
+    std::vector<int> ncb;        // per band (x, y), identical for the three components
+    int ncb_total = 0;
+
+    // GOP state (seq_compress.cpp member names in comments)
+    int L1Sep = 0, num_L1 = 0, gop_len = 0;
+    int m_L1_sep = 0;            // m_L1_sep
+    int gop_start = 0;           // m_gop_start_num
+    int code = 0;                // m_current_code_pnum
+    int cur = -1;                // m_current_display_pnum
+    int last_read = -1;          // m_last_picture_read
+    bool eos = false;            // m_eos_signalled
+    std::map<int, Pic> pics;
+
+    // device memory
+    void* arena = nullptr;
+    std::vector<Slot> slots;
+    void* me_ws = nullptr;
+    size_t me_ws_bytes = 0;
+    int me_max_tasks = 0;
+    void* dwt_ws = nullptr;
+    size_t dwt_ws_bytes = 0;
+    void* q_ws = nullptr;
+    size_t q_ws_bytes = 0;
+    int* d_counts = nullptr;
+    void* stage = nullptr;       // one input / output frame of samples
+    size_t stage_bytes = 0;
+    int* h_counts = nullptr;     // pinned
+
+    ~Encoder() {
+        if (arena) cudaFree(arena);
+        if (h_counts) cudaFreeHost(h_counts);
+    }
+};
+
+int comp_depth(const Encoder& E, int c) { return c == 0 ? E.P.luma_depth : E.P.chroma_depth; }
+
+size_t sample_bytes(const Encoder& E) { return E.P.luma_depth > 8 || E.P.chroma_depth > 8 ? 2 : 1; }
+
+// ---- GOP structure ----------------------------------------------------------------------
+int coded_to_display(const Encoder& E, int cnum) {
+    const int s = E.m_L1_sep;
+    if (s > 0) {
+        if (cnum == 0) return 0;
+        if ((cnum - 1) % s == 0) return cnum + s - 1;
+        return cnum - 1;
+    }
+    return cnum;
+}
+
+bool can_encode(Encoder& E) {
+    if (E.eos) {
+        if (E.num_L1 > 0) {
+            if (E.last_read >= E.code + (E.last_read % E.L1Sep)) return true;
+            if (E.code <= E.last_read) {
+                E.cur = E.code;
+                return true;
+            }
+            return false;
+        }
+        return E.last_read >= E.cur;
+    }
+    return E.last_read >= E.cur + std::max(4, 2 * E.L1Sep);
+}
+
+// FrameSequenceCompressor::SetPicTypeAndRefs with the given separation; `avail` is the last
+// loaded picture number (IsPictureAvail).
+void type_refs(const Encoder& E, int pnum, int sep, int avail, bool& intra, bool& is_ref, std::vector<int>& refs) {
+    const int rel = pnum - E.gop_start;
+    refs.clear();
+    if (E.num_L1 > 0) {
+        if (rel % E.gop_len == 0) {
+            intra = true;
+            is_ref = E.gop_len > 1;
+        } else if (rel % sep == 0) {
+            intra = false;
+            is_ref = true;
+            refs.push_back(pnum - sep);
+            if ((rel - sep) % E.gop_len > 0 && sep > 1) refs.push_back(pnum - 2 * sep);
+        } else if ((rel + 1) % sep == 0) {
+            intra = false;
+            is_ref = false;
+            refs.push_back(pnum - 1);
+            if (pnum + 1 <= avail) refs.push_back(pnum + 1);
+        } else {
+            intra = false;
+            is_ref = true;
+            refs.push_back(pnum - 1);
+            const int next_ref = (pnum / sep + 1) * sep;
+            if (next_ref <= avail) refs.push_back(next_ref);
+        }
+    } else {
+        intra = true;
+        is_ref = false;
+    }
+}
+
+void set_type(Encoder& E, Pic& p) {
+    type_refs(E, p.pnum, E.m_L1_sep, E.last_read, p.intra, p.is_ref, p.refs);
+    p.typed = true;
+}
+
+// ---- device helpers ---------------------------------------------------------------------
+Slot& slot_of(Encoder& E, const Pic& p) { return E.slots[p.slot]; }
+
+int ensure_up(Encoder& E, Pic& r) {
+    if (r.up_valid) return DGPU_OK;
+    Slot& s = slot_of(E, r);
+    const int16_t* pic[3] = {s.data[0], s.data[1], s.data[2]};
+    int16_t* up[3] = {s.up[0], s.up[1], s.up[2]};
+    int ups[3], bd[3];
+    for (int c = 0; c < 3; ++c) {
+        ups[c] = 2 * E.w[c];
+        bd[c] = comp_depth(E, c);
+    }
+    const int rc = dgpu_upconvert_batch(3, pic, E.w, E.h, E.w, bd, up, ups, E.st);
+    if (rc) return rc;
+    r.up_valid = true;
+    return DGPU_OK;
+}
+
+// Refs a not-yet-typed picture will most likely get (the normal separation): used only to
+// estimate ahead; results are keyed by the references they were computed with.
+bool predicted_refs(const Encoder& E, const Pic& q, std::vector<int>& refs) {
+    if (q.typed) {
+        if (q.intra) return false;
+        refs = q.refs;
+        return true;
+    }
+    bool intra, is_ref;
+    type_refs(E, q.pnum, E.L1Sep, E.last_read, intra, is_ref, refs);
+    return !intra;
+}
+
+// Motion estimation of p against its current references, batched with every other loaded
+// picture whose references are (or will most likely be) known and already loaded.
+int ensure_me(Encoder& E, Pic& p) {
+    if (p.me_valid && p.me_refs == p.refs) return DGPU_OK;
+    struct Task {
+        int pnum;
+        std::vector<int> refs;
+    };
+    std::vector<Task> tasks;
+    tasks.push_back({p.pnum, p.refs});
+    for (auto& kv : E.pics) {
+        Pic& q = kv.second;
+        if ((int)tasks.size() >= E.me_max_tasks) break;
+        if (q.pnum == p.pnum || q.coded) continue;
+        // without the end of the sequence, a picture's references may still change as
+        // pictures arrive: only look at pictures a full sub-group before the last loaded
+        if (!E.eos && q.pnum + std::max(E.L1Sep, 1) > E.last_read) continue;
+        std::vector<int> refs;
+        if (!predicted_refs(E, q, refs)) continue;
+        if (q.me_valid && q.me_refs == refs) continue;
+        bool ok = true;
+        for (int r : refs) ok = ok && r >= 0 && r <= E.last_read && E.pics.count(r) && E.pics[r].slot >= 0;
+        if (ok) tasks.push_back({q.pnum, refs});
+    }
+    // pictures involved, in first-use order
+    std::vector<int> pics_used;
+    auto index_of = [&](int pn) {
+        for (size_t k = 0; k < pics_used.size(); ++k)
+            if (pics_used[k] == pn) return (int)k;
+        pics_used.push_back(pn);
+        return (int)pics_used.size() - 1;
+    };
+    const int nt = (int)tasks.size();
+    std::vector<int> tp(nt), t1(nt), t2(nt);
+    std::vector<float> tl(nt, E.L.me);  // L1MELambda == L2MELambda (common.cpp:464-465)
+    for (int t = 0; t < nt; ++t) {
+        tp[t] = index_of(tasks[t].pnum);
+        t1[t] = index_of(tasks[t].refs[0]);
+        t2[t] = tasks[t].refs.size() > 1 ? index_of(tasks[t].refs[1]) : -1;
+    }
+    std::vector<const int16_t*> planes;
+    for (int pn : pics_used) {
+        Slot& s = E.slots[E.pics[pn].slot];
+        for (int c = 0; c < 3; ++c) planes.push_back(s.orig[c]);
+    }
+    std::vector<int16_t*> mv(nt), dc(nt);
+    std::vector<float*> cost(nt), sbc(nt);
+    std::vector<uint8_t*> mode(nt), split(nt);
+    for (int t = 0; t < nt; ++t) {
+        Slot& s = E.slots[E.pics[tasks[t].pnum].slot];
+        mv[t] = s.mv;
+        cost[t] = s.cost;
+        mode[t] = s.mode;
+        dc[t] = s.dc;
+        split[t] = s.split;
+        sbc[t] = s.sbcost;
+    }
+    int rc = dgpu_motion_estimate_batch(E.P.cformat, E.w[0], E.h[0], &E.bp, E.P.luma_depth, (int)pics_used.size(),
+                                        planes.data(), nt, tp.data(), t1.data(), t2.data(), tl.data(), 3, mv.data(),
+                                        cost.data(), mode.data(), dc.data(), split.data(), sbc.data(), E.me_ws,
+                                        E.me_ws_bytes, E.st);
+    if (rc) return rc;
+    for (int t0 = 0; t0 < nt; t0 += kMaxCountTasks) {
+        CountArgs A{};
+        const int k = std::min(kMaxCountTasks, nt - t0);
+        for (int t = 0; t < k; ++t) A.mode[t] = mode[t0 + t];
+        A.n = E.nblocks;
+        count_intra_kernel<<<k, 256, 0, E.st>>>(A, E.d_counts + t0);
+        DGPU_CHECK_LAUNCH();
+    }
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(E.h_counts, E.d_counts, sizeof(int) * nt, cudaMemcpyDeviceToHost, E.st));
+    DGPU_CHECK_CUDA(cudaStreamSynchronize(E.st));
+    for (int t = 0; t < nt; ++t) {
+        Pic& q = E.pics[tasks[t].pnum];
+        q.me_valid = true;
+        q.me_refs = tasks[t].refs;
+        q.ratio = (double)E.h_counts[t] / (double)E.nblocks;
+    }
+    return DGPU_OK;
+}
+
+int motion_compensate(Encoder& E, Pic& p, int add_or_sub, bool clip) {
+    Slot& s = slot_of(E, p);
+    Pic& r1 = E.pics[p.refs[0]];
+    int rc = ensure_up(E, r1);
+    if (rc) return rc;
+    const int16_t* up1[3] = {E.slots[r1.slot].up[0], E.slots[r1.slot].up[1], E.slots[r1.slot].up[2]};
+    const int16_t* up2[3] = {nullptr, nullptr, nullptr};
+    const bool two = p.refs.size() > 1;
+    if (two) {
+        Pic& r2 = E.pics[p.refs[1]];
+        rc = ensure_up(E, r2);
+        if (rc) return rc;
+        for (int c = 0; c < 3; ++c) up2[c] = E.slots[r2.slot].up[c];
+    }
+    int16_t* pic[3] = {s.data[0], s.data[1], s.data[2]};
+    return dgpu_motion_compensate(add_or_sub, E.P.cformat, E.w[0], E.h[0], &E.bp, s.mv,
+                                  two ? s.mv + 2 * E.nblocks : nullptr, s.mode, s.dc, s.split, pic, E.w, up1,
+                                  two ? up2 : nullptr, clip ? E.P.luma_depth : 0, clip ? E.P.chroma_depth : 0, E.st);
+}
+
+int transform(Encoder& E, Pic& p, int dir, int filter) {
+    Slot& s = slot_of(E, p);
+    int filt[3] = {filter, filter, filter};
+    int depth[3] = {E.P.wlt_depth, E.P.wlt_depth, E.P.wlt_depth};
+    int16_t* pic[3] = {s.data[0], s.data[1], s.data[2]};
+    int32_t* coeff[3] = {s.coeff[0], s.coeff[1], s.coeff[2]};
+    return dgpu_wavelet_transform_batch(dir, 3, filt, depth, pic, E.w, E.h, E.w, coeff, E.pw, E.ph, E.pw, E.dwt_ws,
+                                        E.dwt_ws_bytes, E.st);
+}
+
+// PictureCompressor::GetCompLambda (picture_compress.cpp:532-580): std::log10 of the float
+// lambdas is the single-precision overload; the blend is double; U and V factors 1.5 / 0.75
+// (dirac_encoder.cpp:552-553) multiply in float.
+float comp_lambda(const Encoder& E, const Pic& p, int comp) {
+    float lambda;
+    if (p.intra) {
+        lambda = E.L.i;
+    } else {
+        const double log_intra = std::log10(E.L.i);
+        const double log_pic = p.is_b() ? std::log10(E.L.l2) : std::log10(E.L.l1);
+        const float ir = (float)p.ratio;
+        lambda = (float)std::pow(10.0, 3.0 * ir * log_intra + (1.0 - 3.0 * ir) * log_pic);
+    }
+    if (comp == 1) lambda *= 1.5f;
+    if (comp == 2) lambda *= 0.75f;
+    return lambda;
+}
+
+// EntropyCorrector::Init (common.cpp:79-131): the same initial factors for all components.
+void initial_ecf(int depth, bool intra, float* out) {
+    const int nb = 3 * depth + 1;
+    for (int b = 0; b < nb; ++b) out[b] = 0.75f;
+    for (int b = nb - 4; b < nb - 1; ++b) out[b] = intra ? 0.85f : 0.75f;
+    out[nb - 1] = intra ? 1.0f : 0.85f;
+}
+
+int code_residue(Encoder& E, Pic& p, const float* ecf_in) {
+    Slot& s = slot_of(E, p);
+    const int depth = E.P.wlt_depth;
+    const int filter = p.intra ? E.P.intra_filter : E.P.inter_filter;
+    double cpd_scale = 1.0;
+    if (!p.intra) {
+        const float ir = (float)p.ratio;
+        cpd_scale = 5.0 * ir * 1.0 + (1.0 - 5.0 * ir) * 0.125;
+        cpd_scale = std::max(0.125, std::min(1.2, cpd_scale));
+    }
+    const int nb = E.nb;
+    std::vector<float> wt(3 * nb), ecf(3 * nb);
+    std::vector<int> ncb(6 * nb);
+    std::vector<double> wd(nb);
+    float lam[3];
+    int intra[3], dep[3];
+    for (int c = 0; c < 3; ++c) {
+        int rc = dgpu_band_weights(filter, depth, E.pw[c], E.ph[c], c, E.P.cformat, E.P.cpd, (float)cpd_scale, 0,
+                                   wd.data());
+        if (rc) return rc;
+        for (int b = 0; b < nb; ++b) wt[c * nb + b] = (float)wd[b];
+        if (ecf_in)
+            std::memcpy(&ecf[c * nb], ecf_in + c * nb, sizeof(float) * nb);
+        else
+            initial_ecf(depth, p.intra, &ecf[c * nb]);
+        std::memcpy(&ncb[2 * c * nb], E.ncb.data(), sizeof(int) * 2 * nb);
+        lam[c] = comp_lambda(E, p, c);
+        intra[c] = p.intra ? 1 : 0;
+        dep[c] = depth;
+    }
+    std::vector<int> qidx(3 * nb), skip(3 * nb), bits(3 * nb);
+    p.cb_skip.assign((size_t)3 * E.ncb_total, 0);
+    int32_t* coeff[3] = {s.coeff[0], s.coeff[1], s.coeff[2]};
+    int32_t* qout[3] = {s.qout[0], s.qout[1], s.qout[2]};
+    int rc = transform(E, p, DGPU_FORWARD, filter);
+    if (rc) return rc;
+    rc = dgpu_code_residue_batch(3, intra, dep, coeff, E.pw, E.ph, lam, wt.data(), ecf.data(), ncb.data(),
+                                 qidx.data(), skip.data(), bits.data(), p.cb_skip.data(), qout, E.q_ws, E.q_ws_bytes,
+                                 E.st);
+    if (rc) return rc;
+    rc = transform(E, p, DGPU_BACKWARD, filter);
+    if (rc) return rc;
+    p.bands.resize((size_t)9 * nb);
+    for (int k = 0; k < 3 * nb; ++k) {
+        p.bands[3 * k] = qidx[k];
+        p.bands[3 * k + 1] = skip[k];
+        p.bands[3 * k + 2] = bits[k];
+    }
+    dgpu_picture_info& I = p.info;
+    I.filter = filter;
+    I.cpd_scale = cpd_scale;
+    for (int c = 0; c < 3; ++c) I.lambda[c] = lam[c];
+    return DGPU_OK;
+}
+
+// A coded picture no later picture can reference: references reach back at most
+// 2 * L1 separation pictures from the earliest picture not yet coded.
+bool releasable(const Encoder& E, const Pic& p) {
+    if (!p.coded) return false;
+    int first_uncoded = E.last_read + 1;
+    for (const auto& kv : E.pics)
+        if (!kv.second.coded) {
+            first_uncoded = kv.first;
+            break;
+        }
+    return p.pnum < first_uncoded - 2 * std::max(E.L1Sep, 1);
+}
+
+int take_slot(Encoder& E) {
+    for (size_t k = 0; k < E.slots.size(); ++k)
+        if (E.slots[k].pnum < 0) return (int)k;
+    for (auto it = E.pics.begin(); it != E.pics.end(); ++it) {
+        if (releasable(E, it->second)) {
+            const int k = it->second.slot;
+            E.slots[k].pnum = -1;
+            E.pics.erase(it);
+            return k;
+        }
+    }
+    return -1;
+}
+
+}  // namespace
+}  // namespace dgpu
+
+using namespace dgpu;
+
+extern "C" int dgpu_encoder_create(const dgpu_encoder_params* params, int max_pictures, void* stream, void** out) {
+    if (!params || !out) return DGPU_ERR_ARG;
+    *out = nullptr;
+    const dgpu_encoder_params& P = *params;
+    if (P.cformat < 0 || P.cformat > 2 || P.width < 16 || P.height < 16 || P.luma_depth < 8 || P.luma_depth > 14 ||
+        P.chroma_depth < 8 || P.chroma_depth > 14 || P.num_l1 < 0 || (P.num_l1 > 0 && P.l1_sep < 1) ||
+        P.mv_precision < 1 || P.mv_precision > 3 || P.wlt_depth < 1 || P.wlt_depth > 6 || P.intra_filter < 0 ||
+        P.intra_filter > 6 || P.inter_filter < 0 || P.inter_filter > 6 || P.xbsep < 1 || P.ybsep < 1 ||
+        P.xblen < P.xbsep || P.yblen < P.ybsep)
+        return DGPU_ERR_ARG;
+    Encoder* E = new (std::nothrow) Encoder();
+    if (!E) return DGPU_ERR_NOMEM;
+    E->P = P;
+    E->st = as_stream(stream);
+    E->L = calc_lambdas(P.qf);
+    E->xs = P.cformat == 0 ? 0 : 1;
+    E->ys = P.cformat == 2 ? 1 : 0;
+    E->w[0] = P.width;
+    E->h[0] = P.height;
+    E->w[1] = E->w[2] = P.width >> E->xs;
+    E->h[1] = E->h[2] = P.height >> E->ys;
+    const int mul = 1 << P.wlt_depth;
+    for (int c = 0; c < 3; ++c) {
+        E->pw[c] = (E->w[c] + mul - 1) / mul * mul;
+        E->ph[c] = (E->h[c] + mul - 1) / mul * mul;
+    }
+    // SequenceCompressor::SetMotionParameters (seq_compress.cpp:104-133)
+    E->bp.precision = P.mv_precision;
+    E->bp.xblen = P.xblen;
+    E->bp.yblen = P.yblen;
+    E->bp.xbsep = P.xbsep;
+    E->bp.ybsep = P.ybsep;
+    E->bp.xnum_sb = (P.width + 4 * P.xbsep - 1) / (4 * P.xbsep);
+    E->bp.ynum_sb = (P.height + 4 * P.ybsep - 1) / (4 * P.ybsep);
+    E->nsb = E->bp.xnum_sb * E->bp.ynum_sb;
+    E->nblocks = 16 * E->nsb;
+    E->nb = 3 * P.wlt_depth + 1;
+    E->ncb.assign((size_t)2 * E->nb, 0);
+    int rc = dgpu_code_blocks(P.wlt_depth, P.width, P.height, 1, E->ncb.data());
+    if (rc) {
+        delete E;
+        return rc;
+    }
+    for (int b = 0; b < E->nb; ++b) E->ncb_total += E->ncb[2 * b] * E->ncb[2 * b + 1];
+    // GOP (dirac_encoder.cpp:562-572, common.cpp:512-518)
+    E->num_L1 = P.num_l1;
+    E->L1Sep = P.num_l1 > 0 ? P.l1_sep : 0;
+    E->gop_len = P.num_l1 > 0 ? (P.num_l1 + 1) * P.l1_sep : 10;
+    E->m_L1_sep = E->L1Sep;
+    const int min_slots = 4 * std::max(E->L1Sep, 1) + 8;
+    const int nslots = std::max(max_pictures, min_slots);
+
+    // ---- sizes ----
+    size_t plane16 = 0, plane32 = 0, up16 = 0;
+    for (int c = 0; c < 3; ++c) {
+        plane16 += align_up((size_t)E->w[c] * E->h[c] * 2, 256);
+        plane32 += align_up((size_t)E->pw[c] * E->ph[c] * 4, 256);
+        up16 += align_up((size_t)4 * E->w[c] * E->h[c] * 2, 256);
+    }
+    const size_t me_out = align_up((size_t)E->nblocks * 2 * 2 * 2, 256) + align_up((size_t)E->nblocks * 2 * 3 * 4, 256) +
+                          align_up(E->nblocks, 256) + align_up((size_t)E->nblocks * 3 * 2, 256) +
+                          align_up(E->nsb, 256) + align_up((size_t)E->nsb * 4, 256);
+    const size_t slot_bytes = 2 * plane16 + 2 * plane32 + up16 + me_out;
+    E->me_max_tasks = std::min(nslots, 64);
+    {
+        std::vector<int> r2(E->me_max_tasks, 0);
+        const int npics_max = std::min(nslots, 3 * E->me_max_tasks);
+        E->me_ws_bytes = dgpu_me_batch_workspace_bytes(P.cformat, P.width, P.height, &E->bp, npics_max,
+                                                       E->me_max_tasks, r2.data(), 3);
+        if (E->me_ws_bytes == 0) {
+            delete E;
+            return DGPU_ERR_ARG;
+        }
+    }
+    for (int c = 0; c < 3; ++c) E->dwt_ws_bytes += align_up(dgpu_dwt_scratch_bytes(E->pw[c], E->ph[c], P.wlt_depth), 256);
+    {
+        int intra[3] = {1, 1, 1}, dep[3] = {P.wlt_depth, P.wlt_depth, P.wlt_depth};
+        std::vector<int> ncb3(6 * E->nb);
+        for (int c = 0; c < 3; ++c) std::memcpy(&ncb3[2 * c * E->nb], E->ncb.data(), sizeof(int) * 2 * E->nb);
+        E->q_ws_bytes = dgpu_code_residue_workspace_bytes(3, intra, dep, E->pw, E->ph, ncb3.data());
+        if (E->q_ws_bytes == 0) {
+            delete E;
+            return DGPU_ERR_ARG;
+        }
+    }
+    for (int c = 0; c < 3; ++c) E->stage_bytes += align_up((size_t)E->w[c] * E->h[c] * 2, 256);
+    const size_t total = (size_t)nslots * align_up(slot_bytes, 256) + align_up(E->me_ws_bytes, 256) +
+                         align_up(E->dwt_ws_bytes, 256) + align_up(E->q_ws_bytes, 256) +
+                         align_up(sizeof(int) * E->me_max_tasks, 256) + E->stage_bytes;
+    if (cudaMalloc(&E->arena, total) != cudaSuccess) {
+        cudaGetLastError();
+        E->arena = nullptr;
+        delete E;
+        return DGPU_ERR_NOMEM;
+    }
+    if (cudaMallocHost(&E->h_counts, sizeof(int) * E->me_max_tasks) != cudaSuccess) {
+        cudaGetLastError();
+        E->h_counts = nullptr;
+        delete E;
+        return DGPU_ERR_NOMEM;
+    }
+    char* q = static_cast<char*>(E->arena);
+    auto take = [&](size_t bytes) {
+        char* r = q;
+        q += align_up(bytes, 256);
+        return r;
+    };
+    E->slots.resize(nslots);
+    for (int k = 0; k < nslots; ++k) {
+        Slot& s = E->slots[k];
+        for (int c = 0; c < 3; ++c) s.orig[c] = reinterpret_cast<int16_t*>(take((size_t)E->w[c] * E->h[c] * 2));
+        for (int c = 0; c < 3; ++c) s.data[c] = reinterpret_cast<int16_t*>(take((size_t)E->w[c] * E->h[c] * 2));
+        for (int c = 0; c < 3; ++c) s.coeff[c] = reinterpret_cast<int32_t*>(take((size_t)E->pw[c] * E->ph[c] * 4));
+        for (int c = 0; c < 3; ++c) s.qout[c] = reinterpret_cast<int32_t*>(take((size_t)E->pw[c] * E->ph[c] * 4));
+        for (int c = 0; c < 3; ++c) s.up[c] = reinterpret_cast<int16_t*>(take((size_t)4 * E->w[c] * E->h[c] * 2));
+        s.mv = reinterpret_cast<int16_t*>(take((size_t)E->nblocks * 2 * 2 * 2));
+        s.cost = reinterpret_cast<float*>(take((size_t)E->nblocks * 2 * 3 * 4));
+        s.mode = reinterpret_cast<uint8_t*>(take(E->nblocks));
+        s.dc = reinterpret_cast<int16_t*>(take((size_t)E->nblocks * 3 * 2));
+        s.split = reinterpret_cast<uint8_t*>(take(E->nsb));
+        s.sbcost = reinterpret_cast<float*>(take((size_t)E->nsb * 4));
+        q = static_cast<char*>(E->arena) + (size_t)(k + 1) * align_up(slot_bytes, 256);
+    }
+    E->me_ws = take(E->me_ws_bytes);
+    E->dwt_ws = take(E->dwt_ws_bytes);
+    E->q_ws = take(E->q_ws_bytes);
+    E->d_counts = reinterpret_cast<int*>(take(sizeof(int) * E->me_max_tasks));
+    E->stage = take(E->stage_bytes);
+    *out = E;
+    return DGPU_OK;
+}
+
+extern "C" int dgpu_encoder_destroy(void* enc) {
+    Encoder* E = static_cast<Encoder*>(enc);
+    if (!E) return DGPU_ERR_ARG;
+    cudaStreamSynchronize(E->st);
+    delete E;
+    return DGPU_OK;
+}
+
+extern "C" int dgpu_encoder_load(void* enc, const void* const* planes, int on_host) {
+    Encoder* E = static_cast<Encoder*>(enc);
+    if (!E || !planes || !planes[0] || !planes[1] || !planes[2]) return DGPU_ERR_ARG;
+    if (E->eos) return DGPU_ERR_ARG;
+    const int k = take_slot(*E);
+    if (k < 0) return DGPU_ERR_SIZE;
+    Slot& s = E->slots[k];
+    const size_t sb = sample_bytes(*E);
+    Planes3 P3{};
+    size_t off = 0;
+    for (int c = 0; c < 3; ++c) {
+        const size_t bytes = (size_t)E->w[c] * E->h[c] * sb;
+        if (on_host) {
+            void* dst = static_cast<char*>(E->stage) + off;
+            DGPU_CHECK_CUDA(cudaMemcpyAsync(dst, planes[c], bytes, cudaMemcpyHostToDevice, E->st));
+            P3.src[c] = dst;
+            off += align_up(bytes, 256);
+        } else {
+            P3.src[c] = planes[c];
+        }
+        P3.orig[c] = s.orig[c];
+        P3.data[c] = s.data[c];
+        P3.n[c] = E->w[c] * E->h[c];
+    }
+    dim3 grid(std::min((E->w[0] * E->h[0] + 255) / 256, 148 * 8), 3);
+    const int offl = 1 << (E->P.luma_depth - 1), offc = 1 << (E->P.chroma_depth - 1);
+    if (sb == 1)
+        load_kernel<uint8_t><<<grid, 256, 0, E->st>>>(P3, offl, offc);
+    else
+        load_kernel<uint16_t><<<grid, 256, 0, E->st>>>(P3, offl, offc);
+    DGPU_CHECK_LAUNCH();
+    const int pnum = ++E->last_read;
+    s.pnum = pnum;
+    Pic& p = E->pics[pnum];
+    p = Pic();
+    p.pnum = pnum;
+    p.slot = k;
+    return DGPU_OK;
+}
+
+extern "C" int dgpu_encoder_end_sequence(void* enc) {
+    Encoder* E = static_cast<Encoder*>(enc);
+    if (!E) return DGPU_ERR_ARG;
+    E->eos = true;
+    return DGPU_OK;
+}
+
+extern "C" int dgpu_encoder_code_next(void* enc, const float* ecf, dgpu_picture_info* info) {
+    Encoder* E = static_cast<Encoder*>(enc);
+    if (!E) return DGPU_ERR_ARG;
+    if (E->last_read < 0) return 0;
+    // a scheduled return to the normal L1 separation (seq_compress.cpp:215-219)
+    if (E->L1Sep > 0 && E->L1Sep != E->m_L1_sep && (E->code - 1) % E->L1Sep == 0) E->m_L1_sep = E->L1Sep;
+    E->cur = coded_to_display(*E, E->code);
+    if (!can_encode(*E)) return 0;
+    if (!E->pics.count(E->cur) || E->pics[E->cur].coded) return 0;
+    // 1. picture types one sub-group ahead
+    for (auto& kv : E->pics) {
+        Pic& q = kv.second;
+        if (!q.typed && !q.coded && (E->num_L1 == 0 || q.pnum < E->cur + E->L1Sep)) set_type(*E, q);
+    }
+    Pic* p = &E->pics[E->cur];
+    int rc;
+    if (!p->intra) {
+        // 8.-11. estimation, intra analysis, switch to P-only sub-groups
+        for (;;) {
+            rc = ensure_me(*E, *p);
+            if (rc) return rc;
+            if (E->m_L1_sep > 1 && p->ratio > 0.25 && E->cur % E->L1Sep == 0) {
+                E->m_L1_sep = 1;
+                for (int i = 0; i < E->L1Sep; ++i) {
+                    auto it = E->pics.find(E->cur - i);
+                    if (it == E->pics.end()) return DGPU_ERR_ARG;
+                    set_type(*E, it->second);
+                }
+                p->me_valid = false;
+                E->cur = coded_to_display(*E, E->code);
+                p = &E->pics[E->cur];
+                continue;
+            }
+            break;
+        }
+        // cut detection
+        if (p->ratio > 0.3333) {
+            p->cut = true;
+            if (E->L1Sep > 1 && E->cur % E->L1Sep == 0) E->gop_start = p->pnum;
+            p->intra = true;
+        } else {
+            rc = motion_compensate(*E, *p, DGPU_SUBTRACT, false);
+            if (rc) return rc;
+        }
+    }
+    // 16.-19. transform, quantisation, inverse transform
+    rc = code_residue(*E, *p, ecf);
+    if (rc) return rc;
+    // 20.-21. reconstruction and clip
+    if (!p->intra) {
+        rc = motion_compensate(*E, *p, DGPU_ADD, true);
+        if (rc) return rc;
+    } else {
+        Slot& s = slot_of(*E, *p);
+        for (int c = 0; c < 3; ++c) {
+            rc = dgpu_clip(s.data[c], E->w[c], E->h[c], E->w[c], comp_depth(*E, c), E->st);
+            if (rc) return rc;
+        }
+    }
+    p->up_valid = false;
+    p->coded = true;
+    dgpu_picture_info& I = p->info;
+    I.pnum = p->pnum;
+    I.coded_num = E->code;
+    I.intra = p->intra ? 1 : 0;
+    I.is_ref = p->is_ref ? 1 : 0;
+    I.cut = p->cut ? 1 : 0;
+    I.num_refs = (int)p->refs.size();
+    I.ref1 = p->refs.size() > 0 ? p->refs[0] : -1;
+    I.ref2 = p->refs.size() > 1 ? p->refs[1] : -1;
+    I.is_b = p->is_b() ? 1 : 0;
+    I.intra_ratio = p->ratio;
+    if (info) *info = I;
+    ++E->code;
+    return 1;
+}
+
+extern "C" size_t dgpu_encoder_item_bytes(void* enc, int pnum, int what, int comp) {
+    Encoder* E = static_cast<Encoder*>(enc);
+    if (!E || comp < 0 || comp > 2) return 0;
+    auto it = E->pics.find(pnum);
+    if (it == E->pics.end() || !it->second.coded) return 0;
+    const Pic& p = it->second;
+    const bool inter = !p.intra || p.cut;
+    switch (what) {
+        case DGPU_ENC_RECON: return (size_t)E->w[comp] * E->h[comp] * 2;
+        case DGPU_ENC_COEFF:
+        case DGPU_ENC_QINDEX: return (size_t)E->pw[comp] * E->ph[comp] * 4;
+        case DGPU_ENC_MV: return inter ? (size_t)p.refs.size() * E->nblocks * 4 : 0;
+        case DGPU_ENC_MODE: return inter ? (size_t)E->nblocks : 0;
+        case DGPU_ENC_DC: return inter ? (size_t)3 * E->nblocks * 2 : 0;
+        case DGPU_ENC_SPLIT: return inter ? (size_t)E->nsb : 0;
+        case DGPU_ENC_BANDS: return (size_t)E->nb * 3 * sizeof(int);
+        case DGPU_ENC_CBSKIP: return (size_t)E->ncb_total;
+        case DGPU_ENC_OUTPUT: return (size_t)E->w[comp] * E->h[comp] * sample_bytes(*E);
+        default: return 0;
+    }
+}
+
+extern "C" int dgpu_encoder_read(void* enc, int pnum, int what, int comp, void* dst, size_t bytes, int on_host) {
+    Encoder* E = static_cast<Encoder*>(enc);
+    if (!E || !dst) return DGPU_ERR_ARG;
+    const size_t need = dgpu_encoder_item_bytes(enc, pnum, what, comp);
+    if (need == 0 || bytes != need) return DGPU_ERR_ARG;
+    const Pic& p = E->pics[pnum];
+    const Slot& s = E->slots[p.slot];
+    if (what == DGPU_ENC_BANDS || what == DGPU_ENC_CBSKIP) {
+        const void* src = what == DGPU_ENC_BANDS ? (const void*)&p.bands[(size_t)comp * E->nb * 3]
+                                                 : (const void*)&p.cb_skip[(size_t)comp * E->ncb_total];
+        if (on_host) {
+            std::memcpy(dst, src, bytes);
+            return DGPU_OK;
+        }
+        DGPU_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, E->st));
+        DGPU_CHECK_CUDA(cudaStreamSynchronize(E->st));
+        return DGPU_OK;
+    }
+    const void* src = nullptr;
+    if (what == DGPU_ENC_OUTPUT) {
+        const int n = E->w[comp] * E->h[comp];
+        const int off = 1 << (comp_depth(*E, comp) - 1);
+        void* out = on_host ? E->stage : dst;
+        const int grid = std::min((n + 255) / 256, 148 * 8);
+        if (sample_bytes(*E) == 1)
+            output_kernel<uint8_t><<<grid, 256, 0, E->st>>>(s.data[comp], n, off, static_cast<uint8_t*>(out));
+        else
+            output_kernel<uint16_t><<<grid, 256, 0, E->st>>>(s.data[comp], n, off, static_cast<uint16_t*>(out));
+        DGPU_CHECK_LAUNCH();
+        if (!on_host) return DGPU_OK;
+        src = E->stage;
+    } else {
+        switch (what) {
+            case DGPU_ENC_RECON: src = s.data[comp]; break;
+            case DGPU_ENC_COEFF: src = s.coeff[comp]; break;
+            case DGPU_ENC_QINDEX: src = s.qout[comp]; break;
+            case DGPU_ENC_MV: src = s.mv; break;
+            case DGPU_ENC_MODE: src = s.mode; break;
+            case DGPU_ENC_DC: src = s.dc; break;
+            case DGPU_ENC_SPLIT: src = s.split; break;
+            default: return DGPU_ERR_ARG;
+        }
+    }
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, E->st));
+    if (on_host) DGPU_CHECK_CUDA(cudaStreamSynchronize(E->st));
+    return DGPU_OK;
+}

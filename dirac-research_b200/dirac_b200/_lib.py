@@ -97,6 +97,13 @@ SIGNATURES = {
         [c_int, P_int, P_int, P_void, P_int, P_int, c_void_p, c_void_p, c_void_p, P_int, P_int, P_int, P_int,
          c_void_p, P_void, c_void_p, c_size_t, c_void_p],
     ),
+    "dgpu_encoder_create": (c_int, [c_void_p, c_int, c_void_p, P_void]),
+    "dgpu_encoder_destroy": (c_int, [c_void_p]),
+    "dgpu_encoder_load": (c_int, [c_void_p, P_void, c_int]),
+    "dgpu_encoder_end_sequence": (c_int, [c_void_p]),
+    "dgpu_encoder_code_next": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "dgpu_encoder_item_bytes": (c_size_t, [c_void_p, c_int, c_int, c_int]),
+    "dgpu_encoder_read": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_size_t, c_int]),
 }
 
 

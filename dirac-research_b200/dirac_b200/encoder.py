@@ -1,0 +1,128 @@
+"""Host-side mirror of the reference's sequence coding loop over the library's device encoder.
+
+``SequenceEncoder`` wraps the dgpu_encoder_* entry points: pictures are loaded in display
+order (dirac_encoder_load, libdirac_encoder/dirac_encoder.cpp:1067-1087), coded one at a time
+in coding order (SequenceCompressor::CompressNextPicture, seq_compress.cpp:194-499) and their
+results read back per picture.  The arithmetic coder is not part of this path: the caller
+supplies entropy-correction factors per picture, or the encoder keeps the initial ones.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+
+RECON, COEFF, QINDEX, MV, MODE, DC, SPLIT, BANDS, CBSKIP, OUTPUT = range(10)
+
+
+class EncoderParams(ctypes.Structure):
+    """dgpu_encoder_params (include/dirac_gpu.h)."""
+
+    _fields_ = [("cformat", ctypes.c_int), ("width", ctypes.c_int), ("height", ctypes.c_int),
+                ("luma_depth", ctypes.c_int), ("chroma_depth", ctypes.c_int), ("qf", ctypes.c_float),
+                ("l1_sep", ctypes.c_int), ("num_l1", ctypes.c_int), ("cpd", ctypes.c_float),
+                ("xblen", ctypes.c_int), ("yblen", ctypes.c_int), ("xbsep", ctypes.c_int), ("ybsep", ctypes.c_int),
+                ("mv_precision", ctypes.c_int), ("intra_filter", ctypes.c_int), ("inter_filter", ctypes.c_int),
+                ("wlt_depth", ctypes.c_int)]
+
+
+class PictureInfo(ctypes.Structure):
+    """dgpu_picture_info (include/dirac_gpu.h)."""
+
+    _fields_ = [("pnum", ctypes.c_int), ("coded_num", ctypes.c_int), ("intra", ctypes.c_int),
+                ("is_ref", ctypes.c_int), ("cut", ctypes.c_int), ("num_refs", ctypes.c_int), ("ref1", ctypes.c_int),
+                ("ref2", ctypes.c_int), ("is_b", ctypes.c_int), ("filter", ctypes.c_int),
+                ("intra_ratio", ctypes.c_double), ("cpd_scale", ctypes.c_double), ("lambda_", ctypes.c_float * 3)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "lambda_"}
+        d["lambda"] = list(self.lambda_)
+        return d
+
+
+_DTYPES = {RECON: np.int16, COEFF: np.int32, QINDEX: np.int32, MV: np.int16, MODE: np.uint8, DC: np.int16,
+           SPLIT: np.uint8, BANDS: np.int32, CBSKIP: np.uint8}
+
+
+class SequenceEncoder:
+    """One coded sequence on one CUDA stream.
+
+    params: dict with the EncoderParams fields (cformat, width, height, luma_depth,
+    chroma_depth, qf, l1_sep, num_l1, cpd, xblen, yblen, xbsep, ybsep, mv_precision,
+    intra_filter, inter_filter, wlt_depth).  max_pictures: device picture slots."""
+
+    def __init__(self, params, max_pictures=32, stream=None):
+        self.lib = _lib.load()
+        self.params = EncoderParams(**params)
+        self.stream = stream if stream is not None else torch.cuda.current_stream()
+        self.handle = ctypes.c_void_p()
+        _lib.check(self.lib.dgpu_encoder_create(ctypes.byref(self.params), max_pictures, self.stream.cuda_stream,
+                                                ctypes.byref(self.handle)), "dgpu_encoder_create")
+        p = self.params
+        self.depth8 = p.luma_depth <= 8 and p.chroma_depth <= 8
+        xs = 0 if p.cformat == 0 else 1
+        ys = 1 if p.cformat == 2 else 0
+        self.shapes = [(p.height, p.width), (p.height >> ys, p.width >> xs), (p.height >> ys, p.width >> xs)]
+
+    def close(self):
+        if self.handle:
+            self.lib.dgpu_encoder_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load(self, planes):
+        """planes: three unsigned sample planes (numpy arrays in host memory, or CUDA tensors)."""
+        on_host = not isinstance(planes[0], torch.Tensor)
+        if on_host:
+            dt = np.uint8 if self.depth8 else np.uint16
+            arrs = [np.ascontiguousarray(a, dtype=dt) for a in planes]
+            ptrs = [a.ctypes.data for a in arrs]
+        else:
+            ptrs = [t.data_ptr() for t in planes]
+        _lib.check(self.lib.dgpu_encoder_load(self.handle, _lib.ptr_array(ptrs), int(on_host)), "dgpu_encoder_load")
+
+    def end_sequence(self):
+        _lib.check(self.lib.dgpu_encoder_end_sequence(self.handle), "dgpu_encoder_end_sequence")
+
+    def code_next(self, ecf=None):
+        """Codes the next picture in coding order; returns its info dict, or None."""
+        info = PictureInfo()
+        e = None
+        if ecf is not None:
+            e = np.ascontiguousarray(ecf, dtype=np.float32)
+        rc = self.lib.dgpu_encoder_code_next(self.handle, e.ctypes.data if e is not None else None, ctypes.byref(info))
+        if rc < 0:
+            _lib.check(rc, "dgpu_encoder_code_next")
+        return info.as_dict() if rc == 1 else None
+
+    def read(self, pnum, what, comp=0):
+        """One result of a coded picture as a numpy array."""
+        n = self.lib.dgpu_encoder_item_bytes(self.handle, pnum, what, comp)
+        if n == 0:
+            return None
+        if what == OUTPUT:
+            dt = np.uint8 if self.depth8 else np.uint16
+        else:
+            dt = _DTYPES[what]
+        out = np.empty(n // np.dtype(dt).itemsize, dt)
+        _lib.check(self.lib.dgpu_encoder_read(self.handle, pnum, what, comp, out.ctypes.data, n, 1), "dgpu_encoder_read")
+        return out
+
+    def encode(self, frames):
+        """Loads every frame, ends the sequence and codes all pictures; returns the infos in
+        coding order."""
+        for f in frames:
+            self.load(f)
+        self.end_sequence()
+        infos = []
+        while True:
+            i = self.code_next()
+            if i is None:
+                return infos
+            infos.append(i)

@@ -264,6 +264,84 @@ int dgpu_code_residue_batch(int n, const int* intra, const int* depth, int32_t* 
                             int* band_bits, uint8_t* cb_skip, int32_t* const* qout, void* workspace,
                             size_t ws_bytes, void* stream);
 
+/* ---------------------------------------------------------------------------------------
+ * Sequence encoder: the data-parallel part of the reference's frame-coding loop
+ * SequenceCompressor::CompressNextPicture (libdirac_encoder/seq_compress.cpp:194-499) with
+ * FrameSequenceCompressor's GOP structure (seq_compress.cpp:151-192, 563-686) and the
+ * PictureCompressor steps it drives (picture_compress.cpp:76-580): motion estimation on
+ * the original pictures, intra-block analysis, P-only sub-group switch and cut detection,
+ * motion compensation against the reconstructed references, forward transform, quantiser
+ * choice and quantisation, inverse transform, reconstruction and clipping.  Everything stays
+ * resident on the device; the host keeps the GOP state machine and the lambdas.
+ *
+ * What stays with the caller (serial host code in the reference): the arithmetic coding of
+ * the coefficients and motion data, and therefore the adaptation of the entropy-correction
+ * factors (EntropyCorrector::Update, common.cpp:134-151), which dgpu_encoder_code_next
+ * takes as an input (NULL: the initial factors of EntropyCorrector::Init,
+ * common.cpp:79-131).  Not supported: rate control (trate), prefilters, field coding,
+ * lossless coding, num_l1 < 0.
+ *
+ * Use: dgpu_encoder_create; dgpu_encoder_load for each picture in display order;
+ * dgpu_encoder_code_next until it returns 0 (it needs the same look-ahead as the reference:
+ * 2 * l1_sep pictures, or dgpu_encoder_end_sequence); dgpu_encoder_read for results.  A
+ * picture's results stay readable until its slot is reused by a later load (never, when
+ * max_pictures >= the sequence length).  A handle is not thread-safe; different handles
+ * may run on different streams concurrently.
+ * ------------------------------------------------------------------------------------- */
+typedef struct {
+    int cformat;                  /* ChromaFormat: 0 4:4:4, 1 4:2:2, 2 4:2:0 */
+    int width, height;            /* luma picture size */
+    int luma_depth, chroma_depth; /* bits per sample, 8..14 */
+    float qf;                     /* quality factor (EncoderParams::Qf) */
+    int l1_sep, num_l1;           /* GOP: L1 separation and L1 pictures per GOP (0: I only) */
+    float cpd;                    /* perceptual weighting, cycles per degree */
+    int xblen, yblen, xbsep, ybsep; /* luma OBMC block length and separation */
+    int mv_precision;             /* 1 half, 2 quarter, 3 eighth pel */
+    int intra_filter, inter_filter, wlt_depth; /* WltFilter numbering, transform depth */
+} dgpu_encoder_params;
+
+typedef struct {
+    int pnum;         /* picture (display) number */
+    int coded_num;    /* position in coding order */
+    int intra;        /* 1: coded intra (I picture or a detected cut) */
+    int is_ref;       /* 1: reference picture */
+    int cut;          /* 1: an inter picture re-coded as intra by cut detection */
+    int num_refs, ref1, ref2;  /* references (-1 when absent) */
+    int is_b;         /* PictureParams::IsBPicture */
+    int filter;       /* transform filter used */
+    double intra_ratio;   /* MEData::IntraBlockRatio (inter pictures) */
+    double cpd_scale;     /* perceptual-weight scale used for the band weights */
+    float lambda[3];      /* quantiser lambdas (PictureCompressor::GetCompLambda) */
+} dgpu_picture_info;
+
+/* dgpu_encoder_read items; comp selects the component where it applies */
+#define DGPU_ENC_RECON 0    /* int16 [h][w] reconstructed component (codec samples) */
+#define DGPU_ENC_COEFF 1    /* int32 [ch][cw] reconstructed coefficients (padded size) */
+#define DGPU_ENC_QINDEX 2   /* int32 [ch][cw] signed quantised indices */
+#define DGPU_ENC_MV 3       /* int16 [num_refs][blocks][2] motion vectors */
+#define DGPU_ENC_MODE 4     /* uint8 [blocks] prediction modes (0 intra, 1 ref1, 2 ref2, 3 bi) */
+#define DGPU_ENC_DC 5       /* int16 [3][blocks] intra-block DC values */
+#define DGPU_ENC_SPLIT 6    /* uint8 [superblocks] superblock splitting levels */
+#define DGPU_ENC_BANDS 7    /* int32 [3*depth+1][3] per band: quantiser index, skip, estimated bits */
+#define DGPU_ENC_CBSKIP 8   /* uint8 code-block skip flags of all bands, band-list order */
+#define DGPU_ENC_OUTPUT 9   /* uint8 (depth 8) / uint16 [h][w] output samples: recon + 2^(d-1) */
+
+int dgpu_encoder_create(const dgpu_encoder_params* params, int max_pictures, void* stream, void** encoder);
+int dgpu_encoder_destroy(void* encoder);
+/* Loads the next picture in display order: three dense planes of unsigned samples (uint8 for
+ * depth 8, uint16 otherwise), in host memory (on_host = 1) or device memory (0). */
+int dgpu_encoder_load(void* encoder, const void* const* planes, int on_host);
+int dgpu_encoder_end_sequence(void* encoder);
+/* Codes the next picture in coding order.  ecf: NULL, or [3][3*depth+1] entropy-correction
+ * factors for this picture (the caller's EntropyCorrector::Factor values).  Returns 1 and
+ * fills info when a picture was coded, 0 when more input (or nothing) remains. */
+int dgpu_encoder_code_next(void* encoder, const float* ecf, dgpu_picture_info* info);
+size_t dgpu_encoder_item_bytes(void* encoder, int pnum, int what, int comp);
+/* Copies one result of a coded picture to dst (host memory when on_host = 1, else device);
+ * bytes must equal dgpu_encoder_item_bytes.  Synchronises the encoder's stream for host
+ * copies. */
+int dgpu_encoder_read(void* encoder, int pnum, int what, int comp, void* dst, size_t bytes, int on_host);
+
 #ifdef __cplusplus
 }
 #endif

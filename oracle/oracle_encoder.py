@@ -13,6 +13,8 @@ and the bitstream are not part of it.
 Band weights and code-block counts come from the library's host helpers, which the oracle
 tests pin separately against the reference's own values.
 """
+import ctypes
+import ctypes.util
 import math
 
 import numpy as np
@@ -32,12 +34,24 @@ def f32(x):
     return float(np.float32(x))
 
 
+_libm = ctypes.CDLL(ctypes.util.find_library("m"))
+_libm.log10f.restype = ctypes.c_float
+_libm.log10f.argtypes = [ctypes.c_float]
+_libm.sqrtf.restype = ctypes.c_float
+_libm.sqrtf.argtypes = [ctypes.c_float]
+
+
+def log10f(x):
+    """std::log10 of a float argument: the C library's single-precision log10."""
+    return float(_libm.log10f(x))
+
+
 def lambdas(qf):
     """EncoderParams::CalcLambdas with its float members."""
     i = f32(math.pow(10.0, (12.0 - f32(qf)) / 2.5) / 16.0)
     l1 = f32(i * 4.0)
     l2 = f32(i * 32.0)
-    me = f32(math.sqrt(l1) * 2.0)
+    me = f32(float(_libm.sqrtf(l1)) * 2.0)  # std::sqrt of a float member
     return i, l1, l2, me
 
 
@@ -75,8 +89,9 @@ class OracleEncoder:
     """cfg keys: cformat, width, height, luma_depth, chroma_depth, qf, l1_sep, num_l1, cpd,
     xblen, yblen, xbsep, ybsep, mv_precision, intra_filter, inter_filter, wlt_depth."""
 
-    def __init__(self, cfg, weights_fn, blocks_fn, oracle=None):
+    def __init__(self, cfg, weights_fn, blocks_fn, oracle=None, ecf_fn=None):
         self.cfg = dict(cfg)
+        self.ecf_fn = ecf_fn
         self.orc = oracle or Oracle()
         self.weights_fn = weights_fn
         self.blocks_fn = blocks_fn
@@ -224,7 +239,8 @@ class OracleEncoder:
         else:
             ir = f32(p.ratio)
             lp = self.lam_l2 if p.is_b() else self.lam_l1
-            lam = f32(math.pow(10.0, 3.0 * ir * math.log10(self.lam_i) + (1.0 - 3.0 * ir) * math.log10(lp)))
+            # std::log10 of the float lambdas is the single-precision log10; pow is double
+            lam = f32(math.pow(10.0, 3.0 * ir * log10f(self.lam_i) + (1.0 - 3.0 * ir) * log10f(lp)))
         if comp == 1:
             lam = f32(np.float32(lam) * np.float32(1.5))
         elif comp == 2:
@@ -241,7 +257,7 @@ class OracleEncoder:
             ir = f32(p.ratio)
             cpd_scale = max(0.125, min(1.2, 5.0 * ir * 1.0 + (1.0 - 5.0 * ir) * 0.125))
         ncb = self.blocks_fn(depth, c["width"], c["height"])
-        ecf = initial_ecf(depth, p.intra)
+        given = self.ecf_fn(p) if self.ecf_fn is not None else None
         res = {"coeff": [], "qidx": [], "skip": [], "bits": [], "cb_skip": [], "qindex": [], "lambda": [],
                "cpd_scale": cpd_scale, "filter": filt}
         for comp in range(3):
@@ -251,6 +267,7 @@ class OracleEncoder:
             ch, cw = coeff.shape
             wt = self.weights_fn(filt, depth, cw, ch, comp, c["cformat"], c["cpd"], cpd_scale).astype(np.float32)
             lam = self.comp_lambda(p, comp)
+            ecf = initial_ecf(depth, p.intra) if given is None else np.asarray(given[comp], np.float32)
             recon, q, sk, bits, cbs, qo = self.orc.code_residue(int(p.intra), depth, coeff, lam, wt, ecf, ncb)
             p.data[comp] = self.orc.dwt_backward(filt, depth, recon, w, h)
             for k, v in (("coeff", recon), ("qidx", q), ("skip", sk), ("bits", bits), ("cb_skip", cbs),
@@ -263,10 +280,11 @@ class OracleEncoder:
         p.result = res
 
 
-def encode_sequence(cfg, frames, weights_fn, blocks_fn, oracle=None):
+def encode_sequence(cfg, frames, weights_fn, blocks_fn, oracle=None, ecf_fn=None):
     """Encode a list of frames [(Y, U, V) int16 codec-domain planes]; returns the
-    OracleEncoder (pictures in .pics, coding order in .order)."""
-    enc = OracleEncoder(cfg, weights_fn, blocks_fn, oracle)
+    OracleEncoder (pictures in .pics, coding order in .order).  ecf_fn(pic), when given,
+    returns the [3][3*depth+1] entropy-correction factors to use for that picture."""
+    enc = OracleEncoder(cfg, weights_fn, blocks_fn, oracle, ecf_fn)
     for f in frames:
         enc.load(f)
     enc.end_sequence()
