@@ -176,9 +176,39 @@ struct Encoder {
     size_t stage_bytes = 0;
     int* h_counts = nullptr;     // pinned
 
+    // optional per-stage timing with CUDA events on the encoder's stream
+    bool profile = false;
+    cudaEvent_t ev[2 * DGPU_ENC_NSTAGES] = {};
+    double stage_ms[DGPU_ENC_NSTAGES] = {};
+    int stage_calls[DGPU_ENC_NSTAGES] = {};
+
     ~Encoder() {
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
         if (arena) cudaFree(arena);
         if (h_counts) cudaFreeHost(h_counts);
+    }
+};
+
+// Brackets one stage with events when profiling; the elapsed time is collected at the
+// stage's end (a host wait, so profiling perturbs the pipeline: use it outside timed runs).
+struct StageTimer {
+    Encoder& E;
+    int k;
+    StageTimer(Encoder& e, int stage) : E(e), k(stage) {
+        if (E.profile) cudaEventRecord(E.ev[2 * k], E.st);
+    }
+    ~StageTimer() {
+        if (!E.profile) return;
+        cudaEventRecord(E.ev[2 * k + 1], E.st);
+        if (cudaEventSynchronize(E.ev[2 * k + 1]) == cudaSuccess) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, E.ev[2 * k], E.ev[2 * k + 1]) == cudaSuccess) {
+                E.stage_ms[k] += ms;
+                E.stage_calls[k] += 1;
+            }
+        }
+        cudaGetLastError();
     }
 };
 
@@ -254,6 +284,7 @@ Slot& slot_of(Encoder& E, const Pic& p) { return E.slots[p.slot]; }
 
 int ensure_up(Encoder& E, Pic& r) {
     if (r.up_valid) return DGPU_OK;
+    StageTimer timer(E, DGPU_STAGE_UPCONVERT);
     Slot& s = slot_of(E, r);
     const int16_t* pic[3] = {s.data[0], s.data[1], s.data[2]};
     int16_t* up[3] = {s.up[0], s.up[1], s.up[2]};
@@ -285,6 +316,7 @@ bool predicted_refs(const Encoder& E, const Pic& q, std::vector<int>& refs) {
 // picture whose references are (or will most likely be) known and already loaded.
 int ensure_me(Encoder& E, Pic& p) {
     if (p.me_valid && p.me_refs == p.refs) return DGPU_OK;
+    StageTimer timer(E, DGPU_STAGE_ME);
     struct Task {
         int pnum;
         std::vector<int> refs;
@@ -377,12 +409,14 @@ int motion_compensate(Encoder& E, Pic& p, int add_or_sub, bool clip) {
         for (int c = 0; c < 3; ++c) up2[c] = E.slots[r2.slot].up[c];
     }
     int16_t* pic[3] = {s.data[0], s.data[1], s.data[2]};
+    StageTimer timer(E, add_or_sub == DGPU_SUBTRACT ? DGPU_STAGE_MC_SUBTRACT : DGPU_STAGE_MC_ADD);
     return dgpu_motion_compensate(add_or_sub, E.P.cformat, E.w[0], E.h[0], &E.bp, s.mv,
                                   two ? s.mv + 2 * E.nblocks : nullptr, s.mode, s.dc, s.split, pic, E.w, up1,
                                   two ? up2 : nullptr, clip ? E.P.luma_depth : 0, clip ? E.P.chroma_depth : 0, E.st);
 }
 
 int transform(Encoder& E, Pic& p, int dir, int filter) {
+    StageTimer timer(E, dir == DGPU_FORWARD ? DGPU_STAGE_DWT_FORWARD : DGPU_STAGE_DWT_INVERSE);
     Slot& s = slot_of(E, p);
     int filt[3] = {filter, filter, filter};
     int depth[3] = {E.P.wlt_depth, E.P.wlt_depth, E.P.wlt_depth};
@@ -454,9 +488,12 @@ int code_residue(Encoder& E, Pic& p, const float* ecf_in) {
     int32_t* qout[3] = {s.qout[0], s.qout[1], s.qout[2]};
     int rc = transform(E, p, DGPU_FORWARD, filter);
     if (rc) return rc;
-    rc = dgpu_code_residue_batch(3, intra, dep, coeff, E.pw, E.ph, lam, wt.data(), ecf.data(), ncb.data(),
-                                 qidx.data(), skip.data(), bits.data(), p.cb_skip.data(), qout, E.q_ws, E.q_ws_bytes,
-                                 E.st);
+    {
+        StageTimer timer(E, DGPU_STAGE_QUANT);
+        rc = dgpu_code_residue_batch(3, intra, dep, coeff, E.pw, E.ph, lam, wt.data(), ecf.data(), ncb.data(),
+                                     qidx.data(), skip.data(), bits.data(), p.cb_skip.data(), qout, E.q_ws,
+                                     E.q_ws_bytes, E.st);
+    }
     if (rc) return rc;
     rc = transform(E, p, DGPU_BACKWARD, filter);
     if (rc) return rc;
@@ -669,6 +706,7 @@ extern "C" int dgpu_encoder_load(void* enc, const void* const* planes, int on_ho
         P3.data[c] = s.data[c];
         P3.n[c] = E->w[c] * E->h[c];
     }
+    StageTimer timer(*E, DGPU_STAGE_LOAD);
     dim3 grid(std::min((E->w[0] * E->h[0] + 255) / 256, 148 * 8), 3);
     const int offl = 1 << (E->P.luma_depth - 1), offc = 1 << (E->P.chroma_depth - 1);
     if (sb == 1)
@@ -682,6 +720,38 @@ extern "C" int dgpu_encoder_load(void* enc, const void* const* planes, int on_ho
     p = Pic();
     p.pnum = pnum;
     p.slot = k;
+    return DGPU_OK;
+}
+
+extern "C" int dgpu_encoder_reset(void* enc) {
+    Encoder* E = static_cast<Encoder*>(enc);
+    if (!E) return DGPU_ERR_ARG;
+    DGPU_CHECK_CUDA(cudaStreamSynchronize(E->st));
+    E->pics.clear();
+    for (Slot& s : E->slots) s.pnum = -1;
+    E->m_L1_sep = E->L1Sep;
+    E->gop_start = 0;
+    E->code = 0;
+    E->cur = -1;
+    E->last_read = -1;
+    E->eos = false;
+    return DGPU_OK;
+}
+
+extern "C" int dgpu_encoder_profile(void* enc, int enable, double* stage_ms, int* stage_calls) {
+    Encoder* E = static_cast<Encoder*>(enc);
+    if (!E) return DGPU_ERR_ARG;
+    if (stage_ms)
+        for (int k = 0; k < DGPU_ENC_NSTAGES; ++k) stage_ms[k] = E->stage_ms[k];
+    if (stage_calls)
+        for (int k = 0; k < DGPU_ENC_NSTAGES; ++k) stage_calls[k] = E->stage_calls[k];
+    if (enable && !E->ev[0])
+        for (auto& e : E->ev) DGPU_CHECK_CUDA(cudaEventCreate(&e));
+    E->profile = enable != 0;
+    for (int k = 0; k < DGPU_ENC_NSTAGES; ++k) {
+        E->stage_ms[k] = 0.0;
+        E->stage_calls[k] = 0;
+    }
     return DGPU_OK;
 }
 
@@ -745,6 +815,7 @@ extern "C" int dgpu_encoder_code_next(void* enc, const float* ecf, dgpu_picture_
         rc = motion_compensate(*E, *p, DGPU_ADD, true);
         if (rc) return rc;
     } else {
+        StageTimer timer(*E, DGPU_STAGE_MC_ADD);
         Slot& s = slot_of(*E, *p);
         for (int c = 0; c < 3; ++c) {
             rc = dgpu_clip(s.data[c], E->w[c], E->h[c], E->w[c], comp_depth(*E, c), E->st);

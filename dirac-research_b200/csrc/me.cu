@@ -45,7 +45,6 @@ namespace {
 constexpr int WARPS_PER_CTA = 4;
 constexpr int ME_THREADS = 32 * WARPS_PER_CTA;
 constexpr long long SPIN_LIMIT = 1LL << 24;  // about 2 s of polling with __nanosleep(100)
-constexpr int MAX_ME_JOBS = 16;
 
 struct Olb {
     int xblen, yblen, xbsep, ybsep, xoff, yoff;
@@ -147,6 +146,33 @@ __device__ __forceinline__ int warp_ticket(int* counter) {
     int t = 0;
     if ((threadIdx.x & 31) == 0) t = atomicAdd(counter, 1);
     return __shfl_sync(0xffffffffu, t, 0);
+}
+
+// ---- wavefront order over many jobs -------------------------------------------------------
+// Units (x, y) of a W x H grid whose dependencies all lie on earlier "diagonals"
+// t' = x' + slope * y' < t = x + slope * y (slope 2: left and top-right neighbours, slope 1:
+// left, top-left and top).  Tickets enumerate diagonal by diagonal, and within a diagonal job
+// by job, so every job of a launch advances its wavefront at the same time and a ticket only
+// ever waits on smaller tickets.  prefix[t] = units of one job on diagonals before t.
+struct Wave {
+    const int* prefix;  // T + 1 entries
+    int T, W, slope, njobs;
+};
+
+__device__ __forceinline__ void wave_unit(const Wave& w, int u, int& j, int& x, int& y) {
+    int lo = 0, hi = w.T - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&w.prefix[mid]) * w.njobs <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    const int p0 = __ldg(&w.prefix[lo]);
+    const int c = __ldg(&w.prefix[lo + 1]) - p0;  // > 0: lo is the last diagonal starting at or before u
+    const int r = u - p0 * w.njobs;
+    j = r / c;
+    const int ex = lo - (w.W - 1);
+    y = (ex > 0 ? (ex + w.slope - 1) / w.slope : 0) + (r - j * c);
+    x = lo - w.slope * y;
 }
 
 // ---- exact sequential float sums ------------------------------------------------------------
@@ -328,29 +354,25 @@ struct PelJob {
     int* best_sad;          // zero + guide lists: best SAD (INT_MAX if the block is empty)
     short2* best_mv;
     int* flags;             // completion flags of the wavefront
-    int first;              // first global unit index of this job
 };
 
+// All jobs of a launch share one block grid (xnb x ynb = per_job units).
 struct PelLaunch {
-    int njobs, total;
+    int total, per_job;
     Olb o;
     int* ticket;
     int* err;
-    PelJob job[MAX_ME_JOBS];
+    const PelJob* jobs;     // device table
+    Wave wave;
 };
-
-__device__ __forceinline__ int find_pel_job(const PelLaunch& L, int u) {
-    int j = 0;
-    while (j + 1 < L.njobs && L.job[j + 1].first <= u) ++j;
-    return j;
-}
 
 // Parallel phase: the zero-centred and the guide-centred lists of every block.
 __global__ void __launch_bounds__(ME_THREADS) pel_lists_kernel(const __grid_constant__ PelLaunch L) {
     const int u = blockIdx.x * WARPS_PER_CTA + (threadIdx.x >> 5);
     if (u >= L.total) return;
-    const PelJob& J = L.job[find_pel_job(L, u)];
-    const int b = u - J.first;
+    const int jn = u / L.per_job;
+    const PelJob& J = L.jobs[jn];
+    const int b = u - jn * L.per_job;
     const int by = b / J.xnb, bx = b - by * J.xnb;
     const Blim bl = block_limits(L.o, J.pw, J.ph, bx, by);
     int best = INT_MAX;
@@ -391,10 +413,11 @@ __global__ void __launch_bounds__(ME_THREADS) pel_wavefront_kernel(const __grid_
     for (;;) {
         const int u = warp_ticket(L.ticket);
         if (u >= L.total) return;
-        const PelJob& J = L.job[find_pel_job(L, u)];
-        const int b = u - J.first;
-        const int by = b / J.xnb, bx = b - by * J.xnb;
+        int jn, bx, by;
+        wave_unit(L.wave, u, jn, bx, by);
+        const PelJob& J = L.jobs[jn];
         const int W = J.xnb;
+        const int b = by * W + bx;
         if (bx > 0) wait_flag(&J.flags[b - 1], L.err);
         if (by > 0) {
             wait_flag(&J.flags[b - W], L.err);
@@ -454,22 +477,16 @@ struct SubJob {
     float* cost;         // (SAD, mvcost, total) per block, in and out
     const float* lambda; // lambda map
     int* flags;
-    int first;
 };
 
 struct SubLaunch {
-    int njobs, total, prec;
+    int total, prec;
     Olb o;
     int* ticket;
     int* err;
-    SubJob job[MAX_ME_JOBS];
+    const SubJob* jobs;  // device table
+    Wave wave;
 };
-
-__device__ __forceinline__ int find_sub_job(const SubLaunch& L, int u) {
-    int j = 0;
-    while (j + 1 < L.njobs && L.job[j + 1].first <= u) ++j;
-    return j;
-}
 
 struct Cost3 {
     float SAD, mvcost, total;
@@ -494,10 +511,11 @@ __global__ void __launch_bounds__(ME_THREADS) subpel_wavefront_kernel(const __gr
     for (;;) {
         const int u = warp_ticket(L.ticket);
         if (u >= L.total) return;
-        const SubJob& J = L.job[find_sub_job(L, u)];
-        const int b = u - J.first;
-        const int by = b / J.xnb, bx = b - by * J.xnb;
+        int jn, bx, by;
+        wave_unit(L.wave, u, jn, bx, by);
+        const SubJob& J = L.jobs[jn];
         const int W = J.xnb, H = J.ynb;
+        const int b = by * W + bx;
         // neighbours in SubpelRefine::m_nshift order: left, top-left, top, top-right
         const int nsx[4] = {-1, -1, 0, 1}, nsy[4] = {0, -1, -1, -1};
         short2 nbr[4];
@@ -607,23 +625,17 @@ struct ModeJob {
     uint8_t* split;
     int xnsb, ynsb;
     int* flags;          // per superblock
-    int first;
 };
 
 struct ModeLaunch {
-    int njobs, total, nref, prec;
+    int total, nref, prec;
     Olb lb[3];
     float level_factor[3];
     int* ticket;
     int* err;
-    ModeJob job[4];
+    const ModeJob* jobs;  // device table
+    Wave wave;
 };
-
-__device__ __forceinline__ int find_mode_job(const ModeLaunch& L, int u) {
-    int j = 0;
-    while (j + 1 < L.njobs && L.job[j + 1].first <= u) ++j;
-    return j;
-}
 
 // ModeDecider::DoME: the unit's four guide vectors as candidates (BlockMatcher::FindBestMatchSubp).
 __device__ void do_me(const ModeLaunch& L, const ModeJob& J, int x, int y, int level) {
@@ -782,9 +794,10 @@ __global__ void __launch_bounds__(ME_THREADS) mode_wavefront_kernel(const __grid
     for (;;) {
         const int u = warp_ticket(L.ticket);
         if (u >= L.total) return;
-        const ModeJob& J = L.job[find_mode_job(L, u)];
-        const int s = u - J.first;
-        const int ysb = s / J.xnsb, xsb = s - ysb * J.xnsb;
+        int jn, xsb, ysb;
+        wave_unit(L.wave, u, jn, xsb, ysb);
+        const ModeJob& J = L.jobs[jn];
+        const int s = ysb * J.xnsb + xsb;
         if (xsb > 0) wait_flag(&J.flags[s - 1], L.err);
         if (ysb > 0) {
             wait_flag(&J.flags[s - J.xnsb], L.err);
@@ -810,21 +823,19 @@ struct DcJob {
     int16_t* tmp;   // block DCs
     int16_t* dc;    // output plane (last row left as it is)
     int xnb, ynb;
-    int first;
 };
 
 struct DcLaunch {
-    int njobs, total;
-    DcJob job[MAX_ME_JOBS];
+    int total, per_job;
+    const DcJob* jobs;  // device table
 };
 
 __global__ void __launch_bounds__(ME_THREADS) block_dc_kernel(const __grid_constant__ DcLaunch L) {
     const int u = blockIdx.x * WARPS_PER_CTA + (threadIdx.x >> 5);
     if (u >= L.total) return;
-    int j = 0;
-    while (j + 1 < L.njobs && L.job[j + 1].first <= u) ++j;
-    const DcJob& J = L.job[j];
-    const int b = u - J.first;
+    const int j = u / L.per_job;
+    const DcJob& J = L.jobs[j];
+    const int b = u - j * L.per_job;
     const int by = b / J.xnb, bx = b - by * J.xnb;
     const int dc = block_dc(J.pic, J.pw, block_limits(J.o, J.pw, J.ph, bx, by));
     if ((threadIdx.x & 31) == 0) J.tmp[b] = (int16_t)dc;
@@ -833,10 +844,9 @@ __global__ void __launch_bounds__(ME_THREADS) block_dc_kernel(const __grid_const
 __global__ void smooth_dc_kernel(const __grid_constant__ DcLaunch L) {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= L.total) return;
-    int j = 0;
-    while (j + 1 < L.njobs && L.job[j + 1].first <= u) ++j;
-    const DcJob& J = L.job[j];
-    const int b = u - J.first;
+    const int j = u / L.per_job;
+    const DcJob& J = L.jobs[j];
+    const int b = u - j * L.per_job;
     const int y = b / J.xnb, x = b - y * J.xnb;
     const int W = J.xnb;
     if (y == J.ynb - 1) return;
@@ -1050,11 +1060,9 @@ size_t task_layout(const MeGeometry& g, TaskBufs& T, Arena& a) {
     return a.used;
 }
 
-constexpr int MAX_MODE_JOBS = 4;
-
 template <class Launch, class Kernel>
 int launch_wavefront(Launch& L, Kernel kernel, int* ctl, cudaStream_t st) {
-    if (L.njobs == 0) return DGPU_OK;
+    if (L.total == 0) return DGPU_OK;
     L.ticket = ctl;
     L.err = ctl + 1;
     DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
@@ -1079,9 +1087,53 @@ struct BatchArgs {
     float* const* sbcost_out;
 };
 
+// Wave-order prefix table of a W x H grid (see Wave): units of one job on diagonals < t.
+void wave_prefix(int W, int H, int slope, std::vector<int>& pre) {
+    const int T = (W - 1) + slope * (H - 1) + 1;
+    pre.assign(T + 1, 0);
+    for (int t = 0; t < T; ++t) {
+        const int ex = t - (W - 1);
+        const int ylo = ex > 0 ? (ex + slope - 1) / slope : 0;
+        const int yhi = std::min(H - 1, t / slope);
+        pre[t + 1] = pre[t] + std::max(0, yhi - ylo + 1);
+    }
+}
+
+// Device tables of one batch: the jobs of every launch and the wave-order prefixes.
+struct BatchTables {
+    PelJob* pel;      // (depth + 1) levels x 2 * ntasks
+    SubJob* sub;      // 2 * ntasks
+    ModeJob* mode;    // ntasks
+    DcJob* dc;        // 3 * ntasks
+    int* prefix;      // levels 0..depth (slope 2), then superblocks (slope 1)
+    size_t prefix_off[14];
+    size_t prefix_len;
+};
+
+size_t prefix_layout(const MeGeometry& g, size_t* off) {
+    size_t n = 0;
+    for (int l = 0; l <= g.depth; ++l) {
+        off[l] = n;
+        n += (size_t)(g.xnb[l] - 1) + 2 * (size_t)(g.ynb[l] - 1) + 2;
+    }
+    off[g.depth + 1] = n;
+    n += (size_t)(g.xnsb - 1) + (size_t)(g.ynsb - 1) + 2;
+    return n;
+}
+
 size_t batch_bytes(const MeGeometry& g, const BatchArgs& A, std::vector<PicBufs>* P, std::vector<TaskBufs>* T,
-                   char* base, int** ctl) {
+                   char* base, int** ctl, BatchTables* tabs = nullptr) {
     Arena a{base, 0, 0};
+    {
+        BatchTables bt{};
+        bt.pel = a.take<PelJob>((size_t)(g.depth + 1) * 2 * A.ntasks);
+        bt.sub = a.take<SubJob>((size_t)2 * A.ntasks);
+        bt.mode = a.take<ModeJob>((size_t)A.ntasks);
+        bt.dc = a.take<DcJob>((size_t)3 * A.ntasks);
+        bt.prefix_len = prefix_layout(g, bt.prefix_off);
+        bt.prefix = a.take<int>(bt.prefix_len);
+        if (tabs) *tabs = bt;
+    }
     std::vector<char> is_ref(A.npics, 0);
     for (int t = 0; t < A.ntasks; ++t)
         for (int r = 0; r < 2; ++r)
@@ -1105,7 +1157,27 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
     std::vector<PicBufs> P;
     std::vector<TaskBufs> T;
     int* ctl = nullptr;
-    batch_bytes(g, A, &P, &T, static_cast<char*>(workspace), &ctl);
+    BatchTables tabs{};
+    batch_bytes(g, A, &P, &T, static_cast<char*>(workspace), &ctl, &tabs);
+    {
+        std::vector<int> all(tabs.prefix_len), pre;
+        for (int l = 0; l <= g.depth; ++l) {
+            wave_prefix(g.xnb[l], g.ynb[l], 2, pre);
+            std::copy(pre.begin(), pre.end(), all.begin() + tabs.prefix_off[l]);
+        }
+        wave_prefix(g.xnsb, g.ynsb, 1, pre);
+        std::copy(pre.begin(), pre.end(), all.begin() + tabs.prefix_off[g.depth + 1]);
+        DGPU_CHECK_CUDA(cudaMemcpyAsync(tabs.prefix, all.data(), sizeof(int) * all.size(), cudaMemcpyHostToDevice, st));
+    }
+    auto wave_of = [&](int slot, int W, int slope, int njobs) {
+        Wave w;
+        w.prefix = tabs.prefix + tabs.prefix_off[slot];
+        w.W = W;
+        w.slope = slope;
+        w.njobs = njobs;
+        w.T = 0;
+        return w;
+    };
     DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, 2 * sizeof(int), st));
     const size_t nb = (size_t)g.xnb[0] * g.ynb[0];
     auto luma = [&](int p) { return A.pics[3 * p]; };
@@ -1135,31 +1207,12 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
             if (rc) return rc;
         }
     }
-    // ---- pel search, coarsest level first ----
+    // ---- pel search, coarsest level first: every job of a level in one wavefront ----
     for (int l = g.depth; l >= 0; --l) {
-        PelLaunch L{};
-        L.o = g.lb[2];
-        int total = 0;
-        auto flush = [&]() -> int {
-            if (L.njobs == 0) return DGPU_OK;
-            L.total = total;
-            L.ticket = ctl;
-            L.err = ctl + 1;
-            // the candidate-list phase covers every unit: one warp per unit
-            pel_lists_kernel<<<(total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, 0, st>>>(L);
-            DGPU_CHECK_LAUNCH();
-            const int rc = launch_wavefront(L, pel_wavefront_kernel, ctl, st);
-            L.njobs = 0;
-            total = 0;
-            return rc;
-        };
+        std::vector<PelJob> jobs;
         for (int t = 0; t < A.ntasks; ++t)
             for (int r = 0; r < nref_of(t); ++r) {
-                if (L.njobs == MAX_ME_JOBS) {
-                    const int rc = flush();
-                    if (rc) return rc;
-                }
-                PelJob& J = L.job[L.njobs++];
+                PelJob J{};
                 const int pp = A.task_pic[t], rp = ref_of(t, r);
                 J.pic = l ? P[pp].down[l] : luma(pp);
                 J.ref = l ? P[rp].down[l] : luma(rp);
@@ -1176,11 +1229,22 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                 J.best_sad = T[t].best_sad[l][r];
                 J.best_mv = T[t].best_mv[l][r];
                 J.flags = T[t].flags + (size_t)r * g.xnb[l] * g.ynb[l];
-                J.first = total;
-                total += J.xnb * J.ynb;
                 DGPU_CHECK_CUDA(cudaMemsetAsync(J.flags, 0, sizeof(int) * J.xnb * J.ynb, st));
+                jobs.push_back(J);
             }
-        const int rc = flush();
+        PelJob* dj = tabs.pel + (size_t)l * 2 * A.ntasks;
+        DGPU_CHECK_CUDA(cudaMemcpyAsync(dj, jobs.data(), sizeof(PelJob) * jobs.size(), cudaMemcpyHostToDevice, st));
+        PelLaunch L{};
+        L.o = g.lb[2];
+        L.per_job = g.xnb[l] * g.ynb[l];
+        L.total = L.per_job * (int)jobs.size();
+        L.jobs = dj;
+        L.wave = wave_of(l, g.xnb[l], 2, (int)jobs.size());
+        L.wave.T = (g.xnb[l] - 1) + 2 * (g.ynb[l] - 1) + 1;
+        // the candidate-list phase covers every unit: one warp per unit
+        pel_lists_kernel<<<(L.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, 0, st>>>(L);
+        DGPU_CHECK_LAUNCH();
+        const int rc = launch_wavefront(L, pel_wavefront_kernel, ctl, st);
         if (rc) return rc;
     }
     int err_host = 0;
@@ -1216,22 +1280,12 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                 if (rc) return rc;
             }
         }
-        // ---- sub-pel refinement ----
+        // ---- sub-pel refinement: every job in one wavefront ----
         {
-            SubLaunch S{};
-            S.o = g.lb[2];
-            S.prec = A.prec;
-            int total = 0;
+            std::vector<SubJob> jobs;
             for (int t = 0; t < A.ntasks; ++t)
                 for (int r = 0; r < nref_of(t); ++r) {
-                    if (S.njobs == MAX_ME_JOBS) {
-                        S.total = total;
-                        const int rc = launch_wavefront(S, subpel_wavefront_kernel, ctl, st);
-                        if (rc) return rc;
-                        S.njobs = 0;
-                        total = 0;
-                    }
-                    SubJob& J = S.job[S.njobs++];
+                    SubJob J{};
                     J.pic = luma(A.task_pic[t]);
                     J.up = P[ref_of(t, r)].up;
                     J.pw = g.w;
@@ -1242,11 +1296,18 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                     J.cost = cost0(t, r);
                     J.lambda = T[t].lambda[2];
                     J.flags = T[t].flags + (size_t)r * nb;
-                    J.first = total;
-                    total += (int)nb;
                     DGPU_CHECK_CUDA(cudaMemsetAsync(J.flags, 0, sizeof(int) * nb, st));
+                    jobs.push_back(J);
                 }
-            S.total = total;
+            DGPU_CHECK_CUDA(cudaMemcpyAsync(tabs.sub, jobs.data(), sizeof(SubJob) * jobs.size(),
+                                            cudaMemcpyHostToDevice, st));
+            SubLaunch S{};
+            S.o = g.lb[2];
+            S.prec = A.prec;
+            S.total = (int)nb * (int)jobs.size();
+            S.jobs = tabs.sub;
+            S.wave = wave_of(0, g.xnb[0], 2, (int)jobs.size());
+            S.wave.T = (g.xnb[0] - 1) + 2 * (g.ynb[0] - 1) + 1;
             const int rc = launch_wavefront(S, subpel_wavefront_kernel, ctl, st);
             if (rc) return rc;
         }
@@ -1281,20 +1342,14 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
             M.level_factor[0] = f0;
             M.level_factor[1] = f1;
             M.level_factor[2] = 1.0f;
-            int total = 0;
-            // one launch per reference count: the kernel takes nref per launch
+            std::vector<ModeJob> jobs;
+            // one launch per reference count (the kernel takes nref per launch); each launch
+            // runs all its pictures' superblock wavefronts together
             for (int want_nref = 1; want_nref <= 2; ++want_nref) {
-                M.nref = want_nref;
+                const size_t first = jobs.size();
                 for (int t = 0; t < A.ntasks; ++t) {
                     if (nref_of(t) != want_nref) continue;
-                    if (M.njobs == MAX_MODE_JOBS) {
-                        M.total = total;
-                        const int rc = launch_wavefront(M, mode_wavefront_kernel, ctl, st);
-                        if (rc) return rc;
-                        M.njobs = 0;
-                        total = 0;
-                    }
-                    ModeJob& J = M.job[M.njobs++];
+                    ModeJob J{};
                     J.pic = luma(A.task_pic[t]);
                     J.up[0] = P[ref_of(t, 0)].up;
                     J.up[1] = P[ref_of(t, 1)].up;
@@ -1326,51 +1381,50 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                     J.xnsb = g.xnsb;
                     J.ynsb = g.ynsb;
                     J.flags = T[t].flags;
-                    J.first = total;
-                    total += g.xnsb * g.ynsb;
                     DGPU_CHECK_CUDA(cudaMemsetAsync(J.flags, 0, sizeof(int) * g.xnsb * g.ynsb, st));
+                    jobs.push_back(J);
                 }
-                M.total = total;
+                const int nj = (int)(jobs.size() - first);
+                if (nj == 0) continue;
+                DGPU_CHECK_CUDA(cudaMemcpyAsync(tabs.mode + first, jobs.data() + first, sizeof(ModeJob) * nj,
+                                                cudaMemcpyHostToDevice, st));
+                M.nref = want_nref;
+                M.jobs = tabs.mode + first;
+                M.total = g.xnsb * g.ynsb * nj;
+                M.wave = wave_of(g.depth + 1, g.xnsb, 1, nj);
+                M.wave.T = (g.xnsb - 1) + (g.ynsb - 1) + 1;
                 const int rc = launch_wavefront(M, mode_wavefront_kernel, ctl, st);
                 if (rc) return rc;
-                M.njobs = 0;
-                total = 0;
             }
             // ---- DC values of all three components ----
-            DcLaunch D{};
-            int dtotal = 0;
-            auto dflush = [&]() -> int {
-                if (D.njobs == 0) return DGPU_OK;
-                D.total = dtotal;
-                block_dc_kernel<<<(dtotal + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, 0, st>>>(D);
-                DGPU_CHECK_LAUNCH();
-                smooth_dc_kernel<<<(dtotal + 255) / 256, 256, 0, st>>>(D);
-                DGPU_CHECK_LAUNCH();
-                D.njobs = 0;
-                dtotal = 0;
-                return DGPU_OK;
-            };
-            for (int t = 0; t < A.ntasks; ++t)
-                for (int c = 0; c < 3; ++c) {
-                    if (D.njobs == MAX_ME_JOBS) {
-                        const int rc = dflush();
-                        if (rc) return rc;
+            {
+                std::vector<DcJob> jobs;
+                for (int t = 0; t < A.ntasks; ++t)
+                    for (int c = 0; c < 3; ++c) {
+                        const int xs = (c && A.cformat != 0) ? 1 : 0, ys = (c && A.cformat == 2) ? 1 : 0;
+                        DcJob Jd{};
+                        Jd.pic = A.pics[3 * A.task_pic[t] + c];
+                        Jd.pw = g.w >> xs;
+                        Jd.ph = g.h >> ys;
+                        Jd.o = make_olb(g.lb[2].xblen >> xs, g.lb[2].yblen >> ys, g.lb[2].xbsep >> xs,
+                                        g.lb[2].ybsep >> ys);
+                        Jd.tmp = T[t].dctmp + (size_t)c * nb;
+                        Jd.dc = A.dc_out[t] + (size_t)c * nb;
+                        Jd.xnb = g.xnb[0];
+                        Jd.ynb = g.ynb[0];
+                        jobs.push_back(Jd);
                     }
-                    const int xs = (c && A.cformat != 0) ? 1 : 0, ys = (c && A.cformat == 2) ? 1 : 0;
-                    DcJob& Jd = D.job[D.njobs++];
-                    Jd.pic = A.pics[3 * A.task_pic[t] + c];
-                    Jd.pw = g.w >> xs;
-                    Jd.ph = g.h >> ys;
-                    Jd.o = make_olb(g.lb[2].xblen >> xs, g.lb[2].yblen >> ys, g.lb[2].xbsep >> xs, g.lb[2].ybsep >> ys);
-                    Jd.tmp = T[t].dctmp + (size_t)c * nb;
-                    Jd.dc = A.dc_out[t] + (size_t)c * nb;
-                    Jd.xnb = g.xnb[0];
-                    Jd.ynb = g.ynb[0];
-                    Jd.first = dtotal;
-                    dtotal += (int)nb;
-                }
-            const int rc = dflush();
-            if (rc) return rc;
+                DGPU_CHECK_CUDA(cudaMemcpyAsync(tabs.dc, jobs.data(), sizeof(DcJob) * jobs.size(),
+                                                cudaMemcpyHostToDevice, st));
+                DcLaunch D{};
+                D.per_job = (int)nb;
+                D.total = (int)nb * (int)jobs.size();
+                D.jobs = tabs.dc;
+                block_dc_kernel<<<(D.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, 0, st>>>(D);
+                DGPU_CHECK_LAUNCH();
+                smooth_dc_kernel<<<(D.total + 255) / 256, 256, 0, st>>>(D);
+                DGPU_CHECK_LAUNCH();
+            }
         }
     }
     DGPU_CHECK_CUDA(cudaMemcpyAsync(&err_host, ctl + 1, sizeof(int), cudaMemcpyDeviceToHost, st));

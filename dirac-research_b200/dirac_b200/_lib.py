@@ -99,6 +99,8 @@ SIGNATURES = {
     ),
     "dgpu_encoder_create": (c_int, [c_void_p, c_int, c_void_p, P_void]),
     "dgpu_encoder_destroy": (c_int, [c_void_p]),
+    "dgpu_encoder_reset": (c_int, [c_void_p]),
+    "dgpu_encoder_profile": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "dgpu_encoder_load": (c_int, [c_void_p, P_void, c_int]),
     "dgpu_encoder_end_sequence": (c_int, [c_void_p]),
     "dgpu_encoder_code_next": (c_int, [c_void_p, c_void_p, c_void_p]),

@@ -14,6 +14,8 @@ import torch
 from . import _lib
 
 RECON, COEFF, QINDEX, MV, MODE, DC, SPLIT, BANDS, CBSKIP, OUTPUT = range(10)
+STAGES = ["load", "motion_estimation", "mc_subtract", "dwt_forward", "quantisation", "dwt_inverse",
+          "mc_add_clip", "upconvert"]
 
 
 class EncoderParams(ctypes.Structure):
@@ -86,6 +88,17 @@ class SequenceEncoder:
         else:
             ptrs = [t.data_ptr() for t in planes]
         _lib.check(self.lib.dgpu_encoder_load(self.handle, _lib.ptr_array(ptrs), int(on_host)), "dgpu_encoder_load")
+
+    def reset(self):
+        """Start a new sequence, keeping the device memory."""
+        _lib.check(self.lib.dgpu_encoder_reset(self.handle), "dgpu_encoder_reset")
+
+    def profile(self, enable):
+        """Turn stage timing on/off; returns {stage: (ms, calls)} accumulated so far."""
+        ms = (ctypes.c_double * len(STAGES))()
+        calls = (ctypes.c_int * len(STAGES))()
+        _lib.check(self.lib.dgpu_encoder_profile(self.handle, int(enable), ms, calls), "dgpu_encoder_profile")
+        return {n: (ms[k], calls[k]) for k, n in enumerate(STAGES)}
 
     def end_sequence(self):
         _lib.check(self.lib.dgpu_encoder_end_sequence(self.handle), "dgpu_encoder_end_sequence")

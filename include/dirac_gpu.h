@@ -326,8 +326,26 @@ typedef struct {
 #define DGPU_ENC_CBSKIP 8   /* uint8 code-block skip flags of all bands, band-list order */
 #define DGPU_ENC_OUTPUT 9   /* uint8 (depth 8) / uint16 [h][w] output samples: recon + 2^(d-1) */
 
+/* stages timed by dgpu_encoder_profile */
+#define DGPU_STAGE_LOAD 0
+#define DGPU_STAGE_ME 1
+#define DGPU_STAGE_MC_SUBTRACT 2
+#define DGPU_STAGE_DWT_FORWARD 3
+#define DGPU_STAGE_QUANT 4
+#define DGPU_STAGE_DWT_INVERSE 5
+#define DGPU_STAGE_MC_ADD 6   /* motion compensation ADD with the clip, or the clip alone */
+#define DGPU_STAGE_UPCONVERT 7
+#define DGPU_ENC_NSTAGES 8
+
 int dgpu_encoder_create(const dgpu_encoder_params* params, int max_pictures, void* stream, void** encoder);
 int dgpu_encoder_destroy(void* encoder);
+/* Forgets every picture and the GOP state (a new sequence), keeping the device memory. */
+int dgpu_encoder_reset(void* encoder);
+/* Stage timing with CUDA events on the encoder's stream (each stage waits for its end event,
+ * so profiled runs are slower).  Copies the accumulated milliseconds and call counts per
+ * stage (DGPU_STAGE_*) to stage_ms / stage_calls when not NULL, clears them, and turns
+ * profiling on or off. */
+int dgpu_encoder_profile(void* encoder, int enable, double* stage_ms, int* stage_calls);
 /* Loads the next picture in display order: three dense planes of unsigned samples (uint8 for
  * depth 8, uint16 otherwise), in host memory (on_host = 1) or device memory (0). */
 int dgpu_encoder_load(void* encoder, const void* const* planes, int on_host);
