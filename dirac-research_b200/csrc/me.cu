@@ -228,19 +228,43 @@ __device__ __forceinline__ void float_seq_add(FloatSeq& f, int d) {
 
 // ---- block differences ----------------------------------------------------------------------
 
-// Integer SAD of one candidate against a same-size plane, coordinates clamped
-// (PelBlockDiff, me_utils.cpp:138-282).  Lanes own columns; warp-reduced.
-__device__ int pel_sad(const int16_t* pic, const int16_t* ref, int pw, int ph, const Blim& b, short2 mv) {
-    const int lane = threadIdx.x & 31;
-    int s = 0;
-    for (int c = lane; c < b.xl; c += 32) {
-        const int x = b.xp + c;
-        const int rx = clampi(x + mv.x, 0, pw - 1);
-        for (int j = 0; j < b.yl; ++j) {
-            const int y = b.yp + j;
-            const int ry = clampi(y + mv.y, 0, ph - 1);
-            s += abs((int)(int16_t)(pic[(size_t)y * pw + x] - ref[(size_t)ry * pw + rx]));
+// Block pixels are spread over the warp in raster order: pixel k of the block (row-major,
+// xl per row) belongs to lane k % 32 at step k / 32, so every lane is busy whatever the block
+// width, and lane order within a step is raster order.  PixWalk tracks one lane's position.
+struct PixWalk {
+    int row, col, drow, dcol, xl;
+    __device__ __forceinline__ PixWalk(int xl_, int k0 = 0) : xl(xl_) {
+        const int k = k0 + (threadIdx.x & 31);
+        row = k / xl;
+        col = k - row * xl;
+        drow = 32 / xl;
+        dcol = 32 - drow * xl;
+    }
+    __device__ __forceinline__ void next() {
+        col += dcol;
+        row += drow;
+        if (col >= xl) {
+            col -= xl;
+            ++row;
         }
+    }
+};
+
+// Integer SAD of one candidate against a same-size plane, coordinates clamped
+// (PelBlockDiff, me_utils.cpp:138-282).  Warp-reduced.
+__device__ int pel_sad(const int16_t* pic, const int16_t* ref, int pw, int ph, const Blim& b, short2 mv) {
+    if (b.xl <= 0 || b.yl <= 0) return 0;
+    const int lane = threadIdx.x & 31;
+    const int n = b.xl * b.yl;
+    PixWalk w(b.xl);
+    int s = 0;
+#pragma unroll 8
+    for (int k = lane; k < n; k += 32) {
+        const int x = b.xp + w.col, y = b.yp + w.row;
+        const int rx = clampi(x + mv.x, 0, pw - 1);
+        const int ry = clampi(y + mv.y, 0, ph - 1);
+        s += abs((int)(int16_t)(pic[(size_t)y * pw + x] - ref[(size_t)ry * pw + rx]));
+        w.next();
     }
     return __reduce_add_sync(0xffffffffu, s);
 }
@@ -265,20 +289,35 @@ __device__ __forceinline__ int up_pred(const int16_t* up, int uw, int uh, int p,
 }
 
 // Float sum, in raster order from start, of |pred - pic| over a block: the cost loop of
-// BlockDiff{Half,Quarter,Eighth}Pel::Diff.  Returns the reference's float result.
+// BlockDiff{Half,Quarter,Eighth}Pel::Diff.  Returns the reference's float result.  Eight
+// steps (256 pixels) are loaded at once; when their total cannot cross a power of two the
+// whole chunk is added exactly in one go, otherwise step by step in raster order.
 __device__ float subpel_cost(const int16_t* pic, int pw, const int16_t* up, int uw, int uh, int p, const Blim& b,
                              int mx, int my, float start) {
+    if (b.xl <= 0 || b.yl <= 0) return start;
     const int lane = threadIdx.x & 31;
     FloatSeq f = float_seq_start(start);
-    for (int j = 0; j < b.yl; ++j) {
-        const int y = b.yp + j;
-        for (int c0 = 0; c0 < b.xl; c0 += 32) {
-            int d = 0;
-            if (c0 + lane < b.xl) {
-                const int x = b.xp + c0 + lane;
-                d = abs(up_pred(up, uw, uh, p, x, y, mx, my) - pic[(size_t)y * pw + x]);
+    const int n = b.xl * b.yl;
+    PixWalk w(b.xl);
+    for (int k0 = 0; k0 < n; k0 += 256) {
+        int d[8];
+        int tot = 0;
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            d[s] = 0;
+            if (k0 + 32 * s + lane < n) {
+                const int x = b.xp + w.col, y = b.yp + w.row;
+                d[s] = abs(up_pred(up, uw, uh, p, x, y, mx, my) - pic[(size_t)y * pw + x]);
             }
-            float_seq_add(f, d);
+            tot += d[s];
+            w.next();
+        }
+        tot = __reduce_add_sync(0xffffffffu, tot);
+        if (f.c + (double)tot < f.bound) {
+            f.c += (double)tot;
+        } else {
+#pragma unroll
+            for (int s = 0; s < 8; ++s) float_seq_add(f, d[s]);
         }
     }
     return (float)f.c;
@@ -288,9 +327,19 @@ __device__ float subpel_cost(const int16_t* pic, int pw, const int16_t* up, int 
 // intermediates, summed in float from 0 (exact: integer sums below 2^24).  The eighth-pel
 // version walks the second reference from the first one's integer start position when the
 // second one needs bounds checking (me_utils.cpp:1764-1768); reproduced here.
+__device__ int bi_sad_range(const int16_t* pic, int pw, const int16_t* up1, const int16_t* up2, int uw, int uh,
+                            int p, const Blim& b, short2 mv1, short2 mv2, int kb, int ke);
+
 __device__ float bi_cost(const int16_t* pic, int pw, const int16_t* up1, const int16_t* up2, int uw, int uh, int p,
                          const Blim& b, short2 mv1, short2 mv2) {
     if (b.xl <= 0 || b.yl <= 0) return 0.0f;
+    return (float)bi_sad_range(pic, pw, up1, up2, uw, uh, p, b, mv1, mv2, 0, b.xl * b.yl);
+}
+
+// Pixels [kb, ke) (raster order) of the bi-prediction SAD; integer, so it splits freely.
+__device__ int bi_sad_range(const int16_t* pic, int pw, const int16_t* up1, const int16_t* up2, int uw, int uh,
+                            int p, const Blim& b, short2 mv1, short2 mv2, int kb, int ke) {
+    if (b.xl <= 0 || b.yl <= 0 || ke <= kb) return 0;
     int m2x = mv2.x, m2y = mv2.y;
     if (p == 3) {
         const int sx = (b.xp << 1) + (mv2.x >> 2), sy = (b.yp << 1) + (mv2.y >> 2);
@@ -300,28 +349,33 @@ __device__ float bi_cost(const int16_t* pic, int pw, const int16_t* up1, const i
         }
     }
     const int lane = threadIdx.x & 31;
+    PixWalk w(b.xl, kb);
     int s = 0;
-    for (int c = lane; c < b.xl; c += 32) {
-        const int x = b.xp + c;
-        for (int j = 0; j < b.yl; ++j) {
-            const int y = b.yp + j;
-            const int16_t dd = (int16_t)((pic[(size_t)y * pw + x] << 1) - up_pred(up1, uw, uh, p, x, y, mv1.x, mv1.y));
-            const int16_t t = (int16_t)((dd - up_pred(up2, uw, uh, p, x, y, m2x, m2y)) >> 1);
-            s += abs((int)t);
-        }
+#pragma unroll 4
+    for (int k = kb + lane; k < ke; k += 32) {
+        const int x = b.xp + w.col, y = b.yp + w.row;
+        const int16_t dd = (int16_t)((pic[(size_t)y * pw + x] << 1) - up_pred(up1, uw, uh, p, x, y, mv1.x, mv1.y));
+        const int16_t t = (int16_t)((dd - up_pred(up2, uw, uh, p, x, y, m2x, m2y)) >> 1);
+        s += abs((int)t);
+        w.next();
     }
-    return (float)__reduce_add_sync(0xffffffffu, s);
+    return __reduce_add_sync(0xffffffffu, s);
 }
 
 // IntraBlockDiff::CalcDC and ::Diff (me_utils.cpp:284-408): truncating mean, SAD against it.
 __device__ int block_dc(const int16_t* pic, int pw, const Blim& b) {
     if (b.xl <= 0 || b.yl <= 0) return 0;
     const int lane = threadIdx.x & 31;
+    const int n = b.xl * b.yl;
+    PixWalk w(b.xl);
     int s = 0;
-    for (int c = lane; c < b.xl; c += 32)
-        for (int j = 0; j < b.yl; ++j) s += pic[(size_t)(b.yp + j) * pw + b.xp + c];
+#pragma unroll 8
+    for (int k = lane; k < n; k += 32) {
+        s += pic[(size_t)(b.yp + w.row) * pw + b.xp + w.col];
+        w.next();
+    }
     s = __reduce_add_sync(0xffffffffu, s);
-    return (int)(int16_t)(s / (b.xl * b.yl));
+    return (int)(int16_t)(s / n);
 }
 
 __device__ float intra_cost(const int16_t* pic, int pw, const Blim& b, int16_t& dc) {
@@ -331,9 +385,14 @@ __device__ float intra_cost(const int16_t* pic, int pw, const Blim& b, int16_t& 
     }
     dc = (int16_t)block_dc(pic, pw, b);
     const int lane = threadIdx.x & 31;
+    const int n = b.xl * b.yl;
+    PixWalk w(b.xl);
     int s = 0;
-    for (int c = lane; c < b.xl; c += 32)
-        for (int j = 0; j < b.yl; ++j) s += abs(pic[(size_t)(b.yp + j) * pw + b.xp + c] - dc);
+#pragma unroll 8
+    for (int k = lane; k < n; k += 32) {
+        s += abs(pic[(size_t)(b.yp + w.row) * pw + b.xp + w.col] - dc);
+        w.next();
+    }
     return (float)__reduce_add_sync(0xffffffffu, s);
 }
 
@@ -625,6 +684,7 @@ struct ModeJob {
     uint8_t* split;
     int xnsb, ynsb;
     int* flags;          // per superblock
+    float* bcost;        // level-2 (block) decision costs, from mode_blocks_kernel
 };
 
 struct ModeLaunch {
@@ -692,7 +752,7 @@ __device__ void do_me(const ModeLaunch& L, const ModeJob& J, int x, int y, int l
 }
 
 // ModeDecider::DoUnitDecn: best of REF1 / REF2 / bi-prediction / intra for one unit.
-__device__ float do_unit_decn(const ModeLaunch& L, const ModeJob& J, int x, int y, int level) {
+__device__ float do_unit_decn(const ModeLaunch& L, const ModeJob& J, int x, int y, int level, float bsad_in = -1.0f) {
     const LevelData& me = J.lev[level];
     const size_t k = (size_t)y * me.xnb + x;
     const float lambda = me.lambda[k];
@@ -713,8 +773,9 @@ __device__ float do_unit_decn(const ModeLaunch& L, const ModeJob& J, int x, int 
             best_sad = __ldcg(&me.cost[1][3 * k]);
         }
         const float bmvcost = __ldcg(&me.cost[0][3 * k + 1]) + __ldcg(&me.cost[1][3 * k + 1]);
-        const float bsad = bi_cost(J.pic, J.pw, J.up[0], J.up[1], 2 * J.pw, 2 * J.ph, L.prec, bl,
-                                   __ldcg(&me.mv[0][k]), __ldcg(&me.mv[1][k]));
+        const float bsad = bsad_in >= 0.0f ? bsad_in
+                                           : bi_cost(J.pic, J.pw, J.up[0], J.up[1], 2 * J.pw, 2 * J.ph, L.prec, bl,
+                                                     __ldcg(&me.mv[0][k]), __ldcg(&me.mv[1][k]));
         float btotal = bsad + lambda * bmvcost;
         btotal *= f;
         unit = btotal + mode_cost;
@@ -746,69 +807,180 @@ __device__ float do_unit_decn(const ModeLaunch& L, const ModeJob& J, int x, int 
     return min_cost;
 }
 
-// ModeDecider::DoLevelDecn for superblock (xsb, ysb) at one level.
-__device__ void do_level_decn(const ModeLaunch& L, const ModeJob& J, int xsb, int ysb, int level) {
-    const int xs = xsb << level, ys = ysb << level;
-    const int n = 1 << level;
+// Writes the decisions of one level's units over the superblock's 16 blocks
+// (ModeDecider::DoLevelDecn's propagation) and the superblock's split and cost.  Called by
+// thread 0 only, so that its release of the superblock's flag publishes every write.
+__device__ void propagate_level(const ModeLaunch& L, const ModeJob& J, int xsb, int ysb, int level, float sb_cost) {
+    const LevelData& lv = J.lev[level];
+    const LevelData& bl = J.lev[2];
+    const int span = 1 << (2 - level);
+    for (int t = 0; t < 16; ++t) {
+        const int v = (ysb << 2) + (t >> 2), u = (xsb << 2) + (t & 3);
+        const int j = v / span, i = u / span;
+        const size_t src = (size_t)j * lv.xnb + i, dst = (size_t)v * bl.xnb + u;
+        bl.mode[dst] = __ldcg(&lv.mode[src]);
+        bl.dcy[dst] = __ldcg(&lv.dcy[src]);
+        bl.mv[0][dst] = __ldcg(&lv.mv[0][src]);
+        if (L.nref > 1) bl.mv[1][dst] = __ldcg(&lv.mv[1][src]);
+    }
     const size_t sb = (size_t)ysb * J.xnsb + xsb;
-    float sb_cost = 0.0f;
-    for (int j = ys; j < ys + n; ++j)
-        for (int i = xs; i < xs + n; ++i) {
-            if (level < 2) do_me(L, J, i, j, level);
-            sb_cost += do_unit_decn(L, J, i, j, level);
-        }
-    if (level == 2) {
-        if ((threadIdx.x & 31) == 0) {
-            J.split[sb] = 2;
-            J.sbcost[sb] = sb_cost;
-        }
-        __syncwarp();
-        return;
-    }
-    const float cur = __ldcg(&J.sbcost[sb]);
-    if (sb_cost <= cur) {
-        const LevelData& lv = J.lev[level];
-        const LevelData& bl = J.lev[2];
-        const int span = 1 << (2 - level);
-        const int lane = threadIdx.x & 31;
-        // propagate the units' decisions to their blocks (16 blocks per superblock); lane 0
-        // does every write of a superblock so that its release publishes them all
-        for (int t = 0; t < 16 && lane == 0; ++t) {
-            const int v = (ysb << 2) + (t >> 2), u = (xsb << 2) + (t & 3);
-            const int j = v / span, i = u / span;
-            const size_t src = (size_t)j * lv.xnb + i, dst = (size_t)v * bl.xnb + u;
-            bl.mode[dst] = __ldcg(&lv.mode[src]);
-            bl.dcy[dst] = __ldcg(&lv.dcy[src]);
-            bl.mv[0][dst] = __ldcg(&lv.mv[0][src]);
-            if (L.nref > 1) bl.mv[1][dst] = __ldcg(&lv.mv[1][src]);
-        }
-        if (lane == 0) {
-            J.sbcost[sb] = sb_cost;
-            J.split[sb] = (uint8_t)level;
-        }
-        __syncwarp();
-    }
+    J.sbcost[sb] = sb_cost;
+    J.split[sb] = (uint8_t)level;
 }
 
+// Level-2 decisions (every block: REF1 / REF2 / bi / intra) depend on nothing outside the block,
+// so they run for all blocks of all jobs before the superblock wavefront.  One warp per block;
+// the unit cost goes to bcost for the superblock sums.
+__global__ void __launch_bounds__(ME_THREADS) mode_blocks_kernel(const __grid_constant__ ModeLaunch L, int per_job) {
+    const int u = blockIdx.x * WARPS_PER_CTA + (threadIdx.x >> 5);
+    if (u >= L.total) return;
+    const int jn = u / per_job;
+    const ModeJob& J = L.jobs[jn];
+    const int k = u - jn * per_job;
+    const int xnb = J.lev[2].xnb;
+    const int y = k / xnb, x = k - y * xnb;
+    const float c = do_unit_decn(L, J, x, y, 2);
+    if ((threadIdx.x & 31) == 0) J.bcost[k] = c;
+}
+
+// Superblock wavefront (ModeDecider::DoModeDecn per superblock): one CTA of WARPS_PER_CTA
+// warps per superblock.  Level 2 sums the precomputed block costs; level 1 gives one
+// sub-superblock to each warp; level 0 spreads its motion-search candidates and the
+// bi-prediction SAD over the warps.  Float sums keep the reference's order.
 __global__ void __launch_bounds__(ME_THREADS) mode_wavefront_kernel(const __grid_constant__ ModeLaunch L) {
+    static_assert(WARPS_PER_CTA == 4, "level 1 has four sub-superblocks");
+    __shared__ int s_u;
+    __shared__ float s_cost[WARPS_PER_CTA];
+    __shared__ float s_sum[2][WARPS_PER_CTA];
+    __shared__ float s_mvc[2][WARPS_PER_CTA];
+    __shared__ int s_bi[WARPS_PER_CTA];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (;;) {
-        const int u = warp_ticket(L.ticket);
+        __syncthreads();
+        if (threadIdx.x == 0) s_u = atomicAdd(L.ticket, 1);
+        __syncthreads();
+        const int u = s_u;
         if (u >= L.total) return;
         int jn, xsb, ysb;
         wave_unit(L.wave, u, jn, xsb, ysb);
         const ModeJob& J = L.jobs[jn];
         const int s = ysb * J.xnsb + xsb;
-        if (xsb > 0) wait_flag(&J.flags[s - 1], L.err);
-        if (ysb > 0) {
-            wait_flag(&J.flags[s - J.xnsb], L.err);
-            if (xsb > 0) wait_flag(&J.flags[s - J.xnsb - 1], L.err);
+        if (threadIdx.x == 0) {
+            if (xsb > 0) wait_flag(&J.flags[s - 1], L.err);
+            if (ysb > 0) {
+                wait_flag(&J.flags[s - J.xnsb], L.err);
+                if (xsb > 0) wait_flag(&J.flags[s - J.xnsb - 1], L.err);
+            }
         }
-        do_level_decn(L, J, xsb, ysb, 2);
-        const float old = __ldcg(&J.sbcost[(size_t)ysb * J.xnsb + xsb]);
-        do_level_decn(L, J, xsb, ysb, 1);
-        if (__ldcg(&J.sbcost[(size_t)ysb * J.xnsb + xsb]) <= old) do_level_decn(L, J, xsb, ysb, 0);
-        if ((threadIdx.x & 31) == 0) publish(&J.flags[s]);
-        __syncwarp();
+        __syncthreads();
+        // ---- level 2: the 16 block costs in raster order ----
+        const LevelData& blk = J.lev[2];
+        float c2 = 0.0f;
+        for (int j = 0; j < 4; ++j)
+            for (int i = 0; i < 4; ++i) c2 += __ldcg(&J.bcost[(size_t)((ysb << 2) + j) * blk.xnb + (xsb << 2) + i]);
+        // ---- level 1: sub-superblock (2 xsb + (warp & 1), 2 ysb + (warp >> 1)) per warp ----
+        {
+            const int i = (xsb << 1) + (warp & 1), j = (ysb << 1) + (warp >> 1);
+            do_me(L, J, i, j, 1);
+            const float c = do_unit_decn(L, J, i, j, 1);
+            if (lane == 0) s_cost[warp] = c;
+        }
+        __syncthreads();
+        float sb_cur = c2;
+        if (threadIdx.x == 0) {
+            const float c1 = ((s_cost[0] + s_cost[1]) + s_cost[2]) + s_cost[3];
+            const size_t sb = (size_t)s;
+            J.split[sb] = 2;
+            J.sbcost[sb] = c2;
+            if (c1 <= c2) {
+                propagate_level(L, J, xsb, ysb, 1, c1);
+                sb_cur = c1;
+            }
+            s_cost[0] = sb_cur;
+        }
+        __syncthreads();
+        sb_cur = s_cost[0];
+        // ---- level 0: the whole superblock as one unit (always evaluated: sb_cur <= c2) ----
+        if (sb_cur <= c2) {
+            const LevelData& me = J.lev[0];
+            const LevelData& guide = J.lev[1];
+            const size_t k = (size_t)ysb * me.xnb + xsb;
+            const float lambda = me.lambda[k];
+            const Blim bl = block_limits(L.lb[0], J.pw, J.ph, xsb, ysb);
+            const int xb = xsb << 2, yb = ysb << 2;
+            short2 cand[2][4];
+            int ncand[2];
+            for (int r = 0; r < L.nref; ++r) {
+                int nc = 0;
+                for (int jj = 0; jj < 2; ++jj)
+                    for (int ii = 0; ii < 2; ++ii) {
+                        const short2 v = __ldcg(&guide.mv[r][(size_t)((ysb << 1) + jj) * guide.xnb + (xsb << 1) + ii]);
+                        bool dup = false;
+                        for (int q = 0; q < nc; ++q) dup |= (cand[r][q].x == v.x && cand[r][q].y == v.y);
+                        if (!dup) cand[r][nc++] = v;
+                    }
+                ncand[r] = nc;
+                const short2* bv = blk.mv[r];
+                const int W = blk.xnb;
+                short2 pr = make_short2(0, 0);
+                if (xb > 0 && yb > 0)
+                    pr = mv_median3(__ldcg(&bv[(size_t)yb * W + xb - 1]), __ldcg(&bv[(size_t)(yb - 1) * W + xb - 1]),
+                                    __ldcg(&bv[(size_t)(yb - 1) * W + xb]));
+                else if (xb == 0 && yb > 0)
+                    pr = mv_mean(__ldcg(&bv[(size_t)(yb - 1) * W + xb]), __ldcg(&bv[(size_t)(yb - 1) * W + xb + 1]));
+                else if (xb > 0 && yb == 0)
+                    pr = mv_mean(__ldcg(&bv[(size_t)yb * W + xb - 1]), __ldcg(&bv[(size_t)(yb + 1) * W + xb - 1]));
+                // warp q evaluates candidate q (BlockMatcher::FindBestMatchSubp's loop body)
+                if (warp < nc && bl.xl > 0 && bl.yl > 0) {
+                    const float mvcost = (float)getvarup(pr, cand[r][warp].x, cand[r][warp].y);
+                    const float sum = subpel_cost(J.pic, J.pw, J.up[r], 2 * J.pw, 2 * J.ph, L.prec, bl,
+                                                  cand[r][warp].x, cand[r][warp].y, mvcost * lambda);
+                    if (lane == 0) {
+                        s_sum[r][warp] = sum;
+                        s_mvc[r][warp] = mvcost;
+                    }
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                for (int r = 0; r < L.nref; ++r) {
+                    Cost3 best{me.cost[r][3 * k], me.cost[r][3 * k + 1], 100000000.0f};
+                    short2 bmv = me.mv[r][k];
+                    for (int q = 0; q < ncand[r]; ++q) {
+                        if (bl.xl <= 0 || bl.yl <= 0) break;
+                        const float sum = s_sum[r][q], mvcost = s_mvc[r][q];
+                        if (sum < best.total) {
+                            bmv = cand[r][q];
+                            best.total = sum;
+                            best.mvcost = mvcost;
+                            best.SAD = sum - mvcost * lambda;
+                        }
+                    }
+                    me.mv[r][k] = bmv;
+                    me.cost[r][3 * k] = best.SAD;
+                    me.cost[r][3 * k + 1] = best.mvcost;
+                    me.cost[r][3 * k + 2] = best.total;
+                }
+            }
+            __syncthreads();
+            float bsad = -1.0f;
+            if (L.nref > 1) {
+                const int n = bl.xl * bl.yl;
+                const int per = ((n + WARPS_PER_CTA - 1) / WARPS_PER_CTA + 31) / 32 * 32;
+                const int part = bi_sad_range(J.pic, J.pw, J.up[0], J.up[1], 2 * J.pw, 2 * J.ph, L.prec, bl,
+                                              __ldcg(&me.mv[0][k]), __ldcg(&me.mv[1][k]), warp * per,
+                                              min(n, (warp + 1) * per));
+                if (lane == 0) s_bi[warp] = part;
+                __syncthreads();
+                bsad = (float)(s_bi[0] + s_bi[1] + s_bi[2] + s_bi[3]);
+            }
+            if (warp == 0) {
+                const float c0 = do_unit_decn(L, J, xsb, ysb, 0, bsad);
+                if (lane == 0 && c0 <= sb_cur) propagate_level(L, J, xsb, ysb, 0, c0);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) publish(&J.flags[s]);
     }
 }
 
@@ -1023,6 +1195,7 @@ struct TaskBufs {
     uint8_t* lmode[2];
     int16_t* ldcy[2];
     int16_t* dctmp;      // block DCs of the three components
+    float* bcost;        // level-2 mode-decision costs per block
 };
 
 size_t pic_layout(const MeGeometry& g, PicBufs& P, Arena& a, bool need_up) {
@@ -1057,6 +1230,7 @@ size_t task_layout(const MeGeometry& g, TaskBufs& T, Arena& a) {
         T.ldcy[lv] = a.take<int16_t>(n);
     }
     T.dctmp = a.take<int16_t>(3 * nb);
+    T.bcost = a.take<float>(nb);
     return a.used;
 }
 
@@ -1381,6 +1555,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                     J.xnsb = g.xnsb;
                     J.ynsb = g.ynsb;
                     J.flags = T[t].flags;
+                    J.bcost = T[t].bcost;
                     DGPU_CHECK_CUDA(cudaMemsetAsync(J.flags, 0, sizeof(int) * g.xnsb * g.ynsb, st));
                     jobs.push_back(J);
                 }
@@ -1390,11 +1565,19 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                                                 cudaMemcpyHostToDevice, st));
                 M.nref = want_nref;
                 M.jobs = tabs.mode + first;
+                // level 2 for every block of every job, then the superblock wavefront
+                M.total = (int)nb * nj;
+                mode_blocks_kernel<<<(M.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, 0, st>>>(M, (int)nb);
+                DGPU_CHECK_LAUNCH();
                 M.total = g.xnsb * g.ynsb * nj;
                 M.wave = wave_of(g.depth + 1, g.xnsb, 1, nj);
                 M.wave.T = (g.xnsb - 1) + (g.ynsb - 1) + 1;
-                const int rc = launch_wavefront(M, mode_wavefront_kernel, ctl, st);
-                if (rc) return rc;
+                M.ticket = ctl;
+                M.err = ctl + 1;
+                DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
+                const int grid = std::min(M.total, 148 * 8);
+                mode_wavefront_kernel<<<grid, ME_THREADS, 0, st>>>(M);
+                DGPU_CHECK_LAUNCH();
             }
             // ---- DC values of all three components ----
             {
