@@ -250,25 +250,6 @@ struct PixWalk {
     }
 };
 
-// Integer SAD of one candidate against a same-size plane, coordinates clamped
-// (PelBlockDiff, me_utils.cpp:138-282).  Warp-reduced.
-__device__ int pel_sad(const int16_t* pic, const int16_t* ref, int pw, int ph, const Blim& b, short2 mv) {
-    if (b.xl <= 0 || b.yl <= 0) return 0;
-    const int lane = threadIdx.x & 31;
-    const int n = b.xl * b.yl;
-    PixWalk w(b.xl);
-    int s = 0;
-#pragma unroll 8
-    for (int k = lane; k < n; k += 32) {
-        const int x = b.xp + w.col, y = b.yp + w.row;
-        const int rx = clampi(x + mv.x, 0, pw - 1);
-        const int ry = clampi(y + mv.y, 0, ph - 1);
-        s += abs((int)(int16_t)(pic[(size_t)y * pw + x] - ref[(size_t)ry * pw + rx]));
-        w.next();
-    }
-    return __reduce_add_sync(0xffffffffu, s);
-}
-
 // Prediction sample from an upconverted reference (uw x uh) at precision p (1 half,
 // 2 quarter, 3 eighth), coordinates clamped to the array (me_utils.cpp:410-1170).
 __device__ __forceinline__ int up_at(const int16_t* up, int uw, int uh, int yy, int xx) {
@@ -309,6 +290,79 @@ __device__ float subpel_cost(const int16_t* pic, int pw, const int16_t* up, int 
                 const int x = b.xp + w.col, y = b.yp + w.row;
                 d[s] = abs(up_pred(up, uw, uh, p, x, y, mx, my) - pic[(size_t)y * pw + x]);
             }
+            tot += d[s];
+            w.next();
+        }
+        tot = __reduce_add_sync(0xffffffffu, tot);
+        if (f.c + (double)tot < f.bound) {
+            f.c += (double)tot;
+        } else {
+#pragma unroll
+            for (int s = 0; s < 8; ++s) float_seq_add(f, d[s]);
+        }
+    }
+    return (float)f.c;
+}
+
+// A block staged in shared memory for the sub-pel search around its pel vector (mvx, mvy):
+// the block's picture samples and the upconverted reference window that every candidate
+// within +-(2^prec - 1) of (mvx, mvy) << prec reads (prec 1..3): up rows and columns
+// 2 (yp + mvy) - 2 .. 2 (yp + yl + mvy) and likewise for x, each coordinate clamped to the
+// array as up_at does, so reads need no clamping.
+struct SubWin {
+    int16_t* pic;  // xl * yl, raster order
+    int16_t* up;   // (2 yl + 3) rows x (2 xl + 3) columns
+    int ww, wx0, wy0;
+};
+
+__device__ __forceinline__ int win_pred(const SubWin& S, int p, int x, int y, int mx, int my) {
+    if (p == 1) return S.up[(2 * y + my - S.wy0) * S.ww + 2 * x + mx - S.wx0];
+    if (p == 2) {
+        const int rx = mx & 1, ry = my & 1;
+        const int16_t* q = S.up + (2 * y + (my >> 1) - S.wy0) * S.ww + 2 * x + (mx >> 1) - S.wx0;
+        return ((2 - rx) * (2 - ry) * q[0] + rx * (2 - ry) * q[1] + (2 - rx) * ry * q[S.ww] + rx * ry * q[S.ww + 1] +
+                2) >> 2;
+    }
+    const int rx = mx & 3, ry = my & 3;
+    const int16_t* q = S.up + (2 * y + (my >> 2) - S.wy0) * S.ww + 2 * x + (mx >> 2) - S.wx0;
+    return ((4 - rx) * (4 - ry) * q[0] + rx * (4 - ry) * q[1] + (4 - rx) * ry * q[S.ww] + rx * ry * q[S.ww + 1] + 8) >>
+           4;
+}
+
+__device__ void stage_subwin(SubWin& S, int16_t* mem, const int16_t* pic, int pw, const int16_t* up, int uw, int uh,
+                             const Blim& b, short2 mv) {
+    const int lane = threadIdx.x & 31;
+    S.pic = mem;
+    S.up = mem + b.xl * b.yl;
+    S.ww = 2 * b.xl + 3;
+    S.wx0 = 2 * (b.xp + mv.x) - 2;
+    S.wy0 = 2 * (b.yp + mv.y) - 2;
+    const int wh = 2 * b.yl + 3;
+    for (int i = lane; i < b.xl * b.yl; i += 32) {
+        const int r = i / b.xl;
+        S.pic[i] = pic[(size_t)(b.yp + r) * pw + b.xp + i - r * b.xl];
+    }
+    for (int i = lane; i < wh * S.ww; i += 32) {
+        const int r = i / S.ww;
+        S.up[i] = up[(size_t)clampi(S.wy0 + r, 0, uh - 1) * uw + clampi(S.wx0 + i - r * S.ww, 0, uw - 1)];
+    }
+    __syncwarp();
+}
+
+// subpel_cost over a staged block (same arithmetic and order).
+__device__ float subpel_cost_win(const SubWin& S, int p, const Blim& b, int mx, int my, float start) {
+    const int lane = threadIdx.x & 31;
+    FloatSeq f = float_seq_start(start);
+    const int n = b.xl * b.yl;
+    PixWalk w(b.xl);
+    for (int k0 = 0; k0 < n; k0 += 256) {
+        int d[8];
+        int tot = 0;
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            d[s] = 0;
+            const int k = k0 + 32 * s + lane;
+            if (k < n) d[s] = abs(win_pred(S, p, b.xp + w.col, b.yp + w.row, mx, my) - S.pic[k]);
             tot += d[s];
             w.next();
         }
@@ -418,6 +472,7 @@ struct PelJob {
 // All jobs of a launch share one block grid (xnb x ynb = per_job units).
 struct PelLaunch {
     int total, per_job;
+    int win_elems;          // int16 elements of shared memory per warp (block + search window)
     Olb o;
     int* ticket;
     int* err;
@@ -425,8 +480,73 @@ struct PelLaunch {
     Wave wave;
 };
 
+// Best candidate of one list (BlockMatcher::FindBestMatchPel over the list, PelBlockDiff::Diff
+// per candidate): the block and the reference window the list covers (coordinates clamped as
+// BChk does) are copied to the warp's shared memory, then groups of G lanes each take one
+// candidate (G = the largest power of two with 2 G n <= 32, so small lists still use most
+// lanes).  The list's minimum with the earliest index replaces (best, bmv) only when strictly
+// smaller: the same result as the reference's sequential strict-< scan.
+__device__ void pel_list_best(const int16_t* pic, const int16_t* ref, int pw, int ph, const Blim& b, short2 centre,
+                              int r, int16_t* mem, int& best, short2& bmv) {
+    const int lane = threadIdx.x & 31;
+    const int ww = b.xl + 2 * r, wh = b.yl + 2 * r;
+    int16_t* blk = mem;
+    int16_t* win = mem + b.xl * b.yl;
+    for (int i = lane; i < b.xl * b.yl; i += 32) {
+        const int row = i / b.xl;
+        blk[i] = pic[(size_t)(b.yp + row) * pw + b.xp + i - row * b.xl];
+    }
+    const int wx0 = b.xp + centre.x - r, wy0 = b.yp + centre.y - r;
+    for (int i = lane; i < ww * wh; i += 32) {
+        const int row = i / ww;
+        win[i] = ref[(size_t)clampi(wy0 + row, 0, ph - 1) * pw + clampi(wx0 + i - row * ww, 0, pw - 1)];
+    }
+    __syncwarp();
+    const int n = (2 * r + 1) * (2 * r + 1);
+    int G = 1;
+    while (G * 2 * n <= 32) G <<= 1;
+    const int per_round = 32 / G;
+    const int g = lane & (G - 1);
+    int my_best = INT_MAX, my_k = INT_MAX;
+    for (int k0 = 0; k0 < n; k0 += per_round) {
+        const int k = k0 + lane / G;
+        int sad = 0;
+        if (k < n) {
+            const short2 c = cand_at(centre, r, k);
+            const int dx = c.x - centre.x + r, dy = c.y - centre.y + r;
+            for (int y = g; y < b.yl; y += G) {
+                const int16_t* pr = blk + y * b.xl;
+                const int16_t* wr = win + (y + dy) * ww + dx;
+#pragma unroll 4
+                for (int x = 0; x < b.xl; ++x) sad += abs((int)(int16_t)(pr[x] - wr[x]));
+            }
+        }
+        for (int o = 1; o < G; o <<= 1) sad += __shfl_xor_sync(0xffffffffu, sad, o);
+        if (k < n && g == 0 && sad < my_best) {
+            my_best = sad;
+            my_k = k;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const int ob = __shfl_xor_sync(0xffffffffu, my_best, o);
+        const int ok = __shfl_xor_sync(0xffffffffu, my_k, o);
+        if (ob < my_best || (ob == my_best && ok < my_k)) {
+            my_best = ob;
+            my_k = ok;
+        }
+    }
+    if (my_best < best) {
+        best = my_best;
+        bmv = cand_at(centre, r, my_k);
+    }
+    __syncwarp();
+}
+
 // Parallel phase: the zero-centred and the guide-centred lists of every block.
 __global__ void __launch_bounds__(ME_THREADS) pel_lists_kernel(const __grid_constant__ PelLaunch L) {
+    extern __shared__ __align__(16) int16_t pel_smem[];
+    int16_t* const wmem = pel_smem + (size_t)(threadIdx.x >> 5) * L.win_elems;
     const int u = blockIdx.x * WARPS_PER_CTA + (threadIdx.x >> 5);
     if (u >= L.total) return;
     const int jn = u / L.per_job;
@@ -437,27 +557,12 @@ __global__ void __launch_bounds__(ME_THREADS) pel_lists_kernel(const __grid_cons
     int best = INT_MAX;
     short2 bmv = make_short2(0, 0);
     if (bl.xl > 0 && bl.yl > 0) {
-        const int n = (2 * J.radius + 1) * (2 * J.radius + 1);
-        for (int k = 0; k < n; ++k) {
-            const short2 c = cand_at(make_short2(0, 0), J.radius, k);
-            const int s = pel_sad(J.pic, J.ref, J.pw, J.ph, bl, c);
-            if (s < best) {
-                best = s;
-                bmv = c;
-            }
-        }
+        pel_list_best(J.pic, J.ref, J.pw, J.ph, bl, make_short2(0, 0), J.radius, wmem, best, bmv);
         if (J.guide) {
             const int gx = clampi(bx >> 1, 0, J.gxnb - 1), gy = clampi(by >> 1, 0, J.gynb - 1);
-            const short2 g = J.guide[(size_t)gy * J.gxnb + gx];
-            const short2 g2 = make_short2((short)(g.x * 2), (short)(g.y * 2));
-            for (int k = 0; k < n; ++k) {
-                const short2 c = cand_at(g2, J.radius, k);
-                const int s = pel_sad(J.pic, J.ref, J.pw, J.ph, bl, c);
-                if (s < best) {
-                    best = s;
-                    bmv = c;
-                }
-            }
+            const short2 gv = J.guide[(size_t)gy * J.gxnb + gx];
+            pel_list_best(J.pic, J.ref, J.pw, J.ph, bl, make_short2((short)(gv.x * 2), (short)(gv.y * 2)), J.radius,
+                          wmem, best, bmv);
         }
     }
     if ((threadIdx.x & 31) == 0) {
@@ -469,6 +574,8 @@ __global__ void __launch_bounds__(ME_THREADS) pel_lists_kernel(const __grid_cons
 // Wavefront phase: raster predictor, predictor-centred list, final vectors and costs
 // (PixelMatcher::MatchPic / DoBlock, BlockMatcher::FindBestMatchPel).
 __global__ void __launch_bounds__(ME_THREADS) pel_wavefront_kernel(const __grid_constant__ PelLaunch L) {
+    extern __shared__ __align__(16) int16_t pel_smem[];
+    int16_t* const wmem = pel_smem + (size_t)(threadIdx.x >> 5) * L.win_elems;
     for (;;) {
         const int u = warp_ticket(L.ticket);
         if (u >= L.total) return;
@@ -498,15 +605,7 @@ __global__ void __launch_bounds__(ME_THREADS) pel_wavefront_kernel(const __grid_
         short2 bmv = J.best_mv[b];
         float sad;
         if (bl.xl > 0 && bl.yl > 0) {
-            const int n = (2 * J.radius + 1) * (2 * J.radius + 1);
-            for (int k = 0; k < n; ++k) {
-                const short2 c = cand_at(pred, J.radius, k);
-                const int s = pel_sad(J.pic, J.ref, J.pw, J.ph, bl, c);
-                if (s < best) {
-                    best = s;
-                    bmv = c;
-                }
-            }
+            pel_list_best(J.pic, J.ref, J.pw, J.ph, bl, pred, J.radius, wmem, best, bmv);
             sad = (float)best;
         } else {
             bmv = make_short2(0, 0);
@@ -540,6 +639,7 @@ struct SubJob {
 
 struct SubLaunch {
     int total, prec;
+    int win_elems;       // int16 elements of shared memory per warp for SubWin; 0: no staging
     Olb o;
     int* ticket;
     int* err;
@@ -565,7 +665,21 @@ __device__ __forceinline__ void try_cand(const SubJob& J, int p, const Blim& bl,
     }
 }
 
+__device__ __forceinline__ void try_cand_win(const SubWin& S, int p, const Blim& bl, short2 c, float mvcost,
+                                             float lambda, Cost3& best, short2& best_mv) {
+    const float start = mvcost * lambda;
+    const float sum = subpel_cost_win(S, p, bl, c.x, c.y, start);
+    if (sum < best.total) {
+        best_mv = c;
+        best.total = sum;
+        best.mvcost = mvcost;
+        best.SAD = sum - start;
+    }
+}
+
 __global__ void __launch_bounds__(ME_THREADS) subpel_wavefront_kernel(const __grid_constant__ SubLaunch L) {
+    extern __shared__ __align__(16) int16_t sub_smem[];
+    int16_t* const wmem = sub_smem + (size_t)(threadIdx.x >> 5) * L.win_elems;
     const int prec = L.prec;
     for (;;) {
         const int u = warp_ticket(L.ticket);
@@ -613,27 +727,33 @@ __global__ void __launch_bounds__(ME_THREADS) subpel_wavefront_kernel(const __gr
                 Cost3 best = cost;
                 short2 bmv = mv;
                 bool bailed = false;
+                // candidates stay within +-(2^prec - 1) of mv << prec: stage that window once
+                const bool staged = L.win_elems > 0 && bl.xl > 0 && bl.yl > 0;
+                SubWin S{};
+                if (staged) stage_subwin(S, wmem, J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, bl, mv);
+                auto cand = [&](int i, short2 c, int sh, short2& tb) {
+                    const float mvc = (float)getvarup(pred, c.x << sh, c.y << sh);
+                    if (staged) {
+                        try_cand_win(S, i, bl, c, mvc, lambda, best, tb);
+                    } else {
+                        try_cand(J, i, bl, c, mvc, lambda, best, tb);
+                    }
+                };
                 for (int i = 1; i <= prec; ++i) {
                     bmv = make_short2((short)(bmv.x << 1), (short)(bmv.y << 1));
                     short2 tb = bmv;
                     const int sh = prec - i;
                     const short2 c4[4] = {make_short2(bmv.x - 1, bmv.y), make_short2(bmv.x + 1, bmv.y),
                                           make_short2(bmv.x, bmv.y - 1), make_short2(bmv.x, bmv.y + 1)};
-                    for (int q = 0; q < 4; ++q)
-                        try_cand(J, i, bl, c4[q], (float)getvarup(pred, c4[q].x << sh, c4[q].y << sh), lambda, best,
-                                 tb);
+                    for (int q = 0; q < 4; ++q) cand(i, c4[q], sh, tb);
                     if (tb.x != bmv.x) {
                         const short2 nb = tb;
                         const short2 c2[2] = {make_short2(nb.x, nb.y - 1), make_short2(nb.x, nb.y + 1)};
-                        for (int q = 0; q < 2; ++q)
-                            try_cand(J, i, bl, c2[q], (float)getvarup(pred, c2[q].x << sh, c2[q].y << sh), lambda,
-                                     best, tb);
+                        for (int q = 0; q < 2; ++q) cand(i, c2[q], sh, tb);
                     } else if (tb.y != bmv.y) {
                         const short2 nb = tb;
                         const short2 c2[2] = {make_short2(nb.x - 1, nb.y), make_short2(nb.x + 1, nb.y)};
-                        for (int q = 0; q < 2; ++q)
-                            try_cand(J, i, bl, c2[q], (float)getvarup(pred, c2[q].x << sh, c2[q].y << sh), lambda,
-                                     best, tb);
+                        for (int q = 0; q < 2; ++q) cand(i, c2[q], sh, tb);
                     }
                     bmv = tb;
                     if ((double)best.total > 1.1 * (double)pc.total) {
@@ -1415,11 +1535,24 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
         L.jobs = dj;
         L.wave = wave_of(l, g.xnb[l], 2, (int)jobs.size());
         L.wave.T = (g.xnb[l] - 1) + 2 * (g.ynb[l] - 1) + 1;
+        // per-warp shared memory: the block and its search window (radius <= 5)
+        const int xl = g.lb[2].xblen, yl = g.lb[2].yblen, rr = std::min(l + 1, 5);
+        L.win_elems = (int)align_up((size_t)xl * yl + (size_t)(xl + 2 * rr) * (yl + 2 * rr), 8);
+        const size_t smem = (size_t)L.win_elems * 2 * WARPS_PER_CTA;
+        if (smem > 48 * 1024) {
+            DGPU_CHECK_CUDA(cudaFuncSetAttribute(pel_lists_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            DGPU_CHECK_CUDA(
+                cudaFuncSetAttribute(pel_wavefront_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        }
         // the candidate-list phase covers every unit: one warp per unit
-        pel_lists_kernel<<<(L.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, 0, st>>>(L);
+        pel_lists_kernel<<<(L.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, smem, st>>>(L);
         DGPU_CHECK_LAUNCH();
-        const int rc = launch_wavefront(L, pel_wavefront_kernel, ctl, st);
-        if (rc) return rc;
+        L.ticket = ctl;
+        L.err = ctl + 1;
+        DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
+        pel_wavefront_kernel<<<std::min((L.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, 148 * 8), ME_THREADS, smem,
+                               st>>>(L);
+        DGPU_CHECK_LAUNCH();
     }
     int err_host = 0;
     if (A.stages >= 2) {
@@ -1482,8 +1615,16 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
             S.jobs = tabs.sub;
             S.wave = wave_of(0, g.xnb[0], 2, (int)jobs.size());
             S.wave.T = (g.xnb[0] - 1) + 2 * (g.ynb[0] - 1) + 1;
-            const int rc = launch_wavefront(S, subpel_wavefront_kernel, ctl, st);
-            if (rc) return rc;
+            // per-warp staging of the block and its window when it fits a modest budget
+            const int xl = g.lb[2].xblen, yl = g.lb[2].yblen;
+            const int elems = (int)align_up((size_t)xl * yl + (size_t)(2 * xl + 3) * (2 * yl + 3), 8);
+            S.win_elems = elems * 2 * WARPS_PER_CTA <= 24 * 1024 ? elems : 0;
+            S.ticket = ctl;
+            S.err = ctl + 1;
+            DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
+            const int grid = std::min((S.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, 148 * 8);
+            subpel_wavefront_kernel<<<grid, ME_THREADS, (size_t)S.win_elems * 2 * WARPS_PER_CTA, st>>>(S);
+            DGPU_CHECK_LAUNCH();
         }
         if (A.stages >= 3) {
             const float f0 = (float)(16 * g.lb[2].xblen * g.lb[2].yblen) / (float)(g.lb[0].xblen * g.lb[0].yblen);
