@@ -197,14 +197,31 @@ __device__ __forceinline__ FloatSeq float_seq_start(float start) {
     return f;
 }
 
+// Adds a non-negative integer total to the running sum when no addition of its terms, in any
+// order, can round: either no power of two is crossed, or the current value is a multiple of
+// the float spacing at the final value (then every partial sum, a multiple of that spacing
+// below 2^24, is a float).  Returns false, changing nothing, otherwise.
+__device__ __forceinline__ bool float_seq_add_exact(FloatSeq& f, int total) {
+    const double fin = f.c + (double)total;
+    if (fin < f.bound) {
+        f.c = fin;
+        return true;
+    }
+    if (fin >= 16777216.0) return false;
+    int e;
+    frexp(fin, &e);  // fin in [2^(e-1), 2^e): float spacing 2^(e-24)
+    const double t = ldexp(f.c, 24 - e);
+    if (t != floor(t)) return false;
+    f.c = fin;
+    f.bound = pow2_above(fin);
+    return true;
+}
+
 // Adds one term per lane (lane order = raster order; lanes without a term pass 0).
 __device__ __forceinline__ void float_seq_add(FloatSeq& f, int d) {
     const int lane = threadIdx.x & 31;
     const int total = __reduce_add_sync(0xffffffffu, d);
-    if (f.c + (double)total < f.bound) {  // no power of two crossed: every addition exact
-        f.c += (double)total;
-        return;
-    }
+    if (float_seq_add_exact(f, total)) return;
     int pre = d;  // inclusive prefix over lanes
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -294,14 +311,37 @@ __device__ float subpel_cost(const int16_t* pic, int pw, const int16_t* up, int 
             w.next();
         }
         tot = __reduce_add_sync(0xffffffffu, tot);
-        if (f.c + (double)tot < f.bound) {
-            f.c += (double)tot;
-        } else {
+        if (!float_seq_add_exact(f, tot)) {
 #pragma unroll
             for (int s = 0; s < 8; ++s) float_seq_add(f, d[s]);
         }
     }
     return (float)f.c;
+}
+
+// Copies the h x w region at (x0, y0) of a pw x ph plane into shared memory (rows of w),
+// coordinates clamped to the plane; each lane keeps eight loads in flight before storing.
+__device__ __forceinline__ void stage_rect(int16_t* dst, const int16_t* __restrict__ src, int pw, int ph, int x0,
+                                           int y0, int w, int h) {
+    const int lane = threadIdx.x & 31;
+    const int n = w * h;
+    for (int i0 = 0; i0 < n; i0 += 256) {
+        int16_t v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int i = i0 + 32 * k + lane;
+            v[k] = 0;
+            if (i < n) {
+                const int r = i / w;
+                v[k] = __ldg(&src[(size_t)clampi(y0 + r, 0, ph - 1) * pw + clampi(x0 + i - r * w, 0, pw - 1)]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int i = i0 + 32 * k + lane;
+            if (i < n) dst[i] = v[k];
+        }
+    }
 }
 
 // A block staged in shared memory for the sub-pel search around its pel vector (mvx, mvy):
@@ -331,21 +371,14 @@ __device__ __forceinline__ int win_pred(const SubWin& S, int p, int x, int y, in
 
 __device__ void stage_subwin(SubWin& S, int16_t* mem, const int16_t* pic, int pw, const int16_t* up, int uw, int uh,
                              const Blim& b, short2 mv) {
-    const int lane = threadIdx.x & 31;
     S.pic = mem;
     S.up = mem + b.xl * b.yl;
     S.ww = 2 * b.xl + 3;
     S.wx0 = 2 * (b.xp + mv.x) - 2;
     S.wy0 = 2 * (b.yp + mv.y) - 2;
     const int wh = 2 * b.yl + 3;
-    for (int i = lane; i < b.xl * b.yl; i += 32) {
-        const int r = i / b.xl;
-        S.pic[i] = pic[(size_t)(b.yp + r) * pw + b.xp + i - r * b.xl];
-    }
-    for (int i = lane; i < wh * S.ww; i += 32) {
-        const int r = i / S.ww;
-        S.up[i] = up[(size_t)clampi(S.wy0 + r, 0, uh - 1) * uw + clampi(S.wx0 + i - r * S.ww, 0, uw - 1)];
-    }
+    stage_rect(S.pic, pic, pw, 1 << 30, b.xp, b.yp, b.xl, b.yl);
+    stage_rect(S.up, up, uw, uh, S.wx0, S.wy0, S.ww, wh);
     __syncwarp();
 }
 
@@ -367,9 +400,7 @@ __device__ float subpel_cost_win(const SubWin& S, int p, const Blim& b, int mx, 
             w.next();
         }
         tot = __reduce_add_sync(0xffffffffu, tot);
-        if (f.c + (double)tot < f.bound) {
-            f.c += (double)tot;
-        } else {
+        if (!float_seq_add_exact(f, tot)) {
 #pragma unroll
             for (int s = 0; s < 8; ++s) float_seq_add(f, d[s]);
         }
@@ -492,15 +523,8 @@ __device__ void pel_list_best(const int16_t* pic, const int16_t* ref, int pw, in
     const int ww = b.xl + 2 * r, wh = b.yl + 2 * r;
     int16_t* blk = mem;
     int16_t* win = mem + b.xl * b.yl;
-    for (int i = lane; i < b.xl * b.yl; i += 32) {
-        const int row = i / b.xl;
-        blk[i] = pic[(size_t)(b.yp + row) * pw + b.xp + i - row * b.xl];
-    }
-    const int wx0 = b.xp + centre.x - r, wy0 = b.yp + centre.y - r;
-    for (int i = lane; i < ww * wh; i += 32) {
-        const int row = i / ww;
-        win[i] = ref[(size_t)clampi(wy0 + row, 0, ph - 1) * pw + clampi(wx0 + i - row * ww, 0, pw - 1)];
-    }
+    stage_rect(blk, pic, pw, ph, b.xp, b.yp, b.xl, b.yl);
+    stage_rect(win, ref, pw, ph, b.xp + centre.x - r, b.yp + centre.y - r, ww, wh);
     __syncwarp();
     const int n = (2 * r + 1) * (2 * r + 1);
     int G = 1;
