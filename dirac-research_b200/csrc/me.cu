@@ -44,7 +44,7 @@ namespace {
 
 constexpr int WARPS_PER_CTA = 4;
 constexpr int ME_THREADS = 32 * WARPS_PER_CTA;
-constexpr long long SPIN_LIMIT = 1LL << 24;  // about 2 s of polling with __nanosleep(100)
+constexpr long long SPIN_LIMIT = 1LL << 21;  // about 2 s of polling at the longest back-off
 
 struct Olb {
     int xblen, yblen, xbsep, ybsep, xoff, yoff;
@@ -133,12 +133,16 @@ __device__ __forceinline__ void wait_flag(int* flag, int* err) {
     cuda::atomic_ref<int, cuda::thread_scope_device> f(*flag);
     cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
     long long n = 0;
+    unsigned ns = 32;
     while (f.load(cuda::memory_order_acquire) == 0) {
         if (++n > SPIN_LIMIT || ((n & 1023) == 0 && e.load(cuda::memory_order_relaxed) != 0)) {
             atomicOr(err, 1);
             return;
         }
-        __nanosleep(100);
+        // back off (up to ~1 us) so that warps waiting far ahead of the wavefront take few
+        // issue slots from the ones working on it
+        __nanosleep(ns);
+        if (ns < 1024) ns <<= 1;
     }
 }
 
@@ -829,10 +833,11 @@ struct ModeJob {
     int xnsb, ynsb;
     int* flags;          // per superblock
     float* bcost;        // level-2 (block) decision costs, from mode_blocks_kernel
+    int nref;            // references of this picture (1 or 2)
 };
 
 struct ModeLaunch {
-    int total, nref, prec;
+    int total, prec;
     Olb lb[3];
     float level_factor[3];
     int* ticket;
@@ -851,7 +856,7 @@ __device__ void do_me(const ModeLaunch& L, const ModeJob& J, int x, int y, int l
     const size_t k = (size_t)y * me.xnb + x;
     const float lambda = me.lambda[k];
     const Blim bl = block_limits(L.lb[level], J.pw, J.ph, x, y);
-    for (int r = 0; r < L.nref; ++r) {
+    for (int r = 0; r < J.nref; ++r) {
         short2 c[4];
         int nc = 0;
         for (int j = 0; j < 2; ++j)
@@ -908,7 +913,7 @@ __device__ float do_unit_decn(const ModeLaunch& L, const ModeJob& J, int x, int 
     float min_cost = t1 + mode_cost;
     float best_sad = __ldcg(&me.cost[0][3 * k]);
     float t2 = 0.0f;
-    if (L.nref > 1) {
+    if (J.nref > 1) {
         t2 = __ldcg(&me.cost[1][3 * k + 2]) * f;
         float unit = t2 + mode_cost;
         if (unit < min_cost) {
@@ -943,7 +948,7 @@ __device__ float do_unit_decn(const ModeLaunch& L, const ModeJob& J, int x, int 
     }
     if ((threadIdx.x & 31) == 0) {
         me.cost[0][3 * k + 2] = t1;
-        if (L.nref > 1) me.cost[1][3 * k + 2] = t2;
+        if (J.nref > 1) me.cost[1][3 * k + 2] = t2;
         me.mode[k] = (uint8_t)mode;
         if (set_dc) me.dcy[k] = dc;
     }
@@ -965,7 +970,7 @@ __device__ void propagate_level(const ModeLaunch& L, const ModeJob& J, int xsb, 
         bl.mode[dst] = __ldcg(&lv.mode[src]);
         bl.dcy[dst] = __ldcg(&lv.dcy[src]);
         bl.mv[0][dst] = __ldcg(&lv.mv[0][src]);
-        if (L.nref > 1) bl.mv[1][dst] = __ldcg(&lv.mv[1][src]);
+        if (J.nref > 1) bl.mv[1][dst] = __ldcg(&lv.mv[1][src]);
     }
     const size_t sb = (size_t)ysb * J.xnsb + xsb;
     J.sbcost[sb] = sb_cost;
@@ -1054,7 +1059,7 @@ __global__ void __launch_bounds__(ME_THREADS) mode_wavefront_kernel(const __grid
             const int xb = xsb << 2, yb = ysb << 2;
             short2 cand[2][4];
             int ncand[2];
-            for (int r = 0; r < L.nref; ++r) {
+            for (int r = 0; r < J.nref; ++r) {
                 int nc = 0;
                 for (int jj = 0; jj < 2; ++jj)
                     for (int ii = 0; ii < 2; ++ii) {
@@ -1087,7 +1092,7 @@ __global__ void __launch_bounds__(ME_THREADS) mode_wavefront_kernel(const __grid
             }
             __syncthreads();
             if (threadIdx.x == 0) {
-                for (int r = 0; r < L.nref; ++r) {
+                for (int r = 0; r < J.nref; ++r) {
                     Cost3 best{me.cost[r][3 * k], me.cost[r][3 * k + 1], 100000000.0f};
                     short2 bmv = me.mv[r][k];
                     for (int q = 0; q < ncand[r]; ++q) {
@@ -1108,7 +1113,7 @@ __global__ void __launch_bounds__(ME_THREADS) mode_wavefront_kernel(const __grid
             }
             __syncthreads();
             float bsad = -1.0f;
-            if (L.nref > 1) {
+            if (J.nref > 1) {
                 const int n = bl.xl * bl.yl;
                 const int per = ((n + WARPS_PER_CTA - 1) / WARPS_PER_CTA + 31) / 32 * 32;
                 const int part = bi_sad_range(J.pic, J.pw, J.up[0], J.up[1], 2 * J.pw, 2 * J.ph, L.prec, bl,
@@ -1684,52 +1689,51 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
             std::vector<ModeJob> jobs;
             // one launch per reference count (the kernel takes nref per launch); each launch
             // runs all its pictures' superblock wavefronts together
-            for (int want_nref = 1; want_nref <= 2; ++want_nref) {
-                const size_t first = jobs.size();
-                for (int t = 0; t < A.ntasks; ++t) {
-                    if (nref_of(t) != want_nref) continue;
-                    ModeJob J{};
-                    J.pic = luma(A.task_pic[t]);
-                    J.up[0] = P[ref_of(t, 0)].up;
-                    J.up[1] = P[ref_of(t, 1)].up;
-                    J.pw = g.w;
-                    J.ph = g.h;
-                    for (int lv = 0; lv < 3; ++lv) {
-                        LevelData& D = J.lev[lv];
-                        D.xnb = g.xnb[0] >> (2 - lv);
-                        D.ynb = g.ynb[0] >> (2 - lv);
-                        D.lambda = T[t].lambda[lv];
-                        if (lv == 2) {
-                            D.mv[0] = mv0(t, 0);
-                            D.mv[1] = want_nref > 1 ? mv0(t, 1) : mv0(t, 0);
-                            D.cost[0] = cost0(t, 0);
-                            D.cost[1] = want_nref > 1 ? cost0(t, 1) : cost0(t, 0);
-                            D.mode = A.mode_out[t];
-                            D.dcy = A.dc_out[t];
-                        } else {
-                            D.mv[0] = T[t].lmv[lv][0];
-                            D.mv[1] = T[t].lmv[lv][1];
-                            D.cost[0] = T[t].lcost[lv][0];
-                            D.cost[1] = T[t].lcost[lv][1];
-                            D.mode = T[t].lmode[lv];
-                            D.dcy = T[t].ldcy[lv];
-                        }
+            // every picture's superblock wavefront in one launch (nref per job)
+            for (int t = 0; t < A.ntasks; ++t) {
+                const int want_nref = nref_of(t);
+                ModeJob J{};
+                J.nref = want_nref;
+                J.pic = luma(A.task_pic[t]);
+                J.up[0] = P[ref_of(t, 0)].up;
+                J.up[1] = P[ref_of(t, 1)].up;
+                J.pw = g.w;
+                J.ph = g.h;
+                for (int lv = 0; lv < 3; ++lv) {
+                    LevelData& D = J.lev[lv];
+                    D.xnb = g.xnb[0] >> (2 - lv);
+                    D.ynb = g.ynb[0] >> (2 - lv);
+                    D.lambda = T[t].lambda[lv];
+                    if (lv == 2) {
+                        D.mv[0] = mv0(t, 0);
+                        D.mv[1] = want_nref > 1 ? mv0(t, 1) : mv0(t, 0);
+                        D.cost[0] = cost0(t, 0);
+                        D.cost[1] = want_nref > 1 ? cost0(t, 1) : cost0(t, 0);
+                        D.mode = A.mode_out[t];
+                        D.dcy = A.dc_out[t];
+                    } else {
+                        D.mv[0] = T[t].lmv[lv][0];
+                        D.mv[1] = T[t].lmv[lv][1];
+                        D.cost[0] = T[t].lcost[lv][0];
+                        D.cost[1] = T[t].lcost[lv][1];
+                        D.mode = T[t].lmode[lv];
+                        D.dcy = T[t].ldcy[lv];
                     }
-                    J.sbcost = A.sbcost_out[t];
-                    J.split = A.split_out[t];
-                    J.xnsb = g.xnsb;
-                    J.ynsb = g.ynsb;
-                    J.flags = T[t].flags;
-                    J.bcost = T[t].bcost;
-                    DGPU_CHECK_CUDA(cudaMemsetAsync(J.flags, 0, sizeof(int) * g.xnsb * g.ynsb, st));
-                    jobs.push_back(J);
                 }
-                const int nj = (int)(jobs.size() - first);
-                if (nj == 0) continue;
-                DGPU_CHECK_CUDA(cudaMemcpyAsync(tabs.mode + first, jobs.data() + first, sizeof(ModeJob) * nj,
-                                                cudaMemcpyHostToDevice, st));
-                M.nref = want_nref;
-                M.jobs = tabs.mode + first;
+                J.sbcost = A.sbcost_out[t];
+                J.split = A.split_out[t];
+                J.xnsb = g.xnsb;
+                J.ynsb = g.ynsb;
+                J.flags = T[t].flags;
+                J.bcost = T[t].bcost;
+                DGPU_CHECK_CUDA(cudaMemsetAsync(J.flags, 0, sizeof(int) * g.xnsb * g.ynsb, st));
+                jobs.push_back(J);
+            }
+            {
+                const int nj = (int)jobs.size();
+                DGPU_CHECK_CUDA(cudaMemcpyAsync(tabs.mode, jobs.data(), sizeof(ModeJob) * nj, cudaMemcpyHostToDevice,
+                                                st));
+                M.jobs = tabs.mode;
                 // level 2 for every block of every job, then the superblock wavefront
                 M.total = (int)nb * nj;
                 mode_blocks_kernel<<<(M.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, 0, st>>>(M, (int)nb);
