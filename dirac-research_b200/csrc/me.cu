@@ -292,11 +292,14 @@ __device__ __forceinline__ int up_pred(const int16_t* up, int uw, int uh, int p,
 
 // Float sum, in raster order from start, of |pred - pic| over a block: the cost loop of
 // BlockDiff{Half,Quarter,Eighth}Pel::Diff.  Returns the reference's float result.  Eight
-// steps (256 pixels) are loaded at once; when their total cannot cross a power of two the
-// whole chunk is added exactly in one go, otherwise step by step in raster order.
-__device__ float subpel_cost(const int16_t* pic, int pw, const int16_t* up, int uw, int uh, int p, const Blim& b,
-                             int mx, int my, float start) {
-    if (b.xl <= 0 || b.yl <= 0) return start;
+// steps (256 pixels) are loaded at once; when their total cannot make any addition round,
+// the whole chunk is added in one go, otherwise step by step in raster order.
+// The per-precision bodies are templates; the entry points are kept out of line, so that
+// the wavefront kernels hold one copy of each (their instruction footprint, not their
+// arithmetic, limited them).
+template <int P>
+__device__ __forceinline__ float subpel_cost_p(const int16_t* pic, int pw, const int16_t* up, int uw, int uh,
+                                               const Blim& b, int mx, int my, float start) {
     const int lane = threadIdx.x & 31;
     FloatSeq f = float_seq_start(start);
     const int n = b.xl * b.yl;
@@ -309,7 +312,7 @@ __device__ float subpel_cost(const int16_t* pic, int pw, const int16_t* up, int 
             d[s] = 0;
             if (k0 + 32 * s + lane < n) {
                 const int x = b.xp + w.col, y = b.yp + w.row;
-                d[s] = abs(up_pred(up, uw, uh, p, x, y, mx, my) - pic[(size_t)y * pw + x]);
+                d[s] = abs(up_pred(up, uw, uh, P, x, y, mx, my) - pic[(size_t)y * pw + x]);
             }
             tot += d[s];
             w.next();
@@ -321,6 +324,14 @@ __device__ float subpel_cost(const int16_t* pic, int pw, const int16_t* up, int 
         }
     }
     return (float)f.c;
+}
+
+__device__ __noinline__ float subpel_cost(const int16_t* pic, int pw, const int16_t* up, int uw, int uh, int p,
+                                          const Blim& b, int mx, int my, float start) {
+    if (b.xl <= 0 || b.yl <= 0) return start;
+    if (p == 1) return subpel_cost_p<1>(pic, pw, up, uw, uh, b, mx, my, start);
+    if (p == 2) return subpel_cost_p<2>(pic, pw, up, uw, uh, b, mx, my, start);
+    return subpel_cost_p<3>(pic, pw, up, uw, uh, b, mx, my, start);
 }
 
 // Copies the h x w region at (x0, y0) of a pw x ph plane into shared memory (rows of w),
@@ -359,9 +370,10 @@ struct SubWin {
     int ww, wx0, wy0;
 };
 
-__device__ __forceinline__ int win_pred(const SubWin& S, int p, int x, int y, int mx, int my) {
-    if (p == 1) return S.up[(2 * y + my - S.wy0) * S.ww + 2 * x + mx - S.wx0];
-    if (p == 2) {
+template <int P>
+__device__ __forceinline__ int win_pred(const SubWin& S, int x, int y, int mx, int my) {
+    if (P == 1) return S.up[(2 * y + my - S.wy0) * S.ww + 2 * x + mx - S.wx0];
+    if (P == 2) {
         const int rx = mx & 1, ry = my & 1;
         const int16_t* q = S.up + (2 * y + (my >> 1) - S.wy0) * S.ww + 2 * x + (mx >> 1) - S.wx0;
         return ((2 - rx) * (2 - ry) * q[0] + rx * (2 - ry) * q[1] + (2 - rx) * ry * q[S.ww] + rx * ry * q[S.ww + 1] +
@@ -373,7 +385,7 @@ __device__ __forceinline__ int win_pred(const SubWin& S, int p, int x, int y, in
            4;
 }
 
-__device__ void stage_subwin(SubWin& S, int16_t* mem, const int16_t* pic, int pw, const int16_t* up, int uw, int uh,
+__device__ __noinline__ void stage_subwin(SubWin& S, int16_t* mem, const int16_t* pic, int pw, const int16_t* up, int uw, int uh,
                              const Blim& b, short2 mv) {
     S.pic = mem;
     S.up = mem + b.xl * b.yl;
@@ -387,7 +399,8 @@ __device__ void stage_subwin(SubWin& S, int16_t* mem, const int16_t* pic, int pw
 }
 
 // subpel_cost over a staged block (same arithmetic and order).
-__device__ float subpel_cost_win(const SubWin& S, int p, const Blim& b, int mx, int my, float start) {
+template <int P>
+__device__ __forceinline__ float subpel_cost_win_p(const SubWin& S, const Blim& b, int mx, int my, float start) {
     const int lane = threadIdx.x & 31;
     FloatSeq f = float_seq_start(start);
     const int n = b.xl * b.yl;
@@ -399,7 +412,7 @@ __device__ float subpel_cost_win(const SubWin& S, int p, const Blim& b, int mx, 
         for (int s = 0; s < 8; ++s) {
             d[s] = 0;
             const int k = k0 + 32 * s + lane;
-            if (k < n) d[s] = abs(win_pred(S, p, b.xp + w.col, b.yp + w.row, mx, my) - S.pic[k]);
+            if (k < n) d[s] = abs(win_pred<P>(S, b.xp + w.col, b.yp + w.row, mx, my) - S.pic[k]);
             tot += d[s];
             w.next();
         }
@@ -412,11 +425,17 @@ __device__ float subpel_cost_win(const SubWin& S, int p, const Blim& b, int mx, 
     return (float)f.c;
 }
 
+__device__ __noinline__ float subpel_cost_win(const SubWin& S, int p, const Blim& b, int mx, int my, float start) {
+    if (p == 1) return subpel_cost_win_p<1>(S, b, mx, my, start);
+    if (p == 2) return subpel_cost_win_p<2>(S, b, mx, my, start);
+    return subpel_cost_win_p<3>(S, b, mx, my, start);
+}
+
 // BiBlock*Pel::Diff (me_utils.cpp:1172-1785): |((2 pic - p1) - p2) >> 1| with int16
 // intermediates, summed in float from 0 (exact: integer sums below 2^24).  The eighth-pel
 // version walks the second reference from the first one's integer start position when the
 // second one needs bounds checking (me_utils.cpp:1764-1768); reproduced here.
-__device__ int bi_sad_range(const int16_t* pic, int pw, const int16_t* up1, const int16_t* up2, int uw, int uh,
+__device__ __noinline__ int bi_sad_range(const int16_t* pic, int pw, const int16_t* up1, const int16_t* up2, int uw, int uh,
                             int p, const Blim& b, short2 mv1, short2 mv2, int kb, int ke);
 
 __device__ float bi_cost(const int16_t* pic, int pw, const int16_t* up1, const int16_t* up2, int uw, int uh, int p,
@@ -426,7 +445,7 @@ __device__ float bi_cost(const int16_t* pic, int pw, const int16_t* up1, const i
 }
 
 // Pixels [kb, ke) (raster order) of the bi-prediction SAD; integer, so it splits freely.
-__device__ int bi_sad_range(const int16_t* pic, int pw, const int16_t* up1, const int16_t* up2, int uw, int uh,
+__device__ __noinline__ int bi_sad_range(const int16_t* pic, int pw, const int16_t* up1, const int16_t* up2, int uw, int uh,
                             int p, const Blim& b, short2 mv1, short2 mv2, int kb, int ke) {
     if (b.xl <= 0 || b.yl <= 0 || ke <= kb) return 0;
     int m2x = mv2.x, m2y = mv2.y;
@@ -467,7 +486,7 @@ __device__ int block_dc(const int16_t* pic, int pw, const Blim& b) {
     return (int)(int16_t)(s / n);
 }
 
-__device__ float intra_cost(const int16_t* pic, int pw, const Blim& b, int16_t& dc) {
+__device__ __noinline__ float intra_cost(const int16_t* pic, int pw, const Blim& b, int16_t& dc) {
     if (b.xl <= 0 || b.yl <= 0) {
         dc = 0;
         return 0.0f;
@@ -521,7 +540,7 @@ struct PelLaunch {
 // candidate (G = the largest power of two with 2 G n <= 32, so small lists still use most
 // lanes).  The list's minimum with the earliest index replaces (best, bmv) only when strictly
 // smaller: the same result as the reference's sequential strict-< scan.
-__device__ void pel_list_best(const int16_t* pic, const int16_t* ref, int pw, int ph, const Blim& b, short2 centre,
+__device__ __noinline__ void pel_list_best(const int16_t* pic, const int16_t* ref, int pw, int ph, const Blim& b, short2 centre,
                               int r, int16_t* mem, int& best, short2& bmv) {
     const int lane = threadIdx.x & 31;
     const int ww = b.xl + 2 * r, wh = b.yl + 2 * r;
@@ -679,24 +698,16 @@ struct Cost3 {
     float SAD, mvcost, total;
 };
 
-// One candidate of a BlockDiff*Pel::Diff(..., mvcost, lambda, best_costs, best_mv) call.
-__device__ __forceinline__ void try_cand(const SubJob& J, int p, const Blim& bl, short2 c, float mvcost,
-                                         float lambda, Cost3& best, short2& best_mv) {
+// One candidate of the refinement at precision i: cost from the staged window when there is
+// one, else from global memory; (best, best_mv) updated on a strictly smaller total.
+__device__ __noinline__ void eval_subpel_cand(const SubJob& J, const SubWin& S, bool staged, int i, int sh,
+                                              const Blim& bl, short2 c, short2 pred, float lambda, Cost3& best,
+                                              short2& best_mv) {
+    const float mvcost = (float)getvarup(pred, c.x << sh, c.y << sh);
     if (bl.xl <= 0 || bl.yl <= 0) return;
     const float start = mvcost * lambda;
-    const float sum = subpel_cost(J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, p, bl, c.x, c.y, start);
-    if (sum < best.total) {
-        best_mv = c;
-        best.total = sum;
-        best.mvcost = mvcost;
-        best.SAD = sum - start;
-    }
-}
-
-__device__ __forceinline__ void try_cand_win(const SubWin& S, int p, const Blim& bl, short2 c, float mvcost,
-                                             float lambda, Cost3& best, short2& best_mv) {
-    const float start = mvcost * lambda;
-    const float sum = subpel_cost_win(S, p, bl, c.x, c.y, start);
+    const float sum = staged ? subpel_cost_win(S, i, bl, c.x, c.y, start)
+                             : subpel_cost(J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, i, bl, c.x, c.y, start);
     if (sum < best.total) {
         best_mv = c;
         best.total = sum;
@@ -759,29 +770,27 @@ __global__ void __launch_bounds__(ME_THREADS) subpel_wavefront_kernel(const __gr
                 const bool staged = L.win_elems > 0 && bl.xl > 0 && bl.yl > 0;
                 SubWin S{};
                 if (staged) stage_subwin(S, wmem, J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, bl, mv);
-                auto cand = [&](int i, short2 c, int sh, short2& tb) {
-                    const float mvc = (float)getvarup(pred, c.x << sh, c.y << sh);
-                    if (staged) {
-                        try_cand_win(S, i, bl, c, mvc, lambda, best, tb);
-                    } else {
-                        try_cand(J, i, bl, c, mvc, lambda, best, tb);
-                    }
-                };
                 for (int i = 1; i <= prec; ++i) {
                     bmv = make_short2((short)(bmv.x << 1), (short)(bmv.y << 1));
                     short2 tb = bmv;
                     const int sh = prec - i;
-                    const short2 c4[4] = {make_short2(bmv.x - 1, bmv.y), make_short2(bmv.x + 1, bmv.y),
-                                          make_short2(bmv.x, bmv.y - 1), make_short2(bmv.x, bmv.y + 1)};
-                    for (int q = 0; q < 4; ++q) cand(i, c4[q], sh, tb);
-                    if (tb.x != bmv.x) {
-                        const short2 nb = tb;
-                        const short2 c2[2] = {make_short2(nb.x, nb.y - 1), make_short2(nb.x, nb.y + 1)};
-                        for (int q = 0; q < 2; ++q) cand(i, c2[q], sh, tb);
-                    } else if (tb.y != bmv.y) {
-                        const short2 nb = tb;
-                        const short2 c2[2] = {make_short2(nb.x - 1, nb.y), make_short2(nb.x + 1, nb.y)};
-                        for (int q = 0; q < 2; ++q) cand(i, c2[q], sh, tb);
+                    // the four neighbours, then (after a move) the two across the move
+                    short2 cl[6] = {make_short2(bmv.x - 1, bmv.y), make_short2(bmv.x + 1, bmv.y),
+                                    make_short2(bmv.x, bmv.y - 1), make_short2(bmv.x, bmv.y + 1)};
+                    int nc = 4;
+                    for (int q = 0; q < nc; ++q) {
+                        eval_subpel_cand(J, S, staged, i, sh, bl, cl[q], pred, lambda, best, tb);
+                        if (q == 3) {
+                            if (tb.x != bmv.x) {
+                                cl[4] = make_short2(tb.x, tb.y - 1);
+                                cl[5] = make_short2(tb.x, tb.y + 1);
+                                nc = 6;
+                            } else if (tb.y != bmv.y) {
+                                cl[4] = make_short2(tb.x - 1, tb.y);
+                                cl[5] = make_short2(tb.x + 1, tb.y);
+                                nc = 6;
+                            }
+                        }
                     }
                     bmv = tb;
                     if ((double)best.total > 1.1 * (double)pc.total) {
@@ -847,7 +856,7 @@ struct ModeLaunch {
 };
 
 // ModeDecider::DoME: the unit's four guide vectors as candidates (BlockMatcher::FindBestMatchSubp).
-__device__ void do_me(const ModeLaunch& L, const ModeJob& J, int x, int y, int level) {
+__device__ __noinline__ void do_me(const ModeLaunch& L, const ModeJob& J, int x, int y, int level) {
     const LevelData& me = J.lev[level];
     const LevelData& guide = J.lev[level + 1];
     const LevelData& blk = J.lev[2];
@@ -901,7 +910,7 @@ __device__ void do_me(const ModeLaunch& L, const ModeJob& J, int x, int y, int l
 }
 
 // ModeDecider::DoUnitDecn: best of REF1 / REF2 / bi-prediction / intra for one unit.
-__device__ float do_unit_decn(const ModeLaunch& L, const ModeJob& J, int x, int y, int level, float bsad_in = -1.0f) {
+__device__ __noinline__ float do_unit_decn(const ModeLaunch& L, const ModeJob& J, int x, int y, int level, float bsad_in = -1.0f) {
     const LevelData& me = J.lev[level];
     const size_t k = (size_t)y * me.xnb + x;
     const float lambda = me.lambda[k];
