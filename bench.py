@@ -12,10 +12,12 @@ reference); the encoder keeps the initial entropy-correction factors.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gpu|reference]
 
-`value`: frames/s with the input frames resident in HBM.  `e2e`: the same through the
-encoder's C ABI from pinned host frames, reading back per picture what the host coder needs
-(quantised indices, band choices, code-block skips, motion data).  Every step works on
-about 2 GB of distinct device buffers (far above the 126 MB L2), so no L2 flush is needed.
+`value`: frames/s of the batched form (--streams sequences encoded concurrently on one GPU,
+each by its own encoder, CUDA stream and host thread) with the input frames resident in
+HBM; `plain` gives the same for one sequence at a time.  `e2e`: the batched form through
+the encoder's C ABI from pinned host frames, reading back per picture what the host coder
+needs (quantised indices, band choices, code-block skips, motion data).  Every step works on
+gigabytes of distinct device buffers (far above the 126 MB L2), so no L2 flush is needed.
 Under torchrun each rank encodes its own sequence (replicas, weak scaling, no collective on
 the data path); times are device times, max over ranks.  `--impl reference` times the
 reference encoder itself (its public C API) on this host's cores.
@@ -45,6 +47,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--frames", type=int, default=32)
+    ap.add_argument("--streams", type=int, default=8, help="concurrent sequences per GPU (batched form)")
     ap.add_argument("--impl", choices=["gpu", "reference"], default="gpu")
     return ap.parse_args()
 
@@ -228,10 +231,55 @@ def main():
     from dirac_b200.roofline import stage_bytes
 
     lib = dirac_b200.load()
-    stream = torch.cuda.Stream()
     dev_frames = [tuple(torch.from_numpy(p).cuda() for p in fr) for fr in frames]
+    pinned = [tuple(torch.from_numpy(p).pin_memory() for p in fr) for fr in frames]
+    pinned_np = [tuple(t.numpy() for t in fr) for fr in pinned]
     torch.cuda.synchronize()
-    enc = E.SequenceEncoder(PARAMS, max_pictures=args.frames, stream=stream)
+    items = [(E.QINDEX, c) for c in range(3)] + [(E.BANDS, c) for c in range(3)] + \
+            [(E.CBSKIP, c) for c in range(3)] + [(E.MV, 0), (E.MODE, 0), (E.DC, 0), (E.SPLIT, 0)]
+
+    class Lane:
+        """One sequence encoder on its own CUDA stream (the batched form runs several, each
+        driven by its own host thread)."""
+
+        def __init__(self):
+            self.stream = torch.cuda.Stream()
+            self.enc = E.SequenceEncoder(PARAMS, max_pictures=args.frames, stream=self.stream)
+            self.bufs = {}
+            self.d2h = 0
+
+        def read(self, info):
+            pn = info["pnum"]
+            for what, c in items:
+                n = lib.dgpu_encoder_item_bytes(self.enc.handle, pn, what, c)
+                if n == 0:
+                    continue
+                b = self.bufs.get((what, c, n))
+                if b is None:
+                    b = self.bufs[(what, c, n)] = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+                rc = lib.dgpu_encoder_read(self.enc.handle, pn, what, c, b.data_ptr(), n, 1)
+                if rc:
+                    raise RuntimeError(f"dgpu_encoder_read failed: {rc}")
+                self.d2h += n
+
+        def step(self, src, events=None, with_read=False):
+            enc = self.enc
+            enc.reset()
+            for f in src:
+                enc.load(f)
+            enc.end_sequence()
+            infos = []
+            while True:
+                if events is not None:
+                    e = torch.cuda.Event(enable_timing=True)
+                    e.record(self.stream)
+                    events.append(e)
+                info = enc.code_next()
+                if info is None:
+                    return infos
+                infos.append(info)
+                if with_read:
+                    self.read(info)
 
     def barrier():
         if world > 1:
@@ -244,64 +292,88 @@ def main():
             return float(t.item())
         return ms
 
-    def step(src, events=None, read=None):
-        enc.reset()
-        for f in src:
-            enc.load(f)
-        enc.end_sequence()
-        infos = []
-        while True:
-            if events is not None:
-                e = torch.cuda.Event(enable_timing=True)
-                e.record(stream)
-                events.append(e)
-            info = enc.code_next()
-            if info is None:
-                return infos
-            infos.append(info)
-            if read is not None:
-                read(info)
+    def timed(lanes, src, steps, with_read=False):
+        """Device time (ms) of `steps` sequence encodes on every lane, the lanes running
+        concurrently: a start event on the main stream that every lane stream waits on, and an
+        end event after the main stream has waited on every lane's last work."""
+        from concurrent.futures import ThreadPoolExecutor
 
+        main = torch.cuda.current_stream()
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(main)
+        for ln in lanes:
+            ln.stream.wait_event(e0)
+            ln.d2h = 0
+
+        def run(ln):
+            for _ in range(steps):
+                ln.step(src, with_read=with_read)
+
+        if len(lanes) == 1:
+            run(lanes[0])
+        else:
+            with ThreadPoolExecutor(len(lanes)) as ex:
+                list(ex.map(run, lanes))
+        for ln in lanes:
+            done = torch.cuda.Event()
+            done.record(ln.stream)
+            main.wait_event(done)
+        e1.record(main)
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1))
+
+    lanes = [Lane() for _ in range(args.streams)]
+    plain = lanes[0]
+
+    # ---- warm-up: every lane, both input forms ------------------------------------------------
     for _ in range(args.warmup):
-        infos = step(dev_frames)
-    stream.synchronize()
+        timed(lanes, dev_frames, 1)
+    timed(lanes, pinned_np, 1, with_read=True)
 
-    # ---- timed region: inputs resident in HBM ------------------------------------------------
+    # ---- timed region (batched form): inputs resident in HBM ---------------------------------
     clocks = ClockSampler(local_rank)
     clocks.start()
     time.sleep(0.3)
-    barrier()
-    torch.cuda.synchronize()
     launches0 = lib.dgpu_launch_count()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        step(dev_frames)
-    ev1.record(stream)
-    stream.synchronize()
-    barrier()
+    ms = timed(lanes, dev_frames, args.steps)
     launches = lib.dgpu_launch_count() - launches0
     clk = clocks.stop()
-    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    frames_per_step = args.frames * len(lanes)
     ms_per_step = ms / args.steps
-    value = world * args.frames * args.steps / (ms / 1000.0)
+    value = world * frames_per_step * args.steps / (ms / 1000.0)
 
-    # ---- per-picture latency (device timeline, coding order) ---------------------------------
+    # ---- end to end (batched form) through the C ABI with host buffers -------------------------
+    ems = timed(lanes, pinned_np, args.steps, with_read=True)
+    h2d = sum(p.nbytes for fr in pinned_np for p in fr) * len(lanes)
+    e2e = {"value": world * frames_per_step * args.steps / (ems / 1000.0), "unit": "frames/s",
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": sum(ln.d2h for ln in lanes) // args.steps}
+
+    # ---- plain form: one sequence at a time ----------------------------------------------------
+    pms = timed([plain], dev_frames, args.steps)
+    pems = timed([plain], pinned_np, args.steps, with_read=True)
+    plain_line = {"value": world * args.frames * args.steps / (pms / 1000.0), "ms_per_step": pms / args.steps,
+                  "e2e": world * args.frames * args.steps / (pems / 1000.0), "unit": "frames/s"}
+
+    # ---- per-picture latency of the plain form (device timeline, coding order) ---------------
     lat = []
     for _ in range(max(1, args.steps)):
         evs = []
-        step(dev_frames, events=evs)
-        stream.synchronize()
+        plain.step(dev_frames, events=evs)
+        plain.stream.synchronize()
         lat += [evs[k].elapsed_time(evs[k + 1]) for k in range(len(evs) - 1)]
     lat.sort()
     latency = {"p50": statistics.median(lat), "p99": lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))],
-               "max": lat[-1], "pictures": len(lat)}
+               "max": lat[-1], "pictures": len(lat), "form": "plain"}
 
-    # ---- stage breakdown and the roofline of the dominant stage ------------------------------
+    # ---- stage breakdown (plain form) and the roofline of the dominant stage ------------------
+    enc = plain.enc
     enc.profile(True)
     reps = 2
     for _ in range(reps):
-        infos = step(dev_frames)
+        infos = plain.step(dev_frames)
     prof = enc.profile(False)
     stage_ms = {k: v[0] / reps for k, v in prof.items()}
     alg = stage_bytes(PARAMS, infos)
@@ -323,57 +395,21 @@ def main():
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
                 else "fallback 6650 GB/s (of fallback)",
                 "algorithmic_bytes_per_step": alg, "stages": per_stage,
-                "note": "stage times from CUDA events on the encoder stream in a separate profiled pass"}
-
-    # ---- end to end through the C ABI with host buffers --------------------------------------
-    pinned = [tuple(torch.from_numpy(p).pin_memory() for p in fr) for fr in frames]
-    pinned_np = [tuple(t.numpy() for t in fr) for fr in pinned]
-    items = [(E.QINDEX, c) for c in range(3)] + [(E.BANDS, c) for c in range(3)] + \
-            [(E.CBSKIP, c) for c in range(3)] + [(E.MV, 0), (E.MODE, 0), (E.DC, 0), (E.SPLIT, 0)]
-    bufs = {}
-    d2h = [0]
-
-    def read(info):
-        pn = info["pnum"]
-        for what, c in items:
-            n = lib.dgpu_encoder_item_bytes(enc.handle, pn, what, c)
-            if n == 0:
-                continue
-            b = bufs.get((what, c, n))
-            if b is None:
-                b = bufs[(what, c, n)] = torch.empty(n, dtype=torch.uint8, pin_memory=True)
-            rc = lib.dgpu_encoder_read(enc.handle, pn, what, c, b.data_ptr(), n, 1)
-            if rc:
-                raise RuntimeError(f"dgpu_encoder_read failed: {rc}")
-            d2h[0] += n
-
-    for _ in range(max(1, args.warmup)):
-        step(pinned_np, read=read)
-    stream.synchronize()
-    barrier()
-    d2h[0] = 0
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step(pinned_np, read=read)
-    e1.record(stream)
-    stream.synchronize()
-    barrier()
-    ems = max_over_ranks(e0.elapsed_time(e1))
-    h2d = sum(p.nbytes for fr in pinned_np for p in fr)
-    e2e = {"value": world * args.frames * args.steps / (ems / 1000.0), "unit": "frames/s",
-           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h[0] // args.steps}
-    enc.close()
+                "note": "plain form, one sequence; stage times from CUDA events on the encoder stream in a "
+                        "separate profiled pass"}
+    for ln in lanes:
+        ln.enc.close()
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-                "config": {"workload": workload_name(args.frames), "frames_per_step": args.frames,
-                           "global_batch": world * args.frames, "parallelism": f"replicas{world}",
-                           "form": "plain (one sequence per GPU)",
+                "config": {"workload": workload_name(args.frames), "frames_per_step": frames_per_step,
+                           "global_batch": world * frames_per_step, "parallelism": f"replicas{world}",
+                           "form": f"batched: {len(lanes)} concurrent sequences per GPU, each on its own stream "
+                                   "and host thread",
                            "l2": "inputs and working set larger than L2 (no flush needed)"},
-                "roofline": roofline, "cpu_baseline": cpu_baseline, "e2e": e2e,
+                "plain": plain_line, "roofline": roofline, "cpu_baseline": cpu_baseline, "e2e": e2e,
                 "latency_ms": latency, "gpu_launches": launches, "clocks": clk}
         print(json.dumps(line), flush=True)
     if world > 1:
