@@ -541,12 +541,12 @@ struct PelLaunch {
 // lanes).  The list's minimum with the earliest index replaces (best, bmv) only when strictly
 // smaller: the same result as the reference's sequential strict-< scan.
 __device__ __noinline__ void pel_list_best(const int16_t* pic, const int16_t* ref, int pw, int ph, const Blim& b, short2 centre,
-                              int r, int16_t* mem, int& best, short2& bmv) {
+                              int r, int16_t* mem, int& best, short2& bmv, bool blk_staged = false) {
     const int lane = threadIdx.x & 31;
     const int ww = b.xl + 2 * r, wh = b.yl + 2 * r;
     int16_t* blk = mem;
     int16_t* win = mem + b.xl * b.yl;
-    stage_rect(blk, pic, pw, ph, b.xp, b.yp, b.xl, b.yl);
+    if (!blk_staged) stage_rect(blk, pic, pw, ph, b.xp, b.yp, b.xl, b.yl);
     stage_rect(win, ref, pw, ph, b.xp + centre.x - r, b.yp + centre.y - r, ww, wh);
     __syncwarp();
     const int n = (2 * r + 1) * (2 * r + 1);
@@ -631,6 +631,9 @@ __global__ void __launch_bounds__(ME_THREADS) pel_wavefront_kernel(const __grid_
         const PelJob& J = L.jobs[jn];
         const int W = J.xnb;
         const int b = by * W + bx;
+        // the block's own samples do not depend on the neighbours: load them before waiting
+        const Blim bl = block_limits(L.o, J.pw, J.ph, bx, by);
+        if (bl.xl > 0 && bl.yl > 0) stage_rect(wmem, J.pic, J.pw, J.ph, bl.xp, bl.yp, bl.xl, bl.yl);
         if (bx > 0) wait_flag(&J.flags[b - 1], L.err);
         if (by > 0) {
             wait_flag(&J.flags[b - W], L.err);
@@ -647,12 +650,11 @@ __global__ void __launch_bounds__(ME_THREADS) pel_wavefront_kernel(const __grid_
         } else {
             pred = mv_mean(__ldcg(&mv[b - W]), __ldcg(&mv[b - 1]));
         }
-        const Blim bl = block_limits(L.o, J.pw, J.ph, bx, by);
         int best = J.best_sad[b];
         short2 bmv = J.best_mv[b];
         float sad;
         if (bl.xl > 0 && bl.yl > 0) {
-            pel_list_best(J.pic, J.ref, J.pw, J.ph, bl, pred, J.radius, wmem, best, bmv);
+            pel_list_best(J.pic, J.ref, J.pw, J.ph, bl, pred, J.radius, wmem, best, bmv, true);
             sad = (float)best;
         } else {
             bmv = make_short2(0, 0);
@@ -728,6 +730,17 @@ __global__ void __launch_bounds__(ME_THREADS) subpel_wavefront_kernel(const __gr
         const SubJob& J = L.jobs[jn];
         const int W = J.xnb, H = J.ynb;
         const int b = by * W + bx;
+        // Everything that depends only on this block comes before the neighbour waits: its
+        // limits, pel vector and cost, and (when the full search is likely) the staged search
+        // window, whose loads then overlap the wait instead of following it.
+        const Blim bl = block_limits(L.o, J.pw, J.ph, bx, by);
+        const short2 mv = J.mv[b];
+        const float pel_sad = J.cost[3 * b];
+        const float area2 = (float)(2 * bl.xl * bl.yl);
+        const float lambda = J.lambda[b];
+        const bool staged = L.win_elems > 0 && bl.xl > 0 && bl.yl > 0 && !(pel_sad < area2);
+        SubWin S{};
+        if (staged) stage_subwin(S, wmem, J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, bl, mv);
         // neighbours in SubpelRefine::m_nshift order: left, top-left, top, top-right
         const int nsx[4] = {-1, -1, 0, 1}, nsy[4] = {0, -1, -1, -1};
         short2 nbr[4];
@@ -741,13 +754,9 @@ __global__ void __launch_bounds__(ME_THREADS) subpel_wavefront_kernel(const __gr
             }
         }
         const short2 pred = mv_median_list(nbr, n);
-        const float lambda = J.lambda[b];
-        const Blim bl = block_limits(L.o, J.pw, J.ph, bx, by);
-        short2 mv = J.mv[b];
-        Cost3 cost{J.cost[3 * b], 0.0f, 0.0f};
+        Cost3 cost{pel_sad, 0.0f, 0.0f};
         cost.mvcost = (float)getvarup(pred, mv.x << prec, mv.y << prec);
         cost.total = cost.SAD + lambda * cost.mvcost;
-        const float area2 = (float)(2 * bl.xl * bl.yl);
         short2 out_mv;
         Cost3 out_cost;
         if (cost.SAD < area2) {
@@ -766,10 +775,7 @@ __global__ void __launch_bounds__(ME_THREADS) subpel_wavefront_kernel(const __gr
                 Cost3 best = cost;
                 short2 bmv = mv;
                 bool bailed = false;
-                // candidates stay within +-(2^prec - 1) of mv << prec: stage that window once
-                const bool staged = L.win_elems > 0 && bl.xl > 0 && bl.yl > 0;
-                SubWin S{};
-                if (staged) stage_subwin(S, wmem, J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, bl, mv);
+                // candidates stay within +-(2^prec - 1) of mv << prec: the window staged above
                 for (int i = 1; i <= prec; ++i) {
                     bmv = make_short2((short)(bmv.x << 1), (short)(bmv.y << 1));
                     short2 tb = bmv;

@@ -410,6 +410,33 @@ using namespace dgpu;
 
 extern "C" int dgpu_quant_factor4(int q) { return (q < 0 || q > 119) ? DGPU_ERR_ARG : qf4(q); }
 
+// Page-locked host staging for the statistics read-back, one growing buffer per host thread
+// (released at thread exit).
+struct PinnedScratch {
+    void* p = nullptr;
+    size_t n = 0;
+    ~PinnedScratch() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+static int pinned_scratch(size_t bytes, char** out) {
+    thread_local PinnedScratch buf;
+    if (buf.n < bytes) {
+        if (buf.p) cudaFreeHost(buf.p);
+        buf.p = nullptr;
+        buf.n = 0;
+        if (cudaMallocHost(&buf.p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            buf.p = nullptr;
+            return DGPU_ERR_NOMEM;
+        }
+        buf.n = bytes;
+    }
+    *out = static_cast<char*>(buf.p);
+    return DGPU_OK;
+}
+
 // Device workspace of one dgpu_code_residue_batch call: task table, band and code-block
 // maxima, statistics, intra DC prediction residues, code-block skip flags and the
 // sequential-sum fallback cases.
@@ -538,11 +565,19 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
         stats_kernel<<<grid, STAT_THREADS, 0, st>>>(d_tasks, d_band_max, d_stats);
         DGPU_CHECK_LAUNCH();
     }
-    std::vector<Stat> hs((size_t)nb_total * 2 * QMAX);
-    std::vector<int> hmax(nb_total), hcb(ncb_total);
-    DGPU_CHECK_CUDA(cudaMemcpyAsync(hs.data(), d_stats, sizeof(Stat) * hs.size(), cudaMemcpyDeviceToHost, st));
-    DGPU_CHECK_CUDA(cudaMemcpyAsync(hmax.data(), d_band_max, sizeof(int) * nb_total, cudaMemcpyDeviceToHost, st));
-    DGPU_CHECK_CUDA(cudaMemcpyAsync(hcb.data(), d_cb_max, sizeof(int) * ncb_total, cudaMemcpyDeviceToHost, st));
+    // statistics and maxima come back through page-locked memory (one buffer per host thread)
+    const size_t n_stats = (size_t)nb_total * 2 * QMAX;
+    char* pin = nullptr;
+    {
+        const int rc = pinned_scratch(sizeof(Stat) * n_stats + sizeof(int) * (nb_total + ncb_total) + 64, &pin);
+        if (rc) return rc;
+    }
+    Stat* hs = reinterpret_cast<Stat*>(pin);
+    int* hmax = reinterpret_cast<int*>(pin + sizeof(Stat) * n_stats);
+    int* hcb = hmax + nb_total;
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(hs, d_stats, sizeof(Stat) * n_stats, cudaMemcpyDeviceToHost, st));
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(hmax, d_band_max, sizeof(int) * nb_total, cudaMemcpyDeviceToHost, st));
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(hcb, d_cb_max, sizeof(int) * ncb_total, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
     // ---- 3a. sums the exact path could not represent: sequential double kernel ----
     std::vector<SeqCase> cases;
