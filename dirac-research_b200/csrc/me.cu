@@ -334,6 +334,35 @@ __device__ __noinline__ float subpel_cost(const int16_t* pic, int pw, const int1
     return subpel_cost_p<3>(pic, pw, up, uw, uh, b, mx, my, start);
 }
 
+// Integer total of |pred - pic| over a block for one candidate (the terms the cost loop adds).
+template <int P>
+__device__ __forceinline__ int subpel_total_p(const int16_t* pic, int pw, const int16_t* up, int uw, int uh,
+                                              const Blim& b, int mx, int my) {
+    const int lane = threadIdx.x & 31;
+    const int n = b.xl * b.yl;
+    PixWalk w(b.xl);
+    int tot = 0;
+    for (int k0 = 0; k0 < n; k0 += 256) {
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            if (k0 + 32 * s + lane < n) {
+                const int x = b.xp + w.col, y = b.yp + w.row;
+                tot += abs(up_pred(up, uw, uh, P, x, y, mx, my) - pic[(size_t)y * pw + x]);
+            }
+            w.next();
+        }
+    }
+    return __reduce_add_sync(0xffffffffu, tot);
+}
+
+__device__ __noinline__ int subpel_total(const int16_t* pic, int pw, const int16_t* up, int uw, int uh, int p,
+                                         const Blim& b, int mx, int my) {
+    if (b.xl <= 0 || b.yl <= 0) return 0;
+    if (p == 1) return subpel_total_p<1>(pic, pw, up, uw, uh, b, mx, my);
+    if (p == 2) return subpel_total_p<2>(pic, pw, up, uw, uh, b, mx, my);
+    return subpel_total_p<3>(pic, pw, up, uw, uh, b, mx, my);
+}
+
 // Copies the h x w region at (x0, y0) of a pw x ph plane into shared memory (rows of w),
 // coordinates clamped to the plane; each lane keeps eight loads in flight before storing.
 __device__ __forceinline__ void stage_rect(int16_t* dst, const int16_t* __restrict__ src, int pw, int ph, int x0,
@@ -862,7 +891,36 @@ struct ModeLaunch {
 };
 
 // ModeDecider::DoME: the unit's four guide vectors as candidates (BlockMatcher::FindBestMatchSubp).
-__device__ __noinline__ void do_me(const ModeLaunch& L, const ModeJob& J, int x, int y, int level) {
+// Candidate list of ModeDecider::DoME for unit (x, y) and reference r: the four guide
+// vectors of the next finer level, duplicates dropped, in the reference's order.
+__device__ __forceinline__ int dome_candidates(const ModeJob& J, int x, int y, int level, int r, short2* c) {
+    const LevelData& guide = J.lev[level + 1];
+    const int gx = x << 1, gy = y << 1;
+    int nc = 0;
+    for (int j = 0; j < 2; ++j)
+        for (int i = 0; i < 2; ++i) {
+            const short2 v = __ldcg(&guide.mv[r][(size_t)(gy + j) * guide.xnb + gx + i]);
+            bool dup = false;
+            for (int q = 0; q < nc; ++q) dup |= (c[q].x == v.x && c[q].y == v.y);
+            if (!dup) c[nc++] = v;
+        }
+    return nc;
+}
+
+// Integer totals of every DoME candidate of unit (x, y), computed before the superblock's
+// neighbours are done (the candidates do not depend on them; only the vector costs do).
+__device__ __noinline__ void dome_totals(const ModeLaunch& L, const ModeJob& J, int x, int y, int level, int* tot) {
+    const Blim bl = block_limits(L.lb[level], J.pw, J.ph, x, y);
+    for (int r = 0; r < J.nref; ++r) {
+        short2 c[4];
+        const int nc = dome_candidates(J, x, y, level, r, c);
+        for (int q = 0; q < nc; ++q)
+            tot[4 * r + q] = subpel_total(J.pic, J.pw, J.up[r], 2 * J.pw, 2 * J.ph, L.prec, bl, c[q].x, c[q].y);
+    }
+}
+
+__device__ __noinline__ void do_me(const ModeLaunch& L, const ModeJob& J, int x, int y, int level,
+                                   const int* pre_tot = nullptr) {
     const LevelData& me = J.lev[level];
     const LevelData& guide = J.lev[level + 1];
     const LevelData& blk = J.lev[2];
@@ -897,7 +955,12 @@ __device__ __noinline__ void do_me(const ModeLaunch& L, const ModeJob& J, int x,
             if (bl.xl <= 0 || bl.yl <= 0) break;
             const float mvcost = (float)getvarup(pred, c[q].x, c[q].y);
             const float start = mvcost * lambda;
-            const float sum = subpel_cost(J.pic, J.pw, J.up[r], 2 * J.pw, 2 * J.ph, L.prec, bl, c[q].x, c[q].y, start);
+            float sum;
+            FloatSeq f = float_seq_start(start);
+            if (pre_tot && float_seq_add_exact(f, pre_tot[4 * r + q]))
+                sum = (float)f.c;  // no addition of the loop could round
+            else
+                sum = subpel_cost(J.pic, J.pw, J.up[r], 2 * J.pw, 2 * J.ph, L.prec, bl, c[q].x, c[q].y, start);
             if (sum < best.total) {
                 bmv = c[q];
                 best.total = sum;
@@ -1029,6 +1092,9 @@ __global__ void __launch_bounds__(ME_THREADS) mode_wavefront_kernel(const __grid
         wave_unit(L.wave, u, jn, xsb, ysb);
         const ModeJob& J = L.jobs[jn];
         const int s = ysb * J.xnsb + xsb;
+        // level-1 candidate totals of this warp's sub-superblock while the neighbours finish
+        int pre1[8];
+        dome_totals(L, J, (xsb << 1) + (warp & 1), (ysb << 1) + (warp >> 1), 1, pre1);
         if (threadIdx.x == 0) {
             if (xsb > 0) wait_flag(&J.flags[s - 1], L.err);
             if (ysb > 0) {
@@ -1045,7 +1111,7 @@ __global__ void __launch_bounds__(ME_THREADS) mode_wavefront_kernel(const __grid
         // ---- level 1: sub-superblock (2 xsb + (warp & 1), 2 ysb + (warp >> 1)) per warp ----
         {
             const int i = (xsb << 1) + (warp & 1), j = (ysb << 1) + (warp >> 1);
-            do_me(L, J, i, j, 1);
+            do_me(L, J, i, j, 1, pre1);
             const float c = do_unit_decn(L, J, i, j, 1);
             if (lane == 0) s_cost[warp] = c;
         }
