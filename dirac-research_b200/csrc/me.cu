@@ -460,6 +460,33 @@ __device__ __noinline__ float subpel_cost_win(const SubWin& S, int p, const Blim
     return subpel_cost_win_p<3>(S, b, mx, my, start);
 }
 
+// Integer total of |pred - pic| over a staged block for one candidate.
+template <int P>
+__device__ __forceinline__ int subpel_total_win_p(const SubWin& S, const Blim& b, int mx, int my) {
+    const int lane = threadIdx.x & 31;
+    const int n = b.xl * b.yl;
+    PixWalk w(b.xl);
+    int tot = 0;
+    for (int k0 = 0; k0 < n; k0 += 256) {
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            const int k = k0 + 32 * s + lane;
+            if (k < n) tot += abs(win_pred<P>(S, b.xp + w.col, b.yp + w.row, mx, my) - S.pic[k]);
+            w.next();
+        }
+    }
+    return __reduce_add_sync(0xffffffffu, tot);
+}
+
+// The eight half-pel neighbours of (mvx, mvy) << 1, index (dy + 1) * 3 + dx + 1 (the centre,
+// index 4, is the pel vector itself and is never re-evaluated).
+__device__ __noinline__ void half_pel_totals(const SubWin& S, const Blim& b, short2 mv, int* tot) {
+    for (int k = 0; k < 9; ++k) {
+        if (k == 4) continue;
+        tot[k] = subpel_total_win_p<1>(S, b, 2 * mv.x + k % 3 - 1, 2 * mv.y + k / 3 - 1);
+    }
+}
+
 // BiBlock*Pel::Diff (me_utils.cpp:1172-1785): |((2 pic - p1) - p2) >> 1| with int16
 // intermediates, summed in float from 0 (exact: integer sums below 2^24).  The eighth-pel
 // version walks the second reference from the first one's integer start position when the
@@ -733,12 +760,17 @@ struct Cost3 {
 // one, else from global memory; (best, best_mv) updated on a strictly smaller total.
 __device__ __noinline__ void eval_subpel_cand(const SubJob& J, const SubWin& S, bool staged, int i, int sh,
                                               const Blim& bl, short2 c, short2 pred, float lambda, Cost3& best,
-                                              short2& best_mv) {
+                                              short2& best_mv, const int* half_tot, short2 mv) {
     const float mvcost = (float)getvarup(pred, c.x << sh, c.y << sh);
     if (bl.xl <= 0 || bl.yl <= 0) return;
     const float start = mvcost * lambda;
-    const float sum = staged ? subpel_cost_win(S, i, bl, c.x, c.y, start)
-                             : subpel_cost(J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, i, bl, c.x, c.y, start);
+    float sum;
+    FloatSeq f = float_seq_start(start);
+    if (staged && i == 1 && float_seq_add_exact(f, half_tot[(c.y - 2 * mv.y + 1) * 3 + c.x - 2 * mv.x + 1]))
+        sum = (float)f.c;  // precomputed total, and no addition of the loop could round
+    else
+        sum = staged ? subpel_cost_win(S, i, bl, c.x, c.y, start)
+                     : subpel_cost(J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, i, bl, c.x, c.y, start);
     if (sum < best.total) {
         best_mv = c;
         best.total = sum;
@@ -769,7 +801,12 @@ __global__ void __launch_bounds__(ME_THREADS) subpel_wavefront_kernel(const __gr
         const float lambda = J.lambda[b];
         const bool staged = L.win_elems > 0 && bl.xl > 0 && bl.yl > 0 && !(pel_sad < area2);
         SubWin S{};
-        if (staged) stage_subwin(S, wmem, J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, bl, mv);
+        int half_tot[9];
+        if (staged) {
+            stage_subwin(S, wmem, J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, bl, mv);
+            // the first refinement step's candidates are all among these eight
+            half_pel_totals(S, bl, mv, half_tot);
+        }
         // neighbours in SubpelRefine::m_nshift order: left, top-left, top, top-right
         const int nsx[4] = {-1, -1, 0, 1}, nsy[4] = {0, -1, -1, -1};
         short2 nbr[4];
@@ -814,7 +851,7 @@ __global__ void __launch_bounds__(ME_THREADS) subpel_wavefront_kernel(const __gr
                                     make_short2(bmv.x, bmv.y - 1), make_short2(bmv.x, bmv.y + 1)};
                     int nc = 4;
                     for (int q = 0; q < nc; ++q) {
-                        eval_subpel_cand(J, S, staged, i, sh, bl, cl[q], pred, lambda, best, tb);
+                        eval_subpel_cand(J, S, staged, i, sh, bl, cl[q], pred, lambda, best, tb, half_tot, mv);
                         if (q == 3) {
                             if (tb.x != bmv.x) {
                                 cl[4] = make_short2(tb.x, tb.y - 1);
