@@ -542,18 +542,16 @@ int take_slot(Encoder& E) {
 
 using namespace dgpu;
 
-extern "C" int dgpu_encoder_create(const dgpu_encoder_params* params, int max_pictures, void* stream, void** out) {
-    if (!params || !out) return DGPU_ERR_ARG;
-    *out = nullptr;
-    const dgpu_encoder_params& P = *params;
+// Checks the parameters and fills the encoder's geometry, GOP constants and workspace sizes;
+// *total receives the bytes of its device arena.  Allocates nothing.
+static int encoder_setup(const dgpu_encoder_params& P, int max_pictures, void* stream, Encoder* E, size_t* total,
+                         size_t* slot_bytes, int* nslots_out) {
     if (P.cformat < 0 || P.cformat > 2 || P.width < 16 || P.height < 16 || P.luma_depth < 8 || P.luma_depth > 14 ||
         P.chroma_depth < 8 || P.chroma_depth > 14 || P.num_l1 < 0 || (P.num_l1 > 0 && P.l1_sep < 1) ||
         P.mv_precision < 1 || P.mv_precision > 3 || P.wlt_depth < 1 || P.wlt_depth > 6 || P.intra_filter < 0 ||
         P.intra_filter > 6 || P.inter_filter < 0 || P.inter_filter > 6 || P.xbsep < 1 || P.ybsep < 1 ||
         P.xblen < P.xbsep || P.yblen < P.ybsep)
         return DGPU_ERR_ARG;
-    Encoder* E = new (std::nothrow) Encoder();
-    if (!E) return DGPU_ERR_NOMEM;
     E->P = P;
     E->st = as_stream(stream);
     E->L = calc_lambdas(P.qf);
@@ -581,10 +579,7 @@ extern "C" int dgpu_encoder_create(const dgpu_encoder_params* params, int max_pi
     E->nb = 3 * P.wlt_depth + 1;
     E->ncb.assign((size_t)2 * E->nb, 0);
     int rc = dgpu_code_blocks(P.wlt_depth, P.width, P.height, 1, E->ncb.data());
-    if (rc) {
-        delete E;
-        return rc;
-    }
+    if (rc) return rc;
     for (int b = 0; b < E->nb; ++b) E->ncb_total += E->ncb[2 * b] * E->ncb[2 * b + 1];
     // GOP (dirac_encoder.cpp:562-572, common.cpp:512-518)
     E->num_L1 = P.num_l1;
@@ -592,7 +587,8 @@ extern "C" int dgpu_encoder_create(const dgpu_encoder_params* params, int max_pi
     E->gop_len = P.num_l1 > 0 ? (P.num_l1 + 1) * P.l1_sep : 10;
     E->m_L1_sep = E->L1Sep;
     const int min_slots = 4 * std::max(E->L1Sep, 1) + 8;
-    const int nslots = std::max(max_pictures, min_slots);
+    *nslots_out = std::max(max_pictures, min_slots);
+    const int nslots = *nslots_out;
 
     // ---- sizes ----
     size_t plane16 = 0, plane32 = 0, up16 = 0;
@@ -604,17 +600,14 @@ extern "C" int dgpu_encoder_create(const dgpu_encoder_params* params, int max_pi
     const size_t me_out = align_up((size_t)E->nblocks * 2 * 2 * 2, 256) + align_up((size_t)E->nblocks * 2 * 3 * 4, 256) +
                           align_up(E->nblocks, 256) + align_up((size_t)E->nblocks * 3 * 2, 256) +
                           align_up(E->nsb, 256) + align_up((size_t)E->nsb * 4, 256);
-    const size_t slot_bytes = 2 * plane16 + 2 * plane32 + up16 + me_out;
+    *slot_bytes = 2 * plane16 + 2 * plane32 + up16 + me_out;
     E->me_max_tasks = std::min(nslots, 64);
     {
         std::vector<int> r2(E->me_max_tasks, 0);
         const int npics_max = std::min(nslots, 3 * E->me_max_tasks);
         E->me_ws_bytes = dgpu_me_batch_workspace_bytes(P.cformat, P.width, P.height, &E->bp, npics_max,
                                                        E->me_max_tasks, r2.data(), 3);
-        if (E->me_ws_bytes == 0) {
-            delete E;
-            return DGPU_ERR_ARG;
-        }
+        if (E->me_ws_bytes == 0) return DGPU_ERR_ARG;
     }
     for (int c = 0; c < 3; ++c) E->dwt_ws_bytes += align_up(dgpu_dwt_scratch_bytes(E->pw[c], E->ph[c], P.wlt_depth), 256);
     {
@@ -622,15 +615,37 @@ extern "C" int dgpu_encoder_create(const dgpu_encoder_params* params, int max_pi
         std::vector<int> ncb3(6 * E->nb);
         for (int c = 0; c < 3; ++c) std::memcpy(&ncb3[2 * c * E->nb], E->ncb.data(), sizeof(int) * 2 * E->nb);
         E->q_ws_bytes = dgpu_code_residue_workspace_bytes(3, intra, dep, E->pw, E->ph, ncb3.data());
-        if (E->q_ws_bytes == 0) {
-            delete E;
-            return DGPU_ERR_ARG;
-        }
+        if (E->q_ws_bytes == 0) return DGPU_ERR_ARG;
     }
     for (int c = 0; c < 3; ++c) E->stage_bytes += align_up((size_t)E->w[c] * E->h[c] * 2, 256);
-    const size_t total = (size_t)nslots * align_up(slot_bytes, 256) + align_up(E->me_ws_bytes, 256) +
-                         align_up(E->dwt_ws_bytes, 256) + align_up(E->q_ws_bytes, 256) +
-                         align_up(sizeof(int) * E->me_max_tasks, 256) + E->stage_bytes;
+    *total = (size_t)nslots * align_up(*slot_bytes, 256) + align_up(E->me_ws_bytes, 256) +
+             align_up(E->dwt_ws_bytes, 256) + align_up(E->q_ws_bytes, 256) +
+             align_up(sizeof(int) * E->me_max_tasks, 256) + E->stage_bytes;
+    return DGPU_OK;
+}
+
+extern "C" size_t dgpu_encoder_device_bytes(const dgpu_encoder_params* params, int max_pictures) {
+    if (!params) return 0;
+    Encoder E;
+    size_t total = 0, slot = 0;
+    int nslots = 0;
+    return encoder_setup(*params, max_pictures, nullptr, &E, &total, &slot, &nslots) == DGPU_OK ? total : 0;
+}
+
+extern "C" int dgpu_encoder_create(const dgpu_encoder_params* params, int max_pictures, void* stream, void** out) {
+    if (!params || !out) return DGPU_ERR_ARG;
+    *out = nullptr;
+    Encoder* E = new (std::nothrow) Encoder();
+    if (!E) return DGPU_ERR_NOMEM;
+    size_t total = 0, slot_bytes = 0;
+    int nslots = 0;
+    {
+        const int rc = encoder_setup(*params, max_pictures, stream, E, &total, &slot_bytes, &nslots);
+        if (rc) {
+            delete E;
+            return rc;
+        }
+    }
     if (cudaMalloc(&E->arena, total) != cudaSuccess) {
         cudaGetLastError();
         E->arena = nullptr;

@@ -97,6 +97,7 @@ SIGNATURES = {
         [c_int, P_int, P_int, P_void, P_int, P_int, c_void_p, c_void_p, c_void_p, P_int, P_int, P_int, P_int,
          c_void_p, P_void, c_void_p, c_size_t, c_void_p],
     ),
+    "dgpu_encoder_device_bytes": (c_size_t, [c_void_p, c_int]),
     "dgpu_encoder_create": (c_int, [c_void_p, c_int, c_void_p, P_void]),
     "dgpu_encoder_destroy": (c_int, [c_void_p]),
     "dgpu_encoder_reset": (c_int, [c_void_p]),

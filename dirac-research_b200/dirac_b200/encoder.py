@@ -47,6 +47,15 @@ _DTYPES = {RECON: np.int16, COEFF: np.int32, QINDEX: np.int32, MV: np.int16, MOD
            SPLIT: np.uint8, BANDS: np.int32, CBSKIP: np.uint8}
 
 
+def device_bytes(params, max_pictures=32):
+    """Device memory a SequenceEncoder with these parameters allocates (no GPU needed)."""
+    p = EncoderParams(**params)
+    n = _lib.load().dgpu_encoder_device_bytes(ctypes.byref(p), max_pictures)
+    if n == 0:
+        raise ValueError("invalid encoder parameters")
+    return n
+
+
 class SequenceEncoder:
     """One coded sequence on one CUDA stream.
 

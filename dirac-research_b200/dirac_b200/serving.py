@@ -1,0 +1,223 @@
+"""Serving loop: encode streams as they arrive, admitted against a device-memory budget.
+
+Each request is a sequence of frames of its own size and bit depth.  A request is admitted as
+soon as its encoder's device memory (``encoder.device_bytes``) fits in what the budget has
+left; until then it waits in arrival order.  Every admitted stream gets its own encoder, CUDA
+stream and host thread, so work from streams that arrive while others are on the GPU overlaps
+on the device (continuous admission, not a queue of whole jobs).  Frames of a stream become
+available one frame interval apart from its arrival (live encoding); a picture's latency is
+the time from its frame's availability to the end of its coding on the device.  Results of a
+stream do not depend on what runs beside it: the encoders share no state.
+
+    python -m dirac_b200.serving --seconds 10 --rate 4 --budget-gb 40
+"""
+import argparse
+import json
+import statistics
+import threading
+import time
+
+
+class Request:
+    """One stream: params (encoder parameter dict), frames (host sample planes per frame),
+    arrival (seconds after the loop starts), optional name."""
+
+    def __init__(self, params, frames, arrival=0.0, name=None):
+        self.params = params
+        self.frames = frames
+        self.arrival = arrival
+        self.name = name
+
+
+class ServingLoop:
+    def __init__(self, budget_bytes, max_active=16, frame_interval=0.0, slots=24, collect=None,
+                 encoder_factory=None, bytes_fn=None):
+        """budget_bytes: device memory the loop may give to encoders.  max_active: streams
+        coded at once.  frame_interval: seconds between a stream's frames (0: all at arrival).
+        slots: picture slots per encoder.  collect(request, encoder, info): called after each
+        coded picture (e.g. to read results).  encoder_factory / bytes_fn: injectable for tests."""
+        self.budget = budget_bytes
+        self.max_active = max_active
+        self.frame_interval = frame_interval
+        self.slots = slots
+        self.collect = collect
+        self.warm = encoder_factory is None
+        if encoder_factory is None:
+            from .encoder import SequenceEncoder
+
+            def encoder_factory(params, max_pictures):
+                import torch
+
+                return SequenceEncoder(params, max_pictures=max_pictures, stream=torch.cuda.Stream())
+        if bytes_fn is None:
+            from .encoder import device_bytes as bytes_fn
+        self.encoder_factory = encoder_factory
+        self.bytes_fn = bytes_fn
+
+    def _slots_for(self, req):
+        return min(len(req.frames), self.slots)
+
+    def run(self, requests):
+        """Serve every request; returns a dict of statistics (latencies in ms)."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        for r in reqs:
+            r.need = self.bytes_fn(r.params, self._slots_for(r))
+            if r.need > self.budget:
+                raise ValueError(f"request {r.name} needs {r.need} bytes, more than the whole budget")
+        if self.warm:
+            # CUDA context, library and kernel modules initialised before the clock starts
+            # (the first initialisation holds the interpreter lock for a while)
+            self.encoder_factory(params_for(64, 64), 1).close()
+        lock = threading.Condition()
+        state = {"free": self.budget, "active": 0, "peak_active": 0, "peak_bytes": 0, "errors": []}
+        lat = []
+        frames_done = [0]
+        t0 = time.perf_counter()
+
+        def worker(r):
+            try:
+                enc = self.encoder_factory(r.params, self._slots_for(r))
+                avail = {}
+                pending = []
+
+                def drain():
+                    while True:
+                        info = enc.code_next()
+                        if info is None:
+                            return
+                        pending.append(info)
+                        if hasattr(enc, "stream"):
+                            enc.stream.synchronize()
+                        now = time.perf_counter()
+                        with lock:
+                            lat.append(1000.0 * (now - avail[info["pnum"]]))
+                            frames_done[0] += 1
+                        if self.collect is not None:
+                            self.collect(r, enc, info)
+
+                for i, f in enumerate(r.frames):
+                    due = t0 + r.arrival + i * self.frame_interval
+                    wait = due - time.perf_counter()
+                    if wait > 0:
+                        time.sleep(wait)
+                    avail[i] = max(due, t0 + r.arrival)
+                    enc.load(f)
+                    drain()
+                enc.end_sequence()
+                drain()
+                enc.close()
+            except Exception as e:  # reported after the loop, never swallowed
+                with lock:
+                    state["errors"].append(f"{r.name}: {e!r}")
+            finally:
+                with lock:
+                    state["free"] += r.need
+                    state["active"] -= 1
+                    lock.notify_all()
+
+        threads = []
+        queue = list(reqs)
+        waits = []
+        with lock:
+            while queue:
+                r = queue[0]
+                now = time.perf_counter() - t0
+                if now < r.arrival:
+                    lock.wait(timeout=r.arrival - now)
+                    continue
+                if r.need > state["free"] or state["active"] >= self.max_active:
+                    lock.wait(timeout=0.05)
+                    continue
+                queue.pop(0)
+                waits.append(1000.0 * (time.perf_counter() - t0 - r.arrival))
+                state["free"] -= r.need
+                state["active"] += 1
+                state["peak_active"] = max(state["peak_active"], state["active"])
+                state["peak_bytes"] = max(state["peak_bytes"], self.budget - state["free"])
+                th = threading.Thread(target=worker, args=(r,), daemon=True)
+                th.start()
+                threads.append(th)
+        for th in threads:
+            th.join()
+        wall = time.perf_counter() - t0
+        if state["errors"]:
+            raise RuntimeError("; ".join(state["errors"]))
+        lat.sort()
+
+        def pct(p):
+            return lat[min(len(lat) - 1, int(round(p * (len(lat) - 1))))] if lat else None
+
+        return {"streams": len(reqs), "pictures": frames_done[0], "wall_s": wall,
+                "frames_per_s": frames_done[0] / wall if wall > 0 else None,
+                "latency_ms": {"p50": pct(0.5), "p99": pct(0.99), "max": lat[-1] if lat else None},
+                "admission_wait_ms": {"p50": statistics.median(waits) if waits else None,
+                                      "max": max(waits) if waits else None},
+                "peak_active": state["peak_active"], "peak_bytes": state["peak_bytes"],
+                "budget_bytes": self.budget}
+
+
+RESOLUTIONS = {"cif": (352, 288), "576": (720, 576), "720": (1280, 720), "1080": (1920, 1080),
+               "2160": (3840, 2160)}
+
+
+def params_for(w, h, depth=8):
+    """Coding parameters of a served stream (4:2:0, the bench's GOP, QF and block sizes)."""
+    return dict(cformat=2, width=w, height=h, luma_depth=depth, chroma_depth=depth, qf=7.0, l1_sep=3, num_l1=7,
+                cpd=32.0, xblen=16, yblen=16, xbsep=12, ybsep=12, mv_precision=2, intra_filter=6, inter_filter=0,
+                wlt_depth=4)
+
+
+def make_requests(seconds, rate, resolutions, min_frames, max_frames, seed=0, pool_frames=16):
+    """Poisson arrivals at `rate` streams/s over `seconds`; each stream a resolution drawn
+    uniformly from `resolutions`, a length uniform in [min_frames, max_frames], and frames
+    taken (cycled from a per-stream offset) from a seeded synthetic pool per resolution."""
+    import numpy as np
+
+    from . import synth
+
+    rng = np.random.default_rng(seed)
+    pools = {}
+    reqs = []
+    t = 0.0
+    k = 0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= seconds:
+            break
+        res = resolutions[rng.integers(len(resolutions))]
+        w, h = RESOLUTIONS[res]
+        if res not in pools:
+            pools[res] = synth.make_sequence(w, h, pool_frames, n_rects=8, vmax=8, seed=100 + len(pools))
+        n = int(rng.integers(min_frames, max_frames + 1))
+        off = int(rng.integers(pool_frames))
+        frames = [pools[res][(off + i) % pool_frames] for i in range(n)]
+        reqs.append(Request(params_for(w, h), frames, t, f"s{k}-{res}x{n}"))
+        k += 1
+    return reqs
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--seconds", type=float, default=10.0)
+    ap.add_argument("--rate", type=float, default=4.0, help="stream arrivals per second (Poisson)")
+    ap.add_argument("--budget-gb", type=float, default=40.0)
+    ap.add_argument("--max-active", type=int, default=16)
+    ap.add_argument("--fps", type=float, default=50.0, help="frame rate of the live streams (0: all at once)")
+    ap.add_argument("--resolutions", default="cif,576,720,1080")
+    ap.add_argument("--frames", default="8-64")
+    ap.add_argument("--seed", type=int, default=0)
+    a = ap.parse_args(argv)
+    lo, hi = (int(x) for x in a.frames.split("-"))
+    reqs = make_requests(a.seconds, a.rate, a.resolutions.split(","), lo, hi, a.seed)
+    loop = ServingLoop(int(a.budget_gb * 1e9), a.max_active, 1.0 / a.fps if a.fps > 0 else 0.0)
+    stats = loop.run(reqs)
+    stats["config"] = {"seconds": a.seconds, "rate": a.rate, "resolutions": a.resolutions, "frames": a.frames,
+                       "fps": a.fps, "budget_gb": a.budget_gb}
+    print(json.dumps(stats))
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+
+    sys.exit(main())

@@ -337,6 +337,9 @@ typedef struct {
 #define DGPU_STAGE_UPCONVERT 7
 #define DGPU_ENC_NSTAGES 8
 
+/* Device bytes dgpu_encoder_create would allocate for these parameters (0 if they are
+ * invalid); no GPU use, so a scheduler can admit sequences against a memory budget. */
+size_t dgpu_encoder_device_bytes(const dgpu_encoder_params* params, int max_pictures);
 int dgpu_encoder_create(const dgpu_encoder_params* params, int max_pictures, void* stream, void** encoder);
 int dgpu_encoder_destroy(void* encoder);
 /* Forgets every picture and the GOP state (a new sequence), keeping the device memory. */

@@ -156,3 +156,32 @@ def test_encoder_caller_entropy_factors(gpu):
     oenc = oracle_run(cfg, seq, ecf_fn=lambda p: factors(p.pnum))
     infos, results = run_device(gpu, seq, cfg, ecf_fn=dev_ecf)
     compare(infos, results, oenc)
+
+
+@pytest.mark.parametrize("cformat,depth", [(1, 10), (0, 8), (2, 12)])
+def test_encoder_formats_and_depths(gpu, cformat, depth):
+    """4:2:2 10-bit, 4:4:4 8-bit and 4:2:0 12-bit sequences (16-bit input samples above 8
+    bits) through the device encoder equal the oracle's restatement, picture by picture."""
+    from dirac_b200 import quant, synth
+    from oracle_encoder import encode_sequence
+
+    w, h, n = 176, 144, 7
+    chroma = {0: "444", 1: "422", 2: "420"}[cformat]
+    seq = synth.make_sequence(w, h, n, n_rects=5, vmax=5, seed=40 + cformat, bit_depth=depth, chroma=chroma)
+    cfg = dict(cformat=cformat, width=w, height=h, luma_depth=depth, chroma_depth=depth, qf=6.5, l1_sep=3,
+               num_l1=19, cpd=20.0, xblen=12, yblen=12, xbsep=8, ybsep=8, mv_precision=2, intra_filter=6,
+               inter_filter=2, wlt_depth=3)
+    from dirac_b200.encoder import SequenceEncoder
+
+    enc = SequenceEncoder(cfg, max_pictures=n)
+    infos = enc.encode(seq)
+    results = {i["pnum"]: read_all(enc, i["pnum"]) for i in infos}
+    enc.close()
+    frames = [[synth.to_signed(p, depth) for p in f] for f in seq]
+    oenc = encode_sequence(cfg, frames, quant.band_weights, quant.code_blocks)
+    compare(infos, results, oenc)
+    off = 1 << (depth - 1)
+    for i in range(n):
+        for c in range(3):
+            np.testing.assert_array_equal(results[i]["output"][c],
+                                          (oenc.pics[i].data[c].astype(np.int32) + off).ravel())

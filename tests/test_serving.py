@@ -1,0 +1,117 @@
+"""Serving loop: admission against the device-memory budget, continuous admission of
+arriving streams, latency accounting (CPU, with a stand-in encoder), and on the GPU the
+identity of every stream's results alone and in the mix."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+
+class FakeEncoder:
+    """Codes each loaded picture at the next code_next call after a short pause, tracking
+    how many bytes are live across all fakes."""
+
+    live = 0
+    peak = 0
+    lock = threading.Lock()
+
+    def __init__(self, params, max_pictures):
+        self.need = params["bytes"]
+        with FakeEncoder.lock:
+            FakeEncoder.live += self.need
+            FakeEncoder.peak = max(FakeEncoder.peak, FakeEncoder.live)
+        self.loaded = []
+        self.next = 0
+        self.done = False
+
+    def load(self, frame):
+        self.loaded.append(frame)
+
+    def end_sequence(self):
+        self.done = True
+
+    def code_next(self):
+        if self.next < len(self.loaded):
+            time.sleep(0.002)
+            self.next += 1
+            return {"pnum": self.next - 1}
+        return None
+
+    def close(self):
+        with FakeEncoder.lock:
+            FakeEncoder.live -= self.need
+
+
+def test_admission_respects_budget_and_serves_everything():
+    from dirac_b200.serving import Request, ServingLoop
+
+    FakeEncoder.live = FakeEncoder.peak = 0
+    reqs = [Request({"bytes": 300 + 100 * (k % 3)}, list(range(5 + k % 4)), arrival=0.01 * k, name=str(k))
+            for k in range(12)]
+    coded = {}
+
+    def collect(r, enc, info):
+        coded.setdefault(r.name, []).append(info["pnum"])
+
+    loop = ServingLoop(budget_bytes=1000, max_active=8, frame_interval=0.001, collect=collect,
+                       encoder_factory=FakeEncoder, bytes_fn=lambda p, n: p["bytes"])
+    stats = loop.run(reqs)
+    assert FakeEncoder.peak <= 1000 and FakeEncoder.live == 0
+    assert stats["peak_bytes"] <= 1000 and stats["peak_active"] >= 2
+    assert stats["pictures"] == sum(len(r.frames) for r in reqs)
+    for r in reqs:
+        assert coded[r.name] == list(range(len(r.frames)))
+    assert stats["latency_ms"]["p50"] > 0 and stats["latency_ms"]["p99"] >= stats["latency_ms"]["p50"]
+
+
+def test_request_larger_than_budget_is_refused():
+    from dirac_b200.serving import Request, ServingLoop
+
+    loop = ServingLoop(budget_bytes=100, encoder_factory=FakeEncoder, bytes_fn=lambda p, n: p["bytes"])
+    with pytest.raises(ValueError):
+        loop.run([Request({"bytes": 200}, [0, 1])])
+
+
+def test_encoder_device_bytes_grows_with_size_and_slots():
+    from dirac_b200 import encoder as E
+    from dirac_b200.serving import params_for
+
+    a = E.device_bytes(params_for(352, 288), 16)
+    b = E.device_bytes(params_for(1920, 1080), 16)
+    c = E.device_bytes(params_for(1920, 1080), 40)
+    assert 0 < a < b < c
+
+
+@pytest.mark.gpu
+def test_served_streams_equal_alone_and_in_the_mix(gpu):
+    """Three streams of different sizes coded one at a time and then concurrently (admitted
+    together, overlapping on the device): every picture's output samples and quantised indices
+    are identical."""
+    from dirac_b200 import synth
+    from dirac_b200.encoder import OUTPUT, QINDEX
+    from dirac_b200.serving import Request, ServingLoop, params_for
+
+    specs = [(176, 144, 9, 1), (352, 288, 8, 2), (320, 240, 10, 3)]
+    reqs = [Request(params_for(w, h), synth.make_sequence(w, h, n, n_rects=4, vmax=6, seed=s), 0.0, f"r{s}")
+            for w, h, n, s in specs]
+
+    def run(max_active):
+        out = {}
+        lock = threading.Lock()
+
+        def collect(r, enc, info):
+            pn = info["pnum"]
+            got = [enc.read(pn, OUTPUT, c) for c in range(3)] + [enc.read(pn, QINDEX, c) for c in range(3)]
+            with lock:
+                out[(r.name, pn)] = got
+
+        ServingLoop(budget_bytes=int(8e9), max_active=max_active, collect=collect).run(reqs)
+        return out
+
+    alone = run(1)
+    mixed = run(3)
+    assert alone.keys() == mixed.keys() and len(alone) == sum(n for _, _, n, _ in specs)
+    for k in alone:
+        for a, b in zip(alone[k], mixed[k]):
+            np.testing.assert_array_equal(a, b, err_msg=str(k))
