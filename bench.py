@@ -48,6 +48,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--frames", type=int, default=32)
     ap.add_argument("--streams", type=int, default=8, help="concurrent sequences per GPU (batched form)")
+    ap.add_argument("--serving-seconds", type=float, default=6.0,
+                    help="length of the serving-loop run reported under 'serving' (0: skip)")
     ap.add_argument("--impl", choices=["gpu", "reference"], default="gpu")
     return ap.parse_args()
 
@@ -400,6 +402,17 @@ def main():
     for ln in lanes:
         ln.enc.close()
 
+    # ---- serving loop: Poisson arrivals of live streams of mixed sizes (one GPU) ----------------
+    serving = None
+    if args.serving_seconds > 0 and world == 1:
+        from dirac_b200 import serving as S
+
+        reqs = S.make_requests(args.serving_seconds, 4.0, ["cif", "576", "720", "1080"], 8, 32, seed=7)
+        serving = S.ServingLoop(int(40e9), max_active=16, frame_interval=1.0 / 50).run(reqs)
+        serving["config"] = {"seconds": args.serving_seconds, "arrivals_per_s": 4.0, "fps_per_stream": 50,
+                             "resolutions": "352x288, 720x576, 1280x720, 1920x1080 (4:2:0 8-bit)",
+                             "frames_per_stream": "8-32", "budget_gb": 40}
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -410,7 +423,7 @@ def main():
                                    "and host thread",
                            "l2": "inputs and working set larger than L2 (no flush needed)"},
                 "plain": plain_line, "roofline": roofline, "cpu_baseline": cpu_baseline, "e2e": e2e,
-                "latency_ms": latency, "gpu_launches": launches, "clocks": clk}
+                "latency_ms": latency, "serving": serving, "gpu_launches": launches, "clocks": clk}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
