@@ -151,6 +151,17 @@ __device__ __forceinline__ int stat_range(int maxv) {
 }
 
 // grid: x = chunks of the band's sampled coefficients, y = task, z = pattern (0: 2x2, 1: 1x2).
+// n / d: for n < 2^24 (every magnitude times 4 of 8- to 14-bit video) the float estimate
+// n * RN(1/d) is within one of the quotient (relative error below 2^-23, quotient below
+// 2^22), and one integer correction makes it exact.
+__device__ __forceinline__ unsigned udiv_recip(unsigned n, unsigned d, float inv) {
+    if (n >= (1u << 24)) return n / d;  // outside the estimate's range: plain division
+    unsigned q = (unsigned)((float)n * inv);
+    if (q * d > n) --q;
+    else if ((q + 1) * d <= n) ++q;
+    return q;
+}
+
 __global__ void __launch_bounds__(STAT_THREADS) stats_kernel(const BandTask* tasks, const int* band_max,
                                                              Stat* stats) {
     const BandTask T = tasks[blockIdx.y];
@@ -186,13 +197,14 @@ __global__ void __launch_bounds__(STAT_THREADS) stats_kernel(const BandTask* tas
     const int lane = threadIdx.x & 31;
     for (int q = (pattern ? 0 : 0); q < nq; q += (pattern ? 1 : 2)) {
         const unsigned qf = (unsigned)qf4(q);
+        const float inv = __frcp_rn((float)qf);
         const int off = inter_off4(q);
         unsigned long long c0 = 0, lo = 0, hi = 0;
         unsigned int pos = 0, ng = 0, inx = 0;
 #pragma unroll
         for (int t = 0; t < 8; ++t) {
             if (a[t] < 0) continue;
-            const unsigned qv = ((unsigned)a[t] << 2) / qf;
+            const unsigned qv = udiv_recip((unsigned)a[t] << 2, qf, inv);
             unsigned long long e;
             if (qv == 0) {
                 e = (unsigned long long)a[t];
