@@ -151,6 +151,27 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------------------------
+# multi-rank helpers (one process per GPU; replicas, no collective on the data path)
+# ---------------------------------------------------------------------------------------------
+
+def max_over_ranks_ms(ms, world, device):
+    """The slowest rank's time: every rank calls this with its own device time."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, units_per_rank_step, steps, ms):
+    """Units per second of the whole job: every rank's units over the slowest rank's time."""
+    return world * units_per_rank_step * steps / (ms / 1000.0)
+
+
+# ---------------------------------------------------------------------------------------------
 # GPU clocks sampled during the timed region
 # ---------------------------------------------------------------------------------------------
 
@@ -288,11 +309,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(ms):
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return ms
+        return max_over_ranks_ms(ms, world, "cuda")
 
     def timed(lanes, src, steps, with_read=False):
         """Device time (ms) of `steps` sequence encodes on every lane, the lanes running
@@ -345,12 +362,12 @@ def main():
     clk = clocks.stop()
     frames_per_step = args.frames * len(lanes)
     ms_per_step = ms / args.steps
-    value = world * frames_per_step * args.steps / (ms / 1000.0)
+    value = whole_job_rate(world, frames_per_step, args.steps, ms)
 
     # ---- end to end (batched form) through the C ABI with host buffers -------------------------
     ems = timed(lanes, pinned_np, args.steps, with_read=True)
     h2d = sum(p.nbytes for fr in pinned_np for p in fr) * len(lanes)
-    e2e = {"value": world * frames_per_step * args.steps / (ems / 1000.0), "unit": "frames/s",
+    e2e = {"value": whole_job_rate(world, frames_per_step, args.steps, ems), "unit": "frames/s",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": sum(ln.d2h for ln in lanes) // args.steps}
 
     # ---- plain form: one sequence at a time ----------------------------------------------------
