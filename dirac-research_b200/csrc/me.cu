@@ -35,6 +35,7 @@
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "dgpu_internal.cuh"
@@ -1373,6 +1374,33 @@ void lambda_map(const short2* mv1, const short2* mv2, int nref, int W, int H, fl
         }
 }
 
+// Page-locked host staging for the batch's vector read-back and lambda maps, one growing
+// buffer per host thread (released at thread exit).
+struct MePinned {
+    void* p = nullptr;
+    size_t n = 0;
+    ~MePinned() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+int me_pinned(size_t bytes, char** out) {
+    thread_local MePinned buf;
+    if (buf.n < bytes) {
+        if (buf.p) cudaFreeHost(buf.p);
+        buf.p = nullptr;
+        buf.n = 0;
+        if (cudaMallocHost(&buf.p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            buf.p = nullptr;
+            return DGPU_ERR_NOMEM;
+        }
+        buf.n = bytes;
+    }
+    *out = static_cast<char*>(buf.p);
+    return DGPU_OK;
+}
+
 // MEData::SetLambdaMap(level, block map, wt) (motion.cpp:173-196).
 void level_lambda_map(const float* blk, int W, int level, int lw, int lh, float wt, float* out) {
     const int f = 1 << (2 - level);
@@ -1471,7 +1499,9 @@ size_t pic_layout(const MeGeometry& g, PicBufs& P, Arena& a, bool need_up) {
     return a.used;
 }
 
-size_t task_layout(const MeGeometry& g, TaskBufs& T, Arena& a) {
+// fa / za: arenas over regions shared by all tasks of a batch, so that the wavefront flags and
+// the mode-decision level data each clear with one memset.
+size_t task_layout(const MeGeometry& g, TaskBufs& T, Arena& a, Arena& fa, Arena& za) {
     for (int l = 0; l <= g.depth; ++l)
         for (int r = 0; r < 2; ++r) {
             const size_t n = (size_t)g.xnb[l] * g.ynb[l];
@@ -1482,7 +1512,7 @@ size_t task_layout(const MeGeometry& g, TaskBufs& T, Arena& a) {
         }
     size_t maxunits = 0;
     for (int l = 0; l <= g.depth; ++l) maxunits = std::max(maxunits, (size_t)g.xnb[l] * g.ynb[l]);
-    T.flags = a.take<int>(2 * maxunits);
+    T.flags = fa.take<int>(2 * maxunits);
     const size_t nb = (size_t)g.xnb[0] * g.ynb[0];
     T.lambda[2] = a.take<float>(nb);
     T.lambda[1] = a.take<float>(nb / 4);
@@ -1490,11 +1520,11 @@ size_t task_layout(const MeGeometry& g, TaskBufs& T, Arena& a) {
     for (int lv = 0; lv < 2; ++lv) {
         const size_t n = lv ? nb / 4 : nb / 16;
         for (int r = 0; r < 2; ++r) {
-            T.lmv[lv][r] = a.take<short2>(n);
-            T.lcost[lv][r] = a.take<float>(3 * n);
+            T.lmv[lv][r] = za.take<short2>(n);
+            T.lcost[lv][r] = za.take<float>(3 * n);
         }
-        T.lmode[lv] = a.take<uint8_t>(n);
-        T.ldcy[lv] = a.take<int16_t>(n);
+        T.lmode[lv] = za.take<uint8_t>(n);
+        T.ldcy[lv] = za.take<int16_t>(n);
     }
     T.dctmp = a.take<int16_t>(3 * nb);
     T.bcost = a.take<float>(nb);
@@ -1549,6 +1579,10 @@ struct BatchTables {
     int* prefix;      // levels 0..depth (slope 2), then superblocks (slope 1)
     size_t prefix_off[14];
     size_t prefix_len;
+    char* flags;      // every task's wavefront flags
+    size_t flags_bytes;
+    char* zero;       // every task's mode-decision level data (cleared per batch)
+    size_t zero_bytes;
 };
 
 size_t prefix_layout(const MeGeometry& g, size_t* off) {
@@ -1585,9 +1619,23 @@ size_t batch_bytes(const MeGeometry& g, const BatchArgs& A, std::vector<PicBufs>
         if (P) P->push_back(pb);
     }
     TaskBufs tb;
-    for (int t = 0; t < A.ntasks; ++t) {
-        task_layout(g, tb, a);
-        if (T) T->push_back(tb);
+    {
+        Arena sa{nullptr, 0, 0}, sf{nullptr, 0, 0}, sz{nullptr, 0, 0};
+        task_layout(g, tb, sa, sf, sz);
+        const size_t fper = align_up(sf.used, 256), zper = align_up(sz.used, 256);
+        char* fbase = a.take<char>(fper * A.ntasks);
+        char* zbase = a.take<char>(zper * A.ntasks);
+        if (tabs) {
+            tabs->flags = fbase;
+            tabs->flags_bytes = fper * A.ntasks;
+            tabs->zero = zbase;
+            tabs->zero_bytes = zper * A.ntasks;
+        }
+        Arena fa{fbase, 0, 0}, za{zbase, 0, 0};
+        for (int t = 0; t < A.ntasks; ++t) {
+            task_layout(g, tb, a, fa, za);
+            if (T) T->push_back(tb);
+        }
     }
     int* c = a.take<int>(64);
     if (ctl) *ctl = c;
@@ -1670,9 +1718,9 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                 J.best_sad = T[t].best_sad[l][r];
                 J.best_mv = T[t].best_mv[l][r];
                 J.flags = T[t].flags + (size_t)r * g.xnb[l] * g.ynb[l];
-                DGPU_CHECK_CUDA(cudaMemsetAsync(J.flags, 0, sizeof(int) * J.xnb * J.ynb, st));
                 jobs.push_back(J);
             }
+        DGPU_CHECK_CUDA(cudaMemsetAsync(tabs.flags, 0, tabs.flags_bytes, st));
         PelJob* dj = tabs.pel + (size_t)l * 2 * A.ntasks;
         DGPU_CHECK_CUDA(cudaMemcpyAsync(dj, jobs.data(), sizeof(PelJob) * jobs.size(), cudaMemcpyHostToDevice, st));
         PelLaunch L{};
@@ -1704,19 +1752,37 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
     int err_host = 0;
     if (A.stages >= 2) {
         // ---- lambda maps on the host (long double statistics, as the reference) ----
-        std::vector<std::vector<short2>> hmv(A.ntasks, std::vector<short2>(2 * nb));
-        std::vector<std::vector<float>> hl(A.ntasks, std::vector<float>(nb));
+        // vectors come back and maps go out through page-locked memory; the tasks' maps are
+        // independent, so host threads share them
+        char* pin = nullptr;
+        {
+            const int rc = me_pinned((sizeof(short2) * 2 * nb + sizeof(float) * nb) * A.ntasks + 256, &pin);
+            if (rc) return rc;
+        }
+        short2* hmv_all = reinterpret_cast<short2*>(pin);
+        float* hl_all = reinterpret_cast<float*>(pin + sizeof(short2) * 2 * nb * A.ntasks);
+        auto hmv = [&](int t) { return hmv_all + (size_t)t * 2 * nb; };
+        auto hlm = [&](int t) { return hl_all + (size_t)t * nb; };
         for (int t = 0; t < A.ntasks; ++t)
-            DGPU_CHECK_CUDA(cudaMemcpyAsync(hmv[t].data(), A.mv_out[t], sizeof(short2) * nref_of(t) * nb,
+            DGPU_CHECK_CUDA(cudaMemcpyAsync(hmv(t), A.mv_out[t], sizeof(short2) * nref_of(t) * nb,
                                             cudaMemcpyDeviceToHost, st));
         DGPU_CHECK_CUDA(cudaMemcpyAsync(&err_host, ctl + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
         DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
         if (err_host) return DGPU_ERR_CUDA;
-        for (int t = 0; t < A.ntasks; ++t) {
-            lambda_map(hmv[t].data(), hmv[t].data() + nb, nref_of(t), g.xnb[0], g.ynb[0], A.task_lambda[t],
-                       hl[t].data());
-            DGPU_CHECK_CUDA(cudaMemcpyAsync(T[t].lambda[2], hl[t].data(), sizeof(float) * nb, cudaMemcpyHostToDevice, st));
+        {
+            const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+            const int nth = std::min(A.ntasks, std::min(hw, 16));
+            auto work = [&](int first) {
+                for (int t = first; t < A.ntasks; t += nth)
+                    lambda_map(hmv(t), hmv(t) + nb, nref_of(t), g.xnb[0], g.ynb[0], A.task_lambda[t], hlm(t));
+            };
+            std::vector<std::thread> pool;
+            for (int k = 1; k < nth; ++k) pool.emplace_back(work, k);
+            work(0);
+            for (auto& th : pool) th.join();
         }
+        for (int t = 0; t < A.ntasks; ++t)
+            DGPU_CHECK_CUDA(cudaMemcpyAsync(T[t].lambda[2], hlm(t), sizeof(float) * nb, cudaMemcpyHostToDevice, st));
         // ---- upconverted original references (EncPicture::UpOrigData) ----
         {
             std::vector<const int16_t*> in;
@@ -1750,9 +1816,9 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                     J.cost = cost0(t, r);
                     J.lambda = T[t].lambda[2];
                     J.flags = T[t].flags + (size_t)r * nb;
-                    DGPU_CHECK_CUDA(cudaMemsetAsync(J.flags, 0, sizeof(int) * nb, st));
                     jobs.push_back(J);
                 }
+            DGPU_CHECK_CUDA(cudaMemsetAsync(tabs.flags, 0, tabs.flags_bytes, st));
             DGPU_CHECK_CUDA(cudaMemcpyAsync(tabs.sub, jobs.data(), sizeof(SubJob) * jobs.size(),
                                             cudaMemcpyHostToDevice, st));
             SubLaunch S{};
@@ -1776,26 +1842,19 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
         if (A.stages >= 3) {
             const float f0 = (float)(16 * g.lb[2].xblen * g.lb[2].yblen) / (float)(g.lb[0].xblen * g.lb[0].yblen);
             const float f1 = (float)(4 * g.lb[2].xblen * g.lb[2].yblen) / (float)(g.lb[1].xblen * g.lb[1].yblen);
+            // fresh level data for every task (a new MEData per picture in the reference)
+            DGPU_CHECK_CUDA(cudaMemsetAsync(tabs.zero, 0, tabs.zero_bytes, st));
             std::vector<std::vector<float>> l0(A.ntasks), l1(A.ntasks);
             for (int t = 0; t < A.ntasks; ++t) {
                 l0[t].resize(nb / 16);
                 l1[t].resize(nb / 4);
-                level_lambda_map(hl[t].data(), g.xnb[0], 0, g.xnb[0] / 4, g.ynb[0] / 4, (float)(1.0 / f0), l0[t].data());
-                level_lambda_map(hl[t].data(), g.xnb[0], 1, g.xnb[0] / 2, g.ynb[0] / 2, (float)(1.0 / f1), l1[t].data());
+                level_lambda_map(hlm(t), g.xnb[0], 0, g.xnb[0] / 4, g.ynb[0] / 4, (float)(1.0 / f0), l0[t].data());
+                level_lambda_map(hlm(t), g.xnb[0], 1, g.xnb[0] / 2, g.ynb[0] / 2, (float)(1.0 / f1), l1[t].data());
                 DGPU_CHECK_CUDA(cudaMemcpyAsync(T[t].lambda[0], l0[t].data(), sizeof(float) * l0[t].size(),
                                                 cudaMemcpyHostToDevice, st));
                 DGPU_CHECK_CUDA(cudaMemcpyAsync(T[t].lambda[1], l1[t].data(), sizeof(float) * l1[t].size(),
                                                 cudaMemcpyHostToDevice, st));
-                // fresh level data (a new MEData in the reference) and zero DC arrays (a fresh MvData)
-                for (int lv = 0; lv < 2; ++lv) {
-                    const size_t n = lv ? nb / 4 : nb / 16;
-                    for (int r = 0; r < 2; ++r) {
-                        DGPU_CHECK_CUDA(cudaMemsetAsync(T[t].lmv[lv][r], 0, sizeof(short2) * n, st));
-                        DGPU_CHECK_CUDA(cudaMemsetAsync(T[t].lcost[lv][r], 0, sizeof(float) * 3 * n, st));
-                    }
-                    DGPU_CHECK_CUDA(cudaMemsetAsync(T[t].ldcy[lv], 0, sizeof(int16_t) * n, st));
-                    DGPU_CHECK_CUDA(cudaMemsetAsync(T[t].lmode[lv], 0, n, st));
-                }
+                // zero DC arrays (a fresh MvData)
                 DGPU_CHECK_CUDA(cudaMemsetAsync(A.dc_out[t], 0, sizeof(int16_t) * 3 * nb, st));
             }
             ModeLaunch M{};
@@ -1844,9 +1903,9 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                 J.ynsb = g.ynsb;
                 J.flags = T[t].flags;
                 J.bcost = T[t].bcost;
-                DGPU_CHECK_CUDA(cudaMemsetAsync(J.flags, 0, sizeof(int) * g.xnsb * g.ynsb, st));
                 jobs.push_back(J);
             }
+            DGPU_CHECK_CUDA(cudaMemsetAsync(tabs.flags, 0, tabs.flags_bytes, st));
             {
                 const int nj = (int)jobs.size();
                 DGPU_CHECK_CUDA(cudaMemcpyAsync(tabs.mode, jobs.data(), sizeof(ModeJob) * nj, cudaMemcpyHostToDevice,
