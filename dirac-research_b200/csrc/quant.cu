@@ -162,10 +162,13 @@ __device__ __forceinline__ unsigned udiv_recip(unsigned n, unsigned d, float inv
     return q;
 }
 
+// Statistics of one sampling pattern (0: 2 x 2 for the first two passes, over every even
+// quantiser; 1: 1 x 2 for the third pass, over the per-band range qrange[band] = (lo, hi)).
+// Layout: stats[(pattern * nbands + band) * QMAX + q].
 __global__ void __launch_bounds__(STAT_THREADS) stats_kernel(const BandTask* tasks, const int* band_max,
-                                                             Stat* stats) {
+                                                             Stat* stats, int pattern, int nbands,
+                                                             const int2* qrange) {
     const BandTask T = tasks[blockIdx.y];
-    const int pattern = blockIdx.z;
     const int xr = pattern ? 1 : 2;
     const int nq = stat_range(band_max[T.band]);
     const int sx = (T.xl + xr - 1) / xr, sy = (T.yl + 1) / 2;
@@ -195,7 +198,9 @@ __global__ void __launch_bounds__(STAT_THREADS) stats_kernel(const BandTask* tas
         }
     }
     const int lane = threadIdx.x & 31;
-    for (int q = (pattern ? 0 : 0); q < nq; q += (pattern ? 1 : 2)) {
+    const int qlo = qrange ? qrange[T.band].x : 0;
+    const int qhi = qrange ? min(qrange[T.band].y, nq - 1) : nq - 1;
+    for (int q = qlo; q <= qhi; q += (pattern ? 1 : 2)) {
         const unsigned qf = (unsigned)qf4(q);
         const float inv = __frcp_rn((float)qf);
         const int off = inter_off4(q);
@@ -244,7 +249,7 @@ __global__ void __launch_bounds__(STAT_THREADS) stats_kernel(const BandTask* tas
         }
     }
     __syncthreads();
-    Stat* S = stats + ((size_t)T.band * 2 + pattern) * QMAX;
+    Stat* S = stats + ((size_t)pattern * nbands + T.band) * QMAX;
     for (int q = threadIdx.x; q < nq; q += STAT_THREADS) {
         if (s_c0[q] == 0 && s_pn[q] == 0 && s_lo[q] == 0 && s_hi[q] == 0 && s_inx[q] == 0) continue;
         atomicAdd(&S[q].count0, s_c0[q]);
@@ -454,6 +459,7 @@ static int pinned_scratch(size_t bytes, char** out) {
 // sequential-sum fallback cases.
 static size_t residue_ws_need(int nb_total, int ncb_total, size_t dcwork_elems) {
     return align_up(sizeof(BandTask) * nb_total, 256) + align_up(sizeof(int) * nb_total, 256) +
+           align_up(sizeof(int2) * nb_total, 256) +
            align_up(sizeof(int) * ncb_total, 256) + align_up(sizeof(Stat) * nb_total * 2 * QMAX, 256) +
            align_up(sizeof(int32_t) * dcwork_elems, 256) + align_up(ncb_total, 256) +
            align_up((sizeof(SeqCase) + sizeof(double)) * nb_total * 2 * QMAX, 256) + 256;
@@ -521,6 +527,7 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     };
     BandTask* d_tasks = reinterpret_cast<BandTask*>(take(sizeof(BandTask) * nb_total));
     int* d_band_max = reinterpret_cast<int*>(take(sizeof(int) * nb_total));
+    int2* d_range = reinterpret_cast<int2*>(take(sizeof(int2) * nb_total));
     int* d_cb_max = reinterpret_cast<int*>(take(sizeof(int) * ncb_total));
     Stat* d_stats = reinterpret_cast<Stat*>(take(sizeof(Stat) * nb_total * 2 * QMAX));
     int32_t* d_dcwork = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * dcwork_elems));
@@ -569,50 +576,57 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
         band_max_kernel<<<grid, 256, 0, st>>>(d_tasks, d_band_max, d_cb_max);
         DGPU_CHECK_LAUNCH();
     }
-    // ---- 2. statistics ----
-    {
-        int maxs = 0;
-        for (const BandTask& T : tasks) maxs = std::max(maxs, T.xl * ((T.yl + 1) / 2));
-        dim3 grid((maxs + STAT_THREADS * 8 - 1) / (STAT_THREADS * 8), nb_total, 2);
-        stats_kernel<<<grid, STAT_THREADS, 0, st>>>(d_tasks, d_band_max, d_stats);
-        DGPU_CHECK_LAUNCH();
-    }
+    // ---- 2. statistics and the reference's three-pass Lagrangian choice per band ----
+    // Passes 1 and 2 use the 2 x 2 pattern over every even quantiser; pass 3 needs the 1 x 2
+    // pattern at three quantisers only, known once pass 2 is decided: its statistics are
+    // gathered in a second, much smaller launch.
+    int maxs = 0;
+    for (const BandTask& T : tasks) maxs = std::max(maxs, T.xl * ((T.yl + 1) / 2));
+    const dim3 sgrid((maxs + STAT_THREADS * 8 - 1) / (STAT_THREADS * 8), nb_total, 1);
+    stats_kernel<<<sgrid, STAT_THREADS, 0, st>>>(d_tasks, d_band_max, d_stats, 0, nb_total, nullptr);
+    DGPU_CHECK_LAUNCH();
     // statistics and maxima come back through page-locked memory (one buffer per host thread)
-    const size_t n_stats = (size_t)nb_total * 2 * QMAX;
+    const size_t n_pat = (size_t)nb_total * QMAX;
     char* pin = nullptr;
     {
-        const int rc = pinned_scratch(sizeof(Stat) * n_stats + sizeof(int) * (nb_total + ncb_total) + 64, &pin);
+        const int rc = pinned_scratch(sizeof(Stat) * 2 * n_pat + sizeof(int) * (nb_total + ncb_total) +
+                                          sizeof(int2) * nb_total + 256, &pin);
         if (rc) return rc;
     }
     Stat* hs = reinterpret_cast<Stat*>(pin);
-    int* hmax = reinterpret_cast<int*>(pin + sizeof(Stat) * n_stats);
+    int* hmax = reinterpret_cast<int*>(pin + sizeof(Stat) * 2 * n_pat);
     int* hcb = hmax + nb_total;
-    DGPU_CHECK_CUDA(cudaMemcpyAsync(hs, d_stats, sizeof(Stat) * n_stats, cudaMemcpyDeviceToHost, st));
+    int2* hrange = reinterpret_cast<int2*>(align_up(reinterpret_cast<size_t>(hcb + ncb_total), 16));
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(hs, d_stats, sizeof(Stat) * n_pat, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaMemcpyAsync(hmax, d_band_max, sizeof(int) * nb_total, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaMemcpyAsync(hcb, d_cb_max, sizeof(int) * ncb_total, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
-    // ---- 3a. sums the exact path could not represent: sequential double kernel ----
-    std::vector<SeqCase> cases;
-    std::vector<int> case_of((size_t)nb_total * 2 * QMAX, -1);
-    for (int t = 0; t < nb_total; ++t)
-        for (int pat = 0; pat < 2; ++pat)
+    // sums the exact path could not represent: the sequential double kernel for those cases
+    std::vector<int> case_of(2 * n_pat, -1);
+    std::vector<double> seq;
+    auto resolve_inexact = [&](int pat) -> int {
+        std::vector<SeqCase> cases;
+        for (int t = 0; t < nb_total; ++t)
             for (int q = 0; q < QMAX; ++q) {
-                const Stat& S = hs[((size_t)t * 2 + pat) * QMAX + q];
+                const size_t k = pat * n_pat + (size_t)t * QMAX + q;
+                const Stat& S = hs[k];
                 if (S.inexact || S.err_hi != 0 || S.err_lo >= (1ull << 53)) {
-                    case_of[((size_t)t * 2 + pat) * QMAX + q] = (int)cases.size();
+                    case_of[k] = (int)(seq.size() + cases.size());
                     cases.push_back(SeqCase{t, pat, q});
                 }
             }
-    std::vector<double> seq(cases.size());
-    if (!cases.empty()) {
+        if (cases.empty()) return DGPU_OK;
+        std::vector<double> out(cases.size());
         DGPU_CHECK_CUDA(cudaMemcpyAsync(d_cases, cases.data(), sizeof(SeqCase) * cases.size(), cudaMemcpyHostToDevice, st));
         seq_error_kernel<<<((int)cases.size() + 127) / 128, 128, 0, st>>>(d_tasks, d_cases, (int)cases.size(), d_seq);
         DGPU_CHECK_LAUNCH();
-        DGPU_CHECK_CUDA(cudaMemcpyAsync(seq.data(), d_seq, sizeof(double) * cases.size(), cudaMemcpyDeviceToHost, st));
+        DGPU_CHECK_CUDA(cudaMemcpyAsync(out.data(), d_seq, sizeof(double) * cases.size(), cudaMemcpyDeviceToHost, st));
         DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
-    }
+        seq.insert(seq.end(), out.begin(), out.end());
+        return DGPU_OK;
+    };
     auto host_stat = [&](int t, int pat, int q) {
-        const size_t k = ((size_t)t * 2 + pat) * QMAX + q;
+        const size_t k = pat * n_pat + (size_t)t * QMAX + q;
         const Stat& S = hs[k];
         HostStat h;
         h.count0 = (int)(uint32_t)S.count0;
@@ -621,38 +635,66 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
         h.error = case_of[k] >= 0 ? seq[case_of[k]] : (double)S.err_lo;
         return h;
     };
-    // ---- 3b. the reference's three-pass Lagrangian choice per band ----
-    std::vector<uint8_t> hskip(ncb_total, 0);
+    {
+        const int rc = resolve_inexact(0);
+        if (rc) return rc;
+    }
+    std::vector<std::vector<CostD>> cost(nb_total);
+    std::vector<int> mn2(nb_total, 0), nqs(nb_total, 0);
     for (int t = 0; t < nb_total; ++t) {
         const BandTask& T = tasks[t];
         const int maxv = hmax[t];
-        int q = 0, bits = 0;
-        if (maxv >= 1) {
-            const int max_bit = int(std::floor(std::log(float(maxv)) / std::log(2.0)));
-            const int nq = 4 * max_bit + 5;
-            if (nq > QMAX) return DGPU_ERR_SIZE;
-            std::vector<CostD> cost(nq);
-            int lo = 0, hi = nq - 1, step = 4, pat = 0, xr = 2, mn = 0;
-            for (int pass = 0; pass < 3; ++pass) {
-                if (pass == 1) {
-                    lo = std::max(mn - 2, 0);
-                    hi = std::min(mn + 2, nq - 1);
-                    step = 2;
-                } else if (pass == 2) {
-                    lo = std::max(mn - 1, 0);
-                    hi = std::min(mn + 1, nq - 1);
-                    step = 1;
-                    pat = 1;
-                    xr = 1;
-                }
-                const int count1 = (T.xl / xr) * (T.yl / 2);
-                for (int qq = lo; qq <= hi; qq += step)
-                    cost[qq] = lagrangian(host_stat(t, pat, qq), count1, band_wt[t], lambda[T.comp], band_ecf[t]);
-                mn = lo;
-                for (int qq = lo + step; qq <= hi; qq += step)
-                    if (cost[qq].TOTAL < cost[mn].TOTAL) mn = qq;
+        hrange[t] = make_int2(0, -1);
+        if (maxv < 1) continue;
+        const int max_bit = int(std::floor(std::log(float(maxv)) / std::log(2.0)));
+        const int nq = 4 * max_bit + 5;
+        if (nq > QMAX) return DGPU_ERR_SIZE;
+        nqs[t] = nq;
+        cost[t].resize(nq);
+        int lo = 0, hi = nq - 1, step = 4, mn = 0;
+        for (int pass = 0; pass < 2; ++pass) {
+            if (pass == 1) {
+                lo = std::max(mn - 2, 0);
+                hi = std::min(mn + 2, nq - 1);
+                step = 2;
             }
-            const double bit_sum = cost[mn].ENTROPY * T.xl * T.yl;
+            const int count1 = (T.xl / 2) * (T.yl / 2);
+            for (int qq = lo; qq <= hi; qq += step)
+                cost[t][qq] = lagrangian(host_stat(t, 0, qq), count1, band_wt[t], lambda[T.comp], band_ecf[t]);
+            mn = lo;
+            for (int qq = lo + step; qq <= hi; qq += step)
+                if (cost[t][qq].TOTAL < cost[t][mn].TOTAL) mn = qq;
+        }
+        mn2[t] = mn;
+        hrange[t] = make_int2(std::max(mn - 1, 0), std::min(mn + 1, nq - 1));
+    }
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(d_range, hrange, sizeof(int2) * nb_total, cudaMemcpyHostToDevice, st));
+    {
+        int maxs1 = 0;
+        for (const BandTask& T : tasks) maxs1 = std::max(maxs1, T.xl * ((T.yl + 1) / 2));
+        const dim3 grid1((maxs1 + STAT_THREADS * 8 - 1) / (STAT_THREADS * 8), nb_total, 1);
+        stats_kernel<<<grid1, STAT_THREADS, 0, st>>>(d_tasks, d_band_max, d_stats, 1, nb_total, d_range);
+        DGPU_CHECK_LAUNCH();
+    }
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(hs + n_pat, d_stats + n_pat, sizeof(Stat) * n_pat, cudaMemcpyDeviceToHost, st));
+    DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
+    {
+        const int rc = resolve_inexact(1);
+        if (rc) return rc;
+    }
+    std::vector<uint8_t> hskip(ncb_total, 0);
+    for (int t = 0; t < nb_total; ++t) {
+        const BandTask& T = tasks[t];
+        int q = 0, bits = 0;
+        if (hmax[t] >= 1) {
+            const int lo = hrange[t].x, hi = hrange[t].y;
+            const int count1 = (T.xl / 1) * (T.yl / 2);
+            for (int qq = lo; qq <= hi; ++qq)
+                cost[t][qq] = lagrangian(host_stat(t, 1, qq), count1, band_wt[t], lambda[T.comp], band_ecf[t]);
+            int mn = lo;
+            for (int qq = lo + 1; qq <= hi; ++qq)
+                if (cost[t][qq].TOTAL < cost[t][mn].TOTAL) mn = qq;
+            const double bit_sum = cost[t][mn].ENTROPY * T.xl * T.yl;
             bits = int(bit_sum);
             q = mn;
             const int thr = qf4(q);
