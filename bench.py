@@ -12,9 +12,10 @@ reference); the encoder keeps the initial entropy-correction factors.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gpu|reference]
 
-`value`: frames/s of the batched form (--streams sequences encoded concurrently on one GPU,
-each by its own encoder, CUDA stream and host thread) with the input frames resident in
-HBM; `plain` gives the same for one sequence at a time.  `e2e`: the batched form through
+`value`: frames/s of the batched form (--streams sequences per GPU, each with its own
+encoder, CUDA stream and host thread; the motion estimation of all of them runs as one
+batched launch through an encoder group) with the input frames resident in HBM;
+`batched_streams_only` gives the same without the group (each sequence estimating alone); `plain` gives the same for one sequence at a time.  `e2e`: the batched form through
 the encoder's C ABI from pinned host frames, reading back per picture what the host coder
 needs (quantised indices, band choices, code-block skips, motion data).  Every step works on
 gigabytes of distinct device buffers (far above the 126 MB L2), so no L2 flush is needed.
@@ -285,12 +286,17 @@ def main():
                     raise RuntimeError(f"dgpu_encoder_read failed: {rc}")
                 self.d2h += n
 
-        def step(self, src, events=None, with_read=False):
+        def load(self, src):
             enc = self.enc
             enc.reset()
             for f in src:
                 enc.load(f)
             enc.end_sequence()
+
+        def step(self, src, events=None, with_read=False, loaded=False):
+            enc = self.enc
+            if not loaded:
+                self.load(src)
             infos = []
             while True:
                 if events is not None:
@@ -311,10 +317,12 @@ def main():
     def max_over_ranks(ms):
         return max_over_ranks_ms(ms, world, "cuda")
 
-    def timed(lanes, src, steps, with_read=False):
+    def timed(lanes, src, steps, with_read=False, group=None):
         """Device time (ms) of `steps` sequence encodes on every lane, the lanes running
         concurrently: a start event on the main stream that every lane stream waits on, and an
-        end event after the main stream has waited on every lane's last work."""
+        end event after the main stream has waited on every lane's last work.  With a group,
+        each step loads every lane's sequence (lane threads), runs the group's batched motion
+        estimation, then codes every lane (lane threads)."""
         from concurrent.futures import ThreadPoolExecutor
 
         main = torch.cuda.current_stream()
@@ -330,7 +338,13 @@ def main():
             for _ in range(steps):
                 ln.step(src, with_read=with_read)
 
-        if len(lanes) == 1:
+        if group is not None:
+            with ThreadPoolExecutor(len(lanes)) as ex:
+                for _ in range(steps):
+                    list(ex.map(lambda ln: ln.load(src), lanes))
+                    group.estimate()
+                    list(ex.map(lambda ln: ln.step(src, with_read=with_read, loaded=True), lanes))
+        elif len(lanes) == 1:
             run(lanes[0])
         else:
             with ThreadPoolExecutor(len(lanes)) as ex:
@@ -346,18 +360,19 @@ def main():
 
     lanes = [Lane() for _ in range(args.streams)]
     plain = lanes[0]
+    group = E.EncoderGroup([ln.enc for ln in lanes])
 
     # ---- warm-up: every lane, both input forms ------------------------------------------------
     for _ in range(args.warmup):
-        timed(lanes, dev_frames, 1)
-    timed(lanes, pinned_np, 1, with_read=True)
+        timed(lanes, dev_frames, 1, group=group)
+    timed(lanes, pinned_np, 1, with_read=True, group=group)
 
     # ---- timed region (batched form): inputs resident in HBM ---------------------------------
     clocks = ClockSampler(local_rank)
     clocks.start()
     time.sleep(0.3)
     launches0 = lib.dgpu_launch_count()
-    ms = timed(lanes, dev_frames, args.steps)
+    ms = timed(lanes, dev_frames, args.steps, group=group)
     launches = lib.dgpu_launch_count() - launches0
     clk = clocks.stop()
     frames_per_step = args.frames * len(lanes)
@@ -365,10 +380,16 @@ def main():
     value = whole_job_rate(world, frames_per_step, args.steps, ms)
 
     # ---- end to end (batched form) through the C ABI with host buffers -------------------------
-    ems = timed(lanes, pinned_np, args.steps, with_read=True)
+    ems = timed(lanes, pinned_np, args.steps, with_read=True, group=group)
     h2d = sum(p.nbytes for fr in pinned_np for p in fr) * len(lanes)
     e2e = {"value": whole_job_rate(world, frames_per_step, args.steps, ems), "unit": "frames/s",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": sum(ln.d2h for ln in lanes) // args.steps}
+
+    # ---- batched form without the group: concurrent sequences, each estimating alone -----------
+    sms = timed(lanes, dev_frames, args.steps)
+    streams_only = {"value": whole_job_rate(world, frames_per_step, args.steps, sms), "unit": "frames/s",
+                    "ms_per_step": sms / args.steps,
+                    "form": f"{len(lanes)} concurrent sequences, each with its own motion-estimation launches"}
 
     # ---- plain form: one sequence at a time ----------------------------------------------------
     pms = timed([plain], dev_frames, args.steps)
@@ -416,6 +437,7 @@ def main():
                 "algorithmic_bytes_per_step": alg, "stages": per_stage,
                 "note": "plain form, one sequence; stage times from CUDA events on the encoder stream in a "
                         "separate profiled pass"}
+    group.close()
     for ln in lanes:
         ln.enc.close()
 
@@ -436,10 +458,11 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
                 "config": {"workload": workload_name(args.frames), "frames_per_step": frames_per_step,
                            "global_batch": world * frames_per_step, "parallelism": f"replicas{world}",
-                           "form": f"batched: {len(lanes)} concurrent sequences per GPU, each on its own stream "
-                                   "and host thread",
+                           "form": f"batched: {len(lanes)} sequences per GPU; the motion estimation of all of "
+                                   "them in one batched launch (encoder group), the rest of each sequence's coding "
+                                   "on its own stream and host thread",
                            "l2": "inputs and working set larger than L2 (no flush needed)"},
-                "plain": plain_line, "roofline": roofline, "cpu_baseline": cpu_baseline, "e2e": e2e,
+                "plain": plain_line, "batched_streams_only": streams_only, "roofline": roofline, "cpu_baseline": cpu_baseline, "e2e": e2e,
                 "latency_ms": latency, "serving": serving, "gpu_launches": launches, "clocks": clk}
         print(json.dumps(line), flush=True)
     if world > 1:

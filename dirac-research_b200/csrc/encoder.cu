@@ -312,21 +312,26 @@ bool predicted_refs(const Encoder& E, const Pic& q, std::vector<int>& refs) {
     return !intra;
 }
 
-// Motion estimation of p against its current references, batched with every other loaded
-// picture whose references are (or will most likely be) known and already loaded.
-int ensure_me(Encoder& E, Pic& p) {
-    if (p.me_valid && p.me_refs == p.refs) return DGPU_OK;
-    StageTimer timer(E, DGPU_STAGE_ME);
-    struct Task {
-        int pnum;
-        std::vector<int> refs;
-    };
-    std::vector<Task> tasks;
-    tasks.push_back({p.pnum, p.refs});
+struct MeTask {
+    Encoder* E;
+    int pnum;
+    std::vector<int> refs;
+};
+
+// Motion-estimation tasks of E: `first` (when given) against its current references, then
+// every other loaded, uncoded picture whose references are (or will most likely be) known and
+// already loaded and whose estimate is missing or was made against other references; at most
+// `cap` tasks.
+void collect_me_tasks(Encoder& E, const Pic* first, int cap, std::vector<MeTask>& tasks) {
+    int n = 0;
+    if (first) {
+        tasks.push_back({&E, first->pnum, first->refs});
+        ++n;
+    }
     for (auto& kv : E.pics) {
         Pic& q = kv.second;
-        if ((int)tasks.size() >= E.me_max_tasks) break;
-        if (q.pnum == p.pnum || q.coded) continue;
+        if (n >= cap) break;
+        if ((first && q.pnum == first->pnum) || q.coded || q.slot < 0) continue;
         // without the end of the sequence, a picture's references may still change as
         // pictures arrive: only look at pictures a full sub-group before the last loaded
         if (!E.eos && q.pnum + std::max(E.L1Sep, 1) > E.last_read) continue;
@@ -335,33 +340,48 @@ int ensure_me(Encoder& E, Pic& p) {
         if (q.me_valid && q.me_refs == refs) continue;
         bool ok = true;
         for (int r : refs) ok = ok && r >= 0 && r <= E.last_read && E.pics.count(r) && E.pics[r].slot >= 0;
-        if (ok) tasks.push_back({q.pnum, refs});
+        if (ok) {
+            tasks.push_back({&E, q.pnum, refs});
+            ++n;
+        }
     }
+}
+
+// Runs the tasks (of one or several encoders with the same picture size, chroma format,
+// block parameters and luma depth) in one batched estimation on stream st, then records each
+// picture's estimate and intra-block ratio.  ws: workspace of ws_bytes; d_counts / h_counts:
+// device / pinned host ints, one per task.
+int run_me_tasks(const std::vector<MeTask>& tasks, cudaStream_t st, void* ws, size_t ws_bytes, int* d_counts,
+                 int* h_counts) {
+    if (tasks.empty()) return DGPU_OK;
+    Encoder& E0 = *tasks[0].E;
     // pictures involved, in first-use order
-    std::vector<int> pics_used;
-    auto index_of = [&](int pn) {
+    std::vector<std::pair<Encoder*, int>> pics_used;
+    auto index_of = [&](Encoder* e, int pn) {
         for (size_t k = 0; k < pics_used.size(); ++k)
-            if (pics_used[k] == pn) return (int)k;
-        pics_used.push_back(pn);
+            if (pics_used[k].first == e && pics_used[k].second == pn) return (int)k;
+        pics_used.push_back({e, pn});
         return (int)pics_used.size() - 1;
     };
     const int nt = (int)tasks.size();
     std::vector<int> tp(nt), t1(nt), t2(nt);
-    std::vector<float> tl(nt, E.L.me);  // L1MELambda == L2MELambda (common.cpp:464-465)
+    std::vector<float> tl(nt);
     for (int t = 0; t < nt; ++t) {
-        tp[t] = index_of(tasks[t].pnum);
-        t1[t] = index_of(tasks[t].refs[0]);
-        t2[t] = tasks[t].refs.size() > 1 ? index_of(tasks[t].refs[1]) : -1;
+        tp[t] = index_of(tasks[t].E, tasks[t].pnum);
+        t1[t] = index_of(tasks[t].E, tasks[t].refs[0]);
+        t2[t] = tasks[t].refs.size() > 1 ? index_of(tasks[t].E, tasks[t].refs[1]) : -1;
+        tl[t] = tasks[t].E->L.me;  // L1MELambda == L2MELambda (common.cpp:464-465)
     }
     std::vector<const int16_t*> planes;
-    for (int pn : pics_used) {
-        Slot& s = E.slots[E.pics[pn].slot];
+    for (auto& pu : pics_used) {
+        Slot& s = pu.first->slots[pu.first->pics[pu.second].slot];
         for (int c = 0; c < 3; ++c) planes.push_back(s.orig[c]);
     }
     std::vector<int16_t*> mv(nt), dc(nt);
     std::vector<float*> cost(nt), sbc(nt);
     std::vector<uint8_t*> mode(nt), split(nt);
     for (int t = 0; t < nt; ++t) {
+        Encoder& E = *tasks[t].E;
         Slot& s = E.slots[E.pics[tasks[t].pnum].slot];
         mv[t] = s.mv;
         cost[t] = s.cost;
@@ -370,28 +390,39 @@ int ensure_me(Encoder& E, Pic& p) {
         split[t] = s.split;
         sbc[t] = s.sbcost;
     }
-    int rc = dgpu_motion_estimate_batch(E.P.cformat, E.w[0], E.h[0], &E.bp, E.P.luma_depth, (int)pics_used.size(),
-                                        planes.data(), nt, tp.data(), t1.data(), t2.data(), tl.data(), 3, mv.data(),
-                                        cost.data(), mode.data(), dc.data(), split.data(), sbc.data(), E.me_ws,
-                                        E.me_ws_bytes, E.st);
+    int rc = dgpu_motion_estimate_batch(E0.P.cformat, E0.w[0], E0.h[0], &E0.bp, E0.P.luma_depth,
+                                        (int)pics_used.size(), planes.data(), nt, tp.data(), t1.data(), t2.data(),
+                                        tl.data(), 3, mv.data(), cost.data(), mode.data(), dc.data(), split.data(),
+                                        sbc.data(), ws, ws_bytes, st);
     if (rc) return rc;
     for (int t0 = 0; t0 < nt; t0 += kMaxCountTasks) {
         CountArgs A{};
         const int k = std::min(kMaxCountTasks, nt - t0);
         for (int t = 0; t < k; ++t) A.mode[t] = mode[t0 + t];
-        A.n = E.nblocks;
-        count_intra_kernel<<<k, 256, 0, E.st>>>(A, E.d_counts + t0);
+        A.n = E0.nblocks;
+        count_intra_kernel<<<k, 256, 0, st>>>(A, d_counts + t0);
         DGPU_CHECK_LAUNCH();
     }
-    DGPU_CHECK_CUDA(cudaMemcpyAsync(E.h_counts, E.d_counts, sizeof(int) * nt, cudaMemcpyDeviceToHost, E.st));
-    DGPU_CHECK_CUDA(cudaStreamSynchronize(E.st));
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(h_counts, d_counts, sizeof(int) * nt, cudaMemcpyDeviceToHost, st));
+    DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
     for (int t = 0; t < nt; ++t) {
+        Encoder& E = *tasks[t].E;
         Pic& q = E.pics[tasks[t].pnum];
         q.me_valid = true;
         q.me_refs = tasks[t].refs;
-        q.ratio = (double)E.h_counts[t] / (double)E.nblocks;
+        q.ratio = (double)h_counts[t] / (double)E.nblocks;
     }
     return DGPU_OK;
+}
+
+// Motion estimation of p against its current references, batched with every other loaded
+// picture whose references are (or will most likely be) known and already loaded.
+int ensure_me(Encoder& E, Pic& p) {
+    if (p.me_valid && p.me_refs == p.refs) return DGPU_OK;
+    StageTimer timer(E, DGPU_STAGE_ME);
+    std::vector<MeTask> tasks;
+    collect_me_tasks(E, &p, E.me_max_tasks, tasks);
+    return run_me_tasks(tasks, E.st, E.me_ws, E.me_ws_bytes, E.d_counts, E.h_counts);
 }
 
 int motion_compensate(Encoder& E, Pic& p, int add_or_sub, bool clip) {
@@ -922,5 +953,132 @@ extern "C" int dgpu_encoder_read(void* enc, int pnum, int what, int comp, void* 
     }
     DGPU_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, E->st));
     if (on_host) DGPU_CHECK_CUDA(cudaStreamSynchronize(E->st));
+    return DGPU_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Encoder groups: the motion estimation of several sequences in one batched launch
+// ---------------------------------------------------------------------------------------
+namespace dgpu {
+namespace {
+
+struct Group {
+    std::vector<Encoder*> enc;
+    cudaStream_t st = nullptr;   // owned
+    cudaEvent_t ev = nullptr;    // ordering between the encoders' streams and st
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    int max_tasks = 0;
+    int* d_counts = nullptr;
+    int* h_counts = nullptr;     // pinned
+
+    ~Group() {
+        if (st) cudaStreamSynchronize(st);
+        if (ws) cudaFree(ws);
+        if (d_counts) cudaFree(d_counts);
+        if (h_counts) cudaFreeHost(h_counts);
+        if (ev) cudaEventDestroy(ev);
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+bool same_geometry(const Encoder& a, const Encoder& b) {
+    return a.P.cformat == b.P.cformat && a.P.width == b.P.width && a.P.height == b.P.height &&
+           a.P.luma_depth == b.P.luma_depth && a.bp.precision == b.bp.precision && a.bp.xblen == b.bp.xblen &&
+           a.bp.yblen == b.bp.yblen && a.bp.xbsep == b.bp.xbsep && a.bp.ybsep == b.bp.ybsep;
+}
+
+// Workspace of one batch holding every member's largest estimation batch.
+size_t group_ws_bytes(const std::vector<Encoder*>& enc, int* max_tasks) {
+    int nt = 0, np = 0;
+    for (Encoder* E : enc) {
+        nt += E->me_max_tasks;
+        np += std::min((int)E->slots.size(), 3 * E->me_max_tasks);
+    }
+    *max_tasks = nt;
+    std::vector<int> r2(nt, 0);
+    const Encoder& E0 = *enc[0];
+    return dgpu_me_batch_workspace_bytes(E0.P.cformat, E0.P.width, E0.P.height, &E0.bp, np, nt, r2.data(), 3);
+}
+
+}  // namespace
+}  // namespace dgpu
+
+extern "C" size_t dgpu_encoder_group_device_bytes(void* const* encoders, int n) {
+    if (!encoders || n < 1) return 0;
+    std::vector<Encoder*> enc;
+    for (int k = 0; k < n; ++k) {
+        Encoder* E = static_cast<Encoder*>(encoders[k]);
+        if (!E || !same_geometry(*E, *static_cast<Encoder*>(encoders[0]))) return 0;
+        enc.push_back(E);
+    }
+    int nt = 0;
+    const size_t ws = group_ws_bytes(enc, &nt);
+    return ws ? align_up(ws, 256) + align_up(sizeof(int) * nt, 256) : 0;
+}
+
+extern "C" int dgpu_encoder_group_create(void* const* encoders, int n, void** out) {
+    if (!encoders || n < 1 || !out) return DGPU_ERR_ARG;
+    *out = nullptr;
+    Group* G = new (std::nothrow) Group();
+    if (!G) return DGPU_ERR_NOMEM;
+    for (int k = 0; k < n; ++k) {
+        Encoder* E = static_cast<Encoder*>(encoders[k]);
+        bool dup = false;
+        for (Encoder* e : G->enc) dup = dup || e == E;
+        if (!E || dup || !same_geometry(*E, *static_cast<Encoder*>(encoders[0]))) {
+            delete G;
+            return DGPU_ERR_ARG;
+        }
+        G->enc.push_back(E);
+    }
+    G->ws_bytes = group_ws_bytes(G->enc, &G->max_tasks);
+    if (G->ws_bytes == 0) {
+        delete G;
+        return DGPU_ERR_ARG;
+    }
+    if (cudaStreamCreateWithFlags(&G->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&G->ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMalloc(&G->ws, G->ws_bytes) != cudaSuccess ||
+        cudaMalloc(reinterpret_cast<void**>(&G->d_counts), sizeof(int) * G->max_tasks) != cudaSuccess ||
+        cudaMallocHost(reinterpret_cast<void**>(&G->h_counts), sizeof(int) * G->max_tasks) != cudaSuccess) {
+        cudaGetLastError();
+        delete G;
+        return DGPU_ERR_NOMEM;
+    }
+    *out = G;
+    return DGPU_OK;
+}
+
+extern "C" int dgpu_encoder_group_destroy(void* group) {
+    Group* G = static_cast<Group*>(group);
+    if (!G) return DGPU_ERR_ARG;
+    delete G;
+    return DGPU_OK;
+}
+
+extern "C" int dgpu_encoder_group_estimate(void* group, int* ntasks) {
+    Group* G = static_cast<Group*>(group);
+    if (ntasks) *ntasks = 0;
+    if (!G) return DGPU_ERR_ARG;
+    std::vector<MeTask> tasks;
+    for (Encoder* E : G->enc) {
+        if (E->last_read < 0) continue;
+        // the loop's picture types are set one sub-group ahead of the coded picture, exactly
+        // as dgpu_encoder_code_next sets them; untyped pictures get their likely references
+        collect_me_tasks(*E, nullptr, E->me_max_tasks, tasks);
+    }
+    if (tasks.empty()) return DGPU_OK;
+    // the group's stream follows every member's stream (their loads), and each member's
+    // stream follows the estimation (the host waits for it below as well)
+    for (Encoder* E : G->enc) {
+        DGPU_CHECK_CUDA(cudaEventRecord(G->ev, E->st));
+        DGPU_CHECK_CUDA(cudaStreamWaitEvent(G->st, G->ev, 0));
+    }
+    const int rc = run_me_tasks(tasks, G->st, G->ws, G->ws_bytes, G->d_counts, G->h_counts);
+    if (rc) return rc;
+    DGPU_CHECK_CUDA(cudaEventRecord(G->ev, G->st));
+    for (Encoder* E : G->enc) DGPU_CHECK_CUDA(cudaStreamWaitEvent(E->st, G->ev, 0));
+    if (ntasks) *ntasks = (int)tasks.size();
     return DGPU_OK;
 }

@@ -107,6 +107,10 @@ SIGNATURES = {
     "dgpu_encoder_code_next": (c_int, [c_void_p, c_void_p, c_void_p]),
     "dgpu_encoder_item_bytes": (c_size_t, [c_void_p, c_int, c_int, c_int]),
     "dgpu_encoder_read": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_size_t, c_int]),
+    "dgpu_encoder_group_device_bytes": (c_size_t, [P_void, c_int]),
+    "dgpu_encoder_group_create": (c_int, [P_void, c_int, P_void]),
+    "dgpu_encoder_group_destroy": (c_int, [c_void_p]),
+    "dgpu_encoder_group_estimate": (c_int, [c_void_p, P_int]),
 }
 
 

@@ -148,3 +148,35 @@ class SequenceEncoder:
             if i is None:
                 return infos
             infos.append(i)
+
+
+class EncoderGroup:
+    """Several SequenceEncoders (same picture size, chroma format, luma depth and block
+    parameters) whose motion estimation runs in one batched launch: after each member has
+    loaded its pictures, estimate() estimates every member's inter pictures whose references
+    are known; the members' code_next calls then reuse those estimates."""
+
+    def __init__(self, encoders):
+        self.lib = _lib.load()
+        self.members = list(encoders)
+        self.handle = ctypes.c_void_p()
+        hs = _lib.ptr_array([e.handle.value for e in self.members])
+        _lib.check(self.lib.dgpu_encoder_group_create(hs, len(self.members), ctypes.byref(self.handle)),
+                   "dgpu_encoder_group_create")
+
+    def estimate(self):
+        """Runs the batched estimation; returns the number of picture estimates made."""
+        n = ctypes.c_int(0)
+        _lib.check(self.lib.dgpu_encoder_group_estimate(self.handle, ctypes.byref(n)), "dgpu_encoder_group_estimate")
+        return n.value
+
+    def close(self):
+        if self.handle:
+            self.lib.dgpu_encoder_group_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -363,6 +363,27 @@ size_t dgpu_encoder_item_bytes(void* encoder, int pnum, int what, int comp);
  * copies. */
 int dgpu_encoder_read(void* encoder, int pnum, int what, int comp, void* dst, size_t bytes, int on_host);
 
+/* ---------------------------------------------------------------------------------------
+ * Encoder groups (batched form): the motion estimation of several sequences in one launch.
+ * Replaces nothing in the reference, which codes one sequence per SequenceCompressor; each
+ * member's results are those of PictureCompressor::PixelME / SubPixelME / ModeDecisionME
+ * (libdirac_encoder/picture_compress.cpp:180-298) for the same picture and references.
+ *
+ * Members must share picture size, chroma format, luma depth and block parameters.
+ * dgpu_encoder_group_estimate estimates, for every member, each loaded and uncoded inter
+ * picture whose references are known (a full sub-group behind the last loaded picture, or
+ * any after dgpu_encoder_end_sequence) in one batched launch on the group's own stream, after
+ * the members' pending work; the members' later dgpu_encoder_code_next calls reuse those
+ * estimates (pictures whose references change, e.g. by cut detection, are re-estimated by
+ * their encoder).  *ntasks receives the number of picture estimates made.  The call
+ * synchronises with the estimation; no member may be used by another thread meanwhile.
+ * The group holds a workspace for every member's largest estimation batch.
+ * ------------------------------------------------------------------------------------- */
+size_t dgpu_encoder_group_device_bytes(void* const* encoders, int n);
+int dgpu_encoder_group_create(void* const* encoders, int n, void** group);
+int dgpu_encoder_group_destroy(void* group);
+int dgpu_encoder_group_estimate(void* group, int* ntasks);
+
 #ifdef __cplusplus
 }
 #endif

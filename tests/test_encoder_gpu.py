@@ -185,3 +185,54 @@ def test_encoder_formats_and_depths(gpu, cformat, depth):
         for c in range(3):
             np.testing.assert_array_equal(results[i]["output"][c],
                                           (oenc.pics[i].data[c].astype(np.int32) + off).ravel())
+
+
+def test_encoder_group_estimation(gpu, golden):
+    """Three sequences (a switch to P-only sub-groups, a cut at a B position, a cut at a P
+    position) coded by three encoders whose motion estimation runs as one group batch: every
+    picture equals the oracle's, and the locally decoded pictures the reference encoder's."""
+    from dirac_b200.encoder import EncoderGroup, SequenceEncoder
+
+    cases = [c for c in ENCODE_CASES if c[0] in ("reconfig", "cut_b", "cut_p")]
+    inputs = [encode_inputs(c) for c in cases]
+    encs = [SequenceEncoder(encoder_params(cfg), max_pictures=len(seq)) for seq, cfg in inputs]
+    group = EncoderGroup(encs)
+    for enc, (seq, _) in zip(encs, inputs):
+        for f in seq:
+            enc.load(f)
+        enc.end_sequence()
+    n = group.estimate()
+    assert n == sum(len(seq) - 1 for seq, _ in inputs)  # every picture but the first is inter at first
+    assert group.estimate() == 0  # nothing left to estimate
+    g = golden("encode.npz")
+    for case, enc, (seq, cfg) in zip(cases, encs, inputs):
+        infos = []
+        while True:
+            info = enc.code_next()
+            if info is None:
+                break
+            infos.append(info)
+        results = {i["pnum"]: read_all(enc, i["pnum"]) for i in infos}
+        compare(infos, results, oracle_run(cfg, seq))
+        crc = np.array([[zlib.crc32(np.ascontiguousarray(results[i]["output"][c]).tobytes()) for c in range(3)]
+                        for i in range(len(seq))], np.uint32)
+        np.testing.assert_array_equal(crc, g[case[0] + "_crc"])
+    group.close()
+    for enc in encs:
+        enc.close()
+
+
+def test_encoder_group_rejects_mixed_geometry(gpu):
+    from dirac_b200 import _lib
+    from dirac_b200.encoder import EncoderGroup, SequenceEncoder
+
+    _, cfg = encode_inputs(ENCODE_CASES[1])
+    a = SequenceEncoder(encoder_params(cfg), max_pictures=4)
+    other = dict(encoder_params(cfg), width=352, height=288)
+    b = SequenceEncoder(other, max_pictures=4)
+    with pytest.raises(_lib.DgpuError):
+        EncoderGroup([a, b])
+    with pytest.raises(_lib.DgpuError):
+        EncoderGroup([a, a])
+    a.close()
+    b.close()
