@@ -370,15 +370,24 @@ __device__ __forceinline__ void stage_rect(int16_t* dst, const int16_t* __restri
                                            int y0, int w, int h) {
     const int lane = threadIdx.x & 31;
     const int n = w * h;
+    if (n <= 0) return;
+    // this lane's element i = 32 k + lane sits at row r, column c; both advance by fixed
+    // steps per 32 elements, so no division per element
+    int r = lane / w, c = lane - r * w;
+    const int dr = 32 / w, dc = 32 - dr * w;
     for (int i0 = 0; i0 < n; i0 += 256) {
         int16_t v[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             const int i = i0 + 32 * k + lane;
             v[k] = 0;
-            if (i < n) {
-                const int r = i / w;
-                v[k] = __ldg(&src[(size_t)clampi(y0 + r, 0, ph - 1) * pw + clampi(x0 + i - r * w, 0, pw - 1)]);
+            if (i < n)
+                v[k] = __ldg(&src[(size_t)clampi(y0 + r, 0, ph - 1) * pw + clampi(x0 + c, 0, pw - 1)]);
+            c += dc;
+            r += dr;
+            if (c >= w) {
+                c -= w;
+                ++r;
             }
         }
 #pragma unroll
@@ -455,37 +464,71 @@ __device__ __forceinline__ float subpel_cost_win_p(const SubWin& S, const Blim& 
     return (float)f.c;
 }
 
-__device__ __noinline__ float subpel_cost_win(const SubWin& S, int p, const Blim& b, int mx, int my, float start) {
+__device__ __noinline__ float subpel_cost_win(const SubWin S, int p, const Blim b, int mx, int my, float start) {
     if (p == 1) return subpel_cost_win_p<1>(S, b, mx, my, start);
     if (p == 2) return subpel_cost_win_p<2>(S, b, mx, my, start);
     return subpel_cost_win_p<3>(S, b, mx, my, start);
 }
 
-// Integer total of |pred - pic| over a staged block for one candidate.
+// Integer totals of |pred - pic| over a staged block for the eight neighbours
+// (cx + dx, cy + dy), dx, dy in {-1, 0, 1}, of a centre at precision P, all in one pass over
+// the block: P = 1, the half-pel neighbours of a pel position (each prediction a window
+// sample); P = 2, the quarter-pel neighbours of a half-pel position (cx, cy even: each
+// prediction the rounded mean of two or four samples of the centre's 3 x 3 window
+// neighbourhood, which is what win_pred<2> computes for those offsets).  Lane k returns the
+// total of neighbour k = (dy + 1) * 3 + dx + 1 (lane 4, the centre: 0).
 template <int P>
-__device__ __forceinline__ int subpel_total_win_p(const SubWin& S, const Blim& b, int mx, int my) {
+__device__ __forceinline__ int neighbour_totals(const SubWin S, const Blim& b, int cx, int cy) {
     const int lane = threadIdx.x & 31;
     const int n = b.xl * b.yl;
+    const int ww = S.ww;
+    const int ox = (P == 1 ? cx : cx >> 1) - S.wx0, oy = (P == 1 ? cy : cy >> 1) - S.wy0;
     PixWalk w(b.xl);
-    int tot = 0;
-    for (int k0 = 0; k0 < n; k0 += 256) {
-#pragma unroll
-        for (int s = 0; s < 8; ++s) {
-            const int k = k0 + 32 * s + lane;
-            if (k < n) tot += abs(win_pred<P>(S, b.xp + w.col, b.yp + w.row, mx, my) - S.pic[k]);
-            w.next();
+    int t0 = 0, t1 = 0, t2 = 0, t3 = 0, t5 = 0, t6 = 0, t7 = 0, t8 = 0;
+#pragma unroll 4
+    for (int k = lane; k < n; k += 32) {
+        const int16_t* q = S.up + (2 * (b.yp + w.row) + oy) * ww + 2 * (b.xp + w.col) + ox;
+        const int p = S.pic[k];
+        const int a = q[-ww - 1], bb = q[-ww], c = q[-ww + 1], d = q[-1], f = q[1], g = q[ww - 1], h = q[ww],
+                  i = q[ww + 1];
+        if (P == 1) {
+            t0 += abs(a - p);
+            t1 += abs(bb - p);
+            t2 += abs(c - p);
+            t3 += abs(d - p);
+            t5 += abs(f - p);
+            t6 += abs(g - p);
+            t7 += abs(h - p);
+            t8 += abs(i - p);
+        } else {
+            const int e = q[0];
+            t0 += abs(((a + bb + d + e + 2) >> 2) - p);
+            t1 += abs(((bb + e + 1) >> 1) - p);
+            t2 += abs(((bb + c + e + f + 2) >> 2) - p);
+            t3 += abs(((d + e + 1) >> 1) - p);
+            t5 += abs(((e + f + 1) >> 1) - p);
+            t6 += abs(((d + e + g + h + 2) >> 2) - p);
+            t7 += abs(((e + h + 1) >> 1) - p);
+            t8 += abs(((e + f + h + i + 2) >> 2) - p);
         }
+        w.next();
     }
-    return __reduce_add_sync(0xffffffffu, tot);
+    int mine = 0;
+    const int r0 = __reduce_add_sync(0xffffffffu, t0), r1 = __reduce_add_sync(0xffffffffu, t1),
+              r2 = __reduce_add_sync(0xffffffffu, t2), r3 = __reduce_add_sync(0xffffffffu, t3),
+              r5 = __reduce_add_sync(0xffffffffu, t5), r6 = __reduce_add_sync(0xffffffffu, t6),
+              r7 = __reduce_add_sync(0xffffffffu, t7), r8 = __reduce_add_sync(0xffffffffu, t8);
+    mine = lane == 0 ? r0 : lane == 1 ? r1 : lane == 2 ? r2 : lane == 3 ? r3 : lane == 5 ? r5 : lane == 6 ? r6
+         : lane == 7 ? r7 : lane == 8 ? r8 : 0;
+    return mine;
 }
 
-// The eight half-pel neighbours of (mvx, mvy) << 1, index (dy + 1) * 3 + dx + 1 (the centre,
-// index 4, is the pel vector itself and is never re-evaluated).
-__device__ __noinline__ void half_pel_totals(const SubWin& S, const Blim& b, short2 mv, int* tot) {
-    for (int k = 0; k < 9; ++k) {
-        if (k == 4) continue;
-        tot[k] = subpel_total_win_p<1>(S, b, 2 * mv.x + k % 3 - 1, 2 * mv.y + k / 3 - 1);
-    }
+__device__ __noinline__ int half_pel_totals(const SubWin S, const Blim b, short2 mv) {
+    return neighbour_totals<1>(S, b, 2 * mv.x, 2 * mv.y);
+}
+
+__device__ __noinline__ int quarter_pel_totals(const SubWin S, const Blim b, short2 c) {
+    return neighbour_totals<2>(S, b, c.x, c.y);
 }
 
 // BiBlock*Pel::Diff (me_utils.cpp:1172-1785): |((2 pic - p1) - p2) >> 1| with int16
@@ -607,15 +650,16 @@ __device__ __noinline__ void pel_list_best(const int16_t* pic, const int16_t* re
     stage_rect(win, ref, pw, ph, b.xp + centre.x - r, b.yp + centre.y - r, ww, wh);
     __syncwarp();
     const int n = (2 * r + 1) * (2 * r + 1);
-    int G = 1;
-    while (G * 2 * n <= 32) G <<= 1;
+    // G lanes per candidate, each summing every G-th row: as many lanes busy as the list
+    // allows (9 candidates: 27 lanes)
+    const int G = n >= 32 ? 1 : 32 / n;
     const int per_round = 32 / G;
-    const int g = lane & (G - 1);
+    const int grp = lane / G, g = lane - grp * G;
     int my_best = INT_MAX, my_k = INT_MAX;
     for (int k0 = 0; k0 < n; k0 += per_round) {
-        const int k = k0 + lane / G;
+        const int k = k0 + grp;
         int sad = 0;
-        if (k < n) {
+        if (k < n && grp < per_round) {
             const short2 c = cand_at(centre, r, k);
             const int dx = c.x - centre.x + r, dy = c.y - centre.y + r;
             for (int y = g; y < b.yl; y += G) {
@@ -625,8 +669,14 @@ __device__ __noinline__ void pel_list_best(const int16_t* pic, const int16_t* re
                 for (int x = 0; x < b.xl; ++x) sad += abs((int)(int16_t)(pr[x] - wr[x]));
             }
         }
-        for (int o = 1; o < G; o <<= 1) sad += __shfl_xor_sync(0xffffffffu, sad, o);
-        if (k < n && g == 0 && sad < my_best) {
+        // the group's leader (g == 0) gathers its G - 1 partners, which sit just above it
+        int tot = sad;
+        for (int o = 1; o < G; ++o) {
+            const int v = __shfl_down_sync(0xffffffffu, sad, o);
+            tot += v;
+        }
+        sad = tot;
+        if (k < n && grp < per_round && g == 0 && sad < my_best) {
             my_best = sad;
             my_k = k;
         }
@@ -666,7 +716,7 @@ __global__ void __launch_bounds__(ME_THREADS) pel_lists_kernel(const __grid_cons
             const int gx = clampi(bx >> 1, 0, J.gxnb - 1), gy = clampi(by >> 1, 0, J.gynb - 1);
             const short2 gv = J.guide[(size_t)gy * J.gxnb + gx];
             pel_list_best(J.pic, J.ref, J.pw, J.ph, bl, make_short2((short)(gv.x * 2), (short)(gv.y * 2)), J.radius,
-                          wmem, best, bmv);
+                          wmem, best, bmv, true);
         }
     }
     if ((threadIdx.x & 31) == 0) {
@@ -757,18 +807,20 @@ struct Cost3 {
     float SAD, mvcost, total;
 };
 
-// One candidate of the refinement at precision i: cost from the staged window when there is
-// one, else from global memory; (best, best_mv) updated on a strictly smaller total.
-__device__ __noinline__ void eval_subpel_cand(const SubJob& J, const SubWin& S, bool staged, int i, int sh,
-                                              const Blim& bl, short2 c, short2 pred, float lambda, Cost3& best,
-                                              short2& best_mv, const int* half_tot, short2 mv) {
+// One candidate of the refinement at precision i: from its integer total when the step's
+// neighbour totals are known (fused) and no addition of the reference's loop could round,
+// else from the staged window when there is one, else from global memory; (best, best_mv)
+// updated on a strictly smaller total.
+__device__ __forceinline__ void eval_subpel_cand(const SubJob& J, const SubWin& S, bool staged, bool fused,
+                                                 int total, int i, int sh, const Blim& bl, short2 c, short2 pred,
+                                                 float lambda, Cost3& best, short2& best_mv) {
     const float mvcost = (float)getvarup(pred, c.x << sh, c.y << sh);
     if (bl.xl <= 0 || bl.yl <= 0) return;
     const float start = mvcost * lambda;
     float sum;
     FloatSeq f = float_seq_start(start);
-    if (staged && i == 1 && float_seq_add_exact(f, half_tot[(c.y - 2 * mv.y + 1) * 3 + c.x - 2 * mv.x + 1]))
-        sum = (float)f.c;  // precomputed total, and no addition of the loop could round
+    if (fused && float_seq_add_exact(f, total))
+        sum = (float)f.c;
     else
         sum = staged ? subpel_cost_win(S, i, bl, c.x, c.y, start)
                      : subpel_cost(J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, i, bl, c.x, c.y, start);
@@ -780,7 +832,7 @@ __device__ __noinline__ void eval_subpel_cand(const SubJob& J, const SubWin& S, 
     }
 }
 
-__global__ void __launch_bounds__(ME_THREADS) subpel_wavefront_kernel(const __grid_constant__ SubLaunch L) {
+__global__ void __launch_bounds__(ME_THREADS, 8) subpel_wavefront_kernel(const __grid_constant__ SubLaunch L) {
     extern __shared__ __align__(16) int16_t sub_smem[];
     int16_t* const wmem = sub_smem + (size_t)(threadIdx.x >> 5) * L.win_elems;
     const int prec = L.prec;
@@ -802,11 +854,11 @@ __global__ void __launch_bounds__(ME_THREADS) subpel_wavefront_kernel(const __gr
         const float lambda = J.lambda[b];
         const bool staged = L.win_elems > 0 && bl.xl > 0 && bl.yl > 0 && !(pel_sad < area2);
         SubWin S{};
-        int half_tot[9];
+        int half_tot = 0;  // lane k: total of half-pel neighbour k of the pel vector
         if (staged) {
             stage_subwin(S, wmem, J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, bl, mv);
             // the first refinement step's candidates are all among these eight
-            half_pel_totals(S, bl, mv, half_tot);
+            half_tot = half_pel_totals(S, bl, mv);
         }
         // neighbours in SubpelRefine::m_nshift order: left, top-left, top, top-right
         const int nsx[4] = {-1, -1, 0, 1}, nsy[4] = {0, -1, -1, -1};
@@ -831,9 +883,16 @@ __global__ void __launch_bounds__(ME_THREADS) subpel_wavefront_kernel(const __gr
             out_cost = cost;
         } else {
             Cost3 pc{0.0f, 0.0f, 0.0f};
-            pc.SAD = (bl.xl > 0 && bl.yl > 0)
-                         ? subpel_cost(J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, prec, bl, pred.x, pred.y, 0.0f)
-                         : 0.0f;
+            // the predictor reads the staged window when it lies within the search range
+            const int reach = (1 << prec) - 1;
+            const bool pred_in_win = staged && abs(pred.x - (mv.x << prec)) <= reach &&
+                                     abs(pred.y - (mv.y << prec)) <= reach;
+            if (bl.xl <= 0 || bl.yl <= 0)
+                pc.SAD = 0.0f;
+            else if (pred_in_win)
+                pc.SAD = subpel_cost_win(S, prec, bl, pred.x, pred.y, 0.0f);
+            else
+                pc.SAD = subpel_cost(J.pic, J.pw, J.up, 2 * J.pw, 2 * J.ph, prec, bl, pred.x, pred.y, 0.0f);
             pc.total = pc.SAD;
             if (pc.SAD < area2) {
                 out_mv = pred;
@@ -847,23 +906,32 @@ __global__ void __launch_bounds__(ME_THREADS) subpel_wavefront_kernel(const __gr
                     bmv = make_short2((short)(bmv.x << 1), (short)(bmv.y << 1));
                     short2 tb = bmv;
                     const int sh = prec - i;
+                    // every candidate of the step is one of bmv's eight neighbours: their
+                    // integer totals in one pass (half-pel: computed before the waits)
+                    const bool fused = staged && i <= 2;
+                    const int step_tot = !fused ? 0 : i == 1 ? half_tot : quarter_pel_totals(S, bl, bmv);
                     // the four neighbours, then (after a move) the two across the move
-                    short2 cl[6] = {make_short2(bmv.x - 1, bmv.y), make_short2(bmv.x + 1, bmv.y),
-                                    make_short2(bmv.x, bmv.y - 1), make_short2(bmv.x, bmv.y + 1)};
-                    int nc = 4;
-                    for (int q = 0; q < nc; ++q) {
-                        eval_subpel_cand(J, S, staged, i, sh, bl, cl[q], pred, lambda, best, tb, half_tot, mv);
-                        if (q == 3) {
-                            if (tb.x != bmv.x) {
-                                cl[4] = make_short2(tb.x, tb.y - 1);
-                                cl[5] = make_short2(tb.x, tb.y + 1);
-                                nc = 6;
-                            } else if (tb.y != bmv.y) {
-                                cl[4] = make_short2(tb.x - 1, tb.y);
-                                cl[5] = make_short2(tb.x + 1, tb.y);
-                                nc = 6;
-                            }
+                    int mx = 0, my = 0;  // the move of the first four (0, 0: none)
+                    for (int q = 0; q < 6; ++q) {
+                        int dx, dy;
+                        if (q == 4) {
+                            mx = tb.x - bmv.x;
+                            my = tb.y - bmv.y;
+                            if (mx == 0 && my == 0) break;
                         }
+                        if (q < 4) {
+                            dx = q == 0 ? -1 : q == 1 ? 1 : 0;
+                            dy = q == 2 ? -1 : q == 3 ? 1 : 0;
+                        } else if (mx != 0) {
+                            dx = mx;
+                            dy = q == 4 ? -1 : 1;
+                        } else {
+                            dx = q == 4 ? -1 : 1;
+                            dy = my;
+                        }
+                        const int total = __shfl_sync(0xffffffffu, step_tot, (dy + 1) * 3 + dx + 1);
+                        const short2 c = make_short2((short)(bmv.x + dx), (short)(bmv.y + dy));
+                        eval_subpel_cand(J, S, staged, fused, total, i, sh, bl, c, pred, lambda, best, tb);
                     }
                     bmv = tb;
                     if ((double)best.total > 1.1 * (double)pc.total) {
