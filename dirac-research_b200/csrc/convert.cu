@@ -48,8 +48,9 @@ __device__ __forceinline__ int16_t up_tap_sum(int a0, int b0, int a1, int b1, in
 }
 
 __global__ void __launch_bounds__(UP_THREADS) upconvert_kernel(const __grid_constant__ UpJobs jobs) {
-    __shared__ int16_t src[UTY + 2 * UH][UTX + 2 * UH];  // source tile + halo (clamped)
-    __shared__ int16_t vh[UTY][UTX + 2 * UH];             // vertical half-pel rows
+    constexpr int SWU = UTX + 2 * UH;  // staged width (72)
+    __shared__ int16_t src[UTY + 2 * UH][SWU];  // source tile + halo (clamped)
+    __shared__ int16_t vh[UTY][SWU];             // vertical half-pel rows
 
     int j = 0;
     while (j + 1 < jobs.njobs && jobs.job[j + 1].tile_begin <= (int)blockIdx.x) ++j;
@@ -58,53 +59,71 @@ __global__ void __launch_bounds__(UP_THREADS) upconvert_kernel(const __grid_cons
     const int ty = t / jb.tiles_x, tx = t - ty * jb.tiles_x;
     const int x0 = tx * UTX, y0 = ty * UTY;
 
-    for (int idx = threadIdx.x; idx < (UTY + 2 * UH) * (UTX + 2 * UH); idx += UP_THREADS) {
-        const int r = idx / (UTX + 2 * UH), c = idx - r * (UTX + 2 * UH);
+    // The staged tile holds the source at clamped coordinates, so the taps below index it
+    // directly: a tap row / column clamped to the picture is the staged one (halo >= 4).
+    for (int idx = threadIdx.x; idx < (UTY + 2 * UH) * SWU; idx += UP_THREADS) {
+        const int r = idx / SWU, c = idx - r * SWU;
         const int gy = clampi(y0 - UH + r, 0, jb.h - 1);
         const int gx = clampi(x0 - UH + c, 0, jb.w - 1);
         src[r][c] = jb.src[(size_t)gy * jb.src_stride + gx];
     }
     __syncthreads();
-    // vertical half-pel sample between source rows y and y+1, for every staged column
-    for (int idx = threadIdx.x; idx < UTY * (UTX + 2 * UH); idx += UP_THREADS) {
-        const int r = idx / (UTX + 2 * UH), c = idx - r * (UTX + 2 * UH);
-        const int gy = y0 + r;
-        // source rows gy - t and gy + 1 + t, clamped to the picture
-        int v[8];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            v[2 * k] = src[clampi(gy - k, 0, jb.h - 1) - (y0 - UH)][c];
-            v[2 * k + 1] = src[clampi(gy + 1 + k, 0, jb.h - 1) - (y0 - UH)][c];
-        }
-        const int16_t s = up_tap_sum(v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7]);
+    // vertical half-pel sample between source rows y and y+1 (rows y-3 .. y+4), every column
+    for (int idx = threadIdx.x; idx < UTY * SWU; idx += UP_THREADS) {
+        const int r = idx / SWU, c = idx - r * SWU;
+        const int16_t s = up_tap_sum(src[r + UH][c], src[r + UH + 1][c], src[r + UH - 1][c], src[r + UH + 2][c],
+                                     src[r + UH - 2][c], src[r + UH + 3][c], src[r + UH - 3][c], src[r + UH + 4][c]);
         vh[r][c] = (int16_t)clampi(s, jb.lo, jb.hi);
     }
     __syncthreads();
-    // 2 x 2 output quads; a warp covers 32 consecutive source columns of one row
-    for (int idx = threadIdx.x; idx < UTY * UTX; idx += UP_THREADS) {
-        const int r = idx / UTX, c = idx - r * UTX;
-        const int gy = y0 + r, gx = x0 + c;
-        if (gy >= jb.h || gx >= jb.w) continue;
-        const int sc = c + UH;
-        int a[8], b[8];
+    // 2 x 2 output quads: a thread takes four consecutive source columns of one row and slides
+    // the 8-tap windows of the source row and the vertical half-pel row along them
+    constexpr int NQ = 4;
+    const int r = threadIdx.x / (UTX / NQ), c0 = (threadIdx.x - r * (UTX / NQ)) * NQ;
+    const int gy = y0 + r, gx0 = x0 + c0;
+    if (gy >= jb.h || gx0 >= jb.w) return;
+    int a[NQ + 7], b[NQ + 7];  // staged columns c0 + UH - 3 .. c0 + UH + NQ + 3
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int xl = clampi(gx - k, 0, jb.w - 1) - (x0 - UH);
-            const int xr = clampi(gx + 1 + k, 0, jb.w - 1) - (x0 - UH);
-            a[2 * k] = src[r + UH][xl];
-            a[2 * k + 1] = src[r + UH][xr];
-            b[2 * k] = vh[r][xl];
-            b[2 * k + 1] = vh[r][xr];
-        }
-        const int16_t e1 = (int16_t)clampi(up_tap_sum(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7]), jb.lo, jb.hi);
-        const int16_t o1 = (int16_t)clampi(up_tap_sum(b[0], b[1], b[2], b[3], b[4], b[5], b[6], b[7]), jb.lo, jb.hi);
-        const int16_t e0 = src[r + UH][sc];
-        const int16_t o0 = vh[r][sc];
-        int16_t* d0 = jb.dst + (size_t)(2 * gy) * jb.dst_stride + 2 * gx;
-        int16_t* d1 = d0 + jb.dst_stride;
+    for (int k = 0; k < NQ + 7; ++k) {
+        a[k] = src[r + UH][c0 + UH - 3 + k];
+        b[k] = vh[r][c0 + UH - 3 + k];
+    }
+    int16_t e[2 * NQ], o[2 * NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        // source column c0 + q sits at window index q + 3
+        const int m = q + 3;
+        e[2 * q] = (int16_t)a[m];
+        o[2 * q] = (int16_t)b[m];
+        e[2 * q + 1] = (int16_t)clampi(up_tap_sum(a[m], a[m + 1], a[m - 1], a[m + 2], a[m - 2], a[m + 3], a[m - 3],
+                                                  a[m + 4]), jb.lo, jb.hi);
+        o[2 * q + 1] = (int16_t)clampi(up_tap_sum(b[m], b[m + 1], b[m - 1], b[m + 2], b[m - 2], b[m + 3], b[m - 3],
+                                                  b[m + 4]), jb.lo, jb.hi);
+    }
+    int16_t* d0 = jb.dst + (size_t)(2 * gy) * jb.dst_stride + 2 * gx0;
+    int16_t* d1 = d0 + jb.dst_stride;
+    const int nq = min(NQ, jb.w - gx0);
+    if (nq == NQ && ((reinterpret_cast<uintptr_t>(d0) | reinterpret_cast<uintptr_t>(d1)) & 15) == 0) {
+        int4 ve, vo;
+        ve.x = (int)(uint16_t)e[0] | ((int)(uint16_t)e[1] << 16);
+        ve.y = (int)(uint16_t)e[2] | ((int)(uint16_t)e[3] << 16);
+        ve.z = (int)(uint16_t)e[4] | ((int)(uint16_t)e[5] << 16);
+        ve.w = (int)(uint16_t)e[6] | ((int)(uint16_t)e[7] << 16);
+        vo.x = (int)(uint16_t)o[0] | ((int)(uint16_t)o[1] << 16);
+        vo.y = (int)(uint16_t)o[2] | ((int)(uint16_t)o[3] << 16);
+        vo.z = (int)(uint16_t)o[4] | ((int)(uint16_t)o[5] << 16);
+        vo.w = (int)(uint16_t)o[6] | ((int)(uint16_t)o[7] << 16);
+        *reinterpret_cast<int4*>(d0) = ve;
+        *reinterpret_cast<int4*>(d1) = vo;
+    } else {
         // 4-byte aligned pair stores (dst_stride and the base are even-aligned)
-        *reinterpret_cast<short2*>(d0) = make_short2(e0, e1);
-        *reinterpret_cast<short2*>(d1) = make_short2(o0, o1);
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            if (q < nq) {
+                *reinterpret_cast<short2*>(d0 + 2 * q) = make_short2(e[2 * q], e[2 * q + 1]);
+                *reinterpret_cast<short2*>(d1 + 2 * q) = make_short2(o[2 * q], o[2 * q + 1]);
+            }
+        }
     }
 }
 

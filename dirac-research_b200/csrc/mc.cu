@@ -16,8 +16,11 @@
 // stores them in ValueType.  Prediction samples come from the upconverted reference with
 // coordinates clamped to [0, 2*size-2] (the reference's BChk(., 2*size-1)).
 //
-// Threads map to 32 x 8 sample tiles of one component; each thread reads the block data
-// of its units (L1-resident) and 1-4 upconverted samples per prediction.
+// Threads map to 32 x 8 sample tiles of one component.  A tile first tabulates, in shared
+// memory, the block rows covering each of its rows (with their vertical weights) and, for each
+// column and each of the three split modes, the units covering it (with their horizontal
+// weights), so that no sample divides; then each thread reads the block data of its units
+// (L1-resident) and 1-4 upconverted samples per prediction, at compile-time precision.
 
 #include "dgpu_internal.cuh"
 
@@ -74,79 +77,188 @@ __device__ __forceinline__ int up_at(const int16_t* up, int stride2, int W2, int
     return up[(size_t)clampi(yy, 0, H2 - 1) * stride2 + clampi(xx, 0, W2 - 1)];
 }
 
-// BlockPixelPred for one sample (mot_comp.cpp:846-1239)
-__device__ __forceinline__ int pixel_pred(int prec, const int16_t* up, int w, int h, int px, int py, int mvx,
-                                          int mvy) {
+// BlockPixelPred for one sample (mot_comp.cpp:846-1239) at compile-time precision PREC.
+template <int PREC>
+__device__ __forceinline__ int pixel_pred(const int16_t* up, int w, int h, int px, int py, int mvx, int mvy) {
     const int W2 = 2 * w - 1, H2 = 2 * h - 1, s2 = 2 * w;
-    switch (prec) {
-        case 0:
-            return up_at(up, s2, W2, H2, 2 * (py + mvy), 2 * (px + mvx));
-        case 1:
-            return up_at(up, s2, W2, H2, 2 * py + mvy, 2 * px + mvx);
-        case 2: {
-            const int rx = mvx & 1, ry = mvy & 1;
-            const int bx = 2 * px + (mvx >> 1), by = 2 * py + (mvy >> 1);
-            return (int16_t)(((2 - rx) * (2 - ry) * up_at(up, s2, W2, H2, by, bx) +
-                              rx * (2 - ry) * up_at(up, s2, W2, H2, by, bx + 1) +
-                              (2 - rx) * ry * up_at(up, s2, W2, H2, by + 1, bx) +
-                              rx * ry * up_at(up, s2, W2, H2, by + 1, bx + 1) + 2) >> 2);
-        }
-        default: {
-            const int rx = mvx & 3, ry = mvy & 3;
-            const int bx = 2 * px + (mvx >> 2), by = 2 * py + (mvy >> 2);
-            return (int16_t)(((4 - rx) * (4 - ry) * up_at(up, s2, W2, H2, by, bx) +
-                              rx * (4 - ry) * up_at(up, s2, W2, H2, by, bx + 1) +
-                              (4 - rx) * ry * up_at(up, s2, W2, H2, by + 1, bx) +
-                              rx * ry * up_at(up, s2, W2, H2, by + 1, bx + 1) + 8) >> 4);
-        }
-    }
+    if (PREC == 0) return up_at(up, s2, W2, H2, 2 * (py + mvy), 2 * (px + mvx));
+    if (PREC == 1) return up_at(up, s2, W2, H2, 2 * py + mvy, 2 * px + mvx);
+    constexpr int M = PREC == 2 ? 1 : 3, SH = PREC == 2 ? 1 : 2, ONE = M + 1, RND = PREC == 2 ? 2 : 8,
+                  OUT = PREC == 2 ? 2 : 4;
+    const int rx = mvx & M, ry = mvy & M;
+    const int bx = 2 * px + (mvx >> SH), by = 2 * py + (mvy >> SH);
+    // clamped rows and columns of the 2 x 2 neighbourhood (BChk)
+    const int x0 = clampi(bx, 0, W2 - 1), x1 = clampi(bx + 1, 0, W2 - 1);
+    const int16_t* r0 = up + (size_t)clampi(by, 0, H2 - 1) * s2;
+    const int16_t* r1 = up + (size_t)clampi(by + 1, 0, H2 - 1) * s2;
+    return (int16_t)(((ONE - rx) * (ONE - ry) * r0[x0] + rx * (ONE - ry) * r0[x1] + (ONE - rx) * ry * r1[x0] +
+                      rx * ry * r1[x1] + RND) >> OUT);
 }
 
+// Per tile row: the (at most two) block rows covering it, with their vertical weights.
+struct McRow {
+    int yb[2];
+    int V[2];  // 0: the block row does not cover this row
+};
+
+// Per tile column and superblock split mode: the (at most two) units covering it.
+struct McCol {
+    int xb[2];   // candidate block column (-1: none); its superblock gives the split mode
+    int xs0[2];  // first block of the unit under this split mode (-1: not used)
+    int H[2];
+};
+
+// Tile-local cache of the block data: for block (yb, xb) of the tile's range, the unit
+// (yb, xs0) covering it under its superblock's split, with that unit's mode, vectors (scaled
+// to the component) and DC.
+constexpr int CBY = 4, CBX = 12;
+struct McUnit {
+    short2 mv1, mv2;
+    int16_t dc;
+    uint8_t mode, sm;
+};
+
+template <int PREC>
 __global__ void __launch_bounds__(MTX* MTY) obmc_kernel(const __grid_constant__ McParams P) {
+    __shared__ McRow rows[MTY];
+    __shared__ McCol cols[3][MTX];
+    __shared__ McUnit cache[CBY][CBX];
     int ci = 0;
     while (ci + 1 < P.ncomp && P.comp[ci + 1].tile_begin <= (int)blockIdx.x) ++ci;
     const McComp& C = P.comp[ci];
     const int t = blockIdx.x - C.tile_begin;
     const int ty = t / C.tiles_x, tx = t - ty * C.tiles_x;
-    const int px = tx * MTX + threadIdx.x % MTX;
-    const int py = ty * MTY + threadIdx.x / MTX;
-    if (px >= C.w || py >= C.h) return;
-
-    int acc = 0;
-    const int yb_hi = (py + C.yoff) / C.ybsep;
-    for (int yb = yb_hi - 1; yb <= yb_hi; ++yb) {
-        if (yb < 0 || yb >= C.y_used) continue;
-        const int pos_y = yb * C.ybsep - C.yoff;
-        if (py < pos_y || py >= pos_y + C.yblen) continue;
-        const int rcls = pos_y < 0 ? 0 : (yb + 1 < C.y_used ? 1 : 2);
-        const int V = obmc_window(C.yblen, C.ybsep, rcls, py - pos_y);
-        const int xb_hi = (px + C.xoff) / C.xbsep;
-        int last_unit = -1;
-        for (int xb = xb_hi - 1; xb <= xb_hi; ++xb) {
-            if (xb < 0 || xb >= P.xnb) continue;
-            if (px < xb * C.xbsep - C.xoff || px >= xb * C.xbsep - C.xoff + C.xblen) continue;
+    const int tid = threadIdx.x;
+    // the tile's block range: cached when it fits (it does for block separations >= 4 / 6)
+    const int yb_lo = (ty * MTY + C.yoff) / C.ybsep - 1, yb_hi = (ty * MTY + MTY - 1 + C.yoff) / C.ybsep;
+    const int xb_lo = (tx * MTX + C.xoff) / C.xbsep - 1, xb_hi = (tx * MTX + MTX - 1 + C.xoff) / C.xbsep;
+    const bool cached = yb_hi - yb_lo < CBY && xb_hi - xb_lo < CBX;
+    // ---- tables of the tile: block rows per row, units per column and split mode ----
+    if (cached && tid >= 128 && tid < 128 + CBY * CBX) {
+        const int i = tid - 128, yr = i / CBX, xr = i - yr * CBX;
+        const int yb = yb_lo + yr, xb = xb_lo + xr;
+        McUnit u{};
+        if (yb >= 0 && yb < P.ynb && xb >= 0 && xb < P.xnb) {
             const int sm = P.split[(size_t)(yb >> 2) * P.xnum_sb + (xb >> 2)];
             const int nb = sm == 0 ? 4 : (sm == 1 ? 2 : 1);
+            const size_t b = (size_t)yb * P.xnb + xb - (xb % nb);
+            u.sm = (uint8_t)sm;
+            u.mode = P.mode[b];
+            const short2 m1 = reinterpret_cast<const short2*>(P.mv1)[b];
+            const short2 m2 = reinterpret_cast<const short2*>(P.mv2)[b];
+            u.mv1 = make_short2((short)(m1.x >> C.xshift), (short)(m1.y >> C.yshift));
+            u.mv2 = make_short2((short)(m2.x >> C.xshift), (short)(m2.y >> C.yshift));
+            u.dc = P.dc[(size_t)C.comp * P.xnb * P.ynb + b];
+        }
+        cache[yr][xr] = u;
+    }
+    if (tid < MTY) {
+        const int py = ty * MTY + tid;
+        const int yb_hi = (py + C.yoff) / C.ybsep;
+        McRow r;
+        for (int k = 0; k < 2; ++k) {
+            const int yb = yb_hi - 1 + k;
+            const int pos_y = yb * C.ybsep - C.yoff;
+            r.yb[k] = yb;
+            r.V[k] = 0;
+            if (yb < 0 || yb >= C.y_used || py < pos_y || py >= pos_y + C.yblen) continue;
+            const int rcls = pos_y < 0 ? 0 : (yb + 1 < C.y_used ? 1 : 2);
+            r.V[k] = obmc_window(C.yblen, C.ybsep, rcls, py - pos_y);
+        }
+        rows[tid] = r;
+    } else if (tid >= 32 && tid < 32 + 3 * MTX) {
+        const int sm = (tid - 32) / MTX, col = (tid - 32) - sm * MTX;
+        const int px = tx * MTX + col;
+        const int nb = sm == 0 ? 4 : (sm == 1 ? 2 : 1);
+        const int xb_hi = (px + C.xoff) / C.xbsep;
+        McCol c;
+        for (int k = 0; k < 2; ++k) {
+            const int xb = xb_hi - 1 + k;
+            c.xb[k] = -1;
+            c.xs0[k] = -1;
+            c.H[k] = 0;
+            if (xb < 0 || xb >= P.xnb) continue;
+            if (px < xb * C.xbsep - C.xoff || px >= xb * C.xbsep - C.xoff + C.xblen) continue;
+            c.xb[k] = xb;
             const int xs0 = xb - (xb % nb);
-            if (xs0 == last_unit || xs0 >= C.x_used) continue;
-            last_unit = xs0;
+            if (xs0 >= C.x_used) continue;
             const int pos_x = xs0 * C.xbsep - C.xoff;
             const int len = nb * C.xbsep + 2 * C.xoff;
             const int ccls = (pos_x >= 0 && xs0 + nb < C.x_used) ? 1 : (pos_x < 0 ? 0 : 2);
-            const int H = obmc_window(len, nb * C.xbsep, ccls, px - pos_x);
-            const int16_t wgt = (int16_t)(V * H);
+            c.xs0[k] = xs0;
+            c.H[k] = obmc_window(len, nb * C.xbsep, ccls, px - pos_x);
+        }
+        cols[sm][col] = c;
+    }
+    __syncthreads();
+    const int col = tid % MTX, row = tid / MTX;
+    const int px = tx * MTX + col;
+    const int py = ty * MTY + row;
+    if (px >= C.w || py >= C.h) return;
+
+    int acc = 0;
+    const McRow& R = rows[row];
+    if (cached) {
+#pragma unroll
+        for (int ky = 0; ky < 2; ++ky) {
+            if (R.V[ky] == 0) continue;
+            const McUnit* crow = cache[R.yb[ky] - yb_lo];
+            int last_unit = -1;
+#pragma unroll
+            for (int kx = 0; kx < 2; ++kx) {
+                const int xb = cols[0][col].xb[kx];
+                if (xb < 0) continue;
+                const McUnit u = crow[xb - xb_lo];
+                const McCol& U = cols[u.sm][col];
+                const int xs0 = U.xs0[kx];
+                if (xs0 < 0 || xs0 == last_unit) continue;
+                last_unit = xs0;
+                const int16_t wgt = (int16_t)(R.V[ky] * U.H[kx]);
+                int pred;
+                if (u.mode == 0) {
+                    pred = u.dc;
+                } else {
+                    const short2 m = u.mode == 2 ? u.mv2 : u.mv1;
+                    pred = pixel_pred<PREC>(u.mode == 2 ? C.up2 : C.up1, C.w, C.h, px, py, m.x, m.y);
+                    if (u.mode == 3) {
+                        const int p2 = pixel_pred<PREC>(C.up2, C.w, C.h, px, py, u.mv2.x, u.mv2.y);
+                        pred = (int16_t)((pred + p2 + 1) >> 1);
+                    }
+                }
+                acc = (int16_t)(acc + (int16_t)(pred * wgt));
+            }
+        }
+    }
+    const short2* mv1 = reinterpret_cast<const short2*>(P.mv1);
+    const short2* mv2 = reinterpret_cast<const short2*>(P.mv2);
+#pragma unroll
+    for (int ky = 0; ky < 2 && !cached; ++ky) {
+        if (R.V[ky] == 0) continue;
+        const int yb = R.yb[ky];
+        const uint8_t* split_row = P.split + (size_t)(yb >> 2) * P.xnum_sb;
+        int last_unit = -1;
+#pragma unroll
+        for (int kx = 0; kx < 2; ++kx) {
+            const int xb = cols[0][col].xb[kx];
+            if (xb < 0) continue;
+            const int sm = split_row[xb >> 2];
+            const McCol& U = cols[sm][col];
+            const int xs0 = U.xs0[kx];
+            if (xs0 < 0 || xs0 == last_unit) continue;
+            last_unit = xs0;
+            const int16_t wgt = (int16_t)(R.V[ky] * U.H[kx]);
             const size_t b = (size_t)yb * P.xnb + xs0;
             const int md = P.mode[b];
             int pred;
             if (md == 0) {
                 pred = P.dc[(size_t)C.comp * P.xnb * P.ynb + b];
             } else {
-                const int16_t* m = (md == 2) ? P.mv2 : P.mv1;
+                const short2 m = (md == 2) ? mv2[b] : mv1[b];
                 const int16_t* u = (md == 2) ? C.up2 : C.up1;
-                pred = pixel_pred(P.precision, u, C.w, C.h, px, py, m[2 * b] >> C.xshift, m[2 * b + 1] >> C.yshift);
+                pred = pixel_pred<PREC>(u, C.w, C.h, px, py, m.x >> C.xshift, m.y >> C.yshift);
                 if (md == 3) {
-                    const int p2 = pixel_pred(P.precision, C.up2, C.w, C.h, px, py, P.mv2[2 * b] >> C.xshift,
-                                              P.mv2[2 * b + 1] >> C.yshift);
+                    const short2 m2 = mv2[b];
+                    const int p2 = pixel_pred<PREC>(C.up2, C.w, C.h, px, py, m2.x >> C.xshift, m2.y >> C.yshift);
                     pred = (int16_t)((pred + p2 + 1) >> 1);
                 }
             }
@@ -228,7 +340,13 @@ extern "C" int dgpu_motion_compensate(int add_or_sub, int cformat, int w, int h,
         C.tile_begin = tiles;
         tiles += C.tiles_x * ((C.h + MTY - 1) / MTY);
     }
-    obmc_kernel<<<tiles, MTX * MTY, 0, as_stream(stream)>>>(P);
+    cudaStream_t st = as_stream(stream);
+    switch (P.precision) {
+        case 0: obmc_kernel<0><<<tiles, MTX * MTY, 0, st>>>(P); break;
+        case 1: obmc_kernel<1><<<tiles, MTX * MTY, 0, st>>>(P); break;
+        case 2: obmc_kernel<2><<<tiles, MTX * MTY, 0, st>>>(P); break;
+        default: obmc_kernel<3><<<tiles, MTX * MTY, 0, st>>>(P); break;
+    }
     DGPU_CHECK_LAUNCH();
     return DGPU_OK;
 }
