@@ -16,7 +16,7 @@
 // stores them in ValueType.  Prediction samples come from the upconverted reference with
 // coordinates clamped to [0, 2*size-2] (the reference's BChk(., 2*size-1)).
 //
-// Threads map to 32 x 8 sample tiles of one component.  A tile first tabulates, in shared
+// CTAs of 256 threads map to 32 x 32 sample tiles of one component (four rows per thread).  A tile first tabulates, in shared
 // memory, the block rows covering each of its rows (with their vertical weights) and, for each
 // column and each of the three split modes, the units covering it (with their horizontal
 // weights), so that no sample divides; then each thread reads the block data of its units
@@ -27,7 +27,8 @@
 namespace dgpu {
 namespace {
 
-constexpr int MTX = 32, MTY = 8;
+constexpr int MTX = 32, MTY = 32;  // tile (columns x rows)
+constexpr int MT_THREADS = 256;     // eight rows at a time: four samples per thread
 
 struct McComp {
     int16_t* pic;
@@ -111,15 +112,54 @@ struct McCol {
 // Tile-local cache of the block data: for block (yb, xb) of the tile's range, the unit
 // (yb, xs0) covering it under its superblock's split, with that unit's mode, vectors (scaled
 // to the component) and DC.
-constexpr int CBY = 4, CBX = 12;
+// Each reference's prediction is also precomputed as an offset into the upconverted plane
+// and four bilinear weights; `inside` says that every prediction of the unit reads within the
+// plane, so that its samples need no clamping.
+constexpr int CBY = 10, CBX = 12;  // CBY * CBX <= 128 threads fill it
 struct McUnit {
     short2 mv1, mv2;
+    int delta[2];      // (2 py + oy) * 2w + 2 px + ox - (2 py * 2w + 2 px) per reference
+    uint32_t wts[2];   // bilinear weights w00 | w01 << 8 | w10 << 16 | w11 << 24 per reference
     int16_t dc;
-    uint8_t mode, sm;
+    uint8_t mode, sm, inside;
 };
 
+// Offset and weights of one reference's prediction (pixel_pred's arithmetic, split so that
+// only the sample position remains per sample); returns whether the unit's sample rectangle
+// [x0, x1] x [y0, y1] reads inside the (2w - 1) x (2h - 1) upconverted plane.
 template <int PREC>
-__global__ void __launch_bounds__(MTX* MTY) obmc_kernel(const __grid_constant__ McParams P) {
+__device__ __forceinline__ bool pred_params(int mvx, int mvy, int s2, int W2, int H2, int x0, int x1, int y0, int y1,
+                                            int& delta, uint32_t& wts) {
+    int ox, oy, span;
+    if (PREC <= 1) {
+        ox = PREC == 0 ? 2 * mvx : mvx;
+        oy = PREC == 0 ? 2 * mvy : mvy;
+        wts = 1u;
+        span = 0;
+    } else {
+        constexpr int M = PREC == 2 ? 1 : 3, SH = PREC == 2 ? 1 : 2, ONE = M + 1;
+        const int rx = mvx & M, ry = mvy & M;
+        ox = mvx >> SH;
+        oy = mvy >> SH;
+        wts = (uint32_t)((ONE - rx) * (ONE - ry)) | ((uint32_t)(rx * (ONE - ry)) << 8) |
+              ((uint32_t)((ONE - rx) * ry) << 16) | ((uint32_t)(rx * ry) << 24);
+        span = 1;
+    }
+    delta = oy * s2 + ox;
+    return 2 * x0 + ox >= 0 && 2 * x1 + ox + span <= W2 - 1 && 2 * y0 + oy >= 0 && 2 * y1 + oy + span <= H2 - 1;
+}
+
+// The prediction at q (the unit's base sample for this position) from the packed weights.
+template <int PREC>
+__device__ __forceinline__ int pred_fast(const int16_t* q, int s2, uint32_t wts) {
+    if (PREC <= 1) return q[0];
+    constexpr int RND = PREC == 2 ? 2 : 8, OUT = PREC == 2 ? 2 : 4;
+    return (int16_t)(((int)(wts & 0xff) * q[0] + (int)((wts >> 8) & 0xff) * q[1] +
+                      (int)((wts >> 16) & 0xff) * q[s2] + (int)(wts >> 24) * q[s2 + 1] + RND) >> OUT);
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(MT_THREADS) obmc_kernel(const __grid_constant__ McParams P) {
     __shared__ McRow rows[MTY];
     __shared__ McCol cols[3][MTX];
     __shared__ McUnit cache[CBY][CBX];
@@ -141,7 +181,8 @@ __global__ void __launch_bounds__(MTX* MTY) obmc_kernel(const __grid_constant__ 
         if (yb >= 0 && yb < P.ynb && xb >= 0 && xb < P.xnb) {
             const int sm = P.split[(size_t)(yb >> 2) * P.xnum_sb + (xb >> 2)];
             const int nb = sm == 0 ? 4 : (sm == 1 ? 2 : 1);
-            const size_t b = (size_t)yb * P.xnb + xb - (xb % nb);
+            const int xs0 = xb - (xb % nb);
+            const size_t b = (size_t)yb * P.xnb + xs0;
             u.sm = (uint8_t)sm;
             u.mode = P.mode[b];
             const short2 m1 = reinterpret_cast<const short2*>(P.mv1)[b];
@@ -149,6 +190,15 @@ __global__ void __launch_bounds__(MTX* MTY) obmc_kernel(const __grid_constant__ 
             u.mv1 = make_short2((short)(m1.x >> C.xshift), (short)(m1.y >> C.yshift));
             u.mv2 = make_short2((short)(m2.x >> C.xshift), (short)(m2.y >> C.yshift));
             u.dc = P.dc[(size_t)C.comp * P.xnb * P.ynb + b];
+            // the unit's samples: columns pos_x .. pos_x + len - 1, rows pos_y .. + yblen - 1
+            const int pos_x = xs0 * C.xbsep - C.xoff, len = nb * C.xbsep + 2 * C.xoff;
+            const int pos_y = yb * C.ybsep - C.yoff;
+            const int x0 = max(pos_x, 0), x1 = min(pos_x + len, C.w) - 1;
+            const int y0 = max(pos_y, 0), y1 = min(pos_y + C.yblen, C.h) - 1;
+            const int s2 = 2 * C.w, W2 = 2 * C.w - 1, H2 = 2 * C.h - 1;
+            const bool in1 = pred_params<PREC>(u.mv1.x, u.mv1.y, s2, W2, H2, x0, x1, y0, y1, u.delta[0], u.wts[0]);
+            const bool in2 = pred_params<PREC>(u.mv2.x, u.mv2.y, s2, W2, H2, x0, x1, y0, y1, u.delta[1], u.wts[1]);
+            u.inside = (uint8_t)(u.mode == 0 || (u.mode == 1 && in1) || (u.mode == 2 && in2) || (in1 && in2));
         }
         cache[yr][xr] = u;
     }
@@ -191,8 +241,9 @@ __global__ void __launch_bounds__(MTX* MTY) obmc_kernel(const __grid_constant__ 
         cols[sm][col] = c;
     }
     __syncthreads();
-    const int col = tid % MTX, row = tid / MTX;
+    const int col = tid % MTX;
     const int px = tx * MTX + col;
+    for (int row = tid / MTX; row < MTY; row += MT_THREADS / MTX) {
     const int py = ty * MTY + row;
     if (px >= C.w || py >= C.h) return;
 
@@ -208,7 +259,7 @@ __global__ void __launch_bounds__(MTX* MTY) obmc_kernel(const __grid_constant__ 
             for (int kx = 0; kx < 2; ++kx) {
                 const int xb = cols[0][col].xb[kx];
                 if (xb < 0) continue;
-                const McUnit u = crow[xb - xb_lo];
+                const McUnit& u = crow[xb - xb_lo];
                 const McCol& U = cols[u.sm][col];
                 const int xs0 = U.xs0[kx];
                 if (xs0 < 0 || xs0 == last_unit) continue;
@@ -217,6 +268,14 @@ __global__ void __launch_bounds__(MTX* MTY) obmc_kernel(const __grid_constant__ 
                 int pred;
                 if (u.mode == 0) {
                     pred = u.dc;
+                } else if (u.inside) {
+                    const int base = 2 * py * (2 * C.w) + 2 * px;
+                    const int r = u.mode == 2 ? 1 : 0;
+                    pred = pred_fast<PREC>((r ? C.up2 : C.up1) + base + u.delta[r], 2 * C.w, u.wts[r]);
+                    if (u.mode == 3) {
+                        const int p2 = pred_fast<PREC>(C.up2 + base + u.delta[1], 2 * C.w, u.wts[1]);
+                        pred = (int16_t)((pred + p2 + 1) >> 1);
+                    }
                 } else {
                     const short2 m = u.mode == 2 ? u.mv2 : u.mv1;
                     pred = pixel_pred<PREC>(u.mode == 2 ? C.up2 : C.up1, C.w, C.h, px, py, m.x, m.y);
@@ -271,6 +330,7 @@ __global__ void __launch_bounds__(MTX* MTY) obmc_kernel(const __grid_constant__ 
     r = (int16_t)r;
     if (C.clip_lo <= C.clip_hi) r = clampi(r, C.clip_lo, C.clip_hi);
     *o = (int16_t)r;
+    }
 }
 
 }  // namespace
@@ -342,10 +402,10 @@ extern "C" int dgpu_motion_compensate(int add_or_sub, int cformat, int w, int h,
     }
     cudaStream_t st = as_stream(stream);
     switch (P.precision) {
-        case 0: obmc_kernel<0><<<tiles, MTX * MTY, 0, st>>>(P); break;
-        case 1: obmc_kernel<1><<<tiles, MTX * MTY, 0, st>>>(P); break;
-        case 2: obmc_kernel<2><<<tiles, MTX * MTY, 0, st>>>(P); break;
-        default: obmc_kernel<3><<<tiles, MTX * MTY, 0, st>>>(P); break;
+        case 0: obmc_kernel<0><<<tiles, MT_THREADS, 0, st>>>(P); break;
+        case 1: obmc_kernel<1><<<tiles, MT_THREADS, 0, st>>>(P); break;
+        case 2: obmc_kernel<2><<<tiles, MT_THREADS, 0, st>>>(P); break;
+        default: obmc_kernel<3><<<tiles, MT_THREADS, 0, st>>>(P); break;
     }
     DGPU_CHECK_LAUNCH();
     return DGPU_OK;
