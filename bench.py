@@ -56,6 +56,9 @@ def parse_args():
                     help="encoder groups the batched form's sequences are split into (run concurrently)")
     ap.add_argument("--serving-seconds", type=float, default=6.0,
                     help="length of the serving-loop run reported under 'serving' (0: skip)")
+    ap.add_argument("--hetero-steps", type=int, default=5,
+                    help="timed runs of the heterogeneous 64-picture batch reported under 'heterogeneous_batch' "
+                         "(0: skip)")
     ap.add_argument("--impl", choices=["gpu", "reference"], default="gpu")
     return ap.parse_args()
 
@@ -224,6 +227,88 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------------------
+# heterogeneous picture batch (the batched launch of 64 mixed pictures)
+# ---------------------------------------------------------------------------------------------
+
+def run_hetero(args, peak, peaks):
+    """64 pictures (16 each of CIF 8-bit, 576p 8-bit, 720p 10-bit 4:2:0, 1080p 10-bit 4:2:2) with
+    random filters and depths: motion compensation SUBTRACT, forward transform, quantisation,
+    inverse transform, motion compensation ADD per picture, in one batch (CUDA graphs around
+    the host quantiser choice).  Device-resident inputs for `value`; `e2e` loads every picture
+    from pinned host memory and reads its quantised indices back each step."""
+    import torch
+
+    from dirac_b200 import hetero as H
+    from dirac_b200.batch import QINDEX, PictureBatch
+
+    pictures, motion, planes, keep = H.make_inputs()
+    n = len(pictures)
+    batch = PictureBatch(pictures, motion)
+    st = torch.cuda.current_stream()
+
+    def step(src, reads=None):
+        for k in range(n):
+            batch.load(k, src[k])
+        batch.run()
+        if reads is not None:
+            for k in range(n):
+                for c in range(3):
+                    buf = reads[k][c]
+                    batch.lib.dgpu_batch_read(batch.handle, k, QINDEX, c, buf.data_ptr(), buf.numel() * 4, 1)
+
+    def timed(src, steps, reads=None):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            step(src, reads)
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    for _ in range(max(3, args.warmup)):
+        step(planes)
+    launches0 = batch.lib.dgpu_launch_count()
+    ms = timed(planes, args.hetero_steps)
+    launches = (batch.lib.dgpu_launch_count() - launches0) // args.hetero_steps
+    host = [[t.cpu().pin_memory() for t in pl] for pl in planes]
+    host_np = [[t.numpy() for t in pl] for pl in host]
+    reads = []
+    for k in range(n):
+        reads.append([torch.empty(batch.lib.dgpu_batch_item_bytes(batch.handle, k, QINDEX, c) // 4,
+                                  dtype=torch.int32, pin_memory=True) for c in range(3)])
+    step(host_np, reads)
+    ems = timed(host_np, args.hetero_steps, reads)
+    stage_ms = [0.0, 0.0, 0.0]
+    reps = 3
+    for _ in range(reps):
+        t = batch.stage_times()
+        stage_ms = [a + b / reps for a, b in zip(stage_ms, t)]
+    alg = H.stage_bytes(pictures)
+    alg["pre"] += H.upconvert_bytes(motion)
+    stages = {}
+    for name, t in zip(("pre", "quant", "post"), stage_ms):
+        gbs = alg[name] / (t / 1000.0) / 1e9
+        stages[name] = {"ms": round(t, 3), "algorithmic_bytes": alg[name], "gbs": round(gbs, 1),
+                        "frac": round(gbs / peak, 4)}
+    h2d = sum(a.nbytes for pl in host_np for a in pl)
+    d2h = sum(b.numel() * 4 for r in reads for b in r)
+    out = {"value": n * args.hetero_steps / (ms / 1000.0), "unit": "pictures/s", "pictures_per_step": n,
+           "ms_per_step": ms / args.hetero_steps, "steps": args.hetero_steps,
+           "e2e": {"value": n * args.hetero_steps / (ems / 1000.0), "unit": "pictures/s",
+                   "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+           "stages": stages, "gpu_launches_per_step": launches,
+           "workload": "16x 352x288 4:2:0 8-bit, 16x 720x576 4:2:0 8-bit, 16x 1280x720 4:2:0 10-bit, "
+                       "16x 1920x1080 4:2:2 10-bit; random filter (Haar, LeGall, DD13_7, Fidelity, DAUB9_7) "
+                       "and depth 3-5; P and B pictures with motion from the library's estimation; QF 7",
+           "note": "stages timed in a separate pass with CUDA events on the batch stream; 'pre' = reference "
+                   "upconversions + motion compensation SUBTRACT + forward transforms (one CUDA graph), "
+                   "'quant' = quantiser choice (host Lagrangian) + quantisation, 'post' = inverse transforms + "
+                   "motion compensation ADD with the clip (one CUDA graph)"}
+    batch.close()
+    del keep
+    return out
+
 
 def main():
     args = parse_args()
@@ -472,6 +557,11 @@ def main():
     for ex in pools.values():
         ex.shutdown()
 
+    # ---- heterogeneous picture batch: 64 mixed pictures coded together (one GPU) ----------------
+    hetero = None
+    if args.hetero_steps > 0:
+        hetero = run_hetero(args, peak, peaks)
+
     # ---- serving loop: Poisson arrivals of live streams of mixed sizes (one GPU) ----------------
     serving = None
     if args.serving_seconds > 0 and world == 1:
@@ -494,7 +584,8 @@ def main():
                                    "each sequence's coding on its own stream and host thread",
                            "l2": "inputs and working set larger than L2 (no flush needed)"},
                 "plain": plain_line, "batched_one_group": one_group, "batched_streams_only": streams_only, "roofline": roofline, "cpu_baseline": cpu_baseline, "e2e": e2e,
-                "latency_ms": latency, "serving": serving, "gpu_launches": launches, "clocks": clk}
+                "latency_ms": latency, "heterogeneous_batch": hetero, "serving": serving,
+                "gpu_launches": launches, "clocks": clk}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <functional>
 #include <stddef.h>
 #include <stdint.h>
 
@@ -27,6 +28,8 @@ namespace dgpu {
     } while (0)
 
 void count_launch();
+// Adds n launches to the running total (kernels replayed from a captured CUDA graph).
+void count_launches(unsigned long long n);
 
 void set_last_cuda_error(cudaError_t e, const char* what, const char* file, int line);
 
@@ -38,6 +41,11 @@ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // Grown with cudaMalloc on demand (synchronising the device first so that no kernel still
 // in flight uses the old buffer), kept until process exit.
 int library_scratch(size_t bytes, void** out);
+
+// Runs body(begin, end) over [0, n) split into chunks of at least `grain` items on the
+// library's host worker threads (a process-wide pool) and the calling thread; returns when
+// every chunk is done.  Small ranges run inline.
+void parallel_for(int n, int grain, const std::function<void(int, int)>& body);
 
 __host__ __device__ inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 

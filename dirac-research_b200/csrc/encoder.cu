@@ -29,6 +29,7 @@
 #include <new>
 #include <vector>
 
+#include "coding_params.h"
 #include "dgpu_internal.cuh"
 
 namespace dgpu {
@@ -36,20 +37,6 @@ namespace {
 
 constexpr int kIntraMode = 0;  // PredMode INTRA (libdirac_common/common.h:84)
 constexpr int kMaxCountTasks = 64;
-
-struct Lambdas {
-    float i, l1, l2, me;
-};
-
-// EncoderParams::CalcLambdas: float members, std::sqrt of a float member.
-Lambdas calc_lambdas(float qf) {
-    Lambdas L;
-    L.i = (float)(std::pow(10.0, (12.0 - (double)qf) / 2.5) / 16.0);
-    L.l1 = (float)((double)L.i * 4.0);
-    L.l2 = (float)((double)L.i * 32.0);
-    L.me = (float)((double)std::sqrt(L.l1) * 2.0);
-    return L;
-}
 
 // ---------------------------------------------------------------------------------------
 // small kernels: input conversion, output conversion, intra-block counts
@@ -457,42 +444,15 @@ int transform(Encoder& E, Pic& p, int dir, int filter) {
                                         E.dwt_ws_bytes, E.st);
 }
 
-// PictureCompressor::GetCompLambda (picture_compress.cpp:532-580): std::log10 of the float
-// lambdas is the single-precision overload; the blend is double; U and V factors 1.5 / 0.75
-// (dirac_encoder.cpp:552-553) multiply in float.
 float comp_lambda(const Encoder& E, const Pic& p, int comp) {
-    float lambda;
-    if (p.intra) {
-        lambda = E.L.i;
-    } else {
-        const double log_intra = std::log10(E.L.i);
-        const double log_pic = p.is_b() ? std::log10(E.L.l2) : std::log10(E.L.l1);
-        const float ir = (float)p.ratio;
-        lambda = (float)std::pow(10.0, 3.0 * ir * log_intra + (1.0 - 3.0 * ir) * log_pic);
-    }
-    if (comp == 1) lambda *= 1.5f;
-    if (comp == 2) lambda *= 0.75f;
-    return lambda;
-}
-
-// EntropyCorrector::Init (common.cpp:79-131): the same initial factors for all components.
-void initial_ecf(int depth, bool intra, float* out) {
-    const int nb = 3 * depth + 1;
-    for (int b = 0; b < nb; ++b) out[b] = 0.75f;
-    for (int b = nb - 4; b < nb - 1; ++b) out[b] = intra ? 0.85f : 0.75f;
-    out[nb - 1] = intra ? 1.0f : 0.85f;
+    return component_lambda(E.L, p.intra, p.is_b(), p.ratio, comp);
 }
 
 int code_residue(Encoder& E, Pic& p, const float* ecf_in) {
     Slot& s = slot_of(E, p);
     const int depth = E.P.wlt_depth;
     const int filter = p.intra ? E.P.intra_filter : E.P.inter_filter;
-    double cpd_scale = 1.0;
-    if (!p.intra) {
-        const float ir = (float)p.ratio;
-        cpd_scale = 5.0 * ir * 1.0 + (1.0 - 5.0 * ir) * 0.125;
-        cpd_scale = std::max(0.125, std::min(1.2, cpd_scale));
-    }
+    const double cpd_scale = perceptual_scale(p.intra, p.ratio);
     const int nb = E.nb;
     std::vector<float> wt(3 * nb), ecf(3 * nb);
     std::vector<int> ncb(6 * nb);

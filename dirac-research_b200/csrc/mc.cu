@@ -27,8 +27,9 @@
 namespace dgpu {
 namespace {
 
-constexpr int MTX = 32, MTY = 32;  // tile (columns x rows)
-constexpr int MT_THREADS = 256;     // eight rows at a time: four samples per thread
+constexpr int MTX = 32;             // tile columns; tile rows (8, 16 or 32) are a template parameter
+constexpr int MT_THREADS = 256;     // eight rows at a time
+constexpr int MC_ROWS[3] = {32, 16, 8};  // tile-height variants (index 0 is the default)
 
 struct McComp {
     int16_t* pic;
@@ -158,7 +159,7 @@ __device__ __forceinline__ int pred_fast(const int16_t* q, int s2, uint32_t wts)
                       (int)((wts >> 16) & 0xff) * q[s2] + (int)(wts >> 24) * q[s2 + 1] + RND) >> OUT);
 }
 
-template <int PREC>
+template <int PREC, int MTY>
 __global__ void __launch_bounds__(MT_THREADS) obmc_kernel(const __grid_constant__ McParams P) {
     __shared__ McRow rows[MTY];
     __shared__ McCol cols[3][MTX];
@@ -338,12 +339,28 @@ __global__ void __launch_bounds__(MT_THREADS) obmc_kernel(const __grid_constant_
 
 using namespace dgpu;
 
-extern "C" int dgpu_motion_compensate(int add_or_sub, int cformat, int w, int h, const dgpu_block_params* bp,
-                                      const int16_t* mv1, const int16_t* mv2, const uint8_t* mode,
-                                      const int16_t* dc, const uint8_t* split, int16_t* const* pic,
-                                      const int* pic_stride, const int16_t* const* ref1up,
-                                      const int16_t* const* ref2up, int clip_luma_depth, int clip_chroma_depth,
-                                      void* stream) {
+namespace dgpu {
+
+template <int MTY>
+void launch_obmc(int tiles, const McParams& P, cudaStream_t st) {
+    switch (P.precision) {
+        case 0: obmc_kernel<0, MTY><<<tiles, MT_THREADS, 0, st>>>(P); break;
+        case 1: obmc_kernel<1, MTY><<<tiles, MT_THREADS, 0, st>>>(P); break;
+        case 2: obmc_kernel<2, MTY><<<tiles, MT_THREADS, 0, st>>>(P); break;
+        default: obmc_kernel<3, MTY><<<tiles, MT_THREADS, 0, st>>>(P); break;
+    }
+}
+
+int mc_tile_variants() { return 3; }
+
+// dgpu_motion_compensate with a chosen tile height (variant indexes MC_ROWS).
+int motion_compensate_tiled(int variant, int add_or_sub, int cformat, int w, int h, const dgpu_block_params* bp,
+                            const int16_t* mv1, const int16_t* mv2, const uint8_t* mode, const int16_t* dc,
+                            const uint8_t* split, int16_t* const* pic, const int* pic_stride,
+                            const int16_t* const* ref1up, const int16_t* const* ref2up, int clip_luma_depth,
+                            int clip_chroma_depth, cudaStream_t st) {
+    if (variant < 0 || variant >= 3) return DGPU_ERR_ARG;
+    const int MTY = MC_ROWS[variant];
     if (!bp || !mv1 || !mode || !dc || !split || !pic || !pic_stride || !ref1up) return DGPU_ERR_ARG;
     if (add_or_sub != 0 && add_or_sub != 1) return DGPU_ERR_ARG;
     if (cformat < 0 || cformat > 2) return DGPU_ERR_ARG;
@@ -400,13 +417,21 @@ extern "C" int dgpu_motion_compensate(int add_or_sub, int cformat, int w, int h,
         C.tile_begin = tiles;
         tiles += C.tiles_x * ((C.h + MTY - 1) / MTY);
     }
-    cudaStream_t st = as_stream(stream);
-    switch (P.precision) {
-        case 0: obmc_kernel<0><<<tiles, MT_THREADS, 0, st>>>(P); break;
-        case 1: obmc_kernel<1><<<tiles, MT_THREADS, 0, st>>>(P); break;
-        case 2: obmc_kernel<2><<<tiles, MT_THREADS, 0, st>>>(P); break;
-        default: obmc_kernel<3><<<tiles, MT_THREADS, 0, st>>>(P); break;
-    }
+    if (MTY == 32) launch_obmc<32>(tiles, P, st);
+    else if (MTY == 16) launch_obmc<16>(tiles, P, st);
+    else launch_obmc<8>(tiles, P, st);
     DGPU_CHECK_LAUNCH();
     return DGPU_OK;
+}
+
+}  // namespace dgpu
+
+extern "C" int dgpu_motion_compensate(int add_or_sub, int cformat, int w, int h, const dgpu_block_params* bp,
+                                      const int16_t* mv1, const int16_t* mv2, const uint8_t* mode,
+                                      const int16_t* dc, const uint8_t* split, int16_t* const* pic,
+                                      const int* pic_stride, const int16_t* const* ref1up,
+                                      const int16_t* const* ref2up, int clip_luma_depth, int clip_chroma_depth,
+                                      void* stream) {
+    return motion_compensate_tiled(0, add_or_sub, cformat, w, h, bp, mv1, mv2, mode, dc, split, pic, pic_stride,
+                                   ref1up, ref2up, clip_luma_depth, clip_chroma_depth, as_stream(stream));
 }

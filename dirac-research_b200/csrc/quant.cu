@@ -25,6 +25,8 @@
 #include <cstring>
 #include <vector>
 
+#include <atomic>
+
 #include "dgpu_internal.cuh"
 
 namespace dgpu {
@@ -90,15 +92,12 @@ struct BandTask {  // one band: where its data lives and where its statistics go
     int comp;
     int band;                 // global band index
     int cb_first, xn, yn;     // code blocks of the band
+    int chunk_first[2];       // first CTA of the band in each sampling pattern's flattened grid
 };
 
-constexpr int MAX_COMPS = 48;
+constexpr int MAX_COMPS = 256;
 constexpr int MAX_TASKS = MAX_COMPS * MAX_BANDS;
 
-struct BandTable {
-    int ntasks;
-    BandTask task[MAX_TASKS];
-};
 
 // ---- 1. DC DPCM and maxima ----------------------------------------------------------------
 
@@ -150,7 +149,8 @@ __device__ __forceinline__ int stat_range(int maxv) {
     return min(4 * bitlen + 5, QMAX);
 }
 
-// grid: x = chunks of the band's sampled coefficients, y = task, z = pattern (0: 2x2, 1: 1x2).
+// grid: one CTA per chunk of STAT_THREADS * 8 sampled coefficients, the bands' chunks laid end
+// to end (BandTask::chunk_first of the pattern; 0: 2x2, 1: 1x2).
 // n / d: for n < 2^24 (every magnitude times 4 of 8- to 14-bit video) the float estimate
 // n * RN(1/d) is within one of the quotient (relative error below 2^-23, quotient below
 // 2^22), and one integer correction makes it exact.
@@ -168,13 +168,20 @@ __device__ __forceinline__ unsigned udiv_recip(unsigned n, unsigned d, float inv
 __global__ void __launch_bounds__(STAT_THREADS) stats_kernel(const BandTask* tasks, const int* band_max,
                                                              Stat* stats, int pattern, int nbands,
                                                              const int2* qrange) {
-    const BandTask T = tasks[blockIdx.y];
+    // the band whose chunks hold this CTA: the last with chunk_first <= blockIdx.x
+    int lo_b = 0, hi_b = nbands - 1;
+    while (lo_b < hi_b) {
+        const int mid = (lo_b + hi_b + 1) >> 1;
+        if (tasks[mid].chunk_first[pattern] <= (int)blockIdx.x) lo_b = mid;
+        else hi_b = mid - 1;
+    }
+    const BandTask T = tasks[lo_b];
     const int xr = pattern ? 1 : 2;
     const int nq = stat_range(band_max[T.band]);
     const int sx = (T.xl + xr - 1) / xr, sy = (T.yl + 1) / 2;
     const int nsamp = sx * sy;
     const int per_cta = STAT_THREADS * 8;
-    const int base = blockIdx.x * per_cta;
+    const int base = ((int)blockIdx.x - T.chunk_first[pattern]) * per_cta;
     if (base >= nsamp || nq == 0) return;
     __shared__ unsigned long long s_c0[QMAX], s_pn[QMAX], s_lo[QMAX], s_hi[QMAX];
     __shared__ unsigned int s_inx[QMAX];
@@ -266,27 +273,49 @@ struct SeqCase {
     int task, pattern, q;
 };
 
+// One warp per case: the lanes compute the terms of 32 consecutive samples (raster order) and
+// lane 0 adds them one by one in that order, so the loads and the arithmetic run in parallel
+// and only the additions stay sequential.
 __global__ void seq_error_kernel(const BandTask* tasks, const SeqCase* cases, int ncases, double* out) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
     if (k >= ncases) return;
     const SeqCase C = cases[k];
     const BandTask T = tasks[C.task];
     const int xr = C.pattern ? 1 : 2;
+    const int sx = (T.xl + xr - 1) / xr, sy = (T.yl + 1) / 2;
+    const int n = sx * sy;
     const int qf = qf4(C.q), off = inter_off4(C.q);
     double s = 0.0;
-    for (int j = 0; j < T.yl; j += 2)
-        for (int i = 0; i < T.xl; i += xr) {
-            const int a = abs(T.data[(size_t)j * T.stride + i]);
+    for (int k0 = 0; k0 < n; k0 += 32) {
+        double term = 0.0;
+        const int i = k0 + lane;
+        if (i < n) {
+            const int sj = i / sx, si = i - sj * sx;
+            const int a = abs(T.data[(size_t)(2 * sj) * T.stride + xr * si]);
             const int qv = (a << 2) / qf;
-            double e;
-            if (!qv) {
-                e = (double)a;
-            } else {
-                e = (double)(a - ((qv * qf + off + 2) >> 2));
-            }
-            s = __dadd_rn(s, __dmul_rn(__dmul_rn(__dmul_rn(e, e), e), e));
+            const double e = !qv ? (double)a : (double)(a - ((qv * qf + off + 2) >> 2));
+            term = __dmul_rn(__dmul_rn(__dmul_rn(e, e), e), e);
         }
-    out[k] = s;
+        const int m = min(32, n - k0);
+        for (int l = 0; l < m; ++l) {
+            const double t = __shfl_sync(0xffffffffu, term, l);
+            s = __dadd_rn(s, t);
+        }
+    }
+    if (lane == 0) out[k] = s;
+}
+
+// Gathers the third pass's statistics, the three quantisers qrange[band] of each band, into
+// a compact [band][3] array for the host.
+__global__ void gather_stats_kernel(const Stat* stats, const int2* qrange, int nbands, Stat* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3 * nbands) return;
+    const int t = i / 3, j = i - 3 * t;
+    const int2 r = qrange[t];
+    Stat v{};
+    if (r.x + j <= r.y) v = stats[(size_t)t * QMAX + r.x + j];
+    out[i] = v;
 }
 
 // ---- 4. quantise and reconstruct ------------------------------------------------------------
@@ -462,7 +491,8 @@ static size_t residue_ws_need(int nb_total, int ncb_total, size_t dcwork_elems) 
            align_up(sizeof(int2) * nb_total, 256) +
            align_up(sizeof(int) * ncb_total, 256) + align_up(sizeof(Stat) * nb_total * 2 * QMAX, 256) +
            align_up(sizeof(int32_t) * dcwork_elems, 256) + align_up(ncb_total, 256) +
-           align_up((sizeof(SeqCase) + sizeof(double)) * nb_total * 2 * QMAX, 256) + 256;
+           align_up((sizeof(SeqCase) + sizeof(double)) * nb_total * 2 * QMAX, 256) +
+           align_up(sizeof(Stat) * nb_total * 3, 256) + 256;
 }
 
 extern "C" size_t dgpu_code_residue_workspace_bytes(int n, const int* intra, const int* depth, const int* cw,
@@ -534,8 +564,10 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     uint8_t* d_cbskip = reinterpret_cast<uint8_t*>(take(ncb_total));
     SeqCase* d_cases = reinterpret_cast<SeqCase*>(take(sizeof(SeqCase) * nb_total * 2 * QMAX));
     double* d_seq = reinterpret_cast<double*>(take(sizeof(double) * nb_total * 2 * QMAX));
+    Stat* d_stats3 = reinterpret_cast<Stat*>(take(sizeof(Stat) * nb_total * 3));
 
     size_t dcoff = 0;
+    int chunks[2] = {0, 0};
     for (int c = 0; c < n; ++c) {
         Comp& C = comps[c];
         if (C.intra) {
@@ -556,6 +588,12 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
             T.cb_first = band_cb_first[T.band];
             T.xn = band_ncb[2 * T.band];
             T.yn = band_ncb[2 * T.band + 1];
+            for (int pat = 0; pat < 2; ++pat) {
+                const int xr = pat ? 1 : 2;
+                const long long ns = (long long)((xl + xr - 1) / xr) * ((yl + 1) / 2);
+                T.chunk_first[pat] = chunks[pat];
+                chunks[pat] += (int)((ns + STAT_THREADS * 8 - 1) / (STAT_THREADS * 8));
+            }
             tasks.push_back(T);
         }
     }
@@ -580,45 +618,53 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     // Passes 1 and 2 use the 2 x 2 pattern over every even quantiser; pass 3 needs the 1 x 2
     // pattern at three quantisers only, known once pass 2 is decided: its statistics are
     // gathered in a second, much smaller launch.
-    int maxs = 0;
-    for (const BandTask& T : tasks) maxs = std::max(maxs, T.xl * ((T.yl + 1) / 2));
-    const dim3 sgrid((maxs + STAT_THREADS * 8 - 1) / (STAT_THREADS * 8), nb_total, 1);
-    stats_kernel<<<sgrid, STAT_THREADS, 0, st>>>(d_tasks, d_band_max, d_stats, 0, nb_total, nullptr);
+    stats_kernel<<<chunks[0], STAT_THREADS, 0, st>>>(d_tasks, d_band_max, d_stats, 0, nb_total, nullptr);
     DGPU_CHECK_LAUNCH();
     // statistics and maxima come back through page-locked memory (one buffer per host thread)
     const size_t n_pat = (size_t)nb_total * QMAX;
     char* pin = nullptr;
     {
-        const int rc = pinned_scratch(sizeof(Stat) * 2 * n_pat + sizeof(int) * (nb_total + ncb_total) +
-                                          sizeof(int2) * nb_total + 256, &pin);
+        const int rc = pinned_scratch(sizeof(Stat) * (n_pat + 3 * (size_t)nb_total) +
+                                          sizeof(int) * (nb_total + ncb_total) + sizeof(int2) * nb_total + 256, &pin);
         if (rc) return rc;
     }
     Stat* hs = reinterpret_cast<Stat*>(pin);
-    int* hmax = reinterpret_cast<int*>(pin + sizeof(Stat) * 2 * n_pat);
+    Stat* hs3 = hs + n_pat;  // third pass: [band][3], the quantisers qrange[band]
+    int* hmax = reinterpret_cast<int*>(pin + sizeof(Stat) * (n_pat + 3 * (size_t)nb_total));
     int* hcb = hmax + nb_total;
     int2* hrange = reinterpret_cast<int2*>(align_up(reinterpret_cast<size_t>(hcb + ncb_total), 16));
     DGPU_CHECK_CUDA(cudaMemcpyAsync(hs, d_stats, sizeof(Stat) * n_pat, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaMemcpyAsync(hmax, d_band_max, sizeof(int) * nb_total, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaMemcpyAsync(hcb, d_cb_max, sizeof(int) * ncb_total, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
-    // sums the exact path could not represent: the sequential double kernel for those cases
-    std::vector<int> case_of(2 * n_pat, -1);
+    // sums the exact path could not represent: the sequential double kernel for those cases.
+    // Statistics of (band t, pattern, q): pattern 0 at hs[t * QMAX + q]; pattern 1 (only the
+    // three quantisers of the band's range) at hs3[t * 3 + q - lo].
+    std::vector<int2> hrange_v(nb_total, make_int2(0, -1));
+    auto stat_at = [&](int t, int pat, int q) -> const Stat& {
+        return pat == 0 ? hs[(size_t)t * QMAX + q] : hs3[(size_t)t * 3 + (q - hrange_v[t].x)];
+    };
+    auto key_of = [&](int t, int pat, int q) -> size_t {
+        return pat == 0 ? (size_t)t * QMAX + q : n_pat + (size_t)t * 3 + (q - hrange_v[t].x);
+    };
+    std::vector<int> case_of(n_pat + 3 * (size_t)nb_total, -1);
     std::vector<double> seq;
     auto resolve_inexact = [&](int pat) -> int {
         std::vector<SeqCase> cases;
-        for (int t = 0; t < nb_total; ++t)
-            for (int q = 0; q < QMAX; ++q) {
-                const size_t k = pat * n_pat + (size_t)t * QMAX + q;
-                const Stat& S = hs[k];
+        for (int t = 0; t < nb_total; ++t) {
+            const int lo = pat == 0 ? 0 : hrange_v[t].x, hi = pat == 0 ? QMAX - 1 : hrange_v[t].y;
+            for (int q = lo; q <= hi; ++q) {
+                const Stat& S = stat_at(t, pat, q);
                 if (S.inexact || S.err_hi != 0 || S.err_lo >= (1ull << 53)) {
-                    case_of[k] = (int)(seq.size() + cases.size());
+                    case_of[key_of(t, pat, q)] = (int)(seq.size() + cases.size());
                     cases.push_back(SeqCase{t, pat, q});
                 }
             }
+        }
         if (cases.empty()) return DGPU_OK;
         std::vector<double> out(cases.size());
         DGPU_CHECK_CUDA(cudaMemcpyAsync(d_cases, cases.data(), sizeof(SeqCase) * cases.size(), cudaMemcpyHostToDevice, st));
-        seq_error_kernel<<<((int)cases.size() + 127) / 128, 128, 0, st>>>(d_tasks, d_cases, (int)cases.size(), d_seq);
+        seq_error_kernel<<<((int)cases.size() + 3) / 4, 128, 0, st>>>(d_tasks, d_cases, (int)cases.size(), d_seq);
         DGPU_CHECK_LAUNCH();
         DGPU_CHECK_CUDA(cudaMemcpyAsync(out.data(), d_seq, sizeof(double) * cases.size(), cudaMemcpyDeviceToHost, st));
         DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
@@ -626,13 +672,13 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
         return DGPU_OK;
     };
     auto host_stat = [&](int t, int pat, int q) {
-        const size_t k = pat * n_pat + (size_t)t * QMAX + q;
-        const Stat& S = hs[k];
+        const Stat& S = stat_at(t, pat, q);
+        const int ci = case_of[key_of(t, pat, q)];
         HostStat h;
         h.count0 = (int)(uint32_t)S.count0;
         h.pos = (int)(uint32_t)(S.posneg & 0xffffffffu);
         h.neg = (int)(uint32_t)(S.posneg >> 32);
-        h.error = case_of[k] >= 0 ? seq[case_of[k]] : (double)S.err_lo;
+        h.error = ci >= 0 ? seq[ci] : (double)S.err_lo;
         return h;
     };
     {
@@ -641,14 +687,19 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     }
     std::vector<std::vector<CostD>> cost(nb_total);
     std::vector<int> mn2(nb_total, 0), nqs(nb_total, 0);
-    for (int t = 0; t < nb_total; ++t) {
+    std::atomic<int> too_big{0};
+    parallel_for(nb_total, 64, [&](int t0, int t1) {
+    for (int t = t0; t < t1; ++t) {
         const BandTask& T = tasks[t];
         const int maxv = hmax[t];
         hrange[t] = make_int2(0, -1);
         if (maxv < 1) continue;
         const int max_bit = int(std::floor(std::log(float(maxv)) / std::log(2.0)));
         const int nq = 4 * max_bit + 5;
-        if (nq > QMAX) return DGPU_ERR_SIZE;
+        if (nq > QMAX) {
+            too_big = 1;
+            continue;
+        }
         nqs[t] = nq;
         cost[t].resize(nq);
         int lo = 0, hi = nq - 1, step = 4, mn = 0;
@@ -668,22 +719,23 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
         mn2[t] = mn;
         hrange[t] = make_int2(std::max(mn - 1, 0), std::min(mn + 1, nq - 1));
     }
+    });
+    if (too_big) return DGPU_ERR_SIZE;
+    for (int t = 0; t < nb_total; ++t) hrange_v[t] = hrange[t];
     DGPU_CHECK_CUDA(cudaMemcpyAsync(d_range, hrange, sizeof(int2) * nb_total, cudaMemcpyHostToDevice, st));
-    {
-        int maxs1 = 0;
-        for (const BandTask& T : tasks) maxs1 = std::max(maxs1, T.xl * ((T.yl + 1) / 2));
-        const dim3 grid1((maxs1 + STAT_THREADS * 8 - 1) / (STAT_THREADS * 8), nb_total, 1);
-        stats_kernel<<<grid1, STAT_THREADS, 0, st>>>(d_tasks, d_band_max, d_stats, 1, nb_total, d_range);
-        DGPU_CHECK_LAUNCH();
-    }
-    DGPU_CHECK_CUDA(cudaMemcpyAsync(hs + n_pat, d_stats + n_pat, sizeof(Stat) * n_pat, cudaMemcpyDeviceToHost, st));
+    stats_kernel<<<chunks[1], STAT_THREADS, 0, st>>>(d_tasks, d_band_max, d_stats, 1, nb_total, d_range);
+    DGPU_CHECK_LAUNCH();
+    gather_stats_kernel<<<(3 * nb_total + 255) / 256, 256, 0, st>>>(d_stats + n_pat, d_range, nb_total, d_stats3);
+    DGPU_CHECK_LAUNCH();
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(hs3, d_stats3, sizeof(Stat) * 3 * nb_total, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
     {
         const int rc = resolve_inexact(1);
         if (rc) return rc;
     }
     std::vector<uint8_t> hskip(ncb_total, 0);
-    for (int t = 0; t < nb_total; ++t) {
+    parallel_for(nb_total, 64, [&](int t0, int t1) {
+    for (int t = t0; t < t1; ++t) {
         const BandTask& T = tasks[t];
         int q = 0, bits = 0;
         if (hmax[t] >= 1) {
@@ -704,6 +756,7 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
         band_bits[t] = bits;
         band_skip[t] = bits == 0;
     }
+    });
     std::memcpy(cb_skip, hskip.data(), ncb_total);
     DGPU_CHECK_CUDA(cudaMemcpyAsync(d_cbskip, hskip.data(), ncb_total, cudaMemcpyHostToDevice, st));
     // ---- 4. quantise and reconstruct, DC bands first ----
@@ -719,13 +772,13 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
         DGPU_CHECK_LAUNCH();
     }
     QLaunch L{};
-    int chunks = 0;
+    int qchunks = 0;
     auto flush = [&]() -> int {
         if (L.n == 0) return DGPU_OK;
-        quantise_kernel<<<chunks, 256, 0, st>>>(L);
+        quantise_kernel<<<qchunks, 256, 0, st>>>(L);
         DGPU_CHECK_LAUNCH();
         L.n = 0;
-        chunks = 0;
+        qchunks = 0;
         return DGPU_OK;
     };
     for (int t = 0; t < nb_total; ++t) {
@@ -750,8 +803,8 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
         B.off = C.intra ? intra_off4(band_qidx[t]) : inter_off4(band_qidx[t]);
         B.skip = band_skip[t];
         B.cb_skip = d_cbskip + T.cb_first;
-        B.first = chunks;
-        chunks += (xl * yl + 255) / 256;
+        B.first = qchunks;
+        qchunks += (xl * yl + 255) / 256;
     }
     return flush();
 }

@@ -1,9 +1,14 @@
 // Library-wide runtime pieces: version, device check, last-error record and the
 // per-device scratch buffer used when callers pass no scratch.
 
+#include <algorithm>
 #include <atomic>
+#include <condition_variable>
 #include <cstdio>
+#include <deque>
 #include <mutex>
+#include <thread>
+#include <vector>
 
 #include "dgpu_internal.cuh"
 
@@ -21,6 +26,7 @@ std::atomic<unsigned long long> g_launches{0};
 }  // namespace
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 void set_last_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
     std::lock_guard<std::mutex> lk(g_err_mu);
@@ -50,6 +56,86 @@ int library_scratch(size_t bytes, void** out) {
     }
     *out = g_scratch[dev];
     return DGPU_OK;
+}
+
+namespace {
+
+// Host worker threads shared by every caller of parallel_for (several host threads may submit
+// at once: each waits only for its own chunks).
+class HostPool {
+   public:
+    explicit HostPool(int n) {
+        for (int i = 0; i < n; ++i) workers_.emplace_back([this] { loop(); });
+    }
+    ~HostPool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+    }
+    int size() const { return (int)workers_.size(); }
+    void submit(std::function<void()> f) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            q_.push_back(std::move(f));
+        }
+        cv_.notify_one();
+    }
+
+   private:
+    void loop() {
+        for (;;) {
+            std::function<void()> f;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [this] { return stop_ || !q_.empty(); });
+                if (q_.empty()) return;
+                f = std::move(q_.front());
+                q_.pop_front();
+            }
+            f();
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<std::function<void()>> q_;
+    bool stop_ = false;
+};
+
+HostPool& host_pool() {
+    static HostPool pool(std::max(1, std::min(15, (int)std::thread::hardware_concurrency() - 1)));
+    return pool;
+}
+
+}  // namespace
+
+void parallel_for(int n, int grain, const std::function<void(int, int)>& body) {
+    if (n <= 0) return;
+    grain = std::max(1, grain);
+    HostPool& pool = host_pool();
+    const int chunks = std::min(pool.size() + 1, (n + grain - 1) / grain);
+    if (chunks <= 1) {
+        body(0, n);
+        return;
+    }
+    const int per = (n + chunks - 1) / chunks;
+    std::mutex m;
+    std::condition_variable done;
+    int left = chunks - 1;
+    for (int c = 1; c < chunks; ++c) {
+        const int b = c * per, e = std::min(n, b + per);
+        pool.submit([&, b, e] {
+            if (b < e) body(b, e);
+            std::lock_guard<std::mutex> lk(m);
+            if (--left == 0) done.notify_all();
+        });
+    }
+    body(0, std::min(n, per));
+    std::unique_lock<std::mutex> lk(m);
+    done.wait(lk, [&] { return left == 0; });
 }
 
 }  // namespace dgpu

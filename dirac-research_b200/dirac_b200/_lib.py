@@ -107,6 +107,15 @@ SIGNATURES = {
     "dgpu_encoder_code_next": (c_int, [c_void_p, c_void_p, c_void_p]),
     "dgpu_encoder_item_bytes": (c_size_t, [c_void_p, c_int, c_int, c_int]),
     "dgpu_encoder_read": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_size_t, c_int]),
+    "dgpu_batch_device_bytes": (c_size_t, [c_int, c_void_p, c_void_p]),
+    "dgpu_batch_create": (c_int, [c_int, c_void_p, c_void_p, c_void_p, P_void]),
+    "dgpu_batch_destroy": (c_int, [c_void_p]),
+    "dgpu_batch_planes": (c_int, [c_void_p, c_int, P_void]),
+    "dgpu_batch_load": (c_int, [c_void_p, c_int, P_void, c_int]),
+    "dgpu_batch_run": (c_int, [c_void_p]),
+    "dgpu_batch_stage_times": (c_int, [c_void_p, c_void_p]),
+    "dgpu_batch_item_bytes": (c_size_t, [c_void_p, c_int, c_int, c_int]),
+    "dgpu_batch_read": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_size_t, c_int]),
     "dgpu_encoder_group_device_bytes": (c_size_t, [P_void, c_int]),
     "dgpu_encoder_group_create": (c_int, [P_void, c_int, P_void]),
     "dgpu_encoder_group_destroy": (c_int, [c_void_p]),

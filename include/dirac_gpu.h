@@ -364,6 +364,73 @@ size_t dgpu_encoder_item_bytes(void* encoder, int pnum, int what, int comp);
 int dgpu_encoder_read(void* encoder, int pnum, int what, int comp, void* dst, size_t bytes, int on_host);
 
 /* ---------------------------------------------------------------------------------------
+ * Heterogeneous picture batch (batched form): many pictures of different sizes, chroma
+ * formats, bit depths, filters and depths coded together, each exactly as
+ * PictureCompressor codes one picture once its motion data is known
+ * (libdirac_encoder/picture_compress.cpp:92-180, 418-531): motion compensation SUBTRACT
+ * against the upconverted references (Picture::UpData), forward transform, quantiser choice
+ * with quantisation and reconstruction (CodeResidue), inverse transform, motion
+ * compensation ADD with the clip (inter) or the clip (intra).
+ *
+ * Per picture: the coding parameters below; for inter pictures the references' planes
+ * (codec samples, dense, device memory; distinct planes are upconverted once per run) and
+ * the motion data in the layout of dgpu_motion_compensate.  The batch keeps the given
+ * device pointers, which must stay valid while it lives.  The lambdas, band weights and
+ * initial entropy-correction factors are the encoder's (GetCompLambda with the given intra
+ * ratio and B flag; CodeResidue's perceptual scale; EntropyCorrector::Init).
+ *
+ * dgpu_batch_planes gives picture k's three device planes: the caller writes the picture's
+ * codec samples there (or loads them with dgpu_batch_load) before a run and reads the
+ * reconstruction after it.  dgpu_batch_run
+ * codes every picture: on its first call it tunes the motion-compensation tile shape
+ * (keeping the planes' contents) and captures the device work before and after the
+ * quantiser choice in two CUDA graphs, which later calls replay; the quantiser choice
+ * synchronises the stream (host Lagrangian, as the reference).  On return the band results
+ * are readable with dgpu_batch_read (DGPU_ENC_BANDS / CBSKIP); the reconstruction
+ * (DGPU_ENC_RECON), coefficients and quantised indices are complete once the stream reaches
+ * the end of the run.  The first call must not be made during a stream capture.
+ * ------------------------------------------------------------------------------------- */
+typedef struct {
+    int cformat, width, height;   /* ChromaFormat and luma size */
+    int luma_depth, chroma_depth; /* bits per sample, 8..14 */
+    int filter, wlt_depth;        /* WltFilter and transform depth */
+    int intra;                    /* 1: intra picture */
+    int is_b;                     /* inter: PictureParams::IsBPicture (quantiser lambda) */
+    float qf, cpd;                /* quality factor, perceptual cycles per degree */
+    double intra_ratio;           /* inter: MEData::IntraBlockRatio of the motion data */
+    dgpu_block_params bp;         /* inter: block parameters */
+} dgpu_batch_picture;
+
+typedef struct {
+    const int16_t* ref1[3];       /* first reference's planes */
+    const int16_t* ref2[3];       /* second reference's planes, or NULLs */
+    const int16_t* mv1;
+    const int16_t* mv2;           /* NULL with one reference */
+    const uint8_t* mode;
+    const int16_t* dc;
+    const uint8_t* split;
+} dgpu_batch_motion;
+
+/* motion: n entries (read for inter pictures only), or NULL when every picture is intra */
+size_t dgpu_batch_device_bytes(int n, const dgpu_batch_picture* pics, const dgpu_batch_motion* motion);
+int dgpu_batch_create(int n, const dgpu_batch_picture* pics, const dgpu_batch_motion* motion, void* stream,
+                      void** batch);
+int dgpu_batch_destroy(void* batch);
+int dgpu_batch_planes(void* batch, int k, int16_t** planes);
+/* Copies picture k's three planes (int16 codec samples, dense) into the batch, from host
+ * (on_host = 1; page-locked memory keeps the copy asynchronous) or device memory. */
+int dgpu_batch_load(void* batch, int k, const int16_t* const* planes, int on_host);
+int dgpu_batch_run(void* batch);
+/* One run timed by stage with CUDA events on the batch's stream (synchronises): ms[0] the
+ * upconversions, motion compensation SUBTRACT and forward transforms, ms[1] the quantiser
+ * choice with quantisation (host Lagrangian included), ms[2] the inverse transforms and
+ * motion compensation ADD / clips. */
+int dgpu_batch_stage_times(void* batch, float* ms);
+size_t dgpu_batch_item_bytes(void* batch, int k, int what, int comp);
+int dgpu_batch_read(void* batch, int k, int what, int comp, void* dst, size_t bytes, int on_host);
+
+
+/* ---------------------------------------------------------------------------------------
  * Encoder groups (batched form): the motion estimation of several sequences in one launch.
  * Replaces nothing in the reference, which codes one sequence per SequenceCompressor; each
  * member's results are those of PictureCompressor::PixelME / SubPixelME / ModeDecisionME

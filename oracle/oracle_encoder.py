@@ -291,3 +291,37 @@ def encode_sequence(cfg, frames, weights_fn, blocks_fn, oracle=None, ecf_fn=None
     while enc.code_next() is not None:
         pass
     return enc
+
+
+def code_picture(pic, planes, weights_fn, blocks_fn, oracle=None, refs=None, me=None):
+    """One picture coded as the loop above codes it once its motion data is known (the
+    PictureCompressor steps after motion estimation: motion compensation SUBTRACT, transform,
+    residue coding, inverse transform, motion compensation ADD and clip).
+
+    pic: the picture's parameters (cformat, width, height, luma_depth, chroma_depth, filter,
+    wlt_depth, intra, is_b, qf, cpd, intra_ratio; inter pictures also mv_precision, xblen,
+    yblen, xbsep, ybsep); planes: its int16 codec samples; refs: the references' planes (one
+    or two); me: the motion data {"mv": [mv1, mv2], "mode", "dc", "split"}.  A B picture
+    (is_b) needs two references.  Returns (reconstructed planes, result dict of code_residue)."""
+    cfg = {k: pic[k] for k in ("cformat", "width", "height", "luma_depth", "chroma_depth", "qf", "cpd",
+                               "wlt_depth")}
+    cfg.update(intra_filter=pic["filter"], inter_filter=pic["filter"], l1_sep=1, num_l1=0)
+    for k in ("mv_precision", "xblen", "yblen", "xbsep", "ybsep"):
+        cfg[k] = pic.get(k, 8 if k != "mv_precision" else 2)
+    enc = OracleEncoder(cfg, weights_fn, blocks_fn, oracle)
+    pn = 10
+    p = Pic(pn, planes)
+    p.intra = bool(pic["intra"])
+    if not p.intra:
+        nref = len(refs)
+        if pic.get("is_b") and nref != 2:
+            raise ValueError("a B picture has two references")
+        ids = [pn - 1, pn + 1] if pic.get("is_b") else [pn - 1, pn - 2][:nref]
+        for i, r in zip(ids, refs):
+            enc.pics[i] = Pic(i, r)
+        p.refs = ids
+        p.ratio = pic["intra_ratio"]
+        p.me = me
+        enc.motion_compensate(p, 1)
+    enc.code_residue(p)
+    return p.data, p.result
