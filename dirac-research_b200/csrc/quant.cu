@@ -267,43 +267,63 @@ __global__ void __launch_bounds__(STAT_THREADS) stats_kernel(const BandTask* tas
     }
 }
 
-// Fallback: the reference's sequential double accumulation of pow4(error) for one
-// (band, pattern, q) per thread, in its raster order (quant_chooser.cpp:149-264).
-struct SeqCase {
-    int task, pattern, q;
-};
+// Fallback for the sums the exact path cannot represent (a term or the total at or above
+// 2^53): the reference's sequential double accumulation of pow4(error) in its raster order
+// (quant_chooser.cpp:149-264), written back into the entry (err_lo holds the double's bits,
+// pad = 1).  Entries: pattern 0, stats[t * QMAX + q]; pattern 1, the compact third-pass
+// array stats[t * 3 + j] for q = qrange[t].x + j.  Each warp scans 32 entries at a time and
+// resolves the flagged ones together: the lanes compute the terms of 32 consecutive samples,
+// lane 0 adds them one by one in order.
+__device__ __forceinline__ bool stat_inexact(const Stat& S) {
+    return S.inexact || S.err_hi != 0 || S.err_lo >= (1ull << 53);
+}
 
-// One warp per case: the lanes compute the terms of 32 consecutive samples (raster order) and
-// lane 0 adds them one by one in that order, so the loads and the arithmetic run in parallel
-// and only the additions stay sequential.
-__global__ void seq_error_kernel(const BandTask* tasks, const SeqCase* cases, int ncases, double* out) {
-    const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+__global__ void seq_resolve_kernel(const BandTask* tasks, Stat* stats, int n_entries, int pattern,
+                                   const int2* qrange) {
     const int lane = threadIdx.x & 31;
-    if (k >= ncases) return;
-    const SeqCase C = cases[k];
-    const BandTask T = tasks[C.task];
-    const int xr = C.pattern ? 1 : 2;
-    const int sx = (T.xl + xr - 1) / xr, sy = (T.yl + 1) / 2;
-    const int n = sx * sy;
-    const int qf = qf4(C.q), off = inter_off4(C.q);
-    double s = 0.0;
-    for (int k0 = 0; k0 < n; k0 += 32) {
-        double term = 0.0;
-        const int i = k0 + lane;
-        if (i < n) {
-            const int sj = i / sx, si = i - sj * sx;
-            const int a = abs(T.data[(size_t)(2 * sj) * T.stride + xr * si]);
-            const int qv = (a << 2) / qf;
-            const double e = !qv ? (double)a : (double)(a - ((qv * qf + off + 2) >> 2));
-            term = __dmul_rn(__dmul_rn(__dmul_rn(e, e), e), e);
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    const int per = pattern ? 3 : QMAX;
+    for (int base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < n_entries; base += warps * 32) {
+        const int e = base + lane;
+        bool flag = false;
+        if (e < n_entries) {
+            const Stat& S = stats[e];
+            flag = S.pad == 0 && stat_inexact(S);
+            if (flag && pattern) flag = qrange[e / 3].x + e % 3 <= qrange[e / 3].y;
         }
-        const int m = min(32, n - k0);
-        for (int l = 0; l < m; ++l) {
-            const double t = __shfl_sync(0xffffffffu, term, l);
-            s = __dadd_rn(s, t);
+        unsigned m = __ballot_sync(0xffffffffu, flag);
+        while (m) {
+            const int l = __ffs(m) - 1;
+            m &= m - 1;
+            const int ent = base + l;
+            const int t = ent / per;
+            const int q = pattern ? qrange[t].x + ent % 3 : ent % QMAX;
+            const BandTask T = tasks[t];
+            const int xr = pattern ? 1 : 2;
+            const int sx = (T.xl + xr - 1) / xr, sy = (T.yl + 1) / 2;
+            const int n = sx * sy;
+            const int qf = qf4(q), off = inter_off4(q);
+            double s = 0.0;
+            for (int k0 = 0; k0 < n; k0 += 32) {
+                double term = 0.0;
+                const int i = k0 + lane;
+                if (i < n) {
+                    const int sj = i / sx, si = i - sj * sx;
+                    const int a = abs(T.data[(size_t)(2 * sj) * T.stride + xr * si]);
+                    const int qv = (a << 2) / qf;
+                    const double ev = !qv ? (double)a : (double)(a - ((qv * qf + off + 2) >> 2));
+                    term = __dmul_rn(__dmul_rn(__dmul_rn(ev, ev), ev), ev);
+                }
+                const int cnt = min(32, n - k0);
+                for (int k = 0; k < cnt; ++k) s = __dadd_rn(s, __shfl_sync(0xffffffffu, term, k));
+            }
+            if (lane == 0) {
+                stats[ent].err_lo = (unsigned long long)__double_as_longlong(s);
+                stats[ent].err_hi = 0;
+                stats[ent].pad = 1;
+            }
         }
     }
-    if (lane == 0) out[k] = s;
 }
 
 // Gathers the third pass's statistics, the three quantisers qrange[band] of each band, into
@@ -491,7 +511,6 @@ static size_t residue_ws_need(int nb_total, int ncb_total, size_t dcwork_elems) 
            align_up(sizeof(int2) * nb_total, 256) +
            align_up(sizeof(int) * ncb_total, 256) + align_up(sizeof(Stat) * nb_total * 2 * QMAX, 256) +
            align_up(sizeof(int32_t) * dcwork_elems, 256) + align_up(ncb_total, 256) +
-           align_up((sizeof(SeqCase) + sizeof(double)) * nb_total * 2 * QMAX, 256) +
            align_up(sizeof(Stat) * nb_total * 3, 256) + 256;
 }
 
@@ -562,8 +581,6 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     Stat* d_stats = reinterpret_cast<Stat*>(take(sizeof(Stat) * nb_total * 2 * QMAX));
     int32_t* d_dcwork = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * dcwork_elems));
     uint8_t* d_cbskip = reinterpret_cast<uint8_t*>(take(ncb_total));
-    SeqCase* d_cases = reinterpret_cast<SeqCase*>(take(sizeof(SeqCase) * nb_total * 2 * QMAX));
-    double* d_seq = reinterpret_cast<double*>(take(sizeof(double) * nb_total * 2 * QMAX));
     Stat* d_stats3 = reinterpret_cast<Stat*>(take(sizeof(Stat) * nb_total * 3));
 
     size_t dcoff = 0;
@@ -620,6 +637,8 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     // gathered in a second, much smaller launch.
     stats_kernel<<<chunks[0], STAT_THREADS, 0, st>>>(d_tasks, d_band_max, d_stats, 0, nb_total, nullptr);
     DGPU_CHECK_LAUNCH();
+    seq_resolve_kernel<<<148 * 4, 128, 0, st>>>(d_tasks, d_stats, (int)((size_t)nb_total * QMAX), 0, nullptr);
+    DGPU_CHECK_LAUNCH();
     // statistics and maxima come back through page-locked memory (one buffer per host thread)
     const size_t n_pat = (size_t)nb_total * QMAX;
     char* pin = nullptr;
@@ -637,54 +656,25 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     DGPU_CHECK_CUDA(cudaMemcpyAsync(hmax, d_band_max, sizeof(int) * nb_total, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaMemcpyAsync(hcb, d_cb_max, sizeof(int) * ncb_total, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
-    // sums the exact path could not represent: the sequential double kernel for those cases.
     // Statistics of (band t, pattern, q): pattern 0 at hs[t * QMAX + q]; pattern 1 (only the
-    // three quantisers of the band's range) at hs3[t * 3 + q - lo].
+    // three quantisers of the band's range) at hs3[t * 3 + q - lo].  Sums the exact path could
+    // not represent were replaced on the device by the reference's sequential double sums.
     std::vector<int2> hrange_v(nb_total, make_int2(0, -1));
-    auto stat_at = [&](int t, int pat, int q) -> const Stat& {
-        return pat == 0 ? hs[(size_t)t * QMAX + q] : hs3[(size_t)t * 3 + (q - hrange_v[t].x)];
-    };
-    auto key_of = [&](int t, int pat, int q) -> size_t {
-        return pat == 0 ? (size_t)t * QMAX + q : n_pat + (size_t)t * 3 + (q - hrange_v[t].x);
-    };
-    std::vector<int> case_of(n_pat + 3 * (size_t)nb_total, -1);
-    std::vector<double> seq;
-    auto resolve_inexact = [&](int pat) -> int {
-        std::vector<SeqCase> cases;
-        for (int t = 0; t < nb_total; ++t) {
-            const int lo = pat == 0 ? 0 : hrange_v[t].x, hi = pat == 0 ? QMAX - 1 : hrange_v[t].y;
-            for (int q = lo; q <= hi; ++q) {
-                const Stat& S = stat_at(t, pat, q);
-                if (S.inexact || S.err_hi != 0 || S.err_lo >= (1ull << 53)) {
-                    case_of[key_of(t, pat, q)] = (int)(seq.size() + cases.size());
-                    cases.push_back(SeqCase{t, pat, q});
-                }
-            }
-        }
-        if (cases.empty()) return DGPU_OK;
-        std::vector<double> out(cases.size());
-        DGPU_CHECK_CUDA(cudaMemcpyAsync(d_cases, cases.data(), sizeof(SeqCase) * cases.size(), cudaMemcpyHostToDevice, st));
-        seq_error_kernel<<<((int)cases.size() + 3) / 4, 128, 0, st>>>(d_tasks, d_cases, (int)cases.size(), d_seq);
-        DGPU_CHECK_LAUNCH();
-        DGPU_CHECK_CUDA(cudaMemcpyAsync(out.data(), d_seq, sizeof(double) * cases.size(), cudaMemcpyDeviceToHost, st));
-        DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
-        seq.insert(seq.end(), out.begin(), out.end());
-        return DGPU_OK;
-    };
     auto host_stat = [&](int t, int pat, int q) {
-        const Stat& S = stat_at(t, pat, q);
-        const int ci = case_of[key_of(t, pat, q)];
+        const Stat& S = pat == 0 ? hs[(size_t)t * QMAX + q] : hs3[(size_t)t * 3 + (q - hrange_v[t].x)];
         HostStat h;
         h.count0 = (int)(uint32_t)S.count0;
         h.pos = (int)(uint32_t)(S.posneg & 0xffffffffu);
         h.neg = (int)(uint32_t)(S.posneg >> 32);
-        h.error = ci >= 0 ? seq[ci] : (double)S.err_lo;
+        if (S.pad) {
+            double d;
+            std::memcpy(&d, &S.err_lo, sizeof d);
+            h.error = d;
+        } else {
+            h.error = (double)S.err_lo;
+        }
         return h;
     };
-    {
-        const int rc = resolve_inexact(0);
-        if (rc) return rc;
-    }
     std::vector<std::vector<CostD>> cost(nb_total);
     std::vector<int> mn2(nb_total, 0), nqs(nb_total, 0);
     std::atomic<int> too_big{0};
@@ -727,12 +717,10 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     DGPU_CHECK_LAUNCH();
     gather_stats_kernel<<<(3 * nb_total + 255) / 256, 256, 0, st>>>(d_stats + n_pat, d_range, nb_total, d_stats3);
     DGPU_CHECK_LAUNCH();
+    seq_resolve_kernel<<<148 * 4, 128, 0, st>>>(d_tasks, d_stats3, 3 * nb_total, 1, d_range);
+    DGPU_CHECK_LAUNCH();
     DGPU_CHECK_CUDA(cudaMemcpyAsync(hs3, d_stats3, sizeof(Stat) * 3 * nb_total, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
-    {
-        const int rc = resolve_inexact(1);
-        if (rc) return rc;
-    }
     std::vector<uint8_t> hskip(ncb_total, 0);
     parallel_for(nb_total, 64, [&](int t0, int t1) {
     for (int t = t0; t < t1; ++t) {
