@@ -93,6 +93,7 @@ struct BandTask {  // one band: where its data lives and where its statistics go
     int band;                 // global band index
     int cb_first, xn, yn;     // code blocks of the band
     int chunk_first[2];       // first CTA of the band in each sampling pattern's flattened grid
+    int elem_first;           // first CTA of the band in the element-wise grid (maxima)
 };
 
 constexpr int MAX_COMPS = 256;
@@ -111,24 +112,38 @@ __global__ void dc_dpcm_kernel(const int32_t* c, int stride, int xl, int yl, int
 
 // Per band: max |c|.  Per code block: max |c| (for QuantChooser::SetSkip).  Lanes of a warp
 // that fall in the same code block combine their maxima before one atomic.
-__global__ void band_max_kernel(const BandTask* tasks, int* band_max, int* cb_max) {
-    const BandTask T = tasks[blockIdx.y];
+// Code block (0 .. n-1) holding position pos of a band side of length len split into n:
+// block c covers [c * len / n, (c + 1) * len / n) (integer division), as the band coders
+// split a band.
+__device__ __forceinline__ int cb_of(int pos, int len, int n) {
+    int c = (pos * n) / len;
+    while (c + 1 < n && ((c + 1) * len) / n <= pos) ++c;
+    while (c > 0 && (c * len) / n > pos) --c;
+    return c;
+}
+
+constexpr int MAX_PER_CTA = 256 * 8;  // elements per CTA of the element-wise grids
+
+// grid: one CTA per MAX_PER_CTA elements of a band, the bands laid end to end
+// (BandTask::elem_first).
+__global__ void band_max_kernel(const BandTask* tasks, int ntasks, int* band_max, int* cb_max) {
+    int lo_b = 0, hi_b = ntasks - 1;
+    while (lo_b < hi_b) {
+        const int mid = (lo_b + hi_b + 1) >> 1;
+        if (tasks[mid].elem_first <= (int)blockIdx.x) lo_b = mid;
+        else hi_b = mid - 1;
+    }
+    const BandTask T = tasks[lo_b];
     const int n = T.xl * T.yl;
-    const int stride = gridDim.x * blockDim.x;
+    const int base = ((int)blockIdx.x - T.elem_first) * MAX_PER_CTA;
     int m = 0;
-    for (int k0 = blockIdx.x * blockDim.x; k0 < n; k0 += stride) {
+    for (int k0 = base; k0 < min(n, base + MAX_PER_CTA); k0 += blockDim.x) {
         const int k = k0 + threadIdx.x;
         int a = 0, cb = -1;
         if (k < n) {
             const int j = k / T.xl, i = k - j * T.xl;
             a = abs(T.data[(size_t)j * T.stride + i]);
-            int cx = (int)(((long long)i * T.xn) / T.xl);
-            while (cx + 1 < T.xn && ((cx + 1) * T.xl) / T.xn <= i) ++cx;
-            while (cx > 0 && (cx * T.xl) / T.xn > i) --cx;
-            int cy = (int)(((long long)j * T.yn) / T.yl);
-            while (cy + 1 < T.yn && ((cy + 1) * T.yl) / T.yn <= j) ++cy;
-            while (cy > 0 && (cy * T.yl) / T.yn > j) --cy;
-            cb = T.cb_first + cy * T.xn + cx;
+            cb = T.cb_first + cb_of(j, T.yl, T.yn) * T.xn + cb_of(i, T.xl, T.xn);
         }
         m = max(m, a);
         const unsigned grp = __match_any_sync(0xffffffffu, cb);
@@ -350,23 +365,23 @@ struct QBand {
     int first;          // first thread-chunk index
 };
 
-constexpr int MAX_QBANDS = 48;
-struct QLaunch {
-    int n;
-    QBand band[MAX_QBANDS];
-};
 
 __device__ __forceinline__ int cb_index(int pos, int len, int n) {
-    int c = (int)(((long long)pos * n) / len);
+    int c = (pos * n) / len;
     while (c + 1 < n && ((c + 1) * len) / n <= pos) ++c;
     while (c > 0 && (c * len) / n > pos) --c;
     return c;
 }
 
-__global__ void quantise_kernel(const __grid_constant__ QLaunch L) {
-    int b = 0;
-    while (b + 1 < L.n && L.band[b + 1].first <= (int)blockIdx.x) ++b;
-    const QBand& B = L.band[b];
+// grid: one CTA per 256 coefficients of a band, the bands (device table) laid end to end.
+__global__ void quantise_kernel(const QBand* bands, int nbands) {
+    int lo_b = 0, hi_b = nbands - 1;
+    while (lo_b < hi_b) {
+        const int mid = (lo_b + hi_b + 1) >> 1;
+        if (bands[mid].first <= (int)blockIdx.x) lo_b = mid;
+        else hi_b = mid - 1;
+    }
+    const QBand B = bands[lo_b];
     const int k = (blockIdx.x - B.first) * blockDim.x + threadIdx.x;
     if (k >= B.xl * B.yl) return;
     const int j = k / B.xl, i = k - j * B.xl;
@@ -511,7 +526,7 @@ static size_t residue_ws_need(int nb_total, int ncb_total, size_t dcwork_elems) 
            align_up(sizeof(int2) * nb_total, 256) +
            align_up(sizeof(int) * ncb_total, 256) + align_up(sizeof(Stat) * nb_total * 2 * QMAX, 256) +
            align_up(sizeof(int32_t) * dcwork_elems, 256) + align_up(ncb_total, 256) +
-           align_up(sizeof(Stat) * nb_total * 3, 256) + 256;
+           align_up(sizeof(Stat) * nb_total * 3, 256) + align_up(sizeof(QBand) * nb_total, 256) + 256;
 }
 
 extern "C" size_t dgpu_code_residue_workspace_bytes(int n, const int* intra, const int* depth, const int* cw,
@@ -582,9 +597,10 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     int32_t* d_dcwork = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * dcwork_elems));
     uint8_t* d_cbskip = reinterpret_cast<uint8_t*>(take(ncb_total));
     Stat* d_stats3 = reinterpret_cast<Stat*>(take(sizeof(Stat) * nb_total * 3));
+    QBand* d_qbands = reinterpret_cast<QBand*>(take(sizeof(QBand) * nb_total));
 
     size_t dcoff = 0;
-    int chunks[2] = {0, 0};
+    int chunks[2] = {0, 0}, echunks = 0;
     for (int c = 0; c < n; ++c) {
         Comp& C = comps[c];
         if (C.intra) {
@@ -605,6 +621,8 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
             T.cb_first = band_cb_first[T.band];
             T.xn = band_ncb[2 * T.band];
             T.yn = band_ncb[2 * T.band + 1];
+            T.elem_first = echunks;
+            echunks += (xl * yl + MAX_PER_CTA - 1) / MAX_PER_CTA;
             for (int pat = 0; pat < 2; ++pat) {
                 const int xr = pat ? 1 : 2;
                 const long long ns = (long long)((xl + xr - 1) / xr) * ((yl + 1) / 2);
@@ -626,11 +644,8 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
         dc_dpcm_kernel<<<(xl * yl + 255) / 256, 256, 0, st>>>(C.coeff, C.cw, xl, yl, C.dcwork);
         DGPU_CHECK_LAUNCH();
     }
-    {
-        dim3 grid(64, nb_total);
-        band_max_kernel<<<grid, 256, 0, st>>>(d_tasks, d_band_max, d_cb_max);
-        DGPU_CHECK_LAUNCH();
-    }
+    band_max_kernel<<<echunks, 256, 0, st>>>(d_tasks, nb_total, d_band_max, d_cb_max);
+    DGPU_CHECK_LAUNCH();
     // ---- 2. statistics and the reference's three-pass Lagrangian choice per band ----
     // Passes 1 and 2 use the 2 x 2 pattern over every even quantiser; pass 3 needs the 1 x 2
     // pattern at three quantisers only, known once pass 2 is decided: its statistics are
@@ -759,27 +774,17 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
                                                tasks[t].yn, qf4(q), intra_off4(q), d_cbskip + tasks[t].cb_first);
         DGPU_CHECK_LAUNCH();
     }
-    QLaunch L{};
+    // one launch over every band not quantised above, from a device table
+    std::vector<QBand> qb;
+    qb.reserve(nb_total);
     int qchunks = 0;
-    auto flush = [&]() -> int {
-        if (L.n == 0) return DGPU_OK;
-        quantise_kernel<<<qchunks, 256, 0, st>>>(L);
-        DGPU_CHECK_LAUNCH();
-        L.n = 0;
-        qchunks = 0;
-        return DGPU_OK;
-    };
     for (int t = 0; t < nb_total; ++t) {
         const BandTask& T = tasks[t];
         const Comp& C = comps[T.comp];
         if (C.intra && t == C.band_first + C.nbands - 1 && !band_skip[t]) continue;  // done above
         int xp, yp, xl, yl;
         band_rect(C.depth, C.cw, C.ch, t - C.band_first + 1, xp, yp, xl, yl);
-        if (L.n == MAX_QBANDS) {
-            int rc = flush();
-            if (rc) return rc;
-        }
-        QBand& B = L.band[L.n++];
+        QBand B;
         B.data = const_cast<int32_t*>(C.coeff) + (size_t)yp * C.cw + xp;
         B.qout = qout && qout[T.comp] ? qout[T.comp] + (size_t)yp * C.cw + xp : nullptr;
         B.stride = C.cw;
@@ -793,8 +798,14 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
         B.cb_skip = d_cbskip + T.cb_first;
         B.first = qchunks;
         qchunks += (xl * yl + 255) / 256;
+        qb.push_back(B);
     }
-    return flush();
+    if (qb.empty()) return DGPU_OK;
+    // a copy from pageable memory returns once the source has been staged, so qb may go
+    DGPU_CHECK_CUDA(cudaMemcpyAsync(d_qbands, qb.data(), sizeof(QBand) * qb.size(), cudaMemcpyHostToDevice, st));
+    quantise_kernel<<<qchunks, 256, 0, st>>>(d_qbands, (int)qb.size());
+    DGPU_CHECK_LAUNCH();
+    return DGPU_OK;
 }
 
 // CoeffArray::SetBandWeights (libdirac_common/wavelet_utils.cpp:192-382) with

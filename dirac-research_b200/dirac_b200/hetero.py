@@ -71,8 +71,7 @@ def stage_bytes(pictures):
     from .roofline import dwt_bytes
 
     pre = quant = post = 0
-    refs = set()
-    for k, p in enumerate(pictures):
+    for p in pictures:
         xs = 0 if p["cformat"] == 0 else 1
         ys = 1 if p["cformat"] == 2 else 0
         comps = [(p["width"], p["height"]), (p["width"] >> xs, p["height"] >> ys),
@@ -101,3 +100,34 @@ def upconvert_bytes(motion):
             for t in m[key]:
                 seen[t.data_ptr()] = t.numel()
     return 10 * sum(seen.values())
+
+
+def main(argv=None):
+    """python -m dirac_b200.hetero [--runs N]: builds the workload, codes it N times and prints
+    the wall time per run and one run's stage times (also the command for profiling)."""
+    import argparse
+    import time
+
+    from .batch import PictureBatch
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--runs", type=int, default=4)
+    a = ap.parse_args(argv)
+    pictures, motion, planes, keep = make_inputs()
+    batch = PictureBatch(pictures, motion)
+    for r in range(a.runs):
+        for k in range(len(planes)):
+            batch.load(k, planes[k])
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        batch.run()
+        torch.cuda.synchronize()
+        print(f"run {r}: {1000 * (time.perf_counter() - t):.2f} ms for {len(pictures)} pictures")
+    print("stage ms (pre, quant, post):", [round(x, 3) for x in batch.stage_times()])
+    batch.close()
+    del keep
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
