@@ -640,9 +640,29 @@ struct PelLaunch {
 // candidate (G = the largest power of two with 2 G n <= 32, so small lists still use most
 // lanes).  The list's minimum with the earliest index replaces (best, bmv) only when strictly
 // smaller: the same result as the reference's sequential strict-< scan.
+// Earlier lists: the square of radius r around each of n centres (AddVect drops a candidate
+// already listed, block_match.cpp:170-190).
+struct SeenLists {
+    short2 c[2];
+    int n;
+    __device__ __forceinline__ bool has(short2 v, int r) const {
+        for (int k = 0; k < n; ++k)
+            if (abs(v.x - c[k].x) <= r && abs(v.y - c[k].y) <= r) return true;
+        return false;
+    }
+};
+
 __device__ __noinline__ void pel_list_best(const int16_t* pic, const int16_t* ref, int pw, int ph, const Blim& b, short2 centre,
-                              int r, int16_t* mem, int& best, short2& bmv, bool blk_staged = false) {
+                              int r, int16_t* mem, int& best, short2& bmv, bool blk_staged = false,
+                              SeenLists seen = SeenLists{{}, 0}) {
     const int lane = threadIdx.x & 31;
+    const int n_all = (2 * r + 1) * (2 * r + 1);
+    if (seen.n) {
+        // a list wholly inside the earlier lists adds no candidate: nothing to stage or sum
+        bool fresh = false;
+        for (int k = lane; k < n_all; k += 32) fresh |= !seen.has(cand_at(centre, r, k), r);
+        if (!__any_sync(0xffffffffu, fresh)) return;
+    }
     const int ww = b.xl + 2 * r, wh = b.yl + 2 * r;
     int16_t* blk = mem;
     int16_t* win = mem + b.xl * b.yl;
@@ -659,7 +679,12 @@ __device__ __noinline__ void pel_list_best(const int16_t* pic, const int16_t* re
     for (int k0 = 0; k0 < n; k0 += per_round) {
         const int k = k0 + grp;
         int sad = 0;
+        bool dup = false;
         if (k < n && grp < per_round) {
+            const short2 c = cand_at(centre, r, k);
+            dup = seen.n && seen.has(c, r);
+        }
+        if (k < n && grp < per_round && !dup) {
             const short2 c = cand_at(centre, r, k);
             const int dx = c.x - centre.x + r, dy = c.y - centre.y + r;
             for (int y = g; y < b.yl; y += G) {
@@ -676,7 +701,7 @@ __device__ __noinline__ void pel_list_best(const int16_t* pic, const int16_t* re
             tot += v;
         }
         sad = tot;
-        if (k < n && grp < per_round && g == 0 && sad < my_best) {
+        if (k < n && grp < per_round && !dup && g == 0 && sad < my_best) {
             my_best = sad;
             my_k = k;
         }
@@ -761,7 +786,15 @@ __global__ void __launch_bounds__(ME_THREADS) pel_wavefront_kernel(const __grid_
         short2 bmv = J.best_mv[b];
         float sad;
         if (bl.xl > 0 && bl.yl > 0) {
-            pel_list_best(J.pic, J.ref, J.pw, J.ph, bl, pred, J.radius, wmem, best, bmv, true);
+            // the zero- and guide-centred lists (pel_lists_kernel) came first
+            SeenLists seen{{make_short2(0, 0), make_short2(0, 0)}, 1};
+            if (J.guide) {
+                const int gx = clampi(bx >> 1, 0, J.gxnb - 1), gy = clampi(by >> 1, 0, J.gynb - 1);
+                const short2 gv = J.guide[(size_t)gy * J.gxnb + gx];
+                seen.c[1] = make_short2((short)(gv.x * 2), (short)(gv.y * 2));
+                seen.n = 2;
+            }
+            pel_list_best(J.pic, J.ref, J.pw, J.ph, bl, pred, J.radius, wmem, best, bmv, true, seen);
             sad = (float)best;
         } else {
             bmv = make_short2(0, 0);

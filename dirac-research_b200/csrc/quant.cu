@@ -93,7 +93,8 @@ struct BandTask {  // one band: where its data lives and where its statistics go
     int band;                 // global band index
     int cb_first, xn, yn;     // code blocks of the band
     int chunk_first[2];       // first CTA of the band in each sampling pattern's flattened grid
-    int elem_first;           // first CTA of the band in the element-wise grid (maxima)
+    int elem_first;           // first CTA of the band in the row-chunked grid (maxima)
+    int rows_per_cta;         // rows of the band per CTA of that grid
 };
 
 constexpr int MAX_COMPS = 256;
@@ -122,11 +123,39 @@ __device__ __forceinline__ int cb_of(int pos, int len, int n) {
     return c;
 }
 
-constexpr int MAX_PER_CTA = 256 * 8;  // elements per CTA of the element-wise grids
+constexpr int MAX_PER_CTA = 256 * 8;  // about the elements per CTA of the row-chunked grids
+constexpr int ROW_THREADS = 256;      // eight warps: a warp per row, lanes across the row
 
-// grid: one CTA per MAX_PER_CTA elements of a band, the bands laid end to end
-// (BandTask::elem_first).
-__global__ void band_max_kernel(const BandTask* tasks, int ntasks, int* band_max, int* cb_max) {
+// Rows of a band side of length xl per CTA of the row-chunked grids.
+__host__ __device__ inline int rows_per_cta(int xl) { return max(1, MAX_PER_CTA / max(xl, 1)); }
+
+// A lane's walk along one band row at columns lane, lane + 32, ...: its code block column cx
+// (blocks split the row at (c * xl) / xn, integer division) follows with one comparison per
+// step instead of a division per element.
+struct CbWalk {
+    int cx, bnd, xl, xn;
+    __device__ __forceinline__ CbWalk(int i0, int xl_, int xn_) : xl(xl_), xn(xn_) {
+        cx = cb_of(i0, xl, xn);
+        bnd = ((cx + 1) * xl) / xn;
+    }
+    // moves to column i (non-decreasing); returns whether the block changed
+    __device__ __forceinline__ bool to(int i) {
+        bool moved = false;
+        while (cx + 1 < xn && i >= bnd) {
+            ++cx;
+            bnd = ((cx + 1) * xl) / xn;
+            moved = true;
+        }
+        return moved;
+    }
+};
+
+// grid: row chunks of the bands laid end to end (BandTask::elem_first, rows_per_cta).  Each
+// warp takes rows; a lane keeps the maximum of its current code block and folds it into the
+// CTA's shared copy when it leaves the block; the CTA then folds those into cb_max.
+__global__ void __launch_bounds__(ROW_THREADS) band_max_kernel(const BandTask* tasks, int ntasks, int* band_max,
+                                                               int* cb_max) {
+    __shared__ int s_cb[256];
     int lo_b = 0, hi_b = ntasks - 1;
     while (lo_b < hi_b) {
         const int mid = (lo_b + hi_b + 1) >> 1;
@@ -134,24 +163,44 @@ __global__ void band_max_kernel(const BandTask* tasks, int ntasks, int* band_max
         else hi_b = mid - 1;
     }
     const BandTask T = tasks[lo_b];
-    const int n = T.xl * T.yl;
-    const int base = ((int)blockIdx.x - T.elem_first) * MAX_PER_CTA;
+    const int r0 = ((int)blockIdx.x - T.elem_first) * T.rows_per_cta;
+    const int r1 = min(T.yl, r0 + T.rows_per_cta);
+    const int cy0 = cb_of(r0, T.yl, T.yn), cy1 = cb_of(r1 - 1, T.yl, T.yn);
+    const int ncell = (cy1 - cy0 + 1) * T.xn;
+    const bool local = ncell <= 256;
+    for (int k = threadIdx.x; k < ncell && local; k += blockDim.x) s_cb[k] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int m = 0;
-    for (int k0 = base; k0 < min(n, base + MAX_PER_CTA); k0 += blockDim.x) {
-        const int k = k0 + threadIdx.x;
-        int a = 0, cb = -1;
-        if (k < n) {
-            const int j = k / T.xl, i = k - j * T.xl;
-            a = abs(T.data[(size_t)j * T.stride + i]);
-            cb = T.cb_first + cb_of(j, T.yl, T.yn) * T.xn + cb_of(i, T.xl, T.xn);
+    for (int j = r0 + warp; j < r1; j += ROW_THREADS / 32) {
+        const int cy = cb_of(j, T.yl, T.yn);
+        const int32_t* row = T.data + (size_t)j * T.stride;
+        if (lane >= T.xl) continue;
+        CbWalk w(lane, T.xl, T.xn);
+        int run = 0;
+        for (int i = lane; i < T.xl; i += 32) {
+            const int prev = w.cx;
+            if (w.to(i)) {
+                if (run) {
+                    if (local) atomicMax(&s_cb[(cy - cy0) * T.xn + prev], run);
+                    else atomicMax(&cb_max[T.cb_first + cy * T.xn + prev], run);
+                }
+                run = 0;
+            }
+            const int a = abs(row[i]);
+            run = max(run, a);
+            m = max(m, a);
         }
-        m = max(m, a);
-        const unsigned grp = __match_any_sync(0xffffffffu, cb);
-        const int gm = __reduce_max_sync(grp, (unsigned)a);
-        if (cb >= 0 && gm > 0 && (threadIdx.x & 31) == __ffs(grp) - 1) atomicMax(&cb_max[cb], gm);
+        if (run) {
+            if (local) atomicMax(&s_cb[(cy - cy0) * T.xn + w.cx], run);
+            else atomicMax(&cb_max[T.cb_first + cy * T.xn + w.cx], run);
+        }
     }
     m = __reduce_max_sync(0xffffffffu, (unsigned)m);
-    if ((threadIdx.x & 31) == 0 && m) atomicMax(&band_max[T.band], m);
+    if (lane == 0 && m) atomicMax(&band_max[T.band], m);
+    __syncthreads();
+    for (int k = threadIdx.x; k < ncell && local; k += blockDim.x)
+        if (s_cb[k]) atomicMax(&cb_max[T.cb_first + cy0 * T.xn + k], s_cb[k]);
 }
 
 // ---- 2. statistics ------------------------------------------------------------------------
@@ -362,7 +411,8 @@ struct QBand {
     int xl, yl, xn, yn;
     int qf, off, skip;
     const uint8_t* cb_skip;  // code blocks of this band
-    int first;          // first thread-chunk index
+    int first;          // first CTA of the band in the row-chunked grid
+    int rows;           // rows per CTA
 };
 
 
@@ -373,8 +423,9 @@ __device__ __forceinline__ int cb_index(int pos, int len, int n) {
     return c;
 }
 
-// grid: one CTA per 256 coefficients of a band, the bands (device table) laid end to end.
-__global__ void quantise_kernel(const QBand* bands, int nbands) {
+// grid: row chunks of the bands (device table) laid end to end; a warp per row, lanes
+// across it, the code block followed by CbWalk.  (|v| << 2) / qf through udiv_recip (exact).
+__global__ void __launch_bounds__(ROW_THREADS) quantise_kernel(const QBand* bands, int nbands) {
     int lo_b = 0, hi_b = nbands - 1;
     while (lo_b < hi_b) {
         const int mid = (lo_b + hi_b + 1) >> 1;
@@ -382,28 +433,50 @@ __global__ void quantise_kernel(const QBand* bands, int nbands) {
         else hi_b = mid - 1;
     }
     const QBand B = bands[lo_b];
-    const int k = (blockIdx.x - B.first) * blockDim.x + threadIdx.x;
-    if (k >= B.xl * B.yl) return;
-    const int j = k / B.xl, i = k - j * B.xl;
-    int32_t* v = B.data + (size_t)j * B.stride + i;
-    int r = 0, qi = 0;
-    if (!B.skip && !B.cb_skip[cb_index(j, B.yl, B.yn) * B.xn + cb_index(i, B.xl, B.xn)]) {
-        const int val = *v;
-        const unsigned qv = ((unsigned)abs(val) << 2) / (unsigned)B.qf;
-        if (qv) {
-            r = (int)((qv * (unsigned)B.qf + B.off + 2) >> 2);
-            if (val <= 0) r = -r;
+    const int r0 = ((int)blockIdx.x - B.first) * B.rows;
+    const int r1 = min(B.yl, r0 + B.rows);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const float inv = __frcp_rn((float)B.qf);
+    for (int j = r0 + warp; j < r1; j += ROW_THREADS / 32) {
+        if (lane >= B.xl) break;
+        const uint8_t* skip_row = B.cb_skip + cb_index(j, B.yl, B.yn) * B.xn;
+        int32_t* row = B.data + (size_t)j * B.stride;
+        int32_t* qrow = B.qout ? B.qout + (size_t)j * B.stride : nullptr;
+        CbWalk w(lane, B.xl, B.xn);
+        for (int i = lane; i < B.xl; i += 32) {
+            w.to(i);
+            int r = 0, qi = 0;
+            if (!B.skip && !skip_row[w.cx]) {
+                const int val = row[i];
+                const unsigned qv = udiv_recip((unsigned)abs(val) << 2, (unsigned)B.qf, inv);
+                if (qv) {
+                    r = (int)((qv * (unsigned)B.qf + B.off + 2) >> 2);
+                    if (val <= 0) r = -r;
+                }
+                qi = val < 0 ? -(int)qv : (int)qv;
+            }
+            row[i] = r;
+            if (qrow) qrow[i] = qi;
         }
-        qi = val < 0 ? -(int)qv : (int)qv;
     }
-    *v = r;
-    if (B.qout) B.qout[(size_t)j * B.stride + i] = qi;
 }
 
 // Intra DC band: prediction from reconstructed left / top-left / top neighbours
 // (GetPrediction, band_codec_template.h:531-557), one anti-diagonal per step.
-__global__ void dc_intra_kernel(int32_t* c, int32_t* qout, int stride, int xl, int yl, int xn, int yn, int qf,
-                                int off, const uint8_t* cb_skip) {
+struct DcJob {
+    int32_t* c;
+    int32_t* qout;
+    const uint8_t* cb_skip;
+    int stride, xl, yl, xn, yn, qf, off;
+};
+
+// One CTA per intra component's DC band (a device table of jobs).
+__global__ void dc_intra_kernel(const DcJob* jobs) {
+    const DcJob J = jobs[blockIdx.x];
+    int32_t* const c = J.c;
+    int32_t* const qout = J.qout;
+    const uint8_t* const cb_skip = J.cb_skip;
+    const int stride = J.stride, xl = J.xl, yl = J.yl, xn = J.xn, yn = J.yn, qf = J.qf, off = J.off;
     for (int t = 0; t < xl + yl - 1; ++t) {
         for (int x = threadIdx.x; x < xl; x += blockDim.x) {
             const int y = t - x;
@@ -526,7 +599,8 @@ static size_t residue_ws_need(int nb_total, int ncb_total, size_t dcwork_elems) 
            align_up(sizeof(int2) * nb_total, 256) +
            align_up(sizeof(int) * ncb_total, 256) + align_up(sizeof(Stat) * nb_total * 2 * QMAX, 256) +
            align_up(sizeof(int32_t) * dcwork_elems, 256) + align_up(ncb_total, 256) +
-           align_up(sizeof(Stat) * nb_total * 3, 256) + align_up(sizeof(QBand) * nb_total, 256) + 256;
+           align_up(sizeof(Stat) * nb_total * 3, 256) + align_up(sizeof(QBand) * nb_total, 256) +
+           align_up(sizeof(DcJob) * nb_total, 256) + 256;
 }
 
 extern "C" size_t dgpu_code_residue_workspace_bytes(int n, const int* intra, const int* depth, const int* cw,
@@ -598,6 +672,7 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     uint8_t* d_cbskip = reinterpret_cast<uint8_t*>(take(ncb_total));
     Stat* d_stats3 = reinterpret_cast<Stat*>(take(sizeof(Stat) * nb_total * 3));
     QBand* d_qbands = reinterpret_cast<QBand*>(take(sizeof(QBand) * nb_total));
+    DcJob* d_dcjobs = reinterpret_cast<DcJob*>(take(sizeof(DcJob) * nb_total));
 
     size_t dcoff = 0;
     int chunks[2] = {0, 0}, echunks = 0;
@@ -622,7 +697,8 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
             T.xn = band_ncb[2 * T.band];
             T.yn = band_ncb[2 * T.band + 1];
             T.elem_first = echunks;
-            echunks += (xl * yl + MAX_PER_CTA - 1) / MAX_PER_CTA;
+            T.rows_per_cta = rows_per_cta(xl);
+            echunks += (yl + T.rows_per_cta - 1) / T.rows_per_cta;
             for (int pat = 0; pat < 2; ++pat) {
                 const int xr = pat ? 1 : 2;
                 const long long ns = (long long)((xl + xr - 1) / xr) * ((yl + 1) / 2);
@@ -644,7 +720,7 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
         dc_dpcm_kernel<<<(xl * yl + 255) / 256, 256, 0, st>>>(C.coeff, C.cw, xl, yl, C.dcwork);
         DGPU_CHECK_LAUNCH();
     }
-    band_max_kernel<<<echunks, 256, 0, st>>>(d_tasks, nb_total, d_band_max, d_cb_max);
+    band_max_kernel<<<echunks, ROW_THREADS, 0, st>>>(d_tasks, nb_total, d_band_max, d_cb_max);
     DGPU_CHECK_LAUNCH();
     // ---- 2. statistics and the reference's three-pass Lagrangian choice per band ----
     // Passes 1 and 2 use the 2 x 2 pattern over every even quantiser; pass 3 needs the 1 x 2
@@ -762,17 +838,25 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     });
     std::memcpy(cb_skip, hskip.data(), ncb_total);
     DGPU_CHECK_CUDA(cudaMemcpyAsync(d_cbskip, hskip.data(), ncb_total, cudaMemcpyHostToDevice, st));
-    // ---- 4. quantise and reconstruct, DC bands first ----
-    for (int c = 0; c < n; ++c) {
-        const Comp& C = comps[c];
-        const int t = C.band_first + C.nbands - 1;
-        if (!C.intra || band_skip[t]) continue;
-        const int xl = C.cw >> C.depth, yl = C.ch >> C.depth;
-        const int q = band_qidx[t];
-        const int threads = std::min(1024, ((xl + 31) / 32) * 32);
-        dc_intra_kernel<<<1, threads, 0, st>>>(const_cast<int32_t*>(C.coeff), qout ? qout[c] : nullptr, C.cw, xl, yl, tasks[t].xn,
-                                               tasks[t].yn, qf4(q), intra_off4(q), d_cbskip + tasks[t].cb_first);
-        DGPU_CHECK_LAUNCH();
+    // ---- 4. quantise and reconstruct, DC bands first (every intra component in one launch) ----
+    {
+        std::vector<DcJob> dj;
+        int threads = 32;
+        for (int c = 0; c < n; ++c) {
+            const Comp& C = comps[c];
+            const int t = C.band_first + C.nbands - 1;
+            if (!C.intra || band_skip[t]) continue;
+            const int xl = C.cw >> C.depth, yl = C.ch >> C.depth;
+            const int q = band_qidx[t];
+            threads = std::max(threads, std::min(1024, ((xl + 31) / 32) * 32));
+            dj.push_back(DcJob{const_cast<int32_t*>(C.coeff), qout ? qout[c] : nullptr, d_cbskip + tasks[t].cb_first,
+                               C.cw, xl, yl, tasks[t].xn, tasks[t].yn, qf4(q), intra_off4(q)});
+        }
+        if (!dj.empty()) {
+            DGPU_CHECK_CUDA(cudaMemcpyAsync(d_dcjobs, dj.data(), sizeof(DcJob) * dj.size(), cudaMemcpyHostToDevice, st));
+            dc_intra_kernel<<<(int)dj.size(), threads, 0, st>>>(d_dcjobs);
+            DGPU_CHECK_LAUNCH();
+        }
     }
     // one launch over every band not quantised above, from a device table
     std::vector<QBand> qb;
@@ -797,13 +881,14 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
         B.skip = band_skip[t];
         B.cb_skip = d_cbskip + T.cb_first;
         B.first = qchunks;
-        qchunks += (xl * yl + 255) / 256;
+        B.rows = rows_per_cta(xl);
+        qchunks += (yl + B.rows - 1) / B.rows;
         qb.push_back(B);
     }
     if (qb.empty()) return DGPU_OK;
     // a copy from pageable memory returns once the source has been staged, so qb may go
     DGPU_CHECK_CUDA(cudaMemcpyAsync(d_qbands, qb.data(), sizeof(QBand) * qb.size(), cudaMemcpyHostToDevice, st));
-    quantise_kernel<<<qchunks, 256, 0, st>>>(d_qbands, (int)qb.size());
+    quantise_kernel<<<qchunks, ROW_THREADS, 0, st>>>(d_qbands, (int)qb.size());
     DGPU_CHECK_LAUNCH();
     return DGPU_OK;
 }
