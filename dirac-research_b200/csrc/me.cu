@@ -740,8 +740,9 @@ __global__ void __launch_bounds__(ME_THREADS) pel_lists_kernel(const __grid_cons
         if (J.guide) {
             const int gx = clampi(bx >> 1, 0, J.gxnb - 1), gy = clampi(by >> 1, 0, J.gynb - 1);
             const short2 gv = J.guide[(size_t)gy * J.gxnb + gx];
+            // candidates already in the zero-centred list are not listed again
             pel_list_best(J.pic, J.ref, J.pw, J.ph, bl, make_short2((short)(gv.x * 2), (short)(gv.y * 2)), J.radius,
-                          wmem, best, bmv, true);
+                          wmem, best, bmv, true, SeenLists{{make_short2(0, 0), make_short2(0, 0)}, 1});
         }
     }
     if ((threadIdx.x & 31) == 0) {
@@ -1220,6 +1221,10 @@ __global__ void __launch_bounds__(ME_THREADS) mode_wavefront_kernel(const __grid
     __shared__ float s_sum[2][WARPS_PER_CTA];
     __shared__ float s_mvc[2][WARPS_PER_CTA];
     __shared__ int s_bi[WARPS_PER_CTA];
+    constexpr int MAX_V0 = 8;               // distinct block vectors per reference worth precomputing
+    __shared__ short2 s_v0[2][MAX_V0];      // the superblock's distinct block vectors per reference
+    __shared__ int s_t0[2][MAX_V0];         // their integer totals at superblock size
+    __shared__ int s_n0[2];                 // how many (0: none precomputed)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (;;) {
         __syncthreads();
@@ -1234,6 +1239,37 @@ __global__ void __launch_bounds__(ME_THREADS) mode_wavefront_kernel(const __grid
         // level-1 candidate totals of this warp's sub-superblock while the neighbours finish
         int pre1[8];
         dome_totals(L, J, (xsb << 1) + (warp & 1), (ysb << 1) + (warp >> 1), 1, pre1);
+        // Level-0 candidates are level-1 vectors, each chosen among its sub-superblock's block
+        // vectors: the integer totals at superblock size of the distinct block vectors (when
+        // few) are computed here too, also before the waits.
+        {
+            const LevelData& bk = J.lev[2];
+            if (threadIdx.x == 0) {
+                for (int r = 0; r < 2; ++r) {
+                    int n0 = 0;
+                    for (int t = 0; t < 16 && r < J.nref && n0 <= MAX_V0; ++t) {
+                        const short2 v =
+                            __ldcg(&bk.mv[r][(size_t)((ysb << 2) + (t >> 2)) * bk.xnb + (xsb << 2) + (t & 3)]);
+                        bool dup = false;
+                        for (int q = 0; q < n0 && q < MAX_V0; ++q) dup |= s_v0[r][q].x == v.x && s_v0[r][q].y == v.y;
+                        if (dup) continue;
+                        if (n0 < MAX_V0) s_v0[r][n0] = v;
+                        ++n0;
+                    }
+                    s_n0[r] = r < J.nref && n0 <= MAX_V0 ? n0 : 0;
+                }
+            }
+            __syncthreads();
+            const Blim bl0 = block_limits(L.lb[0], J.pw, J.ph, xsb, ysb);
+            for (int r = 0; r < J.nref; ++r)
+                for (int q = warp; q < s_n0[r]; q += WARPS_PER_CTA) {
+                    const int t = (bl0.xl > 0 && bl0.yl > 0)
+                                      ? subpel_total(J.pic, J.pw, J.up[r], 2 * J.pw, 2 * J.ph, L.prec, bl0,
+                                                     s_v0[r][q].x, s_v0[r][q].y)
+                                      : 0;
+                    if (lane == 0) s_t0[r][q] = t;
+                }
+        }
         if (threadIdx.x == 0) {
             if (xsb > 0) wait_flag(&J.flags[s - 1], L.err);
             if (ysb > 0) {
@@ -1302,8 +1338,17 @@ __global__ void __launch_bounds__(ME_THREADS) mode_wavefront_kernel(const __grid
                 // warp q evaluates candidate q (BlockMatcher::FindBestMatchSubp's loop body)
                 if (warp < nc && bl.xl > 0 && bl.yl > 0) {
                     const float mvcost = (float)getvarup(pr, cand[r][warp].x, cand[r][warp].y);
-                    const float sum = subpel_cost(J.pic, J.pw, J.up[r], 2 * J.pw, 2 * J.ph, L.prec, bl,
-                                                  cand[r][warp].x, cand[r][warp].y, mvcost * lambda);
+                    const float start = mvcost * lambda;
+                    int pre = -1;
+                    for (int q = 0; q < s_n0[r]; ++q)
+                        if (s_v0[r][q].x == cand[r][warp].x && s_v0[r][q].y == cand[r][warp].y) pre = q;
+                    FloatSeq f = float_seq_start(start);
+                    float sum;
+                    if (pre >= 0 && float_seq_add_exact(f, s_t0[r][pre]))
+                        sum = (float)f.c;  // precomputed total, and no addition of the loop could round
+                    else
+                        sum = subpel_cost(J.pic, J.pw, J.up[r], 2 * J.pw, 2 * J.ph, L.prec, bl, cand[r][warp].x,
+                                          cand[r][warp].y, start);
                     if (lane == 0) {
                         s_sum[r][warp] = sum;
                         s_mvc[r][warp] = mvcost;
