@@ -298,12 +298,51 @@ __device__ __forceinline__ int up_pred(const int16_t* up, int uw, int uh, int p,
 // The per-precision bodies are templates; the entry points are kept out of line, so that
 // the wavefront kernels hold one copy of each (their instruction footprint, not their
 // arithmetic, limited them).
+// Whether every sample up_pred reads for the block at vector (mx, my), precision P, lies in
+// the uw x uh plane (then no coordinate needs clamping); and the block's prediction as the
+// offset of its first sample's base position and four bilinear weights.
+template <int P>
+struct UpFast {
+    int ox, oy, w00, w01, w10, w11;
+    bool inside;
+    __device__ __forceinline__ UpFast(const Blim& b, int uw, int uh, int mx, int my) {
+        int span;
+        if (P == 1) {
+            ox = mx;
+            oy = my;
+            w00 = 1;
+            w01 = w10 = w11 = 0;
+            span = 0;
+        } else {
+            constexpr int M = P == 2 ? 1 : 3, SH = P == 2 ? 1 : 2, ONE = M + 1;
+            const int rx = mx & M, ry = my & M;
+            ox = mx >> SH;
+            oy = my >> SH;
+            w00 = (ONE - rx) * (ONE - ry);
+            w01 = rx * (ONE - ry);
+            w10 = (ONE - rx) * ry;
+            w11 = rx * ry;
+            span = 1;
+        }
+        inside = 2 * b.xp + ox >= 0 && 2 * (b.xp + b.xl - 1) + ox + span <= uw - 1 && 2 * b.yp + oy >= 0 &&
+                 2 * (b.yp + b.yl - 1) + oy + span <= uh - 1;
+    }
+    // up_pred at sample (x, y) when inside
+    __device__ __forceinline__ int at(const int16_t* up, int uw, int x, int y) const {
+        const int16_t* q = up + (size_t)(2 * y + oy) * uw + 2 * x + ox;
+        if (P == 1) return q[0];
+        constexpr int RND = P == 2 ? 2 : 8, OUT = P == 2 ? 2 : 4;
+        return (w00 * q[0] + w01 * q[1] + w10 * q[uw] + w11 * q[uw + 1] + RND) >> OUT;
+    }
+};
+
 template <int P>
 __device__ __forceinline__ float subpel_cost_p(const int16_t* pic, int pw, const int16_t* up, int uw, int uh,
                                                const Blim& b, int mx, int my, float start) {
     const int lane = threadIdx.x & 31;
     FloatSeq f = float_seq_start(start);
     const int n = b.xl * b.yl;
+    const UpFast<P> fast(b, uw, uh, mx, my);
     PixWalk w(b.xl);
     for (int k0 = 0; k0 < n; k0 += 256) {
         int d[8];
@@ -313,7 +352,8 @@ __device__ __forceinline__ float subpel_cost_p(const int16_t* pic, int pw, const
             d[s] = 0;
             if (k0 + 32 * s + lane < n) {
                 const int x = b.xp + w.col, y = b.yp + w.row;
-                d[s] = abs(up_pred(up, uw, uh, P, x, y, mx, my) - pic[(size_t)y * pw + x]);
+                const int pr = fast.inside ? fast.at(up, uw, x, y) : up_pred(up, uw, uh, P, x, y, mx, my);
+                d[s] = abs(pr - pic[(size_t)y * pw + x]);
             }
             tot += d[s];
             w.next();
@@ -341,8 +381,22 @@ __device__ __forceinline__ int subpel_total_p(const int16_t* pic, int pw, const 
                                               const Blim& b, int mx, int my) {
     const int lane = threadIdx.x & 31;
     const int n = b.xl * b.yl;
+    const UpFast<P> fast(b, uw, uh, mx, my);
     PixWalk w(b.xl);
     int tot = 0;
+    if (fast.inside) {
+        for (int k0 = 0; k0 < n; k0 += 256) {
+#pragma unroll
+            for (int s = 0; s < 8; ++s) {
+                if (k0 + 32 * s + lane < n) {
+                    const int x = b.xp + w.col, y = b.yp + w.row;
+                    tot += abs(fast.at(up, uw, x, y) - pic[(size_t)y * pw + x]);
+                }
+                w.next();
+            }
+        }
+        return __reduce_add_sync(0xffffffffu, tot);
+    }
     for (int k0 = 0; k0 < n; k0 += 256) {
 #pragma unroll
         for (int s = 0; s < 8; ++s) {
@@ -559,6 +613,21 @@ __device__ __noinline__ int bi_sad_range(const int16_t* pic, int pw, const int16
     const int lane = threadIdx.x & 31;
     PixWalk w(b.xl, kb);
     int s = 0;
+    if (p == 2) {
+        // quarter-pel with both predictions inside their planes: no clamping
+        const UpFast<2> f1(b, uw, uh, mv1.x, mv1.y), f2(b, uw, uh, m2x, m2y);
+        if (f1.inside && f2.inside) {
+#pragma unroll 4
+            for (int k = kb + lane; k < ke; k += 32) {
+                const int x = b.xp + w.col, y = b.yp + w.row;
+                const int16_t dd = (int16_t)((pic[(size_t)y * pw + x] << 1) - f1.at(up1, uw, x, y));
+                const int16_t t = (int16_t)((dd - f2.at(up2, uw, x, y)) >> 1);
+                s += abs((int)t);
+                w.next();
+            }
+            return __reduce_add_sync(0xffffffffu, s);
+        }
+    }
 #pragma unroll 4
     for (int k = kb + lane; k < ke; k += 32) {
         const int x = b.xp + w.col, y = b.yp + w.row;
@@ -1214,7 +1283,7 @@ __global__ void __launch_bounds__(ME_THREADS) mode_blocks_kernel(const __grid_co
 // warps per superblock.  Level 2 sums the precomputed block costs; level 1 gives one
 // sub-superblock to each warp; level 0 spreads its motion-search candidates and the
 // bi-prediction SAD over the warps.  Float sums keep the reference's order.
-__global__ void __launch_bounds__(ME_THREADS) mode_wavefront_kernel(const __grid_constant__ ModeLaunch L) {
+__global__ void __launch_bounds__(ME_THREADS, 5) mode_wavefront_kernel(const __grid_constant__ ModeLaunch L) {
     static_assert(WARPS_PER_CTA == 4, "level 1 has four sub-superblocks");
     __shared__ int s_u;
     __shared__ float s_cost[WARPS_PER_CTA];
