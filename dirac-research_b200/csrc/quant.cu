@@ -293,7 +293,8 @@ __global__ void __launch_bounds__(STAT_THREADS) stats_kernel(const BandTask* tas
             if (e >= EXACT_TERM) {
                 inx = 1;
             } else {
-                const unsigned long long p = e * e * e * e;
+                const unsigned e2 = (unsigned)e * (unsigned)e;  // e < 9741: e^2 < 2^27
+                const unsigned long long p = (unsigned long long)e2 * e2;
                 lo += p;
                 if (lo < p) ++hi;
             }
@@ -389,6 +390,10 @@ __global__ void seq_resolve_kernel(const BandTask* tasks, Stat* stats, int n_ent
         }
     }
 }
+
+// CTAs of 128 threads (four warps, 32 entries per warp per scan step) for n entries, at most
+// four per SM.
+inline int resolve_grid(int n) { return std::max(1, std::min(148 * 4, (n + 127) / 128)); }
 
 // Gathers the third pass's statistics, the three quantisers qrange[band] of each band, into
 // a compact [band][3] array for the host.
@@ -728,7 +733,8 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     // gathered in a second, much smaller launch.
     stats_kernel<<<chunks[0], STAT_THREADS, 0, st>>>(d_tasks, d_band_max, d_stats, 0, nb_total, nullptr);
     DGPU_CHECK_LAUNCH();
-    seq_resolve_kernel<<<148 * 4, 128, 0, st>>>(d_tasks, d_stats, (int)((size_t)nb_total * QMAX), 0, nullptr);
+    seq_resolve_kernel<<<resolve_grid((int)((size_t)nb_total * QMAX)), 128, 0, st>>>(
+        d_tasks, d_stats, (int)((size_t)nb_total * QMAX), 0, nullptr);
     DGPU_CHECK_LAUNCH();
     // statistics and maxima come back through page-locked memory (one buffer per host thread)
     const size_t n_pat = (size_t)nb_total * QMAX;
@@ -808,7 +814,7 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     DGPU_CHECK_LAUNCH();
     gather_stats_kernel<<<(3 * nb_total + 255) / 256, 256, 0, st>>>(d_stats + n_pat, d_range, nb_total, d_stats3);
     DGPU_CHECK_LAUNCH();
-    seq_resolve_kernel<<<148 * 4, 128, 0, st>>>(d_tasks, d_stats3, 3 * nb_total, 1, d_range);
+    seq_resolve_kernel<<<resolve_grid(3 * nb_total), 128, 0, st>>>(d_tasks, d_stats3, 3 * nb_total, 1, d_range);
     DGPU_CHECK_LAUNCH();
     DGPU_CHECK_CUDA(cudaMemcpyAsync(hs3, d_stats3, sizeof(Stat) * 3 * nb_total, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
