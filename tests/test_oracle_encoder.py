@@ -59,3 +59,30 @@ def test_gop_structure_of_the_reconfigured_case():
     assert enc.pics[3].cut and enc.pics[3].refs == [2]
     assert enc.pics[1].refs == [0] and enc.pics[2].refs == [1]
     assert enc.pics[6].refs == [3] and enc.pics[9].refs == [6, 3]
+
+
+@pytest.mark.parametrize("case", [c for c in ENCODE_CASES if c[0] in ("reconfig", "cut_b")], ids=lambda c: c[0])
+def test_code_picture_matches_the_coding_loop(case):
+    """The oracle's single-picture coder (code_picture, which checks the picture batch) gives,
+    for every picture of a sequence, what the coding loop gave it: the same reconstruction
+    and residue results from the picture's original planes, its references' reconstructions
+    and its motion data.  Covers intra, P, B and cut pictures."""
+    from dirac_b200 import quant
+    from oracle_encoder import code_picture
+
+    _, cfg, enc = oracle_encode(case)
+    c = enc.cfg
+    for pn in enc.order:
+        p = enc.pics[pn]
+        pic = dict(cformat=c["cformat"], width=c["width"], height=c["height"], luma_depth=8, chroma_depth=8,
+                   filter=c["intra_filter"] if p.intra else c["inter_filter"], wlt_depth=c["wlt_depth"],
+                   intra=int(p.intra), is_b=int(p.is_b()), qf=c["qf"], cpd=c["cpd"], intra_ratio=p.ratio,
+                   mv_precision=c["mv_precision"], xblen=c["xblen"], yblen=c["yblen"], xbsep=c["xbsep"],
+                   ybsep=c["ybsep"])
+        refs = None if p.intra else [enc.pics[r].data for r in p.refs]
+        data, res = code_picture(pic, p.orig, quant.band_weights, quant.code_blocks, enc.orc, refs=refs,
+                                 me=None if p.intra else p.me)
+        for comp in range(3):
+            np.testing.assert_array_equal(data[comp], p.data[comp], err_msg=f"picture {pn} component {comp}")
+            for k in ("coeff", "qindex", "skip", "bits", "cb_skip"):
+                np.testing.assert_array_equal(res[k][comp], p.result[k][comp], err_msg=f"picture {pn} {k}")
