@@ -388,7 +388,8 @@ int dgpu_encoder_read(void* encoder, int pnum, int what, int comp, void* dst, si
  * synchronises the stream (host Lagrangian, as the reference).  On return the band results
  * are readable with dgpu_batch_read (DGPU_ENC_BANDS / CBSKIP); the reconstruction
  * (DGPU_ENC_RECON), coefficients and quantised indices are complete once the stream reaches
- * the end of the run.  The first call must not be made during a stream capture.
+ * the end of the run.  The first call must not be made during a stream capture.  A batch is
+ * not thread-safe; different batches may run on different threads and streams.
  * ------------------------------------------------------------------------------------- */
 typedef struct {
     int cformat, width, height;   /* ChromaFormat and luma size */
