@@ -567,11 +567,18 @@ def main():
     if args.serving_seconds > 0 and world == 1:
         from dirac_b200 import serving as S
 
-        reqs = S.make_requests(args.serving_seconds, 4.0, ["cif", "576", "720", "1080"], 8, 32, seed=7)
-        serving = S.ServingLoop(int(40e9), max_active=16, frame_interval=1.0 / 50).run(reqs)
-        serving["config"] = {"seconds": args.serving_seconds, "arrivals_per_s": 4.0, "fps_per_stream": 50,
-                             "resolutions": "352x288, 720x576, 1280x720, 1920x1080 (4:2:0 8-bit)",
-                             "frames_per_stream": "8-32", "budget_gb": 40}
+        cfg = {"seconds": args.serving_seconds, "arrivals_per_s": 4.0, "fps_per_stream": 50,
+               "resolutions": "352x288, 720x576, 1280x720, 1920x1080, 3840x2160 (4:2:0, 8- or 10-bit)",
+               "frames_per_stream": "8-64", "budget_gb": 40,
+               "input": "per resolution and depth a pool of synthetic frames (16; 8 at 3840x2160), each stream "
+                        "cycling through its pool from a random offset"}
+        try:
+            reqs = S.make_requests(args.serving_seconds, 4.0, ["cif", "576", "720", "1080", "2160"], 8, 64, seed=7,
+                                   depths=(8, 10))
+            serving = S.ServingLoop(int(40e9), max_active=16, frame_interval=1.0 / 50).run(reqs)
+        except Exception as e:  # the serving leg must not cost the bench line; its failure is reported
+            serving = {"error": repr(e)}
+        serving["config"] = cfg
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,

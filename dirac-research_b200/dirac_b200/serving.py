@@ -167,10 +167,12 @@ def params_for(w, h, depth=8):
                 wlt_depth=4)
 
 
-def make_requests(seconds, rate, resolutions, min_frames, max_frames, seed=0, pool_frames=16):
+def make_requests(seconds, rate, resolutions, min_frames, max_frames, seed=0, pool_frames=16, depths=(8,)):
     """Poisson arrivals at `rate` streams/s over `seconds`; each stream a resolution drawn
-    uniformly from `resolutions`, a length uniform in [min_frames, max_frames], and frames
-    taken (cycled from a per-stream offset) from a seeded synthetic pool per resolution."""
+    uniformly from `resolutions` and a bit depth from `depths`, a length uniform in
+    [min_frames, max_frames], and frames taken (cycled from a per-stream offset) from a seeded
+    synthetic pool per resolution and depth (pool_frames frames; half as many for 3840x2160,
+    whose generation on the host is slow)."""
     import numpy as np
 
     from . import synth
@@ -185,13 +187,17 @@ def make_requests(seconds, rate, resolutions, min_frames, max_frames, seed=0, po
         if t >= seconds:
             break
         res = resolutions[rng.integers(len(resolutions))]
+        depth = int(depths[rng.integers(len(depths))])
         w, h = RESOLUTIONS[res]
-        if res not in pools:
-            pools[res] = synth.make_sequence(w, h, pool_frames, n_rects=8, vmax=8, seed=100 + len(pools))
+        npool = max(2, pool_frames // 2) if w * h > 1920 * 1088 else pool_frames
+        if (res, depth) not in pools:
+            pools[(res, depth)] = synth.make_sequence(w, h, npool, n_rects=8, vmax=8, seed=100 + len(pools),
+                                                      bit_depth=depth)
+        pool = pools[(res, depth)]
         n = int(rng.integers(min_frames, max_frames + 1))
-        off = int(rng.integers(pool_frames))
-        frames = [pools[res][(off + i) % pool_frames] for i in range(n)]
-        reqs.append(Request(params_for(w, h), frames, t, f"s{k}-{res}x{n}"))
+        off = int(rng.integers(npool))
+        frames = [pool[(off + i) % npool] for i in range(n)]
+        reqs.append(Request(params_for(w, h, depth), frames, t, f"s{k}-{res}-{depth}bit-x{n}"))
         k += 1
     return reqs
 
@@ -205,14 +211,16 @@ def main(argv=None):
     ap.add_argument("--fps", type=float, default=50.0, help="frame rate of the live streams (0: all at once)")
     ap.add_argument("--resolutions", default="cif,576,720,1080")
     ap.add_argument("--frames", default="8-64")
+    ap.add_argument("--depths", default="8", help="bit depths drawn per stream, e.g. 8,10")
     ap.add_argument("--seed", type=int, default=0)
     a = ap.parse_args(argv)
     lo, hi = (int(x) for x in a.frames.split("-"))
-    reqs = make_requests(a.seconds, a.rate, a.resolutions.split(","), lo, hi, a.seed)
+    reqs = make_requests(a.seconds, a.rate, a.resolutions.split(","), lo, hi, a.seed,
+                         depths=[int(d) for d in a.depths.split(",")])
     loop = ServingLoop(int(a.budget_gb * 1e9), a.max_active, 1.0 / a.fps if a.fps > 0 else 0.0)
     stats = loop.run(reqs)
     stats["config"] = {"seconds": a.seconds, "rate": a.rate, "resolutions": a.resolutions, "frames": a.frames,
-                       "fps": a.fps, "budget_gb": a.budget_gb}
+                       "depths": a.depths, "fps": a.fps, "budget_gb": a.budget_gb}
     print(json.dumps(stats))
     return 0
 
