@@ -126,8 +126,8 @@ __device__ __forceinline__ int cb_of(int pos, int len, int n) {
 constexpr int MAX_PER_CTA = 256 * 8;  // about the elements per CTA of the row-chunked grids
 constexpr int ROW_THREADS = 256;      // eight warps: a warp per row, lanes across the row
 
-// Rows of a band side of length xl per CTA of the row-chunked grids.
-__host__ __device__ inline int rows_per_cta(int xl) { return max(1, MAX_PER_CTA / max(xl, 1)); }
+// Rows of a band side of length xl per CTA of the row-chunked grids: at least one per warp.
+__host__ __device__ inline int rows_per_cta(int xl) { return max(ROW_THREADS / 32, MAX_PER_CTA / max(xl, 1)); }
 
 // A lane's walk along one band row at columns lane, lane + 32, ...: its code block column cx
 // (blocks split the row at (c * xl) / xn, integer division) follows with one comparison per
