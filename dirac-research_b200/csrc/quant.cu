@@ -249,9 +249,19 @@ __global__ void __launch_bounds__(STAT_THREADS) stats_kernel(const BandTask* tas
     if (base >= nsamp || nq == 0) return;
     __shared__ unsigned long long s_c0[QMAX], s_pn[QMAX], s_lo[QMAX], s_hi[QMAX];
     __shared__ unsigned int s_inx[QMAX];
+    // Pattern 0 tail: a sample quantises to zero for every quantiser from the first whose factor
+    // exceeds 4|v| on, and then adds the same term |v|^4 (count and signs unchanged).  Its term
+    // goes once to the bin of that first even quantiser; a running sum over the bins then gives
+    // every quantiser its tail.
+    __shared__ unsigned long long s_tlo[QMAX], s_thi[QMAX];
+    __shared__ unsigned int s_tinx[QMAX];
+    __shared__ int s_qf[QMAX];
     for (int q = threadIdx.x; q < QMAX; q += STAT_THREADS) {
         s_c0[q] = s_pn[q] = s_lo[q] = s_hi[q] = 0;
         s_inx[q] = 0;
+        s_tlo[q] = s_thi[q] = 0;
+        s_tinx[q] = 0;
+        s_qf[q] = qf4(q);
     }
     __syncthreads();
     int a[8];
@@ -271,7 +281,54 @@ __global__ void __launch_bounds__(STAT_THREADS) stats_kernel(const BandTask* tas
     const int lane = threadIdx.x & 31;
     const int qlo = qrange ? qrange[T.band].x : 0;
     const int qhi = qrange ? min(qrange[T.band].y, nq - 1) : nq - 1;
-    for (int q = qlo; q <= qhi; q += (pattern ? 1 : 2)) {
+    // q0[t]: the first quantiser of the loop whose factor exceeds 4 a (every later one too);
+    // from it on the sample is in the tail (pattern 0 only; pattern 1 has no tail)
+    int q0[8];
+    int qmax_w = qlo;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        q0[t] = qhi + 2;
+        if (a[t] < 0 || pattern) continue;
+        const unsigned a4 = (unsigned)a[t] << 2;
+        int lo_q = 0, hi_q = (qhi >> 1) + 1;  // even quantisers 2 k, k in [lo_q, hi_q)
+        while (lo_q < hi_q) {
+            const int mid = (lo_q + hi_q) >> 1;
+            if ((unsigned)s_qf[2 * mid] > a4) hi_q = mid;
+            else lo_q = mid + 1;
+        }
+        q0[t] = 2 * lo_q;
+        qmax_w = max(qmax_w, q0[t]);
+    }
+    if (!pattern) {
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const int key = (a[t] >= 0 && q0[t] <= qhi) ? q0[t] : -1;
+            const unsigned grp = __match_any_sync(0xffffffffu, key);
+            unsigned long long p = 0;
+            unsigned inx = 0;
+            if (key >= 0) {
+                if ((unsigned)a[t] >= EXACT_TERM) {
+                    inx = 1;
+                } else {
+                    const unsigned e2 = (unsigned)a[t] * (unsigned)a[t];
+                    p = (unsigned long long)e2 * e2;
+                }
+            }
+            // group sums in 27-bit pieces, so that 32-bit reductions cannot overflow
+            const unsigned plo = (unsigned)(p & ((1ull << 27) - 1)), phi = (unsigned)(p >> 27);
+            const unsigned slo = __reduce_add_sync(grp, plo), shi = __reduce_add_sync(grp, phi);
+            const unsigned sinx = __reduce_or_sync(grp, inx);
+            if (key >= 0 && lane == __ffs(grp) - 1) {
+                const unsigned long long v = (unsigned long long)slo + ((unsigned long long)shi << 27);
+                const unsigned long long old = atomicAdd(&s_tlo[key], v);
+                if (old + v < old) atomicAdd(&s_thi[key], 1ull);
+                if (sinx) atomicOr(&s_tinx[key], 1u);
+            }
+        }
+    }
+    // quantisers past every sample's first zero need no per-sample work in this warp
+    const int qend = pattern ? qhi : min(qhi, (int)__reduce_max_sync(0xffffffffu, (unsigned)qmax_w) - 2);
+    for (int q = qlo; q <= qend; q += (pattern ? 1 : 2)) {
         const unsigned qf = (unsigned)qf4(q);
         const float inv = __frcp_rn((float)qf);
         const int off = inter_off4(q);
@@ -279,7 +336,7 @@ __global__ void __launch_bounds__(STAT_THREADS) stats_kernel(const BandTask* tas
         unsigned int pos = 0, ng = 0, inx = 0;
 #pragma unroll
         for (int t = 0; t < 8; ++t) {
-            if (a[t] < 0) continue;
+            if (a[t] < 0 || q >= q0[t]) continue;  // the tail holds q >= q0
             const unsigned qv = udiv_recip((unsigned)a[t] << 2, qf, inv);
             unsigned long long e;
             if (qv == 0) {
@@ -318,6 +375,22 @@ __global__ void __launch_bounds__(STAT_THREADS) stats_kernel(const BandTask* tas
             const unsigned long long old = atomicAdd(&s_lo[q], lo);
             atomicAdd(&s_hi[q], hi + (old + lo < old ? 1 : 0));
             if (inx) atomicOr(&s_inx[q], 1u);
+        }
+    }
+    __syncthreads();
+    if (!pattern && threadIdx.x == 0) {
+        // running sum of the tail bins over the even quantisers
+        unsigned long long rlo = 0, rhi = 0;
+        unsigned rinx = 0;
+        for (int q = qlo; q <= qhi; q += 2) {
+            const unsigned long long nlo = rlo + s_tlo[q];
+            rhi += s_thi[q] + (nlo < rlo ? 1 : 0);
+            rlo = nlo;
+            rinx |= s_tinx[q];
+            const unsigned long long old = s_lo[q];
+            s_lo[q] = old + rlo;
+            s_hi[q] += rhi + (old + rlo < old ? 1 : 0);
+            s_inx[q] |= rinx;
         }
     }
     __syncthreads();
