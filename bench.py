@@ -22,6 +22,9 @@ without groups (each sequence estimating alone), `plain` for one sequence at a t
 the encoder's C ABI from pinned host frames, reading back per picture what the host coder
 needs (quantised indices, band choices, code-block skips, motion data).  Every step works on
 gigabytes of distinct device buffers (far above the 126 MB L2), so no L2 flush is needed.
+`decoding`: the plain form's coded sequence decoded by the device decoder (dequantisation,
+inverse transform, motion compensation, clip, output samples), its output checked against the
+encoder's local decode.
 Under torchrun each rank encodes its own sequence (replicas, weak scaling, no collective on
 the data path); times are device times, max over ranks.  `--impl reference` times the
 reference encoder itself (its public C API) on this host's cores.
@@ -59,6 +62,8 @@ def parse_args():
     ap.add_argument("--hetero-steps", type=int, default=5,
                     help="timed runs of the heterogeneous 64-picture batch reported under 'heterogeneous_batch' "
                          "(0: skip)")
+    ap.add_argument("--decode", type=int, default=1,
+                    help="1: report the device decoder on the plain form's coded sequence under 'decoding'")
     ap.add_argument("--impl", choices=["gpu", "reference"], default="gpu")
     return ap.parse_args()
 
@@ -310,6 +315,144 @@ def run_hetero(args, peak, peaks):
     return out
 
 
+def run_decoding(args, enc, infos, peak):
+    """The decoding leg: the 1080p sequence the plain form coded, decoded by the device decoder
+    (dgpu_decoder_*) from its quantised indices, band and code-block choices and motion data, in
+    coding order; every picture's output samples checked against the encoder's locally decoded
+    ones.  Device-resident inputs for `value`; page-locked host inputs and output samples read
+    back to page-locked host memory for `e2e`.  The oracle's restatement of the decoder timed on
+    one host core is the CPU baseline."""
+    import numpy as np
+    import torch
+
+    from dirac_b200 import decoder as D
+    from dirac_b200 import encoder as E
+    from dirac_b200.roofline import decode_bytes
+
+    st = torch.cuda.current_stream()
+    dec = D.SequenceDecoder(D.decoder_params(PARAMS), max_pictures=len(infos), stream=st)
+    lib = dec.lib
+    m = 1 << PARAMS["wlt_depth"]
+    sizes = [(PARAMS["height"], PARAMS["width"]), (PARAMS["height"] // 2, PARAMS["width"] // 2)]
+    shapes = [tuple((x + m - 1) // m * m for x in sizes[min(c, 1)]) for c in range(3)]
+    dev, host, want, pnums = [], [], [], []
+    keep = []
+    h2d = 0
+    for info in infos:
+        pn = info["pnum"]
+        pnums.append(pn)
+        q = [enc.read(pn, E.QINDEX, c).reshape(shapes[c]) for c in range(3)]
+        bands = [enc.read(pn, E.BANDS, c) for c in range(3)]
+        cbs = np.concatenate([enc.read(pn, E.CBSKIP, c) for c in range(3)])
+        refs = [] if info["intra"] else [x for x in (info["ref1"], info["ref2"]) if x >= 0]
+        mot = None
+        if not info["intra"]:
+            mv = enc.read(pn, E.MV).reshape(info["num_refs"], -1, 2)
+            mot = {"mv": [mv[k] for k in range(len(refs))], "mode": enc.read(pn, E.MODE), "dc": enc.read(pn, E.DC),
+                   "split": enc.read(pn, E.SPLIT)}
+        want.append([enc.read(pn, E.OUTPUT, c) for c in range(3)])
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+        hq, hc = [pin(a) for a in q], pin(cbs)
+        hm = None if mot is None else {"mv": [pin(v) for v in mot["mv"]],
+                                       **{k: pin(mot[k]) for k in ("mode", "dc", "split")}}
+        keep += [hq, hc, hm]
+        h2d += sum(t.numel() * t.element_size() for t in hq) + hc.numel()
+        if hm is not None:
+            h2d += sum(t.numel() * t.element_size() for t in hm["mv"]) + sum(
+                hm[k].numel() * hm[k].element_size() for k in ("mode", "dc", "split"))
+        np_m = None if hm is None else {"mv": [t.numpy() for t in hm["mv"]],
+                                        **{k: hm[k].numpy() for k in ("mode", "dc", "split")}}
+        host.append(dec.prepare(pn, info["intra"], refs, info["filter"], [t.numpy() for t in hq], bands,
+                                hc.numpy(), np_m))
+        dm = None if hm is None else {"mv": [t.cuda() for t in hm["mv"]],
+                                      **{k: hm[k].cuda() for k in ("mode", "dc", "split")}}
+        dev.append(dec.prepare(pn, info["intra"], refs, info["filter"], [t.cuda() for t in hq], bands, hc.cuda(),
+                               dm))
+    n_out = [a.size for a in want[0]]
+    out_dev = [torch.empty(n, dtype=torch.uint8, device="cuda") for n in n_out]
+    out_host = [[torch.empty(n, dtype=torch.uint8, pin_memory=True) for n in n_out] for _ in infos]
+    d2h = sum(n_out) * len(infos)
+
+    def step(inputs, read=False):
+        for k, I in enumerate(inputs):
+            dec.decode_prepared(I)
+            if read:
+                for c in range(3):
+                    rc = lib.dgpu_decoder_read(dec.handle, pnums[k], E.OUTPUT, c, out_dev[c].data_ptr(), n_out[c], 0)
+                    if rc:
+                        raise RuntimeError(f"dgpu_decoder_read: {rc}")
+                    out_host[k][c].copy_(out_dev[c], non_blocking=True)
+        for pn in pnums:
+            dec.release(pn)
+
+    def timed(inputs, steps, read=False):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            step(inputs, read)
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    for _ in range(max(3, args.warmup)):
+        step(dev)
+    step(host, read=True)
+    launches0 = lib.dgpu_launch_count()
+    ms = timed(dev, args.steps)
+    launches = (lib.dgpu_launch_count() - launches0) // args.steps
+    ems = timed(host, args.steps, read=True)
+    matches = all(np.array_equal(out_host[k][c].numpy(), want[k][c]) for k in range(len(infos)) for c in range(3))
+    alg = decode_bytes(PARAMS, infos)
+    total_alg = sum(alg.values())
+    achieved = total_alg * args.steps / (ms / 1000.0) / 1e9
+    dec.close()
+    del keep
+
+    # CPU baseline: the oracle's restatement of the decoder on the first pictures in coding order
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from dirac_b200 import quant
+    from oracle_decoder import decode_picture
+
+    ncb = quant.code_blocks(PARAMS["wlt_depth"], PARAMS["width"], PARAMS["height"])
+    cfg = dict(PARAMS)
+    done, t_cpu = {}, 0.0
+    for k, info in enumerate(infos):
+        pn = info["pnum"]
+        qn = [enc.read(pn, E.QINDEX, c).reshape(shapes[c]) for c in range(3)]
+        b = [np.asarray(x).reshape(-1, 3) for x in [enc.read(pn, E.BANDS, c) for c in range(3)]]
+        cb = [enc.read(pn, E.CBSKIP, c) for c in range(3)]
+        pic = {"intra": info["intra"], "filter": info["filter"], "qindex": qn, "qidx": [x[:, 0] for x in b],
+               "skip": [x[:, 1] for x in b], "cb_skip": cb}
+        refs = None
+        if not info["intra"]:
+            mv = enc.read(pn, E.MV).reshape(info["num_refs"], -1, 2)
+            pic["me"] = {"mv": [mv[j] for j in range(info["num_refs"])], "mode": enc.read(pn, E.MODE),
+                         "dc": enc.read(pn, E.DC), "split": enc.read(pn, E.SPLIT)}
+            refs = [done[x] for x in (info["ref1"], info["ref2"]) if x >= 0]
+        t0 = time.perf_counter()
+        done[pn] = decode_picture(cfg, pic, refs, ncb)
+        t_cpu += time.perf_counter() - t0
+        if t_cpu > 10.0 or k + 1 >= 8:
+            break
+    ncpu = len(done)
+    return {"value": len(infos) * args.steps / (ms / 1000.0), "unit": "frames/s", "frames_per_step": len(infos),
+            "ms_per_step": ms / args.steps, "steps": args.steps,
+            "e2e": {"value": len(infos) * args.steps / (ems / 1000.0), "unit": "frames/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "output_matches_encoder": bool(matches), "gpu_launches_per_step": launches,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4),
+                         "algorithmic_bytes_per_step": alg},
+            "cpu_baseline": {"value": ncpu / t_cpu, "unit": "frames/s", "cores": 1, "kind": "port",
+                             "sample": f"the oracle's plain-C restatement of the decoder (dequantisation, inverse "
+                                       f"transform, motion compensation, clip) on the first {ncpu} pictures in "
+                                       f"coding order: {t_cpu:.2f} s on 1 core"},
+            "workload": "decode of the plain form's coded 1920x1080 4:2:0 8-bit 32-picture sequence from its "
+                        "quantised indices (int32), band and code-block choices and motion data; output 8-bit "
+                        "samples"}
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -550,6 +693,10 @@ def main():
                 "algorithmic_bytes_per_step": alg, "stages": per_stage,
                 "note": "plain form, one sequence; stage times from CUDA events on the encoder stream in a "
                         "separate profiled pass"}
+    # ---- decoding: the plain form's coded sequence through the device decoder ----------------
+    decoding = None
+    if args.decode and world == 1:
+        decoding = run_decoding(args, enc, infos, peak)
     for g, _ in groups:
         g.close()
     for ln in lanes:
@@ -591,7 +738,7 @@ def main():
                                    "each sequence's coding on its own stream and host thread",
                            "l2": "inputs and working set larger than L2 (no flush needed)"},
                 "plain": plain_line, "batched_one_group": one_group, "batched_streams_only": streams_only, "roofline": roofline, "cpu_baseline": cpu_baseline, "e2e": e2e,
-                "latency_ms": latency, "heterogeneous_batch": hetero, "serving": serving,
+                "latency_ms": latency, "heterogeneous_batch": hetero, "serving": serving, "decoding": decoding,
                 "gpu_launches": launches, "clocks": clk}
         print(json.dumps(line), flush=True)
     if world > 1:

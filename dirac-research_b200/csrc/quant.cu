@@ -593,6 +593,109 @@ __global__ void dc_intra_kernel(const DcJob* jobs) {
     }
 }
 
+// ---- 5. dequantisation (the decoder's side) -------------------------------------------------
+//
+// After entropy decoding, the band decoders turn each magnitude q into
+// (q * qf4 + offset + 2) >> 2 with the coded sign (GenericBandCodec::DecodeVal,
+// band_codec_template.h:330-356), zero a skipped code block (ClearBlock, :488-496) or a
+// skipped band (CompDecompressor::SetToVal, comp_decompress.cpp:121-125, 154-163), and in an
+// intra picture add to the DC band's values the prediction from their reconstructed
+// neighbours (GenericIntraDCBandCodec::DecodeCoeffBlock / ClearBlock / GetPrediction,
+// band_codec_template.h:500-557).  The band table travels as a kernel parameter, so a call
+// needs no device table and no host synchronisation.
+
+constexpr int DQ_MAX_BANDS = 64;
+
+struct DqBand {
+    const int32_t* q;   // band top-left in the index array
+    int32_t* c;         // band top-left in the coefficient array
+    const uint8_t* cb;  // the band's code-block skip flags (device)
+    int stride, xl, yl, xn, yn;
+    int qf, off;        // QuantFactor4 and the intra / inter offset of the band's quantiser
+    int skip;           // whole band zero
+    int dc;             // intra DC band: decoded by dc_decode_kernel
+    int first, rows;    // first CTA and rows per CTA in the row-chunked grid
+};
+
+struct DqArgs {
+    DqBand band[DQ_MAX_BANDS];
+    int nbands;
+    int dc_band[DQ_MAX_BANDS];  // bands decoded by dc_decode_kernel, one CTA each
+};
+
+// The decoded value of a signed index: int32 arithmetic as DecodeVal's (CoeffType).
+__device__ __forceinline__ int dequant_value(int qi, int qf, int off) {
+    if (qi == 0) return 0;
+    const unsigned mag = qi < 0 ? 0u - (unsigned)qi : (unsigned)qi;
+    const int v = (int)(mag * (unsigned)qf + (unsigned)(off + 2)) >> 2;
+    return qi < 0 ? -v : v;
+}
+
+// grid: row chunks of the bands laid end to end, a warp per row, lanes across it, the code
+// block followed by CbWalk.  Intra DC bands are left to dc_decode_kernel.
+__global__ void __launch_bounds__(ROW_THREADS) dequantise_kernel(const __grid_constant__ DqArgs A) {
+    int lo_b = 0, hi_b = A.nbands - 1;
+    while (lo_b < hi_b) {
+        const int mid = (lo_b + hi_b + 1) >> 1;
+        if (A.band[mid].first <= (int)blockIdx.x) lo_b = mid;
+        else hi_b = mid - 1;
+    }
+    const DqBand& B = A.band[lo_b];
+    if (B.dc) return;
+    const int r0 = ((int)blockIdx.x - B.first) * B.rows;
+    const int r1 = min(B.yl, r0 + B.rows);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int j = r0 + warp; j < r1; j += ROW_THREADS / 32) {
+        if (lane >= B.xl) break;
+        const int32_t* qrow = B.q + (size_t)j * B.stride;  // may alias row (in place)
+        int32_t* row = B.c + (size_t)j * B.stride;
+        if (B.skip) {
+            for (int i = lane; i < B.xl; i += 32) row[i] = 0;
+            continue;
+        }
+        const uint8_t* skip_row = B.cb + cb_of(j, B.yl, B.yn) * B.xn;
+        CbWalk w(lane, B.xl, B.xn);
+        for (int i = lane; i < B.xl; i += 32) {
+            w.to(i);
+            row[i] = skip_row[w.cx] ? 0 : dequant_value(qrow[i], B.qf, B.off);
+        }
+    }
+}
+
+// Intra DC bands, one CTA each: value = decoded residue + prediction from the reconstructed
+// left / top-left / top neighbours (int32, as the decoder's GetPrediction computes it); a
+// skipped code block takes the prediction alone.  Positions on one anti-diagonal depend only
+// on earlier diagonals, so the diagonals run in order and each one in parallel; that equals
+// the reference's code block by code block raster order.
+__global__ void dc_decode_kernel(const __grid_constant__ DqArgs A) {
+    const DqBand& B = A.band[A.dc_band[blockIdx.x]];
+    const int32_t* const q = B.q;
+    int32_t* const c = B.c;
+    const int stride = B.stride, xl = B.xl, yl = B.yl;
+    for (int t = 0; t < xl + yl - 1; ++t) {
+        for (int x = threadIdx.x; x < xl; x += blockDim.x) {
+            const int y = t - x;
+            if (y < 0 || y >= yl) continue;
+            int pred;
+            if (y != 0) {
+                if (x != 0) {
+                    const int sum = c[(size_t)y * stride + x - 1] + c[(size_t)(y - 1) * stride + x - 1] +
+                                    c[(size_t)(y - 1) * stride + x] + 3 / 2;
+                    pred = sum < 0 ? (sum - 2) / 3 : sum / 3;
+                } else {
+                    pred = c[(size_t)(y - 1) * stride];
+                }
+            } else {
+                pred = x != 0 ? c[x - 1] : 0;
+            }
+            const size_t at = (size_t)y * stride + x;
+            const bool skip = B.cb[cb_of(y, yl, B.yn) * B.xn + cb_of(x, xl, B.xn)];
+            c[at] = skip ? pred : dequant_value(q[at], B.qf, B.off) + pred;
+        }
+        __syncthreads();
+    }
+}
+
 // ---- host: the reference's Lagrangian choice (quant_chooser.cpp:62-147, 266-318) -------------
 
 struct HostStat {
@@ -970,6 +1073,90 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     quantise_kernel<<<qchunks, ROW_THREADS, 0, st>>>(d_qbands, (int)qb.size());
     DGPU_CHECK_LAUNCH();
     return DGPU_OK;
+}
+
+namespace {
+
+// Launches the dequantisation of the bands collected in A (row-chunked grid, then the intra
+// DC wavefronts) and empties A.
+int launch_dequantise(DqArgs& A, int ndc, int chunks, cudaStream_t st) {
+    if (A.nbands == 0) return DGPU_OK;
+    if (chunks > 0) {
+        dequantise_kernel<<<chunks, ROW_THREADS, 0, st>>>(A);
+        DGPU_CHECK_LAUNCH();
+    }
+    if (ndc > 0) {
+        dc_decode_kernel<<<ndc, 256, 0, st>>>(A);
+        DGPU_CHECK_LAUNCH();
+    }
+    A.nbands = 0;
+    return DGPU_OK;
+}
+
+}  // namespace
+
+extern "C" int dgpu_dequantise_batch(int n, const int* intra, const int* depth, const int32_t* const* qindex,
+                                     int32_t* const* coeff, const int* cw, const int* ch, const int* band_ncb,
+                                     const int* band_qidx, const int* band_skip, const uint8_t* cb_skip,
+                                     void* stream) {
+    if (n <= 0 || n > MAX_COMPS || !intra || !depth || !qindex || !coeff || !cw || !ch || !band_ncb || !band_qidx ||
+        !band_skip || !cb_skip)
+        return DGPU_ERR_ARG;
+    // validate everything before the first launch
+    for (int c = 0, b0 = 0; c < n; ++c) {
+        const int d = depth[c];
+        if (d < 1 || d > 8 || !qindex[c] || !coeff[c] || cw[c] <= 0 || ch[c] <= 0 || (cw[c] % (1 << d)) != 0 ||
+            (ch[c] % (1 << d)) != 0)
+            return DGPU_ERR_ARG;
+        for (int b = 0; b < 3 * d + 1; ++b) {
+            const int g = b0 + b;
+            if (band_ncb[2 * g] < 1 || band_ncb[2 * g + 1] < 1) return DGPU_ERR_ARG;
+            // an index the decoder would refuse (band_codec_template.h:250-258)
+            if (!band_skip[g] && (band_qidx[g] < 0 || band_qidx[g] > 119)) return DGPU_ERR_ARG;
+        }
+        b0 += 3 * d + 1;
+    }
+    cudaStream_t st = as_stream(stream);
+    DqArgs A;
+    A.nbands = 0;
+    int chunks = 0, ndc = 0;
+    size_t cb_off = 0;
+    for (int c = 0, b0 = 0; c < n; ++c) {
+        const int d = depth[c], nb = 3 * d + 1;
+        if (A.nbands + nb > DQ_MAX_BANDS) {
+            const int rc = launch_dequantise(A, ndc, chunks, st);
+            if (rc) return rc;
+            chunks = ndc = 0;
+        }
+        for (int b = 1; b <= nb; ++b) {
+            const int g = b0 + b - 1;
+            int xp, yp, xl, yl;
+            band_rect(d, cw[c], ch[c], b, xp, yp, xl, yl);
+            DqBand& B = A.band[A.nbands];
+            const size_t at = (size_t)yp * cw[c] + xp;
+            B.q = qindex[c] + at;
+            B.c = coeff[c] + at;
+            B.cb = cb_skip + cb_off;
+            B.stride = cw[c];
+            B.xl = xl;
+            B.yl = yl;
+            B.xn = band_ncb[2 * g];
+            B.yn = band_ncb[2 * g + 1];
+            B.skip = band_skip[g] ? 1 : 0;
+            const int q = B.skip ? 0 : band_qidx[g];
+            B.qf = qf4(q);
+            B.off = intra[c] ? intra_off4(q) : inter_off4(q);
+            B.dc = (intra[c] && b == nb && !B.skip) ? 1 : 0;
+            B.rows = rows_per_cta(xl);
+            B.first = chunks;
+            chunks += (yl + B.rows - 1) / B.rows;
+            if (B.dc) A.dc_band[ndc++] = A.nbands;
+            cb_off += (size_t)B.xn * B.yn;
+            ++A.nbands;
+        }
+        b0 += nb;
+    }
+    return launch_dequantise(A, ndc, chunks, st);
 }
 
 // CoeffArray::SetBandWeights (libdirac_common/wavelet_utils.cpp:192-382) with

@@ -66,3 +66,22 @@ def stage_bytes(params, infos):
                     refs_used.add(r)
     out["upconvert"] = len(refs_used) * samples * 10
     return out
+
+
+def decode_bytes(params, infos):
+    """Algorithmic bytes per stage of the device decoder for the pictures described by infos
+    (coded pictures in coding order): dequantisation 8 B per coefficient (index read,
+    coefficient write), the inverse transform, motion compensation ADD with the clip (or the
+    clip alone for intra pictures) and the upconversion of every reference picture, as above."""
+    enc = stage_bytes(params, infos)
+    w, h = params["width"], params["height"]
+    cf = params["cformat"]
+    xs = 0 if cf == 0 else 1
+    ys = 1 if cf == 2 else 0
+    mul = 1 << params["wlt_depth"]
+    comps = [(w, h), (w >> xs, h >> ys), (w >> xs, h >> ys)]
+    coeffs = sum((a + mul - 1) // mul * mul * ((b + mul - 1) // mul * mul) for a, b in comps)
+    samples = sum(a * b for a, b in comps)
+    refs = {r for i in infos if not i["intra"] for r in (i["ref1"], i["ref2"]) if r >= 0}
+    return {"dequantisation": 8 * coeffs * len(infos), "dwt_inverse": enc["dwt_inverse"],
+            "mc_add_clip": enc["mc_add_clip"], "upconvert": len(refs) * samples * 10}

@@ -265,6 +265,28 @@ int dgpu_code_residue_batch(int n, const int* intra, const int* depth, int32_t* 
                             size_t ws_bytes, void* stream);
 
 /* ---------------------------------------------------------------------------------------
+ * Dequantisation of entropy-decoded components (the decoder's side of the residue coding).
+ * Replaces the arithmetic the band decoders apply after decoding each magnitude and sign:
+ * GenericBandCodec::DecodeVal with the band's quantiser (band_codec_template.h:231-270,
+ * 330-356), ClearBlock for skipped code blocks (:488-496), the intra DC band's prediction
+ * from reconstructed neighbours (GenericIntraDCBandCodec, :500-557) and
+ * CompDecompressor::SetToVal for skipped bands (libdirac_decoder/comp_decompress.cpp:64-163).
+ * A host binding makes DecodeVal store the signed index instead of the dequantised value.
+ *
+ * n components.  qindex[c] (device, dense cw[c] x ch[c] int32, Mallat layout): signed
+ * quantised indices, the intra DC band holding its prediction residues' indices (the layout
+ * dgpu_code_residue_batch writes to qout); coeff[c] (device, same layout) receives the
+ * coefficients and may equal qindex[c] (in place).  Per band, components concatenated in
+ * band-list order as for dgpu_code_residue_batch: band_ncb, band_qidx, band_skip (host);
+ * cb_skip (DEVICE): the code-block skip flags of every band in that order.  Asynchronous on
+ * the stream, no workspace, no synchronisation.  DGPU_ERR_ARG (nothing launched) when a
+ * coded band's quantiser index is outside 0..119, as the reference decoder refuses it.
+ * ------------------------------------------------------------------------------------- */
+int dgpu_dequantise_batch(int n, const int* intra, const int* depth, const int32_t* const* qindex,
+                          int32_t* const* coeff, const int* cw, const int* ch, const int* band_ncb,
+                          const int* band_qidx, const int* band_skip, const uint8_t* cb_skip, void* stream);
+
+/* ---------------------------------------------------------------------------------------
  * Sequence encoder: the data-parallel part of the reference's frame-coding loop
  * SequenceCompressor::CompressNextPicture (libdirac_encoder/seq_compress.cpp:194-499) with
  * FrameSequenceCompressor's GOP structure (seq_compress.cpp:151-192, 563-686) and the
@@ -451,6 +473,71 @@ size_t dgpu_encoder_group_device_bytes(void* const* encoders, int n);
 int dgpu_encoder_group_create(void* const* encoders, int n, void** group);
 int dgpu_encoder_group_destroy(void* group);
 int dgpu_encoder_group_estimate(void* group, int* ntasks);
+
+/* ---------------------------------------------------------------------------------------
+ * Sequence decoder: the data-parallel part of PictureDecompressor::Decompress
+ * (libdirac_decoder/picture_decompress.cpp:73-212) and of the frame output of dirac_parse
+ * (set_frame_component, libdirac_decoder/dirac_parser.cpp:159-226): dequantisation (as
+ * dgpu_dequantise_batch), the inverse transform of the three components, motion
+ * compensation ADD against the upconverted reference pictures (Picture::UpData, made once
+ * per reference) with the clip, or the clip alone for intra pictures, and the conversion to
+ * unsigned output samples.  What stays with the caller (serial host code in the reference):
+ * parsing, the entropy decoding of coefficients (to signed quantised indices) and of motion
+ * data, and the picture buffer's policy (dgpu_decoder_release drops a picture).
+ *
+ * Per picture (dgpu_decode_input): its number, intra flag, references, transform filter,
+ * the zero-residual flag (no coefficients coded: the residue is zero), per band the
+ * quantiser indices and skip flags (host, components concatenated), and, in host memory
+ * (on_host = 1) or device memory (on_host = 0): the signed quantised indices of the three
+ * components (int32 [ch][cw] padded to the transform depth: the layout of DGPU_ENC_QINDEX),
+ * the code-block skip flags (per component in band-list order as DGPU_ENC_CBSKIP, components
+ * concatenated) and, for inter pictures, the motion data in the layout of
+ * dgpu_motion_compensate.  Transform depth, code blocks and block parameters are fixed per
+ * decoder (as the reference encoder keeps them), the filter is per picture.  Host inputs are
+ * copied on the decoder's stream: page-locked ones must stay unchanged until the stream has
+ * passed the call, pageable ones may be reused on return.
+ *
+ * dgpu_decoder_decode returns DGPU_ERR_ARG for invalid arguments and for a reference that is
+ * not in the buffer (the reference decoder does not decode such a picture,
+ * picture_decompress.cpp:107-113), DGPU_ERR_SIZE when every picture slot is taken.  Results
+ * are read with dgpu_decoder_read (DGPU_ENC_RECON, DGPU_ENC_COEFF, DGPU_ENC_OUTPUT), which
+ * synchronises the stream for host copies.  A handle is not thread-safe; different handles
+ * may run on different streams concurrently.
+ * ------------------------------------------------------------------------------------- */
+typedef struct {
+    int cformat, width, height;   /* ChromaFormat and luma size */
+    int luma_depth, chroma_depth; /* bits per sample, 8..14 */
+    int wlt_depth;                /* transform depth */
+    int spatial_partition;        /* 1: SetUsualCodeBlocks' code blocks (dgpu_code_blocks), 0: one per band */
+    dgpu_block_params bp;         /* block parameters of the inter pictures */
+} dgpu_decoder_params;
+
+typedef struct {
+    int pnum;                     /* picture number */
+    int intra;                    /* 1: intra picture (no motion data) */
+    int num_refs, ref1, ref2;     /* inter: references (picture numbers) */
+    int filter;                   /* WltFilter of the picture's transform */
+    int zero_residual;            /* 1: no coefficients coded */
+    const int* band_qidx;         /* host, [3][3*depth+1] quantiser indices */
+    const int* band_skip;         /* host, [3][3*depth+1] band skip flags */
+    int on_host;                  /* 1: the arrays below are in host memory */
+    const int32_t* qindex[3];
+    const uint8_t* cb_skip;
+    const int16_t* mv1;
+    const int16_t* mv2;           /* NULL with one reference */
+    const uint8_t* mode;
+    const int16_t* dc;
+    const uint8_t* split;
+} dgpu_decode_input;
+
+size_t dgpu_decoder_device_bytes(const dgpu_decoder_params* params, int max_pictures);
+int dgpu_decoder_create(const dgpu_decoder_params* params, int max_pictures, void* stream, void** decoder);
+int dgpu_decoder_destroy(void* decoder);
+int dgpu_decoder_decode(void* decoder, const dgpu_decode_input* in);
+/* Drops a picture from the buffer (PictureBuffer::Remove); its slot is reused by a later decode. */
+int dgpu_decoder_release(void* decoder, int pnum);
+size_t dgpu_decoder_item_bytes(void* decoder, int pnum, int what, int comp);
+int dgpu_decoder_read(void* decoder, int pnum, int what, int comp, void* dst, size_t bytes, int on_host);
 
 #ifdef __cplusplus
 }

@@ -97,6 +97,13 @@ int orc_code_residue(int intra, int depth, int32_t* c, int cw, int ch, float lam
                      const float* band_ecf, const int* band_ncb, int* band_qidx, int* band_skip, int* band_bits,
                      uint8_t* cb_skip, int32_t* qout);
 
+/* The decoder's dequantisation of one component from its signed quantised indices (the intra
+ * DC band holding its prediction residues' indices), band quantisers and skip flags, and
+ * code-block skip flags (layouts as orc_code_residue writes them); coeff may equal qindex.
+ * Returns -1 for a coded band's quantiser index outside 0..119. */
+int orc_dequantise(int intra, int depth, const int32_t* qindex, int32_t* coeff, int cw, int ch,
+                   const int* band_ncb, const int* band_qidx, const int* band_skip, const uint8_t* cb_skip);
+
 /* Picture::ClipComponent: clamp to [-2^(d-1), 2^(d-1)-1]. */
 void orc_clip(int16_t* pic, size_t n, int bit_depth);
 

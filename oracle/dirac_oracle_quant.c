@@ -291,3 +291,69 @@ int orc_code_residue(int intra, int depth, int32_t* c, int cw, int ch, float lam
     free(cb_first);
     return 0;
 }
+
+/* Dequantisation of one entropy-decoded component, in the reference decoder's order:
+ * CompDecompressor::Decompress walks the bands from the DC band down to band 1
+ * (libdirac_decoder/comp_decompress.cpp:64-127) and zeroes a skipped band (SetToVal,
+ * :121-125, 154-163); a band decoder walks its code blocks in raster order
+ * (GenericBandCodec::DoWorkDecode, band_codec_template.h:204-228), decodes each value as
+ * (q * qf4 + offset + 2) >> 2 with its sign (DecodeVal, :330-356; quantiser and offset from
+ * DecodeCoeffBlock, :231-270) and zeroes a skipped code block (ClearBlock, :488-496).  The
+ * intra DC band first decodes a code block's residues, then adds, in raster order, the
+ * prediction from the reconstructed neighbours; a skipped code block takes the prediction
+ * alone (GenericIntraDCBandCodec::DecodeCoeffBlock / ClearBlock / GetPrediction, :500-557;
+ * int32 arithmetic, CoeffType).  Code block (i, j) of a band covers columns
+ * [i * xl / xn, (i + 1) * xl / xn) (Subband::SetNumBlocks, wavelet_utils.cpp:116-140).
+ * qindex and coeff are cw x ch, dense; they may be the same array. */
+static int decode_val(int q, int qf, int off) {
+    if (q == 0) return 0;
+    const int mag = q < 0 ? -q : q;
+    const int v = (int)((unsigned)mag * (unsigned)qf + (unsigned)(off + 2)) >> 2;
+    return q < 0 ? -v : v;
+}
+
+int orc_dequantise(int intra, int depth, const int32_t* qindex, int32_t* coeff, int cw, int ch,
+                   const int* band_ncb, const int* band_qidx, const int* band_skip, const uint8_t* cb_skip) {
+    const int nb = 3 * depth + 1;
+    int* cb_first = (int*)malloc(sizeof(int) * (nb + 1));
+    if (!cb_first) return -4;
+    cb_first[0] = 0;
+    for (int b = 0; b < nb; ++b) cb_first[b + 1] = cb_first[b] + band_ncb[2 * b] * band_ncb[2 * b + 1];
+    for (int b = nb; b >= 1; --b) {
+        int xp, yp, xl, yl;
+        orc_band_rect(depth, cw, ch, b, &xp, &yp, &xl, &yl);
+        if (band_skip[b - 1]) {
+            for (int j = yp; j < yp + yl; ++j)
+                for (int i = xp; i < xp + xl; ++i) coeff[(size_t)j * cw + i] = 0;
+            continue;
+        }
+        const int q = band_qidx[b - 1];
+        if (q < 0 || q > 119) {
+            free(cb_first);
+            return -1;
+        }
+        const int qf = orc_qf4(q), off = intra ? orc_intra_offset4(q) : orc_inter_offset4(q);
+        const int xn = band_ncb[2 * (b - 1)], yn = band_ncb[2 * (b - 1) + 1];
+        const int dc_intra = intra && b == nb;
+        for (int by = 0; by < yn; ++by)
+            for (int bx = 0; bx < xn; ++bx) {
+                const int skip = cb_skip[cb_first[b - 1] + by * xn + bx];
+                const int x0 = xp + bx * xl / xn, x1 = xp + (bx + 1) * xl / xn;
+                const int y0 = yp + by * yl / yn, y1 = yp + (by + 1) * yl / yn;
+                for (int j = y0; j < y1; ++j)
+                    for (int i = x0; i < x1; ++i) {
+                        const size_t at = (size_t)j * cw + i;
+                        coeff[at] = skip ? 0 : decode_val(qindex[at], qf, off);
+                    }
+                if (dc_intra)
+                    for (int j = y0; j < y1; ++j)
+                        for (int i = x0; i < x1; ++i) {
+                            const size_t at = (size_t)j * cw + i;
+                            const int pred = dc_prediction(coeff, cw, i, j);
+                            coeff[at] = skip ? pred : coeff[at] + pred;
+                        }
+            }
+    }
+    free(cb_first);
+    return 0;
+}

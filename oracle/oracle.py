@@ -147,6 +147,20 @@ class Oracle:
             raise ValueError(f"orc_code_residue rc={rc}")
         return c, q, sk, bits, cbs, qo
 
+    def dequantise(self, intra, depth, qindex, band_qidx, band_skip, band_ncb, cb_skip):
+        """The decoder's dequantisation of one component; returns the coefficients."""
+        q = np.ascontiguousarray(qindex, dtype=np.int32)
+        ch, cw = q.shape
+        out = np.zeros_like(q)
+        bq = np.ascontiguousarray(band_qidx, dtype=np.int32)
+        bs = np.ascontiguousarray(band_skip, dtype=np.int32)
+        ncb = np.ascontiguousarray(band_ncb, dtype=np.int32)
+        cbs = np.ascontiguousarray(cb_skip, dtype=np.uint8)
+        rc = self.lib.orc_dequantise(int(intra), depth, _p(q), _p(out), cw, ch, _p(ncb), _p(bq), _p(bs), _p(cbs))
+        if rc:
+            raise ValueError(f"orc_dequantise rc={rc}")
+        return out
+
 
 def _me_call(fn, is_oracle, cformat, pic, ref1, ref2, bp, lambda_, stages, luma_depth):
     """Shared driver of orc_motion_estimate / ref_motion_estimate; returns a dict of arrays."""
