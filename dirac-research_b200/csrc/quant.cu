@@ -696,6 +696,110 @@ __global__ void dc_decode_kernel(const __grid_constant__ DqArgs A) {
     }
 }
 
+// ---- intra DC wavefronts in shared memory ---------------------------------------------------
+//
+// The same recurrences with the band staged in shared memory: one coalesced pass in, the
+// anti-diagonals against shared memory (a step costs a barrier and a few shared accesses
+// instead of dependent global round trips), one coalesced pass out.  Used when the band fits.
+
+constexpr int DC_SMEM_MAX = 200 * 1024;
+constexpr int DC_THREADS = 256;
+
+__device__ __forceinline__ int dc_pred_smem(const int32_t* s, int xl, int x, int y) {
+    if (y != 0) {
+        if (x != 0) {
+            const int sum = s[y * xl + x - 1] + s[(y - 1) * xl + x - 1] + s[(y - 1) * xl + x] + 3 / 2;
+            return sum < 0 ? (sum - 2) / 3 : sum / 3;
+        }
+        return s[(y - 1) * xl];
+    }
+    return x != 0 ? s[x - 1] : 0;
+}
+
+// Encoder side (dc_intra_kernel's arithmetic).
+__global__ void __launch_bounds__(DC_THREADS) dc_intra_smem_kernel(const DcJob* jobs) {
+    extern __shared__ int32_t s_dc[];
+    const DcJob J = jobs[blockIdx.x];
+    const int xl = J.xl, yl = J.yl, n = xl * yl;
+    for (int k = threadIdx.x; k < n; k += DC_THREADS) {
+        const int y = k / xl;
+        s_dc[k] = J.c[(size_t)y * J.stride + (k - y * xl)];
+    }
+    __syncthreads();
+    for (int t = 0; t < xl + yl - 1; ++t) {
+        const int x0 = max(0, t - yl + 1), x1 = min(t, xl - 1);
+        for (int x = x0 + (int)threadIdx.x; x <= x1; x += DC_THREADS) {
+            const int y = t - x;
+            const int pred = (int16_t)dc_pred_smem(s_dc, xl, x, y);
+            const bool skip = J.cb_skip[cb_index(y, yl, J.yn) * J.xn + cb_index(x, xl, J.xn)];
+            int32_t& v = s_dc[y * xl + x];
+            int qi = 0;
+            if (skip) {
+                v = pred;
+            } else {
+                const int val = (int16_t)(v - pred);
+                const unsigned qv = ((unsigned)abs(val) << 2) / (unsigned)J.qf;
+                int r = 0;
+                if (qv) {
+                    r = (int)((qv * (unsigned)J.qf + J.off + 2) >> 2);
+                    if (val <= 0) r = -r;
+                }
+                qi = val < 0 ? -(int)qv : (int)qv;
+                v = r + pred;
+            }
+            if (J.qout) J.qout[(size_t)y * J.stride + x] = qi;
+        }
+        __syncthreads();
+    }
+    for (int k = threadIdx.x; k < n; k += DC_THREADS) {
+        const int y = k / xl;
+        J.c[(size_t)y * J.stride + (k - y * xl)] = s_dc[k];
+    }
+}
+
+// Decoder side (dc_decode_kernel's arithmetic): the residues (zero in skipped code blocks,
+// where the value is the prediction alone) are staged first.
+__global__ void __launch_bounds__(DC_THREADS) dc_decode_smem_kernel(const __grid_constant__ DqArgs A) {
+    extern __shared__ int32_t s_dc[];
+    const DqBand& B = A.band[A.dc_band[blockIdx.x]];
+    const int xl = B.xl, yl = B.yl, n = xl * yl;
+    for (int k = threadIdx.x; k < n; k += DC_THREADS) {
+        const int y = k / xl, x = k - y * xl;
+        const bool skip = B.cb[cb_of(y, yl, B.yn) * B.xn + cb_of(x, xl, B.xn)];
+        s_dc[k] = skip ? 0 : dequant_value(B.q[(size_t)y * B.stride + x], B.qf, B.off);
+    }
+    __syncthreads();
+    for (int t = 0; t < xl + yl - 1; ++t) {
+        const int x0 = max(0, t - yl + 1), x1 = min(t, xl - 1);
+        for (int x = x0 + (int)threadIdx.x; x <= x1; x += DC_THREADS) {
+            const int y = t - x;
+            s_dc[y * xl + x] += dc_pred_smem(s_dc, xl, x, y);
+        }
+        __syncthreads();
+    }
+    for (int k = threadIdx.x; k < n; k += DC_THREADS) {
+        const int y = k / xl;
+        B.c[(size_t)y * B.stride + (k - y * xl)] = s_dc[k];
+    }
+}
+
+// Opts the shared-memory DC kernels into DC_SMEM_MAX bytes of dynamic shared memory (once).
+int dc_smem_setup() {
+    static const cudaError_t e = [] {
+        cudaError_t r = cudaFuncSetAttribute(dc_intra_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             DC_SMEM_MAX);
+        if (r == cudaSuccess)
+            r = cudaFuncSetAttribute(dc_decode_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     DC_SMEM_MAX);
+        return r;
+    }();
+    if (e != cudaSuccess) {
+        set_last_cuda_error(e, "cudaFuncSetAttribute (DC kernels)", __FILE__, __LINE__);
+        return DGPU_ERR_CUDA;
+    }
+    return DGPU_OK;
+}
+
 // ---- host: the reference's Lagrangian choice (quant_chooser.cpp:62-147, 266-318) -------------
 
 struct HostStat {
@@ -1024,6 +1128,7 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     {
         std::vector<DcJob> dj;
         int threads = 32;
+        size_t smem = 0;
         for (int c = 0; c < n; ++c) {
             const Comp& C = comps[c];
             const int t = C.band_first + C.nbands - 1;
@@ -1031,12 +1136,19 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
             const int xl = C.cw >> C.depth, yl = C.ch >> C.depth;
             const int q = band_qidx[t];
             threads = std::max(threads, std::min(1024, ((xl + 31) / 32) * 32));
+            smem = std::max(smem, (size_t)xl * yl * sizeof(int32_t));
             dj.push_back(DcJob{const_cast<int32_t*>(C.coeff), qout ? qout[c] : nullptr, d_cbskip + tasks[t].cb_first,
                                C.cw, xl, yl, tasks[t].xn, tasks[t].yn, qf4(q), intra_off4(q)});
         }
         if (!dj.empty()) {
             DGPU_CHECK_CUDA(cudaMemcpyAsync(d_dcjobs, dj.data(), sizeof(DcJob) * dj.size(), cudaMemcpyHostToDevice, st));
-            dc_intra_kernel<<<(int)dj.size(), threads, 0, st>>>(d_dcjobs);
+            if (smem <= (size_t)DC_SMEM_MAX) {
+                const int rc = dc_smem_setup();
+                if (rc) return rc;
+                dc_intra_smem_kernel<<<(int)dj.size(), DC_THREADS, smem, st>>>(d_dcjobs);
+            } else {
+                dc_intra_kernel<<<(int)dj.size(), threads, 0, st>>>(d_dcjobs);
+            }
             DGPU_CHECK_LAUNCH();
         }
     }
@@ -1086,7 +1198,18 @@ int launch_dequantise(DqArgs& A, int ndc, int chunks, cudaStream_t st) {
         DGPU_CHECK_LAUNCH();
     }
     if (ndc > 0) {
-        dc_decode_kernel<<<ndc, 256, 0, st>>>(A);
+        size_t smem = 0;
+        for (int k = 0; k < ndc; ++k) {
+            const DqBand& B = A.band[A.dc_band[k]];
+            smem = std::max(smem, (size_t)B.xl * B.yl * sizeof(int32_t));
+        }
+        if (smem <= (size_t)DC_SMEM_MAX) {
+            const int rc = dc_smem_setup();
+            if (rc) return rc;
+            dc_decode_smem_kernel<<<ndc, DC_THREADS, smem, st>>>(A);
+        } else {
+            dc_decode_kernel<<<ndc, 256, 0, st>>>(A);
+        }
         DGPU_CHECK_LAUNCH();
     }
     A.nbands = 0;
