@@ -613,7 +613,7 @@ struct DqBand {
     int stride, xl, yl, xn, yn;
     int qf, off;        // QuantFactor4 and the intra / inter offset of the band's quantiser
     int skip;           // whole band zero
-    int dc;             // intra DC band: decoded by dc_decode_kernel
+    int dc;             // intra DC band: predictions added by dc_decode_kernel
     int first, rows;    // first CTA and rows per CTA in the row-chunked grid
 };
 
@@ -632,7 +632,8 @@ __device__ __forceinline__ int dequant_value(int qi, int qf, int off) {
 }
 
 // grid: row chunks of the bands laid end to end, a warp per row, lanes across it, the code
-// block followed by CbWalk.  Intra DC bands are left to dc_decode_kernel.
+// block followed by CbWalk.  An intra DC band gets its decoded residues here (zero in skipped
+// code blocks); dc_decode_kernel then adds the predictions.
 __global__ void __launch_bounds__(ROW_THREADS) dequantise_kernel(const __grid_constant__ DqArgs A) {
     int lo_b = 0, hi_b = A.nbands - 1;
     while (lo_b < hi_b) {
@@ -641,35 +642,46 @@ __global__ void __launch_bounds__(ROW_THREADS) dequantise_kernel(const __grid_co
         else hi_b = mid - 1;
     }
     const DqBand& B = A.band[lo_b];
-    if (B.dc) return;
     const int r0 = ((int)blockIdx.x - B.first) * B.rows;
     const int r1 = min(B.yl, r0 + B.rows);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int xl = B.xl;
     for (int j = r0 + warp; j < r1; j += ROW_THREADS / 32) {
-        if (lane >= B.xl) break;
+        if (lane >= xl) break;
         const int32_t* qrow = B.q + (size_t)j * B.stride;  // may alias row (in place)
         int32_t* row = B.c + (size_t)j * B.stride;
         if (B.skip) {
-            for (int i = lane; i < B.xl; i += 32) row[i] = 0;
+            for (int i = lane; i < xl; i += 32) row[i] = 0;
             continue;
         }
         const uint8_t* skip_row = B.cb + cb_of(j, B.yl, B.yn) * B.xn;
-        CbWalk w(lane, B.xl, B.xn);
-        for (int i = lane; i < B.xl; i += 32) {
-            w.to(i);
-            row[i] = skip_row[w.cx] ? 0 : dequant_value(qrow[i], B.qf, B.off);
+        CbWalk w(lane, xl, B.xn);
+        // four loads in flight per lane before the first store (each element is read before
+        // it is written, by the same lane, so in-place calls are safe)
+        for (int i0 = lane; i0 < xl; i0 += 128) {
+            int v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = i0 + 32 * u < xl ? qrow[i0 + 32 * u] : 0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int i = i0 + 32 * u;
+                if (i < xl) {
+                    w.to(i);
+                    row[i] = skip_row[w.cx] ? 0 : dequant_value(v[u], B.qf, B.off);
+                }
+            }
         }
     }
 }
 
-// Intra DC bands, one CTA each: value = decoded residue + prediction from the reconstructed
-// left / top-left / top neighbours (int32, as the decoder's GetPrediction computes it); a
-// skipped code block takes the prediction alone.  Positions on one anti-diagonal depend only
-// on earlier diagonals, so the diagonals run in order and each one in parallel; that equals
-// the reference's code block by code block raster order.
+// Intra DC bands, one CTA each, after dequantise_kernel has written the decoded residues:
+// value = residue + prediction from the reconstructed left / top-left / top neighbours
+// (int32, as the decoder's GetPrediction computes it); in a skipped code block the residue is
+// zero and the value the prediction alone.  Positions on one anti-diagonal depend only on
+// earlier diagonals, so the diagonals run in order and each one in parallel; that equals the
+// reference's code block by code block raster order.
 __global__ void dc_decode_kernel(const __grid_constant__ DqArgs A) {
     const DqBand& B = A.band[A.dc_band[blockIdx.x]];
-    const int32_t* const q = B.q;
     int32_t* const c = B.c;
     const int stride = B.stride, xl = B.xl, yl = B.yl;
     for (int t = 0; t < xl + yl - 1; ++t) {
@@ -688,9 +700,7 @@ __global__ void dc_decode_kernel(const __grid_constant__ DqArgs A) {
             } else {
                 pred = x != 0 ? c[x - 1] : 0;
             }
-            const size_t at = (size_t)y * stride + x;
-            const bool skip = B.cb[cb_of(y, yl, B.yn) * B.xn + cb_of(x, xl, B.xn)];
-            c[at] = skip ? pred : dequant_value(q[at], B.qf, B.off) + pred;
+            c[(size_t)y * stride + x] += pred;
         }
         __syncthreads();
     }
@@ -716,15 +726,29 @@ __device__ __forceinline__ int dc_pred_smem(const int32_t* s, int xl, int x, int
     return x != 0 ? s[x - 1] : 0;
 }
 
+// Loads an xl x yl band (row stride `stride`) into shared memory with several loads in flight
+// per thread.
+__device__ __forceinline__ void dc_stage_in(int32_t* s, const int32_t* g, int stride, int xl, int n) {
+    for (int k0 = threadIdx.x; k0 < n; k0 += 8 * DC_THREADS) {
+        int v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int k = k0 + u * DC_THREADS;
+            const int y = k / xl;
+            v[u] = k < n ? g[(size_t)y * stride + (k - y * xl)] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (k0 + u * DC_THREADS < n) s[k0 + u * DC_THREADS] = v[u];
+    }
+}
+
 // Encoder side (dc_intra_kernel's arithmetic).
 __global__ void __launch_bounds__(DC_THREADS) dc_intra_smem_kernel(const DcJob* jobs) {
     extern __shared__ int32_t s_dc[];
     const DcJob J = jobs[blockIdx.x];
     const int xl = J.xl, yl = J.yl, n = xl * yl;
-    for (int k = threadIdx.x; k < n; k += DC_THREADS) {
-        const int y = k / xl;
-        s_dc[k] = J.c[(size_t)y * J.stride + (k - y * xl)];
-    }
+    dc_stage_in(s_dc, J.c, J.stride, xl, n);
     __syncthreads();
     for (int t = 0; t < xl + yl - 1; ++t) {
         const int x0 = max(0, t - yl + 1), x1 = min(t, xl - 1);
@@ -757,17 +781,12 @@ __global__ void __launch_bounds__(DC_THREADS) dc_intra_smem_kernel(const DcJob* 
     }
 }
 
-// Decoder side (dc_decode_kernel's arithmetic): the residues (zero in skipped code blocks,
-// where the value is the prediction alone) are staged first.
+// Decoder side (dc_decode_kernel's arithmetic) over the residues dequantise_kernel wrote.
 __global__ void __launch_bounds__(DC_THREADS) dc_decode_smem_kernel(const __grid_constant__ DqArgs A) {
     extern __shared__ int32_t s_dc[];
     const DqBand& B = A.band[A.dc_band[blockIdx.x]];
     const int xl = B.xl, yl = B.yl, n = xl * yl;
-    for (int k = threadIdx.x; k < n; k += DC_THREADS) {
-        const int y = k / xl, x = k - y * xl;
-        const bool skip = B.cb[cb_of(y, yl, B.yn) * B.xn + cb_of(x, xl, B.xn)];
-        s_dc[k] = skip ? 0 : dequant_value(B.q[(size_t)y * B.stride + x], B.qf, B.off);
-    }
+    dc_stage_in(s_dc, B.c, B.stride, xl, n);
     __syncthreads();
     for (int t = 0; t < xl + yl - 1; ++t) {
         const int x0 = max(0, t - yl + 1), x1 = min(t, xl - 1);
