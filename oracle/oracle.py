@@ -304,14 +304,52 @@ def reference_encode(cfg, frames, freeze=True, path=REF_SO):
     rc = lib.ref_encode_sequence(ctypes.byref(p), n, _p(flat), int(freeze), _p(recon), _p(ptype), ctypes.byref(nbytes))
     if rc:
         raise ValueError("ref_encode_sequence failed")
-    shapes = [c.shape for c in frames[0]]
+    return _split_frames(recon, [c.shape for c in frames[0]], n), ptype, nbytes.value
+
+
+def _split_frames(flat, shapes, n):
     fsize = sum(int(np.prod(s)) for s in shapes)
     out = []
     for i in range(n):
         fr, o = [], i * fsize
         for s in shapes:
             k = int(np.prod(s))
-            fr.append(recon[o:o + k].reshape(s))
+            fr.append(flat[o:o + k].reshape(s))
             o += k
         out.append(tuple(fr))
-    return out, ptype, nbytes.value
+    return out
+
+
+def reference_encode_stream(cfg, frames, freeze=True, path=REF_SO):
+    """As reference_encode, returning (recon frames, intra flags, the coded bitstream bytes)."""
+    lib = Reference(path).lib
+    p = RefEncParams(**cfg)
+    n = len(frames)
+    flat = np.concatenate([np.concatenate([np.ascontiguousarray(c, np.uint8).ravel() for c in f]) for f in frames])
+    recon = np.zeros_like(flat)
+    ptype = np.zeros(n, np.int32)
+    cap = max(1 << 20, 2 * flat.size)
+    stream = np.zeros(cap, np.uint8)
+    nbytes = ctypes.c_longlong(0)
+    rc = lib.ref_encode_stream(ctypes.byref(p), n, _p(flat), int(freeze), _p(recon), _p(ptype), _p(stream),
+                               ctypes.c_longlong(cap), ctypes.byref(nbytes))
+    if rc:
+        raise ValueError(f"ref_encode_stream failed: {rc}")
+    return _split_frames(recon, [c.shape for c in frames[0]], n), ptype, stream[:nbytes.value].copy()
+
+
+def reference_decode(stream, width, height, cformat, nframes, path=REF_SO):
+    """Decode an 8-bit Dirac bitstream with the reference decoder's public API; returns the
+    frames [(Y, U, V) uint8 planes] by frame number (None where no frame was delivered)."""
+    lib = Reference(path).lib
+    xs, ys = chroma_shift(cformat)
+    cw, ch = width >> xs, height >> ys
+    data = np.ascontiguousarray(stream, np.uint8)
+    flat = np.zeros(nframes * (width * height + 2 * cw * ch), np.uint8)
+    got = np.zeros(nframes, np.int32)
+    rc = lib.ref_decode_stream(_p(data), ctypes.c_longlong(data.size), width, height, cw, ch, nframes, _p(flat),
+                               _p(got))
+    if rc < 0:
+        raise ValueError("ref_decode_stream: invalid stream")
+    frames = _split_frames(flat, [(height, width), (ch, cw), (ch, cw)], nframes)
+    return [f if got[i] else None for i, f in enumerate(frames)]

@@ -1,7 +1,8 @@
 // Test infrastructure only: runs the reference encoder through its own public C API
 // (libdirac_encoder/dirac_encoder.h: dirac_encoder_context_init, dirac_encoder_init,
 // dirac_encoder_load, dirac_encoder_output, dirac_encoder_end_sequence, dirac_encoder_close)
-// and returns its locally decoded pictures, so that the tests can pin a whole coding loop
+// and returns its locally decoded pictures (and, from ref_encode_stream, its bitstream), so
+// that the tests can pin a whole coding loop
 // (GOP structure, cut detection, lambdas, motion estimation, compensation, transform and
 // quantisation) against the reference itself.  Linked into oracle/_ref/libdirac_ref.so.
 //
@@ -57,8 +58,13 @@ struct RefEncParams {
 // number; ptype[pnum] = 1 for intra, 0 for inter, -1 if never returned; *bytes = total
 // bitstream bytes.  freeze: keep the initial entropy-correction factors.
 // Returns 0, or -1 on an encoder failure.
-int ref_encode_sequence(const RefEncParams* p, int nframes, const unsigned char* frames, int freeze,
-                        unsigned char* recon, int* ptype, long long* bytes) {
+}  // extern "C"
+
+namespace {
+
+// The encode of ref_encode_sequence; the coded bitstream is appended to *stream when given.
+int encode_impl(const RefEncParams* p, int nframes, const unsigned char* frames, int freeze, unsigned char* recon,
+                int* ptype, long long* bytes, std::vector<unsigned char>* stream) {
     g_freeze_factors = freeze != 0;
     dirac_encoder_context_t ctx;
     dirac_encoder_context_init(&ctx, static_cast<dirac_encoder_presets_t>(p->video_format));
@@ -109,7 +115,10 @@ int ref_encode_sequence(const RefEncParams* p, int nframes, const unsigned char*
             enc->enc_buf.size = (int)out.size();
             const dirac_encoder_state_t st = dirac_encoder_output(enc);
             if (st == ENC_STATE_INVALID) return -1;
-            if (st == ENC_STATE_AVAIL || st == ENC_STATE_EOS) total += enc->enc_buf.size;
+            if (st == ENC_STATE_AVAIL || st == ENC_STATE_EOS) {
+                total += enc->enc_buf.size;
+                if (stream) stream->insert(stream->end(), out.data(), out.data() + enc->enc_buf.size);
+            }
             if (enc->decoded_frame_avail) {
                 const int pn = enc->dec_pparams.pnum;
                 if (pn >= 0 && pn < nframes) {
@@ -139,6 +148,28 @@ int ref_encode_sequence(const RefEncParams* p, int nframes, const unsigned char*
     g_freeze_factors = false;
     *bytes = total;
     return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_encode_sequence(const RefEncParams* p, int nframes, const unsigned char* frames, int freeze,
+                        unsigned char* recon, int* ptype, long long* bytes) {
+    return encode_impl(p, nframes, frames, freeze, recon, ptype, bytes, nullptr);
+}
+
+// As ref_encode_sequence, and the coded bitstream copied to stream (capacity cap bytes;
+// *bytes is its length).  Returns -2 when the stream does not fit.
+int ref_encode_stream(const RefEncParams* p, int nframes, const unsigned char* frames, int freeze,
+                      unsigned char* recon, int* ptype, unsigned char* stream, long long cap, long long* bytes) {
+    std::vector<unsigned char> s;
+    const int rc = encode_impl(p, nframes, frames, freeze, recon, ptype, bytes, &s);
+    if (rc) return rc;
+    if ((long long)s.size() > cap) return -2;
+    std::memcpy(stream, s.data(), s.size());
+    *bytes = (long long)s.size();
+    return 0;
 }
 
 }  // extern "C"

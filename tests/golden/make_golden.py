@@ -3,7 +3,7 @@
 Needs oracle/_ref/libdirac_ref.so (the reference's own C++, plain-C build, compiled from
 its sources by `make -C oracle`).  Inputs are seeded, so re-running reproduces the files.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [dwt convert mc me quant encode decode]
 """
 import os
 import sys
@@ -197,15 +197,39 @@ def encode_cases():
     return out
 
 
-def main():
+def decode_cases():
+    """The reference decoder run through its public API on the reference encoder's bitstream
+    of each ENCODE_CASES sequence: CRC-32 of every decoded plane by frame number, and the
+    stream length."""
+    import zlib
+
+    from oracle import reference_decode, reference_encode_stream
+
+    out = {}
+    for case in ENCODE_CASES:
+        seq, cfg = encode_inputs(case)
+        _, _, stream = reference_encode_stream(cfg, seq, freeze=True)
+        dec = reference_decode(stream, cfg["width"], cfg["height"], cfg["cformat"], len(seq))
+        if any(f is None for f in dec):
+            raise RuntimeError(f"{case[0]}: the reference decoder did not deliver every frame")
+        name = case[0]
+        out[name + "_crc"] = np.array([[zlib.crc32(np.ascontiguousarray(p).tobytes()) for p in f] for f in dec],
+                                      np.uint32)
+        out[name + "_bytes"] = np.array(len(stream), np.int64)
+    return out
+
+
+def main(argv=None):
+    """Writes the named fixtures (default: all)."""
+    names = (argv if argv is not None else sys.argv[1:]) or ["dwt", "convert", "mc", "me", "quant", "encode",
+                                                              "decode"]
     ref = Reference()
-    np.savez_compressed(os.path.join(HERE, "dwt.npz"), **dwt_cases(ref))
-    np.savez_compressed(os.path.join(HERE, "convert.npz"), **conv_cases(ref))
-    np.savez_compressed(os.path.join(HERE, "mc.npz"), **mc_cases(ref))
-    np.savez_compressed(os.path.join(HERE, "me.npz"), **me_cases(ref))
-    np.savez_compressed(os.path.join(HERE, "quant.npz"), **quant_cases(ref))
-    np.savez_compressed(os.path.join(HERE, "encode.npz"), **encode_cases())
-    print("wrote dwt.npz, convert.npz, mc.npz, me.npz, quant.npz, encode.npz")
+    makers = {"dwt": lambda: dwt_cases(ref), "convert": lambda: conv_cases(ref), "mc": lambda: mc_cases(ref),
+              "me": lambda: me_cases(ref), "quant": lambda: quant_cases(ref), "encode": encode_cases,
+              "decode": decode_cases}
+    for n in names:
+        np.savez_compressed(os.path.join(HERE, n + ".npz"), **makers[n]())
+    print("wrote " + ", ".join(n + ".npz" for n in names))
 
 
 if __name__ == "__main__":

@@ -4,7 +4,8 @@ against the oracle and the reference.
 Round trip: what the device encoder coded (quantised indices, band quantisers and skips,
 code-block skips, motion data) decoded by the device decoder in coding order gives, bit for
 bit, the encoder's locally decoded pictures and reconstructed coefficients, and output
-samples equal to the reference encoder's (golden CRC-32s); the same pictures decoded by the
+samples equal to the reference decoder's decode of the reference encoder's bitstream (golden
+CRC-32s); the same pictures decoded by the
 oracle's restatement of the reference decoder agree.  The stage alone is checked against
 orc_dequantise on random indices, skips and quantisers, intra and inter, depths 1-5."""
 import os
@@ -116,7 +117,7 @@ def test_decoder_round_trip_matches_reference(gpu, golden, case):
     check_round_trip(infos, results, dec)
     crc = np.array([[zlib.crc32(np.ascontiguousarray(dec[i]["output"][c]).tobytes()) for c in range(3)]
                     for i in range(len(infos))], np.uint32)
-    np.testing.assert_array_equal(crc, golden("encode.npz")[case[0] + "_crc"])
+    np.testing.assert_array_equal(crc, golden("decode.npz")[case[0] + "_crc"])   # the reference decoder's
 
 
 def test_decoder_device_inputs(gpu):

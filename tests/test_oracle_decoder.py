@@ -1,9 +1,9 @@
 """The oracle's restatement of the reference decoder's picture decoding (oracle/oracle_decoder.py,
 orc_dequantise) against the reference: decoding what the restated encoder coded (quantised
 indices, band quantisers and skips, code-block skips, motion data) must give the encoder's
-locally decoded pictures, whose output samples are pinned to the reference encoder's own
-(tests/golden/encode.npz, made through the reference's public encoder API).  A Dirac
-decoder's output equals the encoder's local decode (the reference's own colourbars test)."""
+locally decoded pictures and output samples equal to the reference decoder's own decode of the
+reference encoder's bitstream (tests/golden/decode.npz, made through the reference's public
+encoder and decoder APIs; equal to the reference encoder's local decode, encode.npz)."""
 import os
 import sys
 import zlib
@@ -34,13 +34,32 @@ def test_oracle_decoder_round_trip(golden, oracle, case):
     cfg, enc = oracle_encode(case)
     ncb = quant.code_blocks(cfg["wlt_depth"], cfg["width"], cfg["height"])
     dec = decode_coded_sequence(cfg, enc, ncb, oracle)
-    g = golden("encode.npz")
     crc = []
     for pn in range(len(enc.pics)):
         for c in range(3):
             np.testing.assert_array_equal(dec[pn][c], enc.pics[pn].data[c], err_msg=f"picture {pn} component {c}")
         crc.append([zlib.crc32(np.ascontiguousarray(p).tobytes()) for p in output_samples(dec[pn], 8, 8)])
-    np.testing.assert_array_equal(np.array(crc, np.uint32), g[case[0] + "_crc"])
+    np.testing.assert_array_equal(np.array(crc, np.uint32), golden("decode.npz")[case[0] + "_crc"])
+    np.testing.assert_array_equal(golden("decode.npz")[case[0] + "_crc"], golden("encode.npz")[case[0] + "_crc"])
+
+
+def test_oracle_decoder_matches_live_reference_decoder(oracle):
+    """The oracle's decode against the reference decoder's, sample for sample, on the
+    reference encoder's own bitstream of the reconfigured sequence."""
+    from dirac_b200 import quant
+    from oracle import Reference, reference_decode, reference_encode_stream
+    from oracle_decoder import decode_coded_sequence, output_samples
+
+    if not Reference.available():
+        pytest.skip("reference library not built here")
+    seq, rcfg = encode_inputs(ENCODE_CASES[1])
+    _, _, stream = reference_encode_stream(rcfg, seq, freeze=True)
+    ref = reference_decode(stream, rcfg["width"], rcfg["height"], rcfg["cformat"], len(seq))
+    cfg, enc = oracle_encode(ENCODE_CASES[1])
+    dec = decode_coded_sequence(cfg, enc, quant.code_blocks(cfg["wlt_depth"], cfg["width"], cfg["height"]), oracle)
+    for pn in range(len(seq)):
+        for c, p in enumerate(output_samples(dec[pn], 8, 8)):
+            np.testing.assert_array_equal(p, ref[pn][c], err_msg=f"picture {pn} component {c}")
 
 
 def test_dequantise_values(oracle):
