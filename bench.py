@@ -100,13 +100,17 @@ def _init_worker(frames):
     _WORKER_FRAMES = frames
 
 
-def _ref_encode(_):
-    """One reference encode of the worker's frames (stock encoder: adaptive entropy factors)."""
+def _ref_encode(_, keep_stream=None):
+    """One reference encode of the worker's frames (stock encoder: adaptive entropy factors);
+    with keep_stream (a list), its bitstream is appended there."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from oracle import reference_encode
+    from oracle import reference_encode, reference_encode_stream
 
     t0 = time.perf_counter()
-    reference_encode(ref_config(), _WORKER_FRAMES, freeze=False)
+    if keep_stream is None:
+        reference_encode(ref_config(), _WORKER_FRAMES, freeze=False)
+    else:
+        keep_stream.append(reference_encode_stream(ref_config(), _WORKER_FRAMES, freeze=False)[2])
     return time.perf_counter() - t0
 
 
@@ -117,15 +121,34 @@ def reference_available():
     return Reference.available()
 
 
-def cpu_baseline_single(frames):
-    """The reference encoder in this process (one core) on the first frames of the sequence."""
+def cpu_baseline_single(frames, streams=None):
+    """The reference encoder in this process (one core) on the first frames of the sequence;
+    with streams (a list), the timed encode's bitstream is appended there."""
     global _WORKER_FRAMES
     _WORKER_FRAMES = frames
     _ref_encode(None)  # warm-up (page-in, allocator)
-    dt = _ref_encode(None)
+    dt = _ref_encode(None, streams)
     return {"value": len(frames) / dt, "unit": "frames/s", "cores": 1, "kind": "reference",
             "sample": f"reference encoder (dirac_encoder_* API, plain-C build) on the first {len(frames)} frames "
                       f"of the step's sequence: {dt:.2f} s on 1 core"}
+
+
+def cpu_decode_baseline(stream, nframes):
+    """The reference decoder in this process (one core) on the reference encoder's bitstream of
+    the first frames of the sequence."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import reference_decode
+
+    w, h = PARAMS["width"], PARAMS["height"]
+    reference_decode(stream, w, h, PARAMS["cformat"], nframes)  # warm-up
+    t0 = time.perf_counter()
+    out = reference_decode(stream, w, h, PARAMS["cformat"], nframes)
+    dt = time.perf_counter() - t0
+    n = sum(f is not None for f in out)
+    return {"value": n / dt, "unit": "frames/s", "cores": 1, "kind": "reference",
+            "sample": f"reference decoder (dirac_decoder_* API, plain-C build) on the reference encoder's bitstream "
+                      f"of the first {nframes} frames of the sequence ({len(stream)} bytes): {n} frames in "
+                      f"{dt:.2f} s on 1 core, its arithmetic decoding included"}
 
 
 def run_reference(args):
@@ -315,13 +338,14 @@ def run_hetero(args, peak, peaks):
     return out
 
 
-def run_decoding(args, enc, infos, peak):
+def run_decoding(args, enc, infos, peak, cpu_decode=None):
     """The decoding leg: the 1080p sequence the plain form coded, decoded by the device decoder
     (dgpu_decoder_*) from its quantised indices, band and code-block choices and motion data, in
     coding order; every picture's output samples checked against the encoder's locally decoded
     ones.  Device-resident inputs for `value`; page-locked host inputs and output samples read
-    back to page-locked host memory for `e2e`.  The oracle's restatement of the decoder timed on
-    one host core is the CPU baseline."""
+    back to page-locked host memory for `e2e`.  The CPU baseline is the reference decoder on one
+    host core (cpu_decode, measured before any GPU work), with the oracle's restatement of the
+    decoder timed beside it."""
     import numpy as np
     import torch
 
@@ -436,6 +460,10 @@ def run_decoding(args, enc, infos, peak):
         if t_cpu > 10.0 or k + 1 >= 8:
             break
     ncpu = len(done)
+    port = {"value": ncpu / t_cpu, "unit": "frames/s", "cores": 1, "kind": "port",
+            "sample": f"the oracle's plain-C restatement of the decoder (dequantisation, inverse transform, motion "
+                      f"compensation, clip) on the first {ncpu} pictures in coding order: {t_cpu:.2f} s on 1 core"}
+    baseline = cpu_decode if cpu_decode and cpu_decode.get("value") else port
     return {"value": len(infos) * args.steps / (ms / 1000.0), "unit": "frames/s", "frames_per_step": len(infos),
             "ms_per_step": ms / args.steps, "steps": args.steps,
             "e2e": {"value": len(infos) * args.steps / (ems / 1000.0), "unit": "frames/s",
@@ -444,10 +472,7 @@ def run_decoding(args, enc, infos, peak):
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
                          "algorithmic_bytes_per_step": alg},
-            "cpu_baseline": {"value": ncpu / t_cpu, "unit": "frames/s", "cores": 1, "kind": "port",
-                             "sample": f"the oracle's plain-C restatement of the decoder (dequantisation, inverse "
-                                       f"transform, motion compensation, clip) on the first {ncpu} pictures in "
-                                       f"coding order: {t_cpu:.2f} s on 1 core"},
+            "cpu_baseline": baseline, "cpu_port": port,
             "workload": "decode of the plain form's coded 1920x1080 4:2:0 8-bit 32-picture sequence from its "
                         "quantised indices (int32), band and code-block choices and motion data; output 8-bit "
                         "samples"}
@@ -466,9 +491,16 @@ def main():
     frames = make_frames(args.frames, seed=1000 + rank)
     # CPU baseline first (rank 0, N=1), before any GPU call
     cpu_baseline = None
+    cpu_decode = None
     if world == 1 and rank == 0:
         if reference_available():
-            cpu_baseline = cpu_baseline_single(frames[:CPU_SAMPLE_FRAMES])
+            streams = []
+            cpu_baseline = cpu_baseline_single(frames[:CPU_SAMPLE_FRAMES], streams)
+            if args.decode:
+                try:
+                    cpu_decode = cpu_decode_baseline(streams[0], CPU_SAMPLE_FRAMES)
+                except Exception as e:  # the decoding leg falls back to the oracle's decoder
+                    cpu_decode = {"error": repr(e)}
         else:
             cpu_baseline = {"value": None, "unit": "frames/s", "cores": 1, "kind": "reference",
                             "sample": "unavailable: oracle/_ref/libdirac_ref.so was not built"}
@@ -696,7 +728,7 @@ def main():
     # ---- decoding: the plain form's coded sequence through the device decoder ----------------
     decoding = None
     if args.decode and world == 1:
-        decoding = run_decoding(args, enc, infos, peak)
+        decoding = run_decoding(args, enc, infos, peak, cpu_decode)
     for g, _ in groups:
         g.close()
     for ln in lanes:
