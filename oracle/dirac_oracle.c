@@ -1,7 +1,7 @@
 /*
  * dirac_oracle.c -- TEST INFRASTRUCTURE ONLY (see dirac_oracle.h).
  *
- * Plain-C restatement of the Dirac hot path used as the parity checker for the CUDA
+ * Plain-C restatement of the Dirac hot path used as the parity oracle for the CUDA
  * kernels and as the timed CPU baseline.  Written from the reference's behaviour, not
  * copied: the per-filter edge formulas of libdirac_common/wavelet_utils.cpp are expressed
  * through a single rule (a neighbour index is clamped inside its own parity

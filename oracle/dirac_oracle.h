@@ -3,7 +3,7 @@
  *
  * A plain-C restatement of the Dirac research codec's data-parallel hot path, written
  * for this project from the reference's behaviour (each function cites the reference
- * file:line it restates).  It is the checker the tests compare the CUDA path against and
+ * file:line it restates).  It is the oracle the tests compare the CUDA path against and
  * the CPU baseline bench.py times; nothing in the product links or loads it.
  *
  * Conventions: pictures are int16 (the reference's ValueType), wavelet coefficients int32

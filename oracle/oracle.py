@@ -1,4 +1,4 @@
-"""TEST INFRASTRUCTURE ONLY: ctypes access to the CPU checkers built by oracle/Makefile.
+"""TEST INFRASTRUCTURE ONLY: ctypes access to the CPU oracles built by oracle/Makefile.
 
 ``Oracle`` wraps liboracle.so, this project's plain-C restatement of the Dirac hot path
 (oracle/dirac_oracle.c).  ``Reference`` wraps oracle/_ref/libdirac_ref.so, the reference

@@ -16,7 +16,7 @@ for p in (PKG, ORACLE):
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a B200 (sm_100a) GPU")
-    # The checkers and the library are built in place (both are quick, idempotent makes).
+    # The oracle and the library are built in place (both are quick, idempotent makes).
     subprocess.run(["make", "-s", "-C", ORACLE, "oracle"], check=True)
     subprocess.run(["make", "-s", "-C", PKG], check=True)
 
