@@ -26,6 +26,7 @@
 #include <vector>
 
 #include <atomic>
+#include <mutex>
 
 #include "dgpu_internal.cuh"
 
@@ -802,20 +803,22 @@ __global__ void __launch_bounds__(DC_THREADS) dc_decode_smem_kernel(const __grid
     }
 }
 
-// Opts the shared-memory DC kernels into DC_SMEM_MAX bytes of dynamic shared memory (once).
+// Opts the shared-memory DC kernels into DC_SMEM_MAX bytes of dynamic shared memory, once
+// per device (the attribute belongs to the current device; one fixed value, so concurrent
+// host threads never launch against a smaller setting).
 int dc_smem_setup() {
-    static const cudaError_t e = [] {
-        cudaError_t r = cudaFuncSetAttribute(dc_intra_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             DC_SMEM_MAX);
-        if (r == cudaSuccess)
-            r = cudaFuncSetAttribute(dc_decode_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     DC_SMEM_MAX);
-        return r;
-    }();
-    if (e != cudaSuccess) {
-        set_last_cuda_error(e, "cudaFuncSetAttribute (DC kernels)", __FILE__, __LINE__);
-        return DGPU_ERR_CUDA;
-    }
+    static std::mutex mu;
+    static uint64_t done = 0;  // devices 0..63 already set up
+    int dev = 0;
+    DGPU_CHECK_CUDA(cudaGetDevice(&dev));
+    const uint64_t bit = dev < 64 ? (uint64_t)1 << dev : 0;
+    std::lock_guard<std::mutex> lock(mu);
+    if (bit && (done & bit)) return DGPU_OK;
+    DGPU_CHECK_CUDA(
+        cudaFuncSetAttribute(dc_intra_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, DC_SMEM_MAX));
+    DGPU_CHECK_CUDA(
+        cudaFuncSetAttribute(dc_decode_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, DC_SMEM_MAX));
+    done |= bit;
     return DGPU_OK;
 }
 
