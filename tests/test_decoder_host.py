@@ -76,3 +76,22 @@ def test_decoder_null_handles():
     assert L.dgpu_decoder_item_bytes(None, 0, 0, 0) == 0
     buf = np.zeros(4, np.uint8)
     assert L.dgpu_decoder_read(None, 0, 0, 0, buf.ctypes.data, 4, 1) == -1
+
+
+def test_decode_bytes_model():
+    """The decoding leg's algorithmic bytes: 8 B per coefficient for the dequantisation, the
+    inverse transform as the encoder's, OBMC ADD with the clip for inter pictures (the clip
+    alone for intra ones) and one upconversion per reference picture used."""
+    from dirac_b200.roofline import decode_bytes, dwt_bytes
+
+    params = dict(cformat=2, width=64, height=32, luma_depth=8, chroma_depth=8, wlt_depth=2)
+    infos = [dict(intra=1, num_refs=0, ref1=-1, ref2=-1),
+             dict(intra=0, num_refs=1, ref1=0, ref2=-1),
+             dict(intra=0, num_refs=2, ref1=0, ref2=1)]
+    b = decode_bytes(params, infos)
+    coeffs = 64 * 32 + 2 * 32 * 16
+    samples = coeffs  # sizes are multiples of 4: no padding
+    assert b["dequantisation"] == 3 * 8 * coeffs
+    assert b["dwt_inverse"] == 3 * (dwt_bytes(64, 32, 2) + 2 * dwt_bytes(32, 16, 2))
+    assert b["mc_add_clip"] == samples * 4 + samples * (4 + 8) + samples * (4 + 16)
+    assert b["upconvert"] == 2 * samples * 10
