@@ -1,0 +1,74 @@
+"""Host-side arithmetic coding of quantised subbands and the entropy-correction factors.
+
+``code_bands`` wraps dgpu_code_bands_host: the bytes the reference's band coders write
+(CompCompressor::Compress, libdirac_encoder/comp_compress.cpp:64-140) from the signed quantised
+indices the device path produces.  ``EntropyCorrector`` wraps dgpu_entropy_*: the reference's
+EntropyCorrector (libdirac_common/common.cpp:57-151), whose factors, adapted from the coded
+byte counts, make the device encoder choose quantisers as the stock reference encoder does.
+No GPU is used here.
+"""
+import numpy as np
+
+from . import _lib
+
+
+def code_bands(intra, depth, qindex, bands, ncb, cb_skip):
+    """Codes components.  qindex: list of int32 [ch][cw] arrays; bands: per component
+    [3*depth+1][>=2] (quantiser index, skip, ...), e.g. DGPU_ENC_BANDS; ncb: per component the
+    [nb][2] code-block counts; cb_skip: per component the flags.  intra / depth: one value or
+    one per component.  Returns (data bytes, band_bytes per component)."""
+    lib = _lib.load()
+    n = len(qindex)
+    intra = list(intra) if hasattr(intra, "__len__") else [int(intra)] * n
+    depth = list(depth) if hasattr(depth, "__len__") else [int(depth)] * n
+    q = [np.ascontiguousarray(a, np.int32) for a in qindex]
+    b = [np.asarray(x, np.int32).reshape(3 * d + 1, -1) for x, d in zip(bands, depth)]
+    bq = np.ascontiguousarray(np.concatenate([x[:, 0] for x in b]), np.int32)
+    bs = np.ascontiguousarray(np.concatenate([x[:, 1] for x in b]), np.int32)
+    nc = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32).ravel() for x in ncb]), np.int32)
+    cbs = np.ascontiguousarray(np.concatenate([np.asarray(x, np.uint8).ravel() for x in cb_skip]), np.uint8)
+    nbytes = np.zeros(bq.size, np.int32)
+    cap = sum(a.size for a in q) * 4 + 4096
+    while True:
+        out = np.zeros(cap, np.uint8)
+        rc = lib.dgpu_code_bands_host(
+            n, _lib.int_array(intra), _lib.int_array(depth), _lib.ptr_array([a.ctypes.data for a in q]),
+            _lib.int_array([a.shape[1] for a in q]), _lib.int_array([a.shape[0] for a in q]),
+            nc.ctypes.data_as(_lib.P_int), bq.ctypes.data_as(_lib.P_int), bs.ctypes.data_as(_lib.P_int),
+            cbs.ctypes.data, out.ctypes.data, cap, nbytes.ctypes.data_as(_lib.P_int))
+        if rc == -2:
+            cap = int(nbytes.sum()) + 16
+            continue
+        _lib.check(rc, "dgpu_code_bands_host")
+        break
+    per, k = [], 0
+    for d in depth:
+        per.append(nbytes[k:k + 3 * d + 1].copy())
+        k += 3 * d + 1
+    return out[:int(nbytes.sum())].copy(), per
+
+
+class EntropyCorrector:
+    """The reference's EntropyCorrector for one sequence (transform depth fixed)."""
+
+    def __init__(self, depth):
+        self.lib = _lib.load()
+        self.depth = depth
+        self.nb = 3 * depth + 1
+        self.state = np.zeros(9 * self.nb, np.float32)
+        _lib.check(self.lib.dgpu_entropy_init(depth, self.state.ctypes.data), "dgpu_entropy_init")
+
+    def factors(self, intra, is_b):
+        """[3][3*depth+1] factors for a picture (the ecf argument of code_next)."""
+        out = np.zeros((3, self.nb), np.float32)
+        _lib.check(self.lib.dgpu_entropy_factors(self.depth, self.state.ctypes.data, int(bool(intra)), int(bool(is_b)),
+                                                 out.ctypes.data), "dgpu_entropy_factors")
+        return out
+
+    def update(self, intra, is_b, comp, band_skip, est_bits, band_bytes):
+        sk = np.ascontiguousarray(band_skip, np.int32)
+        eb = np.ascontiguousarray(est_bits, np.int32)
+        bb = np.ascontiguousarray(band_bytes, np.int32)
+        _lib.check(self.lib.dgpu_entropy_update(self.depth, self.state.ctypes.data, int(bool(intra)), int(bool(is_b)),
+                                                comp, sk.ctypes.data_as(_lib.P_int), eb.ctypes.data_as(_lib.P_int),
+                                                bb.ctypes.data_as(_lib.P_int)), "dgpu_entropy_update")

@@ -475,6 +475,40 @@ int dgpu_encoder_group_destroy(void* group);
 int dgpu_encoder_group_estimate(void* group, int* ntasks);
 
 /* ---------------------------------------------------------------------------------------
+ * Arithmetic coding of quantised subbands on the host, and entropy-correction factors.
+ * dgpu_code_bands_host replaces the entropy coding of the reference's band coders
+ * (CompCompressor::Compress, libdirac_encoder/comp_compress.cpp:64-140; GenericBandCodec /
+ * IntraDCBandCodec, libdirac_common/band_codec_template.h:24-200, band_codec.cpp:81-96;
+ * ArithCodecBase, arith_codec.h:65-360, arith_codec.cpp:40-120): the same bytes, from the
+ * signed quantised indices instead of the coefficients.  No GPU use; the bands are coded in
+ * parallel on the library's host threads.
+ *
+ * n components; qindex[c] (HOST, dense cw[c] x ch[c] int32): the signed quantised indices
+ * as dgpu_code_residue_batch writes them (DGPU_ENC_QINDEX; the intra DC band its prediction
+ * residues' indices).  Per band, components concatenated in band-list order: band_ncb,
+ * band_qidx, band_skip (as for dgpu_code_residue_batch); cb_skip: the code-block skip flags
+ * (host, as it writes them).  out (out_cap bytes) receives every coded band's data (the bytes
+ * the reference's SubbandByteIO carries after its header), component by component, each
+ * component's bands from the DC band down (the reference's coding order); band_bytes[g] is
+ * band g's length (0 when skipped).  DGPU_ERR_SIZE when out is too small (band_bytes is still
+ * filled, so a caller can size the buffer).
+ *
+ * EntropyCorrector (libdirac_common/common.cpp:57-151): state holds [3][3][3*depth+1] floats
+ * (picture kind: intra, B, other inter; component; band).  dgpu_entropy_factors gives the
+ * [3][3*depth+1] factors dgpu_encoder_code_next takes for a picture; dgpu_entropy_update
+ * applies one coded component's bands (EntropyCorrector::Update with the quantiser's estimated
+ * bits, DGPU_ENC_BANDS, and 8 x the coded bytes).
+ * ------------------------------------------------------------------------------------- */
+int dgpu_code_bands_host(int n, const int* intra, const int* depth, const int32_t* const* qindex,
+                         const int* cw, const int* ch, const int* band_ncb, const int* band_qidx,
+                         const int* band_skip, const uint8_t* cb_skip, uint8_t* out, size_t out_cap,
+                         int* band_bytes);
+int dgpu_entropy_init(int depth, float* state);
+int dgpu_entropy_factors(int depth, const float* state, int intra, int is_b, float* ecf);
+int dgpu_entropy_update(int depth, float* state, int intra, int is_b, int comp, const int* band_skip,
+                        const int* est_bits, const int* band_bytes);
+
+/* ---------------------------------------------------------------------------------------
  * Sequence decoder: the data-parallel part of PictureDecompressor::Decompress
  * (libdirac_decoder/picture_decompress.cpp:73-212) and of the frame output of dirac_parse
  * (set_frame_component, libdirac_decoder/dirac_parser.cpp:159-226): dequantisation (as

@@ -23,6 +23,8 @@
 #include <libdirac_encoder/quant_chooser.h>
 #include <libdirac_encoder/comp_compress.h>
 #include <libdirac_byteio/component_byteio.h>
+#include <libdirac_byteio/subband_byteio.h>
+#include <libdirac_common/band_codec.h>
 
 using namespace dirac;
 
@@ -294,9 +296,51 @@ int ref_motion_estimate(int cformat, int w, int h, int luma_depth, int chroma_de
 // coeff (ch x cw) is read and overwritten with the reconstruction.  Per band (band-list
 // order, 1-based band b at index b-1): quantiser index, skip flag, weight, entropy factor,
 // estimated bits, code-block grid (x, y) and the code blocks' skip flags (concatenated).
-int ref_code_residue(int cformat, int w, int h, int comp, int intra, int filter, int depth, int* coeff, int cw,
-                     int ch, float lambda, float cpd_scale, int* band_qidx, int* band_skip, double* band_wt,
-                     float* band_ecf, int* band_bits, int* band_ncb, unsigned char* cb_skip) {
+}  // extern "C"
+
+namespace {
+
+// The band loop of CompCompressor::Compress (comp_compress.cpp:64-140) with each band's coded
+// data captured: the same codec per band (IntraDCBandCodec for an intra DC band,
+// LFBandCodec for the other low-frequency bands, BandCodec otherwise), coding the bands from
+// DC to HF; skipped bands set to zero.  band_data receives the bands' data (the bytes their
+// SubbandByteIO carries after its header) in that order; band_bytes[b - 1] their lengths.
+int code_bands_capture(CoeffArray& c, SubbandList& bands, bool intra, unsigned char* band_data, long long cap,
+                       int* band_bytes) {
+    long long at = 0;
+    for (int b = bands.Length(); b >= 1; --b) {
+        band_bytes[b - 1] = 0;
+        if (bands(b).Skipped()) {
+            for (int j = bands(b).Yp(); j < bands(b).Yp() + bands(b).Yl(); ++j)
+                for (int i = bands(b).Xp(); i < bands(b).Xp() + bands(b).Xl(); ++i) c[j][i] = 0;
+            continue;
+        }
+        SubbandByteIO sb(bands(b));
+        BandCodec* bc;
+        if (b >= bands.Length() - 3) {
+            if (intra && b == bands.Length())
+                bc = new IntraDCBandCodec(&sb, TOTAL_COEFF_CTXS, bands);
+            else
+                bc = new LFBandCodec(&sb, TOTAL_COEFF_CTXS, bands, b, intra);
+        } else {
+            bc = new BandCodec(&sb, TOTAL_COEFF_CTXS, bands, b, intra);
+        }
+        const int n = bc->Compress(c);
+        delete bc;
+        const std::string data = sb.ByteIO::GetBytes();
+        if ((long long)data.size() != n) return -2;
+        if (at + n > cap) return -3;
+        std::memcpy(band_data + at, data.data(), n);
+        at += n;
+        band_bytes[b - 1] = n;
+    }
+    return 0;
+}
+
+int code_residue_impl(int cformat, int w, int h, int comp, int intra, int filter, int depth, int* coeff, int cw,
+                      int ch, float lambda, float cpd_scale, int* band_qidx, int* band_skip, double* band_wt,
+                      float* band_ecf, int* band_bits, int* band_ncb, unsigned char* cb_skip,
+                      unsigned char* band_data, long long cap, int* band_bytes) {
     try {
         const ChromaFormat cf = (ChromaFormat)cformat;
         const PictureType pt = intra ? INTRA_PICTURE : INTER_PICTURE;
@@ -373,15 +417,43 @@ int ref_code_residue(int cformat, int w, int h, int comp, int intra, int filter,
             for (int j = 0; j < cbs.LengthY(); ++j)
                 for (int i = 0; i < cbs.LengthX(); ++i) cb_skip[k++] = cbs[j][i].Skipped() ? 1 : 0;
         }
-        CompCompressor cc(ep, pp);
-        ComponentByteIO* out = cc.Compress(c, bands, (CompSort)comp, est_bits);
-        delete out;
+        if (band_data) {
+            const int rc = code_bands_capture(c, bands, intra != 0, band_data, cap, band_bytes);
+            if (rc) {
+                delete ec;
+                return rc;
+            }
+        } else {
+            CompCompressor cc(ep, pp);
+            ComponentByteIO* out = cc.Compress(c, bands, (CompSort)comp, est_bits);
+            delete out;
+        }
         read_arr(c, coeff);
         delete ec;
         return 0;
     } catch (...) {
         return -1;
     }
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_code_residue(int cformat, int w, int h, int comp, int intra, int filter, int depth, int* coeff, int cw,
+                     int ch, float lambda, float cpd_scale, int* band_qidx, int* band_skip, double* band_wt,
+                     float* band_ecf, int* band_bits, int* band_ncb, unsigned char* cb_skip) {
+    return code_residue_impl(cformat, w, h, comp, intra, filter, depth, coeff, cw, ch, lambda, cpd_scale, band_qidx,
+                             band_skip, band_wt, band_ecf, band_bits, band_ncb, cb_skip, nullptr, 0, nullptr);
+}
+
+// As ref_code_residue, and each coded band's arithmetic-coded data captured (DC band first).
+int ref_code_residue_bytes(int cformat, int w, int h, int comp, int intra, int filter, int depth, int* coeff, int cw,
+                           int ch, float lambda, float cpd_scale, int* band_qidx, int* band_skip, double* band_wt,
+                           float* band_ecf, int* band_bits, int* band_ncb, unsigned char* cb_skip,
+                           unsigned char* band_data, long long cap, int* band_bytes) {
+    return code_residue_impl(cformat, w, h, comp, intra, filter, depth, coeff, cw, ch, lambda, cpd_scale, band_qidx,
+                             band_skip, band_wt, band_ecf, band_bits, band_ncb, cb_skip, band_data, cap, band_bytes);
 }
 
 }  // extern "C"

@@ -3,7 +3,7 @@
 Needs oracle/_ref/libdirac_ref.so (the reference's own C++, plain-C build, compiled from
 its sources by `make -C oracle`).  Inputs are seeded, so re-running reproduces the files.
 
-    python tests/golden/make_golden.py [dwt convert mc me quant encode decode]
+    python tests/golden/make_golden.py [dwt convert mc me quant encode decode adaptive bands]
 """
 import os
 import sys
@@ -219,14 +219,67 @@ def decode_cases():
     return out
 
 
+def adaptive_cases():
+    """The stock reference encoder (entropy-correction factors adapted from its arithmetic
+    coder's byte counts, as it ships) on each ENCODE_CASES sequence: CRC-32 of every locally
+    decoded plane and the picture types."""
+    import zlib
+
+    from oracle import reference_encode
+
+    out = {}
+    for case in ENCODE_CASES:
+        seq, cfg = encode_inputs(case)
+        rec, ptype, _ = reference_encode(cfg, seq, freeze=False)
+        name = case[0]
+        out[name + "_crc"] = np.array([[zlib.crc32(np.ascontiguousarray(p).tobytes()) for p in f] for f in rec],
+                                      np.uint32)
+        out[name + "_ptype"] = ptype
+    return out
+
+
+def band_cases(ref):
+    """The reference's band coders on seeded components (intra and inter, several filters,
+    depths and sizes): the quantiser choices and the CRC-32 and length of every coded band's
+    data, with the inputs to rebuild them (seed, size, filter, depth, lambda)."""
+    import zlib
+
+    out = {}
+    for k, (intra, filt, depth, w, h, lam) in enumerate(BAND_CASES):
+        rng = np.random.default_rng(900 + k)
+        pic = rng.integers(-60, 60, size=(h, w)).astype(np.int16)
+        co = ref.dwt_forward(filt, depth, pic)
+        r = ref.code_residue_bytes(2, w, h, 0, intra, filt, depth, co, lam)
+        start = 0
+        crcs = []
+        for b in range(3 * depth + 1, 0, -1):  # coding order, DC band first
+            n = int(r["band_bytes"][b - 1])
+            crcs.append(zlib.crc32(r["data"][start:start + n].tobytes()))
+            start += n
+        out[f"c{k}_band_bytes"] = r["band_bytes"]
+        out[f"c{k}_band_crc"] = np.array(crcs[::-1], np.uint32)  # band-list order
+        out[f"c{k}_qidx"] = r["qidx"]
+        out[f"c{k}_skip"] = r["skip"]
+        out[f"c{k}_wt"] = r["wt"]
+        out[f"c{k}_ecf"] = r["ecf"]
+        out[f"c{k}_ncb"] = r["ncb"]
+        out[f"c{k}_cb_skip"] = r["cb_skip"]
+    return out
+
+
+# (intra, filter, depth, width, height, lambda) of band_cases
+BAND_CASES = [(1, 1, 4, 176, 144, 5.0), (0, 0, 4, 176, 144, 30.0), (1, 6, 3, 88, 72, 3.0),
+              (0, 2, 5, 352, 288, 100.0), (1, 3, 2, 64, 48, 1.0), (0, 4, 3, 96, 80, 8.0)]
+
+
 def main(argv=None):
     """Writes the named fixtures (default: all)."""
     names = (argv if argv is not None else sys.argv[1:]) or ["dwt", "convert", "mc", "me", "quant", "encode",
-                                                              "decode"]
+                                                              "decode", "adaptive", "bands"]
     ref = Reference()
     makers = {"dwt": lambda: dwt_cases(ref), "convert": lambda: conv_cases(ref), "mc": lambda: mc_cases(ref),
               "me": lambda: me_cases(ref), "quant": lambda: quant_cases(ref), "encode": encode_cases,
-              "decode": decode_cases}
+              "decode": decode_cases, "adaptive": adaptive_cases, "bands": lambda: band_cases(ref)}
     for n in names:
         np.savez_compressed(os.path.join(HERE, n + ".npz"), **makers[n]())
     print("wrote " + ", ".join(n + ".npz" for n in names))

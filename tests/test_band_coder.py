@@ -1,0 +1,153 @@
+"""The host arithmetic coder of quantised subbands (dgpu_code_bands_host) and the
+entropy-correction factors (dgpu_entropy_*) against the reference, without a GPU.
+
+Band data: for seeded components (intra and inter, several filters, depths and sizes) the
+coder, given the oracle's quantised indices for the reference's quantiser choices, writes the
+bytes the reference's band coders write (tests/golden/bands.npz: CRC-32 and length of every
+band's data, made through the reference's own BandCodec / IntraDCBandCodec; live comparison
+where oracle/_ref exists).  Whole loop: the oracle's restated coding loop, with the
+entropy-correction factors adapted from this coder's byte counts, reproduces the stock
+reference encoder (adaptive factors, as it ships) picture for picture
+(tests/golden/adaptive.npz)."""
+import os
+import sys
+import zlib
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+from make_golden import BAND_CASES, ENCODE_CASES, encode_inputs  # noqa: E402
+
+
+def band_inputs(oracle, golden, k):
+    intra, filt, depth, w, h, lam = BAND_CASES[k]
+    g = golden("bands.npz")
+    rng = np.random.default_rng(900 + k)
+    pic = rng.integers(-60, 60, size=(h, w)).astype(np.int16)
+    co = oracle.dwt_forward(filt, depth, pic)
+    _, q, sk, bits, cbs, qo = oracle.code_residue(intra, depth, co, lam, g[f"c{k}_wt"].astype(np.float32),
+                                                  g[f"c{k}_ecf"], g[f"c{k}_ncb"])
+    return intra, depth, q, sk, cbs, qo, g
+
+
+@pytest.mark.parametrize("k", range(len(BAND_CASES)))
+def test_band_data_matches_reference_fixture(oracle, golden, k):
+    from dirac_b200.entropy import code_bands
+
+    intra, depth, q, sk, cbs, qo, g = band_inputs(oracle, golden, k)
+    np.testing.assert_array_equal(sk, g[f"c{k}_skip"])
+    np.testing.assert_array_equal(q[sk == 0], g[f"c{k}_qidx"][sk == 0])
+    np.testing.assert_array_equal(cbs, g[f"c{k}_cb_skip"])
+    data, per = code_bands(intra, depth, [qo], [np.stack([q, sk], 1)], [g[f"c{k}_ncb"]], [cbs])
+    np.testing.assert_array_equal(per[0], g[f"c{k}_band_bytes"])
+    crc, start = [], 0
+    for b in range(3 * depth + 1, 0, -1):
+        n = int(per[0][b - 1])
+        crc.append(zlib.crc32(data[start:start + n].tobytes()))
+        start += n
+    np.testing.assert_array_equal(np.array(crc[::-1], np.uint32), g[f"c{k}_band_crc"])
+
+
+def test_band_data_matches_live_reference(oracle):
+    from dirac_b200.entropy import code_bands
+    from oracle import Reference
+
+    if not Reference.available():
+        pytest.skip("reference library not built here")
+    ref = Reference()
+    rng = np.random.default_rng(77)
+    for intra, filt, depth, w, h, lam, comp in [(1, 0, 4, 160, 96, 2.0, 1), (0, 6, 3, 120, 72, 12.0, 2)]:
+        pic = rng.integers(-90, 90, size=(h, w)).astype(np.int16)
+        co = oracle.dwt_forward(filt, depth, pic)
+        r = ref.code_residue_bytes(2, 2 * w if comp else w, 2 * h if comp else h, comp, intra, filt, depth, co, lam)
+        _, q, sk, _, cbs, qo = oracle.code_residue(intra, depth, co, lam, r["wt"].astype(np.float32), r["ecf"],
+                                                   r["ncb"])
+        data, per = code_bands(intra, depth, [qo], [np.stack([q, sk], 1)], [r["ncb"]], [cbs])
+        np.testing.assert_array_equal(per[0], r["band_bytes"])
+        np.testing.assert_array_equal(data, r["data"])
+
+
+def adaptive_encode(case):
+    """The oracle's coding loop with factors adapted from dgpu_code_bands_host's byte counts."""
+    from dirac_b200 import quant, synth
+    from dirac_b200.entropy import EntropyCorrector, code_bands
+    from oracle_encoder import OracleEncoder
+
+    seq, rcfg = encode_inputs(case)
+    cfg = {k: v for k, v in rcfg.items() if k != "video_format"}
+    cfg.update(luma_depth=8, chroma_depth=8)
+    depth = cfg["wlt_depth"]
+    ec = EntropyCorrector(depth)
+    enc = OracleEncoder(cfg, quant.band_weights, quant.code_blocks, ecf_fn=lambda p: ec.factors(p.intra, p.is_b()))
+    for f in seq:
+        enc.load([synth.to_signed(x) for x in f])
+    enc.end_sequence()
+    ncb = quant.code_blocks(depth, cfg["width"], cfg["height"])
+    while True:
+        p = enc.code_next()
+        if p is None:
+            break
+        r = p.result
+        for c in range(3):
+            _, per = code_bands(p.intra, depth, [r["qindex"][c]], [np.stack([r["qidx"][c], r["skip"][c]], 1)], [ncb],
+                                [r["cb_skip"][c]])
+            ec.update(p.intra, p.is_b(), c, r["skip"][c], r["bits"][c], per[0])
+    return enc
+
+
+@pytest.mark.parametrize("case", ENCODE_CASES, ids=[c[0] for c in ENCODE_CASES])
+def test_adaptive_loop_matches_stock_reference_encoder(golden, case):
+    enc = adaptive_encode(case)
+    g = golden("adaptive.npz")
+    crc = np.array([[zlib.crc32(np.ascontiguousarray((p.astype(np.int32) + 128).astype(np.uint8)).tobytes())
+                     for p in enc.pics[i].data] for i in range(len(enc.pics))], np.uint32)
+    np.testing.assert_array_equal(crc, g[case[0] + "_crc"])
+    np.testing.assert_array_equal([int(enc.pics[i].intra) for i in range(len(enc.pics))], g[case[0] + "_ptype"])
+    # the adapted factors matter: the stock encoder's pictures differ from the frozen-factor ones
+    assert not np.array_equal(g[case[0] + "_crc"], golden("encode.npz")[case[0] + "_crc"])
+
+
+@pytest.mark.parametrize("depth", [1, 3, 4, 6])
+def test_entropy_corrector_initial_factors(depth):
+    from dirac_b200.entropy import EntropyCorrector
+    from oracle_encoder import initial_ecf
+
+    ec = EntropyCorrector(depth)
+    for intra, is_b in [(1, 0), (0, 1), (0, 0)]:
+        f = ec.factors(intra, is_b)
+        for c in range(3):
+            np.testing.assert_array_equal(f[c], initial_ecf(depth, bool(intra)))
+
+
+def test_entropy_corrector_update_rule():
+    """EntropyCorrector::Update: factor *= float(actual bits) / float(estimated bits), for the
+    picture kind (intra, B, other inter) and component given; skipped bands unchanged; a zero
+    count leaves the factor alone."""
+    from dirac_b200.entropy import EntropyCorrector
+
+    ec = EntropyCorrector(1)
+    before = ec.factors(0, 1).copy()
+    ec.update(0, 1, 2, [0, 1, 0, 0], [100, 100, 0, 80], [25, 25, 25, 0])
+    after = ec.factors(0, 1)
+    np.testing.assert_array_equal(after[:2], before[:2])
+    assert after[2, 0] == np.float32(before[2, 0] * np.float32(np.float32(200) / np.float32(100)))
+    assert after[2, 1] == before[2, 1] and after[2, 2] == before[2, 2] and after[2, 3] == before[2, 3]
+    np.testing.assert_array_equal(ec.factors(0, 0), EntropyCorrector(1).factors(0, 0))
+
+
+def test_code_bands_reports_size():
+    """A too-small output buffer returns DGPU_ERR_SIZE with every band's length filled."""
+    import ctypes
+
+    from dirac_b200 import _lib
+
+    q = np.zeros((8, 8), np.int32)
+    q[0, 0] = 3
+    n = np.zeros(4, np.int32)
+    out = np.zeros(1, np.uint8)
+    rc = _lib.load().dgpu_code_bands_host(
+        1, _lib.int_array([1]), _lib.int_array([1]), _lib.ptr_array([q.ctypes.data]), _lib.int_array([8]),
+        _lib.int_array([8]), _lib.int_array([1, 1] * 4), _lib.int_array([0] * 4), _lib.int_array([0] * 4),
+        np.zeros(4, np.uint8).ctypes.data, out.ctypes.data, ctypes.c_size_t(0), n.ctypes.data_as(_lib.P_int))
+    assert rc == -2 and (n > 0).all()
