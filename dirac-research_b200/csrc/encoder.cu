@@ -768,9 +768,31 @@ extern "C" int dgpu_encoder_end_sequence(void* enc) {
     return DGPU_OK;
 }
 
+namespace dgpu {
+namespace {
+int code_next_impl(Encoder* E, const float* ecf, const float* ecf_state, dgpu_picture_info* info);
+}  // namespace
+}  // namespace dgpu
+
 extern "C" int dgpu_encoder_code_next(void* enc, const float* ecf, dgpu_picture_info* info) {
     Encoder* E = static_cast<Encoder*>(enc);
     if (!E) return DGPU_ERR_ARG;
+    return code_next_impl(E, ecf, nullptr, info);
+}
+
+extern "C" int dgpu_encoder_code_next_adaptive(void* enc, const float* ecf_state, dgpu_picture_info* info) {
+    Encoder* E = static_cast<Encoder*>(enc);
+    if (!E || !ecf_state) return DGPU_ERR_ARG;
+    return code_next_impl(E, nullptr, ecf_state, info);
+}
+
+namespace dgpu {
+namespace {
+
+// dgpu_encoder_code_next; with ecf_state, the picture's factors are taken from it once its
+// kind is final (after cut detection): EntropyCorrector::Factor's index, intra 0, B 1, other
+// inter 2 (common.cpp:65-75).
+int code_next_impl(Encoder* E, const float* ecf, const float* ecf_state, dgpu_picture_info* info) {
     if (E->last_read < 0) return 0;
     // a scheduled return to the normal L1 separation (seq_compress.cpp:215-219)
     if (E->L1Sep > 0 && E->L1Sep != E->m_L1_sep && (E->code - 1) % E->L1Sep == 0) E->m_L1_sep = E->L1Sep;
@@ -814,6 +836,7 @@ extern "C" int dgpu_encoder_code_next(void* enc, const float* ecf, dgpu_picture_
         }
     }
     // 16.-19. transform, quantisation, inverse transform
+    if (ecf_state) ecf = ecf_state + (size_t)(p->intra ? 0 : (p->is_b() ? 1 : 2)) * 3 * E->nb;
     rc = code_residue(*E, *p, ecf);
     if (rc) return rc;
     // 20.-21. reconstruction and clip
@@ -845,6 +868,9 @@ extern "C" int dgpu_encoder_code_next(void* enc, const float* ecf, dgpu_picture_
     ++E->code;
     return 1;
 }
+
+}  // namespace
+}  // namespace dgpu
 
 extern "C" size_t dgpu_encoder_item_bytes(void* enc, int pnum, int what, int comp) {
     Encoder* E = static_cast<Encoder*>(enc);

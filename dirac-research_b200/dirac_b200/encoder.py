@@ -112,9 +112,18 @@ class SequenceEncoder:
     def end_sequence(self):
         _lib.check(self.lib.dgpu_encoder_end_sequence(self.handle), "dgpu_encoder_end_sequence")
 
-    def code_next(self, ecf=None):
-        """Codes the next picture in coding order; returns its info dict, or None."""
+    def code_next(self, ecf=None, ecf_state=None):
+        """Codes the next picture in coding order; returns its info dict, or None.  ecf: the
+        picture's [3][3*depth+1] entropy-correction factors; ecf_state: instead, a whole
+        EntropyCorrector state (entropy.EntropyCorrector.state), from which the encoder picks
+        the picture's factors once its kind is final."""
         info = PictureInfo()
+        if ecf_state is not None:
+            st = np.ascontiguousarray(ecf_state, dtype=np.float32)
+            rc = self.lib.dgpu_encoder_code_next_adaptive(self.handle, st.ctypes.data, ctypes.byref(info))
+            if rc < 0:
+                _lib.check(rc, "dgpu_encoder_code_next_adaptive")
+            return info.as_dict() if rc == 1 else None
         e = None
         if ecf is not None:
             e = np.ascontiguousarray(ecf, dtype=np.float32)

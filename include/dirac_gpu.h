@@ -379,6 +379,13 @@ int dgpu_encoder_end_sequence(void* encoder);
  * factors for this picture (the caller's EntropyCorrector::Factor values).  Returns 1 and
  * fills info when a picture was coded, 0 when more input (or nothing) remains. */
 int dgpu_encoder_code_next(void* encoder, const float* ecf, dgpu_picture_info* info);
+/* As dgpu_encoder_code_next, with the caller's whole EntropyCorrector state (the
+ * [3][3][3*depth+1] layout of dgpu_entropy_init): the encoder takes the picture's factors
+ * from it once the picture's kind (intra, B, other inter) is final, cut detection included,
+ * as the reference's quantiser choice does.  With the state adapted after each coded picture
+ * (dgpu_code_bands_host's byte counts, dgpu_entropy_update) the choices are the stock
+ * reference encoder's. */
+int dgpu_encoder_code_next_adaptive(void* encoder, const float* ecf_state, dgpu_picture_info* info);
 size_t dgpu_encoder_item_bytes(void* encoder, int pnum, int what, int comp);
 /* Copies one result of a coded picture to dst (host memory when on_host = 1, else device);
  * bytes must equal dgpu_encoder_item_bytes.  Synchronises the encoder's stream for host

@@ -1,0 +1,58 @@
+"""The device encoder as a drop-in for the stock reference encoder: each picture coded with the
+encoder's whole entropy-correction state (dgpu_encoder_code_next_adaptive), its quantised
+subbands then arithmetic-coded on the host (dgpu_code_bands_host) and the state adapted from
+the byte counts (dgpu_entropy_update), as the reference's CompCompressor does.  The locally
+decoded pictures equal the stock reference encoder's, adaptive factors included
+(tests/golden/adaptive.npz, made through the reference's public encoder API)."""
+import os
+import sys
+import zlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+from make_golden import ENCODE_CASES, encode_inputs  # noqa: E402
+
+
+@pytest.mark.parametrize("case", ENCODE_CASES, ids=[c[0] for c in ENCODE_CASES])
+def test_device_encoder_with_host_coder_matches_stock_reference(gpu, golden, case):
+    from dirac_b200 import encoder as E
+    from dirac_b200 import quant
+    from dirac_b200.encoder import SequenceEncoder
+    from dirac_b200.entropy import EntropyCorrector, code_bands
+    from test_encoder_gpu import encoder_params
+
+    seq, rcfg = encode_inputs(case)
+    cfg = encoder_params(rcfg)
+    depth = cfg["wlt_depth"]
+    ncb = quant.code_blocks(depth, cfg["width"], cfg["height"])
+    ec = EntropyCorrector(depth)
+    enc = SequenceEncoder(cfg, max_pictures=len(seq))
+    for f in seq:
+        enc.load(f)
+    enc.end_sequence()
+    outputs, ptype = {}, {}
+    while True:
+        info = enc.code_next(ecf_state=ec.state)
+        if info is None:
+            break
+        pn = info["pnum"]
+        xs = 1
+        for c in range(3):
+            bands = enc.read(pn, E.BANDS, c).reshape(-1, 3)
+            q = enc.read(pn, E.QINDEX, c)
+            cw = ((cfg["width"] >> (xs if c else 0)) + (1 << depth) - 1) >> depth << depth
+            _, per = code_bands(info["intra"], depth, [q.reshape(-1, cw)], [bands], [ncb],
+                                [enc.read(pn, E.CBSKIP, c)])
+            ec.update(info["intra"], info["is_b"], c, bands[:, 1], bands[:, 2], per[0])
+        outputs[pn] = [enc.read(pn, E.OUTPUT, c) for c in range(3)]
+        ptype[pn] = info["intra"]
+    enc.close()
+    g = golden("adaptive.npz")
+    crc = np.array([[zlib.crc32(np.ascontiguousarray(outputs[i][c]).tobytes()) for c in range(3)]
+                    for i in range(len(seq))], np.uint32)
+    np.testing.assert_array_equal(crc, g[case[0] + "_crc"])
+    np.testing.assert_array_equal([ptype[i] for i in range(len(seq))], g[case[0] + "_ptype"])
