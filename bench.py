@@ -338,6 +338,29 @@ def run_hetero(args, peak, peaks):
     return out
 
 
+def host_band_coding(pictures, depth, ncb):
+    """Throughput of the host arithmetic coder (dgpu_code_bands_host, every band of a picture in
+    parallel on the library's host threads) over coded pictures [(intra, qindex planes, band
+    tables, code-block flags)]: pictures/s and bytes per picture."""
+    from dirac_b200.entropy import code_bands
+
+    def run():
+        total = 0
+        for intra, q, bands, cbs in pictures:
+            data, _ = code_bands([intra] * 3, [depth] * 3, q, bands, [ncb] * 3, cbs)
+            total += data.size
+        return total
+
+    run()  # warm-up (host threads, allocator)
+    t0 = time.perf_counter()
+    total = run()
+    dt = time.perf_counter() - t0
+    return {"value": len(pictures) / dt, "unit": "pictures/s", "bytes_per_picture": total / len(pictures),
+            "host_threads": min(16, os.cpu_count() or 1),
+            "form": "the subbands of the plain form's coded 1080p pictures arithmetic-coded on the host "
+                    "(bytes equal to the reference's band coders'), one call per picture"}
+
+
 def run_decoding(args, enc, infos, peak, cpu_decode=None):
     """The decoding leg: the 1080p sequence the plain form coded, decoded by the device decoder
     (dgpu_decoder_*) from its quantised indices, band and code-block choices and motion data, in
@@ -359,7 +382,7 @@ def run_decoding(args, enc, infos, peak, cpu_decode=None):
     m = 1 << PARAMS["wlt_depth"]
     sizes = [(PARAMS["height"], PARAMS["width"]), (PARAMS["height"] // 2, PARAMS["width"] // 2)]
     shapes = [tuple((x + m - 1) // m * m for x in sizes[min(c, 1)]) for c in range(3)]
-    dev, host, want, pnums = [], [], [], []
+    dev, host, want, pnums, coded = [], [], [], [], []
     keep = []
     h2d = 0
     for info in infos:
@@ -375,6 +398,7 @@ def run_decoding(args, enc, infos, peak, cpu_decode=None):
             mot = {"mv": [mv[k] for k in range(len(refs))], "mode": enc.read(pn, E.MODE), "dc": enc.read(pn, E.DC),
                    "split": enc.read(pn, E.SPLIT)}
         want.append([enc.read(pn, E.OUTPUT, c) for c in range(3)])
+        coded.append((info["intra"], q, bands, [enc.read(pn, E.CBSKIP, c) for c in range(3)]))
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
         hq, hc = [pin(a) for a in q], pin(cbs)
         hm = None if mot is None else {"mv": [pin(v) for v in mot["mv"]],
@@ -460,6 +484,10 @@ def run_decoding(args, enc, infos, peak, cpu_decode=None):
         if t_cpu > 10.0 or k + 1 >= 8:
             break
     ncpu = len(done)
+    try:
+        coding = host_band_coding(coded, PARAMS["wlt_depth"], ncb)
+    except Exception as e:  # the coder's measurement must not cost the decoding line
+        coding = {"error": repr(e)}
     port = {"value": ncpu / t_cpu, "unit": "frames/s", "cores": 1, "kind": "port",
             "sample": f"the oracle's plain-C restatement of the decoder (dequantisation, inverse transform, motion "
                       f"compensation, clip) on the first {ncpu} pictures in coding order: {t_cpu:.2f} s on 1 core"}
@@ -472,7 +500,7 @@ def run_decoding(args, enc, infos, peak, cpu_decode=None):
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
                          "algorithmic_bytes_per_step": alg},
-            "cpu_baseline": baseline, "cpu_port": port,
+            "cpu_baseline": baseline, "cpu_port": port, "host_band_coding": coding,
             "workload": "decode of the plain form's coded 1920x1080 4:2:0 8-bit 32-picture sequence from its "
                         "quantised indices (int32), band and code-block choices and motion data; output 8-bit "
                         "samples"}
