@@ -145,6 +145,7 @@ struct Encoder {
     int code = 0;                // m_current_code_pnum
     int cur = -1;                // m_current_display_pnum
     int last_read = -1;          // m_last_picture_read
+    int prepared = -1;           // picture prepared by dgpu_encoder_prepare_next, or -1
     bool eos = false;            // m_eos_signalled
     std::map<int, Pic> pics;
 
@@ -448,7 +449,9 @@ float comp_lambda(const Encoder& E, const Pic& p, int comp) {
     return component_lambda(E.L, p.intra, p.is_b(), p.ratio, comp);
 }
 
-int code_residue(Encoder& E, Pic& p, const float* ecf_in) {
+// Transform (unless done already, forward_done), quantiser choice and quantisation, inverse
+// transform.
+int code_residue(Encoder& E, Pic& p, const float* ecf_in, bool forward_done = false) {
     Slot& s = slot_of(E, p);
     const int depth = E.P.wlt_depth;
     const int filter = p.intra ? E.P.intra_filter : E.P.inter_filter;
@@ -477,7 +480,7 @@ int code_residue(Encoder& E, Pic& p, const float* ecf_in) {
     p.cb_skip.assign((size_t)3 * E.ncb_total, 0);
     int32_t* coeff[3] = {s.coeff[0], s.coeff[1], s.coeff[2]};
     int32_t* qout[3] = {s.qout[0], s.qout[1], s.qout[2]};
-    int rc = transform(E, p, DGPU_FORWARD, filter);
+    int rc = forward_done ? DGPU_OK : transform(E, p, DGPU_FORWARD, filter);
     if (rc) return rc;
     {
         StageTimer timer(E, DGPU_STAGE_QUANT);
@@ -740,6 +743,7 @@ extern "C" int dgpu_encoder_reset(void* enc) {
     E->code = 0;
     E->cur = -1;
     E->last_read = -1;
+    E->prepared = -1;
     E->eos = false;
     return DGPU_OK;
 }
@@ -771,8 +775,22 @@ extern "C" int dgpu_encoder_end_sequence(void* enc) {
 namespace dgpu {
 namespace {
 int code_next_impl(Encoder* E, const float* ecf, const float* ecf_state, dgpu_picture_info* info);
+int prepare_impl(Encoder* E, dgpu_picture_info* info);
+int finish_impl(Encoder* E, const float* ecf, const float* ecf_state, dgpu_picture_info* info);
 }  // namespace
 }  // namespace dgpu
+
+extern "C" int dgpu_encoder_prepare_next(void* enc, dgpu_picture_info* info) {
+    Encoder* E = static_cast<Encoder*>(enc);
+    if (!E) return DGPU_ERR_ARG;
+    return prepare_impl(E, info);
+}
+
+extern "C" int dgpu_encoder_finish_next(void* enc, const float* ecf, const float* ecf_state, dgpu_picture_info* info) {
+    Encoder* E = static_cast<Encoder*>(enc);
+    if (!E) return DGPU_ERR_ARG;
+    return finish_impl(E, ecf, ecf_state, info);
+}
 
 extern "C" int dgpu_encoder_code_next(void* enc, const float* ecf, dgpu_picture_info* info) {
     Encoder* E = static_cast<Encoder*>(enc);
@@ -792,7 +810,15 @@ namespace {
 // dgpu_encoder_code_next; with ecf_state, the picture's factors are taken from it once its
 // kind is final (after cut detection): EntropyCorrector::Factor's index, intra 0, B 1, other
 // inter 2 (common.cpp:65-75).
-int code_next_impl(Encoder* E, const float* ecf, const float* ecf_state, dgpu_picture_info* info) {
+// Steps of a picture's coding that do not depend on the entropy-correction factors: picture
+// types, motion estimation, intra analysis, the P-only switch and cut detection, motion
+// compensation SUBTRACT and the forward transform.  Returns 1 with the picture's provisional
+// info (its kind is final), 0 when more input is needed.
+int prepare_impl(Encoder* E, dgpu_picture_info* info) {
+    if (E->prepared >= 0) {  // already prepared
+        if (info) *info = E->pics[E->prepared].info;
+        return 1;
+    }
     if (E->last_read < 0) return 0;
     // a scheduled return to the normal L1 separation (seq_compress.cpp:215-219)
     if (E->L1Sep > 0 && E->L1Sep != E->m_L1_sep && (E->code - 1) % E->L1Sep == 0) E->m_L1_sep = E->L1Sep;
@@ -835,9 +861,36 @@ int code_next_impl(Encoder* E, const float* ecf, const float* ecf_state, dgpu_pi
             if (rc) return rc;
         }
     }
-    // 16.-19. transform, quantisation, inverse transform
+    // 16. forward transform
+    rc = transform(*E, *p, DGPU_FORWARD, p->intra ? E->P.intra_filter : E->P.inter_filter);
+    if (rc) return rc;
+    dgpu_picture_info& I = p->info;
+    I.pnum = p->pnum;
+    I.coded_num = E->code;
+    I.intra = p->intra ? 1 : 0;
+    I.is_ref = p->is_ref ? 1 : 0;
+    I.cut = p->cut ? 1 : 0;
+    I.num_refs = (int)p->refs.size();
+    I.ref1 = p->refs.size() > 0 ? p->refs[0] : -1;
+    I.ref2 = p->refs.size() > 1 ? p->refs[1] : -1;
+    I.is_b = p->is_b() ? 1 : 0;
+    I.intra_ratio = p->ratio;
+    I.filter = p->intra ? E->P.intra_filter : E->P.inter_filter;
+    E->prepared = p->pnum;
+    if (info) *info = I;
+    return 1;
+}
+
+// The rest of the prepared picture's coding: quantiser choice with the given factors (or the
+// picture kind's factors from ecf_state), quantisation, inverse transform, reconstruction.
+int finish_impl(Encoder* E, const float* ecf, const float* ecf_state, dgpu_picture_info* info) {
+    if (E->prepared < 0) return DGPU_ERR_ARG;
+    Pic* p = &E->pics[E->prepared];
+    E->prepared = -1;
+    int rc;
+    // 17.-19. quantisation, inverse transform
     if (ecf_state) ecf = ecf_state + (size_t)(p->intra ? 0 : (p->is_b() ? 1 : 2)) * 3 * E->nb;
-    rc = code_residue(*E, *p, ecf);
+    rc = code_residue(*E, *p, ecf, true);
     if (rc) return rc;
     // 20.-21. reconstruction and clip
     if (!p->intra) {
@@ -853,20 +906,15 @@ int code_next_impl(Encoder* E, const float* ecf, const float* ecf_state, dgpu_pi
     }
     p->up_valid = false;
     p->coded = true;
-    dgpu_picture_info& I = p->info;
-    I.pnum = p->pnum;
-    I.coded_num = E->code;
-    I.intra = p->intra ? 1 : 0;
-    I.is_ref = p->is_ref ? 1 : 0;
-    I.cut = p->cut ? 1 : 0;
-    I.num_refs = (int)p->refs.size();
-    I.ref1 = p->refs.size() > 0 ? p->refs[0] : -1;
-    I.ref2 = p->refs.size() > 1 ? p->refs[1] : -1;
-    I.is_b = p->is_b() ? 1 : 0;
-    I.intra_ratio = p->ratio;
-    if (info) *info = I;
+    if (info) *info = p->info;
     ++E->code;
     return 1;
+}
+
+int code_next_impl(Encoder* E, const float* ecf, const float* ecf_state, dgpu_picture_info* info) {
+    const int rc = prepare_impl(E, nullptr);
+    if (rc != 1) return rc;
+    return finish_impl(E, ecf, ecf_state, info);
 }
 
 }  // namespace

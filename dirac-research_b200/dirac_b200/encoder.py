@@ -132,6 +132,26 @@ class SequenceEncoder:
             _lib.check(rc, "dgpu_encoder_code_next")
         return info.as_dict() if rc == 1 else None
 
+    def prepare_next(self):
+        """First half of code_next (no entropy factors needed): returns the prepared picture's
+        info (kind final), or None when more input is needed."""
+        info = PictureInfo()
+        rc = self.lib.dgpu_encoder_prepare_next(self.handle, ctypes.byref(info))
+        if rc < 0:
+            _lib.check(rc, "dgpu_encoder_prepare_next")
+        return info.as_dict() if rc == 1 else None
+
+    def finish_next(self, ecf=None, ecf_state=None):
+        """Second half: quantiser choice with ecf (or the kind's factors from ecf_state),
+        quantisation, reconstruction.  Returns the picture's final info."""
+        info = PictureInfo()
+        e = np.ascontiguousarray(ecf, dtype=np.float32) if ecf is not None else None
+        st = np.ascontiguousarray(ecf_state, dtype=np.float32) if ecf_state is not None else None
+        rc = self.lib.dgpu_encoder_finish_next(self.handle, e.ctypes.data if e is not None else None,
+                                               st.ctypes.data if st is not None else None, ctypes.byref(info))
+        _lib.check(rc if rc < 0 else 0, "dgpu_encoder_finish_next")
+        return info.as_dict()
+
     def read(self, pnum, what, comp=0):
         """One result of a coded picture as a numpy array."""
         n = self.lib.dgpu_encoder_item_bytes(self.handle, pnum, what, comp)

@@ -386,6 +386,17 @@ int dgpu_encoder_code_next(void* encoder, const float* ecf, dgpu_picture_info* i
  * (dgpu_code_bands_host's byte counts, dgpu_entropy_update) the choices are the stock
  * reference encoder's. */
 int dgpu_encoder_code_next_adaptive(void* encoder, const float* ecf_state, dgpu_picture_info* info);
+/* dgpu_encoder_code_next in two halves, so that a caller can arithmetic-code picture n on the
+ * host while the device works on picture n + 1.  prepare_next runs what does not depend on
+ * the entropy-correction factors (picture types, motion estimation, intra analysis, the
+ * P-only switch and cut detection, motion compensation SUBTRACT, the forward transform) and
+ * returns 1 with the picture's info (its kind final; lambdas and cpd scale follow at finish),
+ * 0 when more input is needed; calling it again before finish_next returns the same picture.
+ * finish_next completes it with ecf (as dgpu_encoder_code_next) or, when ecf_state is not
+ * NULL, the kind's factors from that state (as dgpu_encoder_code_next_adaptive); it returns 1
+ * and the final info, DGPU_ERR_ARG when no picture is prepared. */
+int dgpu_encoder_prepare_next(void* encoder, dgpu_picture_info* info);
+int dgpu_encoder_finish_next(void* encoder, const float* ecf, const float* ecf_state, dgpu_picture_info* info);
 size_t dgpu_encoder_item_bytes(void* encoder, int pnum, int what, int comp);
 /* Copies one result of a coded picture to dst (host memory when on_host = 1, else device);
  * bytes must equal dgpu_encoder_item_bytes.  Synchronises the encoder's stream for host

@@ -56,3 +56,65 @@ def test_device_encoder_with_host_coder_matches_stock_reference(gpu, golden, cas
                     for i in range(len(seq))], np.uint32)
     np.testing.assert_array_equal(crc, g[case[0] + "_crc"])
     np.testing.assert_array_equal([ptype[i] for i in range(len(seq))], g[case[0] + "_ptype"])
+
+
+def read_coded(enc, info, cfg):
+    """A coded picture's quantised indices, band tables and code-block flags (host copies)."""
+    from dirac_b200 import encoder as E
+
+    depth = cfg["wlt_depth"]
+    pn = info["pnum"]
+    out = []
+    for c in range(3):
+        cw = ((cfg["width"] >> (1 if c else 0)) + (1 << depth) - 1) >> depth << depth
+        out.append((enc.read(pn, E.QINDEX, c).reshape(-1, cw), enc.read(pn, E.BANDS, c).reshape(-1, 3),
+                    enc.read(pn, E.CBSKIP, c)))
+    return out
+
+
+@pytest.mark.parametrize("case", [ENCODE_CASES[0], ENCODE_CASES[3]], ids=[ENCODE_CASES[0][0], ENCODE_CASES[3][0]])
+def test_pipelined_host_coding_matches_stock_reference(gpu, golden, case):
+    """Picture n's subbands arithmetic-coded on a host thread while the device prepares picture
+    n + 1 (estimation, compensation, transform); n + 1's quantisers chosen after n's byte counts
+    have updated the factors.  Same pictures as the stock reference encoder."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from dirac_b200 import encoder as E
+    from dirac_b200 import quant
+    from dirac_b200.encoder import SequenceEncoder
+    from dirac_b200.entropy import EntropyCorrector, code_bands
+    from test_encoder_gpu import encoder_params
+
+    seq, rcfg = encode_inputs(case)
+    cfg = encoder_params(rcfg)
+    depth = cfg["wlt_depth"]
+    ncb = quant.code_blocks(depth, cfg["width"], cfg["height"])
+    ec = EntropyCorrector(depth)
+    enc = SequenceEncoder(cfg, max_pictures=len(seq))
+    for f in seq:
+        enc.load(f)
+    enc.end_sequence()
+
+    def code_and_adapt(info, comps):
+        for c, (q, bands, cbs) in enumerate(comps):
+            _, per = code_bands(info["intra"], depth, [q], [bands], [ncb], [cbs])
+            ec.update(info["intra"], info["is_b"], c, bands[:, 1], bands[:, 2], per[0])
+
+    outputs, pending = {}, None
+    with ThreadPoolExecutor(1) as ex:
+        while True:
+            fut = ex.submit(code_and_adapt, *pending) if pending else None
+            nxt = enc.prepare_next()
+            if fut:
+                fut.result()
+            if nxt is None:
+                break
+            info = enc.finish_next(ecf_state=ec.state)
+            assert info["pnum"] == nxt["pnum"] and info["intra"] == nxt["intra"]
+            outputs[info["pnum"]] = [enc.read(info["pnum"], E.OUTPUT, c) for c in range(3)]
+            pending = (info, read_coded(enc, info, cfg))
+    enc.close()
+    g = golden("adaptive.npz")
+    crc = np.array([[zlib.crc32(np.ascontiguousarray(outputs[i][c]).tobytes()) for c in range(3)]
+                    for i in range(len(seq))], np.uint32)
+    np.testing.assert_array_equal(crc, g[case[0] + "_crc"])
