@@ -12,11 +12,13 @@ import numpy as np
 from . import _lib
 
 
-def code_bands(intra, depth, qindex, bands, ncb, cb_skip):
-    """Codes components.  qindex: list of int32 [ch][cw] arrays; bands: per component
+def code_bands(intra, depth, qindex, bands, ncb, cb_skip, vlc=False):
+    """Codes components (vlc: the variable-length form, dgpu_code_bands_vlc_host).  qindex: list
+    of int32 [ch][cw] arrays; bands: per component
     [3*depth+1][>=2] (quantiser index, skip, ...), e.g. DGPU_ENC_BANDS; ncb: per component the
     [nb][2] code-block counts; cb_skip: per component the flags.  intra / depth: one value or
-    one per component.  Returns (data bytes, band_bytes per component)."""
+    one per component.  Returns (data bytes, band_bytes per component), and with vlc the exact
+    bit counts per component as a third item."""
     lib = _lib.load()
     n = len(qindex)
     intra = list(intra) if hasattr(intra, "__len__") else [int(intra)] * n
@@ -28,14 +30,15 @@ def code_bands(intra, depth, qindex, bands, ncb, cb_skip):
     nc = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32).ravel() for x in ncb]), np.int32)
     cbs = np.ascontiguousarray(np.concatenate([np.asarray(x, np.uint8).ravel() for x in cb_skip]), np.uint8)
     nbytes = np.zeros(bq.size, np.int32)
+    nbits = np.zeros(bq.size, np.int64)
     cap = sum(a.size for a in q) * 4 + 4096
     while True:
         out = np.zeros(cap, np.uint8)
-        rc = lib.dgpu_code_bands_host(
-            n, _lib.int_array(intra), _lib.int_array(depth), _lib.ptr_array([a.ctypes.data for a in q]),
-            _lib.int_array([a.shape[1] for a in q]), _lib.int_array([a.shape[0] for a in q]),
-            nc.ctypes.data_as(_lib.P_int), bq.ctypes.data_as(_lib.P_int), bs.ctypes.data_as(_lib.P_int),
-            cbs.ctypes.data, out.ctypes.data, cap, nbytes.ctypes.data_as(_lib.P_int))
+        args = [n, _lib.int_array(intra), _lib.int_array(depth), _lib.ptr_array([a.ctypes.data for a in q]),
+                _lib.int_array([a.shape[1] for a in q]), _lib.int_array([a.shape[0] for a in q]),
+                nc.ctypes.data_as(_lib.P_int), bq.ctypes.data_as(_lib.P_int), bs.ctypes.data_as(_lib.P_int),
+                cbs.ctypes.data, out.ctypes.data, cap, nbytes.ctypes.data_as(_lib.P_int)]
+        rc = lib.dgpu_code_bands_vlc_host(*args, nbits.ctypes.data) if vlc else lib.dgpu_code_bands_host(*args)
         if rc == -2:
             cap = int(nbytes.sum()) + 16
             continue
@@ -45,6 +48,12 @@ def code_bands(intra, depth, qindex, bands, ncb, cb_skip):
     for d in depth:
         per.append(nbytes[k:k + 3 * d + 1].copy())
         k += 3 * d + 1
+    if vlc:
+        bits_per, k = [], 0
+        for d in depth:
+            bits_per.append(nbits[k:k + 3 * d + 1].copy())
+            k += 3 * d + 1
+        return out[:int(nbytes.sum())].copy(), per, bits_per
     return out[:int(nbytes.sum())].copy(), per
 
 

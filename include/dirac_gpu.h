@@ -521,6 +521,15 @@ int dgpu_code_bands_host(int n, const int* intra, const int* depth, const int32_
                          const int* cw, const int* ch, const int* band_ncb, const int* band_qidx,
                          const int* band_skip, const uint8_t* cb_skip, uint8_t* out, size_t out_cap,
                          int* band_bytes);
+/* The variable-length form of the band coders (-use_vlc: BandVLC / IntraDCBandVLC over
+ * ArithCodecToVLCAdapter, libdirac_common/band_vlc.cpp:49-100): the same symbols as plain
+ * bits, each band's data padded to a byte.  band_bits (optional) receives each band's exact
+ * bit count (the reference's EntropyCorrector update after a VLC band counts its whole bytes,
+ * 8 * (band_bits / 8)). */
+int dgpu_code_bands_vlc_host(int n, const int* intra, const int* depth, const int32_t* const* qindex,
+                             const int* cw, const int* ch, const int* band_ncb, const int* band_qidx,
+                             const int* band_skip, const uint8_t* cb_skip, uint8_t* out, size_t out_cap,
+                             int* band_bytes, long long* band_bits);
 int dgpu_entropy_init(int depth, float* state);
 int dgpu_entropy_factors(int depth, const float* state, int intra, int is_b, float* ecf);
 int dgpu_entropy_update(int depth, float* state, int intra, int is_b, int comp, const int* band_skip,

@@ -278,6 +278,30 @@ class Reference:
         return {"recon": c, "qidx": q, "skip": sk, "wt": wt, "ecf": ecf, "bits": bits, "ncb": ncb,
                 "cb_skip": cbs[:ncbt].copy()}
 
+    def code_residue_vlc_bytes(self, cformat, w, h, comp, intra, filt, depth, coeff, lambda_, cpd_scale=1.0):
+        """As code_residue_bytes with the variable-length band coders (-use_vlc); also
+        "compress_bytes": what each coder's Compress returned (whole bytes before alignment)."""
+        c = np.array(coeff, dtype=np.int32, copy=True, order="C")
+        ch, cw = c.shape
+        nb = 3 * depth + 1
+        q, sk, bits = np.zeros(nb, np.int32), np.zeros(nb, np.int32), np.zeros(nb, np.int32)
+        wt, ecf = np.zeros(nb, np.float64), np.zeros(nb, np.float32)
+        ncb = np.zeros(2 * nb, np.int32)
+        cbs = np.zeros(1 << 20, np.uint8)
+        cap = 8 * c.size + 4096
+        data = np.zeros(cap, np.uint8)
+        nbytes, whole = np.zeros(nb, np.int32), np.zeros(nb, np.int32)
+        rc = self.lib.ref_code_residue_vlc_bytes(cformat, w, h, comp, intra, filt, depth, _p(c), cw, ch,
+                                                 ctypes.c_float(lambda_), ctypes.c_float(cpd_scale), _p(q), _p(sk),
+                                                 _p(wt), _p(ecf), _p(bits), _p(ncb), _p(cbs), _p(data),
+                                                 ctypes.c_longlong(cap), _p(nbytes), _p(whole))
+        if rc:
+            raise ValueError(f"ref_code_residue_vlc_bytes failed: {rc}")
+        ncbt = int(np.sum(ncb[0::2] * ncb[1::2]))
+        return {"recon": c, "qidx": q, "skip": sk, "wt": wt, "ecf": ecf, "bits": bits, "ncb": ncb,
+                "cb_skip": cbs[:ncbt].copy(), "data": data[:int(nbytes.sum())].copy(), "band_bytes": nbytes,
+                "compress_bytes": whole}
+
     def code_residue_bytes(self, cformat, w, h, comp, intra, filt, depth, coeff, lambda_, cpd_scale=1.0):
         """As code_residue, plus the reference band coders' output: "data" (every coded band's
         arithmetic-coded bytes, DC band first) and "band_bytes" (per band, 0 when skipped)."""

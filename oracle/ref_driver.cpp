@@ -25,6 +25,7 @@
 #include <libdirac_byteio/component_byteio.h>
 #include <libdirac_byteio/subband_byteio.h>
 #include <libdirac_common/band_codec.h>
+#include <libdirac_common/band_vlc.h>
 
 using namespace dirac;
 
@@ -305,8 +306,11 @@ namespace {
 // LFBandCodec for the other low-frequency bands, BandCodec otherwise), coding the bands from
 // DC to HF; skipped bands set to zero.  band_data receives the bands' data (the bytes their
 // SubbandByteIO carries after its header) in that order; band_bytes[b - 1] their lengths.
+// vlc: the variable-length band coders (BandVLC / IntraDCBandVLC, comp_compress.cpp:105-120);
+// compress_bytes (optional) receives what each coder's Compress returned (whole bytes written
+// before the final alignment).
 int code_bands_capture(CoeffArray& c, SubbandList& bands, bool intra, unsigned char* band_data, long long cap,
-                       int* band_bytes) {
+                       int* band_bytes, bool vlc = false, int* compress_bytes = nullptr) {
     long long at = 0;
     for (int b = bands.Length(); b >= 1; --b) {
         band_bytes[b - 1] = 0;
@@ -316,17 +320,31 @@ int code_bands_capture(CoeffArray& c, SubbandList& bands, bool intra, unsigned c
             continue;
         }
         SubbandByteIO sb(bands(b));
-        BandCodec* bc;
-        if (b >= bands.Length() - 3) {
+        int n;
+        if (vlc) {
+            BandVLC* bc;
             if (intra && b == bands.Length())
-                bc = new IntraDCBandCodec(&sb, TOTAL_COEFF_CTXS, bands);
+                bc = new IntraDCBandVLC(&sb, bands);
             else
-                bc = new LFBandCodec(&sb, TOTAL_COEFF_CTXS, bands, b, intra);
+                bc = new BandVLC(&sb, 0, bands, b, intra);
+            const int whole = bc->Compress(c);
+            delete bc;
+            if (compress_bytes) compress_bytes[b - 1] = whole;
+            sb.ByteAlignOutput();
+            n = sb.GetSize();
         } else {
-            bc = new BandCodec(&sb, TOTAL_COEFF_CTXS, bands, b, intra);
+            BandCodec* bc;
+            if (b >= bands.Length() - 3) {
+                if (intra && b == bands.Length())
+                    bc = new IntraDCBandCodec(&sb, TOTAL_COEFF_CTXS, bands);
+                else
+                    bc = new LFBandCodec(&sb, TOTAL_COEFF_CTXS, bands, b, intra);
+            } else {
+                bc = new BandCodec(&sb, TOTAL_COEFF_CTXS, bands, b, intra);
+            }
+            n = bc->Compress(c);
+            delete bc;
         }
-        const int n = bc->Compress(c);
-        delete bc;
         const std::string data = sb.ByteIO::GetBytes();
         if ((long long)data.size() != n) return -2;
         if (at + n > cap) return -3;
@@ -340,7 +358,8 @@ int code_bands_capture(CoeffArray& c, SubbandList& bands, bool intra, unsigned c
 int code_residue_impl(int cformat, int w, int h, int comp, int intra, int filter, int depth, int* coeff, int cw,
                       int ch, float lambda, float cpd_scale, int* band_qidx, int* band_skip, double* band_wt,
                       float* band_ecf, int* band_bits, int* band_ncb, unsigned char* cb_skip,
-                      unsigned char* band_data, long long cap, int* band_bytes) {
+                      unsigned char* band_data, long long cap, int* band_bytes, bool vlc = false,
+                      int* compress_bytes = nullptr) {
     try {
         const ChromaFormat cf = (ChromaFormat)cformat;
         const PictureType pt = intra ? INTRA_PICTURE : INTER_PICTURE;
@@ -418,7 +437,7 @@ int code_residue_impl(int cformat, int w, int h, int comp, int intra, int filter
                 for (int i = 0; i < cbs.LengthX(); ++i) cb_skip[k++] = cbs[j][i].Skipped() ? 1 : 0;
         }
         if (band_data) {
-            const int rc = code_bands_capture(c, bands, intra != 0, band_data, cap, band_bytes);
+            const int rc = code_bands_capture(c, bands, intra != 0, band_data, cap, band_bytes, vlc, compress_bytes);
             if (rc) {
                 delete ec;
                 return rc;
@@ -454,6 +473,17 @@ int ref_code_residue_bytes(int cformat, int w, int h, int comp, int intra, int f
                            unsigned char* band_data, long long cap, int* band_bytes) {
     return code_residue_impl(cformat, w, h, comp, intra, filter, depth, coeff, cw, ch, lambda, cpd_scale, band_qidx,
                              band_skip, band_wt, band_ecf, band_bits, band_ncb, cb_skip, band_data, cap, band_bytes);
+}
+
+// The variable-length band coders' data (-use_vlc), and each coder's Compress result.
+int ref_code_residue_vlc_bytes(int cformat, int w, int h, int comp, int intra, int filter, int depth, int* coeff,
+                               int cw, int ch, float lambda, float cpd_scale, int* band_qidx, int* band_skip,
+                               double* band_wt, float* band_ecf, int* band_bits, int* band_ncb,
+                               unsigned char* cb_skip, unsigned char* band_data, long long cap, int* band_bytes,
+                               int* compress_bytes) {
+    return code_residue_impl(cformat, w, h, comp, intra, filter, depth, coeff, cw, ch, lambda, cpd_scale, band_qidx,
+                             band_skip, band_wt, band_ecf, band_bits, band_ncb, cb_skip, band_data, cap, band_bytes,
+                             true, compress_bytes);
 }
 
 }  // extern "C"

@@ -240,8 +240,9 @@ def adaptive_cases():
 
 def band_cases(ref):
     """The reference's band coders on seeded components (intra and inter, several filters,
-    depths and sizes): the quantiser choices and the CRC-32 and length of every coded band's
-    data, with the inputs to rebuild them (seed, size, filter, depth, lambda)."""
+    depths and sizes), arithmetic and variable-length (-use_vlc): the quantiser choices and the
+    CRC-32 and length of every coded band's data, with the inputs to rebuild them (seed, size,
+    filter, depth, lambda)."""
     import zlib
 
     out = {}
@@ -260,6 +261,15 @@ def band_cases(ref):
         out[f"c{k}_band_crc"] = np.array(crcs[::-1], np.uint32)  # band-list order
         out[f"c{k}_qidx"] = r["qidx"]
         out[f"c{k}_skip"] = r["skip"]
+        v = ref.code_residue_vlc_bytes(2, w, h, 0, intra, filt, depth, co, lam)
+        start, vcrc = 0, []
+        for b in range(3 * depth + 1, 0, -1):
+            n = int(v["band_bytes"][b - 1])
+            vcrc.append(zlib.crc32(v["data"][start:start + n].tobytes()))
+            start += n
+        out[f"c{k}_vlc_band_bytes"] = v["band_bytes"]
+        out[f"c{k}_vlc_band_crc"] = np.array(vcrc[::-1], np.uint32)
+        out[f"c{k}_vlc_compress_bytes"] = v["compress_bytes"]
         out[f"c{k}_wt"] = r["wt"]
         out[f"c{k}_ecf"] = r["ecf"]
         out[f"c{k}_ncb"] = r["ncb"]

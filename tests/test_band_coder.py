@@ -3,7 +3,7 @@ entropy-correction factors (dgpu_entropy_*) against the reference, without a GPU
 
 Band data: for seeded components (intra and inter, several filters, depths and sizes) the
 coder, given the oracle's quantised indices for the reference's quantiser choices, writes the
-bytes the reference's band coders write (tests/golden/bands.npz: CRC-32 and length of every
+bytes the reference's band coders write, arithmetic and variable-length (tests/golden/bands.npz: CRC-32 and length of every
 band's data, made through the reference's own BandCodec / IntraDCBandCodec; live comparison
 where oracle/_ref exists).  Whole loop: the oracle's restated coding loop, with the
 entropy-correction factors adapted from this coder's byte counts, reproduces the stock
@@ -49,6 +49,24 @@ def test_band_data_matches_reference_fixture(oracle, golden, k):
     np.testing.assert_array_equal(np.array(crc[::-1], np.uint32), g[f"c{k}_band_crc"])
 
 
+@pytest.mark.parametrize("k", range(len(BAND_CASES)))
+def test_vlc_band_data_matches_reference_fixture(oracle, golden, k):
+    """The variable-length form (dgpu_code_bands_vlc_host) against the reference's BandVLC /
+    IntraDCBandVLC: bytes, lengths, and the whole-byte counts its Compress returns."""
+    from dirac_b200.entropy import code_bands
+
+    intra, depth, q, sk, cbs, qo, g = band_inputs(oracle, golden, k)
+    data, per, bits = code_bands(intra, depth, [qo], [np.stack([q, sk], 1)], [g[f"c{k}_ncb"]], [cbs], vlc=True)
+    np.testing.assert_array_equal(per[0], g[f"c{k}_vlc_band_bytes"])
+    np.testing.assert_array_equal(bits[0] // 8, g[f"c{k}_vlc_compress_bytes"])
+    crc, start = [], 0
+    for b in range(3 * depth + 1, 0, -1):
+        n = int(per[0][b - 1])
+        crc.append(zlib.crc32(data[start:start + n].tobytes()))
+        start += n
+    np.testing.assert_array_equal(np.array(crc[::-1], np.uint32), g[f"c{k}_vlc_band_crc"])
+
+
 def test_band_data_matches_live_reference(oracle):
     from dirac_b200.entropy import code_bands
     from oracle import Reference
@@ -66,6 +84,11 @@ def test_band_data_matches_live_reference(oracle):
         data, per = code_bands(intra, depth, [qo], [np.stack([q, sk], 1)], [r["ncb"]], [cbs])
         np.testing.assert_array_equal(per[0], r["band_bytes"])
         np.testing.assert_array_equal(data, r["data"])
+        v = ref.code_residue_vlc_bytes(2, 2 * w if comp else w, 2 * h if comp else h, comp, intra, filt, depth, co,
+                                       lam)
+        vdata, vper, _ = code_bands(intra, depth, [qo], [np.stack([q, sk], 1)], [r["ncb"]], [cbs], vlc=True)
+        np.testing.assert_array_equal(vper[0], v["band_bytes"])
+        np.testing.assert_array_equal(vdata, v["data"])
 
 
 def adaptive_encode(case):
