@@ -189,6 +189,45 @@ __global__ void __launch_bounds__(DN_THREADS) downconvert_kernel(const __grid_co
 
 // ---- clip ---------------------------------------------------------------------------------
 
+// Centre-weighted median prefilter (CWMFilterComponent, libdirac_encoder/prefilter.cpp:50-82,
+// Median :84-125): each sample with rows 1 .. h-2 and columns 1 .. w-3 (the reference's loop
+// stops two columns short of the right edge) becomes the median of its 3 x 3 neighbourhood
+// with the centre counted `weight` times (weight = max(1, 10 - strength)); an even count
+// takes the rounded mean of the two middle values.  Other samples are copied.  The k-th
+// smallest of that multiset follows from the eight sorted neighbours and how many of them
+// are below the centre.
+__global__ void cwm_kernel(const int16_t* __restrict__ in, int in_stride, int16_t* __restrict__ out,
+                           int out_stride, int w, int h, int weight) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    const int16_t* r = in + (size_t)y * in_stride;
+    const int c = r[x];
+    int v = c;
+    if (y >= 1 && y <= h - 2 && x >= 1 && x <= w - 3) {
+        int n[8];
+        int k = 0;
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx)
+                if (dy || dx) n[k++] = in[(size_t)(y + dy) * in_stride + x + dx];
+        for (int i = 1; i < 8; ++i) {  // insertion sort of the eight neighbours
+            const int t = n[i];
+            int j = i - 1;
+            while (j >= 0 && n[j] > t) {
+                n[j + 1] = n[j];
+                --j;
+            }
+            n[j + 1] = t;
+        }
+        int below = 0;
+        for (int i = 0; i < 8; ++i) below += n[i] < c;
+        const int len = weight + 8;
+        auto kth = [&](int q) { return q < below ? n[q] : (q < below + weight ? c : n[q - weight]); };
+        v = (len & 1) ? kth((len - 1) / 2) : (kth(len / 2 - 1) + kth(len / 2) + 1) >> 1;
+    }
+    out[(size_t)y * out_stride + x] = (int16_t)v;
+}
+
 __global__ void clip_kernel(int16_t* p, int w, int h, int stride, int lo, int hi) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
@@ -298,4 +337,14 @@ extern "C" int dgpu_downconvert_batch(int n, const int16_t* const* pic, const in
 
 extern "C" int dgpu_clip(int16_t* pic, int w, int h, int stride, int bit_depth, void* stream) {
     return launch_clip(pic, w, h, stride, bit_depth, as_stream(stream));
+}
+
+extern "C" int dgpu_cwm_filter(const int16_t* in, int in_stride, int16_t* out, int out_stride, int w, int h,
+                               int strength, void* stream) {
+    if (!in || !out || in == out || w < 1 || h < 1 || in_stride < w || out_stride < w) return DGPU_ERR_ARG;
+    const int weight = strength >= 9 ? 1 : 10 - strength;
+    dim3 grid((w + 255) / 256, h);
+    cwm_kernel<<<grid, 256, 0, as_stream(stream)>>>(in, in_stride, out, out_stride, w, h, weight);
+    DGPU_CHECK_LAUNCH();
+    return DGPU_OK;
 }

@@ -143,6 +143,18 @@ int dgpu_downconvert_batch(int n, const int16_t* const* pic, const int* w, const
 int dgpu_clip(int16_t* pic, int w, int h, int stride, int bit_depth, void* stream);
 
 /* ---------------------------------------------------------------------------------------
+ * Centre-weighted median prefilter of one component
+ * Replaces CWMFilterComponent (libdirac_encoder/prefilter.cpp:50-125), which the encoder
+ * applies to each input picture's working data when the CWM prefilter is selected
+ * (seq_compress.cpp:649-651, 725-726; the original data, used by motion estimation, stays
+ * unfiltered).  in and out: h x w int16 (distinct buffers: the reference filters from a copy);
+ * strength as EncoderParams::PrefilterStrength.  Rows 1 .. h-2 and columns 1 .. w-3 are
+ * filtered (the reference's loop leaves the last two columns), the rest copied.
+ * ------------------------------------------------------------------------------------- */
+int dgpu_cwm_filter(const int16_t* in, int in_stride, int16_t* out, int out_stride, int w, int h,
+                    int strength, void* stream);
+
+/* ---------------------------------------------------------------------------------------
  * Overlapped-block motion compensation
  * Replaces MotionCompensator::CompensatePicture(const PicturePredParams&, AddOrSub,
  * const MvData&, Picture*, Picture*[2]) (libdirac_common/mot_comp.h, mot_comp.cpp:63-1239).

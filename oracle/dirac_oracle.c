@@ -448,3 +448,37 @@ void orc_clip(int16_t* pic, size_t n, int bit_depth) {
     const int lo = -(1 << (bit_depth - 1)), hi = (1 << (bit_depth - 1)) - 1;
     for (size_t i = 0; i < n; ++i) pic[i] = (int16_t)clampi(pic[i], lo, hi);
 }
+
+/* CWMFilterComponent (libdirac_encoder/prefilter.cpp:50-125): the median of the list made of
+ * the centre sample repeated max(1, 10 - strength) - 1 times and the nine samples of its 3 x 3
+ * window, for rows 1 .. h-2 and columns 1 .. w-3 (the reference's column loop ends at
+ * LastX() - 1); an even-length list gives the rounded mean of its two middle values.  Reads
+ * `in`, writes every sample of `out` (unfiltered ones copied). */
+int orc_cwm_filter(const int16_t* in, int16_t* out, int w, int h, int strength) {
+    if (!in || !out || w < 1 || h < 1) return -1;
+    const int weight = (10 - strength) > 1 ? 10 - strength : 1;
+    const int len = weight + 8;
+    int16_t* list = (int16_t*)malloc(sizeof(int16_t) * (size_t)len);
+    if (!list) return -4;
+    memcpy(out, in, sizeof(int16_t) * (size_t)w * h);
+    for (int y = 1; y < h - 1; ++y)
+        for (int x = 1; x < w - 2; ++x) {
+            int n = 0;
+            for (int k = 0; k < weight - 1; ++k) list[n++] = in[(size_t)y * w + x];
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) list[n++] = in[(size_t)(y + dy) * w + x + dx];
+            for (int i = 1; i < n; ++i) { /* insertion sort */
+                const int16_t t = list[i];
+                int j = i - 1;
+                while (j >= 0 && list[j] > t) {
+                    list[j + 1] = list[j];
+                    --j;
+                }
+                list[j + 1] = t;
+            }
+            out[(size_t)y * w + x] = (len & 1) ? list[(len - 1) / 2]
+                                               : (int16_t)((list[len / 2 - 1] + list[len / 2] + 1) >> 1);
+        }
+    free(list);
+    return 0;
+}

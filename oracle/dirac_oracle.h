@@ -104,6 +104,9 @@ int orc_code_residue(int intra, int depth, int32_t* c, int cw, int ch, float lam
 int orc_dequantise(int intra, int depth, const int32_t* qindex, int32_t* coeff, int cw, int ch,
                    const int* band_ncb, const int* band_qidx, const int* band_skip, const uint8_t* cb_skip);
 
+/* CWMFilterComponent: centre-weighted median prefilter of a dense w x h component. */
+int orc_cwm_filter(const int16_t* in, int16_t* out, int w, int h, int strength);
+
 /* Picture::ClipComponent: clamp to [-2^(d-1), 2^(d-1)-1]. */
 void orc_clip(int16_t* pic, size_t n, int bit_depth);
 

@@ -66,6 +66,15 @@ class Oracle:
     def dwt_min_len(self, filt):
         return self.lib.orc_dwt_min_len(filt)
 
+    def cwm_filter(self, pic, strength):
+        """CWMFilterComponent of a 2-D int16 component; returns the filtered copy."""
+        p = np.ascontiguousarray(pic, dtype=np.int16)
+        out = np.empty_like(p)
+        h, w = p.shape
+        if self.lib.orc_cwm_filter(_p(p), _p(out), w, h, strength):
+            raise ValueError("orc_cwm_filter failed")
+        return out
+
     def dwt_forward(self, filt, depth, pic, cw=None, ch=None):
         pic = np.ascontiguousarray(pic, dtype=np.int16)
         h, w = pic.shape
@@ -228,6 +237,13 @@ class Reference:
         if self.lib.ref_upconvert(_p(pic), w, h, bit_depth, _p(up)):
             raise ValueError("ref_upconvert failed")
         return up
+
+    def cwm_filter(self, pic, strength):
+        p = np.array(pic, dtype=np.int16, copy=True, order="C")
+        h, w = p.shape
+        if self.lib.ref_cwm_filter(_p(p), w, h, strength):
+            raise ValueError("ref_cwm_filter failed")
+        return p
 
     def downconvert(self, pic):
         pic = np.ascontiguousarray(pic, dtype=np.int16)

@@ -26,6 +26,7 @@
 #include <libdirac_byteio/subband_byteio.h>
 #include <libdirac_common/band_codec.h>
 #include <libdirac_common/band_vlc.h>
+#include <libdirac_encoder/prefilter.h>
 
 using namespace dirac;
 
@@ -484,6 +485,21 @@ int ref_code_residue_vlc_bytes(int cformat, int w, int h, int comp, int intra, i
     return code_residue_impl(cformat, w, h, comp, intra, filter, depth, coeff, cw, ch, lambda, cpd_scale, band_qidx,
                              band_skip, band_wt, band_ecf, band_bits, band_ncb, cb_skip, band_data, cap, band_bytes,
                              true, compress_bytes);
+}
+
+// CWMFilterComponent on a dense w x h component, in place.
+int ref_cwm_filter(short* pic, int w, int h, int strength) {
+    try {
+        PicArray a(h, w);
+        for (int y = 0; y < h; ++y)
+            for (int x = 0; x < w; ++x) a[y][x] = pic[y * w + x];
+        CWMFilterComponent(a, strength);
+        for (int y = 0; y < h; ++y)
+            for (int x = 0; x < w; ++x) pic[y * w + x] = a[y][x];
+        return 0;
+    } catch (...) {
+        return -1;
+    }
 }
 
 }  // extern "C"

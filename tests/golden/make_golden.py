@@ -3,7 +3,7 @@
 Needs oracle/_ref/libdirac_ref.so (the reference's own C++, plain-C build, compiled from
 its sources by `make -C oracle`).  Inputs are seeded, so re-running reproduces the files.
 
-    python tests/golden/make_golden.py [dwt convert mc me quant encode decode adaptive bands]
+    python tests/golden/make_golden.py [dwt convert mc me quant encode decode adaptive bands prefilter]
 """
 import os
 import sys
@@ -277,6 +277,21 @@ def band_cases(ref):
     return out
 
 
+# (width, height, strength) of prefilter_cases
+PREFILTER_CASES = [(64, 48, 0), (37, 23, 3), (48, 40, 5), (33, 17, 8), (40, 32, 9), (16, 9, 11)]
+
+
+def prefilter_cases(ref):
+    """CWMFilterComponent of the reference on seeded 8-bit-range components."""
+    out = {}
+    for k, (w, h, strength) in enumerate(PREFILTER_CASES):
+        rng = np.random.default_rng(500 + k)
+        pic = rng.integers(-128, 128, size=(h, w)).astype(np.int16)
+        out[f"c{k}_in"] = pic
+        out[f"c{k}_out"] = ref.cwm_filter(pic, strength)
+    return out
+
+
 # (intra, filter, depth, width, height, lambda) of band_cases
 BAND_CASES = [(1, 1, 4, 176, 144, 5.0), (0, 0, 4, 176, 144, 30.0), (1, 6, 3, 88, 72, 3.0),
               (0, 2, 5, 352, 288, 100.0), (1, 3, 2, 64, 48, 1.0), (0, 4, 3, 96, 80, 8.0)]
@@ -285,11 +300,12 @@ BAND_CASES = [(1, 1, 4, 176, 144, 5.0), (0, 0, 4, 176, 144, 30.0), (1, 6, 3, 88,
 def main(argv=None):
     """Writes the named fixtures (default: all)."""
     names = (argv if argv is not None else sys.argv[1:]) or ["dwt", "convert", "mc", "me", "quant", "encode",
-                                                              "decode", "adaptive", "bands"]
+                                                              "decode", "adaptive", "bands", "prefilter"]
     ref = Reference()
     makers = {"dwt": lambda: dwt_cases(ref), "convert": lambda: conv_cases(ref), "mc": lambda: mc_cases(ref),
               "me": lambda: me_cases(ref), "quant": lambda: quant_cases(ref), "encode": encode_cases,
-              "decode": decode_cases, "adaptive": adaptive_cases, "bands": lambda: band_cases(ref)}
+              "decode": decode_cases, "adaptive": adaptive_cases, "bands": lambda: band_cases(ref),
+              "prefilter": lambda: prefilter_cases(ref)}
     for n in names:
         np.savez_compressed(os.path.join(HERE, n + ".npz"), **makers[n]())
     print("wrote " + ", ".join(n + ".npz" for n in names))
