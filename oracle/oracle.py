@@ -353,7 +353,7 @@ class RefEncParams(ctypes.Structure):
                 ("num_l1", ctypes.c_int), ("cpd", ctypes.c_float), ("xblen", ctypes.c_int),
                 ("yblen", ctypes.c_int), ("xbsep", ctypes.c_int), ("ybsep", ctypes.c_int),
                 ("mv_precision", ctypes.c_int), ("intra_filter", ctypes.c_int), ("inter_filter", ctypes.c_int),
-                ("wlt_depth", ctypes.c_int)]
+                ("wlt_depth", ctypes.c_int), ("use_vlc", ctypes.c_int)]
 
 
 def reference_encode(cfg, frames, freeze=True, path=REF_SO):

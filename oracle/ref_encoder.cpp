@@ -51,6 +51,7 @@ struct RefEncParams {
     int xblen, yblen, xbsep, ybsep;
     int mv_precision;
     int intra_filter, inter_filter, wlt_depth;
+    int use_vlc;        // 1: variable-length coefficient coding (-use_vlc), 0: arithmetic coding
 };
 
 // Encodes nframes 8-bit planar frames (Y then U then V, dense, frame after frame).
@@ -86,7 +87,7 @@ int encode_impl(const RefEncParams* p, int nframes, const unsigned char* frames,
     ctx.enc_params.wlt_depth = p->wlt_depth;
     ctx.enc_params.spatial_partition = 1;
     ctx.enc_params.multi_quants = 0;
-    ctx.enc_params.using_ac = 1;
+    ctx.enc_params.using_ac = p->use_vlc ? 0 : 1;
     ctx.enc_params.trate = 0;
     ctx.enc_params.lossless = 0;
     ctx.enc_params.full_search = 0;

@@ -220,9 +220,10 @@ def decode_cases():
 
 
 def adaptive_cases():
-    """The stock reference encoder (entropy-correction factors adapted from its arithmetic
-    coder's byte counts, as it ships) on each ENCODE_CASES sequence: CRC-32 of every locally
-    decoded plane and the picture types."""
+    """The stock reference encoder (entropy-correction factors adapted from its coder's byte
+    counts, as it ships) on each ENCODE_CASES sequence, with arithmetic coding and with
+    variable-length coding (-use_vlc, "<name>_vlc_*"): CRC-32 of every locally decoded plane
+    and the picture types."""
     import zlib
 
     from oracle import reference_encode
@@ -230,11 +231,12 @@ def adaptive_cases():
     out = {}
     for case in ENCODE_CASES:
         seq, cfg = encode_inputs(case)
-        rec, ptype, _ = reference_encode(cfg, seq, freeze=False)
         name = case[0]
-        out[name + "_crc"] = np.array([[zlib.crc32(np.ascontiguousarray(p).tobytes()) for p in f] for f in rec],
-                                      np.uint32)
-        out[name + "_ptype"] = ptype
+        for tag, vlc in (("", 0), ("_vlc", 1)):
+            rec, ptype, _ = reference_encode(dict(cfg, use_vlc=vlc), seq, freeze=False)
+            out[name + tag + "_crc"] = np.array([[zlib.crc32(np.ascontiguousarray(p).tobytes()) for p in f]
+                                                 for f in rec], np.uint32)
+            out[name + tag + "_ptype"] = ptype
     return out
 
 

@@ -7,8 +7,8 @@ bytes the reference's band coders write, arithmetic and variable-length (tests/g
 band's data, made through the reference's own BandCodec / IntraDCBandCodec; live comparison
 where oracle/_ref exists).  Whole loop: the oracle's restated coding loop, with the
 entropy-correction factors adapted from this coder's byte counts, reproduces the stock
-reference encoder (adaptive factors, as it ships) picture for picture
-(tests/golden/adaptive.npz)."""
+reference encoder (adaptive factors, as it ships), with arithmetic and with variable-length
+coefficient coding, picture for picture (tests/golden/adaptive.npz)."""
 import os
 import sys
 import zlib
@@ -91,8 +91,10 @@ def test_band_data_matches_live_reference(oracle):
         np.testing.assert_array_equal(vdata, v["data"])
 
 
-def adaptive_encode(case):
-    """The oracle's coding loop with factors adapted from dgpu_code_bands_host's byte counts."""
+def adaptive_encode(case, vlc=False):
+    """The oracle's coding loop with factors adapted from the host coder's byte counts
+    (dgpu_code_bands_host; with vlc, dgpu_code_bands_vlc_host and the whole bytes the
+    reference's VLC coders report)."""
     from dirac_b200 import quant, synth
     from dirac_b200.entropy import EntropyCorrector, code_bands
     from oracle_encoder import OracleEncoder
@@ -113,9 +115,10 @@ def adaptive_encode(case):
             break
         r = p.result
         for c in range(3):
-            _, per = code_bands(p.intra, depth, [r["qindex"][c]], [np.stack([r["qidx"][c], r["skip"][c]], 1)], [ncb],
-                                [r["cb_skip"][c]])
-            ec.update(p.intra, p.is_b(), c, r["skip"][c], r["bits"][c], per[0])
+            coded = code_bands(p.intra, depth, [r["qindex"][c]], [np.stack([r["qidx"][c], r["skip"][c]], 1)], [ncb],
+                               [r["cb_skip"][c]], vlc=vlc)
+            counts = coded[2][0] // 8 if vlc else coded[1][0]
+            ec.update(p.intra, p.is_b(), c, r["skip"][c], r["bits"][c], counts)
     return enc
 
 
@@ -129,6 +132,18 @@ def test_adaptive_loop_matches_stock_reference_encoder(golden, case):
     np.testing.assert_array_equal([int(enc.pics[i].intra) for i in range(len(enc.pics))], g[case[0] + "_ptype"])
     # the adapted factors matter: the stock encoder's pictures differ from the frozen-factor ones
     assert not np.array_equal(g[case[0] + "_crc"], golden("encode.npz")[case[0] + "_crc"])
+
+
+@pytest.mark.parametrize("case", ENCODE_CASES, ids=[c[0] for c in ENCODE_CASES])
+def test_adaptive_vlc_loop_matches_stock_reference_encoder(golden, case):
+    """The same with variable-length coefficient coding (-use_vlc): the stock reference
+    encoder's pictures."""
+    enc = adaptive_encode(case, vlc=True)
+    g = golden("adaptive.npz")
+    crc = np.array([[zlib.crc32(np.ascontiguousarray((p.astype(np.int32) + 128).astype(np.uint8)).tobytes())
+                     for p in enc.pics[i].data] for i in range(len(enc.pics))], np.uint32)
+    np.testing.assert_array_equal(crc, g[case[0] + "_vlc_crc"])
+    np.testing.assert_array_equal([int(enc.pics[i].intra) for i in range(len(enc.pics))], g[case[0] + "_vlc_ptype"])
 
 
 @pytest.mark.parametrize("depth", [1, 3, 4, 6])
