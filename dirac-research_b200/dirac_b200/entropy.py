@@ -57,6 +57,32 @@ def code_bands(intra, depth, qindex, bands, ncb, cb_skip, vlc=False):
     return out[:int(nbytes.sum())].copy(), per
 
 
+def decode_bands(depth, shapes, band_skip, ncb, data, band_bytes, vlc=False):
+    """dgpu_decode_bands_host: components' signed quantised indices from their coded band data.
+    depth: one value or one per component; shapes: (ch, cw) per component; band_skip, ncb and
+    band_bytes per component (band-list order); data: the bands' bytes (per component, DC band
+    first).  Returns (list of int32 [ch][cw] indices, list of code-block flag arrays)."""
+    lib = _lib.load()
+    n = len(shapes)
+    depth = list(depth) if hasattr(depth, "__len__") else [int(depth)] * n
+    q = [np.zeros(s, np.int32) for s in shapes]
+    bs = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32).ravel() for x in band_skip]), np.int32)
+    nc = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32).ravel() for x in ncb]), np.int32)
+    bb = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32).ravel() for x in band_bytes]), np.int32)
+    d = np.ascontiguousarray(data, np.uint8) if len(data) else np.zeros(1, np.uint8)
+    ncbt = [int((np.asarray(x).reshape(-1, 2)[:, 0] * np.asarray(x).reshape(-1, 2)[:, 1]).sum()) for x in ncb]
+    cbs = np.zeros(sum(ncbt), np.uint8)
+    _lib.check(lib.dgpu_decode_bands_host(
+        n, _lib.int_array(depth), _lib.int_array([s[1] for s in shapes]), _lib.int_array([s[0] for s in shapes]),
+        nc.ctypes.data_as(_lib.P_int), bs.ctypes.data_as(_lib.P_int), d.ctypes.data, bb.ctypes.data_as(_lib.P_int),
+        int(bool(vlc)), _lib.ptr_array([a.ctypes.data for a in q]), cbs.ctypes.data), "dgpu_decode_bands_host")
+    flags, k = [], 0
+    for t in ncbt:
+        flags.append(cbs[k:k + t].copy())
+        k += t
+    return q, flags
+
+
 class EntropyCorrector:
     """The reference's EntropyCorrector for one sequence (transform depth fixed)."""
 

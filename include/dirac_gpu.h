@@ -542,6 +542,18 @@ int dgpu_code_bands_vlc_host(int n, const int* intra, const int* depth, const in
                              const int* cw, const int* ch, const int* band_ncb, const int* band_qidx,
                              const int* band_skip, const uint8_t* cb_skip, uint8_t* out, size_t out_cap,
                              int* band_bytes, long long* band_bits);
+/* The decoding side (the band decoders' symbol decoding: band_codec_template.h:204-357,
+ * 500-557 over ArithCodecBase's decoder, arith_codec.h:200-250, arith_codec.cpp:132-165, or
+ * the VLC adapter when vlc != 0): from the coded bands' data (the layout dgpu_code_bands_host
+ * writes: per component, bands from the DC band down; band_bytes as the subband headers give
+ * them) to the signed quantised indices dgpu_dequantise_batch takes.  qindex[c] (host, dense
+ * cw[c] x ch[c] int32) is written in full (zeros in skipped bands and code blocks); cb_skip
+ * receives the decoded code-block skip flags (band-list order, components concatenated).  The
+ * bands of a level are decoded in parallel, levels from coarse to fine (a band's contexts
+ * read its parent band).  No GPU use. */
+int dgpu_decode_bands_host(int n, const int* depth, const int* cw, const int* ch, const int* band_ncb,
+                           const int* band_skip, const uint8_t* data, const int* band_bytes, int vlc,
+                           int32_t* const* qindex, uint8_t* cb_skip);
 int dgpu_entropy_init(int depth, float* state);
 int dgpu_entropy_factors(int depth, const float* state, int intra, int is_b, float* ecf);
 int dgpu_entropy_update(int depth, float* state, int intra, int is_b, int comp, const int* band_skip,

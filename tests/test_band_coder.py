@@ -189,3 +189,71 @@ def test_code_bands_reports_size():
         _lib.int_array([8]), _lib.int_array([1, 1] * 4), _lib.int_array([0] * 4), _lib.int_array([0] * 4),
         np.zeros(4, np.uint8).ctypes.data, out.ctypes.data, ctypes.c_size_t(0), n.ctypes.data_as(_lib.P_int))
     assert rc == -2 and (n > 0).all()
+
+
+@pytest.mark.parametrize("vlc", [False, True], ids=["ac", "vlc"])
+def test_decode_bands_round_trip(oracle, golden, vlc):
+    """dgpu_decode_bands_host inverts the coder (whose bytes are the reference's, above)."""
+    from dirac_b200.entropy import code_bands, decode_bands
+
+    for k in range(len(BAND_CASES)):
+        intra, depth, q, sk, cbs, qo, g = band_inputs(oracle, golden, k)
+        coded = code_bands(intra, depth, [qo], [np.stack([q, sk], 1)], [g[f"c{k}_ncb"]], [cbs], vlc=vlc)
+        got, flags = decode_bands(depth, [qo.shape], [sk], [g[f"c{k}_ncb"]], coded[0], [coded[1][0]], vlc=vlc)
+        np.testing.assert_array_equal(got[0], qo, err_msg=f"case {k}")
+        np.testing.assert_array_equal(flags[0], cbs, err_msg=f"case {k}")
+
+
+def test_decode_bands_of_live_reference_bytes(oracle):
+    """The reference band coders' own bytes decode to the indices the oracle quantises to."""
+    from dirac_b200.entropy import decode_bands
+    from oracle import Reference
+
+    if not Reference.available():
+        pytest.skip("reference library not built here")
+    ref = Reference()
+    rng = np.random.default_rng(31)
+    for intra, filt, depth, w, h, lam in [(1, 6, 4, 176, 144, 4.0), (0, 0, 3, 120, 72, 25.0)]:
+        pic = rng.integers(-70, 70, size=(h, w)).astype(np.int16)
+        co = oracle.dwt_forward(filt, depth, pic)
+        for vlc in (False, True):
+            r = (ref.code_residue_vlc_bytes if vlc else ref.code_residue_bytes)(2, w, h, 0, intra, filt, depth, co,
+                                                                                 lam)
+            _, q, sk, _, cbs, qo = oracle.code_residue(intra, depth, co, lam, r["wt"].astype(np.float32), r["ecf"],
+                                                       r["ncb"])
+            got, flags = decode_bands(depth, [qo.shape], [r["skip"]], [r["ncb"]], r["data"], [r["band_bytes"]],
+                                      vlc=vlc)
+            np.testing.assert_array_equal(got[0], qo)
+            np.testing.assert_array_equal(flags[0], cbs)
+
+
+def test_coded_bytes_decode_to_the_reference_decoders_pictures(oracle, golden):
+    """From coded band bytes to pictures: a sequence's bands coded, decoded back to indices and
+    flags, and decoded by the oracle's restatement of the decoder, give the reference decoder's
+    pictures (decode.npz)."""
+    from dirac_b200 import quant, synth
+    from dirac_b200.entropy import code_bands, decode_bands
+    from oracle_decoder import decode_picture, output_samples
+    from oracle_encoder import encode_sequence
+
+    seq, rcfg = encode_inputs(ENCODE_CASES[1])
+    cfg = {k: v for k, v in rcfg.items() if k != "video_format"}
+    cfg.update(luma_depth=8, chroma_depth=8)
+    enc = encode_sequence(cfg, [[synth.to_signed(x) for x in f] for f in seq], quant.band_weights, quant.code_blocks,
+                          oracle)
+    depth = cfg["wlt_depth"]
+    ncb = quant.code_blocks(depth, cfg["width"], cfg["height"])
+    out = {}
+    for pn in enc.order:
+        p = enc.pics[pn]
+        r = p.result
+        shapes = [x.shape for x in r["qindex"]]
+        bands = [np.stack([r["qidx"][c], r["skip"][c]], 1) for c in range(3)]
+        data, per = code_bands(p.intra, depth, r["qindex"], bands, [ncb] * 3, r["cb_skip"])
+        q, flags = decode_bands(depth, shapes, r["skip"], [ncb] * 3, data, per)
+        pic = {"intra": p.intra, "filter": r["filter"], "qindex": q, "qidx": r["qidx"], "skip": r["skip"],
+               "cb_skip": flags, "me": p.me}
+        out[pn] = decode_picture(cfg, pic, [out[x] for x in p.refs] if not p.intra else None, ncb, oracle)
+    crc = np.array([[zlib.crc32(np.ascontiguousarray(x).tobytes()) for x in output_samples(out[i], 8, 8)]
+                    for i in range(len(seq))], np.uint32)
+    np.testing.assert_array_equal(crc, golden("decode.npz")[ENCODE_CASES[1][0] + "_crc"])
