@@ -16,6 +16,9 @@
 // contiguous 256-byte run.  The decimator stages its vertically filtered row buffer in
 // shared memory and writes one output sample per thread.
 
+#include <algorithm>
+#include <cmath>
+
 #include "dgpu_internal.cuh"
 
 namespace dgpu {
@@ -228,6 +231,35 @@ __global__ void cwm_kernel(const int16_t* __restrict__ in, int in_stride, int16_
     out[(size_t)y * out_stride + x] = (int16_t)v;
 }
 
+// RECTLP residue prefilter (LPFilter / HFilter / VFilter, libdirac_encoder/prefilter.cpp:
+// 141-306): a 17-tap integer low-pass filter (taps summing to about 2^14) applied along rows,
+// then along columns, each output (sum + 2^13) >> 14 clamped to [-128, 127] (the reference's
+// bounds, whatever the bit depth), source indices clamped to the component.
+struct LpTaps {
+    int t[17];  // t[k + 8] multiplies the sample at offset -k
+};
+
+__global__ void lp_rows_kernel(const int16_t* __restrict__ in, int in_stride, int16_t* __restrict__ out,
+                               int out_stride, int w, int h, const __grid_constant__ LpTaps T) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    const int16_t* r = in + (size_t)y * in_stride;
+    int sum = 1 << 13;
+    for (int k = -8; k <= 8; ++k) sum += T.t[k + 8] * r[clampi(x - k, 0, w - 1)];
+    out[(size_t)y * out_stride + x] = (int16_t)clampi(sum >> 14, -128, 127);
+}
+
+__global__ void lp_cols_kernel(const int16_t* __restrict__ in, int in_stride, int16_t* __restrict__ out,
+                               int out_stride, int w, int h, const __grid_constant__ LpTaps T) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    int sum = 1 << 13;
+    for (int k = -8; k <= 8; ++k) sum += T.t[k + 8] * in[(size_t)clampi(y - k, 0, h - 1) * in_stride + x];
+    out[(size_t)y * out_stride + x] = (int16_t)clampi(sum >> 14, -128, 127);
+}
+
 __global__ void clip_kernel(int16_t* p, int w, int h, int stride, int lo, int hi) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
@@ -337,6 +369,50 @@ extern "C" int dgpu_downconvert_batch(int n, const int16_t* const* pic, const in
 
 extern "C" int dgpu_clip(int16_t* pic, int w, int h, int stride, int bit_depth, void* stream) {
     return launch_clip(pic, w, h, stride, bit_depth, as_stream(stream));
+}
+
+// MakeLPRectFilter (prefilter.cpp:141-181) for LPFilter's bandwidth (:183-193): a Hanning-
+// windowed sinc of 17 taps in double, scaled to a DC gain of 2^18, rounded half away from zero
+// and brought to 2^14 by (t + 8) >> 4.
+static void rect_lp_taps(float qf, int strength, LpTaps& T) {
+    const float bw = std::min(std::max(qf + 3.0f - float(strength), 1.0f), 10.0f) / 10.0f;
+    const float pi = 3.1415926535f;
+    double d[17];
+    for (int i = -8; i <= 8; ++i) d[i + 8] = std::cos(double((pi * i) / 18));  // float argument, double cosine
+    for (int i = -8; i <= 8; ++i) {
+        const double v = pi * 1.0 * bw * i;
+        d[i + 8] *= v == 0.0 ? 1.0 : std::sin(v) / v;
+    }
+    double sum = 0.0;
+    for (int i = 0; i < 17; ++i) sum += d[i];
+    for (int i = 0; i < 17; ++i) {
+        d[i] *= double(1 << 18);
+        d[i] /= sum;
+        const int r = d[i] > 0 ? int(d[i] + 0.5) : -int(-d[i] + 0.5);
+        T.t[i] = (r + 8) >> 4;
+    }
+}
+
+extern "C" int dgpu_rect_lp_filter(int16_t* pic, int w, int h, int stride, float qf, int strength, int16_t* scratch,
+                                   void* stream) {
+    if (!pic || stride < w) return DGPU_ERR_ARG;
+    if (w < 17 || h < 17) return DGPU_ERR_SIZE;  // the reference's edge loops assume 17 samples
+    int16_t* tmp = scratch;
+    if (!tmp) {
+        void* p = nullptr;
+        const int rc = library_scratch((size_t)w * h * sizeof(int16_t), &p);
+        if (rc) return rc;
+        tmp = static_cast<int16_t*>(p);
+    }
+    LpTaps T;
+    rect_lp_taps(qf, strength, T);
+    cudaStream_t st = as_stream(stream);
+    dim3 grid((w + 255) / 256, h);
+    lp_rows_kernel<<<grid, 256, 0, st>>>(pic, stride, tmp, w, w, h, T);
+    DGPU_CHECK_LAUNCH();
+    lp_cols_kernel<<<grid, 256, 0, st>>>(tmp, w, pic, stride, w, h, T);
+    DGPU_CHECK_LAUNCH();
+    return DGPU_OK;
 }
 
 extern "C" int dgpu_cwm_filter(const int16_t* in, int in_stride, int16_t* out, int out_stride, int w, int h,

@@ -70,6 +70,7 @@ SIGNATURES = {
     "dgpu_downconvert_batch": (c_int, [c_int, P_void, P_int, P_int, P_int, P_void, P_int, c_void_p]),
     "dgpu_clip": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p]),
     "dgpu_cwm_filter": (c_int, [c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_int, c_void_p]),
+    "dgpu_rect_lp_filter": (c_int, [c_void_p, c_int, c_int, c_int, ctypes.c_float, c_int, c_void_p, c_void_p]),
     "dgpu_motion_compensate": (
         c_int,
         [c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,

@@ -154,6 +154,16 @@ int dgpu_clip(int16_t* pic, int w, int h, int stride, int bit_depth, void* strea
 int dgpu_cwm_filter(const int16_t* in, int in_stride, int16_t* out, int out_stride, int w, int h,
                     int strength, void* stream);
 
+/* RECTLP residue prefilter of one component, in place: replaces LPFilter
+ * (libdirac_encoder/prefilter.cpp:141-306), which PictureCompressor::Prefilter applies to each
+ * component before the forward transform when RECTLP is selected (picture_compress.cpp:
+ * 340-355).  The 17 taps are designed on the host in double from qf and strength as the
+ * reference does; rows, then columns, outputs clamped to [-128, 127] as in the reference.
+ * scratch: device w x h int16, or NULL for the library's own buffer.  DGPU_ERR_SIZE below
+ * 17 x 17 (the reference's edge loops need 17 samples). */
+int dgpu_rect_lp_filter(int16_t* pic, int w, int h, int stride, float qf, int strength, int16_t* scratch,
+                        void* stream);
+
 /* ---------------------------------------------------------------------------------------
  * Overlapped-block motion compensation
  * Replaces MotionCompensator::CompensatePicture(const PicturePredParams&, AddOrSub,

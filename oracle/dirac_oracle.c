@@ -10,6 +10,7 @@
  */
 #include "dirac_oracle.h"
 
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -480,5 +481,48 @@ int orc_cwm_filter(const int16_t* in, int16_t* out, int w, int h, int strength) 
                                                : (int16_t)((list[len / 2 - 1] + list[len / 2] + 1) >> 1);
         }
     free(list);
+    return 0;
+}
+
+/* LPFilter (libdirac_encoder/prefilter.cpp:141-306), the RECTLP residue prefilter: taps of a
+ * 17-point Hanning-windowed sinc designed in double (MakeLPRectFilter with 14-bit accuracy and
+ * LPFilter's bandwidth), then HFilter and VFilter: each output (sum + 2^13) >> 14 clamped to
+ * [-128, 127], source indices clamped to the component.  In place; w, h >= 17. */
+int orc_rect_lp_filter(int16_t* pic, int w, int h, float qf, int strength) {
+    if (!pic || w < 17 || h < 17) return -1;
+    float bw = qf + 3.0f - (float)strength;
+    bw = bw < 1.0f ? 1.0f : (bw > 10.0f ? 10.0f : bw);
+    bw /= 10.0f;
+    const float pi = 3.1415926535f;
+    double d[17], sum = 0.0;
+    int t[17];
+    for (int i = -8; i <= 8; ++i) {
+        const float a = (pi * i) / 18;
+        const double v = pi * 1.0 * bw * i;
+        d[i + 8] = cos((double)a) * (v == 0.0 ? 1.0 : sin(v) / v);
+    }
+    for (int i = 0; i < 17; ++i) sum += d[i];
+    for (int i = 0; i < 17; ++i) {
+        const double x = d[i] * (double)(1 << 18) / sum;
+        const int r = x > 0 ? (int)(x + 0.5) : -(int)(-x + 0.5);
+        t[i] = (r + 8) >> 4;
+    }
+    int16_t* tmp = (int16_t*)malloc(sizeof(int16_t) * (size_t)w * h);
+    if (!tmp) return -4;
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            int s = 1 << 13;
+            for (int k = -8; k <= 8; ++k) s += t[k + 8] * pic[(size_t)y * w + clampi(x - k, 0, w - 1)];
+            s >>= 14;
+            tmp[(size_t)y * w + x] = (int16_t)clampi(s, -128, 127);
+        }
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            int s = 1 << 13;
+            for (int k = -8; k <= 8; ++k) s += t[k + 8] * tmp[(size_t)clampi(y - k, 0, h - 1) * w + x];
+            s >>= 14;
+            pic[(size_t)y * w + x] = (int16_t)clampi(s, -128, 127);
+        }
+    free(tmp);
     return 0;
 }

@@ -66,6 +66,14 @@ class Oracle:
     def dwt_min_len(self, filt):
         return self.lib.orc_dwt_min_len(filt)
 
+    def rect_lp_filter(self, pic, qf, strength):
+        """LPFilter (RECTLP) of a 2-D int16 component; returns the filtered copy."""
+        p = np.array(pic, dtype=np.int16, copy=True, order="C")
+        h, w = p.shape
+        if self.lib.orc_rect_lp_filter(_p(p), w, h, ctypes.c_float(qf), strength):
+            raise ValueError("orc_rect_lp_filter failed")
+        return p
+
     def cwm_filter(self, pic, strength):
         """CWMFilterComponent of a 2-D int16 component; returns the filtered copy."""
         p = np.ascontiguousarray(pic, dtype=np.int16)
@@ -237,6 +245,13 @@ class Reference:
         if self.lib.ref_upconvert(_p(pic), w, h, bit_depth, _p(up)):
             raise ValueError("ref_upconvert failed")
         return up
+
+    def rect_lp_filter(self, pic, qf, strength):
+        p = np.array(pic, dtype=np.int16, copy=True, order="C")
+        h, w = p.shape
+        if self.lib.ref_lp_filter(_p(p), w, h, ctypes.c_float(qf), strength):
+            raise ValueError("ref_lp_filter failed")
+        return p
 
     def cwm_filter(self, pic, strength):
         p = np.array(pic, dtype=np.int16, copy=True, order="C")

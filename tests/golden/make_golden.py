@@ -283,14 +283,23 @@ def band_cases(ref):
 PREFILTER_CASES = [(64, 48, 0), (37, 23, 3), (48, 40, 5), (33, 17, 8), (40, 32, 9), (16, 9, 11)]
 
 
+# (width, height, quality factor, strength) of the RECTLP cases
+RECTLP_CASES = [(48, 40, 7.0, 0), (17, 17, 2.0, 1), (33, 21, 10.0, 5), (64, 24, 0.5, 3), (40, 36, 12.0, 10)]
+
+
 def prefilter_cases(ref):
-    """CWMFilterComponent of the reference on seeded 8-bit-range components."""
+    """CWMFilterComponent and LPFilter (RECTLP) of the reference on seeded components."""
     out = {}
     for k, (w, h, strength) in enumerate(PREFILTER_CASES):
         rng = np.random.default_rng(500 + k)
         pic = rng.integers(-128, 128, size=(h, w)).astype(np.int16)
         out[f"c{k}_in"] = pic
         out[f"c{k}_out"] = ref.cwm_filter(pic, strength)
+    for k, (w, h, qf, strength) in enumerate(RECTLP_CASES):
+        rng = np.random.default_rng(600 + k)
+        pic = rng.integers(-300, 300, size=(h, w)).astype(np.int16)
+        out[f"lp{k}_in"] = pic
+        out[f"lp{k}_out"] = ref.rect_lp_filter(pic, qf, strength)
     return out
 
 
