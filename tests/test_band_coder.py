@@ -257,3 +257,52 @@ def test_coded_bytes_decode_to_the_reference_decoders_pictures(oracle, golden):
     crc = np.array([[zlib.crc32(np.ascontiguousarray(x).tobytes()) for x in output_samples(out[i], 8, 8)]
                     for i in range(len(seq))], np.uint32)
     np.testing.assert_array_equal(crc, golden("decode.npz")[ENCODE_CASES[1][0] + "_crc"])
+
+
+@pytest.mark.parametrize("vlc", [False, True], ids=["ac", "vlc"])
+def test_round_trip_extreme_indices(vlc):
+    """Magnitudes up to 2^30, all-zero bands, empty code blocks (more blocks than samples) and
+    a single-block band survive coding and decoding."""
+    from dirac_b200.entropy import code_bands, decode_bands
+
+    rng = np.random.default_rng(41)
+    depth, cw, ch = 3, 40, 24
+    nb = 3 * depth + 1
+    q = np.zeros((ch, cw), np.int32)
+    mask = rng.random((ch, cw)) < 0.3
+    q[mask] = rng.integers(-(1 << 30), 1 << 30, size=int(mask.sum()))
+    q[:ch // 8, :cw // 8] = 0  # an all-zero DC band
+    ncb = np.array([[7, 5]] * (nb - 1) + [[1, 1]], np.int32)  # band 1 is 20 x 12: fine; DC band 5 x 3: one block
+    ncb[nb - 4] = [9, 4]  # a coarse band (5 x 3) with more code blocks than columns: some are empty
+    cbs = (rng.random(int((ncb[:, 0] * ncb[:, 1]).sum())) < 0.2).astype(np.uint8)
+    # skipped code blocks hold zero indices, as the quantiser writes them
+    start = 0
+    for b in range(1, nb + 1):
+        xn, yn = ncb[b - 1]
+        level = (b - 1) // 3 + 1
+        if b == nb:
+            xp = yp = 0
+            xl, yl = cw >> depth, ch >> depth
+        else:
+            xl, yl = cw >> level, ch >> level
+            kind = (b - 1) % 3
+            xp = xl if kind in (0, 2) else 0
+            yp = yl if kind in (0, 1) else 0
+        for by in range(yn):
+            for bx in range(xn):
+                if cbs[start + by * xn + bx]:
+                    q[yp + by * yl // yn:yp + (by + 1) * yl // yn, xp + bx * xl // xn:xp + (bx + 1) * xl // xn] = 0
+        if xn * yn == 1:
+            cbs[start] = 0
+        start += xn * yn
+    skip = np.zeros(nb, np.int32)
+    skip[2] = 1  # a skipped band: its indices are zero
+    xl, yl = cw >> 1, ch >> 1
+    q[0:yl, xl:2 * xl] = 0  # band 3 (level 1, kind 2) sits at (xl, 0)
+    s0 = sum(int(ncb[b, 0] * ncb[b, 1]) for b in range(2))
+    cbs[s0:s0 + int(ncb[2, 0] * ncb[2, 1])] = 0
+    coded = code_bands(1, depth, [q], [np.stack([np.zeros(nb, np.int32), skip], 1)], [ncb], [cbs], vlc=vlc)
+    assert coded[1][0][2] == 0
+    got, flags = decode_bands(depth, [q.shape], [skip], [ncb], coded[0], [coded[1][0]], vlc=vlc)
+    np.testing.assert_array_equal(got[0], q)
+    np.testing.assert_array_equal(flags[0], cbs)
