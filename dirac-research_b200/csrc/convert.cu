@@ -400,7 +400,7 @@ extern "C" int dgpu_rect_lp_filter(int16_t* pic, int w, int h, int stride, float
     int16_t* tmp = scratch;
     if (!tmp) {
         void* p = nullptr;
-        const int rc = library_scratch((size_t)w * h * sizeof(int16_t), &p);
+        const int rc = library_scratch((size_t)w * h * sizeof(int16_t), stream, &p);
         if (rc) return rc;
         tmp = static_cast<int16_t*>(p);
     }

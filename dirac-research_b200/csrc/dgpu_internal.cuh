@@ -35,12 +35,14 @@ void set_last_cuda_error(cudaError_t e, const char* what, const char* file, int 
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
-inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+constexpr size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-// Per-device scratch owned by the library: used when a caller passes scratch == NULL.
-// Grown with cudaMalloc on demand (synchronising the device first so that no kernel still
-// in flight uses the old buffer), kept until process exit.
-int library_scratch(size_t bytes, void** out);
+// Scratch owned by the library, one buffer per (device, stream): used when a caller passes
+// scratch == NULL.  Grown with cudaMalloc on demand; an outgrown buffer is kept (not freed)
+// until process exit, since another host thread may still hold it.  Calls on one stream are
+// ordered by the stream; calls that pass NULL scratch on the same stream from several host
+// threads at once share the buffer and race.
+int library_scratch(size_t bytes, void* stream, void** out);
 
 // Runs body(begin, end) over [0, n) split into chunks of at least `grain` items on the
 // library's host worker threads (a process-wide pool) and the calling thread; returns when

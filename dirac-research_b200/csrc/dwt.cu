@@ -786,7 +786,7 @@ extern "C" int dgpu_wavelet_transform_batch(int direction, int n, const int* fil
     }
     if (rc == DGPU_OK) {
         if (!scratch) {
-            rc = library_scratch(need, &scratch);
+            rc = library_scratch(need, stream, &scratch);
         } else if (scratch_bytes < need) {
             rc = DGPU_ERR_NOMEM;
         }

@@ -146,6 +146,7 @@ struct Encoder {
     int cur = -1;                // m_current_display_pnum
     int last_read = -1;          // m_last_picture_read
     int prepared = -1;           // picture prepared by dgpu_encoder_prepare_next, or -1
+    int failed = DGPU_OK;        // first failure of a picture's coding; sticky until reset
     bool eos = false;            // m_eos_signalled
     std::map<int, Pic> pics;
 
@@ -744,6 +745,7 @@ extern "C" int dgpu_encoder_reset(void* enc) {
     E->cur = -1;
     E->last_read = -1;
     E->prepared = -1;
+    E->failed = DGPU_OK;
     E->eos = false;
     return DGPU_OK;
 }
@@ -780,28 +782,45 @@ int finish_impl(Encoder* E, const float* ecf, const float* ecf_state, dgpu_pictu
 }  // namespace
 }  // namespace dgpu
 
+namespace dgpu {
+namespace {
+// A failure part-way through a picture's coding leaves its slot holding half-coded data (the
+// residue after SUBTRACT, or coefficients); coding on from there would be silently wrong, so
+// the failure is recorded and every later coding call returns it until dgpu_encoder_reset.
+int sticky(Encoder* E, int rc) {
+    if (rc < 0) E->failed = rc;
+    return rc;
+}
+}  // namespace
+}  // namespace dgpu
+
 extern "C" int dgpu_encoder_prepare_next(void* enc, dgpu_picture_info* info) {
     Encoder* E = static_cast<Encoder*>(enc);
     if (!E) return DGPU_ERR_ARG;
-    return prepare_impl(E, info);
+    if (E->failed) return E->failed;
+    return sticky(E, prepare_impl(E, info));
 }
 
 extern "C" int dgpu_encoder_finish_next(void* enc, const float* ecf, const float* ecf_state, dgpu_picture_info* info) {
     Encoder* E = static_cast<Encoder*>(enc);
     if (!E) return DGPU_ERR_ARG;
-    return finish_impl(E, ecf, ecf_state, info);
+    if (E->failed) return E->failed;
+    if (E->prepared < 0) return DGPU_ERR_ARG;  // nothing prepared: no state was touched
+    return sticky(E, finish_impl(E, ecf, ecf_state, info));
 }
 
 extern "C" int dgpu_encoder_code_next(void* enc, const float* ecf, dgpu_picture_info* info) {
     Encoder* E = static_cast<Encoder*>(enc);
     if (!E) return DGPU_ERR_ARG;
-    return code_next_impl(E, ecf, nullptr, info);
+    if (E->failed) return E->failed;
+    return sticky(E, code_next_impl(E, ecf, nullptr, info));
 }
 
 extern "C" int dgpu_encoder_code_next_adaptive(void* enc, const float* ecf_state, dgpu_picture_info* info) {
     Encoder* E = static_cast<Encoder*>(enc);
     if (!E || !ecf_state) return DGPU_ERR_ARG;
-    return code_next_impl(E, nullptr, ecf_state, info);
+    if (E->failed) return E->failed;
+    return sticky(E, code_next_impl(E, nullptr, ecf_state, info));
 }
 
 namespace dgpu {

@@ -35,6 +35,7 @@
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -1857,6 +1858,28 @@ size_t batch_bytes(const MeGeometry& g, const BatchArgs& A, std::vector<PicBufs>
     return a.used + 256;
 }
 
+// Largest per-CTA window staging of the pel kernels: blocks up to 64 x 64 (check_args) and a
+// search radius of at most 5, for each of the CTA's warps.
+constexpr size_t PEL_SMEM_MAX = align_up((size_t)64 * 64 + (size_t)(64 + 10) * (64 + 10), 8) * 2 * WARPS_PER_CTA;
+
+// Opts the pel kernels into PEL_SMEM_MAX bytes of dynamic shared memory once per device.  One
+// fixed value set under a lock, so a host thread never launches while another lowers it.
+int pel_smem_setup() {
+    static std::mutex mu;
+    static uint64_t done = 0;  // devices 0..63 already set up
+    int dev = 0;
+    DGPU_CHECK_CUDA(cudaGetDevice(&dev));
+    const uint64_t bit = dev < 64 ? (uint64_t)1 << dev : 0;
+    std::lock_guard<std::mutex> lock(mu);
+    if (bit && (done & bit)) return DGPU_OK;
+    DGPU_CHECK_CUDA(
+        cudaFuncSetAttribute(pel_lists_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PEL_SMEM_MAX));
+    DGPU_CHECK_CUDA(
+        cudaFuncSetAttribute(pel_wavefront_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PEL_SMEM_MAX));
+    done |= bit;
+    return DGPU_OK;
+}
+
 int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStream_t st) {
     std::vector<PicBufs> P;
     std::vector<TaskBufs> T;
@@ -1949,10 +1972,10 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
         const int xl = g.lb[2].xblen, yl = g.lb[2].yblen, rr = std::min(l + 1, 5);
         L.win_elems = (int)align_up((size_t)xl * yl + (size_t)(xl + 2 * rr) * (yl + 2 * rr), 8);
         const size_t smem = (size_t)L.win_elems * 2 * WARPS_PER_CTA;
-        if (smem > 48 * 1024) {
-            DGPU_CHECK_CUDA(cudaFuncSetAttribute(pel_lists_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            DGPU_CHECK_CUDA(
-                cudaFuncSetAttribute(pel_wavefront_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (smem > PEL_SMEM_MAX) return DGPU_ERR_SIZE;
+        {
+            const int rc = pel_smem_setup();
+            if (rc) return rc;
         }
         // the candidate-list phase covers every unit: one warp per unit
         pel_lists_kernel<<<(L.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, smem, st>>>(L);
@@ -2178,7 +2201,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
 
 int check_args(int cformat, int luma_depth, const MeGeometry& g) {
     if (cformat < 0 || cformat > 2 || luma_depth < 2 || luma_depth > 15) return DGPU_ERR_ARG;
-    if (g.lb[2].xblen > 64) return DGPU_ERR_SIZE;
+    if (g.lb[2].xblen > 64 || g.lb[2].yblen > 64) return DGPU_ERR_SIZE;
     return DGPU_OK;
 }
 
@@ -2263,7 +2286,7 @@ extern "C" int dgpu_motion_estimate_batch(int cformat, int w, int h, const dgpu_
     A.sbcost_out = sbcost_out;
     const size_t need = batch_bytes(g, A, nullptr, nullptr, nullptr, nullptr);
     if (!workspace) {
-        rc = library_scratch(need, &workspace);
+        rc = library_scratch(need, stream, &workspace);
         if (rc) return rc;
     } else if (ws_bytes < need) {
         return DGPU_ERR_NOMEM;

@@ -959,7 +959,7 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     // ---- workspace ----
     const size_t need = residue_ws_need(nb_total, ncb_total, dcwork_elems);
     if (!workspace) {
-        int rc = library_scratch(need, &workspace);
+        int rc = library_scratch(need, stream, &workspace);
         if (rc) return rc;
     } else if (ws_bytes < need) {
         return DGPU_ERR_NOMEM;

@@ -19,9 +19,19 @@ std::mutex g_err_mu;
 char g_last_error[512] = "";
 
 constexpr int kMaxDevices = 64;
+// One scratch buffer per (device, stream).  A buffer outgrown by a later call is retired, not
+// freed: a call on another host thread may still hold its pointer or have kernels queued on it,
+// so retired buffers live until process exit (growth is geometric, so they add up to less than
+// the live buffer).
+struct Scratch {
+    int dev;
+    void* stream;
+    void* p;
+    size_t bytes;
+};
 std::mutex g_scratch_mu;
-void* g_scratch[kMaxDevices] = {};
-size_t g_scratch_bytes[kMaxDevices] = {};
+std::vector<Scratch> g_scratch;
+std::vector<void*> g_retired;
 std::atomic<unsigned long long> g_launches{0};
 }  // namespace
 
@@ -33,28 +43,30 @@ void set_last_cuda_error(cudaError_t e, const char* what, const char* file, int 
     std::snprintf(g_last_error, sizeof(g_last_error), "%s: %s (%s:%d)", cudaGetErrorString(e), what, file, line);
 }
 
-int library_scratch(size_t bytes, void** out) {
+int library_scratch(size_t bytes, void* stream, void** out) {
     int dev = 0;
     DGPU_CHECK_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return DGPU_ERR_DEVICE;
     std::lock_guard<std::mutex> lk(g_scratch_mu);
-    if (g_scratch_bytes[dev] < bytes) {
-        if (g_scratch[dev]) {
-            // kernels queued earlier may still read the old buffer
-            DGPU_CHECK_CUDA(cudaDeviceSynchronize());
-            cudaFree(g_scratch[dev]);
-            g_scratch[dev] = nullptr;
-            g_scratch_bytes[dev] = 0;
-        }
-        size_t want = align_up(bytes, 1 << 20);
-        if (cudaMalloc(&g_scratch[dev], want) != cudaSuccess) {
+    Scratch* s = nullptr;
+    for (Scratch& e : g_scratch)
+        if (e.dev == dev && e.stream == stream) s = &e;
+    if (!s) {
+        g_scratch.push_back(Scratch{dev, stream, nullptr, 0});
+        s = &g_scratch.back();
+    }
+    if (s->bytes < bytes) {
+        const size_t want = align_up(std::max(bytes, 2 * s->bytes), 1 << 20);
+        void* p = nullptr;
+        if (cudaMalloc(&p, want) != cudaSuccess) {
             cudaGetLastError();
-            g_scratch[dev] = nullptr;
             return DGPU_ERR_NOMEM;
         }
-        g_scratch_bytes[dev] = want;
+        if (s->p) g_retired.push_back(s->p);
+        s->p = p;
+        s->bytes = want;
     }
-    *out = g_scratch[dev];
+    *out = s->p;
     return DGPU_OK;
 }
 

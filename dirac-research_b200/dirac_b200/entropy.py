@@ -74,7 +74,8 @@ def decode_bands(depth, shapes, band_skip, ncb, data, band_bytes, vlc=False):
     cbs = np.zeros(sum(ncbt), np.uint8)
     _lib.check(lib.dgpu_decode_bands_host(
         n, _lib.int_array(depth), _lib.int_array([s[1] for s in shapes]), _lib.int_array([s[0] for s in shapes]),
-        nc.ctypes.data_as(_lib.P_int), bs.ctypes.data_as(_lib.P_int), d.ctypes.data, bb.ctypes.data_as(_lib.P_int),
+        nc.ctypes.data_as(_lib.P_int), bs.ctypes.data_as(_lib.P_int), d.ctypes.data, len(data),
+        bb.ctypes.data_as(_lib.P_int),
         int(bool(vlc)), _lib.ptr_array([a.ctypes.data for a in q]), cbs.ctypes.data), "dgpu_decode_bands_host")
     flags, k = [], 0
     for t in ncbt:

@@ -13,6 +13,16 @@
  * stored as u8 - 128, libdirac_common/pic_io.cpp:388-399) and wavelet coefficients are int32
  * (CoeffType of the reference's plain-C build, libdirac_common/common.h:72-78).  Strides are
  * in elements.
+ *
+ * Scratch passed as NULL: the entry points that take a scratch or workspace pointer
+ * (dgpu_wavelet_transform[_batch], dgpu_motion_estimate[_batch], dgpu_code_residue_batch,
+ * dgpu_rect_lp_filter) then use a buffer the library owns, one per (device, stream), grown
+ * with cudaMalloc on first use and on growth.  Calls on one stream are ordered by it, so they
+ * may share that buffer; calls on the same stream issued from several host threads at once
+ * race on it and must be serialised by the caller.  Calls on different streams use different
+ * buffers.  An outgrown buffer is never freed while the process runs (another thread may
+ * still hold it), so the library's scratch grows to at most twice the largest need per stream.
+ * Callers that must not allocate pass their own scratch.
  */
 #ifndef DIRAC_GPU_H
 #define DIRAC_GPU_H
@@ -70,8 +80,8 @@ unsigned long long dgpu_launch_count(void);
  * be at least 6 for DD9_7/DD13_7, 4 for LEGALL5_3/DAUB9_7 and 2 for HAAR0/HAAR1.
  *
  * scratch: device memory of at least dgpu_dwt_scratch_bytes(cw, ch, depth) bytes holding the
- * intermediate low-pass bands, or NULL to let the library use its own per-device buffer
- * (grown with cudaMalloc on first use).
+ * intermediate low-pass bands, or NULL to let the library use its own buffer for the stream
+ * (see "Scratch passed as NULL" above).
  * ------------------------------------------------------------------------------------- */
 size_t dgpu_dwt_scratch_bytes(int cw, int ch, int depth);
 
@@ -399,7 +409,10 @@ int dgpu_encoder_load(void* encoder, const void* const* planes, int on_host);
 int dgpu_encoder_end_sequence(void* encoder);
 /* Codes the next picture in coding order.  ecf: NULL, or [3][3*depth+1] entropy-correction
  * factors for this picture (the caller's EntropyCorrector::Factor values).  Returns 1 and
- * fills info when a picture was coded, 0 when more input (or nothing) remains. */
+ * fills info when a picture was coded, 0 when more input (or nothing) remains.
+ * A failure part-way through a picture (this call, _adaptive, prepare_next or finish_next)
+ * leaves that picture half coded; it is sticky: every later coding call of the encoder
+ * returns the same error code until dgpu_encoder_reset. */
 int dgpu_encoder_code_next(void* encoder, const float* ecf, dgpu_picture_info* info);
 /* As dgpu_encoder_code_next, with the caller's whole EntropyCorrector state (the
  * [3][3][3*depth+1] layout of dgpu_entropy_init): the encoder takes the picture's factors
@@ -560,10 +573,11 @@ int dgpu_code_bands_vlc_host(int n, const int* intra, const int* depth, const in
  * cw[c] x ch[c] int32) is written in full (zeros in skipped bands and code blocks); cb_skip
  * receives the decoded code-block skip flags (band-list order, components concatenated).  The
  * bands of a level are decoded in parallel, levels from coarse to fine (a band's contexts
- * read its parent band).  No GPU use. */
+ * read its parent band).  data_bytes is the length of data: band lengths that add up to more
+ * (a corrupt or truncated stream) return DGPU_ERR_ARG before any band is decoded.  No GPU use. */
 int dgpu_decode_bands_host(int n, const int* depth, const int* cw, const int* ch, const int* band_ncb,
-                           const int* band_skip, const uint8_t* data, const int* band_bytes, int vlc,
-                           int32_t* const* qindex, uint8_t* cb_skip);
+                           const int* band_skip, const uint8_t* data, size_t data_bytes,
+                           const int* band_bytes, int vlc, int32_t* const* qindex, uint8_t* cb_skip);
 int dgpu_entropy_init(int depth, float* state);
 int dgpu_entropy_factors(int depth, const float* state, int intra, int is_b, float* ecf);
 int dgpu_entropy_update(int depth, float* state, int intra, int is_b, int comp, const int* band_skip,

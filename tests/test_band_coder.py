@@ -306,3 +306,24 @@ def test_round_trip_extreme_indices(vlc):
     got, flags = decode_bands(depth, [q.shape], [skip], [ncb], coded[0], [coded[1][0]], vlc=vlc)
     np.testing.assert_array_equal(got[0], q)
     np.testing.assert_array_equal(flags[0], cbs)
+
+
+@pytest.mark.parametrize("vlc", [False, True])
+def test_decoder_rejects_band_lengths_past_the_data(vlc):
+    """Band lengths come from the stream's subband headers: when they add up to more than the
+    data the caller holds (a truncated or corrupt stream), the decoder refuses before reading."""
+    from dirac_b200._lib import DgpuError
+    from dirac_b200.entropy import code_bands, decode_bands
+
+    rng = np.random.default_rng(11)
+    depth, cw, ch = 2, 32, 32
+    q = rng.integers(-20, 21, size=(ch, cw)).astype(np.int32)
+    nb = 3 * depth + 1
+    ncb = np.ones((nb, 2), np.int32)
+    skip = np.zeros(nb, np.int32)
+    cbs = np.zeros(nb, np.uint8)
+    coded = code_bands(1, depth, [q], [np.stack([np.zeros(nb, np.int32), skip], 1)], [ncb], [cbs], vlc=vlc)
+    got, _ = decode_bands(depth, [q.shape], [skip], [ncb], coded[0], [coded[1][0]], vlc=vlc)
+    np.testing.assert_array_equal(got[0], q)
+    with pytest.raises(DgpuError):
+        decode_bands(depth, [q.shape], [skip], [ncb], coded[0][:-1], [coded[1][0]], vlc=vlc)

@@ -82,3 +82,54 @@ def test_static_round_trip_and_size_limit(gpu):
     rc = lib.dgpu_wavelet_transform_static(0, filt, 4, _ptr(pic), big_w, big_h, big_w, _ptr(coeff), big_w,
                                            big_h, big_w, stream)
     assert rc == -2  # DGPU_ERR_SIZE
+
+
+_NO_ALLOC_CHILD = r"""
+import ctypes, os, sys
+sys.path.insert(0, sys.argv[1])
+import dirac_b200
+lib = dirac_b200.load()          # library registered before the context exists (eager loading)
+import torch
+w, h, depth = 1920, 1080, 4
+cw, ch = dirac_b200.padded_size(w, h, depth)
+pic = torch.randint(-128, 128, (h, w), dtype=torch.int16, device="cuda")
+coeff = torch.zeros((ch, cw), dtype=torch.int32, device="cuda")
+back = torch.zeros_like(pic)
+torch.cuda.synchronize()
+P = lambda t: ctypes.c_void_p(t.data_ptr())
+def static_pair():
+    assert lib.dgpu_wavelet_transform_static(0, 6, depth, P(pic), w, h, w, P(coeff), cw, ch, cw, None) == 0
+    assert lib.dgpu_wavelet_transform_static(1, 6, depth, P(back), w, h, w, P(coeff), cw, ch, cw, None) == 0
+    torch.cuda.synchronize()
+free0 = torch.cuda.mem_get_info()[0]
+static_pair()                    # the first call on the device (symbol lookup)
+free1 = torch.cuda.mem_get_info()[0]
+for _ in range(4):
+    static_pair()
+free2 = torch.cuda.mem_get_info()[0]
+assert torch.equal(back, pic)
+# the same measurement sees the scratch-taking entry point's library buffer being created
+assert lib.dgpu_wavelet_transform(0, 6, depth, P(pic), w, h, w, P(coeff), cw, ch, cw, None, 0, None) == 0
+torch.cuda.synchronize()
+free3 = torch.cuda.mem_get_info()[0]
+print(free0, free1, free2, free3)
+"""
+
+
+def test_static_entry_point_allocates_nothing(gpu):
+    """In a fresh process with every module loaded eagerly: device free memory is the same
+    before the first static call, after it and after four more forward + inverse pairs; the
+    scratch-taking entry point with NULL scratch, run afterwards, does lower it (the library's
+    own buffer), so the measurement would see an allocation on the static path."""
+    import os
+    import subprocess
+    import sys
+
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "dirac-research_b200")
+    env = dict(os.environ, CUDA_MODULE_LOADING="EAGER")
+    r = subprocess.run([sys.executable, "-c", _NO_ALLOC_CHILD, pkg], env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    free0, free1, free2, free3 = map(int, r.stdout.split()[-4:])
+    assert free0 == free1 == free2, (free0, free1, free2)
+    assert free3 < free2, (free2, free3)
