@@ -3,7 +3,7 @@
 Needs oracle/_ref/libdirac_ref.so (the reference's own C++, plain-C build, compiled from
 its sources by `make -C oracle`).  Inputs are seeded, so re-running reproduces the files.
 
-    python tests/golden/make_golden.py [dwt convert mc me quant encode decode adaptive bands prefilter]
+    python tests/golden/make_golden.py [dwt convert mc me quant encode decode adaptive bands prefilter hd1080 uhd]
 """
 import os
 import sys
@@ -177,6 +177,112 @@ def encode_inputs(case):
     return seq, cfg
 
 
+# The 1080p coding workload the bench times: 1920x1080 4:2:0 8-bit, 24 rectangles moving at up to
+# 24 px/frame, the HD1080P50 preset (L1 separation 3, 7 L1 pictures per GOP), QF 7, DAUB9_7 intra /
+# DD9_7 inter depth 4, OBMC 16x16 at separation 12, quarter-pel motion vectors.  The fixture codes
+# the first HD_FRAMES frames of the bench's 32-frame sequence (seed 1000) as one sequence, as the
+# bench's CPU baseline does.
+HD_PARAMS = dict(video_format=14, cformat=2, width=1920, height=1080, qf=7.0, l1_sep=3, num_l1=7, cpd=32.0,
+                 xblen=16, yblen=16, xbsep=12, ybsep=12, mv_precision=2, intra_filter=6, inter_filter=0,
+                 wlt_depth=4)
+HD_FRAMES = 10
+HD_SEQUENCE_FRAMES = 32
+HD_SEED = 1000
+
+
+def hd_inputs():
+    """8-bit frames of the 1080p case and its RefEncParams fields."""
+    sys.path.insert(0, os.path.join(HERE, "..", "..", "dirac-research_b200"))
+    from dirac_b200 import synth
+
+    seq = synth.make_sequence(1920, 1080, HD_SEQUENCE_FRAMES, n_rects=24, vmax=24, seed=HD_SEED, bit_depth=8,
+                              chroma="420")
+    return seq[:HD_FRAMES], dict(HD_PARAMS)
+
+
+def hd_cases():
+    """The reference encoder on the 1080p case through its public API, with the initial
+    entropy-correction factors kept (frozen) and as it ships (adaptive), arithmetic coding:
+    CRC-32 of every locally decoded plane, the picture types and the bitstream's length and
+    CRC-32; and the reference decoder's CRC-32s of that bitstream decoded."""
+    import zlib
+
+    from oracle import reference_decode, reference_encode_stream
+
+    seq, cfg = hd_inputs()
+    out = {}
+    for tag, freeze in (("frozen", True), ("adaptive", False)):
+        rec, ptype, stream = reference_encode_stream(cfg, seq, freeze=freeze)
+        out[tag + "_crc"] = np.array([[zlib.crc32(np.ascontiguousarray(p).tobytes()) for p in f] for f in rec],
+                                     np.uint32)
+        out[tag + "_ptype"] = ptype
+        out[tag + "_stream_bytes"] = np.array(len(stream), np.int64)
+        out[tag + "_stream_crc"] = np.array(zlib.crc32(bytes(stream)), np.uint32)
+        dec = reference_decode(stream, cfg["width"], cfg["height"], cfg["cformat"], len(seq))
+        if any(f is None for f in dec):
+            raise RuntimeError("hd1080: the reference decoder did not deliver every frame")
+        out[tag + "_decode_crc"] = np.array([[zlib.crc32(np.ascontiguousarray(p).tobytes()) for p in f]
+                                             for f in dec], np.uint32)
+    return out
+
+
+# The 3840x2160 4:2:2 10-bit workload: 48 rectangles moving at up to 64 px/frame, Deslauriers-Dubuc
+# (9,7) depth 5, OBMC 16x16 at separation 12, quarter-pel vectors, motion estimation over the
+# reference's pyramid of depth 7 (pixel_match.cpp:94-95 at this size).  Frame 1 is a B picture
+# between frames 0 and 2.
+UHD_SIZE = (3840, 2160)
+UHD_SEED = 2160
+UHD_LAMBDA = 10.0
+
+
+def uhd_inputs():
+    """Three 10-bit 4:2:2 frames as int16 codec samples, and the block parameters."""
+    sys.path.insert(0, os.path.join(HERE, "..", "..", "dirac-research_b200"))
+    from dirac_b200 import synth
+    from oracle import BlockParams
+
+    w, h = UHD_SIZE
+    seq = synth.make_sequence(w, h, 3, n_rects=48, vmax=64, seed=UHD_SEED, bit_depth=10, chroma="422")
+    frames = [[synth.to_signed(p, 10) for p in fr] for fr in seq]
+    bp = BlockParams(2, 16, 16, 12, 12, (w + 47) // 48, (h + 47) // 48)
+    return frames, bp
+
+
+def crc(a):
+    import zlib
+
+    return zlib.crc32(np.ascontiguousarray(a).tobytes())
+
+
+def uhd_cases(ref):
+    """The reference's stages on the 4K workload (CRC-32s, the arrays being tens of MB): motion
+    estimation of the B picture (stages 1-3), OBMC SUBTRACT and ADD with those motion data,
+    upconversion of a reference, and forward and inverse DD9_7 depth-5 transforms of each
+    component of the B picture."""
+    f, bp = uhd_inputs()
+    out = {}
+    me = ref.motion_estimate(1, f[1], f[0], f[2], bp, UHD_LAMBDA, 3, luma_depth=10)
+    for k, v in me.items():
+        out["me_" + k] = np.array(crc(v), np.uint32)
+    nref = me["mv"].shape[0]
+    mv1, mv2 = me["mv"][0], me["mv"][1 if nref > 1 else 0]
+    for aos in (0, 1):
+        res = ref.motion_compensate(aos, 1, f[1], f[0], f[2], bp, mv1, mv2, me["mode"], me["dc"], me["split"],
+                                    luma_depth=10, chroma_depth=10)
+        out[f"mc{aos}"] = np.array([crc(c) for c in res], np.uint32)
+    out["up"] = np.array([crc(ref.upconvert(c, 10)) for c in f[0]], np.uint32)
+    fwd, back = [], []
+    for c in range(3):
+        pic = f[1][c]
+        co = ref.dwt_forward(0, 5, pic)
+        fwd.append(crc(co))
+        back.append(crc(ref.dwt_backward(0, 5, co, pic.shape[1], pic.shape[0])))
+    out["dwt_fwd"] = np.array(fwd, np.uint32)
+    out["dwt_back"] = np.array(back, np.uint32)
+    out["in"] = np.array([[crc(c) for c in fr] for fr in f], np.uint32)
+    return out
+
+
 def encode_cases():
     """The reference encoder run through its public API (initial entropy-correction factors
     kept, as a coding loop without the arithmetic coder does): CRC-32 of every locally
@@ -311,12 +417,14 @@ BAND_CASES = [(1, 1, 4, 176, 144, 5.0), (0, 0, 4, 176, 144, 30.0), (1, 6, 3, 88,
 def main(argv=None):
     """Writes the named fixtures (default: all)."""
     names = (argv if argv is not None else sys.argv[1:]) or ["dwt", "convert", "mc", "me", "quant", "encode",
-                                                              "decode", "adaptive", "bands", "prefilter"]
+                                                              "decode", "adaptive", "bands", "prefilter",
+                                                              "hd1080", "uhd"]
     ref = Reference()
     makers = {"dwt": lambda: dwt_cases(ref), "convert": lambda: conv_cases(ref), "mc": lambda: mc_cases(ref),
               "me": lambda: me_cases(ref), "quant": lambda: quant_cases(ref), "encode": encode_cases,
               "decode": decode_cases, "adaptive": adaptive_cases, "bands": lambda: band_cases(ref),
-              "prefilter": lambda: prefilter_cases(ref)}
+              "prefilter": lambda: prefilter_cases(ref), "hd1080": hd_cases,
+              "uhd": lambda: uhd_cases(ref)}
     for n in names:
         np.savez_compressed(os.path.join(HERE, n + ".npz"), **makers[n]())
     print("wrote " + ", ".join(n + ".npz" for n in names))

@@ -17,16 +17,15 @@ sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
 from make_golden import ENCODE_CASES, encode_inputs  # noqa: E402
 
 
-@pytest.mark.parametrize("case", ENCODE_CASES, ids=[c[0] for c in ENCODE_CASES])
-def test_device_encoder_with_host_coder_matches_stock_reference(gpu, golden, case):
+def adaptive_encode(seq, cfg):
+    """Codes seq with the device encoder and the host band coder adapting the entropy-correction
+    state picture by picture (the stock reference encoder's loop); returns the locally decoded
+    output planes and intra flags by picture number."""
     from dirac_b200 import encoder as E
     from dirac_b200 import quant
     from dirac_b200.encoder import SequenceEncoder
     from dirac_b200.entropy import EntropyCorrector, code_bands
-    from test_encoder_gpu import encoder_params
 
-    seq, rcfg = encode_inputs(case)
-    cfg = encoder_params(rcfg)
     depth = cfg["wlt_depth"]
     ncb = quant.code_blocks(depth, cfg["width"], cfg["height"])
     ec = EntropyCorrector(depth)
@@ -51,6 +50,15 @@ def test_device_encoder_with_host_coder_matches_stock_reference(gpu, golden, cas
         outputs[pn] = [enc.read(pn, E.OUTPUT, c) for c in range(3)]
         ptype[pn] = info["intra"]
     enc.close()
+    return outputs, ptype
+
+
+@pytest.mark.parametrize("case", ENCODE_CASES, ids=[c[0] for c in ENCODE_CASES])
+def test_device_encoder_with_host_coder_matches_stock_reference(gpu, golden, case):
+    from test_encoder_gpu import encoder_params
+
+    seq, rcfg = encode_inputs(case)
+    outputs, ptype = adaptive_encode(seq, encoder_params(rcfg))
     g = golden("adaptive.npz")
     crc = np.array([[zlib.crc32(np.ascontiguousarray(outputs[i][c]).tobytes()) for c in range(3)]
                     for i in range(len(seq))], np.uint32)
@@ -118,3 +126,21 @@ def test_pipelined_host_coding_matches_stock_reference(gpu, golden, case):
     crc = np.array([[zlib.crc32(np.ascontiguousarray(outputs[i][c]).tobytes()) for c in range(3)]
                     for i in range(len(seq))], np.uint32)
     np.testing.assert_array_equal(crc, g[case[0] + "_crc"])
+
+
+def test_hd1080_with_host_coder_matches_stock_reference(gpu, golden):
+    """The bench's 1080p workload (first 10 frames of its sequence) coded as the stock reference
+    encoder codes it: device encoder, host band coder, factors adapted after every picture.
+    Every locally decoded plane equals the stock reference encoder's (hd1080.npz, adaptive),
+    which its own decoder reproduces from its bitstream."""
+    from make_golden import hd_inputs
+    from test_encoder_gpu import encoder_params
+
+    seq, rcfg = hd_inputs()
+    outputs, ptype = adaptive_encode(seq, encoder_params(rcfg))
+    g = golden("hd1080.npz")
+    crc = np.array([[zlib.crc32(np.ascontiguousarray(outputs[i][c]).tobytes()) for c in range(3)]
+                    for i in range(len(seq))], np.uint32)
+    np.testing.assert_array_equal([ptype[i] for i in range(len(seq))], g["adaptive_ptype"])
+    np.testing.assert_array_equal(crc, g["adaptive_crc"])
+    np.testing.assert_array_equal(g["adaptive_crc"], g["adaptive_decode_crc"])

@@ -110,3 +110,63 @@ def test_picture_batch_matches_oracle(gpu, oracle):
                 np.testing.assert_array_equal(b[:, 2], res["bits"][c], err_msg=cm)
                 np.testing.assert_array_equal(batch.read(k, CBSKIP, c), res["cb_skip"][c], err_msg=cm)
     batch.close()
+
+
+# Filters and transform depths given to the full-size pictures in turn, so that every filter of
+# the heterogeneous workload (both Haar shifts, LeGall (5,3), Deslauriers-Dubuc (13,7), Fidelity,
+# Daubechies (9,7)) and every depth (3-5) occurs at the workload's real sizes.
+FULL_SIZE_FILTERS = [3, 1, 2, 5, 6, 4, 6, 2]
+FULL_SIZE_DEPTHS = [3, 4, 5, 3, 4, 5, 5, 4]
+
+
+def test_heterogeneous_workload_at_full_size_matches_oracle(gpu, oracle):
+    """The bench's heterogeneous batch at its real picture sizes: two pictures (one P, one B) of
+    each class -- 352x288 4:2:0 8-bit, 720x576 4:2:0 8-bit, 1280x720 4:2:0 10-bit, 1920x1080
+    4:2:2 10-bit -- with motion from the library's estimation, coded in one batch; every picture
+    equal bit for bit to the oracle's coding of it alone, on a first and a replayed run."""
+    import torch
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(__file__)), "oracle"))
+    from oracle_encoder import code_picture
+
+    from dirac_b200 import hetero as H
+    from dirac_b200 import quant
+    from dirac_b200.batch import BANDS, CBSKIP, QINDEX, RECON, PictureBatch
+
+    pictures, motion, planes, keep = H.make_inputs(per_class=2, seed=5)
+    for k, p in enumerate(pictures):
+        p["filter"], p["wlt_depth"] = FULL_SIZE_FILTERS[k], FULL_SIZE_DEPTHS[k]
+    assert [(p["width"], p["height"], p["cformat"], p["luma_depth"]) for p in pictures[::2]] == \
+        [(352, 288, 2, 8), (720, 576, 2, 8), (1280, 720, 2, 10), (1920, 1080, 1, 10)]
+    want = []
+    for p, m, pl in zip(pictures, motion, planes):
+        bp = p["bp"]
+        op = dict(p, mv_precision=bp.precision, xblen=bp.xblen, yblen=bp.yblen, xbsep=bp.xbsep, ybsep=bp.ybsep)
+        refs = [[t.cpu().numpy() for t in m["ref1"]]]
+        mvs = [m["mv1"].cpu().numpy()]
+        if m["ref2"] is not None:
+            refs.append([t.cpu().numpy() for t in m["ref2"]])
+            mvs.append(m["mv2"].cpu().numpy())
+        me = {"mv": mvs, "mode": m["mode"].cpu().numpy(), "dc": m["dc"].cpu().numpy(),
+              "split": m["split"].cpu().numpy()}
+        want.append(code_picture(op, [t.cpu().numpy() for t in pl], quant.band_weights, quant.code_blocks, oracle,
+                                 refs=refs, me=me))
+    batch = PictureBatch(pictures, motion)
+    for run in range(2):
+        load_planes(batch, planes)
+        batch.run()
+        torch.cuda.synchronize()
+        for k, (data, res) in enumerate(want):
+            msg = f"run {run} picture {k}"
+            nb = 3 * pictures[k]["wlt_depth"] + 1
+            for c in range(3):
+                cm = f"{msg} component {c}"
+                np.testing.assert_array_equal(batch.read(k, RECON, c), data[c].ravel(), err_msg=cm)
+                np.testing.assert_array_equal(batch.read(k, QINDEX, c), res["qindex"][c].ravel(), err_msg=cm)
+                b = batch.read(k, BANDS, c).reshape(nb, 3)
+                sk = res["skip"][c]
+                np.testing.assert_array_equal(b[:, 1], sk, err_msg=cm)
+                np.testing.assert_array_equal(b[:, 0][sk == 0], res["qidx"][c][sk == 0], err_msg=cm)
+                np.testing.assert_array_equal(batch.read(k, CBSKIP, c), res["cb_skip"][c], err_msg=cm)
+    batch.close()
+    del keep

@@ -236,3 +236,20 @@ def test_encoder_group_rejects_mixed_geometry(gpu):
         EncoderGroup([a, a])
     a.close()
     b.close()
+
+
+def test_encoder_hd1080_matches_reference(gpu, golden):
+    """The bench's 1080p coding workload (HD1080P50 GOP, QF 7, DAUB9_7 / DD9_7 depth 4, OBMC
+    16/12, quarter-pel): the first 10 frames of its sequence coded by the device encoder with the
+    initial entropy-correction factors, every locally decoded plane equal to the reference
+    encoder's (tests/golden/hd1080.npz, frozen factors), picture types included."""
+    from make_golden import hd_inputs
+
+    seq, cfg = hd_inputs()
+    infos, results = run_device(gpu, seq, cfg)
+    g = golden("hd1080.npz")
+    crc = np.array([[zlib.crc32(np.ascontiguousarray(results[i]["output"][c]).tobytes()) for c in range(3)]
+                    for i in range(len(seq))], np.uint32)
+    np.testing.assert_array_equal([int(i["intra"]) for i in sorted(infos, key=lambda i: i["pnum"])],
+                                  g["frozen_ptype"])
+    np.testing.assert_array_equal(crc, g["frozen_crc"])
