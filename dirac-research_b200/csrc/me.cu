@@ -48,6 +48,21 @@ constexpr int WARPS_PER_CTA = 4;
 constexpr int ME_THREADS = 32 * WARPS_PER_CTA;
 constexpr long long SPIN_LIMIT = 1LL << 21;  // about 2 s of polling at the longest back-off
 
+// Failure-detection and ordering checks of a wavefront launch (dgpu_debug_wavefront): the
+// polls after which a wait gives up, a unit whose completion flag is left unset so that its
+// dependants' waits run out (pel wavefront only; -1: none), and an optional audit array that
+// receives, for every unit of the launch's first job, the position at which it was decided
+// ([0] is the running counter).  Normal calls carry {SPIN_LIMIT, -1, nullptr}.
+struct WaveDebug {
+    long long spin_limit;
+    int skip_unit;
+    int* audit;
+};
+
+__device__ __forceinline__ void audit_unit(const WaveDebug& d, int job, int unit) {
+    if (d.audit && job == 0) d.audit[1 + unit] = atomicAdd(d.audit, 1);
+}
+
 struct Olb {
     int xblen, yblen, xbsep, ybsep, xoff, yoff;
 };
@@ -127,17 +142,17 @@ __device__ __forceinline__ void publish(int* flag) {
     f.store(1, cuda::memory_order_release);
 }
 
-// Every lane waits (acquire) until *flag is set; gives up after SPIN_LIMIT polls and records
-// the failure in *err (the host turns it into DGPU_ERR_CUDA).
-// Once any wait has timed out, every later wait returns at once, so a failed launch ends
-// within about one timeout.
-__device__ __forceinline__ void wait_flag(int* flag, int* err) {
+// Every lane waits (acquire) until *flag is set; gives up after `limit` polls and records the
+// failure in *err (the host turns it into DGPU_ERR_CUDA).
+// Once any wait has timed out, every later wait returns within 1024 polls, so a failed launch
+// ends within about one timeout.
+__device__ __forceinline__ void wait_flag(int* flag, int* err, long long limit) {
     cuda::atomic_ref<int, cuda::thread_scope_device> f(*flag);
     cuda::atomic_ref<int, cuda::thread_scope_device> e(*err);
     long long n = 0;
     unsigned ns = 32;
     while (f.load(cuda::memory_order_acquire) == 0) {
-        if (++n > SPIN_LIMIT || ((n & 1023) == 0 && e.load(cuda::memory_order_relaxed) != 0)) {
+        if (++n > limit || ((n & 1023) == 0 && e.load(cuda::memory_order_relaxed) != 0)) {
             atomicOr(err, 1);
             return;
         }
@@ -702,6 +717,7 @@ struct PelLaunch {
     int* err;
     const PelJob* jobs;     // device table
     Wave wave;
+    WaveDebug dbg;
 };
 
 // Best candidate of one list (BlockMatcher::FindBestMatchPel over the list, PelBlockDiff::Diff
@@ -837,10 +853,10 @@ __global__ void __launch_bounds__(ME_THREADS) pel_wavefront_kernel(const __grid_
         // the block's own samples do not depend on the neighbours: load them before waiting
         const Blim bl = block_limits(L.o, J.pw, J.ph, bx, by);
         if (bl.xl > 0 && bl.yl > 0) stage_rect(wmem, J.pic, J.pw, J.ph, bl.xp, bl.yp, bl.xl, bl.yl);
-        if (bx > 0) wait_flag(&J.flags[b - 1], L.err);
+        if (bx > 0) wait_flag(&J.flags[b - 1], L.err, L.dbg.spin_limit);
         if (by > 0) {
-            wait_flag(&J.flags[b - W], L.err);
-            if (bx < W - 1) wait_flag(&J.flags[b - W + 1], L.err);
+            wait_flag(&J.flags[b - W], L.err, L.dbg.spin_limit);
+            if (bx < W - 1) wait_flag(&J.flags[b - W + 1], L.err, L.dbg.spin_limit);
         }
         const short2* mv = J.mv;
         short2 pred = make_short2(0, 0);
@@ -877,7 +893,8 @@ __global__ void __launch_bounds__(ME_THREADS) pel_wavefront_kernel(const __grid_
             J.cost[3 * b] = sad;
             J.cost[3 * b + 1] = mvcost;
             J.cost[3 * b + 2] = sad + 0.0f * mvcost;
-            publish(&J.flags[b]);
+            audit_unit(L.dbg, jn, b);
+            if (u != L.dbg.skip_unit) publish(&J.flags[b]);
         }
         __syncwarp();
     }
@@ -905,6 +922,7 @@ struct SubLaunch {
     int* err;
     const SubJob* jobs;  // device table
     Wave wave;
+    WaveDebug dbg;
 };
 
 struct Cost3 {
@@ -972,7 +990,7 @@ __global__ void __launch_bounds__(ME_THREADS, 8) subpel_wavefront_kernel(const _
         for (int i = 0; i < 4; ++i) {
             const int x = bx + nsx[i], y = by + nsy[i];
             if (all || (x >= 0 && y >= 0 && x < W && y < H)) {
-                wait_flag(&J.flags[y * W + x], L.err);
+                wait_flag(&J.flags[y * W + x], L.err, L.dbg.spin_limit);
                 nbr[n++] = __ldcg(&J.mv[y * W + x]);
             }
         }
@@ -1057,6 +1075,7 @@ __global__ void __launch_bounds__(ME_THREADS, 8) subpel_wavefront_kernel(const _
             J.cost[3 * b] = out_cost.SAD;
             J.cost[3 * b + 1] = out_cost.mvcost;
             J.cost[3 * b + 2] = out_cost.total;
+            audit_unit(L.dbg, jn, b);
             publish(&J.flags[b]);
         }
         __syncwarp();
@@ -1098,6 +1117,7 @@ struct ModeLaunch {
     int* err;
     const ModeJob* jobs;  // device table
     Wave wave;
+    WaveDebug dbg;
 };
 
 // ModeDecider::DoME: the unit's four guide vectors as candidates (BlockMatcher::FindBestMatchSubp).
@@ -1341,10 +1361,10 @@ __global__ void __launch_bounds__(ME_THREADS, 5) mode_wavefront_kernel(const __g
                 }
         }
         if (threadIdx.x == 0) {
-            if (xsb > 0) wait_flag(&J.flags[s - 1], L.err);
+            if (xsb > 0) wait_flag(&J.flags[s - 1], L.err, L.dbg.spin_limit);
             if (ysb > 0) {
-                wait_flag(&J.flags[s - J.xnsb], L.err);
-                if (xsb > 0) wait_flag(&J.flags[s - J.xnsb - 1], L.err);
+                wait_flag(&J.flags[s - J.xnsb], L.err, L.dbg.spin_limit);
+                if (xsb > 0) wait_flag(&J.flags[s - J.xnsb - 1], L.err, L.dbg.spin_limit);
             }
         }
         __syncthreads();
@@ -1464,7 +1484,10 @@ __global__ void __launch_bounds__(ME_THREADS, 5) mode_wavefront_kernel(const __g
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0) publish(&J.flags[s]);
+        if (threadIdx.x == 0) {
+            audit_unit(L.dbg, jn, s);
+            publish(&J.flags[s]);
+        }
     }
 }
 
@@ -1747,18 +1770,6 @@ size_t task_layout(const MeGeometry& g, TaskBufs& T, Arena& a, Arena& fa, Arena&
     return a.used;
 }
 
-template <class Launch, class Kernel>
-int launch_wavefront(Launch& L, Kernel kernel, int* ctl, cudaStream_t st) {
-    if (L.total == 0) return DGPU_OK;
-    L.ticket = ctl;
-    L.err = ctl + 1;
-    DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
-    const int grid = std::min((L.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, 148 * 8);
-    kernel<<<grid, ME_THREADS, 0, st>>>(L);
-    DGPU_CHECK_LAUNCH();
-    return DGPU_OK;
-}
-
 struct BatchArgs {
     int cformat, w, h, luma_depth, stages, prec;
     int npics, ntasks;
@@ -1880,7 +1891,22 @@ int pel_smem_setup() {
     return DGPU_OK;
 }
 
+// Process-wide settings of dgpu_debug_wavefront, read once by each motion-estimation call.
+struct DebugSettings {
+    int skip_unit = -1;
+    long long spin_limit = SPIN_LIMIT;
+    int* audit[3] = {nullptr, nullptr, nullptr};  // pel (finest level), sub-pel, mode decision
+};
+std::mutex g_debug_mu;
+DebugSettings g_debug;
+
+DebugSettings debug_settings() {
+    std::lock_guard<std::mutex> lk(g_debug_mu);
+    return g_debug;
+}
+
 int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStream_t st) {
+    const DebugSettings dbg = debug_settings();
     std::vector<PicBufs> P;
     std::vector<TaskBufs> T;
     int* ctl = nullptr;
@@ -1962,6 +1988,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
         PelJob* dj = tabs.pel + (size_t)l * 2 * A.ntasks;
         DGPU_CHECK_CUDA(cudaMemcpyAsync(dj, jobs.data(), sizeof(PelJob) * jobs.size(), cudaMemcpyHostToDevice, st));
         PelLaunch L{};
+        L.dbg = WaveDebug{dbg.spin_limit, dbg.skip_unit, l == 0 ? dbg.audit[0] : nullptr};
         L.o = g.lb[2];
         L.per_job = g.xnb[l] * g.ynb[l];
         L.total = L.per_job * (int)jobs.size();
@@ -2060,6 +2087,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
             DGPU_CHECK_CUDA(cudaMemcpyAsync(tabs.sub, jobs.data(), sizeof(SubJob) * jobs.size(),
                                             cudaMemcpyHostToDevice, st));
             SubLaunch S{};
+            S.dbg = WaveDebug{dbg.spin_limit, -1, dbg.audit[1]};
             S.o = g.lb[2];
             S.prec = A.prec;
             S.total = (int)nb * (int)jobs.size();
@@ -2096,6 +2124,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                 DGPU_CHECK_CUDA(cudaMemsetAsync(A.dc_out[t], 0, sizeof(int16_t) * 3 * nb, st));
             }
             ModeLaunch M{};
+            M.dbg = WaveDebug{dbg.spin_limit, -1, dbg.audit[2]};
             M.prec = A.prec;
             for (int i = 0; i < 3; ++i) M.lb[i] = g.lb[i];
             M.level_factor[0] = f0;
@@ -2211,6 +2240,18 @@ int check_args(int cformat, int luma_depth, const MeGeometry& g) {
 using namespace dgpu;
 
 extern "C" int dgpu_me_depth(int w, int h) { return me_depth(w, h); }
+
+extern "C" int dgpu_debug_wavefront(int skip_unit, long long spin_limit, int* audit_pel, int* audit_subpel,
+                                    int* audit_mode) {
+    if (skip_unit < -1 || spin_limit < 0) return DGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lk(g_debug_mu);
+    g_debug.skip_unit = skip_unit;
+    g_debug.spin_limit = spin_limit == 0 ? SPIN_LIMIT : std::min(spin_limit, SPIN_LIMIT);
+    g_debug.audit[0] = audit_pel;
+    g_debug.audit[1] = audit_subpel;
+    g_debug.audit[2] = audit_mode;
+    return DGPU_OK;
+}
 
 extern "C" size_t dgpu_me_batch_workspace_bytes(int cformat, int w, int h, const dgpu_block_params* bp, int npics,
                                                 int ntasks, const int* task_ref2, int stages) {

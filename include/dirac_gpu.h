@@ -256,6 +256,23 @@ int dgpu_motion_estimate(int cformat, int w, int h, const dgpu_block_params* bp,
                          uint8_t* split_out, float* sbcost_out, void* workspace, size_t ws_bytes,
                          void* stream);
 
+/* Failure-detection and ordering checks of the motion-estimation wavefronts.  No counterpart
+ * in the reference, whose search is sequential.  Process-wide settings, read by every later
+ * dgpu_motion_estimate[_batch] call (and the encoders' estimation) until changed; set them
+ * only while no estimation runs.
+ *   skip_unit >= 0: every pel-search wavefront launch leaves the completion flag of that unit
+ *   (its position in the launch's wavefront order) unset, so the waits of its dependants run
+ *   out and the call returns DGPU_ERR_CUDA, with the device context intact; -1: normal.
+ *   spin_limit: polls before a wait gives up (0: the normal limit of about 2 s; larger values
+ *   are clamped to it).
+ *   audit_pel / audit_subpel / audit_mode: NULL, or zeroed device int arrays of 1 + the
+ *   finest level's blocks (pel, sub-pel) or 1 + the superblocks (mode decision); the first
+ *   task's wavefront records there, for each unit (row-major), the position at which it was
+ *   decided (element 0 counts), so a caller can check every unit came after the neighbours
+ *   the reference's raster order makes it depend on. */
+int dgpu_debug_wavefront(int skip_unit, long long spin_limit, int* audit_pel, int* audit_subpel,
+                         int* audit_mode);
+
 /* ---------------------------------------------------------------------------------------
  * Quantiser selection and quantisation of transformed components
  * Replaces PictureCompressor::SelectQuantisers / SelectMultiQuants with QuantChooser

@@ -15,6 +15,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libdirac_ref.so")
+# the reference with its hot-path method bodies calling libdiracgpu (oracle/dropin/)
+DROPIN_SO = os.path.join(HERE, "_ref", "libdirac_dropin.so")
 
 
 def _p(a):

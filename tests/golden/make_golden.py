@@ -328,21 +328,23 @@ def decode_cases():
 def adaptive_cases():
     """The stock reference encoder (entropy-correction factors adapted from its coder's byte
     counts, as it ships) on each ENCODE_CASES sequence, with arithmetic coding and with
-    variable-length coding (-use_vlc, "<name>_vlc_*"): CRC-32 of every locally decoded plane
-    and the picture types."""
+    variable-length coding (-use_vlc, "<name>_vlc_*"): CRC-32 of every locally decoded plane,
+    the picture types, and the bitstream's length and CRC-32."""
     import zlib
 
-    from oracle import reference_encode
+    from oracle import reference_encode_stream
 
     out = {}
     for case in ENCODE_CASES:
         seq, cfg = encode_inputs(case)
         name = case[0]
         for tag, vlc in (("", 0), ("_vlc", 1)):
-            rec, ptype, _ = reference_encode(dict(cfg, use_vlc=vlc), seq, freeze=False)
+            rec, ptype, stream = reference_encode_stream(dict(cfg, use_vlc=vlc), seq, freeze=False)
             out[name + tag + "_crc"] = np.array([[zlib.crc32(np.ascontiguousarray(p).tobytes()) for p in f]
                                                  for f in rec], np.uint32)
             out[name + tag + "_ptype"] = ptype
+            out[name + tag + "_stream_bytes"] = np.array(len(stream), np.int64)
+            out[name + tag + "_stream_crc"] = np.array(zlib.crc32(bytes(stream)), np.uint32)
     return out
 
 
