@@ -53,14 +53,29 @@ constexpr long long SPIN_LIMIT = 1LL << 21;  // about 2 s of polling at the long
 // dependants' waits run out (pel wavefront only; -1: none), and an optional audit array that
 // receives, for every unit of the launch's first job, the position at which it was decided
 // ([0] is the running counter).  Normal calls carry {SPIN_LIMIT, -1, nullptr}.
+// ops, when not null, accumulates the launch's algorithmic integer operations: 3 per
+// pixel of every block difference the reference's search evaluates (subtract, absolute value,
+// add), plus the interpolation of sub-pel predictions (interp_ops) and the bi-prediction and
+// intra terms of mode decision.
 struct WaveDebug {
     long long spin_limit;
     int skip_unit;
     int* audit;
+    unsigned long long* ops;
 };
 
 __device__ __forceinline__ void audit_unit(const WaveDebug& d, int job, int unit) {
     if (d.audit && job == 0) d.audit[1 + unit] = atomicAdd(d.audit, 1);
+}
+
+// Interpolation operations per predicted sample at precision p (1 half-pel: a sample of the
+// upconverted plane; 2 quarter-pel: a rounded mean of two or four samples; 3 eighth-pel: four
+// weighted samples).
+__device__ __forceinline__ int interp_ops(int p) { return p <= 1 ? 0 : p == 2 ? 4 : 8; }
+
+// Adds n operations to the launch's count (one lane per warp).
+__device__ __forceinline__ void count_ops(unsigned long long* ops, long long n) {
+    if (ops && (threadIdx.x & 31) == 0 && n > 0) atomicAdd(ops, (unsigned long long)n);
 }
 
 struct Olb {
@@ -740,7 +755,7 @@ struct SeenLists {
 
 __device__ __noinline__ void pel_list_best(const int16_t* pic, const int16_t* ref, int pw, int ph, const Blim& b, short2 centre,
                               int r, int16_t* mem, int& best, short2& bmv, bool blk_staged = false,
-                              SeenLists seen = SeenLists{{}, 0}) {
+                              SeenLists seen = SeenLists{{}, 0}, unsigned long long* ops = nullptr) {
     const int lane = threadIdx.x & 31;
     const int n_all = (2 * r + 1) * (2 * r + 1);
     if (seen.n) {
@@ -748,6 +763,11 @@ __device__ __noinline__ void pel_list_best(const int16_t* pic, const int16_t* re
         bool fresh = false;
         for (int k = lane; k < n_all; k += 32) fresh |= !seen.has(cand_at(centre, r, k), r);
         if (!__any_sync(0xffffffffu, fresh)) return;
+    }
+    if (ops) {
+        int fresh = 0;
+        for (int k = lane; k < n_all; k += 32) fresh += !(seen.n && seen.has(cand_at(centre, r, k), r));
+        count_ops(ops, 3LL * __reduce_add_sync(0xffffffffu, fresh) * b.xl * b.yl);
     }
     const int ww = b.xl + 2 * r, wh = b.yl + 2 * r;
     int16_t* blk = mem;
@@ -822,13 +842,14 @@ __global__ void __launch_bounds__(ME_THREADS) pel_lists_kernel(const __grid_cons
     int best = INT_MAX;
     short2 bmv = make_short2(0, 0);
     if (bl.xl > 0 && bl.yl > 0) {
-        pel_list_best(J.pic, J.ref, J.pw, J.ph, bl, make_short2(0, 0), J.radius, wmem, best, bmv);
+        pel_list_best(J.pic, J.ref, J.pw, J.ph, bl, make_short2(0, 0), J.radius, wmem, best, bmv, false,
+                      SeenLists{{}, 0}, L.dbg.ops);
         if (J.guide) {
             const int gx = clampi(bx >> 1, 0, J.gxnb - 1), gy = clampi(by >> 1, 0, J.gynb - 1);
             const short2 gv = J.guide[(size_t)gy * J.gxnb + gx];
             // candidates already in the zero-centred list are not listed again
             pel_list_best(J.pic, J.ref, J.pw, J.ph, bl, make_short2((short)(gv.x * 2), (short)(gv.y * 2)), J.radius,
-                          wmem, best, bmv, true, SeenLists{{make_short2(0, 0), make_short2(0, 0)}, 1});
+                          wmem, best, bmv, true, SeenLists{{make_short2(0, 0), make_short2(0, 0)}, 1}, L.dbg.ops);
         }
     }
     if ((threadIdx.x & 31) == 0) {
@@ -881,7 +902,7 @@ __global__ void __launch_bounds__(ME_THREADS) pel_wavefront_kernel(const __grid_
                 seen.c[1] = make_short2((short)(gv.x * 2), (short)(gv.y * 2));
                 seen.n = 2;
             }
-            pel_list_best(J.pic, J.ref, J.pw, J.ph, bl, pred, J.radius, wmem, best, bmv, true, seen);
+            pel_list_best(J.pic, J.ref, J.pw, J.ph, bl, pred, J.radius, wmem, best, bmv, true, seen, L.dbg.ops);
             sad = (float)best;
         } else {
             bmv = make_short2(0, 0);
@@ -935,9 +956,11 @@ struct Cost3 {
 // updated on a strictly smaller total.
 __device__ __forceinline__ void eval_subpel_cand(const SubJob& J, const SubWin& S, bool staged, bool fused,
                                                  int total, int i, int sh, const Blim& bl, short2 c, short2 pred,
-                                                 float lambda, Cost3& best, short2& best_mv) {
+                                                 float lambda, Cost3& best, short2& best_mv,
+                                                 unsigned long long* ops) {
     const float mvcost = (float)getvarup(pred, c.x << sh, c.y << sh);
     if (bl.xl <= 0 || bl.yl <= 0) return;
+    count_ops(ops, (long long)(3 + interp_ops(i)) * bl.xl * bl.yl);
     const float start = mvcost * lambda;
     float sum;
     FloatSeq f = float_seq_start(start);
@@ -1009,6 +1032,7 @@ __global__ void __launch_bounds__(ME_THREADS, 8) subpel_wavefront_kernel(const _
             const int reach = (1 << prec) - 1;
             const bool pred_in_win = staged && abs(pred.x - (mv.x << prec)) <= reach &&
                                      abs(pred.y - (mv.y << prec)) <= reach;
+            if (bl.xl > 0 && bl.yl > 0) count_ops(L.dbg.ops, (long long)(3 + interp_ops(prec)) * bl.xl * bl.yl);
             if (bl.xl <= 0 || bl.yl <= 0)
                 pc.SAD = 0.0f;
             else if (pred_in_win)
@@ -1053,7 +1077,8 @@ __global__ void __launch_bounds__(ME_THREADS, 8) subpel_wavefront_kernel(const _
                         }
                         const int total = __shfl_sync(0xffffffffu, step_tot, (dy + 1) * 3 + dx + 1);
                         const short2 c = make_short2((short)(bmv.x + dx), (short)(bmv.y + dy));
-                        eval_subpel_cand(J, S, staged, fused, total, i, sh, bl, c, pred, lambda, best, tb);
+                        eval_subpel_cand(J, S, staged, fused, total, i, sh, bl, c, pred, lambda, best, tb,
+                                         L.dbg.ops);
                     }
                     bmv = tb;
                     if ((double)best.total > 1.1 * (double)pc.total) {
@@ -1181,6 +1206,8 @@ __device__ __noinline__ void do_me(const ModeLaunch& L, const ModeJob& J, int x,
             pred = mv_mean(__ldcg(&bv[(size_t)yb * W + xb - 1]), __ldcg(&bv[(size_t)(yb + 1) * W + xb - 1]));
         Cost3 best{me.cost[r][3 * k], me.cost[r][3 * k + 1], 100000000.0f};
         short2 bmv = me.mv[r][k];
+        if (bl.xl > 0 && bl.yl > 0)
+            count_ops(L.dbg.ops, (long long)nc * (3 + interp_ops(L.prec)) * bl.xl * bl.yl);
         for (int q = 0; q < nc; ++q) {
             if (bl.xl <= 0 || bl.yl <= 0) break;
             const float mvcost = (float)getvarup(pred, c[q].x, c[q].y);
@@ -1230,6 +1257,9 @@ __device__ __noinline__ float do_unit_decn(const ModeLaunch& L, const ModeJob& J
             best_sad = __ldcg(&me.cost[1][3 * k]);
         }
         const float bmvcost = __ldcg(&me.cost[0][3 * k + 1]) + __ldcg(&me.cost[1][3 * k + 1]);
+        // the bi-prediction difference: two predictions, 2 pic - p1 - p2, halve, absolute value, add
+        if (bl.xl > 0 && bl.yl > 0)
+            count_ops(L.dbg.ops, (long long)(5 + 2 * interp_ops(L.prec)) * bl.xl * bl.yl);
         const float bsad = bsad_in >= 0.0f ? bsad_in
                                            : bi_cost(J.pic, J.pw, J.up[0], J.up[1], 2 * J.pw, 2 * J.ph, L.prec, bl,
                                                      __ldcg(&me.mv[0][k]), __ldcg(&me.mv[1][k]));
@@ -1246,6 +1276,7 @@ __device__ __noinline__ float do_unit_decn(const ModeLaunch& L, const ModeJob& J
     bool set_dc = false;
     if (level == 2 && (double)best_sad > 4.0 * L.lb[level].xblen * L.lb[level].yblen) {
         float ic = intra_cost(J.pic, J.pw, bl, dc);
+        count_ops(L.dbg.ops, 4LL * bl.xl * bl.yl);  // the DC sum, then subtract, absolute value, add
         set_dc = true;
         ic *= f;
         const float unit = ic + mode_cost;
@@ -1896,6 +1927,7 @@ struct DebugSettings {
     int skip_unit = -1;
     long long spin_limit = SPIN_LIMIT;
     int* audit[3] = {nullptr, nullptr, nullptr};  // pel (finest level), sub-pel, mode decision
+    unsigned long long* ops = nullptr;             // [3]: pel, sub-pel, mode decision
 };
 std::mutex g_debug_mu;
 DebugSettings g_debug;
@@ -1905,8 +1937,73 @@ DebugSettings debug_settings() {
     return g_debug;
 }
 
+// Device time per kernel class of the estimation calls made while dgpu_me_profile is on, in
+// the order of DGPU_ME_NKERNELS.
+constexpr int MEK_N = DGPU_ME_NKERNELS;
+struct MeProfile {
+    bool on = false;
+    double ms[MEK_N] = {};
+    int launches[MEK_N] = {};
+};
+MeProfile g_me_prof;  // guarded by g_debug_mu
+
+// Events around each kernel class of one call; elapsed times are added to g_me_prof once
+// the call has synchronised (flush), and the events are released in any case.
+class MeTimer {
+   public:
+    MeTimer(bool on, cudaStream_t st) : on_(on), st_(st) {}
+    ~MeTimer() {
+        for (auto& r : rec_) {
+            cudaEventDestroy(r.a);
+            cudaEventDestroy(r.b);
+        }
+    }
+    void start(int k) {
+        if (!on_) return;
+        Rec r{k, nullptr, nullptr};
+        if (cudaEventCreate(&r.a) != cudaSuccess || cudaEventCreate(&r.b) != cudaSuccess) {
+            cudaGetLastError();
+            on_ = false;
+            return;
+        }
+        cudaEventRecord(r.a, st_);
+        rec_.push_back(r);
+    }
+    void stop() {
+        if (on_ && !rec_.empty()) cudaEventRecord(rec_.back().b, st_);
+    }
+    void flush() {
+        if (!on_) return;
+        std::lock_guard<std::mutex> lk(g_debug_mu);
+        for (auto& r : rec_) {
+            float ms = 0.0f;
+            if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+                g_me_prof.ms[r.k] += ms;
+                g_me_prof.launches[r.k] += 1;
+            } else {
+                cudaGetLastError();
+            }
+        }
+    }
+
+   private:
+    struct Rec {
+        int k;
+        cudaEvent_t a, b;
+    };
+    bool on_;
+    cudaStream_t st_;
+    std::vector<Rec> rec_;
+};
+
+bool me_profile_on() {
+    std::lock_guard<std::mutex> lk(g_debug_mu);
+    return g_me_prof.on;
+}
+
 int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStream_t st) {
     const DebugSettings dbg = debug_settings();
+    MeTimer tm(me_profile_on(), st);
     std::vector<PicBufs> P;
     std::vector<TaskBufs> T;
     int* ctl = nullptr;
@@ -1944,6 +2041,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
         for (int r = 0; r < nref_of(t); ++r) used[ref_of(t, r)] = 1;
     }
     // ---- pyramids of every picture involved (PixelMatcher::MakePicHierarchy) ----
+    tm.start(0);
     for (int l = 1; l <= g.depth; ++l) {
         std::vector<const int16_t*> in;
         std::vector<int16_t*> out;
@@ -1960,6 +2058,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
             if (rc) return rc;
         }
     }
+    tm.stop();
     // ---- pel search, coarsest level first: every job of a level in one wavefront ----
     for (int l = g.depth; l >= 0; --l) {
         std::vector<PelJob> jobs;
@@ -1988,7 +2087,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
         PelJob* dj = tabs.pel + (size_t)l * 2 * A.ntasks;
         DGPU_CHECK_CUDA(cudaMemcpyAsync(dj, jobs.data(), sizeof(PelJob) * jobs.size(), cudaMemcpyHostToDevice, st));
         PelLaunch L{};
-        L.dbg = WaveDebug{dbg.spin_limit, dbg.skip_unit, l == 0 ? dbg.audit[0] : nullptr};
+        L.dbg = WaveDebug{dbg.spin_limit, dbg.skip_unit, l == 0 ? dbg.audit[0] : nullptr, dbg.ops};
         L.o = g.lb[2];
         L.per_job = g.xnb[l] * g.ynb[l];
         L.total = L.per_job * (int)jobs.size();
@@ -2005,13 +2104,17 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
             if (rc) return rc;
         }
         // the candidate-list phase covers every unit: one warp per unit
+        tm.start(1);
         pel_lists_kernel<<<(L.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, smem, st>>>(L);
+        tm.stop();
         DGPU_CHECK_LAUNCH();
         L.ticket = ctl;
         L.err = ctl + 1;
         DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
+        tm.start(2);
         pel_wavefront_kernel<<<std::min((L.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, 148 * 8), ME_THREADS, smem,
                                st>>>(L);
+        tm.stop();
         DGPU_CHECK_LAUNCH();
     }
     int err_host = 0;
@@ -2049,6 +2152,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
         for (int t = 0; t < A.ntasks; ++t)
             DGPU_CHECK_CUDA(cudaMemcpyAsync(T[t].lambda[2], hlm(t), sizeof(float) * nb, cudaMemcpyHostToDevice, st));
         // ---- upconverted original references (EncPicture::UpOrigData) ----
+        tm.start(0);
         {
             std::vector<const int16_t*> in;
             std::vector<int16_t*> out;
@@ -2065,6 +2169,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                 if (rc) return rc;
             }
         }
+        tm.stop();
         // ---- sub-pel refinement: every job in one wavefront ----
         {
             std::vector<SubJob> jobs;
@@ -2087,7 +2192,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
             DGPU_CHECK_CUDA(cudaMemcpyAsync(tabs.sub, jobs.data(), sizeof(SubJob) * jobs.size(),
                                             cudaMemcpyHostToDevice, st));
             SubLaunch S{};
-            S.dbg = WaveDebug{dbg.spin_limit, -1, dbg.audit[1]};
+            S.dbg = WaveDebug{dbg.spin_limit, -1, dbg.audit[1], dbg.ops ? dbg.ops + 1 : nullptr};
             S.o = g.lb[2];
             S.prec = A.prec;
             S.total = (int)nb * (int)jobs.size();
@@ -2102,7 +2207,9 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
             S.err = ctl + 1;
             DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
             const int grid = std::min((S.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, 148 * 8);
+            tm.start(3);
             subpel_wavefront_kernel<<<grid, ME_THREADS, (size_t)S.win_elems * 2 * WARPS_PER_CTA, st>>>(S);
+            tm.stop();
             DGPU_CHECK_LAUNCH();
         }
         if (A.stages >= 3) {
@@ -2124,7 +2231,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                 DGPU_CHECK_CUDA(cudaMemsetAsync(A.dc_out[t], 0, sizeof(int16_t) * 3 * nb, st));
             }
             ModeLaunch M{};
-            M.dbg = WaveDebug{dbg.spin_limit, -1, dbg.audit[2]};
+            M.dbg = WaveDebug{dbg.spin_limit, -1, dbg.audit[2], dbg.ops ? dbg.ops + 2 : nullptr};
             M.prec = A.prec;
             for (int i = 0; i < 3; ++i) M.lb[i] = g.lb[i];
             M.level_factor[0] = f0;
@@ -2180,7 +2287,9 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                 M.jobs = tabs.mode;
                 // level 2 for every block of every job, then the superblock wavefront
                 M.total = (int)nb * nj;
+                tm.start(4);
                 mode_blocks_kernel<<<(M.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, 0, st>>>(M, (int)nb);
+                tm.stop();
                 DGPU_CHECK_LAUNCH();
                 M.total = g.xnsb * g.ynsb * nj;
                 M.wave = wave_of(g.depth + 1, g.xnsb, 1, nj);
@@ -2189,7 +2298,9 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                 M.err = ctl + 1;
                 DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
                 const int grid = std::min(M.total, 148 * 8);
+                tm.start(5);
                 mode_wavefront_kernel<<<grid, ME_THREADS, 0, st>>>(M);
+                tm.stop();
                 DGPU_CHECK_LAUNCH();
             }
             // ---- DC values of all three components ----
@@ -2216,16 +2327,20 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                 D.per_job = (int)nb;
                 D.total = (int)nb * (int)jobs.size();
                 D.jobs = tabs.dc;
+                tm.start(6);
                 block_dc_kernel<<<(D.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, ME_THREADS, 0, st>>>(D);
                 DGPU_CHECK_LAUNCH();
                 smooth_dc_kernel<<<(D.total + 255) / 256, 256, 0, st>>>(D);
+                tm.stop();
                 DGPU_CHECK_LAUNCH();
             }
         }
     }
     DGPU_CHECK_CUDA(cudaMemcpyAsync(&err_host, ctl + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
-    return err_host ? DGPU_ERR_CUDA : DGPU_OK;
+    if (err_host) return DGPU_ERR_CUDA;
+    tm.flush();
+    return DGPU_OK;
 }
 
 int check_args(int cformat, int luma_depth, const MeGeometry& g) {
@@ -2241,8 +2356,20 @@ using namespace dgpu;
 
 extern "C" int dgpu_me_depth(int w, int h) { return me_depth(w, h); }
 
+extern "C" int dgpu_me_profile(int enable, double* kernel_ms, int* launches) {
+    std::lock_guard<std::mutex> lk(g_debug_mu);
+    for (int k = 0; k < MEK_N; ++k) {
+        if (kernel_ms) kernel_ms[k] = g_me_prof.ms[k];
+        if (launches) launches[k] = g_me_prof.launches[k];
+        g_me_prof.ms[k] = 0.0;
+        g_me_prof.launches[k] = 0;
+    }
+    g_me_prof.on = enable != 0;
+    return DGPU_OK;
+}
+
 extern "C" int dgpu_debug_wavefront(int skip_unit, long long spin_limit, int* audit_pel, int* audit_subpel,
-                                    int* audit_mode) {
+                                    int* audit_mode, unsigned long long* ops) {
     if (skip_unit < -1 || spin_limit < 0) return DGPU_ERR_ARG;
     std::lock_guard<std::mutex> lk(g_debug_mu);
     g_debug.skip_unit = skip_unit;
@@ -2250,6 +2377,7 @@ extern "C" int dgpu_debug_wavefront(int skip_unit, long long spin_limit, int* au
     g_debug.audit[0] = audit_pel;
     g_debug.audit[1] = audit_subpel;
     g_debug.audit[2] = audit_mode;
+    g_debug.ops = ops;
     return DGPU_OK;
 }
 

@@ -65,6 +65,13 @@ const char* dgpu_last_error(void);
 /* Running total of kernel launches issued by this library in this process. */
 unsigned long long dgpu_launch_count(void);
 
+/* Measures, on the current device, the rate of the integer block-difference operation
+ * acc += |a - b| (counted as 3 operations: subtract, absolute value, add) on register-resident
+ * data with every SM busy: the integer roofline the motion-estimation kernels' algorithmic
+ * operation counts are compared with.  No counterpart in the reference.  Synchronous; about
+ * 10 ms of GPU time. */
+int dgpu_measure_int_rate(double* ops_per_second);
+
 /* ---------------------------------------------------------------------------------------
  * Wavelet transform
  * Replaces WaveletTransform::Transform(Direction, PicArray&, CoeffArray&)
@@ -256,6 +263,16 @@ int dgpu_motion_estimate(int cformat, int w, int h, const dgpu_block_params* bp,
                          uint8_t* split_out, float* sbcost_out, void* workspace, size_t ws_bytes,
                          void* stream);
 
+/* Device time of the motion-estimation kernels by class, for measurement: while enabled,
+ * every estimation call times each class with CUDA events on its stream (one event pair per
+ * launch, so profiled calls are slower).  kernel_ms / launches (NULL or DGPU_ME_NKERNELS
+ * entries) receive the totals accumulated since the previous call, which are then cleared.
+ * Classes: 0 resampling (pyramid downconversion and upconversion of the references),
+ * 1 pel candidate lists (pel_lists_kernel), 2 pel wavefront, 3 sub-pel wavefront, 4 mode
+ * decision's block pass, 5 mode-decision wavefront, 6 DC values. */
+#define DGPU_ME_NKERNELS 7
+int dgpu_me_profile(int enable, double* kernel_ms, int* launches);
+
 /* Failure-detection and ordering checks of the motion-estimation wavefronts.  No counterpart
  * in the reference, whose search is sequential.  Process-wide settings, read by every later
  * dgpu_motion_estimate[_batch] call (and the encoders' estimation) until changed; set them
@@ -269,9 +286,15 @@ int dgpu_motion_estimate(int cformat, int w, int h, const dgpu_block_params* bp,
  *   finest level's blocks (pel, sub-pel) or 1 + the superblocks (mode decision); the first
  *   task's wavefront records there, for each unit (row-major), the position at which it was
  *   decided (element 0 counts), so a caller can check every unit came after the neighbours
- *   the reference's raster order makes it depend on. */
+ *   the reference's raster order makes it depend on.
+ *   ops: NULL, or a zeroed device array of three counters that accumulate the algorithmic
+ *   integer operations of the pel search, the sub-pel refinement and mode decision: for every
+ *   block difference the reference's search evaluates, 3 per pixel (subtract, absolute value,
+ *   add) plus the sub-pel interpolation (0 half-pel, 4 quarter-pel, 8 eighth-pel per pixel);
+ *   bi-prediction differences 5 + 2 x interpolation, intra costs 4 per pixel.  Counting adds an
+ *   atomic per evaluation: use it in a separate pass, not a timed one. */
 int dgpu_debug_wavefront(int skip_unit, long long spin_limit, int* audit_pel, int* audit_subpel,
-                         int* audit_mode);
+                         int* audit_mode, unsigned long long* ops);
 
 /* ---------------------------------------------------------------------------------------
  * Quantiser selection and quantisation of transformed components

@@ -17,10 +17,11 @@ sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
 from make_golden import ENCODE_CASES, encode_inputs  # noqa: E402
 
 
-def adaptive_encode(seq, cfg):
+def adaptive_encode(seq, cfg, vlc=False):
     """Codes seq with the device encoder and the host band coder adapting the entropy-correction
-    state picture by picture (the stock reference encoder's loop); returns the locally decoded
-    output planes and intra flags by picture number."""
+    state picture by picture (the stock reference encoder's loop; with vlc the variable-length
+    coder, whose whole bytes the reference's update takes); returns the locally decoded output
+    planes and intra flags by picture number."""
     from dirac_b200 import encoder as E
     from dirac_b200 import quant
     from dirac_b200.encoder import SequenceEncoder
@@ -44,9 +45,10 @@ def adaptive_encode(seq, cfg):
             bands = enc.read(pn, E.BANDS, c).reshape(-1, 3)
             q = enc.read(pn, E.QINDEX, c)
             cw = ((cfg["width"] >> (xs if c else 0)) + (1 << depth) - 1) >> depth << depth
-            _, per = code_bands(info["intra"], depth, [q.reshape(-1, cw)], [bands], [ncb],
-                                [enc.read(pn, E.CBSKIP, c)])
-            ec.update(info["intra"], info["is_b"], c, bands[:, 1], bands[:, 2], per[0])
+            coded = code_bands(info["intra"], depth, [q.reshape(-1, cw)], [bands], [ncb],
+                               [enc.read(pn, E.CBSKIP, c)], vlc=vlc)
+            counts = coded[2][0] // 8 if vlc else coded[1][0]
+            ec.update(info["intra"], info["is_b"], c, bands[:, 1], bands[:, 2], counts)
         outputs[pn] = [enc.read(pn, E.OUTPUT, c) for c in range(3)]
         ptype[pn] = info["intra"]
     enc.close()
@@ -126,6 +128,21 @@ def test_pipelined_host_coding_matches_stock_reference(gpu, golden, case):
     crc = np.array([[zlib.crc32(np.ascontiguousarray(outputs[i][c]).tobytes()) for c in range(3)]
                     for i in range(len(seq))], np.uint32)
     np.testing.assert_array_equal(crc, g[case[0] + "_crc"])
+
+
+@pytest.mark.parametrize("case", ENCODE_CASES, ids=[c[0] for c in ENCODE_CASES])
+def test_device_encoder_with_vlc_host_coder_matches_stock_reference(gpu, golden, case):
+    """The stock -use_vlc reference encoder: coefficients coded by the variable-length host coder
+    (dgpu_code_bands_vlc_host), the factors adapted from its whole-byte counts."""
+    from test_encoder_gpu import encoder_params
+
+    seq, rcfg = encode_inputs(case)
+    outputs, ptype = adaptive_encode(seq, encoder_params(rcfg), vlc=True)
+    g = golden("adaptive.npz")
+    crc = np.array([[zlib.crc32(np.ascontiguousarray(outputs[i][c]).tobytes()) for c in range(3)]
+                    for i in range(len(seq))], np.uint32)
+    np.testing.assert_array_equal(crc, g[case[0] + "_vlc_crc"])
+    np.testing.assert_array_equal([ptype[i] for i in range(len(seq))], g[case[0] + "_vlc_ptype"])
 
 
 def test_hd1080_with_host_coder_matches_stock_reference(gpu, golden):

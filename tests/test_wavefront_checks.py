@@ -88,12 +88,12 @@ def test_wait_that_runs_out_returns_an_error_and_the_device_recovers(gpu, oracle
     lib = gpu.load()
     f = _frames()
     try:
-        assert lib.dgpu_debug_wavefront(0, 4096, None, None, None) == 0
+        assert lib.dgpu_debug_wavefront(0, 4096, None, None, None, None) == 0
         with pytest.raises(DgpuError) as e:
             _estimate(gpu, f, stages)
         assert e.value.args[0] == -3  # DGPU_ERR_CUDA
     finally:
-        assert lib.dgpu_debug_wavefront(-1, 0, None, None, None) == 0
+        assert lib.dgpu_debug_wavefront(-1, 0, None, None, None, None) == 0
     torch.cuda.synchronize()  # the context is usable
     got = _estimate(gpu, f, 3)
     want = oracle.motion_estimate(2, f[1], f[0], f[2], _bp(), 10.0, 3)
@@ -112,10 +112,10 @@ def test_wavefront_decision_order_respects_raster_dependencies(gpu, oracle):
     audits = [torch.zeros(1 + n, dtype=torch.int32, device="cuda")
               for n in (xnb * ynb, xnb * ynb, bp.xnum_sb * bp.ynum_sb)]
     try:
-        assert lib.dgpu_debug_wavefront(-1, 0, *[a.data_ptr() for a in audits]) == 0
+        assert lib.dgpu_debug_wavefront(-1, 0, *[a.data_ptr() for a in audits], None) == 0
         got = _estimate(gpu, f, 3)
     finally:
-        assert lib.dgpu_debug_wavefront(-1, 0, None, None, None) == 0
+        assert lib.dgpu_debug_wavefront(-1, 0, None, None, None, None) == 0
     want = oracle.motion_estimate(2, f[1], f[0], f[2], bp, 10.0, 3)
     for k, v in want.items():
         np.testing.assert_array_equal(got[k], v, err_msg=k)
