@@ -7,8 +7,11 @@ up to 24 px/frame): GOP of the HD1080P50 preset (L1 separation 3, 7 L1 pictures 
 quality factor 7, DAUB9_7 intra / DD9_7 inter transforms of depth 4, OBMC blocks 16x16 at
 separation 12, quarter-pel hierarchical motion estimation with mode decision, motion
 compensation, quantiser choice and quantisation, inverse transform and reconstruction, all
-bit-exact with the reference.  Arithmetic coding is not part of the path (host code in the
-reference); the encoder keeps the initial entropy-correction factors.
+bit-exact with the reference.  `value` keeps the initial entropy-correction factors (the device
+work of the path alone); `e2e` codes every picture's subbands on the host and adapts the factors
+from the coded bytes, so its quantiser choices, and its locally decoded pictures, are the stock
+reference encoder's (checked against the reference's own run of the same sequence in
+`parity_vs_reference`).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gpu|reference]
 
@@ -20,7 +23,8 @@ estimation overlaps another's coding) with the input frames resident in HBM;
 without groups (each sequence estimating alone), `plain` for one sequence at a time.
 `e2e`: the batched form through
 the encoder's C ABI from pinned host frames, reading back per picture what the host coder
-needs (quantised indices, band choices, code-block skips, motion data).  Every step works on
+needs (quantised indices, band choices, code-block skips, motion data) and arithmetic-coding
+the subbands on the host threads (`e2e_hot_path`: the same without the host coder).  Every step works on
 gigabytes of distinct device buffers (far above the 126 MB L2), so no L2 flush is needed.
 `decoding`: the plain form's coded sequence decoded by the device decoder (dequantisation,
 inverse transform, motion compensation, clip, output samples), its output checked against the
@@ -45,7 +49,20 @@ PARAMS = dict(cformat=2, width=1920, height=1080, luma_depth=8, chroma_depth=8, 
               cpd=32.0, xblen=16, yblen=16, xbsep=12, ybsep=12, mv_precision=2, intra_filter=6, inter_filter=0,
               wlt_depth=4)
 VIDEO_FORMAT_HD_1080P50 = 14
-CPU_SAMPLE_FRAMES = 10
+REF_WARMUP_FRAMES = 2  # a reference warm-up encode (page-in, allocator): the sequence's first frames
+# the encoder's streaming stages and the kernels each one runs
+STREAMING_KERNELS = {"dwt_forward": "dwt_forward_fast_kernel / dwt_forward_level_kernel",
+                     "dwt_inverse": "dwt_inverse_fast_kernel / dwt_inverse_level_kernel",
+                     "mc_subtract": "obmc_kernel (SUBTRACT)", "mc_add_clip": "obmc_kernel (ADD, clip fused)",
+                     "upconvert": "upconvert_kernel",
+                     "quantisation": "band_max, stats, seq_resolve, gather_stats, quantise, dc_intra kernels "
+                                     "and the host Lagrangian"}
+# motion-estimation kernel classes of dgpu_me_profile and counters of dgpu_debug_wavefront
+ME_CLASSES = {"pel_search": (1, 2), "subpel_refinement": (3,), "mode_decision": (4, 5)}
+ME_OP_INDEX = {"pel_search": 0, "subpel_refinement": 1, "mode_decision": 2}
+# DRAM bytes per algorithmic operation of each motion-estimation kernel, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum over the launch's counted operations)
+ME_TRAFFIC_PER_OP = {}
 
 
 def parse_args():
@@ -100,17 +117,19 @@ def _init_worker(frames):
     _WORKER_FRAMES = frames
 
 
-def _ref_encode(_, keep_stream=None):
-    """One reference encode of the worker's frames (stock encoder: adaptive entropy factors);
-    with keep_stream (a list), its bitstream is appended there."""
+def _ref_encode(nframes, keep=None):
+    """One reference encode of the worker's first nframes frames (stock encoder: adaptive
+    entropy factors); with keep (a list), (locally decoded frames, bitstream) is appended."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import reference_encode, reference_encode_stream
 
+    frames = _WORKER_FRAMES[:nframes]
     t0 = time.perf_counter()
-    if keep_stream is None:
-        reference_encode(ref_config(), _WORKER_FRAMES, freeze=False)
+    if keep is None:
+        reference_encode(ref_config(), frames, freeze=False)
     else:
-        keep_stream.append(reference_encode_stream(ref_config(), _WORKER_FRAMES, freeze=False)[2])
+        rec, _, stream = reference_encode_stream(ref_config(), frames, freeze=False)
+        keep.append((rec, stream))
     return time.perf_counter() - t0
 
 
@@ -121,16 +140,17 @@ def reference_available():
     return Reference.available()
 
 
-def cpu_baseline_single(frames, streams=None):
-    """The reference encoder in this process (one core) on the first frames of the sequence;
-    with streams (a list), the timed encode's bitstream is appended there."""
+def cpu_baseline_single(frames, keep=None):
+    """The reference encoder in this process (one core) on the whole sequence; with keep (a
+    list), the encode's (locally decoded frames, bitstream) is appended there."""
     global _WORKER_FRAMES
     _WORKER_FRAMES = frames
-    _ref_encode(None)  # warm-up (page-in, allocator)
-    dt = _ref_encode(None, streams)
+    _ref_encode(REF_WARMUP_FRAMES)  # warm-up (page-in, allocator)
+    dt = _ref_encode(len(frames), keep)
     return {"value": len(frames) / dt, "unit": "frames/s", "cores": 1, "kind": "reference",
-            "sample": f"reference encoder (dirac_encoder_* API, plain-C build) on the first {len(frames)} frames "
-                      f"of the step's sequence: {dt:.2f} s on 1 core"}
+            "sample": f"reference encoder (dirac_encoder_* API, plain-C build, stock adaptive entropy factors, its "
+                      f"arithmetic coding and bitstream output included) on the step's whole {len(frames)}-frame "
+                      f"sequence: {dt:.2f} s on 1 core"}
 
 
 def cpu_decode_baseline(stream, nframes):
@@ -161,26 +181,27 @@ def run_reference(args):
         return
     import multiprocessing as mp
 
-    frames = make_frames(CPU_SAMPLE_FRAMES, seed=1000)
+    frames = make_frames(args.frames, seed=1000)
     procs = min(os.cpu_count() or 1, 128)  # about 0.5 GB of host memory per encode
     ctx = mp.get_context("spawn")
     walls = []
     with ctx.Pool(procs, initializer=_init_worker, initargs=(frames,)) as pool:
         for k in range(args.warmup + args.steps):
+            n = REF_WARMUP_FRAMES if k < args.warmup else args.frames
             t0 = time.perf_counter()
-            pool.map(_ref_encode, range(procs), chunksize=1)
+            pool.map(_ref_encode, [n] * procs, chunksize=1)
             dt = time.perf_counter() - t0
             if k >= args.warmup:
                 walls.append(dt)
     wall = statistics.median(walls)
-    value = procs * CPU_SAMPLE_FRAMES / wall
-    sample = (f"{procs} concurrent reference encodes (one per host core) of the first {CPU_SAMPLE_FRAMES} frames "
-              f"of the sequence per step; median step {wall:.2f} s")
+    value = procs * args.frames / wall
+    sample = (f"{procs} concurrent reference encodes (one per host core) of the whole {args.frames}-frame sequence "
+              f"per step (warm-up steps: its first {REF_WARMUP_FRAMES} frames); median step {wall:.2f} s")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": {"workload": workload_name(CPU_SAMPLE_FRAMES), "host_processes": procs,
-                       "note": "the reference encoder includes its arithmetic coder and bitstream output"},
+            "config": {"workload": workload_name(args.frames), "host_processes": procs,
+                       "note": "the stock reference encoder, its arithmetic coding and bitstream output included"},
             "cpu_baseline": {"value": value, "unit": "frames/s", "cores": procs, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -520,13 +541,15 @@ def main():
     # CPU baseline first (rank 0, N=1), before any GPU call
     cpu_baseline = None
     cpu_decode = None
+    ref_recon = None  # the reference encoder's locally decoded pictures of this sequence
     if world == 1 and rank == 0:
         if reference_available():
-            streams = []
-            cpu_baseline = cpu_baseline_single(frames[:CPU_SAMPLE_FRAMES], streams)
+            keep = []
+            cpu_baseline = cpu_baseline_single(frames, keep)
+            ref_recon = keep[0][0]
             if args.decode:
                 try:
-                    cpu_decode = cpu_decode_baseline(streams[0], CPU_SAMPLE_FRAMES)
+                    cpu_decode = cpu_decode_baseline(keep[0][1], args.frames)
                 except Exception as e:  # the decoding leg falls back to the oracle's decoder
                     cpu_decode = {"error": repr(e)}
         else:
@@ -543,8 +566,14 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
 
+    import ctypes
+
+    import numpy as np
+
     import dirac_b200
     from dirac_b200 import encoder as E
+    from dirac_b200 import quant
+    from dirac_b200.entropy import EntropyCorrector, code_bands
     from dirac_b200.roofline import stage_bytes
 
     lib = dirac_b200.load()
@@ -554,6 +583,11 @@ def main():
     torch.cuda.synchronize()
     items = [(E.QINDEX, c) for c in range(3)] + [(E.BANDS, c) for c in range(3)] + \
             [(E.CBSKIP, c) for c in range(3)] + [(E.MV, 0), (E.MODE, 0), (E.DC, 0), (E.SPLIT, 0)]
+    depth = PARAMS["wlt_depth"]
+    ncb = quant.code_blocks(depth, PARAMS["width"], PARAMS["height"])
+    mul = 1 << depth
+    qshapes = [(((PARAMS["height"] >> (c > 0)) + mul - 1) // mul * mul,
+                ((PARAMS["width"] >> (c > 0)) + mul - 1) // mul * mul) for c in range(3)]
 
     class Lane:
         """One sequence encoder on its own CUDA stream (the batched form runs several, each
@@ -564,9 +598,14 @@ def main():
             self.enc = E.SequenceEncoder(PARAMS, max_pictures=args.frames, stream=self.stream)
             self.bufs = {}
             self.d2h = 0
+            self.coded_bytes = 0
+            self.ec = None
 
         def read(self, info):
+            """The coded picture's results the host coder needs, into page-locked buffers
+            (reused picture after picture); returns numpy views by (item, component)."""
             pn = info["pnum"]
+            got = {}
             for what, c in items:
                 n = lib.dgpu_encoder_item_bytes(self.enc.handle, pn, what, c)
                 if n == 0:
@@ -578,6 +617,42 @@ def main():
                 if rc:
                     raise RuntimeError(f"dgpu_encoder_read failed: {rc}")
                 self.d2h += n
+                got[(what, c)] = b.numpy()
+            return got
+
+        def code_host(self, info, got):
+            """Arithmetic-codes the picture's subbands on the library's host threads (the
+            reference's band coders' bytes) and adapts the lane's entropy-correction state from
+            the byte counts, as the stock reference encoder does after each component."""
+            q = [got[(E.QINDEX, c)].view(np.int32).reshape(qshapes[c]) for c in range(3)]
+            bands = [got[(E.BANDS, c)].view(np.int32).reshape(-1, 3) for c in range(3)]
+            cbs = [got[(E.CBSKIP, c)] for c in range(3)]
+            data, per = code_bands([info["intra"]] * 3, [depth] * 3, q, bands, [ncb] * 3, cbs)
+            self.coded_bytes += int(data.size)
+            for c in range(3):
+                self.ec.update(info["intra"], info["is_b"], c, bands[c][:, 1], bands[c][:, 2], per[c])
+
+        def step_adaptive(self, src, loaded=False, outputs=None):
+            """The stock encoder's choices: each picture's quantisers chosen with the entropy-
+            correction state adapted from the previous pictures' coded bytes.  Picture n's bands
+            are coded on the host while the device prepares picture n + 1 (motion
+            compensation, forward transform)."""
+            enc = self.enc
+            if not loaded:
+                self.load(src)
+            self.ec = EntropyCorrector(depth)
+            pending = None
+            while True:
+                nxt = enc.prepare_next()
+                if pending is not None:
+                    self.code_host(*pending)
+                    pending = None
+                if nxt is None:
+                    return
+                info = enc.finish_next(ecf_state=self.ec.state)
+                pending = (info, self.read(info))
+                if outputs is not None:
+                    outputs[info["pnum"]] = [enc.read(info["pnum"], E.OUTPUT, c) for c in range(3)]
 
         def load(self, src):
             enc = self.enc
@@ -620,7 +695,7 @@ def main():
             pools[key] = ThreadPoolExecutor(n)
         return pools[key]
 
-    def timed(lanes, src, steps, with_read=False, groups=None):
+    def timed(lanes, src, steps, with_read=False, groups=None, adaptive=False):
         """Device time (ms) of `steps` sequence encodes on every lane, the lanes running
         concurrently: a start event on the main stream that every lane stream waits on, and an
         end event after the main stream has waited on every lane's last work.  With groups
@@ -636,10 +711,17 @@ def main():
         for ln in lanes:
             ln.stream.wait_event(e0)
             ln.d2h = 0
+            ln.coded_bytes = 0
+
+        def code(ln, loaded):
+            if adaptive:
+                ln.step_adaptive(src, loaded=loaded)
+            else:
+                ln.step(src, with_read=with_read, loaded=loaded)
 
         def run(ln):
             for _ in range(steps):
-                ln.step(src, with_read=with_read)
+                code(ln, False)
 
         def run_group(gi):
             g, gl = groups[gi]
@@ -647,7 +729,7 @@ def main():
             for _ in range(steps):
                 list(ex.map(lambda ln: ln.load(src), gl))
                 g.estimate()
-                list(ex.map(lambda ln: ln.step(src, with_read=with_read, loaded=True), gl))
+                list(ex.map(lambda ln: code(ln, True), gl))
 
         if groups is not None:
             list(pool(("groups", len(groups)), len(groups)).map(run_group, range(len(groups))))
@@ -675,25 +757,54 @@ def main():
     # ---- warm-up: every lane, both input forms ------------------------------------------------
     for _ in range(args.warmup):
         timed(lanes, dev_frames, 1, groups=groups)
-    timed(lanes, pinned_np, 1, with_read=True, groups=groups)
+    timed(lanes, pinned_np, 1, groups=groups, adaptive=True)
+
+    # ---- the integer roofline and the motion-estimation kernels' algorithmic operations -------
+    rate = ctypes.c_double(0.0)
+    if lib.dgpu_measure_int_rate(ctypes.byref(rate)):
+        raise RuntimeError("dgpu_measure_int_rate failed")
+    int_peak = rate.value / 1e9  # Gop/s
+    ops_dev = torch.zeros(3, dtype=torch.int64, device="cuda")
+    lib.dgpu_debug_wavefront(-1, 0, None, None, None, ops_dev.data_ptr())
+    lib.dgpu_me_profile(1, None, None)
+    timed(lanes, dev_frames, 1, groups=groups)  # one batched step, counted (untimed)
+    count_launches = (ctypes.c_int * 7)()
+    lib.dgpu_me_profile(0, None, count_launches)
+    lib.dgpu_debug_wavefront(-1, 0, None, None, None, None)
+    me_ops_per_step = [int(x) for x in ops_dev.cpu().tolist()]
 
     # ---- timed region (batched form): inputs resident in HBM ---------------------------------
     clocks = ClockSampler(local_rank)
     clocks.start()
     time.sleep(0.3)
     launches0 = lib.dgpu_launch_count()
+    lib.dgpu_me_profile(1, None, None)  # CUDA events around each motion-estimation kernel
     ms = timed(lanes, dev_frames, args.steps, groups=groups)
+    me_ms = (ctypes.c_double * 7)()
+    me_launches = (ctypes.c_int * 7)()
+    lib.dgpu_me_profile(0, me_ms, me_launches)
     launches = lib.dgpu_launch_count() - launches0
     clk = clocks.stop()
     frames_per_step = args.frames * len(lanes)
     ms_per_step = ms / args.steps
     value = whole_job_rate(world, frames_per_step, args.steps, ms)
 
-    # ---- end to end (batched form) through the C ABI with host buffers -------------------------
-    ems = timed(lanes, pinned_np, args.steps, with_read=True, groups=groups)
+    # ---- end to end (batched form) through the C ABI with host buffers, stock choices ---------
+    # pinned host frames in; per picture the quantised indices, band and code-block choices
+    # and motion data out; every picture's subbands arithmetic-coded on the host and the
+    # entropy-correction state adapted from the byte counts, so the quantiser choices are the
+    # stock reference encoder's
+    ems = timed(lanes, pinned_np, args.steps, groups=groups, adaptive=True)
     h2d = sum(p.nbytes for fr in pinned_np for p in fr) * len(lanes)
     e2e = {"value": whole_job_rate(world, frames_per_step, args.steps, ems), "unit": "frames/s",
-           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": sum(ln.d2h for ln in lanes) // args.steps}
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": sum(ln.d2h for ln in lanes) // args.steps,
+           "coded_band_bytes_per_step": sum(ln.coded_bytes for ln in lanes) // args.steps,
+           "form": "stock choices: adaptive entropy-correction factors, subbands arithmetic-coded on the host "
+                   "(picture n coded while the device prepares n + 1)"}
+    # the same without host coding (initial factors kept): the hot path alone through the ABI
+    hms = timed(lanes, pinned_np, args.steps, with_read=True, groups=groups)
+    e2e_hot = {"value": whole_job_rate(world, frames_per_step, args.steps, hms), "unit": "frames/s",
+               "form": "initial entropy-correction factors, no host coding"}
 
     # ---- batched form without the group: concurrent sequences, each estimating alone -----------
     sms = timed(lanes, dev_frames, args.steps)
@@ -709,9 +820,23 @@ def main():
 
     # ---- plain form: one sequence at a time ----------------------------------------------------
     pms = timed([plain], dev_frames, args.steps)
-    pems = timed([plain], pinned_np, args.steps, with_read=True)
+    pems = timed([plain], pinned_np, args.steps, adaptive=True)
     plain_line = {"value": world * args.frames * args.steps / (pms / 1000.0), "ms_per_step": pms / args.steps,
-                  "e2e": world * args.frames * args.steps / (pems / 1000.0), "unit": "frames/s"}
+                  "e2e": world * args.frames * args.steps / (pems / 1000.0), "unit": "frames/s",
+                  "batched_over_plain": value / (world * args.frames * args.steps / (pms / 1000.0))}
+
+    # ---- self-check: the timed sequence coded with the stock choices equals the reference's ----
+    parity = None
+    if ref_recon is not None:
+        outs = {}
+        plain.step_adaptive(pinned_np, outputs=outs)
+        same = len(outs) == args.frames and all(
+            np.array_equal(outs[i][c], np.ascontiguousarray(ref_recon[i][c]).ravel())
+            for i in range(args.frames) for c in range(3))
+        parity = {"frames": args.frames, "locally_decoded_equal_reference": bool(same),
+                  "form": "the step's whole sequence coded as the e2e form codes it (stock adaptive factors, host "
+                          "band coding), every locally decoded plane compared with the reference encoder's own "
+                          "(its cpu_baseline run)"}
 
     # ---- per-picture latency of the plain form (device timeline, coding order) ---------------
     lat = []
@@ -724,7 +849,7 @@ def main():
     latency = {"p50": statistics.median(lat), "p99": lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))],
                "max": lat[-1], "pictures": len(lat), "form": "plain"}
 
-    # ---- stage breakdown (plain form) and the roofline of the dominant stage ------------------
+    # ---- stage breakdown (plain form): the streaming kernels against the HBM roofline ---------
     enc = plain.enc
     enc.profile(True)
     reps = 2
@@ -740,19 +865,46 @@ def main():
     except OSError:
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
-    dominant = max(stage_ms, key=stage_ms.get)
-    per_stage = {k: {"ms_per_step": round(stage_ms[k], 3),
-                     "gbs": round(alg[k] / (stage_ms[k] / 1000.0) / 1e9, 1) if stage_ms[k] > 0 else None,
-                     "frac": round(alg[k] / (stage_ms[k] / 1000.0) / 1e9 / peak, 4) if stage_ms[k] > 0 else None}
-                 for k in stage_ms}
-    achieved = alg[dominant] / (stage_ms[dominant] / 1000.0) / 1e9
-    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None,
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
-                else "fallback 6650 GB/s (of fallback)",
-                "algorithmic_bytes_per_step": alg, "stages": per_stage,
-                "note": "plain form, one sequence; stage times from CUDA events on the encoder stream in a "
-                        "separate profiled pass"}
+    peak_source = ("MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
+                   else "fallback 6650 GB/s (of fallback)")
+    streaming = {}
+    for k, kern in STREAMING_KERNELS.items():
+        if stage_ms.get(k, 0.0) <= 0:
+            continue
+        gbs = alg[k] / (stage_ms[k] / 1000.0) / 1e9
+        streaming[k] = {"kernels": kern, "ms_per_sequence": round(stage_ms[k], 3), "algorithmic_bytes": alg[k],
+                        "gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
+
+    # ---- the motion-estimation kernels against the integer roofline (batched timed region) ----
+    def me_kernel(name, key):
+        t = sum(me_ms[c] for c in ME_CLASSES[key])
+        n = sum(me_launches[c] for c in ME_CLASSES[key])
+        ops = me_ops_per_step[ME_OP_INDEX[key]] * args.steps
+        achieved = ops / (t / 1000.0) / 1e9 if t > 0 else 0.0
+        return {"kernels": name, "ms_total": round(t, 3), "launches": n, "algorithmic_ops": ops,
+                "achieved": round(achieved, 1), "frac": round(achieved / int_peak, 4)}
+
+    me_kernels = {"pel_search": me_kernel("pel_lists_kernel + pel_wavefront_kernel", "pel_search"),
+                  "subpel_refinement": me_kernel("subpel_wavefront_kernel", "subpel_refinement"),
+                  "mode_decision": me_kernel("mode_blocks_kernel + mode_wavefront_kernel", "mode_decision")}
+    dom = max(me_kernels, key=lambda k: me_kernels[k]["ms_total"])
+    d = me_kernels[dom]
+    per_launch_ops = me_ops_per_step[ME_OP_INDEX[dom]] / max(1, sum(count_launches[c] for c in ME_CLASSES[dom]))
+    traffic = ME_TRAFFIC_PER_OP.get(dom)
+    roofline = {"bound": "int", "kernel": d["kernels"], "achieved": d["achieved"], "peak": round(int_peak, 1),
+                "unit": "Gop/s", "frac": d["frac"],
+                "traffic": round(traffic * per_launch_ops) if traffic else None,
+                "peak_source": "dgpu_measure_int_rate: acc += |a - b| on every SM, 3 operations per term "
+                               "(measured in this run)",
+                "algorithmic_ops": "3 per pixel of every block difference the reference's search evaluates, plus "
+                                   "sub-pel interpolation (4 per pixel at quarter-pel), bi-prediction and intra terms "
+                                   "(counted on the device in an untimed step)",
+                "ops_per_launch": round(per_launch_ops),
+                "me_kernels": me_kernels, "streaming_kernels": streaming,
+                "streaming_peak": {"value": peak, "unit": "GB/s", "source": peak_source},
+                "note": "motion-estimation kernel times: CUDA events around each launch on the encoder groups' "
+                        "streams inside the timed region (concurrent groups' times add up); streaming kernels: "
+                        "plain form, encoder stage events in a separate pass"}
     # ---- decoding: the plain form's coded sequence through the device decoder ----------------
     decoding = None
     if args.decode and world == 1:
@@ -797,9 +949,10 @@ def main():
                                    "running concurrently; each group's motion estimation in one batched launch, "
                                    "each sequence's coding on its own stream and host thread",
                            "l2": "inputs and working set larger than L2 (no flush needed)"},
-                "plain": plain_line, "batched_one_group": one_group, "batched_streams_only": streams_only, "roofline": roofline, "cpu_baseline": cpu_baseline, "e2e": e2e,
-                "latency_ms": latency, "heterogeneous_batch": hetero, "serving": serving, "decoding": decoding,
-                "gpu_launches": launches, "clocks": clk}
+                "e2e": e2e, "cpu_baseline": cpu_baseline, "parity_vs_reference": parity, "plain": plain_line,
+                "gpu_launches": launches, "clocks": clk, "e2e_hot_path": e2e_hot, "roofline": roofline,
+                "batched_one_group": one_group, "batched_streams_only": streams_only, "latency_ms": latency,
+                "heterogeneous_batch": hetero, "serving": serving, "decoding": decoding}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
