@@ -81,6 +81,8 @@ def parse_args():
                          "(0: skip)")
     ap.add_argument("--decode", type=int, default=1,
                     help="1: report the device decoder on the plain form's coded sequence under 'decoding'")
+    ap.add_argument("--cpu-baseline", type=int, default=1,
+                    help="1: time the reference encoder on this host first (cpu_baseline, parity_vs_reference)")
     ap.add_argument("--impl", choices=["gpu", "reference"], default="gpu")
     return ap.parse_args()
 
@@ -542,7 +544,7 @@ def main():
     cpu_baseline = None
     cpu_decode = None
     ref_recon = None  # the reference encoder's locally decoded pictures of this sequence
-    if world == 1 and rank == 0:
+    if world == 1 and rank == 0 and args.cpu_baseline:
         if reference_available():
             keep = []
             cpu_baseline = cpu_baseline_single(frames, keep)
