@@ -91,7 +91,7 @@ def test_wait_that_runs_out_returns_an_error_and_the_device_recovers(gpu, oracle
         assert lib.dgpu_debug_wavefront(0, 4096, None, None, None, None) == 0
         with pytest.raises(DgpuError) as e:
             _estimate(gpu, f, stages)
-        assert e.value.args[0] == -3  # DGPU_ERR_CUDA
+        assert e.value.code == -3  # DGPU_ERR_CUDA
     finally:
         assert lib.dgpu_debug_wavefront(-1, 0, None, None, None, None) == 0
     torch.cuda.synchronize()  # the context is usable
