@@ -1110,28 +1110,84 @@ extern "C" int dgpu_encoder_group_destroy(void* group) {
     return DGPU_OK;
 }
 
-extern "C" int dgpu_encoder_group_estimate(void* group, int* ntasks) {
-    Group* G = static_cast<Group*>(group);
-    if (ntasks) *ntasks = 0;
-    if (!G) return DGPU_ERR_ARG;
+namespace dgpu {
+namespace {
+
+// Estimates, for every listed encoder, each loaded and uncoded inter picture whose references
+// are known, in one batched launch on st after the encoders' pending work; their streams then
+// follow the estimation.  ev orders the streams.
+int estimate_members(const std::vector<Encoder*>& enc, cudaStream_t st, cudaEvent_t ev, void* ws, size_t ws_bytes,
+                     int* d_counts, int* h_counts, int* ntasks) {
     std::vector<MeTask> tasks;
-    for (Encoder* E : G->enc) {
+    for (Encoder* E : enc) {
         if (E->last_read < 0) continue;
         // the loop's picture types are set one sub-group ahead of the coded picture, exactly
         // as dgpu_encoder_code_next sets them; untyped pictures get their likely references
         collect_me_tasks(*E, nullptr, E->me_max_tasks, tasks);
     }
     if (tasks.empty()) return DGPU_OK;
-    // the group's stream follows every member's stream (their loads), and each member's
+    // the estimation's stream follows every member's stream (their loads), and each member's
     // stream follows the estimation (the host waits for it below as well)
-    for (Encoder* E : G->enc) {
-        DGPU_CHECK_CUDA(cudaEventRecord(G->ev, E->st));
-        DGPU_CHECK_CUDA(cudaStreamWaitEvent(G->st, G->ev, 0));
+    for (Encoder* E : enc) {
+        DGPU_CHECK_CUDA(cudaEventRecord(ev, E->st));
+        DGPU_CHECK_CUDA(cudaStreamWaitEvent(st, ev, 0));
     }
-    const int rc = run_me_tasks(tasks, G->st, G->ws, G->ws_bytes, G->d_counts, G->h_counts);
+    const int rc = run_me_tasks(tasks, st, ws, ws_bytes, d_counts, h_counts);
     if (rc) return rc;
-    DGPU_CHECK_CUDA(cudaEventRecord(G->ev, G->st));
-    for (Encoder* E : G->enc) DGPU_CHECK_CUDA(cudaStreamWaitEvent(E->st, G->ev, 0));
+    DGPU_CHECK_CUDA(cudaEventRecord(ev, st));
+    for (Encoder* E : enc) DGPU_CHECK_CUDA(cudaStreamWaitEvent(E->st, ev, 0));
     if (ntasks) *ntasks = (int)tasks.size();
     return DGPU_OK;
+}
+
+// Page-locked task counts and an ordering event per host thread, for dgpu_encoders_estimate.
+struct EstimateHostState {
+    int* h_counts = nullptr;
+    int cap = 0;
+    cudaEvent_t ev = nullptr;
+    ~EstimateHostState() {
+        if (h_counts) cudaFreeHost(h_counts);
+        if (ev) cudaEventDestroy(ev);
+    }
+};
+
+}  // namespace
+}  // namespace dgpu
+
+extern "C" int dgpu_encoder_group_estimate(void* group, int* ntasks) {
+    Group* G = static_cast<Group*>(group);
+    if (ntasks) *ntasks = 0;
+    if (!G) return DGPU_ERR_ARG;
+    return estimate_members(G->enc, G->st, G->ev, G->ws, G->ws_bytes, G->d_counts, G->h_counts, ntasks);
+}
+
+extern "C" int dgpu_encoders_estimate(void* const* encoders, int n, void* workspace, size_t ws_bytes, void* stream,
+                                      int* ntasks) {
+    if (ntasks) *ntasks = 0;
+    if (!encoders || n < 1 || !workspace) return DGPU_ERR_ARG;
+    std::vector<Encoder*> enc;
+    for (int k = 0; k < n; ++k) {
+        Encoder* E = static_cast<Encoder*>(encoders[k]);
+        bool dup = false;
+        for (Encoder* e : enc) dup = dup || e == E;
+        if (!E || dup || !same_geometry(*E, *static_cast<Encoder*>(encoders[0]))) return DGPU_ERR_ARG;
+        enc.push_back(E);
+    }
+    int nt = 0;
+    const size_t me_ws = group_ws_bytes(enc, &nt);
+    if (me_ws == 0) return DGPU_ERR_ARG;
+    const size_t need = align_up(me_ws, 256) + align_up(sizeof(int) * nt, 256);
+    if (ws_bytes < need) return DGPU_ERR_NOMEM;
+    thread_local EstimateHostState hs;
+    if (hs.cap < nt) {
+        if (hs.h_counts) cudaFreeHost(hs.h_counts);
+        hs.h_counts = nullptr;
+        hs.cap = 0;
+        DGPU_CHECK_CUDA(cudaMallocHost(reinterpret_cast<void**>(&hs.h_counts), sizeof(int) * nt));
+        hs.cap = nt;
+    }
+    if (!hs.ev) DGPU_CHECK_CUDA(cudaEventCreateWithFlags(&hs.ev, cudaEventDisableTiming));
+    char* base = static_cast<char*>(workspace);
+    int* d_counts = reinterpret_cast<int*>(base + align_up(me_ws, 256));
+    return estimate_members(enc, as_stream(stream), hs.ev, workspace, me_ws, d_counts, hs.h_counts, ntasks);
 }

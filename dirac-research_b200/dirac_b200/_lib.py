@@ -128,6 +128,7 @@ SIGNATURES = {
     "dgpu_encoder_group_create": (c_int, [P_void, c_int, P_void]),
     "dgpu_encoder_group_destroy": (c_int, [c_void_p]),
     "dgpu_encoder_group_estimate": (c_int, [c_void_p, P_int]),
+    "dgpu_encoders_estimate": (c_int, [P_void, c_int, c_void_p, c_size_t, c_void_p, P_int]),
     "dgpu_dequantise_batch": (
         c_int, [c_int, P_int, P_int, P_void, P_void, P_int, P_int, P_int, P_int, P_int, c_void_p, c_void_p],
     ),

@@ -4,10 +4,14 @@ Each request is a sequence of frames of its own size and bit depth.  A request i
 soon as its encoder's device memory (``encoder.device_bytes``) fits in what the budget has
 left; until then it waits in arrival order.  Every admitted stream gets its own encoder, CUDA
 stream and host thread, so work from streams that arrive while others are on the GPU overlaps
-on the device (continuous admission, not a queue of whole jobs).  Frames of a stream become
+on the device (continuous admission, not a queue of whole jobs).  With batch_me, the streams of
+one picture format also share their motion estimation: a stream that has loaded a frame joins
+its format's MeBatcher, and one launch (dgpu_encoders_estimate) estimates the estimable
+pictures of every stream that joined within a short window.  Frames of a stream become
 available one frame interval apart from its arrival (live encoding); a picture's latency is
-the time from its frame's availability to the end of its coding on the device.  Results of a
-stream do not depend on what runs beside it: the encoders share no state.
+the time from its frame's availability to the end of its coding on the device, reported apart
+from the admission wait (arrival to admission).  Results of a stream do not depend on what
+runs beside it: the encoders share no state, and an estimate is the same in any batch.
 
     python -m dirac_b200.serving --seconds 10 --rate 4 --budget-gb 40
 """
@@ -29,18 +33,99 @@ class Request:
         self.name = name
 
 
+class MeBatcher:
+    """Motion estimation shared by the live streams of one picture format.  A stream thread that
+    has loaded new frames calls estimate(encoder) and blocks; the first caller of a round waits
+    `window` seconds for other streams to join, then estimates every joined encoder's estimable
+    pictures in one dgpu_encoders_estimate launch (their threads are all waiting, so no encoder
+    is in use elsewhere) and releases them.  The workspace grows to the largest round."""
+
+    def __init__(self, window=0.002, max_batch=8):
+        import torch
+
+        from . import _lib
+
+        self.lib = _lib.load()
+        self.window = window
+        self.max_batch = max_batch
+        self.cv = threading.Condition()
+        self.pending = []      # [encoder, done flag holder]
+        self.leading = False
+        self.stream = torch.cuda.Stream()
+        self.ws = None
+        self.rounds = 0
+        self.batched = 0       # encoders estimated, summed over rounds
+        self.tasks = 0
+        self.error = None
+
+    def estimate(self, enc):
+        entry = [enc, False]
+        with self.cv:
+            self.pending.append(entry)
+            while not entry[1]:
+                if not self.leading:
+                    self.leading = True
+                    break
+                self.cv.wait()
+            if entry[1]:
+                if self.error:
+                    raise RuntimeError(self.error)
+                return
+        # leader: gather the round, estimate, release everyone in it
+        time.sleep(self.window)
+        with self.cv:
+            batch = self.pending[:self.max_batch]
+            self.pending = self.pending[self.max_batch:]
+        try:
+            self._run([e[0] for e in batch])
+        except Exception as ex:  # reported to every member of the round
+            self.error = repr(ex)
+        with self.cv:
+            for e in batch:
+                e[1] = True
+            self.leading = False
+            self.cv.notify_all()
+        if self.error:
+            raise RuntimeError(self.error)
+        if not entry[1]:  # the leader's own entry fell beyond max_batch: go round again
+            self.estimate(enc)
+
+    def _run(self, encs):
+        import ctypes
+
+        import torch
+
+        from . import _lib
+
+        handles = _lib.ptr_array([e.handle.value for e in encs])
+        need = self.lib.dgpu_encoder_group_device_bytes(handles, len(encs))
+        if need == 0:
+            raise ValueError("encoders of different formats in one estimation")
+        if self.ws is None or self.ws.numel() < need:
+            self.ws = torch.empty(need, dtype=torch.uint8, device="cuda")
+        n = ctypes.c_int(0)
+        _lib.check(self.lib.dgpu_encoders_estimate(handles, len(encs), self.ws.data_ptr(), self.ws.numel(),
+                                                   self.stream.cuda_stream, ctypes.byref(n)), "dgpu_encoders_estimate")
+        self.rounds += 1
+        self.batched += len(encs)
+        self.tasks += n.value
+
+
 class ServingLoop:
     def __init__(self, budget_bytes, max_active=16, frame_interval=0.0, slots=24, collect=None,
-                 encoder_factory=None, bytes_fn=None):
+                 encoder_factory=None, bytes_fn=None, batch_me=False):
         """budget_bytes: device memory the loop may give to encoders.  max_active: streams
         coded at once.  frame_interval: seconds between a stream's frames (0: all at arrival).
         slots: picture slots per encoder.  collect(request, encoder, info): called after each
-        coded picture (e.g. to read results).  encoder_factory / bytes_fn: injectable for tests."""
+        coded picture (e.g. to read results).  encoder_factory / bytes_fn: injectable for tests.
+        batch_me: share motion-estimation launches between the live streams of one format."""
         self.budget = budget_bytes
         self.max_active = max_active
         self.frame_interval = frame_interval
         self.slots = slots
         self.collect = collect
+        self.batch_me = batch_me
+        self.batchers = {}
         self.warm = encoder_factory is None
         if encoder_factory is None:
             from .encoder import SequenceEncoder
@@ -74,9 +159,19 @@ class ServingLoop:
         frames_done = [0]
         t0 = time.perf_counter()
 
+        def batcher_for(r):
+            if not self.batch_me:
+                return None
+            key = tuple(sorted(r.params.items()))
+            with lock:
+                if key not in self.batchers:
+                    self.batchers[key] = MeBatcher()
+                return self.batchers[key]
+
         def worker(r):
             try:
                 enc = self.encoder_factory(r.params, self._slots_for(r))
+                batcher = batcher_for(r)
                 avail = {}
                 pending = []
 
@@ -102,8 +197,12 @@ class ServingLoop:
                         time.sleep(wait)
                     avail[i] = max(due, t0 + r.arrival)
                     enc.load(f)
+                    if batcher is not None:
+                        batcher.estimate(enc)
                     drain()
                 enc.end_sequence()
+                if batcher is not None:
+                    batcher.estimate(enc)
                 drain()
                 enc.close()
             except Exception as e:  # reported after the loop, never swallowed
@@ -151,9 +250,16 @@ class ServingLoop:
                 "frames_per_s": frames_done[0] / wall if wall > 0 else None,
                 "latency_ms": {"p50": pct(0.5), "p99": pct(0.99), "max": lat[-1] if lat else None},
                 "admission_wait_ms": {"p50": statistics.median(waits) if waits else None,
+                                      "p99": sorted(waits)[min(len(waits) - 1, int(round(0.99 * (len(waits) - 1))))]
+                                      if waits else None,
                                       "max": max(waits) if waits else None},
                 "peak_active": state["peak_active"], "peak_bytes": state["peak_bytes"],
-                "budget_bytes": self.budget}
+                "budget_bytes": self.budget,
+                "shared_estimation": {"rounds": sum(b.rounds for b in self.batchers.values()),
+                                      "streams_per_round": (sum(b.batched for b in self.batchers.values()) /
+                                                            max(1, sum(b.rounds for b in self.batchers.values()))),
+                                      "estimates": sum(b.tasks for b in self.batchers.values())}
+                if self.batch_me else None}
 
 
 RESOLUTIONS = {"cif": (352, 288), "576": (720, 576), "720": (1280, 720), "1080": (1920, 1080),
@@ -213,14 +319,16 @@ def main(argv=None):
     ap.add_argument("--frames", default="8-64")
     ap.add_argument("--depths", default="8", help="bit depths drawn per stream, e.g. 8,10")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--batch-me", type=int, default=1, help="1: streams of one format share estimation launches")
     a = ap.parse_args(argv)
     lo, hi = (int(x) for x in a.frames.split("-"))
     reqs = make_requests(a.seconds, a.rate, a.resolutions.split(","), lo, hi, a.seed,
                          depths=[int(d) for d in a.depths.split(",")])
-    loop = ServingLoop(int(a.budget_gb * 1e9), a.max_active, 1.0 / a.fps if a.fps > 0 else 0.0)
+    loop = ServingLoop(int(a.budget_gb * 1e9), a.max_active, 1.0 / a.fps if a.fps > 0 else 0.0,
+                       batch_me=bool(a.batch_me))
     stats = loop.run(reqs)
     stats["config"] = {"seconds": a.seconds, "rate": a.rate, "resolutions": a.resolutions, "frames": a.frames,
-                       "depths": a.depths, "fps": a.fps, "budget_gb": a.budget_gb}
+                       "depths": a.depths, "fps": a.fps, "budget_gb": a.budget_gb, "batch_me": bool(a.batch_me)}
     print(json.dumps(stats))
     return 0
 

@@ -566,6 +566,13 @@ size_t dgpu_encoder_group_device_bytes(void* const* encoders, int n);
 int dgpu_encoder_group_create(void* const* encoders, int n, void** group);
 int dgpu_encoder_group_destroy(void* group);
 int dgpu_encoder_group_estimate(void* group, int* ntasks);
+/* The same estimation for a set of encoders chosen per call (e.g. the live streams of one
+ * picture format a serving loop has on the GPU at that moment), with a workspace the caller
+ * holds: at least dgpu_encoder_group_device_bytes(encoders, n) bytes of device memory.  Runs
+ * on `stream` after the encoders' pending work; their streams follow it.  Synchronises with
+ * the estimation; none of the encoders may be used by another thread meanwhile. */
+int dgpu_encoders_estimate(void* const* encoders, int n, void* workspace, size_t ws_bytes, void* stream,
+                           int* ntasks);
 
 /* ---------------------------------------------------------------------------------------
  * Arithmetic coding of quantised subbands on the host, and entropy-correction factors.

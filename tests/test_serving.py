@@ -84,10 +84,11 @@ def test_encoder_device_bytes_grows_with_size_and_slots():
 
 
 @pytest.mark.gpu
-def test_served_streams_equal_alone_and_in_the_mix(gpu):
+@pytest.mark.parametrize("batch_me", [False, True], ids=["own", "shared"])
+def test_served_streams_equal_alone_and_in_the_mix(gpu, batch_me):
     """Three streams of different sizes coded one at a time and then concurrently (admitted
-    together, overlapping on the device): every picture's output samples and quantised indices
-    are identical."""
+    together, overlapping on the device; with shared estimation rounds per format): every
+    picture's output samples and quantised indices are identical."""
     from dirac_b200 import synth
     from dirac_b200.encoder import OUTPUT, QINDEX
     from dirac_b200.serving import Request, ServingLoop, params_for
@@ -106,7 +107,7 @@ def test_served_streams_equal_alone_and_in_the_mix(gpu):
             with lock:
                 out[(r.name, pn)] = got
 
-        ServingLoop(budget_bytes=int(8e9), max_active=max_active, collect=collect).run(reqs)
+        ServingLoop(budget_bytes=int(8e9), max_active=max_active, collect=collect, batch_me=batch_me).run(reqs)
         return out
 
     alone = run(1)
@@ -115,3 +116,41 @@ def test_served_streams_equal_alone_and_in_the_mix(gpu):
     for k in alone:
         for a, b in zip(alone[k], mixed[k]):
             np.testing.assert_array_equal(a, b, err_msg=str(k))
+
+
+@pytest.mark.gpu
+def test_shared_estimation_rounds_give_each_stream_its_own_results(gpu):
+    """Four live streams of one format whose motion estimation runs in shared launches
+    (MeBatcher, dgpu_encoders_estimate): every picture equals the same stream coded alone with
+    its encoder's own estimation, and the rounds did batch several streams."""
+    from dirac_b200 import synth
+    from dirac_b200.encoder import MV, OUTPUT, QINDEX
+    from dirac_b200.serving import Request, ServingLoop, params_for
+
+    reqs = [Request(params_for(176, 144), synth.make_sequence(176, 144, 10, n_rects=4, vmax=6, seed=40 + k),
+                    0.0, f"q{k}") for k in range(4)]
+
+    def run(max_active, batch_me):
+        out = {}
+        lock = threading.Lock()
+
+        def collect(r, enc, info):
+            pn = info["pnum"]
+            got = [enc.read(pn, OUTPUT, c) for c in range(3)] + [enc.read(pn, QINDEX, 0)]
+            mv = enc.read(pn, MV)
+            with lock:
+                out[(r.name, pn)] = got + ([mv] if mv is not None else [])
+
+        loop = ServingLoop(budget_bytes=int(8e9), max_active=max_active, frame_interval=0.004, collect=collect,
+                           batch_me=batch_me)
+        return out, loop.run(reqs)
+
+    alone, _ = run(1, False)
+    shared, stats = run(4, True)
+    assert alone.keys() == shared.keys() and len(alone) == 40
+    for k in alone:
+        assert len(alone[k]) == len(shared[k]), k
+        for a, b in zip(alone[k], shared[k]):
+            np.testing.assert_array_equal(a, b, err_msg=str(k))
+    est = stats["shared_estimation"]
+    assert est["estimates"] > 0 and est["streams_per_round"] > 1.0, est
