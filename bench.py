@@ -74,6 +74,7 @@ def parse_args():
     ap.add_argument("--streams", type=int, default=8, help="concurrent sequences per GPU (batched form)")
     ap.add_argument("--me-groups", type=int, default=2,
                     help="encoder groups the batched form's sequences are split into (run concurrently)")
+    ap.add_argument("--serving-rate", type=float, default=40.0, help="stream arrivals per second (Poisson)")
     ap.add_argument("--serving-seconds", type=float, default=6.0,
                     help="length of the serving-loop run reported under 'serving' (0: skip)")
     ap.add_argument("--hetero-steps", type=int, default=5,
@@ -928,15 +929,16 @@ def main():
     if args.serving_seconds > 0 and world == 1:
         from dirac_b200 import serving as S
 
-        cfg = {"seconds": args.serving_seconds, "arrivals_per_s": 4.0, "fps_per_stream": 50,
+        cfg = {"seconds": args.serving_seconds, "arrivals_per_s": args.serving_rate, "fps_per_stream": 50,
                "resolutions": "352x288, 720x576, 1280x720, 1920x1080, 3840x2160 (4:2:0, 8- or 10-bit)",
                "frames_per_stream": "8-64", "budget_gb": 40,
                "input": "per resolution and depth a pool of synthetic frames (16; 8 at 3840x2160), each stream "
                         "cycling through its pool from a random offset"}
         try:
-            reqs = S.make_requests(args.serving_seconds, 4.0, ["cif", "576", "720", "1080", "2160"], 8, 64, seed=7,
+            reqs = S.make_requests(args.serving_seconds, args.serving_rate, ["cif", "576", "720", "1080", "2160"], 8, 64,
+                                   seed=7,
                                    depths=(8, 10))
-            serving = S.ServingLoop(int(40e9), max_active=16, frame_interval=1.0 / 50).run(reqs)
+            serving = S.ServingLoop(int(40e9), max_active=16, frame_interval=1.0 / 50, batch_me=True).run(reqs)
         except Exception as e:  # the serving leg must not cost the bench line; its failure is reported
             serving = {"error": repr(e)}
         serving["config"] = cfg
