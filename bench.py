@@ -36,6 +36,8 @@ reference encoder itself (its public C API) on this host's cores.
 import argparse
 import json
 import os
+
+import numpy as np
 import statistics
 import subprocess
 import sys
@@ -84,6 +86,9 @@ def parse_args():
                     help="1: report the device decoder on the plain form's coded sequence under 'decoding'")
     ap.add_argument("--cpu-baseline", type=int, default=1,
                     help="1: time the reference encoder on this host first (cpu_baseline, parity_vs_reference)")
+    ap.add_argument("--leg", choices=["all", "encode", "decode"], default="all",
+                    help="encode / decode: only the plain form's coding (or its device decoding) of the sequence, "
+                         "--warmup then --steps times, for profilers; prints the launch count, no bench line")
     ap.add_argument("--impl", choices=["gpu", "reference"], default="gpu")
     return ap.parse_args()
 
@@ -530,10 +535,86 @@ def run_decoding(args, enc, infos, peak, cpu_decode=None):
                         "samples"}
 
 
+def run_leg(args):
+    """One leg alone for profilers (ncu's launch lists and captures): the device encoder coding
+    the sequence from device-resident frames (encode), or additionally the device decoder
+    decoding the coded sequence (decode), --warmup untimed then --steps more times."""
+    import torch
+
+    import dirac_b200
+    from dirac_b200 import encoder as E
+    from dirac_b200.decoder import SequenceDecoder, decoder_params
+
+    lib = dirac_b200.load()
+    frames = [tuple(torch.from_numpy(p).cuda() for p in fr) for fr in make_frames(args.frames, seed=1000)]
+    enc = E.SequenceEncoder(PARAMS, max_pictures=args.frames)
+
+    def encode():
+        enc.reset()
+        for f in frames:
+            enc.load(f)
+        enc.end_sequence()
+        out = []
+        while True:
+            info = enc.code_next()
+            if info is None:
+                return out
+            out.append(info)
+
+    if args.leg == "encode":
+        for _ in range(args.warmup):
+            encode()
+        torch.cuda.synchronize()
+        n0 = lib.dgpu_launch_count()
+        for _ in range(args.steps):
+            encode()
+        torch.cuda.synchronize()
+        print(json.dumps({"leg": "encode", "launches_per_step": (lib.dgpu_launch_count() - n0) // max(1, args.steps)}))
+        return
+    infos = encode()
+    dec = SequenceDecoder(decoder_params(PARAMS), max_pictures=args.frames)
+    inputs = []
+    depth = PARAMS["wlt_depth"]
+    mul = 1 << depth
+    shapes = [(((PARAMS["height"] >> (c > 0)) + mul - 1) // mul * mul,
+               ((PARAMS["width"] >> (c > 0)) + mul - 1) // mul * mul) for c in range(3)]
+    for info in infos:
+        pn = info["pnum"]
+        refs = [] if info["intra"] else [x for x in (info["ref1"], info["ref2"]) if x >= 0]
+        mot = None
+        if not info["intra"]:
+            mv = enc.read(pn, E.MV).reshape(info["num_refs"], -1, 2)
+            mot = {"mv": [torch.from_numpy(mv[k].copy()).cuda() for k in range(len(refs))],
+                   **{k: torch.from_numpy(enc.read(pn, w)).cuda() for k, w in (("mode", E.MODE), ("dc", E.DC),
+                                                                                 ("split", E.SPLIT))}}
+        q = [torch.from_numpy(enc.read(pn, E.QINDEX, c).reshape(shapes[c])).cuda() for c in range(3)]
+        cbs = torch.from_numpy(np.concatenate([enc.read(pn, E.CBSKIP, c) for c in range(3)])).cuda()
+        inputs.append((pn, dec.prepare(pn, info["intra"], refs, info["filter"], q,
+                                       [enc.read(pn, E.BANDS, c) for c in range(3)], cbs, mot)))
+
+    def decode():
+        for _, I in inputs:
+            dec.decode_prepared(I)
+        for pn, _ in inputs:
+            dec.release(pn)
+
+    for _ in range(args.warmup):
+        decode()
+    torch.cuda.synchronize()
+    n0 = lib.dgpu_launch_count()
+    for _ in range(args.steps):
+        decode()
+    torch.cuda.synchronize()
+    print(json.dumps({"leg": "decode", "launches_per_step": (lib.dgpu_launch_count() - n0) // max(1, args.steps)}))
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.leg != "all":
+        run_leg(args)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
