@@ -219,11 +219,29 @@ struct FloatSeq {
     double bound;  // smallest power of two above c: additions below it are exact
 };
 
+// The exponent e with v in [2^(e-1), 2^e) of a positive normal double, from its bits.
+__device__ __forceinline__ int exp_above(double v) {
+    return (int)((unsigned long long)__double_as_longlong(v) >> 52 & 0x7ff) - 1022;
+}
+
+// 2^e as a double, from its bits (e within the normal range).
+__device__ __forceinline__ double pow2_of(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+
+// Whether a non-negative double is a multiple of 2^k: the trailing zeros of its mantissa
+// (implicit bit included) plus its binary exponent reach k.
+__device__ __forceinline__ bool multiple_of_pow2(double v, int k) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    const int be = (int)(b >> 52 & 0x7ff);
+    unsigned long long m = b & ((1ULL << 52) - 1);
+    if (be == 0 && m == 0) return true;  // zero
+    if (be) m |= 1ULL << 52;
+    const int e = (be ? be : 1) - 1075;  // v = m * 2^e
+    return __ffsll((long long)m) - 1 + e >= k;
+}
+
 __device__ __forceinline__ double pow2_above(double c) {
     if (c <= 0.0) return 16777216.0;  // integer partial sums from 0 are exact below 2^24
-    int e;
-    frexp(c, &e);  // c in [2^(e-1), 2^e)
-    return ldexp(1.0, e);
+    return pow2_of(exp_above(c));     // c in [2^(e-1), 2^e)
 }
 
 __device__ __forceinline__ FloatSeq float_seq_start(float start) {
@@ -244,12 +262,10 @@ __device__ __forceinline__ bool float_seq_add_exact(FloatSeq& f, int total) {
         return true;
     }
     if (fin >= 16777216.0) return false;
-    int e;
-    frexp(fin, &e);  // fin in [2^(e-1), 2^e): float spacing 2^(e-24)
-    const double t = ldexp(f.c, 24 - e);
-    if (t != floor(t)) return false;
+    const int e = exp_above(fin);  // fin in [2^(e-1), 2^e): float spacing 2^(e-24)
+    if (!multiple_of_pow2(f.c, e - 24)) return false;
     f.c = fin;
-    f.bound = pow2_above(fin);
+    f.bound = pow2_of(e);
     return true;
 }
 
@@ -406,17 +422,19 @@ __device__ __noinline__ float subpel_cost(const int16_t* pic, int pw, const int1
     return subpel_cost_p<3>(pic, pw, up, uw, uh, b, mx, my, start);
 }
 
-// Integer total of |pred - pic| over a block for one candidate (the terms the cost loop adds).
+// Integer total of |pred - pic| over a block for one candidate (the terms the cost loop adds),
+// over the block's pixels [kb, ke) in raster order (kb a multiple of 32; integer, so a block's
+// total may be split between warps).
 template <int P>
 __device__ __forceinline__ int subpel_total_p(const int16_t* pic, int pw, const int16_t* up, int uw, int uh,
-                                              const Blim& b, int mx, int my) {
+                                              const Blim& b, int mx, int my, int kb, int ke) {
     const int lane = threadIdx.x & 31;
-    const int n = b.xl * b.yl;
+    const int n = ke;
     const UpFast<P> fast(b, uw, uh, mx, my);
-    PixWalk w(b.xl);
+    PixWalk w(b.xl, kb);
     int tot = 0;
     if (fast.inside) {
-        for (int k0 = 0; k0 < n; k0 += 256) {
+        for (int k0 = kb; k0 < n; k0 += 256) {
 #pragma unroll
             for (int s = 0; s < 8; ++s) {
                 if (k0 + 32 * s + lane < n) {
@@ -428,7 +446,7 @@ __device__ __forceinline__ int subpel_total_p(const int16_t* pic, int pw, const 
         }
         return __reduce_add_sync(0xffffffffu, tot);
     }
-    for (int k0 = 0; k0 < n; k0 += 256) {
+    for (int k0 = kb; k0 < n; k0 += 256) {
 #pragma unroll
         for (int s = 0; s < 8; ++s) {
             if (k0 + 32 * s + lane < n) {
@@ -442,11 +460,13 @@ __device__ __forceinline__ int subpel_total_p(const int16_t* pic, int pw, const 
 }
 
 __device__ __noinline__ int subpel_total(const int16_t* pic, int pw, const int16_t* up, int uw, int uh, int p,
-                                         const Blim& b, int mx, int my) {
+                                         const Blim& b, int mx, int my, int kb = 0, int ke = -1) {
     if (b.xl <= 0 || b.yl <= 0) return 0;
-    if (p == 1) return subpel_total_p<1>(pic, pw, up, uw, uh, b, mx, my);
-    if (p == 2) return subpel_total_p<2>(pic, pw, up, uw, uh, b, mx, my);
-    return subpel_total_p<3>(pic, pw, up, uw, uh, b, mx, my);
+    if (ke < 0) ke = b.xl * b.yl;
+    if (ke <= kb) return 0;
+    if (p == 1) return subpel_total_p<1>(pic, pw, up, uw, uh, b, mx, my, kb, ke);
+    if (p == 2) return subpel_total_p<2>(pic, pw, up, uw, uh, b, mx, my, kb, ke);
+    return subpel_total_p<3>(pic, pw, up, uw, uh, b, mx, my, kb, ke);
 }
 
 // Copies the h x w region at (x0, y0) of a pw x ph plane into shared memory (rows of w),
@@ -1169,9 +1189,12 @@ __device__ __noinline__ void dome_totals(const ModeLaunch& L, const ModeJob& J, 
     for (int r = 0; r < J.nref; ++r) {
         short2 c[4];
         const int nc = dome_candidates(J, x, y, level, r, c);
-        for (int q = 0; q < nc; ++q)
-            tot[4 * r + q] = subpel_total(J.pic, J.pw, J.up[r], 2 * J.pw, 2 * J.ph, L.prec, bl, c[q].x, c[q].y);
+        for (int q = 0; q < nc; ++q) {
+            const int t = subpel_total(J.pic, J.pw, J.up[r], 2 * J.pw, 2 * J.ph, L.prec, bl, c[q].x, c[q].y);
+            if ((threadIdx.x & 31) == 0) tot[4 * r + q] = t;
+        }
     }
+    __syncwarp();
 }
 
 __device__ __noinline__ void do_me(const ModeLaunch& L, const ModeJob& J, int x, int y, int level,
@@ -1346,6 +1369,9 @@ __global__ void __launch_bounds__(ME_THREADS, 5) mode_wavefront_kernel(const __g
     __shared__ short2 s_v0[2][MAX_V0];      // the superblock's distinct block vectors per reference
     __shared__ int s_t0[2][MAX_V0];         // their integer totals at superblock size
     __shared__ int s_n0[2];                 // how many (0: none precomputed)
+    __shared__ int s_pre1[WARPS_PER_CTA][8];  // each warp's level-1 candidate totals
+    __shared__ short2 s_cand[2][4];           // level-0 candidates per reference
+    __shared__ int s_ncand[2];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (;;) {
         __syncthreads();
@@ -1358,7 +1384,8 @@ __global__ void __launch_bounds__(ME_THREADS, 5) mode_wavefront_kernel(const __g
         const ModeJob& J = L.jobs[jn];
         const int s = ysb * J.xnsb + xsb;
         // level-1 candidate totals of this warp's sub-superblock while the neighbours finish
-        int pre1[8];
+        // (in shared memory: the totals are read back by every lane of the warp)
+        int* const pre1 = s_pre1[warp];
         dome_totals(L, J, (xsb << 1) + (warp & 1), (ysb << 1) + (warp >> 1), 1, pre1);
         // Level-0 candidates are level-1 vectors, each chosen among its sub-superblock's block
         // vectors: the integer totals at superblock size of the distinct block vectors (when
@@ -1434,18 +1461,23 @@ __global__ void __launch_bounds__(ME_THREADS, 5) mode_wavefront_kernel(const __g
             const float lambda = me.lambda[k];
             const Blim bl = block_limits(L.lb[0], J.pw, J.ph, xsb, ysb);
             const int xb = xsb << 2, yb = ysb << 2;
-            short2 cand[2][4];
-            int ncand[2];
-            for (int r = 0; r < J.nref; ++r) {
+            // the candidates (the four level-1 vectors, duplicates dropped) in shared memory, so
+            // that warp q reads its own without a dynamically indexed local array
+            if (threadIdx.x < J.nref) {
+                const int r = threadIdx.x;
                 int nc = 0;
                 for (int jj = 0; jj < 2; ++jj)
                     for (int ii = 0; ii < 2; ++ii) {
                         const short2 v = __ldcg(&guide.mv[r][(size_t)((ysb << 1) + jj) * guide.xnb + (xsb << 1) + ii]);
                         bool dup = false;
-                        for (int q = 0; q < nc; ++q) dup |= (cand[r][q].x == v.x && cand[r][q].y == v.y);
-                        if (!dup) cand[r][nc++] = v;
+                        for (int q = 0; q < nc; ++q) dup |= (s_cand[r][q].x == v.x && s_cand[r][q].y == v.y);
+                        if (!dup) s_cand[r][nc++] = v;
                     }
-                ncand[r] = nc;
+                s_ncand[r] = nc;
+            }
+            __syncthreads();
+            for (int r = 0; r < J.nref; ++r) {
+                const int nc = s_ncand[r];
                 const short2* bv = blk.mv[r];
                 const int W = blk.xnb;
                 short2 pr = make_short2(0, 0);
@@ -1458,18 +1490,18 @@ __global__ void __launch_bounds__(ME_THREADS, 5) mode_wavefront_kernel(const __g
                     pr = mv_mean(__ldcg(&bv[(size_t)yb * W + xb - 1]), __ldcg(&bv[(size_t)(yb + 1) * W + xb - 1]));
                 // warp q evaluates candidate q (BlockMatcher::FindBestMatchSubp's loop body)
                 if (warp < nc && bl.xl > 0 && bl.yl > 0) {
-                    const float mvcost = (float)getvarup(pr, cand[r][warp].x, cand[r][warp].y);
+                    const short2 cw = s_cand[r][warp];
+                    const float mvcost = (float)getvarup(pr, cw.x, cw.y);
                     const float start = mvcost * lambda;
                     int pre = -1;
                     for (int q = 0; q < s_n0[r]; ++q)
-                        if (s_v0[r][q].x == cand[r][warp].x && s_v0[r][q].y == cand[r][warp].y) pre = q;
+                        if (s_v0[r][q].x == cw.x && s_v0[r][q].y == cw.y) pre = q;
                     FloatSeq f = float_seq_start(start);
                     float sum;
                     if (pre >= 0 && float_seq_add_exact(f, s_t0[r][pre]))
                         sum = (float)f.c;  // precomputed total, and no addition of the loop could round
                     else
-                        sum = subpel_cost(J.pic, J.pw, J.up[r], 2 * J.pw, 2 * J.ph, L.prec, bl, cand[r][warp].x,
-                                          cand[r][warp].y, start);
+                        sum = subpel_cost(J.pic, J.pw, J.up[r], 2 * J.pw, 2 * J.ph, L.prec, bl, cw.x, cw.y, start);
                     if (lane == 0) {
                         s_sum[r][warp] = sum;
                         s_mvc[r][warp] = mvcost;
@@ -1481,11 +1513,11 @@ __global__ void __launch_bounds__(ME_THREADS, 5) mode_wavefront_kernel(const __g
                 for (int r = 0; r < J.nref; ++r) {
                     Cost3 best{me.cost[r][3 * k], me.cost[r][3 * k + 1], 100000000.0f};
                     short2 bmv = me.mv[r][k];
-                    for (int q = 0; q < ncand[r]; ++q) {
+                    for (int q = 0; q < s_ncand[r]; ++q) {
                         if (bl.xl <= 0 || bl.yl <= 0) break;
                         const float sum = s_sum[r][q], mvcost = s_mvc[r][q];
                         if (sum < best.total) {
-                            bmv = cand[r][q];
+                            bmv = s_cand[r][q];
                             best.total = sum;
                             best.mvcost = mvcost;
                             best.SAD = sum - mvcost * lambda;
