@@ -415,6 +415,172 @@ extern "C" int dgpu_rect_lp_filter(int16_t* pic, int w, int h, int stride, float
     return DGPU_OK;
 }
 
+namespace dgpu {
+namespace {
+
+// DIAGLP residue prefilter (DiagFilter, libdirac_encoder/prefilter.cpp:535-588, with
+// DiagFilterBchkD / DiagFilterD :307-398): a 13 x 13 two-dimensional low-pass filter given by
+// one quadrant of taps f[j][i] (offsets 0..6 down and across; the other quadrants mirror it),
+// each output (2^15 + sum) >> 16 cast to int16, source indices clamped to the component (the
+// reference's unclamped interior loop reads the same samples).  The quadrants are the
+// reference's hand-designed tables for bandwidths 0.2 .. 0.9 (GetDiagLPFilter, :401-531), mixed
+// with a unit impulse by the strength and quality factor; they decide the filtered samples.
+struct DiagTaps {
+    int f[7][7];
+};
+
+const int kDiagLPTables[8][7][7] = {
+    {  // bandwidth 0.2
+        {  2855,   2540,   1775,    947,    364,     89,     10},
+        {  2540,   2251,   1551,    804,    290,     59,      1},
+        {  1775,   1551,   1020,    475,    130,      3,    -10},
+        {   947,    804,    475,    165,      5,    -22,     -6},
+        {   364,    290,    130,      5,    -28,    -10,      0},
+        {    89,     59,      3,    -22,    -10,      0,      0},
+        {    10,      1,    -10,     -6,      0,      0,      0},
+    },
+    {  // bandwidth 0.3
+        {  5767,   4718,   2498,    745,     72,      5,     23},
+        {  4718,   3796,   1875,    423,    -58,    -41,      7},
+        {  2498,   1875,    643,   -146,   -241,    -88,     -9},
+        {   745,    423,   -146,   -367,   -220,    -51,     -2},
+        {    72,    -58,   -241,   -220,    -78,     -5,      0},
+        {     5,    -41,    -88,    -51,     -5,      0,      0},
+        {    23,      7,     -9,     -2,      0,      0,      0},
+    },
+    {  // bandwidth 0.4
+        { 10534,   7642,   2603,    194,     56,    120,     28},
+        {  7642,   5237,   1218,   -383,   -153,     40,      2},
+        {  2603,   1218,   -771,   -958,   -269,     -3,     -7},
+        {   194,   -383,   -958,   -541,    -18,     48,      4},
+        {    56,   -153,   -269,    -18,     96,     22,      0},
+        {   120,     40,     -3,     48,     22,      0,      0},
+        {    28,      2,     -7,      4,      0,      0,      0},
+    },
+    {  // bandwidth 0.5
+        { 16421,  10159,   1716,     33,    325,     57,      6},
+        { 10159,   5309,   -580,   -747,     44,    -43,    -25},
+        {  1716,   -580,  -2310,   -763,    100,    -19,    -12},
+        {    33,   -747,   -763,    308,    326,     27,      1},
+        {   325,     44,    100,    326,     84,    -14,      0},
+        {    57,    -43,    -19,     27,    -14,      0,      0},
+        {     6,    -25,    -12,      1,      0,      0,      0},
+    },
+    {  // bandwidth 0.6
+        { 23511,  11883,    566,    524,    231,     18,     41},
+        { 11883,   3647,  -2496,   -361,    -96,    -97,      1},
+        {   566,  -2496,  -2329,    459,    152,     -7,     18},
+        {   524,   -361,    459,    979,     33,    -28,      3},
+        {   231,    -96,    152,     33,   -184,    -15,      0},
+        {    18,    -97,     -7,    -28,    -15,      0,      0},
+        {    41,      1,     18,      3,      0,      0,      0},
+    },
+    {  // bandwidth 0.7
+        { 32188,  12652,      3,    921,      1,    128,      0},
+        { 12652,    295,  -3414,     -2,   -343,     -1,    -37},
+        {     3,  -3414,   -212,   1273,      1,     98,      0},
+        {   921,     -2,   1273,    110,   -363,      0,     -8},
+        {     1,   -343,      1,   -363,    -29,     29,      0},
+        {   128,     -1,     98,      0,     29,      0,      0},
+        {     0,    -37,      0,     -8,      0,      0,      0},
+    },
+    {  // bandwidth 0.8
+        { 41902,  12084,    435,    610,    188,     34,     37},
+        { 12084,  -4268,  -2715,   -286,   -144,    -84,     -2},
+        {   435,  -2715,   2809,    640,    127,     10,     17},
+        {   610,   -286,    640,  -1250,    -45,    -26,      2},
+        {   188,   -144,    127,    -45,    259,     -8,      0},
+        {    34,    -84,     10,    -26,     -8,      0,      0},
+        {    37,     -2,     17,      2,      0,      0,      0},
+    },
+    {  // bandwidth 0.9
+        { 53098,  10449,   1546,     73,    342,     38,     12},
+        { 10449,  -9060,   -873,   -727,     52,    -65,    -20},
+        {  1546,   -873,   4261,   -627,    137,    -27,     -7},
+        {    73,   -727,   -627,   -804,    328,     14,      2},
+        {   342,     52,    137,    328,    -83,    -20,      0},
+        {    38,    -65,    -27,     14,    -20,      0,      0},
+        {    12,    -20,     -7,      2,      0,      0,      0},
+    },
+};
+
+constexpr int DIAG_TX = 32, DIAG_TY = 8, DIAG_R = 6;
+
+__global__ void __launch_bounds__(DIAG_TX* DIAG_TY) diag_lp_kernel(const int16_t* __restrict__ in, int in_stride,
+                                                                   int16_t* __restrict__ out, int out_stride, int w,
+                                                                   int h, const __grid_constant__ DiagTaps T) {
+    __shared__ int16_t tile[DIAG_TY + 2 * DIAG_R][DIAG_TX + 2 * DIAG_R];
+    const int x0 = blockIdx.x * DIAG_TX, y0 = blockIdx.y * DIAG_TY;
+    const int tid = threadIdx.y * DIAG_TX + threadIdx.x;
+    // the tile and its halo, coordinates clamped to the component
+    for (int k = tid; k < (DIAG_TY + 2 * DIAG_R) * (DIAG_TX + 2 * DIAG_R); k += DIAG_TX * DIAG_TY) {
+        const int ty = k / (DIAG_TX + 2 * DIAG_R), tx = k - ty * (DIAG_TX + 2 * DIAG_R);
+        const int sy = clampi(y0 + ty - DIAG_R, 0, h - 1), sx = clampi(x0 + tx - DIAG_R, 0, w - 1);
+        tile[ty][tx] = in[(size_t)sy * in_stride + sx];
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const int cx = threadIdx.x + DIAG_R, cy = threadIdx.y + DIAG_R;
+    int val = 1 << 15;
+    val += T.f[0][0] * tile[cy][cx];
+#pragma unroll
+    for (int i = 1; i <= DIAG_R; ++i) val += T.f[0][i] * (tile[cy][cx + i] + tile[cy][cx - i]);
+#pragma unroll
+    for (int j = 1; j <= DIAG_R; ++j) {
+        val += T.f[j][0] * (tile[cy - j][cx] + tile[cy + j][cx]);
+#pragma unroll
+        for (int i = 1; i <= DIAG_R; ++i)
+            val += T.f[j][i] * (tile[cy - j][cx + i] + tile[cy - j][cx - i] + tile[cy + j][cx + i] + tile[cy + j][cx - i]);
+    }
+    out[(size_t)y * out_stride + x] = (int16_t)(val >> 16);
+}
+
+// DiagFilter's taps for a quality factor and strength (prefilter.cpp:535-556, in the
+// reference's float / double arithmetic); false when its bandwidth is above 0.9 and the
+// reference leaves the component unchanged.
+bool diag_lp_taps(float qf, int strength, DiagTaps& T) {
+    const float ffactor = (8.0 + strength - 4.0 - qf) / 5.0;
+    const int factor = std::max(0, std::min(256, int(ffactor * 256.0)));
+    const float bw = (1.0 - ffactor) * 0.6 + 0.4;
+    if (bw > 0.9) return false;
+    const int qbf = std::min(std::max(int(bw * 10.0 + 0.5), 2), 10);
+    for (int j = 0; j < 7; ++j)
+        for (int i = 0; i < 7; ++i)
+            T.f[j][i] = qbf == 10 ? (i == 0 && j == 0 ? 65536 : 0) : kDiagLPTables[qbf - 2][j][i];
+    T.f[0][0] = (factor * T.f[0][0] + ((1 << 8) - factor) * (1 << 16) + (1 << 7)) >> 8;
+    for (int i = 1; i < 7; ++i) T.f[0][i] = (factor * T.f[0][i] + (1 << 7)) >> 8;
+    for (int j = 1; j < 7; ++j)
+        for (int i = 0; i < 7; ++i) T.f[j][i] = (factor * T.f[j][i] + (1 << 7)) >> 8;
+    return true;
+}
+
+}  // namespace
+}  // namespace dgpu
+
+extern "C" int dgpu_diag_lp_filter(int16_t* pic, int w, int h, int stride, float qf, int strength,
+                                   int16_t* scratch, void* stream) {
+    if (!pic || stride < w) return DGPU_ERR_ARG;
+    if (w < 7 || h < 7) return DGPU_ERR_SIZE;  // the reference's edge loops assume 7 samples
+    DiagTaps T;
+    if (!diag_lp_taps(qf, strength, T)) return DGPU_OK;
+    int16_t* tmp = scratch;
+    if (!tmp) {
+        void* p = nullptr;
+        const int rc = library_scratch((size_t)w * h * sizeof(int16_t), stream, &p);
+        if (rc) return rc;
+        tmp = static_cast<int16_t*>(p);
+    }
+    cudaStream_t st = as_stream(stream);
+    // the reference filters from the unfiltered component into a copy
+    DGPU_CHECK_CUDA(cudaMemcpy2DAsync(tmp, (size_t)w * sizeof(int16_t), pic, (size_t)stride * sizeof(int16_t),
+                                      (size_t)w * sizeof(int16_t), h, cudaMemcpyDeviceToDevice, st));
+    dim3 grid((w + DIAG_TX - 1) / DIAG_TX, (h + DIAG_TY - 1) / DIAG_TY);
+    diag_lp_kernel<<<grid, dim3(DIAG_TX, DIAG_TY), 0, st>>>(tmp, w, pic, stride, w, h, T);
+    DGPU_CHECK_LAUNCH();
+    return DGPU_OK;
+}
+
 extern "C" int dgpu_cwm_filter(const int16_t* in, int in_stride, int16_t* out, int out_stride, int w, int h,
                                int strength, void* stream) {
     if (!in || !out || in == out || w < 1 || h < 1 || in_stride < w || out_stride < w) return DGPU_ERR_ARG;

@@ -71,6 +71,7 @@ SIGNATURES = {
     "dgpu_clip": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p]),
     "dgpu_cwm_filter": (c_int, [c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_int, c_void_p]),
     "dgpu_rect_lp_filter": (c_int, [c_void_p, c_int, c_int, c_int, ctypes.c_float, c_int, c_void_p, c_void_p]),
+    "dgpu_diag_lp_filter": (c_int, [c_void_p, c_int, c_int, c_int, ctypes.c_float, c_int, c_void_p, c_void_p]),
     "dgpu_motion_compensate": (
         c_int,
         [c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,

@@ -16,7 +16,7 @@
  *
  * Scratch passed as NULL: the entry points that take a scratch or workspace pointer
  * (dgpu_wavelet_transform[_batch], dgpu_motion_estimate[_batch], dgpu_code_residue_batch,
- * dgpu_rect_lp_filter) then use a buffer the library owns, one per (device, stream), grown
+ * dgpu_rect_lp_filter, dgpu_diag_lp_filter) then use a buffer the library owns, one per (device, stream), grown
  * with cudaMalloc on first use and on growth.  Calls on one stream are ordered by it, so they
  * may share that buffer; calls on the same stream issued from several host threads at once
  * race on it and must be serialised by the caller.  Calls on different streams use different
@@ -179,6 +179,19 @@ int dgpu_cwm_filter(const int16_t* in, int in_stride, int16_t* out, int out_stri
  * scratch: device w x h int16, or NULL for the library's own buffer.  DGPU_ERR_SIZE below
  * 17 x 17 (the reference's edge loops need 17 samples). */
 int dgpu_rect_lp_filter(int16_t* pic, int w, int h, int stride, float qf, int strength, int16_t* scratch,
+                        void* stream);
+
+/* DIAGLP residue prefilter of one component, in place: replaces DiagFilter
+ * (libdirac_encoder/prefilter.cpp:535-588, DiagFilterBchkD / DiagFilterD :307-392), which
+ * PictureCompressor::Prefilter applies to each component before the forward transform when
+ * DIAGLP is selected (picture_compress.cpp:340-355).  A 13 x 13 two-dimensional filter whose
+ * quadrant of taps comes from the reference's tables for the bandwidth the quality factor and
+ * strength give (GetDiagLPFilter, :395-530), mixed with a unit impulse; outputs
+ * (2^15 + sum) >> 16 as int16, source indices clamped to the component.  When that bandwidth
+ * is above 0.9 the reference leaves the component as it is, and so does this call.  scratch:
+ * device w x h int16, or NULL for the library's own buffer.  DGPU_ERR_SIZE below 7 x 7 (the
+ * reference's edge loops need 7 samples). */
+int dgpu_diag_lp_filter(int16_t* pic, int w, int h, int stride, float qf, int strength, int16_t* scratch,
                         void* stream);
 
 /* ---------------------------------------------------------------------------------------

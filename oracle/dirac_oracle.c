@@ -526,3 +526,114 @@ int orc_rect_lp_filter(int16_t* pic, int w, int h, float qf, int strength) {
     free(tmp);
     return 0;
 }
+
+/* DiagFilter (libdirac_encoder/prefilter.cpp:535-588), the DIAGLP residue prefilter: the taps
+ * quadrant of GetDiagLPFilter (:395-530) for the bandwidth, mixed with a unit impulse by the
+ * factor, then every output (2^15 + sum over the 13 x 13 neighbourhood) >> 16 as int16 with
+ * source indices clamped (DiagFilterBchkD, :307-354; DiagFilterD reads the same samples in
+ * the interior).  The expressions keep the reference's float / double mix.  In place; w, h >= 7;
+ * a bandwidth above 0.9 leaves the component unchanged. */
+static const int diag_tables[8][7][7] = {
+    {  // bandwidth 0.2
+        {  2855,   2540,   1775,    947,    364,     89,     10},
+        {  2540,   2251,   1551,    804,    290,     59,      1},
+        {  1775,   1551,   1020,    475,    130,      3,    -10},
+        {   947,    804,    475,    165,      5,    -22,     -6},
+        {   364,    290,    130,      5,    -28,    -10,      0},
+        {    89,     59,      3,    -22,    -10,      0,      0},
+        {    10,      1,    -10,     -6,      0,      0,      0},
+    },
+    {  // bandwidth 0.3
+        {  5767,   4718,   2498,    745,     72,      5,     23},
+        {  4718,   3796,   1875,    423,    -58,    -41,      7},
+        {  2498,   1875,    643,   -146,   -241,    -88,     -9},
+        {   745,    423,   -146,   -367,   -220,    -51,     -2},
+        {    72,    -58,   -241,   -220,    -78,     -5,      0},
+        {     5,    -41,    -88,    -51,     -5,      0,      0},
+        {    23,      7,     -9,     -2,      0,      0,      0},
+    },
+    {  // bandwidth 0.4
+        { 10534,   7642,   2603,    194,     56,    120,     28},
+        {  7642,   5237,   1218,   -383,   -153,     40,      2},
+        {  2603,   1218,   -771,   -958,   -269,     -3,     -7},
+        {   194,   -383,   -958,   -541,    -18,     48,      4},
+        {    56,   -153,   -269,    -18,     96,     22,      0},
+        {   120,     40,     -3,     48,     22,      0,      0},
+        {    28,      2,     -7,      4,      0,      0,      0},
+    },
+    {  // bandwidth 0.5
+        { 16421,  10159,   1716,     33,    325,     57,      6},
+        { 10159,   5309,   -580,   -747,     44,    -43,    -25},
+        {  1716,   -580,  -2310,   -763,    100,    -19,    -12},
+        {    33,   -747,   -763,    308,    326,     27,      1},
+        {   325,     44,    100,    326,     84,    -14,      0},
+        {    57,    -43,    -19,     27,    -14,      0,      0},
+        {     6,    -25,    -12,      1,      0,      0,      0},
+    },
+    {  // bandwidth 0.6
+        { 23511,  11883,    566,    524,    231,     18,     41},
+        { 11883,   3647,  -2496,   -361,    -96,    -97,      1},
+        {   566,  -2496,  -2329,    459,    152,     -7,     18},
+        {   524,   -361,    459,    979,     33,    -28,      3},
+        {   231,    -96,    152,     33,   -184,    -15,      0},
+        {    18,    -97,     -7,    -28,    -15,      0,      0},
+        {    41,      1,     18,      3,      0,      0,      0},
+    },
+    {  // bandwidth 0.7
+        { 32188,  12652,      3,    921,      1,    128,      0},
+        { 12652,    295,  -3414,     -2,   -343,     -1,    -37},
+        {     3,  -3414,   -212,   1273,      1,     98,      0},
+        {   921,     -2,   1273,    110,   -363,      0,     -8},
+        {     1,   -343,      1,   -363,    -29,     29,      0},
+        {   128,     -1,     98,      0,     29,      0,      0},
+        {     0,    -37,      0,     -8,      0,      0,      0},
+    },
+    {  // bandwidth 0.8
+        { 41902,  12084,    435,    610,    188,     34,     37},
+        { 12084,  -4268,  -2715,   -286,   -144,    -84,     -2},
+        {   435,  -2715,   2809,    640,    127,     10,     17},
+        {   610,   -286,    640,  -1250,    -45,    -26,      2},
+        {   188,   -144,    127,    -45,    259,     -8,      0},
+        {    34,    -84,     10,    -26,     -8,      0,      0},
+        {    37,     -2,     17,      2,      0,      0,      0},
+    },
+    {  // bandwidth 0.9
+        { 53098,  10449,   1546,     73,    342,     38,     12},
+        { 10449,  -9060,   -873,   -727,     52,    -65,    -20},
+        {  1546,   -873,   4261,   -627,    137,    -27,     -7},
+        {    73,   -727,   -627,   -804,    328,     14,      2},
+        {   342,     52,    137,    328,    -83,    -20,      0},
+        {    38,    -65,    -27,     14,    -20,      0,      0},
+        {    12,    -20,     -7,      2,      0,      0,      0},
+    },
+};
+
+int orc_diag_lp_filter(int16_t* pic, int w, int h, float qf, int strength) {
+    if (!pic || w < 7 || h < 7) return -1;
+    const float ffactor = (8.0 + strength - 4.0 - qf) / 5.0;
+    int factor = (int)(ffactor * 256.0);
+    factor = factor < 0 ? 0 : (factor > 256 ? 256 : factor);
+    const float bw = (1.0 - ffactor) * 0.6 + 0.4;
+    if (bw > 0.9) return 0;
+    int qbf = (int)(bw * 10.0 + 0.5);
+    qbf = qbf < 2 ? 2 : (qbf > 10 ? 10 : qbf);
+    int f[7][7];
+    for (int j = 0; j < 7; ++j)
+        for (int i = 0; i < 7; ++i) f[j][i] = qbf == 10 ? (i == 0 && j == 0 ? 65536 : 0) : diag_tables[qbf - 2][j][i];
+    for (int j = 0; j < 7; ++j)
+        for (int i = 0; i < 7; ++i)
+            f[j][i] = (factor * f[j][i] + (j == 0 && i == 0 ? (256 - factor) * 65536 : 0) + 128) >> 8;
+    int16_t* src = (int16_t*)malloc(sizeof(int16_t) * (size_t)w * h);
+    if (!src) return -4;
+    memcpy(src, pic, sizeof(int16_t) * (size_t)w * h);
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            int val = 1 << 15;
+            for (int j = -6; j <= 6; ++j)
+                for (int i = -6; i <= 6; ++i)
+                    val += f[abs(j)][abs(i)] * src[(size_t)clampi(y + j, 0, h - 1) * w + clampi(x + i, 0, w - 1)];
+            pic[(size_t)y * w + x] = (int16_t)(val >> 16);
+        }
+    free(src);
+    return 0;
+}

@@ -110,6 +110,9 @@ int orc_cwm_filter(const int16_t* in, int16_t* out, int w, int h, int strength);
 /* LPFilter: the RECTLP residue prefilter of a dense w x h component, in place (w, h >= 17). */
 int orc_rect_lp_filter(int16_t* pic, int w, int h, float qf, int strength);
 
+/* DiagFilter: the DIAGLP residue prefilter of a dense w x h component, in place (w, h >= 7). */
+int orc_diag_lp_filter(int16_t* pic, int w, int h, float qf, int strength);
+
 /* Picture::ClipComponent: clamp to [-2^(d-1), 2^(d-1)-1]. */
 void orc_clip(int16_t* pic, size_t n, int bit_depth);
 

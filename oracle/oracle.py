@@ -76,6 +76,14 @@ class Oracle:
             raise ValueError("orc_rect_lp_filter failed")
         return p
 
+    def diag_lp_filter(self, pic, qf, strength):
+        """DiagFilter (DIAGLP) of a 2-D int16 component; returns the filtered copy."""
+        p = np.array(pic, dtype=np.int16, copy=True, order="C")
+        h, w = p.shape
+        if self.lib.orc_diag_lp_filter(_p(p), w, h, ctypes.c_float(qf), strength):
+            raise ValueError("orc_diag_lp_filter failed")
+        return p
+
     def cwm_filter(self, pic, strength):
         """CWMFilterComponent of a 2-D int16 component; returns the filtered copy."""
         p = np.ascontiguousarray(pic, dtype=np.int16)
@@ -253,6 +261,13 @@ class Reference:
         h, w = p.shape
         if self.lib.ref_lp_filter(_p(p), w, h, ctypes.c_float(qf), strength):
             raise ValueError("ref_lp_filter failed")
+        return p
+
+    def diag_lp_filter(self, pic, qf, strength):
+        p = np.array(pic, dtype=np.int16, copy=True, order="C")
+        h, w = p.shape
+        if self.lib.ref_diag_filter(_p(p), w, h, ctypes.c_float(qf), strength):
+            raise ValueError("ref_diag_filter failed")
         return p
 
     def cwm_filter(self, pic, strength):

@@ -517,4 +517,19 @@ int ref_lp_filter(short* pic, int w, int h, float qf, int strength) {
     }
 }
 
+// DiagFilter (the DIAGLP residue prefilter) on a dense w x h component, in place.
+int ref_diag_filter(short* pic, int w, int h, float qf, int strength) {
+    try {
+        PicArray a(h, w);
+        for (int y = 0; y < h; ++y)
+            for (int x = 0; x < w; ++x) a[y][x] = pic[y * w + x];
+        DiagFilter(a, qf, strength);
+        for (int y = 0; y < h; ++y)
+            for (int x = 0; x < w; ++x) pic[y * w + x] = a[y][x];
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
 }  // extern "C"

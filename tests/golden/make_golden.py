@@ -395,8 +395,16 @@ PREFILTER_CASES = [(64, 48, 0), (37, 23, 3), (48, 40, 5), (33, 17, 8), (40, 32, 
 RECTLP_CASES = [(48, 40, 7.0, 0), (17, 17, 2.0, 1), (33, 21, 10.0, 5), (64, 24, 0.5, 3), (40, 36, 12.0, 10)]
 
 
+# (width, height, quality factor, strength) of the DIAGLP cases: filter bandwidth indices 9 down
+# to 2 (the last clamped), partial and full blending factors, and one pair that leaves the
+# component alone (bandwidth above 0.9)
+DIAGLP_CASES = [(48, 40, 3.0, 0), (17, 17, 4.5, 2), (33, 21, 4.5, 3), (7, 7, 5.7, 5), (40, 36, 5.8, 6),
+                (29, 35, 6.2, 7), (64, 24, 7.2, 9), (23, 9, 6.0, 10), (31, 13, 7.0, 0)]
+
+
 def prefilter_cases(ref):
-    """CWMFilterComponent and LPFilter (RECTLP) of the reference on seeded components."""
+    """CWMFilterComponent, LPFilter (RECTLP) and DiagFilter (DIAGLP) of the reference on seeded
+    components."""
     out = {}
     for k, (w, h, strength) in enumerate(PREFILTER_CASES):
         rng = np.random.default_rng(500 + k)
@@ -408,6 +416,11 @@ def prefilter_cases(ref):
         pic = rng.integers(-300, 300, size=(h, w)).astype(np.int16)
         out[f"lp{k}_in"] = pic
         out[f"lp{k}_out"] = ref.rect_lp_filter(pic, qf, strength)
+    for k, (w, h, qf, strength) in enumerate(DIAGLP_CASES):
+        rng = np.random.default_rng(700 + k)
+        pic = rng.integers(-300, 300, size=(h, w)).astype(np.int16)
+        out[f"dg{k}_in"] = pic
+        out[f"dg{k}_out"] = ref.diag_lp_filter(pic, qf, strength)
     return out
 
 

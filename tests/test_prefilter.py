@@ -3,7 +3,9 @@ against the reference's CWMFilterComponent (tests/golden/prefilter.npz, and live
 oracle/_ref exists), and the CUDA kernel (dgpu_cwm_filter) against the oracle on every
 strength and on sizes that leave no, one or many filtered samples, up to a 1080p component.
 RECTLP low-pass: orc_rect_lp_filter against the reference's LPFilter, and the kernels
-(dgpu_rect_lp_filter) against the oracle over quality factors and strengths."""
+(dgpu_rect_lp_filter) against the oracle over quality factors and strengths.  DIAGLP low-pass:
+orc_diag_lp_filter against the reference's DiagFilter on every bandwidth table, and the kernel
+(dgpu_diag_lp_filter) against the oracle up to a 1080p component."""
 import os
 import sys
 
@@ -11,7 +13,7 @@ import numpy as np
 import pytest
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
-from make_golden import PREFILTER_CASES, RECTLP_CASES  # noqa: E402
+from make_golden import DIAGLP_CASES, PREFILTER_CASES, RECTLP_CASES  # noqa: E402
 
 
 @pytest.mark.parametrize("k", range(len(PREFILTER_CASES)))
@@ -102,3 +104,58 @@ def test_rect_lp_rejects_small_components():
     from dirac_b200 import _lib
 
     assert _lib.load().dgpu_rect_lp_filter(16, 16, 17, 16, 7.0, 0, None, None) == -2
+
+
+@pytest.mark.parametrize("k", range(len(DIAGLP_CASES)))
+def test_oracle_diag_lp_matches_reference_fixture(oracle, golden, k):
+    g = golden("prefilter.npz")
+    _, _, qf, strength = DIAGLP_CASES[k]
+    np.testing.assert_array_equal(oracle.diag_lp_filter(g[f"dg{k}_in"], qf, strength), g[f"dg{k}_out"])
+
+
+def test_oracle_diag_lp_matches_live_reference(oracle):
+    from oracle import Reference
+
+    if not Reference.available():
+        pytest.skip("reference library not built here")
+    ref = Reference()
+    rng = np.random.default_rng(16)
+    for w, h in [(7, 7), (20, 13), (48, 40)]:
+        for qf in (0.5, 3.0, 4.5, 5.7, 7.0, 10.0):
+            for strength in range(11):
+                pic = rng.integers(-512, 512, size=(h, w)).astype(np.int16)
+                np.testing.assert_array_equal(oracle.diag_lp_filter(pic, qf, strength),
+                                              ref.diag_lp_filter(pic, qf, strength))
+
+
+@pytest.mark.gpu
+def test_diag_lp_kernel_matches_oracle(gpu, oracle):
+    import torch
+
+    from dirac_b200.prefilter import diag_lp_filter
+
+    rng = np.random.default_rng(17)
+    cases = [(w, h, qf, s) for (w, h, qf, s) in DIAGLP_CASES]
+    cases += [(176, 144, 5.7, 5), (37, 300, 6.0, 10), (1920, 1080, 4.5, 3), (960, 540, 3.0, 0)]
+    for w, h, qf, strength in cases:
+        pic = rng.integers(-1024, 1024, size=(h, w)).astype(np.int16)
+        t = torch.from_numpy(pic).cuda()
+        diag_lp_filter(t, qf, strength)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(t.cpu().numpy(), oracle.diag_lp_filter(pic, qf, strength),
+                                      err_msg=f"{w}x{h} qf {qf} strength {strength}")
+    # a strided view: the kernel reads and writes through the row pitch
+    base = rng.integers(-1024, 1024, size=(64, 80)).astype(np.int16)
+    t = torch.from_numpy(base).cuda()
+    view = t[3:60, 5:70]
+    diag_lp_filter(view, 6.2, 7)
+    torch.cuda.synchronize()
+    want = base.copy()
+    want[3:60, 5:70] = oracle.diag_lp_filter(base[3:60, 5:70], 6.2, 7)
+    np.testing.assert_array_equal(t.cpu().numpy(), want)
+
+
+def test_diag_lp_rejects_small_components():
+    from dirac_b200 import _lib
+
+    assert _lib.load().dgpu_diag_lp_filter(16, 6, 17, 6, 7.0, 0, None, None) == -2
