@@ -505,12 +505,23 @@ __device__ __forceinline__ void stage_rect(int16_t* dst, const int16_t* __restri
 
 // A block staged in shared memory for the sub-pel search around its pel vector (mvx, mvy):
 // the block's picture samples and the upconverted reference window that every candidate
-// within +-(2^prec - 1) of (mvx, mvy) << prec reads (prec 1..3): up rows and columns
-// 2 (yp + mvy) - 2 .. 2 (yp + yl + mvy) and likewise for x, each coordinate clamped to the
-// array as up_at does, so reads need no clamping.
+// within +-((2 + SUB_EXTRA) 2^(prec-1) - 1) of (mvx, mvy) << prec reads (prec 1..3: the
+// refinement's own candidates, within +-(2^prec - 1), and most predictors): up rows
+// 2 (yp + mvy) - 2 - SUB_EXTRA .. 2 (yp + yl + mvy) + SUB_EXTRA and the same columns, each
+// coordinate clamped to the array as up_at does, so reads need no clamping.  The staged
+// columns start at the 8-sample boundary at or below the first one (16-byte loads) and a
+// row holds sub_win_pitch(xl) samples, a pitch of 16 words modulo 32 so that the two
+// half-warps of the fused passes (two block rows, two window rows apart) use disjoint banks.
+constexpr int SUB_EXTRA = 2;
+
+__host__ __device__ constexpr int sub_win_pitch(int xl) {
+    // at least 2 xl + 3 + 2 SUB_EXTRA columns plus up to 7 of alignment, = 16 modulo 32
+    return ((2 * xl + 3 + 2 * SUB_EXTRA + 7) + 15) / 32 * 32 + 16;
+}
+
 struct SubWin {
     int16_t* pic;  // xl * yl, raster order
-    int16_t* up;   // (2 yl + 3) rows x (2 xl + 3) columns
+    int16_t* up;   // (2 yl + 3 + 2 SUB_EXTRA) rows of ww samples
     int ww, wx0, wy0;
 };
 
@@ -531,14 +542,39 @@ __device__ __forceinline__ int win_pred(const SubWin& S, int x, int y, int mx, i
 
 __device__ __noinline__ void stage_subwin(SubWin& S, int16_t* mem, const int16_t* pic, int pw, const int16_t* up, int uw, int uh,
                              const Blim& b, short2 mv) {
+    const int lane = threadIdx.x & 31;
     S.pic = mem;
-    S.up = mem + b.xl * b.yl;
-    S.ww = 2 * b.xl + 3;
-    S.wx0 = 2 * (b.xp + mv.x) - 2;
-    S.wy0 = 2 * (b.yp + mv.y) - 2;
-    const int wh = 2 * b.yl + 3;
+    S.up = mem + ((b.xl * b.yl + 7) & ~7);
+    S.ww = sub_win_pitch(b.xl);
+    S.wx0 = (2 * (b.xp + mv.x) - 2 - SUB_EXTRA) & ~7;
+    S.wy0 = 2 * (b.yp + mv.y) - 2 - SUB_EXTRA;
+    const int wh = 2 * b.yl + 3 + 2 * SUB_EXTRA;
     stage_rect(S.pic, pic, pw, 1 << 30, b.xp, b.yp, b.xl, b.yl);
-    stage_rect(S.up, up, uw, uh, S.wx0, S.wy0, S.ww, wh);
+    const bool aligned = (uw & 7) == 0 && (reinterpret_cast<uintptr_t>(up) & 15) == 0;
+    if (aligned && S.wx0 >= 0 && S.wx0 + S.ww <= uw && S.wy0 >= 0 && S.wy0 + wh <= uh) {
+        // the window lies inside the plane: 16-byte loads, four per lane in flight
+        const int per_row = S.ww >> 3, n = per_row * wh;
+        for (int i0 = 0; i0 < n; i0 += 128) {
+            int4 v[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int i = i0 + 32 * k + lane;
+                if (i < n) {
+                    const int r = i / per_row, c = i - r * per_row;
+                    v[k] = __ldg(reinterpret_cast<const int4*>(up + (size_t)(S.wy0 + r) * uw + S.wx0) + c);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int i = i0 + 32 * k + lane;
+                if (i < n) reinterpret_cast<int4*>(S.up)[i] = v[k];
+            }
+        }
+    } else {
+        for (int r = 0; r < wh; ++r)
+            for (int c = lane; c < S.ww; c += 32)
+                S.up[r * S.ww + c] = __ldg(&up[(size_t)clampi(S.wy0 + r, 0, uh - 1) * uw + clampi(S.wx0 + c, 0, uw - 1)]);
+    }
     __syncwarp();
 }
 
@@ -1049,7 +1085,7 @@ __global__ void __launch_bounds__(ME_THREADS, 8) subpel_wavefront_kernel(const _
         } else {
             Cost3 pc{0.0f, 0.0f, 0.0f};
             // the predictor reads the staged window when it lies within the search range
-            const int reach = (1 << prec) - 1;
+            const int reach = (2 + SUB_EXTRA) * (1 << (prec - 1)) - 1;
             const bool pred_in_win = staged && abs(pred.x - (mv.x << prec)) <= reach &&
                                      abs(pred.y - (mv.y << prec)) <= reach;
             if (bl.xl > 0 && bl.yl > 0) count_ops(L.dbg.ops, (long long)(3 + interp_ops(prec)) * bl.xl * bl.yl);
@@ -1319,13 +1355,15 @@ __device__ __noinline__ float do_unit_decn(const ModeLaunch& L, const ModeJob& J
 }
 
 // Writes the decisions of one level's units over the superblock's 16 blocks
-// (ModeDecider::DoLevelDecn's propagation) and the superblock's split and cost.  Called by
-// thread 0 only, so that its release of the superblock's flag publishes every write.
+// (ModeDecider::DoLevelDecn's propagation) and the superblock's split and cost.  Called by a
+// whole warp: lanes 0-15 take one block each; the fence makes the writes visible device-wide
+// before the CTA barrier that precedes thread 0's release of the superblock's flag.
 __device__ void propagate_level(const ModeLaunch& L, const ModeJob& J, int xsb, int ysb, int level, float sb_cost) {
     const LevelData& lv = J.lev[level];
     const LevelData& bl = J.lev[2];
     const int span = 1 << (2 - level);
-    for (int t = 0; t < 16; ++t) {
+    const int t = threadIdx.x & 31;
+    if (t < 16) {
         const int v = (ysb << 2) + (t >> 2), u = (xsb << 2) + (t & 3);
         const int j = v / span, i = u / span;
         const size_t src = (size_t)j * lv.xnb + i, dst = (size_t)v * bl.xnb + u;
@@ -1334,9 +1372,13 @@ __device__ void propagate_level(const ModeLaunch& L, const ModeJob& J, int xsb, 
         bl.mv[0][dst] = __ldcg(&lv.mv[0][src]);
         if (J.nref > 1) bl.mv[1][dst] = __ldcg(&lv.mv[1][src]);
     }
-    const size_t sb = (size_t)ysb * J.xnsb + xsb;
-    J.sbcost[sb] = sb_cost;
-    J.split[sb] = (uint8_t)level;
+    if (t == 0) {
+        const size_t sb = (size_t)ysb * J.xnsb + xsb;
+        J.sbcost[sb] = sb_cost;
+        J.split[sb] = (uint8_t)level;
+    }
+    __threadfence();
+    __syncwarp();
 }
 
 // Level-2 decisions (every block: REF1 / REF2 / bi / intra) depend on nothing outside the block,
@@ -1392,20 +1434,23 @@ __global__ void __launch_bounds__(ME_THREADS, 5) mode_wavefront_kernel(const __g
         // few) are computed here too, also before the waits.
         {
             const LevelData& bk = J.lev[2];
-            if (threadIdx.x == 0) {
-                for (int r = 0; r < 2; ++r) {
-                    int n0 = 0;
-                    for (int t = 0; t < 16 && r < J.nref && n0 <= MAX_V0; ++t) {
-                        const short2 v =
-                            __ldcg(&bk.mv[r][(size_t)((ysb << 2) + (t >> 2)) * bk.xnb + (xsb << 2) + (t & 3)]);
-                        bool dup = false;
-                        for (int q = 0; q < n0 && q < MAX_V0; ++q) dup |= s_v0[r][q].x == v.x && s_v0[r][q].y == v.y;
-                        if (dup) continue;
-                        if (n0 < MAX_V0) s_v0[r][n0] = v;
-                        ++n0;
-                    }
-                    s_n0[r] = r < J.nref && n0 <= MAX_V0 ? n0 : 0;
-                }
+            if (warp == 0) {
+                // lanes 0-15: reference 1's block vectors in raster order, lanes 16-31:
+                // reference 2's; a lane keeps its vector when no earlier lane of its half has it
+                const int r = lane >> 4, t = lane & 15;
+                const bool valid = r < J.nref;
+                const short2 v = valid ? __ldcg(&bk.mv[r][(size_t)((ysb << 2) + (t >> 2)) * bk.xnb + (xsb << 2) +
+                                                       (t & 3)])
+                                       : make_short2(0, 0);
+                const unsigned long long key = ((unsigned long long)r << 32) |
+                                               ((unsigned)(uint16_t)v.x << 16) | (unsigned)(uint16_t)v.y;
+                const unsigned same = __match_any_sync(0xffffffffu, key);
+                const bool first = valid && (same & ((1u << lane) - 1)) == 0;
+                const unsigned half = r ? 0xffff0000u : 0x0000ffffu;
+                const unsigned firsts = __ballot_sync(0xffffffffu, first) & half;
+                const int n0 = __popc(firsts);
+                if (first && n0 <= MAX_V0) s_v0[r][__popc(firsts & ((1u << lane) - 1))] = v;
+                if (t == 0) s_n0[r] = valid && n0 <= MAX_V0 ? n0 : 0;
             }
             __syncthreads();
             const Blim bl0 = block_limits(L.lb[0], J.pw, J.ph, xsb, ysb);
@@ -1440,16 +1485,18 @@ __global__ void __launch_bounds__(ME_THREADS, 5) mode_wavefront_kernel(const __g
         }
         __syncthreads();
         float sb_cur = c2;
-        if (threadIdx.x == 0) {
+        if (warp == 0) {
             const float c1 = ((s_cost[0] + s_cost[1]) + s_cost[2]) + s_cost[3];
-            const size_t sb = (size_t)s;
-            J.split[sb] = 2;
-            J.sbcost[sb] = c2;
+            if (lane == 0) {
+                J.split[s] = 2;
+                J.sbcost[s] = c2;
+            }
             if (c1 <= c2) {
                 propagate_level(L, J, xsb, ysb, 1, c1);
                 sb_cur = c1;
             }
-            s_cost[0] = sb_cur;
+            __syncwarp();
+            if (lane == 0) s_cost[0] = sb_cur;
         }
         __syncthreads();
         sb_cur = s_cost[0];
@@ -1543,7 +1590,7 @@ __global__ void __launch_bounds__(ME_THREADS, 5) mode_wavefront_kernel(const __g
             }
             if (warp == 0) {
                 const float c0 = do_unit_decn(L, J, xsb, ysb, 0, bsad);
-                if (lane == 0 && c0 <= sb_cur) propagate_level(L, J, xsb, ysb, 0, c0);
+                if (c0 <= sb_cur) propagate_level(L, J, xsb, ysb, 0, c0);
             }
         }
         __syncthreads();
@@ -2233,7 +2280,8 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
             S.wave.T = (g.xnb[0] - 1) + 2 * (g.ynb[0] - 1) + 1;
             // per-warp staging of the block and its window when it fits a modest budget
             const int xl = g.lb[2].xblen, yl = g.lb[2].yblen;
-            const int elems = (int)align_up((size_t)xl * yl + (size_t)(2 * xl + 3) * (2 * yl + 3), 8);
+            const int elems = (int)align_up(align_up((size_t)xl * yl, 8) +
+                                                (size_t)sub_win_pitch(xl) * (2 * yl + 3 + 2 * SUB_EXTRA), 8);
             S.win_elems = elems * 2 * WARPS_PER_CTA <= 24 * 1024 ? elems : 0;
             S.ticket = ctl;
             S.err = ctl + 1;
