@@ -35,60 +35,82 @@ class Request:
 
 class MeBatcher:
     """Motion estimation shared by the live streams of one picture format.  A stream thread that
-    has loaded new frames calls estimate(encoder) and blocks; the first caller of a round waits
-    `window` seconds for other streams to join, then estimates every joined encoder's estimable
-    pictures in one dgpu_encoders_estimate launch (their threads are all waiting, so no encoder
-    is in use elsewhere) and releases them.  The workspace grows to the largest round."""
+    has loaded new frames calls estimate(encoder) and blocks.  One waiting thread at a time leads:
+    it waits `window` seconds for other streams to join, then estimates the oldest joined
+    encoders' estimable pictures in one dgpu_encoders_estimate launch (their threads are all
+    waiting, so no encoder is in use elsewhere) and releases them, round after round until its
+    own encoder is done; then the lead passes to a waiting thread.  A round holds at most
+    max_batch encoders and at most ws_limit bytes of workspace (always at least one encoder);
+    the workspace grows to the largest round.  An error fails only the round it happened in."""
 
-    def __init__(self, window=0.002, max_batch=8):
-        import torch
-
-        from . import _lib
-
-        self.lib = _lib.load()
+    def __init__(self, window=0.002, max_batch=8, ws_limit=2 << 30):
+        self.lib = None        # library and stream made by the first round
+        self.stream = None
         self.window = window
         self.max_batch = max_batch
+        self.ws_limit = ws_limit
         self.cv = threading.Condition()
-        self.pending = []      # [encoder, done flag holder]
+        self.pending = []      # entries {"enc", "done", "error"} in arrival order
         self.leading = False
-        self.stream = torch.cuda.Stream()
         self.ws = None
         self.rounds = 0
         self.batched = 0       # encoders estimated, summed over rounds
         self.tasks = 0
-        self.error = None
 
     def estimate(self, enc):
-        entry = [enc, False]
+        entry = {"enc": enc, "done": False, "error": None}
         with self.cv:
             self.pending.append(entry)
-            while not entry[1]:
-                if not self.leading:
-                    self.leading = True
-                    break
+            while not entry["done"] and self.leading:
                 self.cv.wait()
-            if entry[1]:
-                if self.error:
-                    raise RuntimeError(self.error)
-                return
-        # leader: gather the round, estimate, release everyone in it
-        time.sleep(self.window)
-        with self.cv:
-            batch = self.pending[:self.max_batch]
-            self.pending = self.pending[self.max_batch:]
-        try:
-            self._run([e[0] for e in batch])
-        except Exception as ex:  # reported to every member of the round
-            self.error = repr(ex)
-        with self.cv:
-            for e in batch:
-                e[1] = True
-            self.leading = False
-            self.cv.notify_all()
-        if self.error:
-            raise RuntimeError(self.error)
-        if not entry[1]:  # the leader's own entry fell beyond max_batch: go round again
-            self.estimate(enc)
+            lead = not entry["done"]
+            if lead:
+                self.leading = True
+        if lead:
+            try:
+                while not entry["done"]:
+                    time.sleep(self.window)
+                    with self.cv:
+                        batch = self._take()
+                    try:
+                        self._run([e["enc"] for e in batch])
+                    except Exception as ex:  # reported to every member of this round
+                        for e in batch:
+                            e["error"] = repr(ex)
+                    with self.cv:
+                        for e in batch:
+                            e["done"] = True
+                        self.cv.notify_all()
+            finally:
+                with self.cv:
+                    if not entry["done"] and entry in self.pending:
+                        self.pending.remove(entry)
+                    self.leading = False
+                    self.cv.notify_all()
+        if entry["error"]:
+            raise RuntimeError(entry["error"])
+
+    def _load(self):
+        if self.lib is None:
+            from . import _lib
+
+            self.lib = _lib.load()
+        return self.lib
+
+    def _need(self, encs):
+        from . import _lib
+
+        return self._load().dgpu_encoder_group_device_bytes(_lib.ptr_array([e.handle.value for e in encs]), len(encs))
+
+    def _take(self):
+        """The oldest pending entries that fit max_batch and ws_limit (at least one); removed from
+        the pending list.  Called with the lock held."""
+        n = min(len(self.pending), self.max_batch)
+        while n > 1 and self._need([e["enc"] for e in self.pending[:n]]) > self.ws_limit:
+            n -= 1
+        batch = self.pending[:n]
+        del self.pending[:n]
+        return batch
 
     def _run(self, encs):
         import ctypes
@@ -97,11 +119,14 @@ class MeBatcher:
 
         from . import _lib
 
+        if self.stream is None:
+            self.stream = torch.cuda.Stream()
         handles = _lib.ptr_array([e.handle.value for e in encs])
-        need = self.lib.dgpu_encoder_group_device_bytes(handles, len(encs))
+        need = self._load().dgpu_encoder_group_device_bytes(handles, len(encs))
         if need == 0:
             raise ValueError("encoders of different formats in one estimation")
         if self.ws is None or self.ws.numel() < need:
+            self.ws = None
             self.ws = torch.empty(need, dtype=torch.uint8, device="cuda")
         n = ctypes.c_int(0)
         _lib.check(self.lib.dgpu_encoders_estimate(handles, len(encs), self.ws.data_ptr(), self.ws.numel(),

@@ -73,6 +73,85 @@ def test_request_larger_than_budget_is_refused():
         loop.run([Request({"bytes": 200}, [0, 1])])
 
 
+def _batcher_class():
+    from dirac_b200.serving import MeBatcher
+
+    class FakeBatcher(MeBatcher):
+        """Rounds recorded instead of launched; 100 bytes of workspace per encoder; a round that
+        holds `fail_on` fails."""
+
+        def __init__(self, fail_on=None, **kw):
+            super().__init__(**kw)
+            self.runs = []
+            self.fail_on = fail_on
+
+        def _need(self, encs):
+            return 100 * len(encs)
+
+        def _run(self, encs):
+            self.runs.append(list(encs))
+            time.sleep(0.001)
+            if self.fail_on in encs:
+                raise RuntimeError("estimation failed")
+
+    return FakeBatcher
+
+
+def _drive(batcher, nthreads, calls):
+    errors = [0] * nthreads
+
+    def worker(k):
+        for _ in range(calls):
+            try:
+                batcher.estimate(k)
+            except RuntimeError:
+                errors[k] += 1
+            time.sleep(0.0005 * (k % 3))
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(nthreads)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=60)
+    assert not any(t.is_alive() for t in threads), "a stream stayed blocked in estimate"
+    return errors
+
+
+def test_shared_estimation_rounds_cover_every_call_once():
+    """Every estimate call is served by exactly one round; no round holds an encoder twice or
+    more than max_batch encoders or ws_limit bytes; rounds do batch several streams."""
+    batcher = _batcher_class()(window=0.002, max_batch=4, ws_limit=300)
+    errors = _drive(batcher, 12, 6)
+    assert errors == [0] * 12
+    counts = {}
+    for r in batcher.runs:
+        assert len(r) == len(set(r)) and 1 <= len(r) <= 3, r
+        for k in r:
+            counts[k] = counts.get(k, 0) + 1
+    assert counts == {k: 6 for k in range(12)}
+    assert max(len(r) for r in batcher.runs) > 1
+    assert not batcher.pending and not batcher.leading
+
+
+def test_shared_estimation_error_fails_only_its_round():
+    """A failing round raises in the threads whose encoders it held, and only there; later
+    rounds run normally."""
+    batcher = _batcher_class()(fail_on=3, window=0.002, max_batch=4)
+    errors = _drive(batcher, 8, 5)
+    failed = [r for r in batcher.runs if 3 in r]
+    assert errors[3] == 5 and len(failed) == 5
+    for k in range(8):
+        assert errors[k] == sum(k in r for r in failed), (k, errors)
+    assert sum(len(r) for r in batcher.runs) == 40
+
+
+def test_shared_estimation_round_of_one_above_the_workspace_limit():
+    """An encoder whose workspace alone exceeds ws_limit is still estimated, in a round of one."""
+    batcher = _batcher_class()(window=0.001, max_batch=8, ws_limit=50)
+    assert _drive(batcher, 4, 3) == [0] * 4
+    assert all(len(r) == 1 for r in batcher.runs) and len(batcher.runs) == 12
+
+
 def test_encoder_device_bytes_grows_with_size_and_slots():
     from dirac_b200 import encoder as E
     from dirac_b200.serving import params_for
