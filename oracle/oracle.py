@@ -350,6 +350,24 @@ class Reference:
                 "cb_skip": cbs[:ncbt].copy(), "data": data[:int(nbytes.sum())].copy(), "band_bytes": nbytes,
                 "compress_bytes": whole}
 
+    def code_inter_indices_bytes(self, depth, idx, band_ncb):
+        """The reference's band coders on given signed indices of an inter component, every
+        quantiser at index 0 (factor 1); band_ncb: [nb][2] code blocks across and down.
+        Returns (data, band_bytes, cb_skip), data DC band first."""
+        q = np.ascontiguousarray(idx, dtype=np.int32)
+        ch, cw = q.shape
+        nb = 3 * depth + 1
+        ncb = np.ascontiguousarray(band_ncb, dtype=np.int32).reshape(-1)
+        cbs = np.zeros(int(np.sum(ncb[0::2] * ncb[1::2])), np.uint8)
+        cap = 8 * q.size + 4096
+        data = np.zeros(cap, np.uint8)
+        nbytes = np.zeros(nb, np.int32)
+        rc = self.lib.ref_code_inter_indices_bytes(depth, _p(q), cw, ch, _p(ncb), _p(cbs), _p(data),
+                                                   ctypes.c_longlong(cap), _p(nbytes))
+        if rc:
+            raise ValueError(f"ref_code_inter_indices_bytes failed: {rc}")
+        return data[:int(nbytes.sum())].copy(), nbytes, cbs
+
     def code_residue_bytes(self, cformat, w, h, comp, intra, filt, depth, coeff, lambda_, cpd_scale=1.0):
         """As code_residue, plus the reference band coders' output: "data" (every coded band's
         arithmetic-coded bytes, DC band first) and "band_bytes" (per band, 0 when skipped)."""

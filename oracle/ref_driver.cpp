@@ -467,6 +467,48 @@ int ref_code_residue(int cformat, int w, int h, int comp, int intra, int filter,
                              band_skip, band_wt, band_ecf, band_bits, band_ncb, cb_skip, nullptr, 0, nullptr);
 }
 
+// The reference's band coders (BandCodec, LFBandCodec; band_codec_template.h:24-200) on given
+// signed indices of an inter picture's component: every band and code block at quantiser index
+// 0, whose factor is 1 (CodeVal's abs << 2 / 4), so the coded values are the indices
+// themselves.  band_ncb: per band the code blocks across and down; a code block is skipped
+// when all its indices are zero (cb_skip receives the flags).  Coded data DC band first, as
+// ref_code_residue_bytes.
+int ref_code_inter_indices_bytes(int depth, const int* idx, int cw, int ch, const int* band_ncb,
+                                 unsigned char* cb_skip, unsigned char* band_data, long long cap, int* band_bytes) {
+    try {
+        CoeffArray c(ch, cw, Y_COMP);
+        fill_arr(c, idx);
+        SubbandList& bands = c.BandList();
+        bands.Init(depth, cw, ch);
+        size_t k = 0;
+        for (int b = 1; b <= bands.Length(); ++b) {
+            Subband& node = bands(b);
+            node.SetNumBlocks(band_ncb[2 * (b - 1) + 1], band_ncb[2 * (b - 1)]);
+            node.SetQuantIndex(0);
+            node.SetSkip(false);
+            node.SetUsingMultiQuants(false);
+            TwoDArray<CodeBlock>& cbs = node.GetCodeBlocks();
+            for (int j = 0; j < cbs.LengthY(); ++j)
+                for (int i = 0; i < cbs.LengthX(); ++i) {
+                    CodeBlock& blk = cbs[j][i];
+                    blk.SetQuantIndex(0);
+                    bool zero = true;
+                    for (int y = blk.Ystart(); y < blk.Yend() && zero; ++y)
+                        for (int x = blk.Xstart(); x < blk.Xend(); ++x)
+                            if (c[y][x] != 0) {
+                                zero = false;
+                                break;
+                            }
+                    blk.SetSkip(zero);
+                    cb_skip[k++] = zero ? 1 : 0;
+                }
+        }
+        return code_bands_capture(c, bands, false, band_data, cap, band_bytes);
+    } catch (...) {
+        return -1;
+    }
+}
+
 // As ref_code_residue, and each coded band's arithmetic-coded data captured (DC band first).
 int ref_code_residue_bytes(int cformat, int w, int h, int comp, int intra, int filter, int depth, int* coeff, int cw,
                            int ch, float lambda, float cpd_scale, int* band_qidx, int* band_skip, double* band_wt,

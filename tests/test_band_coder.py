@@ -31,6 +31,58 @@ def band_inputs(oracle, golden, k):
     return intra, depth, q, sk, cbs, qo, g
 
 
+def _adversarial_indices(kind, rng, cw=128, ch=96):
+    """Index arrays that stress the range coder: no symbols, long follow-bit codes, symbols near
+    even odds (long runs of deferred bits), isolated large values, whole zero code blocks."""
+    if kind == "zero":
+        return np.zeros((ch, cw), np.int32)
+    if kind == "huge":
+        return rng.integers(-(1 << 20), 1 << 20, size=(ch, cw)).astype(np.int32)
+    if kind == "signs":
+        return rng.choice(np.array([-1, 1], np.int32), size=(ch, cw))
+    if kind == "even":
+        return rng.integers(-2, 3, size=(ch, cw)).astype(np.int32)
+    if kind == "sparse":
+        q = np.zeros((ch, cw), np.int32)
+        m = rng.random((ch, cw)) < 0.02
+        q[m] = (rng.geometric(0.05, size=int(m.sum())) * rng.choice([-1, 1], size=int(m.sum()))).astype(np.int32)
+        return q
+    if kind == "blocks":
+        q = rng.integers(-40, 41, size=(ch, cw)).astype(np.int32)
+        q[(np.arange(ch)[:, None] // 8 + np.arange(cw)[None, :] // 8) % 3 == 0] = 0
+        return q
+    if kind == "stripes":
+        q = np.zeros((ch, cw), np.int32)
+        q[::2, :] = np.where(np.arange(cw) % 2 == 0, 5, -5)
+        q[:, ::3] = -np.arange(ch)[:, None] % 7
+        return q
+    raise ValueError(kind)
+
+
+@pytest.mark.parametrize("kind", ["zero", "huge", "signs", "even", "sparse", "blocks", "stripes"])
+def test_band_coder_matches_reference_on_adversarial_indices(kind):
+    """The range coder's bytes equal the reference band coders' own on index arrays chosen to
+    stress it (the reference coding given indices at quantiser index 0, inter bands), with one
+    code block per band and with several, some skipped."""
+    from oracle import Reference
+
+    from dirac_b200.entropy import code_bands
+
+    if not Reference.available():
+        pytest.skip("reference library not built here")
+    ref = Reference()
+    depth = 4
+    rng = np.random.default_rng(sum(map(ord, kind)))
+    q = _adversarial_indices(kind, rng)
+    for ncb in (np.ones((3 * depth + 1, 2), np.int32),
+                np.array([[1, 1]] * 4 + [[2, 2]] * 3 + [[4, 3]] * 3 + [[3, 4]] * 3, np.int32)[::-1].copy()):
+        want, want_bytes, cbs = ref.code_inter_indices_bytes(depth, q, ncb)
+        bands = np.zeros((3 * depth + 1, 3), np.int32)
+        data, per = code_bands(0, depth, [q], [bands], [ncb], [cbs])
+        np.testing.assert_array_equal(per[0], want_bytes, err_msg=kind)
+        assert data.tobytes() == want.tobytes(), kind
+
+
 @pytest.mark.parametrize("k", range(len(BAND_CASES)))
 def test_band_data_matches_reference_fixture(oracle, golden, k):
     from dirac_b200.entropy import code_bands
