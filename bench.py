@@ -36,6 +36,7 @@ reference encoder itself (its public C API) on this host's cores.
 import argparse
 import json
 import os
+import resource
 
 import numpy as np
 import statistics
@@ -74,6 +75,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--frames", type=int, default=32)
     ap.add_argument("--streams", type=int, default=8, help="concurrent sequences per GPU (batched form)")
+    ap.add_argument("--me-occupancy", type=int, default=8,
+                    help="resident CTAs per SM of the motion-estimation wavefront kernels (1-8)")
     ap.add_argument("--me-groups", type=int, default=2,
                     help="encoder groups the batched form's sequences are split into (run concurrently)")
     ap.add_argument("--serving-rate", type=float, default=40.0, help="stream arrivals per second (Poisson)")
@@ -684,6 +687,7 @@ def main():
             self.d2h = 0
             self.coded_bytes = 0
             self.ec = None
+            self.phases = dict.fromkeys(("prepare", "code_host", "finish", "read", "pictures"), 0)
 
         def read(self, info):
             """The coded picture's results the host coder needs, into page-locked buffers
@@ -726,15 +730,26 @@ def main():
                 self.load(src)
             self.ec = EntropyCorrector(depth)
             pending = None
+            ph = self.phases
             while True:
+                t0 = time.perf_counter()
                 nxt = enc.prepare_next()
+                t1 = time.perf_counter()
                 if pending is not None:
                     self.code_host(*pending)
                     pending = None
+                t2 = time.perf_counter()
+                ph["prepare"] += t1 - t0
+                ph["code_host"] += t2 - t1
                 if nxt is None:
                     return
                 info = enc.finish_next(ecf_state=self.ec.state)
+                t3 = time.perf_counter()
                 pending = (info, self.read(info))
+                t4 = time.perf_counter()
+                ph["finish"] += t3 - t2
+                ph["read"] += t4 - t3
+                ph["pictures"] += 1
                 if outputs is not None:
                     outputs[info["pnum"]] = [enc.read(info["pnum"], E.OUTPUT, c) for c in range(3)]
 
@@ -779,6 +794,8 @@ def main():
             pools[key] = ThreadPoolExecutor(n)
         return pools[key]
 
+    group_phases = {}  # host seconds per phase, summed over the groups of the last timed() run
+
     def timed(lanes, src, steps, with_read=False, groups=None, adaptive=False):
         """Device time (ms) of `steps` sequence encodes on every lane, the lanes running
         concurrently: a start event on the main stream that every lane stream waits on, and an
@@ -790,12 +807,14 @@ def main():
         main = torch.cuda.current_stream()
         torch.cuda.synchronize()
         barrier()
+        group_phases.clear()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(main)
         for ln in lanes:
             ln.stream.wait_event(e0)
             ln.d2h = 0
             ln.coded_bytes = 0
+            ln.phases = dict.fromkeys(ln.phases, 0)
 
         def code(ln, loaded):
             if adaptive:
@@ -811,9 +830,15 @@ def main():
             g, gl = groups[gi]
             ex = pool(("group", gi, len(gl)), len(gl))
             for _ in range(steps):
+                t0 = time.perf_counter()
                 list(ex.map(lambda ln: ln.load(src), gl))
+                t1 = time.perf_counter()
                 g.estimate()
+                t2 = time.perf_counter()
                 list(ex.map(lambda ln: code(ln, True), gl))
+                t3 = time.perf_counter()
+                for k, dt in (("load", t1 - t0), ("estimate", t2 - t1), ("code", t3 - t2)):
+                    group_phases[k] = group_phases.get(k, 0.0) + dt
 
         if groups is not None:
             list(pool(("groups", len(groups)), len(groups)).map(run_group, range(len(groups))))
@@ -830,6 +855,8 @@ def main():
         barrier()
         return max_over_ranks(e0.elapsed_time(e1))
 
+    if lib.dgpu_me_set_occupancy(args.me_occupancy):
+        raise ValueError("--me-occupancy must be 1..8")
     lanes = [Lane() for _ in range(args.streams)]
     plain = lanes[0]
     # the batched form: the lanes split into --me-groups encoder groups that run concurrently
@@ -878,13 +905,22 @@ def main():
     # and motion data out; every picture's subbands arithmetic-coded on the host and the
     # entropy-correction state adapted from the byte counts, so the quantiser choices are the
     # stock reference encoder's
+    ru0, w0 = resource.getrusage(resource.RUSAGE_SELF), time.perf_counter()
     ems = timed(lanes, pinned_np, args.steps, groups=groups, adaptive=True)
+    ru1, w1 = resource.getrusage(resource.RUSAGE_SELF), time.perf_counter()
+    cpu_s = (ru1.ru_utime - ru0.ru_utime) + (ru1.ru_stime - ru0.ru_stime)
     h2d = sum(p.nbytes for fr in pinned_np for p in fr) * len(lanes)
     e2e = {"value": whole_job_rate(world, frames_per_step, args.steps, ems), "unit": "frames/s",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": sum(ln.d2h for ln in lanes) // args.steps,
            "coded_band_bytes_per_step": sum(ln.coded_bytes for ln in lanes) // args.steps,
            "form": "stock choices: adaptive entropy-correction factors, subbands arithmetic-coded on the host "
-                   "(picture n coded while the device prepares n + 1)"}
+                   "(picture n coded while the device prepares n + 1)",
+           "lane_ms_per_picture": {k: round(1000.0 * sum(ln.phases[k] for ln in lanes) /
+                                            max(1, sum(ln.phases["pictures"] for ln in lanes)), 3)
+                                   for k in ("prepare", "code_host", "finish", "read")},
+           "group_ms_per_step": {k: round(1000.0 * v / (args.steps * len(groups)), 2) for k, v in group_phases.items()},
+           "host_cpu": {"cores_busy": round(cpu_s / (w1 - w0), 2), "cores": os.cpu_count(),
+                        "ms_per_picture": round(1000.0 * cpu_s / (frames_per_step * args.steps), 3)}}
     # the same without host coding (initial factors kept): the hot path alone through the ABI
     hms = timed(lanes, pinned_np, args.steps, with_read=True, groups=groups)
     e2e_hot = {"value": whole_job_rate(world, frames_per_step, args.steps, hms), "unit": "frames/s",
@@ -1033,6 +1069,7 @@ def main():
                            "form": f"batched: {len(lanes)} sequences per GPU in {len(groups)} encoder groups "
                                    "running concurrently; each group's motion estimation in one batched launch, "
                                    "each sequence's coding on its own stream and host thread",
+                           "me_ctas_per_sm": args.me_occupancy,
                            "l2": "inputs and working set larger than L2 (no flush needed)"},
                 "e2e": e2e, "cpu_baseline": cpu_baseline, "parity_vs_reference": parity, "plain": plain_line,
                 "gpu_launches": launches, "clocks": clk, "e2e_hot_path": e2e_hot, "roofline": roofline,

@@ -35,6 +35,7 @@
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <atomic>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -2001,6 +2002,31 @@ int pel_smem_setup() {
     return DGPU_OK;
 }
 
+// Resident CTAs per SM of the persistent wavefront kernels (dgpu_me_set_occupancy): at 8 a
+// launch holds every register of every SM until its last unit is done; fewer leave room on
+// each SM for other streams' kernels.  Any number is free of deadlock: a CTA waits only on
+// units whose tickets were taken before its own, by CTAs already resident.
+std::atomic<int> g_wave_ctas_per_sm{8};
+
+int wave_grid(int ctas_needed) {
+    static std::atomic<int> sms[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        dev = 0;
+    }
+    std::atomic<int>& n = sms[dev & 63];
+    if (n.load() <= 0) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
+            cudaGetLastError();
+            v = 148;
+        }
+        n.store(v);
+    }
+    return std::max(1, std::min(ctas_needed, n.load() * g_wave_ctas_per_sm.load()));
+}
+
 // Process-wide settings of dgpu_debug_wavefront, read once by each motion-estimation call.
 struct DebugSettings {
     int skip_unit = -1;
@@ -2191,7 +2217,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
         L.err = ctl + 1;
         DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
         tm.start(2);
-        pel_wavefront_kernel<<<std::min((L.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, 148 * 8), ME_THREADS, smem,
+        pel_wavefront_kernel<<<wave_grid((L.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA), ME_THREADS, smem,
                                st>>>(L);
         tm.stop();
         DGPU_CHECK_LAUNCH();
@@ -2286,7 +2312,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
             S.ticket = ctl;
             S.err = ctl + 1;
             DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
-            const int grid = std::min((S.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA, 148 * 8);
+            const int grid = wave_grid((S.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA);
             tm.start(3);
             subpel_wavefront_kernel<<<grid, ME_THREADS, (size_t)S.win_elems * 2 * WARPS_PER_CTA, st>>>(S);
             tm.stop();
@@ -2377,7 +2403,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                 M.ticket = ctl;
                 M.err = ctl + 1;
                 DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
-                const int grid = std::min(M.total, 148 * 8);
+                const int grid = wave_grid(M.total);
                 tm.start(5);
                 mode_wavefront_kernel<<<grid, ME_THREADS, 0, st>>>(M);
                 tm.stop();
@@ -2445,6 +2471,12 @@ extern "C" int dgpu_me_profile(int enable, double* kernel_ms, int* launches) {
         g_me_prof.launches[k] = 0;
     }
     g_me_prof.on = enable != 0;
+    return DGPU_OK;
+}
+
+extern "C" int dgpu_me_set_occupancy(int ctas_per_sm) {
+    if (ctas_per_sm < 1 || ctas_per_sm > 8) return DGPU_ERR_ARG;
+    g_wave_ctas_per_sm.store(ctas_per_sm);
     return DGPU_OK;
 }
 

@@ -286,6 +286,13 @@ int dgpu_motion_estimate(int cformat, int w, int h, const dgpu_block_params* bp,
 #define DGPU_ME_NKERNELS 7
 int dgpu_me_profile(int enable, double* kernel_ms, int* launches);
 
+/* Resident CTAs per SM (1..8, default 8) of the persistent motion-estimation wavefront
+ * kernels (pel search, sub-pel refinement, mode decision), process-wide, read by later
+ * estimation calls.  At 8 a wavefront launch occupies every SM's registers until it ends, so
+ * work on other streams (another encoder's coding) waits for it; fewer leave room for that
+ * work on every SM.  Results do not depend on it.  No counterpart in the reference. */
+int dgpu_me_set_occupancy(int ctas_per_sm);
+
 /* Failure-detection and ordering checks of the motion-estimation wavefronts.  No counterpart
  * in the reference, whose search is sequential.  Process-wide settings, read by every later
  * dgpu_motion_estimate[_batch] call (and the encoders' estimation) until changed; set them

@@ -125,3 +125,29 @@ def test_wavefront_decision_order_respects_raster_dependencies(gpu, oracle):
     for name, arr, shape, deps in (("pel", a[0], (ynb, xnb), PEL_DEPS), ("subpel", a[1], (ynb, xnb), SUBPEL_DEPS),
                                    ("mode", a[2], (bp.ynum_sb, bp.xnum_sb), MODE_DEPS)):
         assert order_violations(arr[1:].reshape(shape), deps) == [], name
+
+
+@pytest.mark.gpu
+def test_estimates_do_not_depend_on_wavefront_occupancy(gpu, oracle):
+    """dgpu_me_set_occupancy changes only how many CTAs of a wavefront launch stay resident per
+    SM (down to one, where most units wait for tickets held by other SMs' CTAs): the results
+    equal the oracle's at every setting."""
+    lib = gpu.load()
+    f = _frames()
+    want = oracle.motion_estimate(2, f[1], f[0], f[2], _bp(), 10.0, 3)
+    try:
+        for occ in (1, 3, 8):
+            assert lib.dgpu_me_set_occupancy(occ) == 0
+            got = _estimate(gpu, f, 3)
+            for k, v in want.items():
+                np.testing.assert_array_equal(got[k], v, err_msg=f"{k} at {occ} CTAs per SM")
+    finally:
+        assert lib.dgpu_me_set_occupancy(8) == 0
+
+
+def test_wavefront_occupancy_rejects_out_of_range_values():
+    from dirac_b200 import _lib
+
+    lib = _lib.load()
+    assert lib.dgpu_me_set_occupancy(0) == -1 and lib.dgpu_me_set_occupancy(9) == -1
+    assert lib.dgpu_me_set_occupancy(8) == 0
