@@ -74,10 +74,10 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--frames", type=int, default=32)
-    ap.add_argument("--streams", type=int, default=8, help="concurrent sequences per GPU (batched form)")
+    ap.add_argument("--streams", type=int, default=12, help="concurrent sequences per GPU (batched form)")
     ap.add_argument("--me-occupancy", type=int, default=8,
                     help="resident CTAs per SM of the motion-estimation wavefront kernels (1-8)")
-    ap.add_argument("--me-groups", type=int, default=2,
+    ap.add_argument("--me-groups", type=int, default=3,
                     help="encoder groups the batched form's sequences are split into (run concurrently)")
     ap.add_argument("--serving-rate", type=float, default=40.0, help="stream arrivals per second (Poisson)")
     ap.add_argument("--serving-seconds", type=float, default=6.0,
@@ -659,8 +659,7 @@ def main():
 
     import dirac_b200
     from dirac_b200 import encoder as E
-    from dirac_b200 import quant
-    from dirac_b200.entropy import EntropyCorrector, code_bands
+    from dirac_b200.adaptive import AdaptiveCoder
     from dirac_b200.roofline import stage_bytes
 
     lib = dirac_b200.load()
@@ -668,13 +667,7 @@ def main():
     pinned = [tuple(torch.from_numpy(p).pin_memory() for p in fr) for fr in frames]
     pinned_np = [tuple(t.numpy() for t in fr) for fr in pinned]
     torch.cuda.synchronize()
-    items = [(E.QINDEX, c) for c in range(3)] + [(E.BANDS, c) for c in range(3)] + \
-            [(E.CBSKIP, c) for c in range(3)] + [(E.MV, 0), (E.MODE, 0), (E.DC, 0), (E.SPLIT, 0)]
-    depth = PARAMS["wlt_depth"]
-    ncb = quant.code_blocks(depth, PARAMS["width"], PARAMS["height"])
-    mul = 1 << depth
-    qshapes = [(((PARAMS["height"] >> (c > 0)) + mul - 1) // mul * mul,
-                ((PARAMS["width"] >> (c > 0)) + mul - 1) // mul * mul) for c in range(3)]
+    from dirac_b200.adaptive import CODED_ITEMS as items
 
     class Lane:
         """One sequence encoder on its own CUDA stream (the batched form runs several, each
@@ -685,9 +678,8 @@ def main():
             self.enc = E.SequenceEncoder(PARAMS, max_pictures=args.frames, stream=self.stream)
             self.bufs = {}
             self.d2h = 0
-            self.coded_bytes = 0
-            self.ec = None
-            self.phases = dict.fromkeys(("prepare", "code_host", "finish", "read", "pictures"), 0)
+            self.coder = AdaptiveCoder(self.enc, PARAMS)
+            self.pictures = 0
 
         def read(self, info):
             """The coded picture's results the host coder needs, into page-locked buffers
@@ -708,50 +700,18 @@ def main():
                 got[(what, c)] = b.numpy()
             return got
 
-        def code_host(self, info, got):
-            """Arithmetic-codes the picture's subbands on the library's host threads (the
-            reference's band coders' bytes) and adapts the lane's entropy-correction state from
-            the byte counts, as the stock reference encoder does after each component."""
-            q = [got[(E.QINDEX, c)].view(np.int32).reshape(qshapes[c]) for c in range(3)]
-            bands = [got[(E.BANDS, c)].view(np.int32).reshape(-1, 3) for c in range(3)]
-            cbs = [got[(E.CBSKIP, c)] for c in range(3)]
-            data, per = code_bands([info["intra"]] * 3, [depth] * 3, q, bands, [ncb] * 3, cbs)
-            self.coded_bytes += int(data.size)
-            for c in range(3):
-                self.ec.update(info["intra"], info["is_b"], c, bands[c][:, 1], bands[c][:, 2], per[c])
-
         def step_adaptive(self, src, loaded=False, outputs=None):
-            """The stock encoder's choices: each picture's quantisers chosen with the entropy-
-            correction state adapted from the previous pictures' coded bytes.  Picture n's bands
-            are coded on the host while the device prepares picture n + 1 (motion
-            compensation, forward transform)."""
-            enc = self.enc
+            """The stock encoder's choices (AdaptiveCoder): each picture's quantisers chosen with
+            the entropy-correction factors of its kind adapted from the coded bytes of the
+            pictures before it; a picture's bands are coded on a host thread while the pictures
+            after it that do not depend on them are finished on the device."""
             if not loaded:
                 self.load(src)
-            self.ec = EntropyCorrector(depth)
-            pending = None
-            ph = self.phases
-            while True:
-                t0 = time.perf_counter()
-                nxt = enc.prepare_next()
-                t1 = time.perf_counter()
-                if pending is not None:
-                    self.code_host(*pending)
-                    pending = None
-                t2 = time.perf_counter()
-                ph["prepare"] += t1 - t0
-                ph["code_host"] += t2 - t1
-                if nxt is None:
-                    return
-                info = enc.finish_next(ecf_state=self.ec.state)
-                t3 = time.perf_counter()
-                pending = (info, self.read(info))
-                t4 = time.perf_counter()
-                ph["finish"] += t3 - t2
-                ph["read"] += t4 - t3
-                ph["pictures"] += 1
-                if outputs is not None:
-                    outputs[info["pnum"]] = [enc.read(info["pnum"], E.OUTPUT, c) for c in range(3)]
+            infos, _, _ = self.coder.run_native(max_pictures=args.frames, keep_data=outputs is not None)
+            self.pictures += len(infos)
+            if outputs is not None:  # every picture keeps its slot: max_pictures = the sequence
+                for info in infos:
+                    outputs[info["pnum"]] = [self.enc.read(info["pnum"], E.OUTPUT, c) for c in range(3)]
 
         def load(self, src):
             enc = self.enc
@@ -813,8 +773,8 @@ def main():
         for ln in lanes:
             ln.stream.wait_event(e0)
             ln.d2h = 0
-            ln.coded_bytes = 0
-            ln.phases = dict.fromkeys(ln.phases, 0)
+            ln.pictures = 0
+            ln.coder.d2h_bytes = ln.coder.coded_bytes = 0
 
         def code(ln, loaded):
             if adaptive:
@@ -911,13 +871,12 @@ def main():
     cpu_s = (ru1.ru_utime - ru0.ru_utime) + (ru1.ru_stime - ru0.ru_stime)
     h2d = sum(p.nbytes for fr in pinned_np for p in fr) * len(lanes)
     e2e = {"value": whole_job_rate(world, frames_per_step, args.steps, ems), "unit": "frames/s",
-           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": sum(ln.d2h for ln in lanes) // args.steps,
-           "coded_band_bytes_per_step": sum(ln.coded_bytes for ln in lanes) // args.steps,
-           "form": "stock choices: adaptive entropy-correction factors, subbands arithmetic-coded on the host "
-                   "(picture n coded while the device prepares n + 1)",
-           "lane_ms_per_picture": {k: round(1000.0 * sum(ln.phases[k] for ln in lanes) /
-                                            max(1, sum(ln.phases["pictures"] for ln in lanes)), 3)
-                                   for k in ("prepare", "code_host", "finish", "read")},
+           "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": sum(ln.d2h + ln.coder.d2h_bytes for ln in lanes) // args.steps,
+           "coded_band_bytes_per_step": sum(ln.coder.coded_bytes for ln in lanes) // args.steps,
+           "form": "stock choices: adaptive entropy-correction factors, subbands arithmetic-coded on the host",
+           "pipeline": "dgpu_encoder_code_adaptive: a picture waits only for the host coding of the last "
+                       "picture of its kind (intra, B, other inter), whose factors it reads",
            "group_ms_per_step": {k: round(1000.0 * v / (args.steps * len(groups)), 2) for k, v in group_phases.items()},
            "host_cpu": {"cores_busy": round(cpu_s / (w1 - w0), 2), "cores": os.cpu_count(),
                         "ms_per_picture": round(1000.0 * cpu_s / (frames_per_step * args.steps), 3)}}

@@ -26,6 +26,8 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <memory>
+#include <future>
 #include <new>
 #include <vector>
 
@@ -171,9 +173,20 @@ struct Encoder {
     double stage_ms[DGPU_ENC_NSTAGES] = {};
     int stage_calls[DGPU_ENC_NSTAGES] = {};
 
+    // dgpu_encoder_code_adaptive: per picture kind (intra, B, other inter) page-locked copies
+    // of a finished picture's indices and motion data, and the event after their copies
+    uint8_t* kind_stage[3] = {};
+    size_t kind_stage_bytes[3] = {};
+    cudaEvent_t kind_ev[3] = {};
+    std::vector<uint8_t> adaptive_data;  // the last call's coded data, coding order
+
     ~Encoder() {
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
+        for (int k = 0; k < 3; ++k) {
+            if (kind_ev[k]) cudaEventDestroy(kind_ev[k]);
+            if (kind_stage[k]) cudaFreeHost(kind_stage[k]);
+        }
         if (arena) cudaFree(arena);
         if (h_counts) cudaFreeHost(h_counts);
     }
@@ -963,9 +976,10 @@ extern "C" size_t dgpu_encoder_item_bytes(void* enc, int pnum, int what, int com
 
 extern "C" int dgpu_encoder_read(void* enc, int pnum, int what, int comp, void* dst, size_t bytes, int on_host) {
     Encoder* E = static_cast<Encoder*>(enc);
-    if (!E || !dst) return DGPU_ERR_ARG;
+    if (!E || !dst || on_host < 0 || on_host > 2) return DGPU_ERR_ARG;
     const size_t need = dgpu_encoder_item_bytes(enc, pnum, what, comp);
     if (need == 0 || bytes != need) return DGPU_ERR_ARG;
+    if (on_host == 2 && what == DGPU_ENC_OUTPUT) return DGPU_ERR_ARG;  // staged through one buffer
     const Pic& p = E->pics[pnum];
     const Slot& s = E->slots[p.slot];
     if (what == DGPU_ENC_BANDS || what == DGPU_ENC_CBSKIP) {
@@ -1005,7 +1019,204 @@ extern "C" int dgpu_encoder_read(void* enc, int pnum, int what, int comp, void* 
         }
     }
     DGPU_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, E->st));
-    if (on_host) DGPU_CHECK_CUDA(cudaStreamSynchronize(E->st));
+    if (on_host == 1) DGPU_CHECK_CUDA(cudaStreamSynchronize(E->st));
+    return DGPU_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Stock-encoder coding with the host band coder, pipelined by picture kind
+// ---------------------------------------------------------------------------------------
+namespace dgpu {
+namespace {
+
+// One finished picture on its way through the host band coder.
+struct CodedPicture {
+    dgpu_picture_info info{};
+    std::vector<int> bands;        // [3][nb][3] quantiser index, skip, estimated bits
+    std::vector<uint8_t> cb_skip;  // [3][ncb_total]
+    std::vector<uint8_t> data;     // coded subbands (dgpu_code_bands_host's layout)
+    std::vector<int> band_bytes;   // [3][nb]
+};
+
+// Codes one picture's subbands from its page-locked indices and adapts its kind's factors.
+int code_picture(const Encoder& E, CodedPicture& C, const uint8_t* stage, float* ecf_state) {
+    const int nb = E.nb, depth = E.P.wlt_depth;
+    const int intra[3] = {C.info.intra, C.info.intra, C.info.intra}, dep[3] = {depth, depth, depth};
+    const int32_t* q[3];
+    size_t off = 0;
+    for (int c = 0; c < 3; ++c) {
+        q[c] = reinterpret_cast<const int32_t*>(stage + off);
+        off += (size_t)E.pw[c] * E.ph[c] * 4;
+    }
+    std::vector<int> ncb3(6 * nb), qidx(3 * nb), skip(3 * nb), est(3 * nb);
+    for (int c = 0; c < 3; ++c)
+        for (int b = 0; b < nb; ++b) {
+            ncb3[2 * (c * nb + b)] = E.ncb[2 * b];
+            ncb3[2 * (c * nb + b) + 1] = E.ncb[2 * b + 1];
+            qidx[c * nb + b] = C.bands[(size_t)(c * nb + b) * 3];
+            skip[c * nb + b] = C.bands[(size_t)(c * nb + b) * 3 + 1];
+            est[c * nb + b] = C.bands[(size_t)(c * nb + b) * 3 + 2];
+        }
+    C.band_bytes.assign(3 * nb, 0);
+    size_t cap = C.data.size() ? C.data.size() : (size_t)E.pw[0] * E.ph[0] / 4 + 4096;
+    for (;;) {
+        C.data.resize(cap);
+        const int rc = dgpu_code_bands_host(3, intra, dep, q, E.pw, E.ph, ncb3.data(), qidx.data(), skip.data(),
+                                            C.cb_skip.data(), C.data.data(), cap, C.band_bytes.data());
+        if (rc == DGPU_OK) break;
+        if (rc != DGPU_ERR_SIZE) return rc;
+        size_t need = 0;
+        for (int v : C.band_bytes) need += (size_t)v;
+        if (need <= cap) return DGPU_ERR_SIZE;
+        cap = need;
+    }
+    size_t used = 0;
+    for (int v : C.band_bytes) used += (size_t)v;
+    C.data.resize(used);
+    for (int c = 0; c < 3; ++c) {
+        const int rc = dgpu_entropy_update(depth, ecf_state, C.info.intra, C.info.is_b, c, skip.data() + c * nb,
+                                           est.data() + c * nb, C.band_bytes.data() + c * nb);
+        if (rc) return rc;
+    }
+    return DGPU_OK;
+}
+
+}  // namespace
+}  // namespace dgpu
+
+extern "C" int dgpu_encoder_code_adaptive(void* enc, float* ecf_state, int max_pictures, dgpu_picture_info* infos,
+                                          uint8_t* out, size_t out_cap, size_t* out_bytes, int* band_bytes,
+                                          size_t* d2h_bytes, int* npictures) {
+    Encoder* E = static_cast<Encoder*>(enc);
+    if (!E || !ecf_state || max_pictures < 0 || !npictures || !out_bytes) return DGPU_ERR_ARG;
+    if (E->failed) return E->failed;
+    *npictures = 0;
+    *out_bytes = 0;
+    if (d2h_bytes) *d2h_bytes = 0;
+    int dev = 0;
+    DGPU_CHECK_CUDA(cudaGetDevice(&dev));
+    const int nb = E->nb;
+    std::vector<std::unique_ptr<CodedPicture>> done;
+    std::future<int> last[3];
+    int rc = DGPU_OK;
+    size_t copied = 0;
+    for (;;) {
+        dgpu_picture_info nxt{};
+        int r = dgpu_encoder_prepare_next(enc, &nxt);
+        if (r <= 0) {
+            rc = r;
+            break;
+        }
+        if ((int)done.size() >= max_pictures) {
+            rc = DGPU_ERR_SIZE;
+            break;
+        }
+        // the stock encoder's factors and their updates are per picture kind: wait only for
+        // the coding of the last picture of this one's kind
+        const int kind = nxt.intra ? 0 : (nxt.is_b ? 1 : 2);
+        if (last[kind].valid() && (r = last[kind].get()) != DGPU_OK) {
+            rc = r;
+            break;
+        }
+        auto C = std::make_unique<CodedPicture>();
+        if ((r = dgpu_encoder_finish_next(enc, nullptr, ecf_state, &C->info)) < 0) {
+            rc = r;
+            break;
+        }
+        const int pn = C->info.pnum;
+        const Pic& p = E->pics[pn];
+        C->bands = p.bands;
+        C->cb_skip = p.cb_skip;
+        // indices and motion data into the kind's page-locked buffer, without waiting
+        const int items[] = {DGPU_ENC_QINDEX, DGPU_ENC_QINDEX, DGPU_ENC_QINDEX, DGPU_ENC_MV,
+                             DGPU_ENC_MODE, DGPU_ENC_DC, DGPU_ENC_SPLIT};
+        size_t need = 0;
+        for (int k = 0; k < 7; ++k) need += dgpu_encoder_item_bytes(enc, pn, items[k], k < 3 ? k : 0);
+        if (E->kind_stage_bytes[kind] < need) {
+            if (E->kind_stage[kind]) cudaFreeHost(E->kind_stage[kind]);
+            E->kind_stage[kind] = nullptr;
+            E->kind_stage_bytes[kind] = 0;
+            if (cudaHostAlloc(reinterpret_cast<void**>(&E->kind_stage[kind]), need, cudaHostAllocDefault) !=
+                cudaSuccess) {
+                cudaGetLastError();
+                rc = DGPU_ERR_NOMEM;
+                break;
+            }
+            E->kind_stage_bytes[kind] = need;
+        }
+        if (!E->kind_ev[kind] &&
+            cudaEventCreateWithFlags(&E->kind_ev[kind], cudaEventDisableTiming | cudaEventBlockingSync) !=
+                cudaSuccess) {
+            cudaGetLastError();
+            rc = DGPU_ERR_CUDA;
+            break;
+        }
+        size_t off = 0;
+        for (int k = 0; k < 7 && r >= 0; ++k) {
+            const size_t n = dgpu_encoder_item_bytes(enc, pn, items[k], k < 3 ? k : 0);
+            if (n == 0) continue;
+            r = dgpu_encoder_read(enc, pn, items[k], k < 3 ? k : 0, E->kind_stage[kind] + off, n, 2);
+            off += n;
+        }
+        if (r < 0) {
+            rc = r;
+            break;
+        }
+        copied += off;
+        if (cudaEventRecord(E->kind_ev[kind], E->st) != cudaSuccess) {
+            cudaGetLastError();
+            rc = DGPU_ERR_CUDA;
+            break;
+        }
+        CodedPicture* cp = C.get();
+        done.push_back(std::move(C));
+        const uint8_t* stage = E->kind_stage[kind];
+        const cudaEvent_t ev = E->kind_ev[kind];
+        last[kind] = std::async(std::launch::async, [E, cp, stage, ev, ecf_state, dev]() -> int {
+            try {
+                if (cudaSetDevice(dev) != cudaSuccess || cudaEventSynchronize(ev) != cudaSuccess) {
+                    cudaGetLastError();
+                    return DGPU_ERR_CUDA;
+                }
+                return code_picture(*E, *cp, stage, ecf_state);
+            } catch (const std::bad_alloc&) {
+                return DGPU_ERR_NOMEM;
+            }
+        });
+    }
+    for (auto& f : last)
+        if (f.valid()) {
+            const int r = f.get();
+            if (rc == DGPU_OK && r != DGPU_OK) rc = r;
+        }
+    if (rc < 0) return rc;
+    size_t at = 0;
+    for (const auto& C : done) at += C->data.size();
+    E->adaptive_data.resize(at);
+    at = 0;
+    for (size_t i = 0; i < done.size(); ++i) {
+        const CodedPicture& C = *done[i];
+        if (infos) infos[i] = C.info;
+        if (band_bytes) std::memcpy(band_bytes + i * 3 * nb, C.band_bytes.data(), sizeof(int) * 3 * nb);
+        if (!C.data.empty()) std::memcpy(E->adaptive_data.data() + at, C.data.data(), C.data.size());
+        at += C.data.size();
+    }
+    *npictures = (int)done.size();
+    *out_bytes = at;
+    if (d2h_bytes) *d2h_bytes = copied;
+    if (!out) return DGPU_OK;
+    if (at > out_cap) return DGPU_ERR_SIZE;
+    if (at) std::memcpy(out, E->adaptive_data.data(), at);
+    return DGPU_OK;
+}
+
+extern "C" int dgpu_encoder_adaptive_data(void* enc, uint8_t* out, size_t out_cap, size_t* out_bytes) {
+    Encoder* E = static_cast<Encoder*>(enc);
+    if (!E || !out_bytes) return DGPU_ERR_ARG;
+    *out_bytes = E->adaptive_data.size();
+    if (!out) return DGPU_OK;
+    if (E->adaptive_data.size() > out_cap) return DGPU_ERR_SIZE;
+    if (!E->adaptive_data.empty()) std::memcpy(out, E->adaptive_data.data(), E->adaptive_data.size());
     return DGPU_OK;
 }
 

@@ -115,6 +115,9 @@ SIGNATURES = {
     "dgpu_encoder_code_next_adaptive": (c_int, [c_void_p, c_void_p, c_void_p]),
     "dgpu_encoder_prepare_next": (c_int, [c_void_p, c_void_p]),
     "dgpu_encoder_finish_next": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "dgpu_encoder_code_adaptive": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_size_t, c_void_p,
+                                           c_void_p, c_void_p, c_void_p]),
+    "dgpu_encoder_adaptive_data": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p]),
     "dgpu_encoder_item_bytes": (c_size_t, [c_void_p, c_int, c_int, c_int]),
     "dgpu_encoder_read": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_size_t, c_int]),
     "dgpu_batch_device_bytes": (c_size_t, [c_int, c_void_p, c_void_p]),

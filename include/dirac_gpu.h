@@ -493,9 +493,12 @@ int dgpu_encoder_code_next_adaptive(void* encoder, const float* ecf_state, dgpu_
 int dgpu_encoder_prepare_next(void* encoder, dgpu_picture_info* info);
 int dgpu_encoder_finish_next(void* encoder, const float* ecf, const float* ecf_state, dgpu_picture_info* info);
 size_t dgpu_encoder_item_bytes(void* encoder, int pnum, int what, int comp);
-/* Copies one result of a coded picture to dst (host memory when on_host = 1, else device);
- * bytes must equal dgpu_encoder_item_bytes.  Synchronises the encoder's stream for host
- * copies. */
+/* Copies one result of a coded picture to dst; bytes must equal dgpu_encoder_item_bytes.
+ * on_host = 0: dst is device memory, the copy queued on the encoder's stream.  1: host
+ * memory, the encoder's stream synchronised.  2: page-locked host memory, the copy queued on
+ * the encoder's stream and not waited for: the data is there once that stream has reached an
+ * event the caller records after the call (DGPU_ENC_BANDS and DGPU_ENC_CBSKIP, kept on the
+ * host, are copied at once; DGPU_ENC_OUTPUT, staged through one buffer, is refused). */
 int dgpu_encoder_read(void* encoder, int pnum, int what, int comp, void* dst, size_t bytes, int on_host);
 
 /* ---------------------------------------------------------------------------------------
@@ -593,6 +596,28 @@ int dgpu_encoder_group_estimate(void* group, int* ntasks);
  * the estimation; none of the encoders may be used by another thread meanwhile. */
 int dgpu_encoders_estimate(void* const* encoders, int n, void* workspace, size_t ws_bytes, void* stream,
                            int* ntasks);
+
+/* Codes every picture the encoder has input for as the stock reference encoder does: each
+ * picture's subbands arithmetic-coded on the host (dgpu_code_bands_host) and its kind's
+ * entropy-correction factors in ecf_state (dgpu_entropy_init) adapted from the coded bytes
+ * (dgpu_entropy_update) before the next picture of that kind is quantised
+ * (SequenceCompressor::CompressNextPicture, seq_compress.cpp:194-499; EntropyCorrector,
+ * common.cpp:57-151).  The reference's factors and their updates are per picture kind
+ * (intra, B, other inter), so a picture waits only for the host coding of the last picture of
+ * its kind: the coding runs on host threads while the pictures after it are prepared and
+ * finished on the device, their indices and motion data copied to page-locked memory without
+ * a wait.  The results equal a serial loop of dgpu_encoder_code_next_adaptive and
+ * dgpu_code_bands_host.  At most max_pictures pictures (DGPU_ERR_SIZE beyond); per picture in
+ * coding order: infos (optional), band_bytes (optional, [3][3*depth+1] as
+ * dgpu_code_bands_host), its coded data in out (optional); out_bytes receives the data's total
+ * length.  The encoder keeps the data until its next such call: when out is smaller the call
+ * returns DGPU_ERR_SIZE after coding every picture, and dgpu_encoder_adaptive_data copies the
+ * data once the caller has room.  d2h_bytes (optional): the device-to-host bytes copied
+ * (indices and motion data); npictures: the count. */
+int dgpu_encoder_code_adaptive(void* encoder, float* ecf_state, int max_pictures, dgpu_picture_info* infos,
+                               uint8_t* out, size_t out_cap, size_t* out_bytes, int* band_bytes,
+                               size_t* d2h_bytes, int* npictures);
+int dgpu_encoder_adaptive_data(void* encoder, uint8_t* out, size_t out_cap, size_t* out_bytes);
 
 /* ---------------------------------------------------------------------------------------
  * Arithmetic coding of quantised subbands on the host, and entropy-correction factors.

@@ -161,3 +161,64 @@ def test_hd1080_with_host_coder_matches_stock_reference(gpu, golden):
     np.testing.assert_array_equal([ptype[i] for i in range(len(seq))], g["adaptive_ptype"])
     np.testing.assert_array_equal(crc, g["adaptive_crc"])
     np.testing.assert_array_equal(g["adaptive_crc"], g["adaptive_decode_crc"])
+
+
+def _pipelined_outputs(seq, cfg, native=False):
+    from dirac_b200 import encoder as E
+    from dirac_b200.adaptive import AdaptiveCoder
+    from dirac_b200.encoder import SequenceEncoder
+
+    enc = SequenceEncoder(cfg, max_pictures=len(seq))
+    for f in seq:
+        enc.load(f)
+    enc.end_sequence()
+    coder = AdaptiveCoder(enc, cfg)
+    outputs = {}
+    coded = {}
+
+    def fin(info):
+        outputs[info["pnum"]] = [enc.read(info["pnum"], E.OUTPUT, c) for c in range(3)]
+
+    def done(info, got, data, per):
+        coded[info["pnum"]] = (zlib.crc32(data.tobytes()), [int(x) for p in per for x in p])
+
+    if native:
+        # every picture keeps its slot (max_pictures = the sequence), so outputs are read after
+        infos, data, bb = coder.run_native(max_pictures=len(seq))
+        for info, d, b in zip(infos, data, bb):
+            fin(info)
+            coded[info["pnum"]] = (zlib.crc32(d.tobytes()), [int(x) for x in b.ravel()])
+    else:
+        infos = coder.run(on_finished=fin, on_coded=done)
+    coder.close()
+    enc.close()
+    crc = np.array([[zlib.crc32(np.ascontiguousarray(outputs[i][c]).tobytes()) for c in range(3)]
+                    for i in range(len(seq))], np.uint32)
+    return crc, infos, coded
+
+
+@pytest.mark.parametrize("case", [ENCODE_CASES[0], "hd1080"], ids=[ENCODE_CASES[0][0], "hd1080"])
+def test_kind_pipelined_coder_matches_stock_reference(gpu, golden, case):
+    """AdaptiveCoder: a picture waits only for the host coding of the last picture of its own
+    kind (the factors it reads), so host coding overlaps the device work of the pictures after
+    it.  Every locally decoded plane equals the stock reference encoder's, and the coded band
+    bytes equal the serial loop's (one picture coded and adapted before the next)."""
+    from test_encoder_gpu import encoder_params
+
+    if case == "hd1080":
+        from make_golden import hd_inputs
+
+        seq, rcfg = hd_inputs()
+        want = golden("hd1080.npz")["adaptive_crc"]
+    else:
+        seq, rcfg = encode_inputs(case)
+        want = golden("adaptive.npz")[case[0] + "_crc"]
+    cfg = encoder_params(rcfg)
+    crc, infos, coded = _pipelined_outputs(seq, cfg)
+    np.testing.assert_array_equal(crc, want)
+    assert sorted(coded) == sorted(i["pnum"] for i in infos) and len(coded) == len(seq)
+    # the library's own pipeline (dgpu_encoder_code_adaptive): same pictures, same coded bytes
+    ncrc, ninfos, ncoded = _pipelined_outputs(seq, cfg, native=True)
+    np.testing.assert_array_equal(ncrc, want)
+    assert [i["pnum"] for i in ninfos] == [i["pnum"] for i in infos]
+    assert ncoded == coded
