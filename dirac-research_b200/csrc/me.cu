@@ -1034,7 +1034,7 @@ __device__ __forceinline__ void eval_subpel_cand(const SubJob& J, const SubWin& 
     }
 }
 
-__global__ void __launch_bounds__(ME_THREADS, 8) subpel_wavefront_kernel(const __grid_constant__ SubLaunch L) {
+__global__ void __launch_bounds__(ME_THREADS, 4) subpel_wavefront_kernel(const __grid_constant__ SubLaunch L) {
     extern __shared__ __align__(16) int16_t sub_smem[];
     int16_t* const wmem = sub_smem + (size_t)(threadIdx.x >> 5) * L.win_elems;
     const int prec = L.prec;
