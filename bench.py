@@ -64,8 +64,10 @@ STREAMING_KERNELS = {"dwt_forward": "dwt_forward_fast_kernel / dwt_forward_level
 ME_CLASSES = {"pel_search": (1, 2), "subpel_refinement": (3,), "mode_decision": (4, 5)}
 ME_OP_INDEX = {"pel_search": 0, "subpel_refinement": 1, "mode_decision": 2}
 # DRAM bytes per algorithmic operation of each motion-estimation kernel, from one ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum over the launch's counted operations)
-ME_TRAFFIC_PER_OP = {}
+# (dram__bytes_read.sum + dram__bytes_write.sum over the launch's counted operations) of the
+# 13-frame encode leg: sub-pel refinement 207.08 MB read + 4.97 MB written over 4378228940
+# operations; the bench's launches are scaled from it by their operation counts
+ME_TRAFFIC_PER_OP = {"subpel_refinement": (207.08e6 + 4.97e6) / 4378228940}
 
 
 def parse_args():
@@ -973,6 +975,9 @@ def main():
     roofline = {"bound": "int", "kernel": d["kernels"], "achieved": d["achieved"], "peak": round(int_peak, 1),
                 "unit": "Gop/s", "frac": d["frac"],
                 "traffic": round(traffic * per_launch_ops) if traffic else None,
+                "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the 13-frame "
+                                  "encode leg (profiles/encoder_1080p13_dram_traffic.md), scaled to this launch by "
+                                  "its algorithmic operations" if traffic else None,
                 "peak_source": "dgpu_measure_int_rate: acc += |a - b| on every SM, 3 operations per term "
                                "(measured in this run)",
                 "algorithmic_ops": "3 per pixel of every block difference the reference's search evaluates, plus "
