@@ -1012,14 +1012,15 @@ def main():
 
         cfg = {"seconds": args.serving_seconds, "arrivals_per_s": args.serving_rate, "fps_per_stream": 50,
                "resolutions": "352x288, 720x576, 1280x720, 1920x1080, 3840x2160 (4:2:0, 8- or 10-bit)",
-               "frames_per_stream": "8-64", "budget_gb": 40,
+               "frames_per_stream": "8-64", "budget_gb": 96, "max_active": 48, "max_load": 16,
                "input": "per resolution and depth a pool of synthetic frames (16; 8 at 3840x2160), each stream "
                         "cycling through its pool from a random offset"}
         try:
             reqs = S.make_requests(args.serving_seconds, args.serving_rate, ["cif", "576", "720", "1080", "2160"], 8, 64,
                                    seed=7,
                                    depths=(8, 10))
-            serving = S.ServingLoop(int(40e9), max_active=16, frame_interval=1.0 / 50, batch_me=True).run(reqs)
+            serving = S.ServingLoop(int(96e9), max_active=48, frame_interval=1.0 / 50, batch_me=True,
+                                    max_load=16).run(reqs)
         except Exception as e:  # the serving leg must not cost the bench line; its failure is reported
             serving = {"error": repr(e)}
         serving["config"] = cfg

@@ -10,6 +10,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "libdiracgpu.so")
 
 DGPU_OK = 0
+DGPU_ERR_SIZE = -2
 ERRORS = {
     -1: "DGPU_ERR_ARG",
     -2: "DGPU_ERR_SIZE",

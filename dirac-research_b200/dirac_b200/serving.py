@@ -21,6 +21,8 @@ import statistics
 import threading
 import time
 
+from . import _lib
+
 
 class Request:
     """One stream: params (encoder parameter dict), frames (host sample planes per frame),
@@ -138,18 +140,21 @@ class MeBatcher:
 
 class ServingLoop:
     def __init__(self, budget_bytes, max_active=16, frame_interval=0.0, slots=24, collect=None,
-                 encoder_factory=None, bytes_fn=None, batch_me=False):
+                 encoder_factory=None, bytes_fn=None, batch_me=False, max_load=16):
         """budget_bytes: device memory the loop may give to encoders.  max_active: streams
         coded at once.  frame_interval: seconds between a stream's frames (0: all at arrival).
         slots: picture slots per encoder.  collect(request, encoder, info): called after each
         coded picture (e.g. to read results).  encoder_factory / bytes_fn: injectable for tests.
-        batch_me: share motion-estimation launches between the live streams of one format."""
+        batch_me: share motion-estimation launches between the live streams of one format.
+        max_load: frames a stream loads at most before each estimation round (all that are due,
+        when it runs behind)."""
         self.budget = budget_bytes
         self.max_active = max_active
         self.frame_interval = frame_interval
         self.slots = slots
         self.collect = collect
         self.batch_me = batch_me
+        self.max_load = max(1, max_load)
         self.batchers = {}
         self.warm = encoder_factory is None
         if encoder_factory is None:
@@ -215,13 +220,26 @@ class ServingLoop:
                         if self.collect is not None:
                             self.collect(r, enc, info)
 
-                for i, f in enumerate(r.frames):
+                i, nfr = 0, len(r.frames)
+                while i < nfr:
                     due = t0 + r.arrival + i * self.frame_interval
                     wait = due - time.perf_counter()
                     if wait > 0:
                         time.sleep(wait)
-                    avail[i] = max(due, t0 + r.arrival)
-                    enc.load(f)
+                    # every frame already due (a stream admitted late has many) goes in before
+                    # one estimation round, up to max_load and while the encoder has free slots
+                    now = time.perf_counter()
+                    k = 0
+                    while i < nfr and k < self.max_load and (k == 0 or t0 + r.arrival + i * self.frame_interval <= now):
+                        try:
+                            enc.load(r.frames[i])
+                        except _lib.DgpuError as e:
+                            if e.code != _lib.DGPU_ERR_SIZE or k == 0:
+                                raise
+                            break  # no free slot: code what is loaded first
+                        avail[i] = max(t0 + r.arrival + i * self.frame_interval, t0 + r.arrival)
+                        i += 1
+                        k += 1
                     if batcher is not None:
                         batcher.estimate(enc)
                     drain()
@@ -345,15 +363,17 @@ def main(argv=None):
     ap.add_argument("--depths", default="8", help="bit depths drawn per stream, e.g. 8,10")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--batch-me", type=int, default=1, help="1: streams of one format share estimation launches")
+    ap.add_argument("--max-load", type=int, default=16, help="frames a stream loads at most per estimation round")
     a = ap.parse_args(argv)
     lo, hi = (int(x) for x in a.frames.split("-"))
     reqs = make_requests(a.seconds, a.rate, a.resolutions.split(","), lo, hi, a.seed,
                          depths=[int(d) for d in a.depths.split(",")])
     loop = ServingLoop(int(a.budget_gb * 1e9), a.max_active, 1.0 / a.fps if a.fps > 0 else 0.0,
-                       batch_me=bool(a.batch_me))
+                       batch_me=bool(a.batch_me), max_load=a.max_load)
     stats = loop.run(reqs)
     stats["config"] = {"seconds": a.seconds, "rate": a.rate, "resolutions": a.resolutions, "frames": a.frames,
-                       "depths": a.depths, "fps": a.fps, "budget_gb": a.budget_gb, "batch_me": bool(a.batch_me)}
+                       "depths": a.depths, "fps": a.fps, "budget_gb": a.budget_gb, "batch_me": bool(a.batch_me),
+                       "max_active": a.max_active, "max_load": a.max_load}
     print(json.dumps(stats))
     return 0
 

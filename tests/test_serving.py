@@ -65,6 +65,38 @@ def test_admission_respects_budget_and_serves_everything():
     assert stats["latency_ms"]["p50"] > 0 and stats["latency_ms"]["p99"] >= stats["latency_ms"]["p50"]
 
 
+def test_frames_already_due_load_together_within_free_slots():
+    """A stream whose frames are all due when it starts loads several of them before each
+    coding pass (one estimation round for many pictures), stops at a refused load (no free
+    slot: DGPU_ERR_SIZE) and codes first; every picture is coded, in order."""
+    from dirac_b200 import _lib
+    from dirac_b200.serving import Request, ServingLoop
+
+    log = []
+
+    class SlotEncoder(FakeEncoder):
+        def load(self, frame):
+            if len(self.loaded) - self.next >= 3:
+                raise _lib.DgpuError(_lib.DGPU_ERR_SIZE, "dgpu_encoder_load")
+            log.append("L")
+            super().load(frame)
+
+        def code_next(self):
+            info = super().code_next()
+            if info is not None:
+                log.append("C")
+            return info
+
+    FakeEncoder.live = FakeEncoder.peak = 0
+    coded = []
+    loop = ServingLoop(budget_bytes=1000, max_active=1, frame_interval=0.0, encoder_factory=SlotEncoder,
+                       bytes_fn=lambda p, n: p["bytes"], collect=lambda r, e, i: coded.append(i["pnum"]))
+    loop.run([Request({"bytes": 100}, list(range(10)), name="late")])
+    assert coded == list(range(10))
+    runs = "".join(log).split("C")
+    assert max(len(x) for x in runs) == 3 and log.count("L") == 10
+
+
 def test_request_larger_than_budget_is_refused():
     from dirac_b200.serving import Request, ServingLoop
 
