@@ -54,8 +54,20 @@ struct McParams {
     int precision;
     int add_or_sub;            // 0 ADD, 1 SUBTRACT
     int ncomp;
+    // reference picture weights (PicturePredParams::Ref1Weight, Ref2Weight,
+    // PictureWeightsBits); wt_custom unless they are the defaults 1, 1, 1
+    int wt_custom, wt1, wt2, wt_bits, wt_bias;
     McComp comp[3];
 };
+
+// AdjustBlockByRefWeights (mot_comp.cpp:620-680) with custom weights, for one sample of a
+// predicted block: the reference scales its int16 block values by ref1 + ref2 weights (one
+// reference) or each by its own weight and adds them (two), then (v + bias) >> bits.
+__device__ __forceinline__ int ref_weighted(const McParams& P, int md, int p1, int p2) {
+    const int16_t v = md == 3 ? (int16_t)((int16_t)(p1 * P.wt1) + (int16_t)(p2 * P.wt2))
+                              : (int16_t)(p1 * (P.wt1 + P.wt2));
+    return (int16_t)((v + P.wt_bias) >> P.wt_bits);
+}
 
 // 1-D window value (CreateBlock) at position pos of a window of length len and
 // separation sep; cls 0 pads the leading ramp flat, 2 is the mirror of 0 (trailing flat).
@@ -275,14 +287,18 @@ __global__ void __launch_bounds__(MT_THREADS) obmc_kernel(const __grid_constant_
                     pred = pred_fast<PREC>((r ? C.up2 : C.up1) + base + u.delta[r], 2 * C.w, u.wts[r]);
                     if (u.mode == 3) {
                         const int p2 = pred_fast<PREC>(C.up2 + base + u.delta[1], 2 * C.w, u.wts[1]);
-                        pred = (int16_t)((pred + p2 + 1) >> 1);
+                        pred = P.wt_custom ? ref_weighted(P, 3, pred, p2) : (int16_t)((pred + p2 + 1) >> 1);
+                    } else if (P.wt_custom) {
+                        pred = ref_weighted(P, u.mode, pred, 0);
                     }
                 } else {
                     const short2 m = u.mode == 2 ? u.mv2 : u.mv1;
                     pred = pixel_pred<PREC>(u.mode == 2 ? C.up2 : C.up1, C.w, C.h, px, py, m.x, m.y);
                     if (u.mode == 3) {
                         const int p2 = pixel_pred<PREC>(C.up2, C.w, C.h, px, py, u.mv2.x, u.mv2.y);
-                        pred = (int16_t)((pred + p2 + 1) >> 1);
+                        pred = P.wt_custom ? ref_weighted(P, 3, pred, p2) : (int16_t)((pred + p2 + 1) >> 1);
+                    } else if (P.wt_custom) {
+                        pred = ref_weighted(P, u.mode, pred, 0);
                     }
                 }
                 acc = (int16_t)(acc + (int16_t)(pred * wgt));
@@ -319,7 +335,9 @@ __global__ void __launch_bounds__(MT_THREADS) obmc_kernel(const __grid_constant_
                 if (md == 3) {
                     const short2 m2 = mv2[b];
                     const int p2 = pixel_pred<PREC>(C.up2, C.w, C.h, px, py, m2.x >> C.xshift, m2.y >> C.yshift);
-                    pred = (int16_t)((pred + p2 + 1) >> 1);
+                    pred = P.wt_custom ? ref_weighted(P, 3, pred, p2) : (int16_t)((pred + p2 + 1) >> 1);
+                } else if (P.wt_custom) {
+                    pred = ref_weighted(P, md, pred, 0);
                 }
             }
             acc = (int16_t)(acc + (int16_t)(pred * wgt));
@@ -353,13 +371,14 @@ void launch_obmc(int tiles, const McParams& P, cudaStream_t st) {
 
 int mc_tile_variants() { return 3; }
 
-// dgpu_motion_compensate with a chosen tile height (variant indexes MC_ROWS).
-int motion_compensate_tiled(int variant, int add_or_sub, int cformat, int w, int h, const dgpu_block_params* bp,
-                            const int16_t* mv1, const int16_t* mv2, const uint8_t* mode, const int16_t* dc,
-                            const uint8_t* split, int16_t* const* pic, const int* pic_stride,
-                            const int16_t* const* ref1up, const int16_t* const* ref2up, int clip_luma_depth,
-                            int clip_chroma_depth, cudaStream_t st) {
+// dgpu_motion_compensate[_weighted] with a chosen tile height (variant indexes MC_ROWS).
+int motion_compensate_impl(int variant, int add_or_sub, int cformat, int w, int h, const dgpu_block_params* bp,
+                           const int16_t* mv1, const int16_t* mv2, const uint8_t* mode, const int16_t* dc,
+                           const uint8_t* split, int16_t* const* pic, const int* pic_stride,
+                           const int16_t* const* ref1up, const int16_t* const* ref2up, int clip_luma_depth,
+                           int clip_chroma_depth, int wt1, int wt2, int wt_bits, cudaStream_t st) {
     if (variant < 0 || variant >= 3) return DGPU_ERR_ARG;
+    if (wt_bits < 0 || wt_bits > 16) return DGPU_ERR_ARG;
     const int MTY = MC_ROWS[variant];
     if (!bp || !mv1 || !mode || !dc || !split || !pic || !pic_stride || !ref1up) return DGPU_ERR_ARG;
     if (add_or_sub != 0 && add_or_sub != 1) return DGPU_ERR_ARG;
@@ -382,6 +401,12 @@ int motion_compensate_tiled(int variant, int add_or_sub, int cformat, int w, int
     P.precision = bp->precision;
     P.add_or_sub = add_or_sub;
     P.ncomp = 3;
+    P.wt_custom = wt_bits != 1 || wt1 != 1 || wt2 != 1;  // PicturePredParams::CustomRefWeights
+    P.wt1 = wt1;
+    P.wt2 = wt2;
+    P.wt_bits = wt_bits;
+    P.wt_bias = 1;  // 2^(bits - 1), built as the reference builds it: 1 when bits is 0
+    for (int i = wt_bits - 1; i > 0; --i) P.wt_bias <<= 1;
     int tiles = 0;
     for (int c = 0; c < 3; ++c) {
         McComp& C = P.comp[c];
@@ -424,6 +449,15 @@ int motion_compensate_tiled(int variant, int add_or_sub, int cformat, int w, int
     return DGPU_OK;
 }
 
+int motion_compensate_tiled(int variant, int add_or_sub, int cformat, int w, int h, const dgpu_block_params* bp,
+                            const int16_t* mv1, const int16_t* mv2, const uint8_t* mode, const int16_t* dc,
+                            const uint8_t* split, int16_t* const* pic, const int* pic_stride,
+                            const int16_t* const* ref1up, const int16_t* const* ref2up, int clip_luma_depth,
+                            int clip_chroma_depth, cudaStream_t st) {
+    return motion_compensate_impl(variant, add_or_sub, cformat, w, h, bp, mv1, mv2, mode, dc, split, pic, pic_stride,
+                                  ref1up, ref2up, clip_luma_depth, clip_chroma_depth, 1, 1, 1, st);
+}
+
 }  // namespace dgpu
 
 extern "C" int dgpu_motion_compensate(int add_or_sub, int cformat, int w, int h, const dgpu_block_params* bp,
@@ -434,4 +468,16 @@ extern "C" int dgpu_motion_compensate(int add_or_sub, int cformat, int w, int h,
                                       void* stream) {
     return motion_compensate_tiled(0, add_or_sub, cformat, w, h, bp, mv1, mv2, mode, dc, split, pic, pic_stride,
                                    ref1up, ref2up, clip_luma_depth, clip_chroma_depth, as_stream(stream));
+}
+
+extern "C" int dgpu_motion_compensate_weighted(int add_or_sub, int cformat, int w, int h,
+                                               const dgpu_block_params* bp, const int16_t* mv1, const int16_t* mv2,
+                                               const uint8_t* mode, const int16_t* dc, const uint8_t* split,
+                                               int16_t* const* pic, const int* pic_stride,
+                                               const int16_t* const* ref1up, const int16_t* const* ref2up,
+                                               int clip_luma_depth, int clip_chroma_depth, int ref1_weight,
+                                               int ref2_weight, int weight_bits, void* stream) {
+    return motion_compensate_impl(0, add_or_sub, cformat, w, h, bp, mv1, mv2, mode, dc, split, pic, pic_stride,
+                                  ref1up, ref2up, clip_luma_depth, clip_chroma_depth, ref1_weight, ref2_weight,
+                                  weight_bits, as_stream(stream));
 }

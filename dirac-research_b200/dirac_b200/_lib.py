@@ -78,6 +78,11 @@ SIGNATURES = {
         [c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
          P_void, P_int, P_void, P_void, c_int, c_int, c_void_p],
     ),
+    "dgpu_motion_compensate_weighted": (
+        c_int,
+        [c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+         P_void, P_int, P_void, P_void, c_int, c_int, c_int, c_int, c_int, c_void_p],
+    ),
     "dgpu_me_depth": (c_int, [c_int, c_int]),
     "dgpu_measure_int_rate": (c_int, [c_void_p]),
     "dgpu_me_profile": (c_int, [c_int, c_void_p, c_void_p]),

@@ -91,18 +91,19 @@ class MotionCompensator:
         self.cformat = cformat
 
     def CompensatePicture(self, direction, mv1, mv2, mode, dc, split, pic, ref1up, ref2up=None,
-                          clip_depths=(0, 0), stream=None):
+                          clip_depths=(0, 0), stream=None, weights=(1, 1, 1)):
+        """weights: the picture's reference weights (ref1, ref2, precision bits)."""
         for t in pic:
             _i16(t, "pic")
         h, w = pic[0].shape
         ups2 = ref2up if ref2up is not None else ref1up
-        rc = self.lib.dgpu_motion_compensate(
+        rc = self.lib.dgpu_motion_compensate_weighted(
             direction, self.cformat, w, h, ctypes.byref(self.bp), mv1.data_ptr(),
             mv2.data_ptr() if mv2 is not None else None, mode.data_ptr(), dc.data_ptr(), split.data_ptr(),
             _lib.ptr_array([p.data_ptr() for p in pic]), _lib.int_array([p.stride(0) for p in pic]),
             _lib.ptr_array([u.data_ptr() for u in ref1up]), _lib.ptr_array([u.data_ptr() for u in ups2]),
-            clip_depths[0], clip_depths[1], _sp(stream))
-        _lib.check(rc, "dgpu_motion_compensate")
+            clip_depths[0], clip_depths[1], int(weights[0]), int(weights[1]), int(weights[2]), _sp(stream))
+        _lib.check(rc, "dgpu_motion_compensate_weighted")
 
 
 class MotionEstimator:

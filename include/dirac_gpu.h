@@ -212,7 +212,10 @@ int dgpu_diag_lp_filter(int16_t* pic, int w, int h, int stride, float qf, int st
  * ref1up/ref2up[3]: the references' upconverted planes ((2h_c) x (2w_c), dense), as
  * produced by dgpu_upconvert; ref2up may be NULL for single-reference pictures.
  * clip_*_depth > 0 clamps the ADD result to that bit depth (Picture::Clip fused);
- * 0 leaves it unclipped.  Default (unit) reference weights only.
+ * 0 leaves it unclipped.  dgpu_motion_compensate uses the default reference picture weights;
+ * dgpu_motion_compensate_weighted takes the picture's (PicturePredParams::Ref1Weight,
+ * Ref2Weight, PictureWeightsBits, 0..16 bits) and applies them as AdjustBlockByRefWeights
+ * does (mot_comp.cpp:620-680) when they are not the defaults 1, 1, 1.
  * ------------------------------------------------------------------------------------- */
 typedef struct {
     int precision; /* MVPrecisionType: 0 pel, 1 half, 2 quarter, 3 eighth */
@@ -229,6 +232,12 @@ int dgpu_motion_compensate(int add_or_sub, int cformat, int w, int h, const dgpu
                            const int* pic_stride, const int16_t* const* ref1up,
                            const int16_t* const* ref2up, int clip_luma_depth,
                            int clip_chroma_depth, void* stream);
+int dgpu_motion_compensate_weighted(int add_or_sub, int cformat, int w, int h, const dgpu_block_params* bp,
+                                    const int16_t* mv1, const int16_t* mv2, const uint8_t* mode,
+                                    const int16_t* dc, const uint8_t* split, int16_t* const* pic,
+                                    const int* pic_stride, const int16_t* const* ref1up,
+                                    const int16_t* const* ref2up, int clip_luma_depth, int clip_chroma_depth,
+                                    int ref1_weight, int ref2_weight, int weight_bits, void* stream);
 
 /* ---------------------------------------------------------------------------------------
  * Motion estimation of one picture

@@ -373,10 +373,37 @@ static int16_t pixel_pred(int prec, const int16_t* up, int cw, int ch, int px, i
 #undef UP
 }
 
+/* AdjustBlockByRefWeights (mot_comp.cpp:620-680) for one sample of a predicted block, with
+ * custom picture weights: the block's values (ValueType, int16) scaled by ref1 + ref2 weights
+ * for one reference, or each by its own weight and added for two, then (v + bias) >> bits,
+ * the bias 2^(bits - 1) built by a loop that leaves it 1 when bits is 0. */
+static int16_t ref_weighted(int md, int16_t p1, int16_t p2, int wt1, int wt2, int wt_bits) {
+    int bias = 1;
+    for (int i = wt_bits - 1; i > 0; --i) bias <<= 1;
+    int16_t v;
+    if (md == 3)
+        v = (int16_t)((int16_t)(p1 * wt1) + (int16_t)(p2 * wt2));
+    else
+        v = (int16_t)(p1 * (wt1 + wt2));
+    return (int16_t)((v + bias) >> wt_bits);
+}
+
 int orc_motion_compensate(int add_or_sub, int cformat, int w, int h, const orc_block_params* bp,
                           const int16_t* mv1, const int16_t* mv2, const uint8_t* mode,
                           const int16_t* dc, const uint8_t* split, int16_t* const* pic,
                           const int16_t* const* ref1up, const int16_t* const* ref2up) {
+    return orc_motion_compensate_wt(add_or_sub, cformat, w, h, bp, mv1, mv2, mode, dc, split, pic, ref1up, ref2up,
+                                    1, 1, 1);
+}
+
+int orc_motion_compensate_wt(int add_or_sub, int cformat, int w, int h, const orc_block_params* bp,
+                             const int16_t* mv1, const int16_t* mv2, const uint8_t* mode,
+                             const int16_t* dc, const uint8_t* split, int16_t* const* pic,
+                             const int16_t* const* ref1up, const int16_t* const* ref2up, int wt1, int wt2,
+                             int wt_bits) {
+    /* PicturePredParams::CustomRefWeights (common.h:986-991) */
+    const int custom = wt_bits != 1 || wt1 != 1 || wt2 != 1;
+    if (wt_bits < 0 || wt_bits > 16) return -1;
     if (!bp || bp->xbsep <= 0 || bp->ybsep <= 0 || bp->xblen < bp->xbsep || bp->yblen < bp->ybsep ||
         bp->xblen > 2 * bp->xbsep || bp->yblen > 2 * bp->ybsep || bp->xnum_sb <= 0 || bp->ynum_sb <= 0)
         return -1;
@@ -430,7 +457,10 @@ int orc_motion_compensate(int add_or_sub, int cformat, int w, int h, const orc_b
                             if (md == 3) {
                                 const int16_t p2 = pixel_pred(bp->precision, ref2up[c], cw, ch, px, py,
                                                               mv2[2 * b] >> xs, mv2[2 * b + 1] >> ys);
-                                pred = (int16_t)((pred + p2 + 1) >> 1);
+                                pred = custom ? ref_weighted(3, pred, p2, wt1, wt2, wt_bits)
+                                              : (int16_t)((pred + p2 + 1) >> 1);
+                            } else if (custom) {
+                                pred = ref_weighted(md, pred, 0, wt1, wt2, wt_bits);
                             }
                         }
                         acc = (int16_t)(acc + (int16_t)(pred * wgt));

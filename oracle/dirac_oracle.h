@@ -65,6 +65,12 @@ int orc_motion_compensate(int add_or_sub, int cformat, int w, int h, const orc_b
                           const int16_t* mv1, const int16_t* mv2, const uint8_t* mode,
                           const int16_t* dc, const uint8_t* split, int16_t* const* pic,
                           const int16_t* const* ref1up, const int16_t* const* ref2up);
+/* The same with custom reference picture weights (ref1, ref2, precision bits; 1, 1, 1 is the
+ * default). */
+int orc_motion_compensate_wt(int add_or_sub, int cformat, int w, int h, const orc_block_params* bp,
+                          const int16_t* mv1, const int16_t* mv2, const uint8_t* mode,
+                          const int16_t* dc, const uint8_t* split, int16_t* const* pic,
+                          const int16_t* const* ref1up, const int16_t* const* ref2up, int wt1, int wt2, int wt_bits);
 
 /* Number of pyramid levels PixelMatcher uses for a w x h picture (pixel_match.cpp:94-95). */
 int orc_me_depth(int w, int h);

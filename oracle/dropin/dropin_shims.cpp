@@ -191,7 +191,6 @@ void MotionCompensator::CompensatePicture(const PicturePredParams& ppp, const Ad
                                           const MvData& mv_data, Picture* in_pic, Picture* refsptr[2]) {
     const PictureParams& pp = in_pic->GetPparams();
     if (!pp.PicSort().IsInter()) return;  // only inter pictures are compensated
-    if (const_cast<PicturePredParams&>(ppp).CustomRefWeights()) fail("custom reference picture weights");
     const int nref = (int)pp.Refs().size();
     if (nref < 2) refsptr[1] = refsptr[0];
     const dgpu_block_params bp = block_params(ppp);
@@ -246,15 +245,17 @@ void MotionCompensator::CompensatePicture(const PicturePredParams& ppp, const Ad
             up[r][c] = ups.back()->as<int16_t>();
         }
     }
-    const int rc = dgpu_motion_compensate(direction == ADD ? DGPU_ADD : DGPU_SUBTRACT, (int)pp.CFormat(), pp.Xl(),
-                                          pp.Yl(), &bp, mv1.as<int16_t>(), nref > 1 ? mv2.as<int16_t>() : nullptr,
-                                          mode.as<uint8_t>(), dc.as<int16_t>(), split.as<uint8_t>(), dpic, pstride,
-                                          up[0], nref > 1 ? up[1] : nullptr, 0, 0, nullptr);
+    // the picture's reference weights (the defaults 1, 1, 1 unless the stream sets others)
+    const int rc = dgpu_motion_compensate_weighted(
+        direction == ADD ? DGPU_ADD : DGPU_SUBTRACT, (int)pp.CFormat(), pp.Xl(), pp.Yl(), &bp, mv1.as<int16_t>(),
+        nref > 1 ? mv2.as<int16_t>() : nullptr, mode.as<uint8_t>(), dc.as<int16_t>(), split.as<uint8_t>(), dpic,
+        pstride, up[0], nref > 1 ? up[1] : nullptr, 0, 0, ppp.Ref1Weight(), ppp.Ref2Weight(),
+        (int)ppp.PictureWeightsBits(), nullptr);
     if (rc == DGPU_OK)
         for (int c = 0; c < 3; ++c) keep[c]->download(in_pic->Data((CompSort)c));
     for (DevPlane* p : keep) delete p;
     for (DevMem* m : ups) delete m;
-    check(rc, "dgpu_motion_compensate");
+    check(rc, "dgpu_motion_compensate_weighted");
 }
 
 void PictureCompressor::PixelME(EncQueue& my_buffer, int pnum) { estimate(my_buffer, pnum, 1, 0.0f); }

@@ -133,16 +133,18 @@ class Oracle:
 
 
     def motion_compensate(self, add_or_sub, cformat, pic, ref1, ref2, bp, mv1, mv2, mode, dc, split,
-                          luma_depth=8, chroma_depth=8):
-        """OBMC of a 3-component picture; refs are plain pictures (upconverted here)."""
+                          luma_depth=8, chroma_depth=8, weights=(1, 1, 1)):
+        """OBMC of a 3-component picture; refs are plain pictures (upconverted here).  weights:
+        the reference picture weights (ref1, ref2, precision bits)."""
         out = [np.array(p, dtype=np.int16, copy=True, order="C") for p in pic]
         r2 = ref2 if ref2 is not None else ref1
         up1 = [self.upconvert(r, luma_depth if c == 0 else chroma_depth) for c, r in enumerate(ref1)]
         up2 = [self.upconvert(r, luma_depth if c == 0 else chroma_depth) for c, r in enumerate(r2)]
         mv1, mv2, mode, dc, split = _mc_args(mv1, mv2, mode, dc, split)
         h, w = out[0].shape
-        rc = self.lib.orc_motion_compensate(add_or_sub, cformat, w, h, ctypes.byref(bp), _p(mv1), _p(mv2),
-                                            _p(mode), _p(dc), _p(split), _ptrs(out), _ptrs(up1), _ptrs(up2))
+        rc = self.lib.orc_motion_compensate_wt(add_or_sub, cformat, w, h, ctypes.byref(bp), _p(mv1), _p(mv2),
+                                               _p(mode), _p(dc), _p(split), _ptrs(out), _ptrs(up1), _ptrs(up2),
+                                               *[int(x) for x in weights])
         if rc:
             raise ValueError(f"orc_motion_compensate rc={rc}")
         return out
@@ -286,16 +288,16 @@ class Reference:
         return out
 
     def motion_compensate(self, add_or_sub, cformat, pic, ref1, ref2, bp, mv1, mv2, mode, dc, split,
-                          luma_depth=8, chroma_depth=8):
+                          luma_depth=8, chroma_depth=8, weights=(1, 1, 1)):
         out = [np.array(p, dtype=np.int16, copy=True, order="C") for p in pic]
         nref = 2 if ref2 is not None else 1
         r1 = [np.ascontiguousarray(r, dtype=np.int16) for r in ref1]
         r2 = [np.ascontiguousarray(r, dtype=np.int16) for r in (ref2 if ref2 is not None else ref1)]
         mv1, mv2, mode, dc, split = _mc_args(mv1, mv2, mode, dc, split)
         h, w = out[0].shape
-        rc = self.lib.ref_motion_compensate(add_or_sub, cformat, w, h, luma_depth, chroma_depth,
-                                            ctypes.byref(bp), nref, _p(mv1), _p(mv2), _p(mode), _p(dc),
-                                            _p(split), _ptrs(out), _ptrs(r1), _ptrs(r2))
+        rc = self.lib.ref_motion_compensate_wt(add_or_sub, cformat, w, h, luma_depth, chroma_depth,
+                                               ctypes.byref(bp), nref, _p(mv1), _p(mv2), _p(mode), _p(dc),
+                                               _p(split), _ptrs(out), _ptrs(r1), _ptrs(r2), *[int(x) for x in weights])
         if rc:
             raise ValueError("ref_motion_compensate failed")
         return out

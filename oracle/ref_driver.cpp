@@ -165,15 +165,35 @@ static void fill_mvdata(MvData& mv, const short* mv1, const short* mv2, const un
 // pic[3] (in/out, component planes) gets the OBMC prediction from ref1[3]/ref2[3] (plain,
 // not upconverted: the reference upconverts them itself through Picture::UpData) added
 // (add_or_sub = 0) or subtracted (1).  cformat: ChromaFormat (0 444, 1 422, 2 420).
+int ref_motion_compensate_wt(int add_or_sub, int cformat, int w, int h, int luma_depth, int chroma_depth,
+                             const RefBlockDesc* d, int nref, const short* mv1, const short* mv2,
+                             const unsigned char* mode, const short* dc, const unsigned char* split,
+                             short* const* pic, const short* const* ref1, const short* const* ref2, int wt1,
+                             int wt2, int wt_bits);
+
 int ref_motion_compensate(int add_or_sub, int cformat, int w, int h, int luma_depth, int chroma_depth,
                           const RefBlockDesc* d, int nref, const short* mv1, const short* mv2,
                           const unsigned char* mode, const short* dc, const unsigned char* split,
                           short* const* pic, const short* const* ref1, const short* const* ref2) {
+    return ref_motion_compensate_wt(add_or_sub, cformat, w, h, luma_depth, chroma_depth, d, nref, mv1, mv2, mode, dc,
+                                    split, pic, ref1, ref2, 1, 1, 1);
+}
+
+// The same with the picture's reference weights set (PicturePredParams::SetRef1Weight,
+// SetRef2Weight, SetPictureWeightsPrecision; 1, 1, 1 are the defaults).
+int ref_motion_compensate_wt(int add_or_sub, int cformat, int w, int h, int luma_depth, int chroma_depth,
+                             const RefBlockDesc* d, int nref, const short* mv1, const short* mv2,
+                             const unsigned char* mode, const short* dc, const unsigned char* split,
+                             short* const* pic, const short* const* ref1, const short* const* ref2, int wt1,
+                             int wt2, int wt_bits) {
     try {
         const ChromaFormat cf = (ChromaFormat)cformat;
         CodecParams cp(VIDEO_FORMAT_CIF, INTER_PICTURE, nref, true);
         PicturePredParams& ppp = cp.GetPicPredParams();
         setup_ppp(ppp, *d, cf);
+        ppp.SetRef1Weight(wt1);
+        ppp.SetRef2Weight(wt2);
+        ppp.SetPictureWeightsPrecision((unsigned int)wt_bits);
         MvData mv(ppp, 2);
         fill_mvdata(mv, mv1, mv2, mode, dc, split, nref);
 

@@ -61,7 +61,13 @@ def mc_cases(ref):
     out = {}
     cases = [(96, 64, 2, 2, (12, 12, 8, 8), 2), (100, 72, 1, 3, (16, 16, 12, 12), 2),
              (64, 48, 0, 1, (8, 8, 8, 8), 1), (72, 56, 2, 0, (16, 12, 12, 8), 2)]
-    for k, (w, h, cf, prec, olb, nref) in enumerate(cases):
+    # then custom reference picture weights (ref1, ref2, precision bits) on 10-bit-range samples
+    cases += [(96, 64, 2, 2, (12, 12, 8, 8), 2, (3, 5, 3)), (72, 56, 1, 1, (16, 16, 12, 12), 2, (-2, 7, 2)),
+              (64, 48, 0, 3, (8, 8, 8, 8), 1, (1, 1, 0)), (80, 48, 2, 2, (16, 12, 12, 8), 2, (255, 1, 8))]
+    for k, case in enumerate(cases):
+        w, h, cf, prec, olb, nref = case[:6]
+        wts = case[6] if len(case) > 6 else (1, 1, 1)
+        amp = 128 if len(case) == 6 else 512
         xbl, ybl, xbs, ybs = olb
         xsb, ysb = (w + 4 * xbs - 1) // (4 * xbs), (h + 4 * ybs - 1) // (4 * ybs)
         nb = (4 * ysb, 4 * xsb)
@@ -69,18 +75,19 @@ def mc_cases(ref):
         mv1 = rng.integers(-rr, rr, size=nb + (2,)).astype(np.int16)
         mv2 = rng.integers(-rr, rr, size=nb + (2,)).astype(np.int16)
         mode = rng.integers(0, 4 if nref == 2 else 2, size=nb).astype(np.uint8)
-        dc = rng.integers(-128, 128, size=(3,) + nb).astype(np.int16)
+        dc = rng.integers(-amp, amp, size=(3,) + nb).astype(np.int16)
         split = rng.integers(0, 3, size=(ysb, xsb)).astype(np.uint8)
         xs, ys = chroma_shift(cf)
 
         def mk():
-            return [rng.integers(-128, 128, size=(h, w)).astype(np.int16)] + \
-                   [rng.integers(-128, 128, size=(h >> ys, w >> xs)).astype(np.int16) for _ in range(2)]
+            return [rng.integers(-amp, amp, size=(h, w)).astype(np.int16)] + \
+                   [rng.integers(-amp, amp, size=(h >> ys, w >> xs)).astype(np.int16) for _ in range(2)]
 
         pic, r1, r2 = mk(), mk(), mk()
         bp = BlockParams(prec, xbl, ybl, xbs, ybs, xsb, ysb)
         key = f"mc{k}"
         out[key + "_meta"] = np.array([w, h, cf, prec, xbl, ybl, xbs, ybs, xsb, ysb, nref], np.int32)
+        out[key + "_wt"] = np.array(wts, np.int32)
         for name, a in (("mv1", mv1), ("mv2", mv2), ("mode", mode), ("dc", dc), ("split", split)):
             out[f"{key}_{name}"] = a
         for c in range(3):
@@ -88,8 +95,9 @@ def mc_cases(ref):
             out[f"{key}_r1_{c}"] = r1[c]
             out[f"{key}_r2_{c}"] = r2[c]
         for aos in (0, 1):
+            bd = 8 if amp == 128 else 10
             res = ref.motion_compensate(aos, cf, pic, r1, r2 if nref == 2 else None, bp, mv1, mv2, mode, dc,
-                                        split)
+                                        split, bd, bd, wts)
             for c in range(3):
                 out[f"{key}_out{aos}_{c}"] = res[c]
     return out

@@ -49,24 +49,28 @@ def test_pyramid_1080p_depth6(gpu, oracle):
         assert cur.shape == (1080 >> lev, 1920 >> lev)
 
 
-def gpu_mc(gpu, aos, cf, bp, a, pic, r1, r2, clip=(0, 0)):
-    lbd = 8
+def gpu_mc(gpu, aos, cf, bp, a, pic, r1, r2, clip=(0, 0), lbd=8):
     ups1 = [gpu.upconvert(dev(r), lbd) for r in r1]
     ups2 = [gpu.upconvert(dev(r), lbd) for r in r2] if r2 is not None else None
     p = [dev(x) for x in pic]
     bpg = gpu.BlockParams(bp.precision, bp.xblen, bp.yblen, bp.xbsep, bp.ybsep, bp.xnum_sb, bp.ynum_sb)
     mc = gpu.MotionCompensator(bpg, cf)
     mc.CompensatePicture(aos, dev(a["mv1"]), dev(a["mv2"]), dev(a["mode"]), dev(a["dc"]), dev(a["split"]), p,
-                         ups1, ups2, clip_depths=clip)
+                         ups1, ups2, clip_depths=clip, weights=a.get("weights", (1, 1, 1)))
     return [x.cpu().numpy() for x in p]
 
 
 def test_mc_golden(gpu, golden):
+    """The reference's CompensatePicture outputs (mc.npz), with default and custom reference
+    picture weights."""
+    from test_oracle import MC_GOLDEN_CASES
+
     g = golden("mc.npz")
-    for k in range(4):
+    for k in range(MC_GOLDEN_CASES):
         cf, bp, a, pic, r1, r2, outs = mc_case(g, k)
+        bd = 8 if a["weights"] == (1, 1, 1) else 10
         for aos in (0, 1):
-            res = gpu_mc(gpu, aos, cf, bp, a, pic, r1, r2)
+            res = gpu_mc(gpu, aos, cf, bp, a, pic, r1, r2, lbd=bd)
             for c in range(3):
                 np.testing.assert_array_equal(res[c], outs[aos][c], err_msg=f"case {k} aos {aos} comp {c}")
 
@@ -97,6 +101,47 @@ def test_mc_vs_oracle(gpu, oracle, trial):
         got = gpu_mc(gpu, aos, cf, bp, a, pic, r1, r2)
         for c in range(3):
             np.testing.assert_array_equal(got[c], want[c], err_msg=f"aos {aos} comp {c}")
+
+
+@pytest.mark.parametrize("trial", range(8))
+def test_weighted_mc_vs_oracle(gpu, oracle, trial):
+    """Custom reference picture weights (dgpu_motion_compensate_weighted) against the oracle,
+    every prediction mode and chroma format, up to 1080p, 10-bit-range samples (so that large
+    weights wrap the reference's int16 block values)."""
+    from oracle import BlockParams, chroma_shift
+    from test_oracle import MC_WEIGHTS
+
+    rng = np.random.default_rng(700 + trial)
+    weights = MC_WEIGHTS[trial % len(MC_WEIGHTS)]
+    cf, prec = trial % 3, (trial + 2) % 4
+    w, h = [(352, 288), (1920, 1080), (176, 144), (130, 98)][trial % 4]
+    xbl, ybl, xbs, ybs = [(12, 12, 8, 8), (16, 16, 12, 12), (8, 8, 8, 8), (16, 12, 12, 8)][trial % 4]
+    xsb, ysb = (w + 4 * xbs - 1) // (4 * xbs), (h + 4 * ybs - 1) // (4 * ybs)
+    bp = BlockParams(prec, xbl, ybl, xbs, ybs, xsb, ysb)
+    nb = (4 * ysb, 4 * xsb)
+    a = {"mv1": rng.integers(-60 << prec, 60 << prec, size=nb + (2,)).astype(np.int16),
+         "mv2": rng.integers(-60 << prec, 60 << prec, size=nb + (2,)).astype(np.int16),
+         "mode": rng.integers(0, 4, size=nb).astype(np.uint8),
+         "dc": rng.integers(-512, 512, size=(3,) + nb).astype(np.int16),
+         "split": rng.integers(0, 3, size=(ysb, xsb)).astype(np.uint8), "weights": weights}
+    xs, ys = chroma_shift(cf)
+    mk = lambda: [rng.integers(-512, 512, size=(h, w)).astype(np.int16)] + [
+        rng.integers(-512, 512, size=(h >> ys, w >> xs)).astype(np.int16) for _ in range(2)]
+    pic, r1, r2 = mk(), mk(), mk()
+    for aos in (0, 1):
+        want = oracle.motion_compensate(aos, cf, pic, r1, r2, bp, a["mv1"], a["mv2"], a["mode"], a["dc"],
+                                        a["split"], 10, 10, weights)
+        got = gpu_mc(gpu, aos, cf, bp, a, pic, r1, r2, lbd=10)
+        for c in range(3):
+            np.testing.assert_array_equal(got[c], want[c], err_msg=f"weights {weights} aos {aos} comp {c}")
+
+
+def test_weighted_mc_rejects_bad_precision():
+    from dirac_b200 import _lib
+
+    lib = _lib.load()
+    assert lib.dgpu_motion_compensate_weighted(0, 2, 64, 64, None, None, None, None, None, None, None, None,
+                                               None, None, 0, 0, 1, 1, 1, None) == -1
 
 
 @pytest.mark.parametrize("prec", range(4))

@@ -111,16 +111,21 @@ def mc_case(g, k):
     r1 = [g[f"mc{k}_r1_{c}"] for c in range(3)]
     r2 = [g[f"mc{k}_r2_{c}"] for c in range(3)] if nref == 2 else None
     outs = {aos: [g[f"mc{k}_out{aos}_{c}"] for c in range(3)] for aos in (0, 1)}
+    arrs["weights"] = tuple(int(x) for x in g[f"mc{k}_wt"])
     return cf, bp, arrs, pic, r1, r2, outs
+
+
+MC_GOLDEN_CASES = 8  # 4 with the default reference weights, then 4 with custom ones
 
 
 def test_motion_compensation_golden(oracle, golden):
     g = golden("mc.npz")
-    for k in range(4):
+    for k in range(MC_GOLDEN_CASES):
         cf, bp, a, pic, r1, r2, outs = mc_case(g, k)
+        bd = 8 if a["weights"] == (1, 1, 1) else 10
         for aos in (0, 1):
             res = oracle.motion_compensate(aos, cf, pic, r1, r2, bp, a["mv1"], a["mv2"], a["mode"], a["dc"],
-                                           a["split"])
+                                           a["split"], bd, bd, a["weights"])
             for c in range(3):
                 np.testing.assert_array_equal(res[c], outs[aos][c], err_msg=f"case {k} aos {aos} comp {c}")
 
@@ -152,6 +157,48 @@ def test_motion_compensation_matches_live_reference(oracle):
             b = ref.motion_compensate(aos, cf, pic, r1, r2, bp, mv1, mv2, mode, dc, split)
             for c in range(3):
                 np.testing.assert_array_equal(a[c], b[c])
+
+
+# reference picture weights (ref1, ref2, precision bits) of the weighted-compensation checks:
+# the precision 0 whose rounding bias the reference leaves at 1, a negative and a zero weight,
+# and weights large enough to wrap the reference's int16 block values
+MC_WEIGHTS = [(1, 1, 0), (3, 5, 3), (-2, 7, 2), (0, 4, 2), (2, 2, 1), (255, 1, 8), (40, -9, 5)]
+
+
+@needs_ref
+@pytest.mark.parametrize("weights", MC_WEIGHTS, ids=[str(w) for w in MC_WEIGHTS])
+def test_weighted_motion_compensation_matches_live_reference(oracle, weights):
+    """Custom reference picture weights (AdjustBlockByRefWeights, mot_comp.cpp:620-680): the
+    oracle equals the reference's CompensatePicture with the weights set in its
+    PicturePredParams, on every prediction mode, both directions and all chroma formats."""
+    from oracle import BlockParams, chroma_shift
+
+    ref = Reference()
+    rng = np.random.default_rng(78 + sum(abs(x) for x in weights))
+    for trial in range(3):
+        cf, prec = trial, (trial + 1) % 4
+        w, h = [(176, 144), (120, 72), (96, 64)][trial]
+        xbl, ybl, xbs, ybs = [(12, 12, 8, 8), (16, 16, 12, 12), (8, 8, 8, 8)][trial]
+        xsb, ysb = (w + 4 * xbs - 1) // (4 * xbs), (h + 4 * ybs - 1) // (4 * ybs)
+        bp = BlockParams(prec, xbl, ybl, xbs, ybs, xsb, ysb)
+        nb = (4 * ysb, 4 * xsb)
+        mv1 = rng.integers(-40 << prec, 40 << prec, size=nb + (2,)).astype(np.int16)
+        mv2 = rng.integers(-40 << prec, 40 << prec, size=nb + (2,)).astype(np.int16)
+        mode = rng.integers(0, 4, size=nb).astype(np.uint8)
+        dc = rng.integers(-512, 512, size=(3,) + nb).astype(np.int16)
+        split = rng.integers(0, 3, size=(ysb, xsb)).astype(np.uint8)
+        xs, ys = chroma_shift(cf)
+        mk = lambda: [rng.integers(-512, 512, size=(h, w)).astype(np.int16)] + [
+            rng.integers(-512, 512, size=(h >> ys, w >> xs)).astype(np.int16) for _ in range(2)]
+        pic, r1, r2 = mk(), mk(), mk()
+        for aos in (0, 1):
+            a = oracle.motion_compensate(aos, cf, pic, r1, r2, bp, mv1, mv2, mode, dc, split, 10, 10, weights)
+            b = ref.motion_compensate(aos, cf, pic, r1, r2, bp, mv1, mv2, mode, dc, split, 10, 10, weights)
+            for c in range(3):
+                np.testing.assert_array_equal(a[c], b[c], err_msg=f"trial {trial} aos {aos} comp {c}")
+            if weights != (1, 1, 1):
+                d = oracle.motion_compensate(aos, cf, pic, r1, r2, bp, mv1, mv2, mode, dc, split, 10, 10)
+                assert any(not np.array_equal(a[c], d[c]) for c in range(3))
 
 
 def me_case(g, k):
