@@ -48,6 +48,8 @@ struct Planes3 {
     int16_t* orig[3];
     int16_t* data[3];
     int n[3];
+    int w[3];      // picture width
+    int pitch[3];  // source row pitch in samples (2 w for a field of a frame)
 };
 
 // Unsigned input samples to codec samples (value - 2^(depth-1)), as StreamFrameInput reads
@@ -57,9 +59,10 @@ __global__ void load_kernel(const __grid_constant__ Planes3 P, int off_luma, int
     const int c = blockIdx.y;
     const T* __restrict__ src = static_cast<const T*>(P.src[c]);
     const int off = c == 0 ? off_luma : off_chroma;
-    const int n = P.n[c];
+    const int n = P.n[c], w = P.w[c], pitch = P.pitch[c];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int16_t v = (int16_t)((int)src[i] - off);
+        const int y = i / w;
+        const int16_t v = (int16_t)((int)src[(size_t)y * pitch + (i - y * w)] - off);
         P.orig[c][i] = v;
         P.data[c][i] = v;
     }
@@ -149,6 +152,8 @@ struct Encoder {
     int last_read = -1;          // m_last_picture_read
     int prepared = -1;           // picture prepared by dgpu_encoder_prepare_next, or -1
     int failed = DGPU_OK;        // first failure of a picture's coding; sticky until reset
+    bool field = false;          // field coding: pictures are fields, two per loaded frame
+    bool tff = false;            // top field first
     bool eos = false;            // m_eos_signalled
     std::map<int, Pic> pics;
 
@@ -221,6 +226,15 @@ size_t sample_bytes(const Encoder& E) { return E.P.luma_depth > 8 || E.P.chroma_
 // ---- GOP structure ----------------------------------------------------------------------
 int coded_to_display(const Encoder& E, int cnum) {
     const int s = E.m_L1_sep;
+    if (E.field) {  // FieldSequenceCompressor::CodedToDisplay (seq_compress.cpp:859-879)
+        const int fnum = cnum >> 1;
+        if (s > 0) {
+            if (fnum == 0) return cnum;
+            if ((fnum - 1) % s == 0) return cnum + (s - 1) * 2;
+            return cnum - 2;
+        }
+        return cnum;
+    }
     if (s > 0) {
         if (cnum == 0) return 0;
         if ((cnum - 1) % s == 0) return cnum + s - 1;
@@ -232,8 +246,11 @@ int coded_to_display(const Encoder& E, int cnum) {
 bool can_encode(Encoder& E) {
     if (E.eos) {
         if (E.num_L1 > 0) {
-            if (E.last_read >= E.code + (E.last_read % E.L1Sep)) return true;
-            if (E.code <= E.last_read) {
+            // in frames: two fields to a frame when field coding (seq_compress.cpp:162-164)
+            const int ff = E.field ? 2 : 1;
+            const int last_frame = E.last_read / ff, code_frame = E.code / ff;
+            if (last_frame >= code_frame + (last_frame % E.L1Sep)) return true;
+            if (code_frame <= last_frame) {
                 E.cur = E.code;
                 return true;
             }
@@ -276,8 +293,56 @@ void type_refs(const Encoder& E, int pnum, int sep, int avail, bool& intra, bool
     }
 }
 
+// FieldSequenceCompressor::SetPicTypeAndRefs (seq_compress.cpp:767-852): fields 2n and 2n + 1
+// of frame n; the second field of an I frame is predicted from the first.
+void type_refs_field(const Encoder& E, int pnum, int sep, int avail, bool& intra, bool& is_ref,
+                     std::vector<int>& refs) {
+    const int rel = pnum - E.gop_start;
+    refs.clear();
+    if (E.num_L1 <= 0) {
+        intra = true;
+        is_ref = false;
+        return;
+    }
+    const bool second = pnum % 2 != 0;
+    if ((rel / 2) % E.gop_len == 0) {
+        if (E.gop_len > 1) {
+            intra = !second;
+            is_ref = true;
+            if (second) refs.push_back(pnum - 1);
+        } else {
+            intra = true;
+            is_ref = false;
+        }
+    } else if ((rel / 2) % sep == 0) {
+        intra = false;
+        is_ref = true;
+        if (second) {
+            refs.push_back(pnum - 1);
+            refs.push_back(pnum - sep * 2);
+        } else {
+            refs.push_back(pnum - sep * 2);
+            refs.push_back(pnum - sep * 2 + 1);
+        }
+    } else if ((rel / 2 + 1) % sep == 0) {
+        intra = false;
+        is_ref = !second;
+        refs.push_back(pnum - 1);
+        if (pnum + 2 <= avail) refs.push_back(pnum + 2);
+    } else {
+        intra = false;
+        is_ref = true;
+        refs.push_back(pnum - 1);
+        const int next_ref = (((pnum / 2) / sep + 1) * sep) * 2 + (pnum % 2);
+        if (next_ref <= avail) refs.push_back(next_ref);
+    }
+}
+
 void set_type(Encoder& E, Pic& p) {
-    type_refs(E, p.pnum, E.m_L1_sep, E.last_read, p.intra, p.is_ref, p.refs);
+    if (E.field)
+        type_refs_field(E, p.pnum, E.m_L1_sep, E.last_read, p.intra, p.is_ref, p.refs);
+    else
+        type_refs(E, p.pnum, E.m_L1_sep, E.last_read, p.intra, p.is_ref, p.refs);
     p.typed = true;
 }
 
@@ -477,7 +542,7 @@ int code_residue(Encoder& E, Pic& p, const float* ecf_in, bool forward_done = fa
     float lam[3];
     int intra[3], dep[3];
     for (int c = 0; c < 3; ++c) {
-        int rc = dgpu_band_weights(filter, depth, E.pw[c], E.ph[c], c, E.P.cformat, E.P.cpd, (float)cpd_scale, 0,
+        int rc = dgpu_band_weights(filter, depth, E.pw[c], E.ph[c], c, E.P.cformat, E.P.cpd, (float)cpd_scale, E.field ? 1 : 0,
                                    wd.data());
         if (rc) return rc;
         for (int b = 0; b < nb; ++b) wt[c * nb + b] = (float)wd[b];
@@ -558,17 +623,22 @@ static int encoder_setup(const dgpu_encoder_params& P, int max_pictures, void* s
         P.chroma_depth < 8 || P.chroma_depth > 14 || P.num_l1 < 0 || (P.num_l1 > 0 && P.l1_sep < 1) ||
         P.mv_precision < 1 || P.mv_precision > 3 || P.wlt_depth < 1 || P.wlt_depth > 6 || P.intra_filter < 0 ||
         P.intra_filter > 6 || P.inter_filter < 0 || P.inter_filter > 6 || P.xbsep < 1 || P.ybsep < 1 ||
-        P.xblen < P.xbsep || P.yblen < P.ybsep)
+        P.xblen < P.xbsep || P.yblen < P.ybsep || P.field_coding < 0 || P.field_coding > 1)
         return DGPU_ERR_ARG;
     E->P = P;
+    E->field = P.field_coding == 1;
+    E->tff = P.top_field_first != 0;
     E->st = as_stream(stream);
     E->L = calc_lambdas(P.qf);
     E->xs = P.cformat == 0 ? 0 : 1;
     E->ys = P.cformat == 2 ? 1 : 0;
+    // field coding codes pictures of half the frame's height (dirac_encoder.cpp:525-530)
+    if (E->field && (P.height % (2 << E->ys) != 0 || P.height < 32)) return DGPU_ERR_SIZE;
+    const int pic_h = E->field ? P.height / 2 : P.height;
     E->w[0] = P.width;
-    E->h[0] = P.height;
+    E->h[0] = pic_h;
     E->w[1] = E->w[2] = P.width >> E->xs;
-    E->h[1] = E->h[2] = P.height >> E->ys;
+    E->h[1] = E->h[2] = pic_h >> E->ys;
     const int mul = 1 << P.wlt_depth;
     for (int c = 0; c < 3; ++c) {
         E->pw[c] = (E->w[c] + mul - 1) / mul * mul;
@@ -581,12 +651,12 @@ static int encoder_setup(const dgpu_encoder_params& P, int max_pictures, void* s
     E->bp.xbsep = P.xbsep;
     E->bp.ybsep = P.ybsep;
     E->bp.xnum_sb = (P.width + 4 * P.xbsep - 1) / (4 * P.xbsep);
-    E->bp.ynum_sb = (P.height + 4 * P.ybsep - 1) / (4 * P.ybsep);
+    E->bp.ynum_sb = (pic_h + 4 * P.ybsep - 1) / (4 * P.ybsep);
     E->nsb = E->bp.xnum_sb * E->bp.ynum_sb;
     E->nblocks = 16 * E->nsb;
     E->nb = 3 * P.wlt_depth + 1;
     E->ncb.assign((size_t)2 * E->nb, 0);
-    int rc = dgpu_code_blocks(P.wlt_depth, P.width, P.height, 1, E->ncb.data());
+    int rc = dgpu_code_blocks(P.wlt_depth, P.width, pic_h, 1, E->ncb.data());
     if (rc) return rc;
     for (int b = 0; b < E->nb; ++b) E->ncb_total += E->ncb[2 * b] * E->ncb[2 * b + 1];
     // GOP (dirac_encoder.cpp:562-572, common.cpp:512-518)
@@ -613,7 +683,7 @@ static int encoder_setup(const dgpu_encoder_params& P, int max_pictures, void* s
     {
         std::vector<int> r2(E->me_max_tasks, 0);
         const int npics_max = std::min(nslots, 3 * E->me_max_tasks);
-        E->me_ws_bytes = dgpu_me_batch_workspace_bytes(P.cformat, P.width, P.height, &E->bp, npics_max,
+        E->me_ws_bytes = dgpu_me_batch_workspace_bytes(P.cformat, P.width, pic_h, &E->bp, npics_max,
                                                        E->me_max_tasks, r2.data(), 3);
         if (E->me_ws_bytes == 0) return DGPU_ERR_ARG;
     }
@@ -625,7 +695,9 @@ static int encoder_setup(const dgpu_encoder_params& P, int max_pictures, void* s
         E->q_ws_bytes = dgpu_code_residue_workspace_bytes(3, intra, dep, E->pw, E->ph, ncb3.data());
         if (E->q_ws_bytes == 0) return DGPU_ERR_ARG;
     }
-    for (int c = 0; c < 3; ++c) E->stage_bytes += align_up((size_t)E->w[c] * E->h[c] * 2, 256);
+    // one input frame (two fields when field coding) or one output picture
+    for (int c = 0; c < 3; ++c)
+        E->stage_bytes += align_up((size_t)E->w[c] * E->h[c] * 2 * (E->field ? 2 : 1), 256);
     *total = (size_t)nslots * align_up(*slot_bytes, 256) + align_up(E->me_ws_bytes, 256) +
              align_up(E->dwt_ws_bytes, 256) + align_up(E->q_ws_bytes, 256) +
              align_up(sizeof(int) * E->me_max_tasks, 256) + E->stage_bytes;
@@ -705,44 +777,83 @@ extern "C" int dgpu_encoder_destroy(void* enc) {
     return DGPU_OK;
 }
 
+namespace dgpu {
+namespace {
+
+// One picture into slot k from device planes src[c] with row pitch pitch[c] (samples).
+int load_slot(Encoder& E, int k, const void* const* src, const int* pitch) {
+    Slot& s = E.slots[k];
+    Planes3 P3{};
+    for (int c = 0; c < 3; ++c) {
+        P3.src[c] = src[c];
+        P3.orig[c] = s.orig[c];
+        P3.data[c] = s.data[c];
+        P3.n[c] = E.w[c] * E.h[c];
+        P3.w[c] = E.w[c];
+        P3.pitch[c] = pitch[c];
+    }
+    StageTimer timer(E, DGPU_STAGE_LOAD);
+    dim3 grid(std::min((E.w[0] * E.h[0] + 255) / 256, 148 * 8), 3);
+    const int offl = 1 << (E.P.luma_depth - 1), offc = 1 << (E.P.chroma_depth - 1);
+    if (sample_bytes(E) == 1)
+        load_kernel<uint8_t><<<grid, 256, 0, E.st>>>(P3, offl, offc);
+    else
+        load_kernel<uint16_t><<<grid, 256, 0, E.st>>>(P3, offl, offc);
+    DGPU_CHECK_LAUNCH();
+    const int pnum = ++E.last_read;
+    s.pnum = pnum;
+    Pic& p = E.pics[pnum];
+    p = Pic();
+    p.pnum = pnum;
+    p.slot = k;
+    return DGPU_OK;
+}
+
+}  // namespace
+}  // namespace dgpu
+
 extern "C" int dgpu_encoder_load(void* enc, const void* const* planes, int on_host) {
     Encoder* E = static_cast<Encoder*>(enc);
     if (!E || !planes || !planes[0] || !planes[1] || !planes[2]) return DGPU_ERR_ARG;
     if (E->eos) return DGPU_ERR_ARG;
-    const int k = take_slot(*E);
-    if (k < 0) return DGPU_ERR_SIZE;
-    Slot& s = E->slots[k];
+    // a frame, or the two fields of an interlaced frame (StreamFieldInput::ReadFieldComponent,
+    // pic_io.cpp:464-530): each field takes every other row of the frame
+    const int npics = E->field ? 2 : 1;
+    int k[2] = {-1, -1};
+    for (int f = 0; f < npics; ++f) {
+        k[f] = take_slot(*E);
+        if (k[f] < 0) {
+            if (f == 1) E->slots[k[0]].pnum = -1;  // nothing loaded: give the first slot back
+            return DGPU_ERR_SIZE;
+        }
+        E->slots[k[f]].pnum = 0x7fffffff;  // reserved, so that the second take finds another slot
+    }
     const size_t sb = sample_bytes(*E);
-    Planes3 P3{};
+    const void* src[3];
     size_t off = 0;
     for (int c = 0; c < 3; ++c) {
-        const size_t bytes = (size_t)E->w[c] * E->h[c] * sb;
+        const size_t bytes = (size_t)E->w[c] * E->h[c] * npics * sb;  // the whole frame
         if (on_host) {
             void* dst = static_cast<char*>(E->stage) + off;
             DGPU_CHECK_CUDA(cudaMemcpyAsync(dst, planes[c], bytes, cudaMemcpyHostToDevice, E->st));
-            P3.src[c] = dst;
+            src[c] = dst;
             off += align_up(bytes, 256);
         } else {
-            P3.src[c] = planes[c];
+            src[c] = planes[c];
         }
-        P3.orig[c] = s.orig[c];
-        P3.data[c] = s.data[c];
-        P3.n[c] = E->w[c] * E->h[c];
     }
-    StageTimer timer(*E, DGPU_STAGE_LOAD);
-    dim3 grid(std::min((E->w[0] * E->h[0] + 255) / 256, 148 * 8), 3);
-    const int offl = 1 << (E->P.luma_depth - 1), offc = 1 << (E->P.chroma_depth - 1);
-    if (sb == 1)
-        load_kernel<uint8_t><<<grid, 256, 0, E->st>>>(P3, offl, offc);
-    else
-        load_kernel<uint16_t><<<grid, 256, 0, E->st>>>(P3, offl, offc);
-    DGPU_CHECK_LAUNCH();
-    const int pnum = ++E->last_read;
-    s.pnum = pnum;
-    Pic& p = E->pics[pnum];
-    p = Pic();
-    p.pnum = pnum;
-    p.slot = k;
+    for (int f = 0; f < npics; ++f) {
+        const void* fsrc[3];
+        int pitch[3];
+        // field f of the frame: the even rows for the first field when the top field is first
+        const int parity = E->field ? (f == 0 ? (E->tff ? 0 : 1) : (E->tff ? 1 : 0)) : 0;
+        for (int c = 0; c < 3; ++c) {
+            pitch[c] = E->w[c] * npics;
+            fsrc[c] = static_cast<const char*>(src[c]) + (size_t)parity * E->w[c] * sb;
+        }
+        const int rc = load_slot(*E, k[f], fsrc, pitch);
+        if (rc) return rc;
+    }
     return DGPU_OK;
 }
 
@@ -852,8 +963,10 @@ int prepare_impl(Encoder* E, dgpu_picture_info* info) {
         return 1;
     }
     if (E->last_read < 0) return 0;
-    // a scheduled return to the normal L1 separation (seq_compress.cpp:215-219)
-    if (E->L1Sep > 0 && E->L1Sep != E->m_L1_sep && (E->code - 1) % E->L1Sep == 0) E->m_L1_sep = E->L1Sep;
+    // a scheduled return to the normal L1 separation (seq_compress.cpp:212-219); ff fields to a
+    // frame when field coding
+    const int ff = E->field ? 2 : 1;
+    if (E->L1Sep > 0 && E->L1Sep != E->m_L1_sep && (E->code - ff) % (E->L1Sep * ff) == 0) E->m_L1_sep = E->L1Sep;
     E->cur = coded_to_display(*E, E->code);
     if (!can_encode(*E)) return 0;
     if (!E->pics.count(E->cur) || E->pics[E->cur].coded) return 0;
@@ -869,10 +982,10 @@ int prepare_impl(Encoder* E, dgpu_picture_info* info) {
         for (;;) {
             rc = ensure_me(*E, *p);
             if (rc) return rc;
-            if (E->m_L1_sep > 1 && p->ratio > 0.25 && E->cur % E->L1Sep == 0) {
+            if (E->m_L1_sep > 1 && p->ratio > 0.25 && E->cur % (E->L1Sep * ff) == 0) {
                 E->m_L1_sep = 1;
-                for (int i = 0; i < E->L1Sep; ++i) {
-                    auto it = E->pics.find(E->cur - i);
+                for (int i = 0; i < ff * E->L1Sep; ++i) {
+                    auto it = E->pics.find(E->cur - i + (ff - 1));
                     if (it == E->pics.end()) return DGPU_ERR_ARG;
                     set_type(*E, it->second);
                 }
@@ -886,7 +999,7 @@ int prepare_impl(Encoder* E, dgpu_picture_info* info) {
         // cut detection
         if (p->ratio > 0.3333) {
             p->cut = true;
-            if (E->L1Sep > 1 && E->cur % E->L1Sep == 0) E->gop_start = p->pnum;
+            if (E->L1Sep > 1 && E->cur % (ff * E->L1Sep) == 0) E->gop_start = p->pnum;
             p->intra = true;
         } else {
             rc = motion_compensate(*E, *p, DGPU_SUBTRACT, false);
@@ -1247,7 +1360,7 @@ struct Group {
 };
 
 bool same_geometry(const Encoder& a, const Encoder& b) {
-    return a.P.cformat == b.P.cformat && a.P.width == b.P.width && a.P.height == b.P.height &&
+    return a.P.cformat == b.P.cformat && a.P.width == b.P.width && a.P.height == b.P.height && a.field == b.field &&
            a.P.luma_depth == b.P.luma_depth && a.bp.precision == b.bp.precision && a.bp.xblen == b.bp.xblen &&
            a.bp.yblen == b.bp.yblen && a.bp.xbsep == b.bp.xbsep && a.bp.ybsep == b.bp.ybsep;
 }
@@ -1262,7 +1375,7 @@ size_t group_ws_bytes(const std::vector<Encoder*>& enc, int* max_tasks) {
     *max_tasks = nt;
     std::vector<int> r2(nt, 0);
     const Encoder& E0 = *enc[0];
-    return dgpu_me_batch_workspace_bytes(E0.P.cformat, E0.P.width, E0.P.height, &E0.bp, np, nt, r2.data(), 3);
+    return dgpu_me_batch_workspace_bytes(E0.P.cformat, E0.P.width, E0.h[0], &E0.bp, np, nt, r2.data(), 3);
 }
 
 }  // namespace

@@ -51,7 +51,7 @@ class AdaptiveCoder:
         self.enc = enc
         self.lib = _lib.load()
         self.depth = params["wlt_depth"]
-        self.ncb = quant.code_blocks(self.depth, params["width"], params["height"])
+        self.ncb = quant.code_blocks(self.depth, enc.shapes[0][1], enc.shapes[0][0])  # picture (field) size
         mul = 1 << self.depth
         self.qshapes = [((h + mul - 1) // mul * mul, (w + mul - 1) // mul * mul) for h, w in enc.shapes]
         self.ex = ThreadPoolExecutor(threads)

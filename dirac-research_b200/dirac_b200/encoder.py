@@ -26,7 +26,7 @@ class EncoderParams(ctypes.Structure):
                 ("l1_sep", ctypes.c_int), ("num_l1", ctypes.c_int), ("cpd", ctypes.c_float),
                 ("xblen", ctypes.c_int), ("yblen", ctypes.c_int), ("xbsep", ctypes.c_int), ("ybsep", ctypes.c_int),
                 ("mv_precision", ctypes.c_int), ("intra_filter", ctypes.c_int), ("inter_filter", ctypes.c_int),
-                ("wlt_depth", ctypes.c_int)]
+                ("wlt_depth", ctypes.c_int), ("field_coding", ctypes.c_int), ("top_field_first", ctypes.c_int)]
 
 
 class PictureInfo(ctypes.Structure):
@@ -74,7 +74,8 @@ class SequenceEncoder:
         self.depth8 = p.luma_depth <= 8 and p.chroma_depth <= 8
         xs = 0 if p.cformat == 0 else 1
         ys = 1 if p.cformat == 2 else 0
-        self.shapes = [(p.height, p.width), (p.height >> ys, p.width >> xs), (p.height >> ys, p.width >> xs)]
+        h = p.height // 2 if p.field_coding else p.height  # a picture is a field when field coding
+        self.shapes = [(h, p.width), (h >> ys, p.width >> xs), (h >> ys, p.width >> xs)]
 
     def close(self):
         if self.handle:

@@ -401,8 +401,15 @@ int dgpu_dequantise_batch(int n, const int* intra, const int* depth, const int32
  * the coefficients and motion data, and therefore the adaptation of the entropy-correction
  * factors (EntropyCorrector::Update, common.cpp:134-151), which dgpu_encoder_code_next
  * takes as an input (NULL: the initial factors of EntropyCorrector::Init,
- * common.cpp:79-131).  Not supported: rate control (trate), prefilters, field coding,
- * lossless coding, num_l1 < 0.
+ * common.cpp:79-131).  Not supported: rate control (trate), prefilters, lossless coding,
+ * num_l1 < 0.
+ *
+ * Field coding (field_coding = 1; FieldSequenceCompressor, seq_compress.cpp:697-892): each
+ * dgpu_encoder_load takes an interlaced frame and makes two pictures of half its height, the
+ * fields (StreamFieldInput::ReadFieldComponent, pic_io.cpp:464-530: the first field the even
+ * rows when top_field_first, else the odd ones), numbered 2n and 2n + 1; their types,
+ * references and coding order follow the field GOP, and every result is per field.  The frame
+ * height must be a multiple of 4 for 4:2:0 (of 2 otherwise).
  *
  * Use: dgpu_encoder_create; dgpu_encoder_load for each picture in display order;
  * dgpu_encoder_code_next until it returns 0 (it needs the same look-ahead as the reference:
@@ -421,6 +428,9 @@ typedef struct {
     int xblen, yblen, xbsep, ybsep; /* luma OBMC block length and separation */
     int mv_precision;             /* 1 half, 2 quarter, 3 eighth pel */
     int intra_filter, inter_filter, wlt_depth; /* WltFilter numbering, transform depth */
+    int field_coding;             /* 1: interlaced frames coded as two field pictures each
+                                     (FieldSequenceCompressor); height is the frame's */
+    int top_field_first;          /* with field_coding: the first field holds the even rows */
 } dgpu_encoder_params;
 
 typedef struct {

@@ -405,7 +405,7 @@ class RefEncParams(ctypes.Structure):
                 ("num_l1", ctypes.c_int), ("cpd", ctypes.c_float), ("xblen", ctypes.c_int),
                 ("yblen", ctypes.c_int), ("xbsep", ctypes.c_int), ("ybsep", ctypes.c_int),
                 ("mv_precision", ctypes.c_int), ("intra_filter", ctypes.c_int), ("inter_filter", ctypes.c_int),
-                ("wlt_depth", ctypes.c_int), ("use_vlc", ctypes.c_int)]
+                ("wlt_depth", ctypes.c_int), ("use_vlc", ctypes.c_int), ("field_coding", ctypes.c_int)]
 
 
 def reference_encode(cfg, frames, freeze=True, path=REF_SO):
@@ -417,12 +417,15 @@ def reference_encode(cfg, frames, freeze=True, path=REF_SO):
     n = len(frames)
     flat = np.concatenate([np.concatenate([np.ascontiguousarray(c, np.uint8).ravel() for c in f]) for f in frames])
     recon = np.zeros_like(flat)
-    ptype = np.zeros(n, np.int32)
+    fields = bool(cfg.get("field_coding", 0))
+    npics = 2 * n if fields else n
+    ptype = np.zeros(npics, np.int32)
     nbytes = ctypes.c_longlong(0)
     rc = lib.ref_encode_sequence(ctypes.byref(p), n, _p(flat), int(freeze), _p(recon), _p(ptype), ctypes.byref(nbytes))
     if rc:
         raise ValueError("ref_encode_sequence failed")
-    return _split_frames(recon, [c.shape for c in frames[0]], n), ptype, nbytes.value
+    shapes = [(c.shape[0] // 2, c.shape[1]) if fields else c.shape for c in frames[0]]
+    return _split_frames(recon, shapes, npics), ptype, nbytes.value
 
 
 def _split_frames(flat, shapes, n):

@@ -52,11 +52,14 @@ struct RefEncParams {
     int mv_precision;
     int intra_filter, inter_filter, wlt_depth;
     int use_vlc;        // 1: variable-length coefficient coding (-use_vlc), 0: arithmetic coding
+    int field_coding;   // 1: interlaced frames coded as fields (picture_coding_mode 1)
 };
 
 // Encodes nframes 8-bit planar frames (Y then U then V, dense, frame after frame).
 // recon (nframes frames, same layout) receives the locally decoded pictures by picture
-// number; ptype[pnum] = 1 for intra, 0 for inter, -1 if never returned; *bytes = total
+// number (field coding: 2 nframes fields of half height, each Y then U then V, dense);
+// ptype[pnum] = 1 for intra, 0 for inter, -1 if never returned, -2 for a first field (the
+// encoder reports a frame's type by its second field); *bytes = total
 // bitstream bytes.  freeze: keep the initial entropy-correction factors.
 // Returns 0, or -1 on an encoder failure.
 }  // extern "C"
@@ -91,7 +94,7 @@ int encode_impl(const RefEncParams* p, int nframes, const unsigned char* frames,
     ctx.enc_params.trate = 0;
     ctx.enc_params.lossless = 0;
     ctx.enc_params.full_search = 0;
-    ctx.enc_params.picture_coding_mode = 0;
+    ctx.enc_params.picture_coding_mode = p->field_coding ? 1 : 0;
     ctx.enc_params.prefilter = NO_PF;
     ctx.instr_flag = 0;
     ctx.decode_flag = 1;
@@ -104,14 +107,18 @@ int encode_impl(const RefEncParams* p, int nframes, const unsigned char* frames,
     const int cw = p->cformat == 0 ? p->width : p->width / 2;
     const int ch = p->cformat == 2 ? p->height / 2 : p->height;
     const size_t fsize = (size_t)p->width * p->height + 2 * (size_t)cw * ch;
-    for (int i = 0; i < nframes; ++i) ptype[i] = -1;
+    // pictures: frames, or two fields per frame; top field first as the video format's
+    // defaults set it (the context's field is not read back by the encoder)
+    const int npics = p->field_coding ? 2 * nframes : nframes;
+    const bool tff = ctx.src_params.topfieldfirst != 0;
+    for (int i = 0; i < npics; ++i) ptype[i] = -1;
     std::vector<unsigned char> out(1 << 24);
     long long total = 0;
     int rc = 0;
     // every output call either codes a picture or reports BUFFER / EOS, so a bounded
     // number of calls per loaded frame always suffices
     auto drain = [&](bool to_eos) -> int {
-        for (int guard = 0; guard < 4 * nframes + 64; ++guard) {
+        for (int guard = 0; guard < 4 * npics + 64; ++guard) {
             enc->enc_buf.buffer = out.data();
             enc->enc_buf.size = (int)out.size();
             const dirac_encoder_state_t st = dirac_encoder_output(enc);
@@ -122,12 +129,30 @@ int encode_impl(const RefEncParams* p, int nframes, const unsigned char* frames,
             }
             if (enc->decoded_frame_avail) {
                 const int pn = enc->dec_pparams.pnum;
-                if (pn >= 0 && pn < nframes) {
+                if (pn >= 0 && pn < npics && !p->field_coding) {
                     unsigned char* dst = recon + (size_t)pn * fsize;
                     std::memcpy(dst, enc->dec_buf.buf[0], (size_t)p->width * p->height);
                     std::memcpy(dst + (size_t)p->width * p->height, enc->dec_buf.buf[1], (size_t)cw * ch);
                     std::memcpy(dst + (size_t)p->width * p->height + (size_t)cw * ch, enc->dec_buf.buf[2],
                                 (size_t)cw * ch);
+                    ptype[pn] = enc->dec_pparams.ptype == INTRA_PICTURE ? 1 : 0;
+                } else if (pn >= 1 && pn < npics && pn % 2 == 1) {
+                    // the API reports a frame once its second field is written
+                    // (StreamFieldOutput::WriteFieldComponent, pic_io.cpp:150-240): the output
+                    // frame then holds fields pn - 1 and pn in alternate rows
+                    for (int f = pn - 1; f <= pn; ++f) {
+                        const int row0 = tff ? (f % 2) : 1 - (f % 2);
+                        unsigned char* dst = recon + (size_t)f * (fsize / 2);
+                        const int ws[3] = {p->width, cw, cw}, hs[3] = {p->height, ch, ch};
+                        for (int c = 0; c < 3; ++c) {
+                            for (int y = 0; y < hs[c] / 2; ++y)
+                                std::memcpy(dst + (size_t)y * ws[c],
+                                            enc->dec_buf.buf[c] + (size_t)(2 * y + row0) * ws[c], (size_t)ws[c]);
+                            dst += (size_t)ws[c] * (hs[c] / 2);
+                        }
+                    }
+                    // only the second field's type is reported
+                    ptype[pn - 1] = -2;
                     ptype[pn] = enc->dec_pparams.ptype == INTRA_PICTURE ? 1 : 0;
                 }
             }

@@ -3,7 +3,8 @@
 Needs oracle/_ref/libdirac_ref.so (the reference's own C++, plain-C build, compiled from
 its sources by `make -C oracle`).  Inputs are seeded, so re-running reproduces the files.
 
-    python tests/golden/make_golden.py [dwt convert mc me quant encode decode adaptive bands prefilter hd1080 uhd]
+    python tests/golden/make_golden.py [dwt convert mc me quant encode decode adaptive bands prefilter hd1080 uhd
+                                        fields]
 """
 import os
 import sys
@@ -311,6 +312,53 @@ def encode_cases():
     return out
 
 
+# Field coding (FieldSequenceCompressor): (name, w, h, frames, seed A, seed B, switch frame or
+# None, n_rects, vmax, qf, num_l1, intra filter, inter filter, depth, xblen, yblen, xbsep, ybsep,
+# precision, video format).  The CIF preset puts the top field first, the custom one (0) the
+# bottom field; the third sequence switches content to trigger cut detection and the switch to
+# P-only sub-groups on fields.
+FIELD_CASES = [
+    ("field_cif_tff", 352, 288, 8, 31, None, None, 8, 8, 7.0, 19, 1, 0, 4, 12, 12, 8, 8, 2, 4),
+    ("field_bff", 176, 144, 10, 32, None, None, 6, 6, 5.0, 2, 6, 2, 3, 16, 16, 12, 12, 3, 0),
+    ("field_cut", 176, 144, 12, 41, 42, 5, 4, 4, 7.0, 19, 1, 0, 3, 12, 12, 8, 8, 2, 0),
+]
+
+
+# top field first as the reference's video-format presets set it (video_format_defaults.cpp:
+# true by default, false for the custom and 525-line formats)
+TOP_FIELD_FIRST = {0: 0, 4: 1}
+
+
+def field_inputs(case):
+    """8-bit frames of one FIELD_CASES entry and its RefEncParams fields (field coding)."""
+    seq, cfg = encode_inputs(case[:19])
+    cfg.update(video_format=case[19], field_coding=1)
+    return seq, cfg
+
+
+def field_cases():
+    """The reference encoder in field-coding mode through its public API: CRC-32 of every
+    locally decoded field's planes it returns (all but the last frame's two) and the types it
+    reports (-2 for first fields, -1 for fields not returned), with the initial
+    entropy-correction factors kept and with the stock adaptive ones."""
+    import zlib
+
+    from oracle import reference_encode
+
+    out = {}
+    for case in FIELD_CASES:
+        seq, cfg = field_inputs(case)
+        for tag, freeze in (("", True), ("_adaptive", False)):
+            rec, ptype, _ = reference_encode(cfg, seq, freeze=freeze)
+            # the encoder's API shows every frame but the sequence's last: its fields stay -1
+            if (ptype[:-2] == -1).any():
+                raise RuntimeError(f"{case[0]}: a field was never returned")
+            out[case[0] + tag + "_crc"] = np.array(
+                [[zlib.crc32(np.ascontiguousarray(p).tobytes()) for p in f] for f in rec], np.uint32)
+            out[case[0] + tag + "_ptype"] = ptype
+    return out
+
+
 def decode_cases():
     """The reference decoder run through its public API on the reference encoder's bitstream
     of each ENCODE_CASES sequence: CRC-32 of every decoded plane by frame number, and the
@@ -441,13 +489,13 @@ def main(argv=None):
     """Writes the named fixtures (default: all)."""
     names = (argv if argv is not None else sys.argv[1:]) or ["dwt", "convert", "mc", "me", "quant", "encode",
                                                               "decode", "adaptive", "bands", "prefilter",
-                                                              "hd1080", "uhd"]
+                                                              "hd1080", "uhd", "fields"]
     ref = Reference()
     makers = {"dwt": lambda: dwt_cases(ref), "convert": lambda: conv_cases(ref), "mc": lambda: mc_cases(ref),
               "me": lambda: me_cases(ref), "quant": lambda: quant_cases(ref), "encode": encode_cases,
               "decode": decode_cases, "adaptive": adaptive_cases, "bands": lambda: band_cases(ref),
               "prefilter": lambda: prefilter_cases(ref), "hd1080": hd_cases,
-              "uhd": lambda: uhd_cases(ref)}
+              "uhd": lambda: uhd_cases(ref), "fields": field_cases}
     for n in names:
         np.savez_compressed(os.path.join(HERE, n + ".npz"), **makers[n]())
     print("wrote " + ", ".join(n + ".npz" for n in names))
