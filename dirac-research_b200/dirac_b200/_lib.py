@@ -160,6 +160,8 @@ SIGNATURES = {
     "dgpu_decode_bands_host": (
         c_int, [c_int, P_int, P_int, P_int, P_int, P_int, c_void_p, c_size_t, P_int, c_int, P_void, c_void_p],
     ),
+    "dgpu_code_bands_vlc": (c_int, [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                    c_void_p, c_size_t, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
     "dgpu_entropy_init": (c_int, [c_int, c_void_p]),
     "dgpu_entropy_factors": (c_int, [c_int, c_void_p, c_int, c_int, c_void_p]),
     "dgpu_entropy_update": (c_int, [c_int, c_void_p, c_int, c_int, c_int, P_int, P_int, P_int]),

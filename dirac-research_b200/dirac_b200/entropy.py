@@ -57,6 +57,43 @@ def code_bands(intra, depth, qindex, bands, ncb, cb_skip, vlc=False):
     return out[:int(nbytes.sum())].copy(), per
 
 
+def code_bands_vlc_device(depth, qindex, bands, ncb, cb_skip, stream=None):
+    """dgpu_code_bands_vlc: the variable-length form of code_bands from CUDA int32 tensors
+    (qindex: list of [ch][cw] tensors); bands, ncb, cb_skip as for code_bands.  Returns (data
+    bytes, band_bytes per component, exact bit counts per component)."""
+    import torch
+
+    lib = _lib.load()
+    n = len(qindex)
+    depth = list(depth) if hasattr(depth, "__len__") else [int(depth)] * n
+    for t in qindex:
+        if t.dtype != torch.int32 or not t.is_cuda or not t.is_contiguous():
+            raise TypeError("expected contiguous int32 CUDA tensors")
+    b = [np.asarray(x, np.int32).reshape(3 * d + 1, -1) for x, d in zip(bands, depth)]
+    bs = np.ascontiguousarray(np.concatenate([x[:, 1] for x in b]), np.int32)
+    nc = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32).ravel() for x in ncb]), np.int32)
+    cbs = np.ascontiguousarray(np.concatenate([np.asarray(x, np.uint8).ravel() for x in cb_skip]), np.uint8)
+    nbytes = np.zeros(bs.size, np.int32)
+    nbits = np.zeros(bs.size, np.int64)
+    st = (stream or torch.cuda.current_stream()).cuda_stream
+    args = [n, _lib.int_array(depth), _lib.ptr_array([t.data_ptr() for t in qindex]),
+            _lib.int_array([t.shape[1] for t in qindex]), _lib.int_array([t.shape[0] for t in qindex]),
+            nc.ctypes.data, bs.ctypes.data, cbs.ctypes.data]
+    _lib.check(lib.dgpu_code_bands_vlc(*args, None, 0, nbytes.ctypes.data, nbits.ctypes.data, None, 0, st),
+               "dgpu_code_bands_vlc")
+    total = int(nbytes.sum())
+    out = torch.empty(max(4, (total + 3) // 4 * 4), dtype=torch.uint8, device="cuda")
+    _lib.check(lib.dgpu_code_bands_vlc(*args, out.data_ptr(), out.numel(), nbytes.ctypes.data, nbits.ctypes.data,
+                                       None, 0, st), "dgpu_code_bands_vlc")
+    data = out[:total].cpu().numpy()
+    per, bits_per, k = [], [], 0
+    for d in depth:
+        per.append(nbytes[k:k + 3 * d + 1].copy())
+        bits_per.append(nbits[k:k + 3 * d + 1].copy())
+        k += 3 * d + 1
+    return data, per, bits_per
+
+
 def decode_bands(depth, shapes, band_skip, ncb, data, band_bytes, vlc=False):
     """dgpu_decode_bands_host: components' signed quantised indices from their coded band data.
     depth: one value or one per component; shapes: (ch, cw) per component; band_skip, ncb and

@@ -676,6 +676,19 @@ int dgpu_code_bands_vlc_host(int n, const int* intra, const int* depth, const in
                              const int* cw, const int* ch, const int* band_ncb, const int* band_qidx,
                              const int* band_skip, const uint8_t* cb_skip, uint8_t* out, size_t out_cap,
                              int* band_bytes, long long* band_bits);
+/* The variable-length form on the device: the same bytes as dgpu_code_bands_vlc_host from
+ * device-resident indices (qindex[c] device, dense cw[c] x ch[c] int32); band_ncb,
+ * band_skip and cb_skip are host arrays as there, out device memory, 4-byte aligned, holding
+ * the data rounded up to 4 bytes (DGPU_ERR_SIZE otherwise, band_bytes filled).  One pass sums
+ * each code block's code lengths, a second places every coefficient's code at its offset
+ * (the codes are independent).  band_bytes / band_bits (host) receive the bands' byte and
+ * exact bit counts; synchronises the stream between the passes (the sizes come back to the
+ * host), the writes then queued on it.  scratch: NULL or at least 64 bytes per code block
+ * plus 512. */
+int dgpu_code_bands_vlc(int n, const int* depth, const int32_t* const* qindex, const int* cw, const int* ch,
+                        const int* band_ncb, const int* band_skip, const uint8_t* cb_skip, uint8_t* out,
+                        size_t out_cap, int* band_bytes, long long* band_bits, void* scratch,
+                        size_t scratch_bytes, void* stream);
 /* The decoding side (the band decoders' symbol decoding: band_codec_template.h:204-357,
  * 500-557 over ArithCodecBase's decoder, arith_codec.h:200-250, arith_codec.cpp:132-165, or
  * the VLC adapter when vlc != 0): from the coded bands' data (the layout dgpu_code_bands_host
