@@ -42,6 +42,7 @@ import numpy as np
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -81,6 +82,9 @@ def parse_args():
                     help="resident CTAs per SM of the motion-estimation wavefront kernels (1-8)")
     ap.add_argument("--me-groups", type=int, default=3,
                     help="encoder groups the batched form's sequences are split into (run concurrently)")
+    ap.add_argument("--double-buffer", type=int, default=0,
+                    help="1: each group alternates two sets of sequences, one set's estimation running "
+                         "while the other set is coded (measured slower: the sets contend for the device)")
     ap.add_argument("--serving-rate", type=float, default=40.0, help="stream arrivals per second (Poisson)")
     ap.add_argument("--serving-seconds", type=float, default=6.0,
                     help="length of the serving-loop run reported under 'serving' (0: skip)")
@@ -757,6 +761,7 @@ def main():
         return pools[key]
 
     group_phases = {}  # host seconds per phase, summed over the groups of the last timed() run
+    phase_lock = threading.Lock()
 
     def timed(lanes, src, steps, with_read=False, groups=None, adaptive=False):
         """Device time (ms) of `steps` sequence encodes on every lane, the lanes running
@@ -788,19 +793,78 @@ def main():
             for _ in range(steps):
                 code(ln, False)
 
+        def add_phase(k, dt):
+            with phase_lock:
+                group_phases[k] = group_phases.get(k, 0.0) + dt
+
         def run_group(gi):
-            g, gl = groups[gi]
-            ex = pool(("group", gi, len(gl)), len(gl))
-            for _ in range(steps):
-                t0 = time.perf_counter()
-                list(ex.map(lambda ln: ln.load(src), gl))
-                t1 = time.perf_counter()
-                g.estimate()
-                t2 = time.perf_counter()
-                list(ex.map(lambda ln: code(ln, True), gl))
-                t3 = time.perf_counter()
-                for k, dt in (("load", t1 - t0), ("estimate", t2 - t1), ("code", t3 - t2)):
-                    group_phases[k] = group_phases.get(k, 0.0) + dt
+            slot = groups[gi]
+            if len(slot) == 1:
+                g, gl = slot[0]
+                ex = pool(("group", gi, 0, len(gl)), len(gl))
+                for _ in range(steps):
+                    t0 = time.perf_counter()
+                    list(ex.map(lambda ln: ln.load(src), gl))
+                    t1 = time.perf_counter()
+                    g.estimate()
+                    t2 = time.perf_counter()
+                    list(ex.map(lambda ln: code(ln, True), gl))
+                    t3 = time.perf_counter()
+                    for k, dt in (("load", t1 - t0), ("estimate", t2 - t1), ("code", t3 - t2)):
+                        add_phase(k, dt)
+                return
+            # two sets alternate: step k runs on set k % 2; the estimation of step k + 1 (the
+            # other set) runs while step k is coded, and a set is loaded again only after its
+            # previous step's coding is done
+            est_done = [threading.Event() for _ in range(steps)]
+            code_done = [threading.Event() for _ in range(steps)]
+            failed = []
+
+            def estimator():
+                try:
+                    for k in range(steps):
+                        g, gl = slot[k % 2]
+                        if k >= 2:
+                            code_done[k - 2].wait()
+                            if failed:
+                                return
+                        ex = pool(("load", gi, k % 2, len(gl)), len(gl))
+                        t0 = time.perf_counter()
+                        list(ex.map(lambda ln: ln.load(src), gl))
+                        t1 = time.perf_counter()
+                        g.estimate()
+                        add_phase("load", t1 - t0)
+                        add_phase("estimate", time.perf_counter() - t1)
+                        est_done[k].set()
+                except BaseException as e:  # the coding thread must not wait for good
+                    failed.append(e)
+                    for ev in est_done:
+                        ev.set()
+
+            def coder():
+                try:
+                    for k in range(steps):
+                        est_done[k].wait()
+                        if failed:
+                            return
+                        g, gl = slot[k % 2]
+                        ex = pool(("code", gi, k % 2, len(gl)), len(gl))
+                        t0 = time.perf_counter()
+                        list(ex.map(lambda ln: code(ln, True), gl))
+                        add_phase("code", time.perf_counter() - t0)
+                        code_done[k].set()
+                except BaseException as e:
+                    failed.append(e)
+                    for ev in code_done:
+                        ev.set()
+
+            th = [threading.Thread(target=estimator), threading.Thread(target=coder)]
+            for t in th:
+                t.start()
+            for t in th:
+                t.join()
+            if failed:
+                raise failed[0]
 
         if groups is not None:
             list(pool(("groups", len(groups)), len(groups)).map(run_group, range(len(groups))))
@@ -819,18 +883,21 @@ def main():
 
     if lib.dgpu_me_set_occupancy(args.me_occupancy):
         raise ValueError("--me-occupancy must be 1..8")
-    lanes = [Lane() for _ in range(args.streams)]
+    nsets = 2 if args.double_buffer else 1
+    lanes = [Lane() for _ in range(args.streams * nsets)]
+    sets = [lanes[i * args.streams:(i + 1) * args.streams] for i in range(nsets)]
+    lanes_a = sets[0]  # the forms that run one set of sequences
     plain = lanes[0]
     # the batched form: the lanes split into --me-groups encoder groups that run concurrently
-    ng = max(1, min(args.me_groups, len(lanes)))
-    per = (len(lanes) + ng - 1) // ng
-    groups = [(E.EncoderGroup([ln.enc for ln in lanes[k:k + per]]), lanes[k:k + per])
-              for k in range(0, len(lanes), per)]
+    ng = max(1, min(args.me_groups, args.streams))
+    per = (args.streams + ng - 1) // ng
+    groups = [[(E.EncoderGroup([ln.enc for ln in st[k:k + per]]), st[k:k + per]) for st in sets]
+              for k in range(0, args.streams, per)]
 
     # ---- warm-up: every lane, both input forms ------------------------------------------------
     for _ in range(args.warmup):
-        timed(lanes, dev_frames, 1, groups=groups)
-    timed(lanes, pinned_np, 1, groups=groups, adaptive=True)
+        timed(lanes, dev_frames, nsets, groups=groups)  # every set
+    timed(lanes, pinned_np, nsets, groups=groups, adaptive=True)
 
     # ---- the integer roofline and the motion-estimation kernels' algorithmic operations -------
     rate = ctypes.c_double(0.0)
@@ -858,7 +925,7 @@ def main():
     lib.dgpu_me_profile(0, me_ms, me_launches)
     launches = lib.dgpu_launch_count() - launches0
     clk = clocks.stop()
-    frames_per_step = args.frames * len(lanes)
+    frames_per_step = args.frames * args.streams  # one set of sequences per step
     ms_per_step = ms / args.steps
     value = whole_job_rate(world, frames_per_step, args.steps, ms)
 
@@ -871,7 +938,7 @@ def main():
     ems = timed(lanes, pinned_np, args.steps, groups=groups, adaptive=True)
     ru1, w1 = resource.getrusage(resource.RUSAGE_SELF), time.perf_counter()
     cpu_s = (ru1.ru_utime - ru0.ru_utime) + (ru1.ru_stime - ru0.ru_stime)
-    h2d = sum(p.nbytes for fr in pinned_np for p in fr) * len(lanes)
+    h2d = sum(p.nbytes for fr in pinned_np for p in fr) * args.streams
     e2e = {"value": whole_job_rate(world, frames_per_step, args.steps, ems), "unit": "frames/s",
            "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": sum(ln.d2h + ln.coder.d2h_bytes for ln in lanes) // args.steps,
@@ -888,16 +955,16 @@ def main():
                "form": "initial entropy-correction factors, no host coding"}
 
     # ---- batched form without the group: concurrent sequences, each estimating alone -----------
-    sms = timed(lanes, dev_frames, args.steps)
+    sms = timed(lanes_a, dev_frames, args.steps)
     streams_only = {"value": whole_job_rate(world, frames_per_step, args.steps, sms), "unit": "frames/s",
                     "ms_per_step": sms / args.steps,
-                    "form": f"{len(lanes)} concurrent sequences, each with its own motion-estimation launches"}
-    g_all = E.EncoderGroup([ln.enc for ln in lanes])
-    oms = timed(lanes, dev_frames, args.steps, groups=[(g_all, lanes)])
+                    "form": f"{len(lanes_a)} concurrent sequences, each with its own motion-estimation launches"}
+    g_all = E.EncoderGroup([ln.enc for ln in lanes_a])
+    oms = timed(lanes_a, dev_frames, args.steps, groups=[[(g_all, lanes_a)]])
     g_all.close()
     one_group = {"value": whole_job_rate(world, frames_per_step, args.steps, oms), "unit": "frames/s",
                  "ms_per_step": oms / args.steps,
-                 "form": f"{len(lanes)} sequences in one encoder group (estimation, then coding)"}
+                 "form": f"{len(lanes_a)} sequences in one encoder group (estimation, then coding)"}
 
     # ---- plain form: one sequence at a time ----------------------------------------------------
     pms = timed([plain], dev_frames, args.steps)
@@ -993,8 +1060,9 @@ def main():
     decoding = None
     if args.decode and world == 1:
         decoding = run_decoding(args, enc, infos, peak, cpu_decode)
-    for g, _ in groups:
-        g.close()
+    for slot in groups:
+        for g, _ in slot:
+            g.close()
     for ln in lanes:
         ln.enc.close()
     for ex in pools.values():
@@ -1012,14 +1080,14 @@ def main():
 
         cfg = {"seconds": args.serving_seconds, "arrivals_per_s": args.serving_rate, "fps_per_stream": 50,
                "resolutions": "352x288, 720x576, 1280x720, 1920x1080, 3840x2160 (4:2:0, 8- or 10-bit)",
-               "frames_per_stream": "8-64", "budget_gb": 96, "max_active": 48, "max_load": 16,
+               "frames_per_stream": "8-64", "budget_gb": 80, "max_active": 40, "max_load": 16,
                "input": "per resolution and depth a pool of synthetic frames (16; 8 at 3840x2160), each stream "
                         "cycling through its pool from a random offset"}
         try:
             reqs = S.make_requests(args.serving_seconds, args.serving_rate, ["cif", "576", "720", "1080", "2160"], 8, 64,
                                    seed=7,
                                    depths=(8, 10))
-            serving = S.ServingLoop(int(96e9), max_active=48, frame_interval=1.0 / 50, batch_me=True,
+            serving = S.ServingLoop(int(80e9), max_active=40, frame_interval=1.0 / 50, batch_me=True,
                                     max_load=16).run(reqs)
         except Exception as e:  # the serving leg must not cost the bench line; its failure is reported
             serving = {"error": repr(e)}
@@ -1031,9 +1099,11 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
                 "config": {"workload": workload_name(args.frames), "frames_per_step": frames_per_step,
                            "global_batch": world * frames_per_step, "parallelism": f"replicas{world}",
-                           "form": f"batched: {len(lanes)} sequences per GPU in {len(groups)} encoder groups "
+                           "form": f"batched: {args.streams} sequences per step in {len(groups)} encoder groups "
                                    "running concurrently; each group's motion estimation in one batched launch, "
-                                   "each sequence's coding on its own stream and host thread",
+                                   "each sequence's coding on its own stream and host thread"
+                                   + ("; each group alternates two sets of sequences, one set's estimation "
+                                      "running while the other set is coded" if nsets == 2 else ""),
                            "me_ctas_per_sm": args.me_occupancy,
                            "l2": "inputs and working set larger than L2 (no flush needed)"},
                 "e2e": e2e, "cpu_baseline": cpu_baseline, "parity_vs_reference": parity, "plain": plain_line,
