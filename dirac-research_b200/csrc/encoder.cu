@@ -1302,7 +1302,8 @@ extern "C" int dgpu_encoder_code_adaptive(void* enc, float* ecf_state, int max_p
             const int r = f.get();
             if (rc == DGPU_OK && r != DGPU_OK) rc = r;
         }
-    if (rc < 0) return rc;
+    // a failure leaves pictures finished but not coded: sticky until dgpu_encoder_reset
+    if (rc < 0) return sticky(E, rc);
     size_t at = 0;
     for (const auto& C : done) at += C->data.size();
     E->adaptive_data.resize(at);

@@ -632,7 +632,8 @@ int dgpu_encoders_estimate(void* const* encoders, int n, void* workspace, size_t
  * length.  The encoder keeps the data until its next such call: when out is smaller the call
  * returns DGPU_ERR_SIZE after coding every picture, and dgpu_encoder_adaptive_data copies the
  * data once the caller has room.  d2h_bytes (optional): the device-to-host bytes copied
- * (indices and motion data); npictures: the count. */
+ * (indices and motion data); npictures: the count.  A failure is sticky, as for
+ * dgpu_encoder_code_next. */
 int dgpu_encoder_code_adaptive(void* encoder, float* ecf_state, int max_pictures, dgpu_picture_info* infos,
                                uint8_t* out, size_t out_cap, size_t* out_bytes, int* band_bytes,
                                size_t* d2h_bytes, int* npictures);
