@@ -423,10 +423,16 @@ def run_decoding(args, enc, infos, peak, cpu_decode=None):
     dev, host, want, pnums, coded = [], [], [], [], []
     keep = []
     h2d = 0
+    n16 = 0  # pictures sent with int16 indices
     for info in infos:
         pn = info["pnum"]
         pnums.append(pn)
         q = [enc.read(pn, E.QINDEX, c).reshape(shapes[c]) for c in range(3)]
+        # a picture whose indices all fit 16 bits goes as int16 (index_bits 16): half the bytes
+        qin = q
+        if all(int(np.abs(a).max()) <= 32767 for a in q):
+            qin = [a.astype(np.int16) for a in q]
+            n16 += 1
         bands = [enc.read(pn, E.BANDS, c) for c in range(3)]
         cbs = np.concatenate([enc.read(pn, E.CBSKIP, c) for c in range(3)])
         refs = [] if info["intra"] else [x for x in (info["ref1"], info["ref2"]) if x >= 0]
@@ -438,7 +444,7 @@ def run_decoding(args, enc, infos, peak, cpu_decode=None):
         want.append([enc.read(pn, E.OUTPUT, c) for c in range(3)])
         coded.append((info["intra"], q, bands, [enc.read(pn, E.CBSKIP, c) for c in range(3)]))
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
-        hq, hc = [pin(a) for a in q], pin(cbs)
+        hq, hc = [pin(a) for a in qin], pin(cbs)
         hm = None if mot is None else {"mv": [pin(v) for v in mot["mv"]],
                                        **{k: pin(mot[k]) for k in ("mode", "dc", "split")}}
         keep += [hq, hc, hm]
@@ -489,7 +495,7 @@ def run_decoding(args, enc, infos, peak, cpu_decode=None):
     launches = (lib.dgpu_launch_count() - launches0) // args.steps
     ems = timed(host, args.steps, read=True)
     matches = all(np.array_equal(out_host[k][c].numpy(), want[k][c]) for k in range(len(infos)) for c in range(3))
-    alg = decode_bytes(PARAMS, infos)
+    alg = decode_bytes(PARAMS, infos, n16)
     total_alg = sum(alg.values())
     achieved = total_alg * args.steps / (ms / 1000.0) / 1e9
     dec.close()
@@ -535,13 +541,14 @@ def run_decoding(args, enc, infos, peak, cpu_decode=None):
             "e2e": {"value": len(infos) * args.steps / (ems / 1000.0), "unit": "frames/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "output_matches_encoder": bool(matches), "gpu_launches_per_step": launches,
+            "int16_index_pictures": n16,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
                          "algorithmic_bytes_per_step": alg},
             "cpu_baseline": baseline, "cpu_port": port, "host_band_coding": coding,
             "workload": "decode of the plain form's coded 1920x1080 4:2:0 8-bit 32-picture sequence from its "
-                        "quantised indices (int32), band and code-block choices and motion data; output 8-bit "
-                        "samples"}
+                        "quantised indices (int16 where a picture's indices fit, else int32), band and code-block "
+                        "choices and motion data; output 8-bit samples"}
 
 
 def run_leg(args):
@@ -596,7 +603,10 @@ def run_leg(args):
             mot = {"mv": [torch.from_numpy(mv[k].copy()).cuda() for k in range(len(refs))],
                    **{k: torch.from_numpy(enc.read(pn, w)).cuda() for k, w in (("mode", E.MODE), ("dc", E.DC),
                                                                                  ("split", E.SPLIT))}}
-        q = [torch.from_numpy(enc.read(pn, E.QINDEX, c).reshape(shapes[c])).cuda() for c in range(3)]
+        q = [enc.read(pn, E.QINDEX, c).reshape(shapes[c]) for c in range(3)]
+        if all(int(np.abs(a).max()) <= 32767 for a in q):  # int16 indices, as the decoding leg sends them
+            q = [a.astype(np.int16) for a in q]
+        q = [torch.from_numpy(a).cuda() for a in q]
         cbs = torch.from_numpy(np.concatenate([enc.read(pn, E.CBSKIP, c) for c in range(3)])).cuda()
         inputs.append((pn, dec.prepare(pn, info["intra"], refs, info["filter"], q,
                                        [enc.read(pn, E.BANDS, c) for c in range(3)], cbs, mot)))

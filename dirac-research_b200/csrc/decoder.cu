@@ -232,6 +232,8 @@ extern "C" int dgpu_decoder_decode(void* dec, const dgpu_decode_input* in) {
     }
     // intra pictures always carry coefficients (picture_decompress.cpp:137-142)
     if (I.intra && I.zero_residual) return DGPU_ERR_ARG;
+    if (I.index_bits != 0 && I.index_bits != 16 && I.index_bits != 32) return DGPU_ERR_ARG;
+    const bool idx16 = I.index_bits == 16;
     if (!I.zero_residual && (!I.band_qidx || !I.band_skip || !I.cb_skip || !I.qindex[0] || !I.qindex[1] ||
                              !I.qindex[2]))
         return DGPU_ERR_ARG;
@@ -248,11 +250,13 @@ extern "C" int dgpu_decoder_decode(void* dec, const dgpu_decode_input* in) {
     int rc;
     // 1. residue: dequantisation and inverse transform, or zero samples
     if (!I.zero_residual) {
-        const int32_t* q[3];
+        // int16 indices (index_bits 16) occupy the first half of the int32 staging area
+        const size_t isz = idx16 ? 2 : 4;
+        const void* q[3];
         const uint8_t* cb = I.cb_skip;
         if (I.on_host) {
             for (int c = 0; c < 3; ++c) {
-                DGPU_CHECK_CUDA(cudaMemcpyAsync(D->s_q[c], I.qindex[c], (size_t)D->pw[c] * D->ph[c] * 4, h2d, st));
+                DGPU_CHECK_CUDA(cudaMemcpyAsync(D->s_q[c], I.qindex[c], (size_t)D->pw[c] * D->ph[c] * isz, h2d, st));
                 q[c] = D->s_q[c];
             }
             DGPU_CHECK_CUDA(cudaMemcpyAsync(D->s_cb, I.cb_skip, (size_t)3 * D->ncb_comp, h2d, st));
@@ -263,8 +267,17 @@ extern "C" int dgpu_decoder_decode(void* dec, const dgpu_decode_input* in) {
         const int intra[3] = {I.intra ? 1 : 0, I.intra ? 1 : 0, I.intra ? 1 : 0};
         const int depth[3] = {D->P.wlt_depth, D->P.wlt_depth, D->P.wlt_depth};
         int32_t* coeff[3] = {s.coeff[0], s.coeff[1], s.coeff[2]};
-        rc = dgpu_dequantise_batch(3, intra, depth, q, coeff, D->pw, D->ph, D->ncb.data(), I.band_qidx, I.band_skip,
-                                   cb, st);
+        if (idx16) {
+            const int16_t* q16[3] = {static_cast<const int16_t*>(q[0]), static_cast<const int16_t*>(q[1]),
+                                     static_cast<const int16_t*>(q[2])};
+            rc = dgpu_dequantise_batch16(3, intra, depth, q16, coeff, D->pw, D->ph, D->ncb.data(), I.band_qidx,
+                                         I.band_skip, cb, st);
+        } else {
+            const int32_t* q32[3] = {static_cast<const int32_t*>(q[0]), static_cast<const int32_t*>(q[1]),
+                                     static_cast<const int32_t*>(q[2])};
+            rc = dgpu_dequantise_batch(3, intra, depth, q32, coeff, D->pw, D->ph, D->ncb.data(), I.band_qidx,
+                                       I.band_skip, cb, st);
+        }
         if (rc) return rc;
         const int filt[3] = {I.filter, I.filter, I.filter};
         int16_t* pic[3] = {s.data[0], s.data[1], s.data[2]};

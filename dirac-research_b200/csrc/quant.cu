@@ -608,7 +608,7 @@ __global__ void dc_intra_kernel(const DcJob* jobs) {
 constexpr int DQ_MAX_BANDS = 64;
 
 struct DqBand {
-    const int32_t* q;   // band top-left in the index array
+    const void* q;      // band top-left in the index array (int32 or int16 elements)
     int32_t* c;         // band top-left in the coefficient array
     const uint8_t* cb;  // the band's code-block skip flags (device)
     int stride, xl, yl, xn, yn;
@@ -634,7 +634,9 @@ __device__ __forceinline__ int dequant_value(int qi, int qf, int off) {
 
 // grid: row chunks of the bands laid end to end, a warp per row, lanes across it, the code
 // block followed by CbWalk.  An intra DC band gets its decoded residues here (zero in skipped
-// code blocks); dc_decode_kernel then adds the predictions.
+// code blocks); dc_decode_kernel then adds the predictions.  Idx: the index element type
+// (int32, or int16 where every index fits: half the bytes read).
+template <typename Idx>
 __global__ void __launch_bounds__(ROW_THREADS) dequantise_kernel(const __grid_constant__ DqArgs A) {
     int lo_b = 0, hi_b = A.nbands - 1;
     while (lo_b < hi_b) {
@@ -649,7 +651,7 @@ __global__ void __launch_bounds__(ROW_THREADS) dequantise_kernel(const __grid_co
     const int xl = B.xl;
     for (int j = r0 + warp; j < r1; j += ROW_THREADS / 32) {
         if (lane >= xl) break;
-        const int32_t* qrow = B.q + (size_t)j * B.stride;  // may alias row (in place)
+        const Idx* qrow = static_cast<const Idx*>(B.q) + (size_t)j * B.stride;  // int32: may alias row
         int32_t* row = B.c + (size_t)j * B.stride;
         if (B.skip) {
             for (int i = lane; i < xl; i += 32) row[i] = 0;
@@ -1213,10 +1215,11 @@ namespace {
 
 // Launches the dequantisation of the bands collected in A (row-chunked grid, then the intra
 // DC wavefronts) and empties A.
-int launch_dequantise(DqArgs& A, int ndc, int chunks, cudaStream_t st) {
+int launch_dequantise(DqArgs& A, int ndc, int chunks, bool idx16, cudaStream_t st) {
     if (A.nbands == 0) return DGPU_OK;
     if (chunks > 0) {
-        dequantise_kernel<<<chunks, ROW_THREADS, 0, st>>>(A);
+        if (idx16) dequantise_kernel<int16_t><<<chunks, ROW_THREADS, 0, st>>>(A);
+        else dequantise_kernel<int32_t><<<chunks, ROW_THREADS, 0, st>>>(A);
         DGPU_CHECK_LAUNCH();
     }
     if (ndc > 0) {
@@ -1240,10 +1243,12 @@ int launch_dequantise(DqArgs& A, int ndc, int chunks, cudaStream_t st) {
 
 }  // namespace
 
-extern "C" int dgpu_dequantise_batch(int n, const int* intra, const int* depth, const int32_t* const* qindex,
-                                     int32_t* const* coeff, const int* cw, const int* ch, const int* band_ncb,
-                                     const int* band_qidx, const int* band_skip, const uint8_t* cb_skip,
-                                     void* stream) {
+namespace {
+
+// dgpu_dequantise_batch over int32 (idx16 false) or int16 (true) index arrays.
+int dequantise_batch(int n, const int* intra, const int* depth, const void* const* qindex, bool idx16,
+                     int32_t* const* coeff, const int* cw, const int* ch, const int* band_ncb, const int* band_qidx,
+                     const int* band_skip, const uint8_t* cb_skip, void* stream) {
     if (n <= 0 || n > MAX_COMPS || !intra || !depth || !qindex || !coeff || !cw || !ch || !band_ncb || !band_qidx ||
         !band_skip || !cb_skip)
         return DGPU_ERR_ARG;
@@ -1269,7 +1274,7 @@ extern "C" int dgpu_dequantise_batch(int n, const int* intra, const int* depth, 
     for (int c = 0, b0 = 0; c < n; ++c) {
         const int d = depth[c], nb = 3 * d + 1;
         if (A.nbands + nb > DQ_MAX_BANDS) {
-            const int rc = launch_dequantise(A, ndc, chunks, st);
+            const int rc = launch_dequantise(A, ndc, chunks, idx16, st);
             if (rc) return rc;
             chunks = ndc = 0;
         }
@@ -1279,7 +1284,8 @@ extern "C" int dgpu_dequantise_batch(int n, const int* intra, const int* depth, 
             band_rect(d, cw[c], ch[c], b, xp, yp, xl, yl);
             DqBand& B = A.band[A.nbands];
             const size_t at = (size_t)yp * cw[c] + xp;
-            B.q = qindex[c] + at;
+            B.q = idx16 ? (const void*)(static_cast<const int16_t*>(qindex[c]) + at)
+                        : (const void*)(static_cast<const int32_t*>(qindex[c]) + at);
             B.c = coeff[c] + at;
             B.cb = cb_skip + cb_off;
             B.stride = cw[c];
@@ -1301,7 +1307,31 @@ extern "C" int dgpu_dequantise_batch(int n, const int* intra, const int* depth, 
         }
         b0 += nb;
     }
-    return launch_dequantise(A, ndc, chunks, st);
+    return launch_dequantise(A, ndc, chunks, idx16, st);
+}
+
+}  // namespace
+
+extern "C" int dgpu_dequantise_batch(int n, const int* intra, const int* depth, const int32_t* const* qindex,
+                                     int32_t* const* coeff, const int* cw, const int* ch, const int* band_ncb,
+                                     const int* band_qidx, const int* band_skip, const uint8_t* cb_skip,
+                                     void* stream) {
+    if (!qindex || n <= 0 || n > MAX_COMPS) return DGPU_ERR_ARG;
+    const void* q[MAX_COMPS];
+    for (int c = 0; c < n; ++c) q[c] = qindex[c];
+    return dequantise_batch(n, intra, depth, q, false, coeff, cw, ch, band_ncb, band_qidx, band_skip, cb_skip,
+                            stream);
+}
+
+extern "C" int dgpu_dequantise_batch16(int n, const int* intra, const int* depth, const int16_t* const* qindex,
+                                       int32_t* const* coeff, const int* cw, const int* ch, const int* band_ncb,
+                                       const int* band_qidx, const int* band_skip, const uint8_t* cb_skip,
+                                       void* stream) {
+    if (!qindex || n <= 0 || n > MAX_COMPS) return DGPU_ERR_ARG;
+    const void* q[MAX_COMPS];
+    for (int c = 0; c < n; ++c) q[c] = qindex[c];
+    return dequantise_batch(n, intra, depth, q, true, coeff, cw, ch, band_ncb, band_qidx, band_skip, cb_skip,
+                            stream);
 }
 
 // CoeffArray::SetBandWeights (libdirac_common/wavelet_utils.cpp:192-382) with

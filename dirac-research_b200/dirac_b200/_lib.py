@@ -143,6 +143,9 @@ SIGNATURES = {
     "dgpu_dequantise_batch": (
         c_int, [c_int, P_int, P_int, P_void, P_void, P_int, P_int, P_int, P_int, P_int, c_void_p, c_void_p],
     ),
+    "dgpu_dequantise_batch16": (
+        c_int, [c_int, P_int, P_int, P_void, P_void, P_int, P_int, P_int, P_int, P_int, c_void_p, c_void_p],
+    ),
     "dgpu_decoder_device_bytes": (c_size_t, [c_void_p, c_int]),
     "dgpu_decoder_create": (c_int, [c_void_p, c_int, c_void_p, P_void]),
     "dgpu_decoder_destroy": (c_int, [c_void_p]),

@@ -37,7 +37,7 @@ class DecodeInput(ctypes.Structure):
                 ("band_qidx", ctypes.c_void_p), ("band_skip", ctypes.c_void_p), ("on_host", ctypes.c_int),
                 ("qindex", ctypes.c_void_p * 3), ("cb_skip", ctypes.c_void_p), ("mv1", ctypes.c_void_p),
                 ("mv2", ctypes.c_void_p), ("mode", ctypes.c_void_p), ("dc", ctypes.c_void_p),
-                ("split", ctypes.c_void_p)]
+                ("split", ctypes.c_void_p), ("index_bits", ctypes.c_int)]
 
 
 def block_params(width, height, precision, xblen, yblen, xbsep, ybsep):
@@ -114,18 +114,22 @@ class SequenceDecoder:
         bq = np.ascontiguousarray(np.concatenate([x[:, 0] for x in b]), np.int32)
         bs = np.ascontiguousarray(np.concatenate([x[:, 1] for x in b]), np.int32)
         keep += [bq, bs]
+        # int16 index arrays (numpy or torch) go as they are: half the bytes copied
+        q0 = qindex[0]
+        idx16 = q0.dtype == torch.int16 if isinstance(q0, torch.Tensor) else np.asarray(q0).dtype == np.int16
         I = DecodeInput(pnum=pnum, intra=int(bool(intra)), num_refs=len(refs), ref1=refs[0] if refs else -1,
                         ref2=refs[1] if len(refs) > 1 else -1, filter=filt, zero_residual=int(bool(zero_residual)),
-                        band_qidx=bq.ctypes.data, band_skip=bs.ctypes.data, on_host=int(on_host))
+                        band_qidx=bq.ctypes.data, band_skip=bs.ctypes.data, on_host=int(on_host),
+                        index_bits=16 if idx16 else 32)
         if on_host:
             for c in range(3):
-                I.qindex[c] = _host_ptr(qindex[c], np.int32, keep)
+                I.qindex[c] = _host_ptr(qindex[c], np.int16 if idx16 else np.int32, keep)
             flags = cb_skip if isinstance(cb_skip, np.ndarray) else \
                 np.concatenate([np.asarray(x, np.uint8).ravel() for x in cb_skip])
             I.cb_skip = _host_ptr(flags, np.uint8, keep)
         else:
             for c in range(3):
-                I.qindex[c] = _dev_ptr(qindex[c], torch.int32, keep)
+                I.qindex[c] = _dev_ptr(qindex[c], torch.int16 if idx16 else torch.int32, keep)
             flags = cb_skip if isinstance(cb_skip, torch.Tensor) else torch.cat([x.reshape(-1) for x in cb_skip])
             I.cb_skip = _dev_ptr(flags, torch.uint8, keep)
         if not intra:
@@ -146,7 +150,7 @@ class SequenceDecoder:
         """Decodes one picture.
 
         qindex: three int32 [ch][cw] index arrays (numpy: host inputs; CUDA tensors: device
-        inputs); bands: three [3*depth+1][>=2] arrays of (quantiser index, skip, ...) per band
+        inputs), or int16 ones when every index fits (index_bits 16); bands: three [3*depth+1][>=2] arrays of (quantiser index, skip, ...) per band
         (the DGPU_ENC_BANDS layout); cb_skip: three uint8 code-block flag arrays, or one with
         the three concatenated (host or device like qindex); motion (inter): {"mv": [mv1, mv2?]
         int16 [blocks][2], "mode", "dc" int16 [3][blocks], "split"}, host or device like
@@ -182,25 +186,30 @@ class SequenceDecoder:
 
 
 def dequantise(intra, depth, qindex, bands, ncb, cb_skip, out=None, stream=None):
-    """dgpu_dequantise_batch over CUDA tensors: qindex (list of int32 [ch][cw]), bands (per
-    component [3*depth+1][>=2] quantiser index, skip), ncb (per component the [nb][2] code
-    block counts), cb_skip (per component uint8 flags, CUDA).  Returns the coefficients."""
+    """dgpu_dequantise_batch over CUDA tensors: qindex (list of int32 [ch][cw], or int16 for
+    dgpu_dequantise_batch16), bands (per component [3*depth+1][>=2] quantiser index, skip), ncb
+    (per component the [nb][2] code block counts), cb_skip (per component uint8 flags, CUDA).
+    Returns the int32 coefficients."""
     lib = _lib.load()
     n = len(qindex)
     intra = list(intra) if hasattr(intra, "__len__") else [intra] * n
     depth = list(depth) if hasattr(depth, "__len__") else [depth] * n
     q = [t.contiguous() for t in qindex]
-    out = out if out is not None else [torch.empty_like(t) for t in q]
+    idx16 = q[0].dtype == torch.int16
+    if any(t.dtype != q[0].dtype for t in q) or q[0].dtype not in (torch.int16, torch.int32):
+        raise TypeError("qindex: int32 or int16 tensors of one type")
+    out = out if out is not None else [torch.empty(t.shape, dtype=torch.int32, device=t.device) for t in q]
     b = [np.asarray(x, np.int32).reshape(3 * d + 1, -1) for x, d in zip(bands, depth)]
     bq = np.ascontiguousarray(np.concatenate([x[:, 0] for x in b]), np.int32)
     bs = np.ascontiguousarray(np.concatenate([x[:, 1] for x in b]), np.int32)
     nc = np.ascontiguousarray(np.concatenate([np.asarray(x, np.int32).ravel() for x in ncb]), np.int32)
     cbs = torch.cat([x.reshape(-1) for x in cb_skip]).contiguous()
     st = stream if stream is not None else torch.cuda.current_stream()
-    rc = lib.dgpu_dequantise_batch(
+    fn = lib.dgpu_dequantise_batch16 if idx16 else lib.dgpu_dequantise_batch
+    rc = fn(
         n, _lib.int_array(intra), _lib.int_array(depth), _lib.ptr_array([t.data_ptr() for t in q]),
         _lib.ptr_array([t.data_ptr() for t in out]), _lib.int_array([t.shape[1] for t in q]),
         _lib.int_array([t.shape[0] for t in q]), nc.ctypes.data_as(_lib.P_int), bq.ctypes.data_as(_lib.P_int),
         bs.ctypes.data_as(_lib.P_int), cbs.data_ptr(), st.cuda_stream)
-    _lib.check(rc, "dgpu_dequantise_batch")
+    _lib.check(rc, "dgpu_dequantise_batch16" if idx16 else "dgpu_dequantise_batch")
     return out

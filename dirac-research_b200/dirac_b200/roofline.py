@@ -68,11 +68,12 @@ def stage_bytes(params, infos):
     return out
 
 
-def decode_bytes(params, infos):
+def decode_bytes(params, infos, int16_pictures=0):
     """Algorithmic bytes per stage of the device decoder for the pictures described by infos
-    (coded pictures in coding order): dequantisation 8 B per coefficient (index read,
-    coefficient write), the inverse transform, motion compensation ADD with the clip (or the
-    clip alone for intra pictures) and the upconversion of every reference picture, as above."""
+    (coded pictures in coding order): dequantisation 8 B per coefficient (int32 index read,
+    coefficient write; 6 B in the int16_pictures whose indices are int16), the inverse
+    transform, motion compensation ADD with the clip (or the clip alone for intra pictures) and
+    the upconversion of every reference picture, as above."""
     enc = stage_bytes(params, infos)
     w, h = params["width"], params["height"]
     cf = params["cformat"]
@@ -83,5 +84,5 @@ def decode_bytes(params, infos):
     coeffs = sum((a + mul - 1) // mul * mul * ((b + mul - 1) // mul * mul) for a, b in comps)
     samples = sum(a * b for a, b in comps)
     refs = {r for i in infos if not i["intra"] for r in (i["ref1"], i["ref2"]) if r >= 0}
-    return {"dequantisation": 8 * coeffs * len(infos), "dwt_inverse": enc["dwt_inverse"],
+    return {"dequantisation": coeffs * (8 * len(infos) - 2 * int16_pictures), "dwt_inverse": enc["dwt_inverse"],
             "mc_add_clip": enc["mc_add_clip"], "upconvert": len(refs) * samples * 10}

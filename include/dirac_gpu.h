@@ -386,6 +386,11 @@ int dgpu_code_residue_batch(int n, const int* intra, const int* depth, int32_t* 
 int dgpu_dequantise_batch(int n, const int* intra, const int* depth, const int32_t* const* qindex,
                           int32_t* const* coeff, const int* cw, const int* ch, const int* band_ncb,
                           const int* band_qidx, const int* band_skip, const uint8_t* cb_skip, void* stream);
+/* As dgpu_dequantise_batch, over int16 index arrays (same layout); coeff[c] must not overlap
+ * qindex[c] (no in-place form). */
+int dgpu_dequantise_batch16(int n, const int* intra, const int* depth, const int16_t* const* qindex,
+                            int32_t* const* coeff, const int* cw, const int* ch, const int* band_ncb,
+                            const int* band_qidx, const int* band_skip, const uint8_t* cb_skip, void* stream);
 
 /* ---------------------------------------------------------------------------------------
  * Sequence encoder: the data-parallel part of the reference's frame-coding loop
@@ -723,7 +728,9 @@ int dgpu_entropy_update(int depth, float* state, int intra, int is_b, int comp, 
  * the zero-residual flag (no coefficients coded: the residue is zero), per band the
  * quantiser indices and skip flags (host, components concatenated), and, in host memory
  * (on_host = 1) or device memory (on_host = 0): the signed quantised indices of the three
- * components (int32 [ch][cw] padded to the transform depth: the layout of DGPU_ENC_QINDEX),
+ * components (int32 [ch][cw] padded to the transform depth: the layout of DGPU_ENC_QINDEX;
+ * int16 in the same layout with index_bits = 16, for a caller that has checked every index
+ * fits 16 bits: half the bytes to copy),
  * the code-block skip flags (per component in band-list order as DGPU_ENC_CBSKIP, components
  * concatenated) and, for inter pictures, the motion data in the layout of
  * dgpu_motion_compensate.  Transform depth, code blocks and block parameters are fixed per
@@ -755,13 +762,14 @@ typedef struct {
     const int* band_qidx;         /* host, [3][3*depth+1] quantiser indices */
     const int* band_skip;         /* host, [3][3*depth+1] band skip flags */
     int on_host;                  /* 1: the arrays below are in host memory */
-    const int32_t* qindex[3];
+    const void* qindex[3];        /* int32 elements, or int16 with index_bits = 16 */
     const uint8_t* cb_skip;
     const int16_t* mv1;
     const int16_t* mv2;           /* NULL with one reference */
     const uint8_t* mode;
     const int16_t* dc;
     const uint8_t* split;
+    int index_bits;               /* 0 or 32: int32 indices; 16: int16 (half the bytes copied) */
 } dgpu_decode_input;
 
 size_t dgpu_decoder_device_bytes(const dgpu_decoder_params* params, int max_pictures);

@@ -61,9 +61,10 @@ def padded_shapes(cfg):
     return out
 
 
-def decode_all(cfg, infos, results, device=False, max_pictures=None, release=False):
+def decode_all(cfg, infos, results, device=False, max_pictures=None, release=False, idx16=False):
     """Decodes the coded pictures in coding order; with release, drops each picture once no
-    later picture references it (after reading its results)."""
+    later picture references it (after reading its results); with idx16, the indices go as
+    int16 arrays (index_bits 16)."""
     import torch
 
     from dirac_b200.decoder import SequenceDecoder, decoder_params
@@ -76,6 +77,9 @@ def decode_all(cfg, infos, results, device=False, max_pictures=None, release=Fal
         pn = info["pnum"]
         r = results[pn]
         q = [r["qindex"][c].reshape(shapes[c]) for c in range(3)]
+        if idx16:
+            assert all(np.abs(a).max() <= 32767 for a in q)
+            q = [a.astype(np.int16) for a in q]
         cbs = r["cb_skip"]
         if device:
             q = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in q]
@@ -123,6 +127,32 @@ def test_decoder_round_trip_matches_reference(gpu, golden, case):
 def test_decoder_device_inputs(gpu):
     cfg, infos, results = encoded(gpu, ENCODE_CASES[1])
     check_round_trip(infos, results, decode_all(cfg, infos, results, device=True))
+
+
+@pytest.mark.parametrize("device", [False, True], ids=["host", "device"])
+def test_decoder_int16_indices(gpu, device):
+    """int16 indices (index_bits 16), from host or device memory, decode to the same
+    pictures as the int32 ones."""
+    cfg, infos, results = encoded(gpu, ENCODE_CASES[1])
+    check_round_trip(infos, results, decode_all(cfg, infos, results, device=device, idx16=True))
+
+
+def test_decoder_rejects_bad_index_bits(gpu):
+    from dirac_b200._lib import DgpuError
+    from dirac_b200.decoder import SequenceDecoder, decoder_params
+
+    cfg, infos, results = encoded(gpu, ENCODE_CASES[1])
+    dec = SequenceDecoder(decoder_params(cfg), max_pictures=2)
+    info = infos[0]
+    r = results[info["pnum"]]
+    q = [r["qindex"][c].reshape(s) for c, s in enumerate(padded_shapes(cfg))]
+    I, keep = dec.prepare(info["pnum"], 1, [], info["filter"], q, r["bands"], r["cb_skip"])
+    I.index_bits = 8
+    with pytest.raises(DgpuError):
+        dec.decode_prepared((I, keep))
+    I.index_bits = 32
+    dec.decode_prepared((I, keep))
+    dec.close()
 
 
 @pytest.mark.parametrize("cformat,depth", [(1, 10), (0, 8), (2, 12)])
@@ -186,11 +216,38 @@ def test_dequantise_stage_against_oracle(gpu, oracle, intra):
     torch.cuda.synchronize()
     for k in range(len(comps)):
         np.testing.assert_array_equal(got[k].cpu().numpy(), want[k], err_msg=f"component {k}")
+    # int16 indices (dgpu_dequantise_batch16)
+    got16 = dequantise(intra, [c[2] for c in comps], [t.to(torch.int16) for t in q], bands, ncbs, cbs)
+    torch.cuda.synchronize()
+    for k in range(len(comps)):
+        np.testing.assert_array_equal(got16[k].cpu().numpy(), want[k], err_msg=f"int16, component {k}")
     # in place
     got2 = dequantise(intra, [c[2] for c in comps], q, bands, ncbs, cbs, out=q)
     torch.cuda.synchronize()
     for k in range(len(comps)):
         np.testing.assert_array_equal(got2[k].cpu().numpy(), want[k], err_msg=f"in place, component {k}")
+
+
+def test_dequantise_int16_extremes(gpu):
+    """The int16 form at the int16 extremes equals the int32 form on the same indices."""
+    import torch
+
+    from dirac_b200 import quant
+    from dirac_b200.decoder import dequantise
+
+    rng = np.random.default_rng(17)
+    cw, ch, d = 128, 96, 4
+    nb = 3 * d + 1
+    qi = rng.integers(-32768, 32768, size=(ch, cw)).astype(np.int16)
+    qi.flat[:4] = [32767, -32768, -32767, 0]
+    ncb = np.asarray(quant.code_blocks(d, cw, ch), np.int32)
+    flags = torch.from_numpy((rng.random(int((ncb[0::2] * ncb[1::2]).sum())) < 0.2).astype(np.uint8)).cuda()
+    bands = [np.stack([rng.integers(0, 40, size=nb).astype(np.int32), np.zeros(nb, np.int32)], 1)]
+    for intra in (0, 1):
+        a = dequantise(intra, d, [torch.from_numpy(qi.astype(np.int32)).cuda()], bands, [ncb], [flags])
+        b = dequantise(intra, d, [torch.from_numpy(qi).cuda()], bands, [ncb], [flags])
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(b[0].cpu().numpy(), a[0].cpu().numpy())
 
 
 def test_dequantise_rejects_bad_quantiser(gpu):
