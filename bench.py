@@ -80,6 +80,11 @@ def parse_args():
     ap.add_argument("--streams", type=int, default=12, help="concurrent sequences per GPU (batched form)")
     ap.add_argument("--me-occupancy", type=int, default=8,
                     help="resident CTAs per SM of the motion-estimation wavefront kernels (1-8)")
+    ap.add_argument("--me-unit-life", type=int, default=0,
+                    help="units a motion-estimation wavefront warp takes before it exits (0: persistent)")
+    ap.add_argument("--lane-priority", type=int, default=0,
+                    help="CUDA stream priority of the sequences' coding streams (negative: above the encoder "
+                         "groups' estimation streams, which run at the default 0)")
     ap.add_argument("--me-groups", type=int, default=3,
                     help="encoder groups the batched form's sequences are split into (run concurrently)")
     ap.add_argument("--double-buffer", type=int, default=0,
@@ -690,7 +695,7 @@ def main():
         driven by its own host thread)."""
 
         def __init__(self):
-            self.stream = torch.cuda.Stream()
+            self.stream = torch.cuda.Stream(priority=args.lane_priority)
             self.enc = E.SequenceEncoder(PARAMS, max_pictures=args.frames, stream=self.stream)
             self.bufs = {}
             self.d2h = 0
@@ -893,6 +898,8 @@ def main():
 
     if lib.dgpu_me_set_occupancy(args.me_occupancy):
         raise ValueError("--me-occupancy must be 1..8")
+    if lib.dgpu_me_set_unit_lifetime(args.me_unit_life):
+        raise ValueError("--me-unit-life must be >= 0")
     nsets = 2 if args.double_buffer else 1
     lanes = [Lane() for _ in range(args.streams * nsets)]
     sets = [lanes[i * args.streams:(i + 1) * args.streams] for i in range(nsets)]
@@ -1114,7 +1121,8 @@ def main():
                                    "each sequence's coding on its own stream and host thread"
                                    + ("; each group alternates two sets of sequences, one set's estimation "
                                       "running while the other set is coded" if nsets == 2 else ""),
-                           "me_ctas_per_sm": args.me_occupancy,
+                           "me_ctas_per_sm": args.me_occupancy, "me_unit_life": args.me_unit_life,
+                           "lane_priority": args.lane_priority,
                            "l2": "inputs and working set larger than L2 (no flush needed)"},
                 "e2e": e2e, "cpu_baseline": cpu_baseline, "parity_vs_reference": parity, "plain": plain_line,
                 "gpu_launches": launches, "clocks": clk, "e2e_hot_path": e2e_hot, "roofline": roofline,

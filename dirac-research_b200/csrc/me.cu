@@ -194,6 +194,7 @@ __device__ __forceinline__ int warp_ticket(int* counter) {
 struct Wave {
     const int* prefix;  // T + 1 entries
     int T, W, slope, njobs;
+    int life;           // units a warp (a CTA of the mode wavefront) takes before it exits
 };
 
 __device__ __forceinline__ void wave_unit(const Wave& w, int u, int& j, int& x, int& y) {
@@ -920,7 +921,7 @@ __global__ void __launch_bounds__(ME_THREADS) pel_lists_kernel(const __grid_cons
 __global__ void __launch_bounds__(ME_THREADS) pel_wavefront_kernel(const __grid_constant__ PelLaunch L) {
     extern __shared__ __align__(16) int16_t pel_smem[];
     int16_t* const wmem = pel_smem + (size_t)(threadIdx.x >> 5) * L.win_elems;
-    for (;;) {
+    for (int it = 0; it < L.wave.life; ++it) {
         const int u = warp_ticket(L.ticket);
         if (u >= L.total) return;
         int jn, bx, by;
@@ -1038,7 +1039,7 @@ __global__ void __launch_bounds__(ME_THREADS, 4) subpel_wavefront_kernel(const _
     extern __shared__ __align__(16) int16_t sub_smem[];
     int16_t* const wmem = sub_smem + (size_t)(threadIdx.x >> 5) * L.win_elems;
     const int prec = L.prec;
-    for (;;) {
+    for (int it = 0; it < L.wave.life; ++it) {
         const int u = warp_ticket(L.ticket);
         if (u >= L.total) return;
         int jn, bx, by;
@@ -1416,7 +1417,7 @@ __global__ void __launch_bounds__(ME_THREADS, 5) mode_wavefront_kernel(const __g
     __shared__ short2 s_cand[2][4];           // level-0 candidates per reference
     __shared__ int s_ncand[2];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (;;) {
+    for (int it = 0; it < L.wave.life; ++it) {
         __syncthreads();
         if (threadIdx.x == 0) s_u = atomicAdd(L.ticket, 1);
         __syncthreads();
@@ -2027,6 +2028,29 @@ int wave_grid(int ctas_needed) {
     return std::max(1, std::min(ctas_needed, n.load() * g_wave_ctas_per_sm.load()));
 }
 
+// Units a warp (pel and sub-pel wavefronts) or a CTA (mode wavefront) takes before it exits
+// (dgpu_me_set_unit_lifetime; 0: until the tickets run out).  A bounded lifetime hands the SMs
+// back to the block scheduler every few units, so that kernels of higher-priority streams
+// start within that time instead of after the whole launch.  Also free of deadlock: a unit
+// waits only on units with earlier tickets, held by warps that are resident and finish them.
+std::atomic<int> g_wave_life{0};
+
+// Grid of a wavefront launch over `total` units, `slots` ticket takers per CTA (warps, or 1),
+// with w.life set: the persistent grid, or with a lifetime at least enough CTAs that
+// grid x slots x life covers every unit.
+int wave_launch_grid(Wave& w, int total, int slots) {
+    const int persistent = wave_grid((total + slots - 1) / slots);
+    const int life = g_wave_life.load();
+    if (life <= 0) {
+        w.life = INT_MAX;
+        return persistent;
+    }
+    w.life = life;
+    const long long per = (long long)slots * life;
+    const long long need = ((long long)total + per - 1) / per;
+    return (int)std::max<long long>(persistent, need);
+}
+
 // Process-wide settings of dgpu_debug_wavefront, read once by each motion-estimation call.
 struct DebugSettings {
     int skip_unit = -1;
@@ -2131,6 +2155,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
         w.slope = slope;
         w.njobs = njobs;
         w.T = 0;
+        w.life = INT_MAX;
         return w;
     };
     DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, 2 * sizeof(int), st));
@@ -2217,8 +2242,8 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
         L.err = ctl + 1;
         DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
         tm.start(2);
-        pel_wavefront_kernel<<<wave_grid((L.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA), ME_THREADS, smem,
-                               st>>>(L);
+        const int grid = wave_launch_grid(L.wave, L.total, WARPS_PER_CTA);
+        pel_wavefront_kernel<<<grid, ME_THREADS, smem, st>>>(L);
         tm.stop();
         DGPU_CHECK_LAUNCH();
     }
@@ -2312,7 +2337,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
             S.ticket = ctl;
             S.err = ctl + 1;
             DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
-            const int grid = wave_grid((S.total + WARPS_PER_CTA - 1) / WARPS_PER_CTA);
+            const int grid = wave_launch_grid(S.wave, S.total, WARPS_PER_CTA);
             tm.start(3);
             subpel_wavefront_kernel<<<grid, ME_THREADS, (size_t)S.win_elems * 2 * WARPS_PER_CTA, st>>>(S);
             tm.stop();
@@ -2403,7 +2428,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
                 M.ticket = ctl;
                 M.err = ctl + 1;
                 DGPU_CHECK_CUDA(cudaMemsetAsync(ctl, 0, sizeof(int), st));
-                const int grid = wave_grid(M.total);
+                const int grid = wave_launch_grid(M.wave, M.total, 1);
                 tm.start(5);
                 mode_wavefront_kernel<<<grid, ME_THREADS, 0, st>>>(M);
                 tm.stop();
@@ -2477,6 +2502,12 @@ extern "C" int dgpu_me_profile(int enable, double* kernel_ms, int* launches) {
 extern "C" int dgpu_me_set_occupancy(int ctas_per_sm) {
     if (ctas_per_sm < 1 || ctas_per_sm > 8) return DGPU_ERR_ARG;
     g_wave_ctas_per_sm.store(ctas_per_sm);
+    return DGPU_OK;
+}
+
+extern "C" int dgpu_me_set_unit_lifetime(int units) {
+    if (units < 0) return DGPU_ERR_ARG;
+    g_wave_life.store(units);
     return DGPU_OK;
 }
 

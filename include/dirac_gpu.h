@@ -302,6 +302,15 @@ int dgpu_me_profile(int enable, double* kernel_ms, int* launches);
  * work on every SM.  Results do not depend on it.  No counterpart in the reference. */
 int dgpu_me_set_occupancy(int ctas_per_sm);
 
+/* Units (blocks or superblocks) one warp of the pel and sub-pel wavefronts, or one CTA of the
+ * mode-decision wavefront, takes before it exits, process-wide, read by later estimation
+ * calls (0, the default: until the launch's units run out).  With a lifetime the grid grows
+ * so that every unit is still taken, and CTAs leave their SMs every few units: kernels on
+ * streams of higher priority (an encoder's coding while a group estimates) start within that
+ * time instead of after the whole launch.  Results do not depend on it.  DGPU_ERR_ARG for a
+ * negative count.  No counterpart in the reference. */
+int dgpu_me_set_unit_lifetime(int units);
+
 /* Failure-detection and ordering checks of the motion-estimation wavefronts.  No counterpart
  * in the reference, whose search is sequential.  Process-wide settings, read by every later
  * dgpu_motion_estimate[_batch] call (and the encoders' estimation) until changed; set them

@@ -145,6 +145,34 @@ def test_estimates_do_not_depend_on_wavefront_occupancy(gpu, oracle):
         assert lib.dgpu_me_set_occupancy(8) == 0
 
 
+@pytest.mark.gpu
+def test_estimates_do_not_depend_on_unit_lifetime(gpu, oracle):
+    """dgpu_me_set_unit_lifetime bounds how many units a warp (a CTA of the mode wavefront)
+    takes before it exits, the grid growing to cover the rest: down to one unit per warp, and
+    with one resident CTA per SM, the results equal the oracle's."""
+    lib = gpu.load()
+    f = _frames()
+    want = oracle.motion_estimate(2, f[1], f[0], f[2], _bp(), 10.0, 3)
+    try:
+        for life, occ in ((1, 8), (3, 8), (64, 8), (2, 1)):
+            assert lib.dgpu_me_set_unit_lifetime(life) == 0
+            assert lib.dgpu_me_set_occupancy(occ) == 0
+            got = _estimate(gpu, f, 3)
+            for k, v in want.items():
+                np.testing.assert_array_equal(got[k], v, err_msg=f"{k} at lifetime {life}, {occ} CTAs per SM")
+    finally:
+        assert lib.dgpu_me_set_unit_lifetime(0) == 0
+        assert lib.dgpu_me_set_occupancy(8) == 0
+
+
+def test_unit_lifetime_rejects_negative_values():
+    from dirac_b200 import _lib
+
+    lib = _lib.load()
+    assert lib.dgpu_me_set_unit_lifetime(-1) == -1
+    assert lib.dgpu_me_set_unit_lifetime(0) == 0
+
+
 def test_wavefront_occupancy_rejects_out_of_range_values():
     from dirac_b200 import _lib
 
