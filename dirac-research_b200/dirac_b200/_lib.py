@@ -157,6 +157,9 @@ SIGNATURES = {
     "dgpu_code_bands_host": (
         c_int, [c_int, P_int, P_int, P_void, P_int, P_int, P_int, P_int, P_int, c_void_p, c_void_p, c_size_t, P_int],
     ),
+    "dgpu_code_bands_host16": (
+        c_int, [c_int, P_int, P_int, P_void, P_int, P_int, P_int, P_int, P_int, c_void_p, c_void_p, c_size_t, P_int],
+    ),
     "dgpu_code_bands_vlc_host": (
         c_int,
         [c_int, P_int, P_int, P_void, P_int, P_int, P_int, P_int, P_int, c_void_p, c_void_p, c_size_t, P_int, c_void_p],

@@ -14,7 +14,8 @@ from . import _lib
 
 def code_bands(intra, depth, qindex, bands, ncb, cb_skip, vlc=False):
     """Codes components (vlc: the variable-length form, dgpu_code_bands_vlc_host).  qindex: list
-    of int32 [ch][cw] arrays; bands: per component
+    of int32 [ch][cw] arrays (int16 ones go to dgpu_code_bands_host16, arithmetic form only);
+    bands: per component
     [3*depth+1][>=2] (quantiser index, skip, ...), e.g. DGPU_ENC_BANDS; ncb: per component the
     [nb][2] code-block counts; cb_skip: per component the flags.  intra / depth: one value or
     one per component.  Returns (data bytes, band_bytes per component), and with vlc the exact
@@ -23,7 +24,8 @@ def code_bands(intra, depth, qindex, bands, ncb, cb_skip, vlc=False):
     n = len(qindex)
     intra = list(intra) if hasattr(intra, "__len__") else [int(intra)] * n
     depth = list(depth) if hasattr(depth, "__len__") else [int(depth)] * n
-    q = [np.ascontiguousarray(a, np.int32) for a in qindex]
+    idx16 = not vlc and all(np.asarray(a).dtype == np.int16 for a in qindex)
+    q = [np.ascontiguousarray(a, np.int16 if idx16 else np.int32) for a in qindex]
     b = [np.asarray(x, np.int32).reshape(3 * d + 1, -1) for x, d in zip(bands, depth)]
     bq = np.ascontiguousarray(np.concatenate([x[:, 0] for x in b]), np.int32)
     bs = np.ascontiguousarray(np.concatenate([x[:, 1] for x in b]), np.int32)
@@ -38,7 +40,10 @@ def code_bands(intra, depth, qindex, bands, ncb, cb_skip, vlc=False):
                 _lib.int_array([a.shape[1] for a in q]), _lib.int_array([a.shape[0] for a in q]),
                 nc.ctypes.data_as(_lib.P_int), bq.ctypes.data_as(_lib.P_int), bs.ctypes.data_as(_lib.P_int),
                 cbs.ctypes.data, out.ctypes.data, cap, nbytes.ctypes.data_as(_lib.P_int)]
-        rc = lib.dgpu_code_bands_vlc_host(*args, nbits.ctypes.data) if vlc else lib.dgpu_code_bands_host(*args)
+        if vlc:
+            rc = lib.dgpu_code_bands_vlc_host(*args, nbits.ctypes.data)
+        else:
+            rc = (lib.dgpu_code_bands_host16 if idx16 else lib.dgpu_code_bands_host)(*args)
         if rc == -2:
             cap = int(nbytes.sum()) + 16
             continue

@@ -682,6 +682,12 @@ int dgpu_code_bands_host(int n, const int* intra, const int* depth, const int32_
                          const int* cw, const int* ch, const int* band_ncb, const int* band_qidx,
                          const int* band_skip, const uint8_t* cb_skip, uint8_t* out, size_t out_cap,
                          int* band_bytes);
+/* As dgpu_code_bands_host over int16 index arrays (same layout, indices that fit 16 bits):
+ * the same bytes, half the index bytes read. */
+int dgpu_code_bands_host16(int n, const int* intra, const int* depth, const int16_t* const* qindex,
+                           const int* cw, const int* ch, const int* band_ncb, const int* band_qidx,
+                           const int* band_skip, const uint8_t* cb_skip, uint8_t* out, size_t out_cap,
+                           int* band_bytes);
 /* The variable-length form of the band coders (-use_vlc: BandVLC / IntraDCBandVLC over
  * ArithCodecToVLCAdapter, libdirac_common/band_vlc.cpp:49-100): the same symbols as plain
  * bits, each band's data padded to a byte.  band_bits (optional) receives each band's exact

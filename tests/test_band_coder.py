@@ -99,6 +99,12 @@ def test_band_data_matches_reference_fixture(oracle, golden, k):
         crc.append(zlib.crc32(data[start:start + n].tobytes()))
         start += n
     np.testing.assert_array_equal(np.array(crc[::-1], np.uint32), g[f"c{k}_band_crc"])
+    # the same indices as int16 (dgpu_code_bands_host16): the same bytes
+    assert np.abs(qo).max() <= 32767
+    data16, per16 = code_bands(intra, depth, [qo.astype(np.int16)], [np.stack([q, sk], 1)], [g[f"c{k}_ncb"]],
+                               [cbs])
+    np.testing.assert_array_equal(per16[0], per[0])
+    np.testing.assert_array_equal(data16, data)
 
 
 @pytest.mark.parametrize("k", range(len(BAND_CASES)))
