@@ -85,6 +85,9 @@ def parse_args():
     ap.add_argument("--lane-priority", type=int, default=0,
                     help="CUDA stream priority of the sequences' coding streams (negative: above the encoder "
                          "groups' estimation streams, which run at the default 0)")
+    ap.add_argument("--blocking-waits", type=int, default=0,
+                    help="1: the library's host waits for the device sleep on blocking-sync events (measured "
+                         "slower: the plain form loses a third); 0: they poll")
     ap.add_argument("--me-groups", type=int, default=3,
                     help="encoder groups the batched form's sequences are split into (run concurrently)")
     ap.add_argument("--double-buffer", type=int, default=0,
@@ -900,6 +903,8 @@ def main():
         raise ValueError("--me-occupancy must be 1..8")
     if lib.dgpu_me_set_unit_lifetime(args.me_unit_life):
         raise ValueError("--me-unit-life must be >= 0")
+    if lib.dgpu_set_blocking_waits(args.blocking_waits):
+        raise ValueError("--blocking-waits must be 0 or 1")
     nsets = 2 if args.double_buffer else 1
     lanes = [Lane() for _ in range(args.streams * nsets)]
     sets = [lanes[i * args.streams:(i + 1) * args.streams] for i in range(nsets)]
@@ -1122,7 +1127,7 @@ def main():
                                    + ("; each group alternates two sets of sequences, one set's estimation "
                                       "running while the other set is coded" if nsets == 2 else ""),
                            "me_ctas_per_sm": args.me_occupancy, "me_unit_life": args.me_unit_life,
-                           "lane_priority": args.lane_priority,
+                           "lane_priority": args.lane_priority, "blocking_waits": args.blocking_waits,
                            "l2": "inputs and working set larger than L2 (no flush needed)"},
                 "e2e": e2e, "cpu_baseline": cpu_baseline, "parity_vs_reference": parity, "plain": plain_line,
                 "gpu_launches": launches, "clocks": clk, "e2e_hot_path": e2e_hot, "roofline": roofline,

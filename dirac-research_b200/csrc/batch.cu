@@ -565,13 +565,13 @@ extern "C" int dgpu_batch_read(void* batch, int k, int what, int comp, void* dst
             return DGPU_OK;
         }
         DGPU_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, B->user));
-        DGPU_CHECK_CUDA(cudaStreamSynchronize(B->user));
+        DGPU_CHECK_CUDA(host_wait(B->user));
         return DGPU_OK;
     }
     const void* src = what == DGPU_ENC_RECON ? (const void*)Q.data[comp]
                       : what == DGPU_ENC_COEFF ? (const void*)Q.coeff[comp] : (const void*)Q.qout[comp];
     DGPU_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
                                     B->user));
-    if (on_host) DGPU_CHECK_CUDA(cudaStreamSynchronize(B->user));
+    if (on_host) DGPU_CHECK_CUDA(host_wait(B->user));
     return DGPU_OK;
 }

@@ -375,6 +375,6 @@ extern "C" int dgpu_decoder_read(void* dec, int pnum, int what, int comp, void* 
     }
     DGPU_CHECK_CUDA(
         cudaMemcpyAsync(dst, src, bytes, on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, D->st));
-    if (on_host) DGPU_CHECK_CUDA(cudaStreamSynchronize(D->st));
+    if (on_host) DGPU_CHECK_CUDA(host_wait(D->st));
     return DGPU_OK;
 }

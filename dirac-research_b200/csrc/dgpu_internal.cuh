@@ -49,6 +49,10 @@ int library_scratch(size_t bytes, void* stream, void** out);
 // every chunk is done.  Small ranges run inline.
 void parallel_for(int n, int grain, const std::function<void(int, int)>& body);
 
+// Waits for the work queued on st so far (cudaStreamSynchronize; with blocking waits switched
+// on, the thread sleeps on a blocking-sync event instead of polling).
+cudaError_t host_wait(cudaStream_t st);
+
 __host__ __device__ inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 }  // namespace dgpu

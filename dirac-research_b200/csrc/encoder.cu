@@ -471,7 +471,7 @@ int run_me_tasks(const std::vector<MeTask>& tasks, cudaStream_t st, void* ws, si
         DGPU_CHECK_LAUNCH();
     }
     DGPU_CHECK_CUDA(cudaMemcpyAsync(h_counts, d_counts, sizeof(int) * nt, cudaMemcpyDeviceToHost, st));
-    DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
+    DGPU_CHECK_CUDA(host_wait(st));
     for (int t = 0; t < nt; ++t) {
         Encoder& E = *tasks[t].E;
         Pic& q = E.pics[tasks[t].pnum];
@@ -1103,7 +1103,7 @@ extern "C" int dgpu_encoder_read(void* enc, int pnum, int what, int comp, void* 
             return DGPU_OK;
         }
         DGPU_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, E->st));
-        DGPU_CHECK_CUDA(cudaStreamSynchronize(E->st));
+        DGPU_CHECK_CUDA(host_wait(E->st));
         return DGPU_OK;
     }
     const void* src = nullptr;
@@ -1132,7 +1132,7 @@ extern "C" int dgpu_encoder_read(void* enc, int pnum, int what, int comp, void* 
         }
     }
     DGPU_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, E->st));
-    if (on_host == 1) DGPU_CHECK_CUDA(cudaStreamSynchronize(E->st));
+    if (on_host == 1) DGPU_CHECK_CUDA(host_wait(E->st));
     return DGPU_OK;
 }
 

@@ -2265,7 +2265,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
             DGPU_CHECK_CUDA(cudaMemcpyAsync(hmv(t), A.mv_out[t], sizeof(short2) * nref_of(t) * nb,
                                             cudaMemcpyDeviceToHost, st));
         DGPU_CHECK_CUDA(cudaMemcpyAsync(&err_host, ctl + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-        DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
+        DGPU_CHECK_CUDA(host_wait(st));
         if (err_host) return DGPU_ERR_CUDA;
         {
             const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
@@ -2468,7 +2468,7 @@ int run_batch(const MeGeometry& g, const BatchArgs& A, void* workspace, cudaStre
         }
     }
     DGPU_CHECK_CUDA(cudaMemcpyAsync(&err_host, ctl + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-    DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
+    DGPU_CHECK_CUDA(host_wait(st));
     if (err_host) return DGPU_ERR_CUDA;
     tm.flush();
     return DGPU_OK;

@@ -1056,7 +1056,7 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     DGPU_CHECK_CUDA(cudaMemcpyAsync(hs, d_stats, sizeof(Stat) * n_pat, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaMemcpyAsync(hmax, d_band_max, sizeof(int) * nb_total, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaMemcpyAsync(hcb, d_cb_max, sizeof(int) * ncb_total, cudaMemcpyDeviceToHost, st));
-    DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
+    DGPU_CHECK_CUDA(host_wait(st));
     // Statistics of (band t, pattern, q): pattern 0 at hs[t * QMAX + q]; pattern 1 (only the
     // three quantisers of the band's range) at hs3[t * 3 + q - lo].  Sums the exact path could
     // not represent were replaced on the device by the reference's sequential double sums.
@@ -1121,7 +1121,7 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     seq_resolve_kernel<<<resolve_grid(3 * nb_total), 128, 0, st>>>(d_tasks, d_stats3, 3 * nb_total, 1, d_range);
     DGPU_CHECK_LAUNCH();
     DGPU_CHECK_CUDA(cudaMemcpyAsync(hs3, d_stats3, sizeof(Stat) * 3 * nb_total, cudaMemcpyDeviceToHost, st));
-    DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
+    DGPU_CHECK_CUDA(host_wait(st));
     std::vector<uint8_t> hskip(ncb_total, 0);
     parallel_for(nb_total, 64, [&](int t0, int t1) {
     for (int t = t0; t < t1; ++t) {

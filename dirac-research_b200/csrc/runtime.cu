@@ -124,6 +124,46 @@ HostPool& host_pool() {
 
 }  // namespace
 
+// Blocking waits (dgpu_set_blocking_waits, default off): host_wait sleeps on an event created
+// with cudaEventBlockingSync instead of polling the stream, which leaves the host cores to
+// other threads while many streams wait at once, at the cost of a later wake-up.
+std::atomic<int> g_blocking_waits{0};
+
+namespace {
+
+// One blocking-sync event per device for each host thread, destroyed when the thread ends.
+struct WaitEvents {
+    std::vector<cudaEvent_t> ev;
+    ~WaitEvents() {
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+};
+
+}  // namespace
+
+cudaError_t host_wait(cudaStream_t st) {
+    if (!g_blocking_waits.load(std::memory_order_relaxed)) return cudaStreamSynchronize(st);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    thread_local WaitEvents T;
+    if ((int)T.ev.size() <= dev) T.ev.resize((size_t)dev + 1, nullptr);
+    if (!T.ev[dev]) {
+        e = cudaEventCreateWithFlags(&T.ev[dev], cudaEventDisableTiming | cudaEventBlockingSync);
+        if (e != cudaSuccess) {
+            T.ev[dev] = nullptr;
+            return e;
+        }
+    }
+    if (cudaEventRecord(T.ev[dev], st) != cudaSuccess) {
+        // a stream of another device than the current one: wait on the stream itself
+        cudaGetLastError();
+        return cudaStreamSynchronize(st);
+    }
+    return cudaEventSynchronize(T.ev[dev]);
+}
+
 void parallel_for(int n, int grain, const std::function<void(int, int)>& body) {
     if (n <= 0) return;
     grain = std::max(1, grain);
@@ -153,6 +193,12 @@ void parallel_for(int n, int grain, const std::function<void(int, int)>& body) {
 }  // namespace dgpu
 
 extern "C" const char* dgpu_version(void) { return "dirac-b200 0.1 (sm_100a)"; }
+
+extern "C" int dgpu_set_blocking_waits(int on) {
+    if (on != 0 && on != 1) return DGPU_ERR_ARG;
+    dgpu::g_blocking_waits.store(on);
+    return DGPU_OK;
+}
 
 extern "C" const char* dgpu_last_error(void) { return dgpu::g_last_error; }
 

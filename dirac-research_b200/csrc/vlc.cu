@@ -228,7 +228,7 @@ extern "C" int dgpu_code_bands_vlc(int n, const int* depth, const int32_t* const
     DGPU_CHECK_LAUNCH();
     std::vector<long long> bits(nblk);
     DGPU_CHECK_CUDA(cudaMemcpyAsync(bits.data(), d_bits, sizeof(long long) * nblk, cudaMemcpyDeviceToHost, st));
-    DGPU_CHECK_CUDA(cudaStreamSynchronize(st));
+    DGPU_CHECK_CUDA(host_wait(st));
     // bit offsets: each band starts on a byte boundary
     std::vector<long long> bbits(g, 0);
     for (int i = 0; i < nblk; ++i) bbits[band_of[i]] += bits[i];

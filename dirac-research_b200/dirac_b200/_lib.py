@@ -88,6 +88,7 @@ SIGNATURES = {
     "dgpu_me_profile": (c_int, [c_int, c_void_p, c_void_p]),
     "dgpu_me_set_occupancy": (c_int, [c_int]),
     "dgpu_me_set_unit_lifetime": (c_int, [c_int]),
+    "dgpu_set_blocking_waits": (c_int, [c_int]),
     "dgpu_debug_wavefront": (c_int, [c_int, ctypes.c_longlong, c_void_p, c_void_p, c_void_p, c_void_p]),
     "dgpu_me_workspace_bytes": (c_size_t, [c_int, c_int, c_int, c_void_p, c_int]),
     "dgpu_me_batch_workspace_bytes": (c_size_t, [c_int, c_int, c_int, c_void_p, c_int, c_int, P_int, c_int]),
