@@ -86,8 +86,8 @@ def parse_args():
                     help="CUDA stream priority of the sequences' coding streams (negative: above the encoder "
                          "groups' estimation streams, which run at the default 0)")
     ap.add_argument("--blocking-waits", type=int, default=0,
-                    help="1: the library's host waits for the device sleep on blocking-sync events (measured "
-                         "slower: the plain form loses a third); 0: they poll")
+                    help="the library's host waits for the device: 0 poll, 1 sleep on blocking-sync events "
+                         "(measured slower: the plain form loses a third), 2 poll and yield (measured no faster)")
     ap.add_argument("--me-groups", type=int, default=3,
                     help="encoder groups the batched form's sequences are split into (run concurrently)")
     ap.add_argument("--double-buffer", type=int, default=0,

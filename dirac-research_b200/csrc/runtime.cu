@@ -5,6 +5,7 @@
 #include <atomic>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <deque>
 #include <mutex>
 #include <thread>
@@ -117,16 +118,27 @@ class HostPool {
     bool stop_ = false;
 };
 
+// Workers of the host pool: DGPU_HOST_THREADS when set (1..256, read once, when the pool is
+// first used), else one fewer than the hardware threads, at most 15.
+int host_pool_size() {
+    if (const char* v = std::getenv("DGPU_HOST_THREADS")) {
+        const int n = std::atoi(v);
+        if (n >= 1 && n <= 256) return n;
+    }
+    return std::max(1, std::min(15, (int)std::thread::hardware_concurrency() - 1));
+}
+
 HostPool& host_pool() {
-    static HostPool pool(std::max(1, std::min(15, (int)std::thread::hardware_concurrency() - 1)));
+    static HostPool pool(host_pool_size());
     return pool;
 }
 
 }  // namespace
 
-// Blocking waits (dgpu_set_blocking_waits, default off): host_wait sleeps on an event created
-// with cudaEventBlockingSync instead of polling the stream, which leaves the host cores to
-// other threads while many streams wait at once, at the cost of a later wake-up.
+// Wait mode (dgpu_set_blocking_waits): 0 (default) polls the stream; 1 sleeps on an event
+// created with cudaEventBlockingSync; 2 polls and yields the core between polls.  Modes 1 and
+// 2 leave the host cores to other threads while many streams wait at once, mode 1 at the cost
+// of a later wake-up.
 std::atomic<int> g_blocking_waits{0};
 
 namespace {
@@ -143,7 +155,16 @@ struct WaitEvents {
 }  // namespace
 
 cudaError_t host_wait(cudaStream_t st) {
-    if (!g_blocking_waits.load(std::memory_order_relaxed)) return cudaStreamSynchronize(st);
+    const int mode = g_blocking_waits.load(std::memory_order_relaxed);
+    if (mode == 0) return cudaStreamSynchronize(st);
+    if (mode == 2) {
+        // poll, handing the core to any other runnable thread between polls
+        for (;;) {
+            const cudaError_t q = cudaStreamQuery(st);
+            if (q != cudaErrorNotReady) return q;
+            std::this_thread::yield();
+        }
+    }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -195,7 +216,7 @@ void parallel_for(int n, int grain, const std::function<void(int, int)>& body) {
 extern "C" const char* dgpu_version(void) { return "dirac-b200 0.1 (sm_100a)"; }
 
 extern "C" int dgpu_set_blocking_waits(int on) {
-    if (on != 0 && on != 1) return DGPU_ERR_ARG;
+    if (on < 0 || on > 2) return DGPU_ERR_ARG;
     dgpu::g_blocking_waits.store(on);
     return DGPU_OK;
 }

@@ -68,10 +68,11 @@ unsigned long long dgpu_launch_count(void);
 /* How the library's host threads wait for the device where a call needs a result on the host
  * (the quantiser's round trips, motion-estimation error words, host reads): 0 (the default)
  * polls the stream (cudaStreamSynchronize under the default device flags), 1 sleeps on an
- * event created with cudaEventBlockingSync.  Sleeping leaves the host cores to other threads
- * when many streams wait at once; polling wakes sooner, which a sequence coded alone, with
- * two quantiser round trips per picture, needs.  Process-wide; DGPU_ERR_ARG for other
- * values.  No counterpart in the reference. */
+ * event created with cudaEventBlockingSync, 2 polls with cudaStreamQuery and yields the core
+ * between polls.  Sleeping or yielding leaves the host cores to other threads when many
+ * streams wait at once; polling wakes sooner, which a sequence coded alone, with two
+ * quantiser round trips per picture, needs.  Process-wide; DGPU_ERR_ARG for other values.
+ * No counterpart in the reference. */
 int dgpu_set_blocking_waits(int on);
 
 /* Measures, on the current device, the rate of the integer block-difference operation

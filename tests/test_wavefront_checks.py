@@ -177,9 +177,9 @@ def test_blocking_waits_switch():
     from dirac_b200 import _lib
 
     lib = _lib.load()
-    assert lib.dgpu_set_blocking_waits(2) == -1 and lib.dgpu_set_blocking_waits(-1) == -1
-    assert lib.dgpu_set_blocking_waits(0) == 0
-    assert lib.dgpu_set_blocking_waits(1) == 0
+    assert lib.dgpu_set_blocking_waits(3) == -1 and lib.dgpu_set_blocking_waits(-1) == -1
+    for mode in (1, 2, 0):
+        assert lib.dgpu_set_blocking_waits(mode) == 0
 
 
 def test_wavefront_occupancy_rejects_out_of_range_values():
