@@ -72,7 +72,11 @@ unsigned long long dgpu_launch_count(void);
  * between polls.  Sleeping or yielding leaves the host cores to other threads when many
  * streams wait at once; polling wakes sooner, which a sequence coded alone, with two
  * quantiser round trips per picture, needs.  Process-wide; DGPU_ERR_ARG for other values.
- * No counterpart in the reference. */
+ * No counterpart in the reference.
+ *
+ * The library's host worker pool (band coding, the quantiser's Lagrangian) has one worker
+ * fewer than the hardware threads, at most 15, or DGPU_HOST_THREADS (1..256) workers when
+ * that environment variable is set before the pool's first use. */
 int dgpu_set_blocking_waits(int on);
 
 /* Measures, on the current device, the rate of the integer block-difference operation
