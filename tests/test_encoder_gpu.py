@@ -128,6 +128,25 @@ def test_encoder_slot_reuse(gpu):
     compare(infos, results, oracle_run(cfg, seq))
 
 
+@pytest.mark.parametrize("mode", [1, 2], ids=["sleep", "yield"])
+def test_encoder_host_wait_modes(gpu, mode):
+    """dgpu_set_blocking_waits changes only how host threads wait for the device: a sequence
+    coded with waits that sleep on a blocking-sync event, or poll and yield, gives the oracle's
+    pictures."""
+    from dirac_b200 import synth
+
+    lib = gpu.load()
+    seq = synth.make_sequence(176, 144, 8, n_rects=5, vmax=5, seed=37)
+    cfg = dict(cformat=2, width=176, height=144, qf=6.0, l1_sep=3, num_l1=2, cpd=20.0, xblen=12, yblen=12, xbsep=8,
+               ybsep=8, mv_precision=2, intra_filter=1, inter_filter=0, wlt_depth=3)
+    try:
+        assert lib.dgpu_set_blocking_waits(mode) == 0
+        infos, results = run_device(gpu, seq, cfg, read_each=True)
+    finally:
+        assert lib.dgpu_set_blocking_waits(0) == 0
+    compare(infos, results, oracle_run(cfg, seq))
+
+
 def test_encoder_caller_entropy_factors(gpu):
     """Entropy-correction factors supplied per picture by the caller (as the host arithmetic
     coder's adaptation would) reach the quantiser choice exactly as in the oracle."""
