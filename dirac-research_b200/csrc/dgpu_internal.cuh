@@ -49,6 +49,16 @@ int library_scratch(size_t bytes, void* stream, void** out);
 // every chunk is done.  Small ranges run inline.
 void parallel_for(int n, int grain, const std::function<void(int, int)>& body);
 
+// dgpu_code_residue_batch, also giving the largest band maximum M of the call (max_coeff, may
+// be NULL; INT_MAX when the call failed before reading the band maxima).  In a component
+// without intra prediction M is its largest |coefficient|, and every quantised index is at
+// most M; an intra component's DC band enters with the maximum of its DPCM differences, so M
+// bounds none of its DC prediction residues.
+int code_residue_batch(int n, const int* intra, const int* depth, int32_t* const* coeff, const int* cw, const int* ch,
+                       const float* lambda, const float* band_wt, const float* band_ecf, const int* band_ncb,
+                       int* band_qidx, int* band_skip, int* band_bits, uint8_t* cb_skip, int32_t* const* qout,
+                       void* workspace, size_t ws_bytes, void* stream, int* max_coeff);
+
 // Waits for the work queued on st so far (cudaStreamSynchronize; with blocking waits switched
 // on, the thread sleeps on a blocking-sync event instead of polling).
 cudaError_t host_wait(cudaStream_t st);

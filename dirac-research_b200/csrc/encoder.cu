@@ -23,6 +23,7 @@
 // creation.  A 1080p 4:2:0 slot is about 64 MB.
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -95,6 +96,26 @@ __global__ void count_intra_kernel(const __grid_constant__ CountArgs A, int* __r
     }
 }
 
+// The three components' quantised indices narrowed to int16, laid end to end in dst; an index
+// outside int16 sets *overflow (the caller's coefficient bound rules that out: a check).
+struct NarrowArgs {
+    const int32_t* src[3];
+    int n[3];  // elements per component
+};
+
+__global__ void narrow_kernel(const __grid_constant__ NarrowArgs A, int16_t* __restrict__ dst,
+                              int* __restrict__ overflow) {
+    const int n01 = A.n[0] + A.n[1], total = n01 + A.n[2];
+    bool bad = false;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int c = i < A.n[0] ? 0 : (i < n01 ? 1 : 2);
+        const int v = A.src[c][i - (c == 0 ? 0 : (c == 1 ? A.n[0] : n01))];
+        bad |= v < -32768 || v > 32767;
+        dst[i] = (int16_t)v;
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(overflow, 1);
+}
+
 // ---------------------------------------------------------------------------------------
 // host structures
 // ---------------------------------------------------------------------------------------
@@ -125,6 +146,7 @@ struct Pic {
     dgpu_picture_info info{};
     std::vector<int> bands;        // [3][nb][3]
     std::vector<uint8_t> cb_skip;  // [3][ncb]
+    int coeff_max = INT_MAX;       // the quantiser's largest band maximum (INT_MAX: unknown)
 
     bool is_b() const {
         return refs.size() == 2 && ((refs[0] < pnum && refs[1] > pnum) || (refs[0] > pnum && refs[1] < pnum));
@@ -183,6 +205,9 @@ struct Encoder {
     uint8_t* kind_stage[3] = {};
     size_t kind_stage_bytes[3] = {};
     cudaEvent_t kind_ev[3] = {};
+    // the three components' indices narrowed to int16 for the copy, then the overflow flag
+    void* q16 = nullptr;
+    size_t q16_bytes = 0;
     std::vector<uint8_t> adaptive_data;  // the last call's coded data, coding order
 
     ~Encoder() {
@@ -192,6 +217,7 @@ struct Encoder {
             if (kind_ev[k]) cudaEventDestroy(kind_ev[k]);
             if (kind_stage[k]) cudaFreeHost(kind_stage[k]);
         }
+        if (q16) cudaFree(q16);
         if (arena) cudaFree(arena);
         if (h_counts) cudaFreeHost(h_counts);
     }
@@ -563,9 +589,9 @@ int code_residue(Encoder& E, Pic& p, const float* ecf_in, bool forward_done = fa
     if (rc) return rc;
     {
         StageTimer timer(E, DGPU_STAGE_QUANT);
-        rc = dgpu_code_residue_batch(3, intra, dep, coeff, E.pw, E.ph, lam, wt.data(), ecf.data(), ncb.data(),
-                                     qidx.data(), skip.data(), bits.data(), p.cb_skip.data(), qout, E.q_ws,
-                                     E.q_ws_bytes, E.st);
+        rc = code_residue_batch(3, intra, dep, coeff, E.pw, E.ph, lam, wt.data(), ecf.data(), ncb.data(), qidx.data(),
+                                skip.data(), bits.data(), p.cb_skip.data(), qout, E.q_ws, E.q_ws_bytes, E.st,
+                                &p.coeff_max);
     }
     if (rc) return rc;
     rc = transform(E, p, DGPU_BACKWARD, filter);
@@ -1145,6 +1171,7 @@ namespace {
 // One finished picture on its way through the host band coder.
 struct CodedPicture {
     dgpu_picture_info info{};
+    bool idx16 = false;            // indices staged as int16 (then the overflow flag)
     std::vector<int> bands;        // [3][nb][3] quantiser index, skip, estimated bits
     std::vector<uint8_t> cb_skip;  // [3][ncb_total]
     std::vector<uint8_t> data;     // coded subbands (dgpu_code_bands_host's layout)
@@ -1155,11 +1182,19 @@ struct CodedPicture {
 int code_picture(const Encoder& E, CodedPicture& C, const uint8_t* stage, float* ecf_state) {
     const int nb = E.nb, depth = E.P.wlt_depth;
     const int intra[3] = {C.info.intra, C.info.intra, C.info.intra}, dep[3] = {depth, depth, depth};
-    const int32_t* q[3];
+    const void* q[3];
     size_t off = 0;
     for (int c = 0; c < 3; ++c) {
-        q[c] = reinterpret_cast<const int32_t*>(stage + off);
-        off += (size_t)E.pw[c] * E.ph[c] * 4;
+        q[c] = stage + off;
+        off += (size_t)E.pw[c] * E.ph[c] * (C.idx16 ? 2 : 4);
+    }
+    // the narrowing's overflow flag: set only if the coefficient bound failed
+    if (C.idx16 && *reinterpret_cast<const int*>(stage + align_up(off, 16))) return DGPU_ERR_CUDA;
+    const int16_t* q16[3];
+    const int32_t* q32[3];
+    for (int c = 0; c < 3; ++c) {
+        q16[c] = static_cast<const int16_t*>(q[c]);
+        q32[c] = static_cast<const int32_t*>(q[c]);
     }
     std::vector<int> ncb3(6 * nb), qidx(3 * nb), skip(3 * nb), est(3 * nb);
     for (int c = 0; c < 3; ++c)
@@ -1174,8 +1209,11 @@ int code_picture(const Encoder& E, CodedPicture& C, const uint8_t* stage, float*
     size_t cap = C.data.size() ? C.data.size() : (size_t)E.pw[0] * E.ph[0] / 4 + 4096;
     for (;;) {
         C.data.resize(cap);
-        const int rc = dgpu_code_bands_host(3, intra, dep, q, E.pw, E.ph, ncb3.data(), qidx.data(), skip.data(),
-                                            C.cb_skip.data(), C.data.data(), cap, C.band_bytes.data());
+        const int rc =
+            C.idx16 ? dgpu_code_bands_host16(3, intra, dep, q16, E.pw, E.ph, ncb3.data(), qidx.data(), skip.data(),
+                                             C.cb_skip.data(), C.data.data(), cap, C.band_bytes.data())
+                    : dgpu_code_bands_host(3, intra, dep, q32, E.pw, E.ph, ncb3.data(), qidx.data(), skip.data(),
+                                           C.cb_skip.data(), C.data.data(), cap, C.band_bytes.data());
         if (rc == DGPU_OK) break;
         if (rc != DGPU_ERR_SIZE) return rc;
         size_t need = 0;
@@ -1240,11 +1278,19 @@ extern "C" int dgpu_encoder_code_adaptive(void* enc, float* ecf_state, int max_p
         const Pic& p = E->pics[pn];
         C->bands = p.bands;
         C->cb_skip = p.cb_skip;
-        // indices and motion data into the kind's page-locked buffer, without waiting
+        // indices and motion data into the kind's page-locked buffer, without waiting.  An
+        // inter picture's indices are at most its largest |coefficient| (no DC prediction):
+        // when that fits int16 they go as int16, followed by the narrowing's overflow flag;
+        // an intra picture's (DC prediction residues) go as int32.
+        const bool idx16 = !C->info.intra && p.coeff_max <= 32767;
+        C->idx16 = idx16;
+        size_t nq = 0;
+        for (int c = 0; c < 3; ++c) nq += (size_t)E->pw[c] * E->ph[c];
+        const size_t q16_off = align_up(nq * 2, 16);  // the flag's offset
         const int items[] = {DGPU_ENC_QINDEX, DGPU_ENC_QINDEX, DGPU_ENC_QINDEX, DGPU_ENC_MV,
                              DGPU_ENC_MODE, DGPU_ENC_DC, DGPU_ENC_SPLIT};
-        size_t need = 0;
-        for (int k = 0; k < 7; ++k) need += dgpu_encoder_item_bytes(enc, pn, items[k], k < 3 ? k : 0);
+        size_t need = idx16 ? q16_off + 16 : 0;
+        for (int k = idx16 ? 3 : 0; k < 7; ++k) need += dgpu_encoder_item_bytes(enc, pn, items[k], k < 3 ? k : 0);
         if (E->kind_stage_bytes[kind] < need) {
             if (E->kind_stage[kind]) cudaFreeHost(E->kind_stage[kind]);
             E->kind_stage[kind] = nullptr;
@@ -1265,7 +1311,44 @@ extern "C" int dgpu_encoder_code_adaptive(void* enc, float* ecf_state, int max_p
             break;
         }
         size_t off = 0;
-        for (int k = 0; k < 7 && r >= 0; ++k) {
+        if (idx16) {
+            if (E->q16_bytes < q16_off + 16) {
+                if (E->q16) cudaFree(E->q16);
+                E->q16 = nullptr;
+                E->q16_bytes = 0;
+                if (cudaMalloc(&E->q16, q16_off + 16) != cudaSuccess) {
+                    cudaGetLastError();
+                    rc = DGPU_ERR_NOMEM;
+                    break;
+                }
+                E->q16_bytes = q16_off + 16;
+            }
+            const Slot& s = E->slots[p.slot];
+            NarrowArgs A;
+            for (int c = 0; c < 3; ++c) {
+                A.src[c] = s.qout[c];
+                A.n[c] = E->pw[c] * E->ph[c];
+            }
+            int16_t* d16 = static_cast<int16_t*>(E->q16);
+            int* dflag = reinterpret_cast<int*>(static_cast<char*>(E->q16) + q16_off);
+            if (cudaMemsetAsync(dflag, 0, sizeof(int), E->st) != cudaSuccess) {
+                cudaGetLastError();
+                rc = DGPU_ERR_CUDA;
+                break;
+            }
+            narrow_kernel<<<(int)std::min<size_t>((nq + 255) / 256, 148 * 8), 256, 0, E->st>>>(A, d16, dflag);
+            count_launch();
+            if (cudaGetLastError() != cudaSuccess ||
+                cudaMemcpyAsync(E->kind_stage[kind], d16, nq * 2, cudaMemcpyDeviceToHost, E->st) != cudaSuccess ||
+                cudaMemcpyAsync(E->kind_stage[kind] + q16_off, dflag, sizeof(int), cudaMemcpyDeviceToHost, E->st) !=
+                    cudaSuccess) {
+                cudaGetLastError();
+                rc = DGPU_ERR_CUDA;
+                break;
+            }
+            off = q16_off + 16;
+        }
+        for (int k = idx16 ? 3 : 0; k < 7 && r >= 0; ++k) {
             const size_t n = dgpu_encoder_item_bytes(enc, pn, items[k], k < 3 ? k : 0);
             if (n == 0) continue;
             r = dgpu_encoder_read(enc, pn, items[k], k < 3 ? k : 0, E->kind_stage[kind] + off, n, 2);
@@ -1275,7 +1358,7 @@ extern "C" int dgpu_encoder_code_adaptive(void* enc, float* ecf_state, int max_p
             rc = r;
             break;
         }
-        copied += off;
+        copied += idx16 ? off - (q16_off + 16) + nq * 2 + sizeof(int) : off;
         if (cudaEventRecord(E->kind_ev[kind], E->st) != cudaSuccess) {
             cudaGetLastError();
             rc = DGPU_ERR_CUDA;

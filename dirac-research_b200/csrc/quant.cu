@@ -21,6 +21,8 @@
 //   4. quantise and reconstruct in place; the intra DC band (prediction from reconstructed
 //      neighbours) as an anti-diagonal wavefront in one CTA.
 
+#include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -928,11 +930,13 @@ extern "C" size_t dgpu_code_residue_workspace_bytes(int n, const int* intra, con
     return residue_ws_need(nb_total, ncb_total, dcwork_elems);
 }
 
-extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth, int32_t* const* coeff,
-                                       const int* cw, const int* ch, const float* lambda, const float* band_wt,
-                                       const float* band_ecf, const int* band_ncb, int* band_qidx, int* band_skip,
-                                       int* band_bits, uint8_t* cb_skip, int32_t* const* qout, void* workspace,
-                                       size_t ws_bytes, void* stream) {
+namespace dgpu {
+
+int code_residue_batch(int n, const int* intra, const int* depth, int32_t* const* coeff, const int* cw, const int* ch,
+                       const float* lambda, const float* band_wt, const float* band_ecf, const int* band_ncb,
+                       int* band_qidx, int* band_skip, int* band_bits, uint8_t* cb_skip, int32_t* const* qout,
+                       void* workspace, size_t ws_bytes, void* stream, int* max_coeff) {
+    if (max_coeff) *max_coeff = INT_MAX;  // unknown until the band maxima are read
     if (n <= 0 || n > MAX_COMPS || !intra || !depth || !coeff || !cw || !ch || !lambda || !band_wt || !band_ecf ||
         !band_ncb || !band_qidx || !band_skip || !band_bits || !cb_skip)
         return DGPU_ERR_ARG;
@@ -1057,6 +1061,7 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     DGPU_CHECK_CUDA(cudaMemcpyAsync(hmax, d_band_max, sizeof(int) * nb_total, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(cudaMemcpyAsync(hcb, d_cb_max, sizeof(int) * ncb_total, cudaMemcpyDeviceToHost, st));
     DGPU_CHECK_CUDA(host_wait(st));
+    if (max_coeff) *max_coeff = nb_total ? *std::max_element(hmax, hmax + nb_total) : 0;
     // Statistics of (band t, pattern, q): pattern 0 at hs[t * QMAX + q]; pattern 1 (only the
     // three quantisers of the band's range) at hs3[t * 3 + q - lo].  Sums the exact path could
     // not represent were replaced on the device by the reference's sequential double sums.
@@ -1209,6 +1214,17 @@ extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth
     quantise_kernel<<<qchunks, ROW_THREADS, 0, st>>>(d_qbands, (int)qb.size());
     DGPU_CHECK_LAUNCH();
     return DGPU_OK;
+}
+
+}  // namespace dgpu
+
+extern "C" int dgpu_code_residue_batch(int n, const int* intra, const int* depth, int32_t* const* coeff,
+                                       const int* cw, const int* ch, const float* lambda, const float* band_wt,
+                                       const float* band_ecf, const int* band_ncb, int* band_qidx, int* band_skip,
+                                       int* band_bits, uint8_t* cb_skip, int32_t* const* qout, void* workspace,
+                                       size_t ws_bytes, void* stream) {
+    return code_residue_batch(n, intra, depth, coeff, cw, ch, lambda, band_wt, band_ecf, band_ncb, band_qidx,
+                              band_skip, band_bits, cb_skip, qout, workspace, ws_bytes, stream, nullptr);
 }
 
 namespace {

@@ -653,7 +653,10 @@ int dgpu_encoders_estimate(void* const* encoders, int n, void* workspace, size_t
  * (intra, B, other inter), so a picture waits only for the host coding of the last picture of
  * its kind: the coding runs on host threads while the pictures after it are prepared and
  * finished on the device, their indices and motion data copied to page-locked memory without
- * a wait.  The results equal a serial loop of dgpu_encoder_code_next_adaptive and
+ * a wait.  An inter picture whose largest |coefficient| fits 16 bits (so does every index:
+ * no DC prediction) has its indices narrowed to int16 on the device and copied at half the
+ * bytes (dgpu_code_bands_host16); intra pictures' go as int32.  The results equal a serial
+ * loop of dgpu_encoder_code_next_adaptive and
  * dgpu_code_bands_host.  At most max_pictures pictures (DGPU_ERR_SIZE beyond); per picture in
  * coding order: infos (optional), band_bytes (optional, [3][3*depth+1] as
  * dgpu_code_bands_host), its coded data in out (optional); out_bytes receives the data's total

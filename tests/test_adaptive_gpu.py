@@ -185,6 +185,7 @@ def _pipelined_outputs(seq, cfg, native=False):
     if native:
         # every picture keeps its slot (max_pictures = the sequence), so outputs are read after
         infos, data, bb = coder.run_native(max_pictures=len(seq))
+        coded["d2h_bytes"] = coder.d2h_bytes
         for info, d, b in zip(infos, data, bb):
             fin(info)
             coded[info["pnum"]] = (zlib.crc32(d.tobytes()), [int(x) for x in b.ravel()])
@@ -220,5 +221,51 @@ def test_kind_pipelined_coder_matches_stock_reference(gpu, golden, case):
     # the library's own pipeline (dgpu_encoder_code_adaptive): same pictures, same coded bytes
     ncrc, ninfos, ncoded = _pipelined_outputs(seq, cfg, native=True)
     np.testing.assert_array_equal(ncrc, want)
+    assert [i["pnum"] for i in ninfos] == [i["pnum"] for i in infos]
+    d2h = ncoded.pop("d2h_bytes")
+    assert ncoded == coded
+    # inter pictures' indices went as int16: fewer bytes than every picture's int32 indices
+    n_idx = sum(a * b for a, b in _padded(cfg))
+    n_inter = sum(1 for i in ninfos if not i["intra"])
+    assert n_inter > 0 and d2h <= 4 * n_idx * len(ninfos) - 2 * n_idx * n_inter + 64 * len(ninfos) + \
+        _motion_bytes(cfg) * len(ninfos)
+
+
+def _padded(cfg):
+    m = 1 << cfg["wlt_depth"]
+    out = []
+    for c in range(3):
+        w = cfg["width"] >> (0 if c == 0 or cfg["cformat"] == 0 else 1)
+        h = cfg["height"] >> (1 if c and cfg["cformat"] == 2 else 0)
+        out.append(((h + m - 1) // m * m, (w + m - 1) // m * m))
+    return out
+
+
+def _motion_bytes(cfg):
+    """Upper bound of one picture's motion-data bytes (two vector sets, modes, DCs, splits)."""
+    xsb = (cfg["width"] + 4 * cfg["xbsep"] - 1) // (4 * cfg["xbsep"])
+    ysb = (cfg["height"] + 4 * cfg["ybsep"] - 1) // (4 * cfg["ybsep"])
+    nb = 16 * xsb * ysb
+    return nb * (2 * 4 + 1 + 3 * 2) + xsb * ysb
+
+
+def test_native_pipeline_wide_residues_match_python_pipeline(gpu):
+    """14-bit noise: inter residues whose coefficients exceed 16 bits, so some inter pictures'
+    indices go as int32 and others may go as int16.  The library's pipeline codes the same bytes
+    and pictures as the Python pipeline, which reads every picture's int32 indices."""
+    from test_encoder_gpu import encoder_params
+
+    rng = np.random.default_rng(23)
+    w, h, n = 128, 96, 7
+    seq = [tuple(rng.integers(0, 1 << 14, size=(h >> (c > 0), w >> (c > 0))).astype(np.uint16) for c in range(3))
+           for _ in range(n)]
+    cfg = encoder_params(dict(cformat=2, width=w, height=h, qf=9.0, l1_sep=3, num_l1=1, cpd=20.0, xblen=12,
+                              yblen=12, xbsep=8, ybsep=8, mv_precision=2, intra_filter=1, inter_filter=4,
+                              wlt_depth=4))
+    cfg.update(luma_depth=14, chroma_depth=14)
+    crc, infos, coded = _pipelined_outputs(seq, cfg)
+    ncrc, ninfos, ncoded = _pipelined_outputs(seq, cfg, native=True)
+    ncoded.pop("d2h_bytes")
+    np.testing.assert_array_equal(ncrc, crc)
     assert [i["pnum"] for i in ninfos] == [i["pnum"] for i in infos]
     assert ncoded == coded
