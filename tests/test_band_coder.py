@@ -83,6 +83,37 @@ def test_band_coder_matches_reference_on_adversarial_indices(kind):
         assert data.tobytes() == want.tobytes(), kind
 
 
+_POOL_SNIPPET = """
+import sys, zlib
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from dirac_b200 import quant
+from dirac_b200.entropy import code_bands
+rng = np.random.default_rng(77)
+depth, cw, ch = 3, 128, 96
+q = rng.integers(-40, 41, size=(ch, cw)).astype(np.int32)
+q[rng.random((ch, cw)) < 0.7] = 0
+ncb = np.asarray(quant.code_blocks(depth, cw, ch), np.int32).reshape(-1, 2)
+bands = np.zeros((3 * depth + 1, 2), np.int32)
+cbs = np.zeros(int((ncb[:, 0] * ncb[:, 1]).sum()), np.uint8)
+data, per = code_bands(0, depth, [q, q[::-1].copy(), -q], [bands] * 3, [ncb] * 3, [cbs] * 3)
+print(zlib.crc32(data.tobytes()), [int(x) for p in per for x in p])
+"""
+
+
+@pytest.mark.parametrize("threads", ["1", "3"])
+def test_host_pool_size_variable(threads):
+    """DGPU_HOST_THREADS sizes the library's host pool when it is first used: the coded bands do
+    not depend on it (a fresh process per setting, against the default pool)."""
+    import subprocess
+
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "dirac-research_b200")
+    run = lambda env: subprocess.run([sys.executable, "-c", _POOL_SNIPPET, pkg], env=env, capture_output=True,  # noqa: E731
+                                     text=True, timeout=120, check=True).stdout
+    base = {k: v for k, v in os.environ.items() if k != "DGPU_HOST_THREADS"}
+    assert run(dict(base, DGPU_HOST_THREADS=threads)) == run(base)
+
+
 @pytest.mark.parametrize("k", range(len(BAND_CASES)))
 def test_band_data_matches_reference_fixture(oracle, golden, k):
     from dirac_b200.entropy import code_bands
