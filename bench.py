@@ -967,7 +967,8 @@ def main():
            "coded_band_bytes_per_step": sum(ln.coder.coded_bytes for ln in lanes) // args.steps,
            "form": "stock choices: adaptive entropy-correction factors, subbands arithmetic-coded on the host",
            "pipeline": "dgpu_encoder_code_adaptive: a picture waits only for the host coding of the last "
-                       "picture of its kind (intra, B, other inter), whose factors it reads",
+                       "picture of its kind (intra, B, other inter), whose factors it reads; inter pictures' "
+                       "indices copied as int16 when their coefficients fit",
            "group_ms_per_step": {k: round(1000.0 * v / (args.steps * len(groups)), 2) for k, v in group_phases.items()},
            "host_cpu": {"cores_busy": round(cpu_s / (w1 - w0), 2), "cores": os.cpu_count(),
                         "ms_per_picture": round(1000.0 * cpu_s / (frames_per_step * args.steps), 3)}}
