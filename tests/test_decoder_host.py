@@ -95,3 +95,8 @@ def test_decode_bytes_model():
     assert b["dwt_inverse"] == 3 * (dwt_bytes(64, 32, 2) + 2 * dwt_bytes(32, 16, 2))
     assert b["mc_add_clip"] == samples * 4 + samples * (4 + 8) + samples * (4 + 16)
     assert b["upconvert"] == 2 * samples * 10
+    # pictures decoded from int16 indices read 2 B instead of 4 per coefficient
+    b16 = decode_bytes(params, infos, int16_pictures=2)
+    assert b16["dequantisation"] == 3 * 8 * coeffs - 2 * 2 * coeffs
+    assert {k: v for k, v in b16.items() if k != "dequantisation"} == \
+        {k: v for k, v in b.items() if k != "dequantisation"}
